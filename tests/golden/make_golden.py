@@ -1,0 +1,224 @@
+"""Generate the golden fixtures by running the reference afsi-torch 0.28.0 on CPU.
+
+Run from the repository root in a container where the reference source tree is
+available (it is not needed afterwards; the fixtures are committed):
+
+    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py [REFERENCE_SRC]
+
+REFERENCE_SRC defaults to ``/root/reference/src``.  Every fixture is produced by
+the reference's own public functions or the CPU expressions its classes use;
+inputs are seeded.  Outputs are small ``.npz`` files next to this script.
+"""
+import sys
+from pathlib import Path
+import numpy as np
+
+SRC = sys.argv[1] if len(sys.argv) > 1 else '/root/reference/src'
+sys.path.insert(0, SRC)
+import torch  # noqa: E402
+from afsi_torch import ib  # noqa: E402
+from afsi_torch.ib import peskin4  # noqa: E402
+from afsi_torch.mac.grid import MACGrid, negative_laplacian  # noqa: E402
+from afsi_torch.mac.compact_transfer import _prepare, CompactFETransfer  # noqa: E402
+from afsi_torch.mac.multigrid import GeometricMultigrid, MGOptions  # noqa: E402
+from afsi_torch.mac.mg_workspace import TensorKernels  # noqa: E402
+from afsi_torch.mac2d.grid import ChannelGrid  # noqa: E402
+from afsi_torch.mac2d.transfer import TriangleTransfer  # noqa: E402
+from afsi_torch.mac2d.multigrid import ChannelMultigrid  # noqa: E402
+from afsi_torch.mac2d.mg_workspace import TensorKernels as ChannelKernels  # noqa: E402
+from afsi_torch.mac.adaptive_transfer import (AdaptiveFETransfer, InteractionQuadratureOptions,  # noqa: E402
+                                              gaussian_tetra_rule)
+from afsi_torch.tetrahedron import reference_nodes, tabulate, promote_p1  # noqa: E402
+from afsi_torch.solid import prepare_p2  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+torch.set_default_dtype(torch.float64)
+
+
+def save(name, **arrays):
+    arrays = {k: (v.detach().cpu().numpy() if torch.is_tensor(v) else np.asarray(v)) for k, v in arrays.items()}
+    np.savez_compressed(OUT / f'{name}.npz', **arrays)
+    print(name, {k: v.shape for k, v in arrays.items()})
+
+
+def peskin():
+    d = torch.linspace(-2.5, 2.5, 1001)
+    d = torch.cat((d, torch.tensor([0., .5, 1., 1.5, 2., -1., -2., 1 - 1e-15, 1 + 1e-15])))
+    save('peskin', d=d, phi=peskin4(d))
+
+
+def compact3d():
+    g = torch.Generator().manual_seed(7)
+    grid = MACGrid((12, 14, 16), (2., 3., 5.), (-.2, .1, -.4))
+    h = torch.tensor(grid.spacing)
+    lo = torch.tensor(grid.origin) + 2.05 * h
+    hi = torch.tensor(grid.origin) + (torch.tensor(grid.shape) - 2.05) * h
+    pts = lo + (hi - lo) * torch.rand((300, 3), generator=g)
+    # a few points exactly on lattice knots / half knots
+    pts[:4] = torch.tensor(grid.origin) + h * torch.tensor([[3., 4., 5.], [3.5, 4.5, 5.5], [5., 6.5, 7.], [9.5, 9., 12.5]])
+    origins = torch.tensor([grid.face_origin(c) for c in range(3)])
+    shared = torch.tensor([grid.origin, tuple(o + .5 * s for o, s in zip(grid.origin, grid.spacing))])
+    offs = torch.arange(4)
+    base, phi = _prepare(pts, origins, h, offs)
+    sbase, sphi = _prepare(pts, shared, h, offs)
+    t = object.__new__(CompactFETransfer)
+    t.grid, t.axis_offsets, t.ib_backend = grid, offs, 'reference'
+    from afsi_torch.mac.compact_transfer import CompactStencil
+    st = CompactStencil(base.contiguous(), phi.contiguous())
+    force = torch.randn((300, 3), generator=g)
+    fields = t.spread_grid(force, st)
+    vel = tuple(torch.randn(grid.face_shape(c), generator=g) for c in range(3))
+    gathered = t.gather_grid(vel, st)
+    save('compact3d', shape=grid.shape, lengths=grid.lengths, origin=grid.origin, spacing=grid.spacing,
+         volume=grid.volume, points=pts, base=base, phi=phi, shared_base=sbase, shared_phi=sphi,
+         force=force, u0=fields[0], u1=fields[1], u2=fields[2], v0=vel[0], v1=vel[1], v2=vel[2],
+         gathered=gathered)
+
+
+def transfer2d():
+    g = torch.Generator().manual_seed(11)
+    grid = ChannelGrid((32, 16), (2., 1.))
+    hx, hy = grid.spacing
+    P = 400
+    x = 2 * hx + (grid.lengths[0] - 4 * hx) * torch.rand(P, generator=g)
+    y = -hy + (grid.lengths[1] + 2 * hy) * torch.rand(P, generator=g)   # includes wall halo
+    pts = torch.stack((x, y), -1)
+    t = object.__new__(TriangleTransfer)
+    t.grid = grid
+    t.offsets = torch.cartesian_prod(torch.arange(4), torch.arange(4))
+    ids, w = t._prepare(pts)
+    force = torch.randn((P, 2), generator=g)
+    spread = [torch.zeros(grid.face_shape(c)).reshape(-1).index_add(0, ids[c].reshape(-1),
+              (force[:, c, None] * w[c] / grid.volume).reshape(-1)) for c in range(2)]
+    vel = tuple(torch.randn(grid.face_shape(c), generator=g) for c in range(2))
+    gathered = torch.stack([(u.reshape(-1)[i] * ww).sum(-1) for u, i, ww in zip(vel, ids, w)], -1)
+    save('transfer2d', shape=grid.shape, lengths=grid.lengths, spacing=grid.spacing, volume=grid.volume,
+         points=pts, ids0=ids[0], ids1=ids[1], w0=w[0], w1=w[1], force=force, s0=spread[0], s1=spread[1],
+         v0=vel[0], v1=vel[1], gathered=gathered)
+
+
+def p2():
+    """Two P2 tetrahedra (promoted P1 pair), adaptive conical quadrature."""
+    g = torch.Generator().manual_seed(5)
+    X1 = torch.tensor([[0., 0., 0.], [1., 0., 0.], [0., 1., 0.], [0., 0., 1.], [2.2, 2.0, 2.1]]) * .4 + 1.7
+    c1 = torch.tensor([[0, 1, 2, 3], [1, 2, 3, 4]])
+    X, cells = promote_p1(X1, c1)
+    geometry = prepare_p2(X, cells)
+    grid = MACGrid((16, 12, 10), (5., 5.5, 6.), (-.2, .1, -.4))
+    opt = InteractionQuadratureOptions(mode='adaptive', point_density=3., max_order=22,
+                                       max_points=500000, rule_family='conical')
+    tr = AdaptiveFETransfer(grid, geometry, fused=False, ib_backend='reference', quadrature_options=opt)
+    x = X.clone()
+    x[4, 1] += .017
+    st = tr.prepare(x)
+    coef = torch.sin(1.3 * X)
+    force_q = torch.cat([tr._weighted_kernel(coef, gg.values, gg.cells, gg.weights) for gg in st.rule.groups])
+    fields = tr.spread_grid(force_q, st)
+    vel = tuple(torch.sin(grid.coordinates(c)[..., (c + 1) % 3]) for c in range(3))
+    gathered = tr.gather_grid(vel, st)
+    rhs = torch.zeros_like(tr.diagonal)
+    off = 0
+    for gg in st.rule.groups:
+        n = gg.weights.numel()
+        rhs += tr._assemble_kernel(gathered[off:off + n], gg.values, gg.cells, gg.weights, tr.diagonal)
+        off += n
+    groups = {}
+    for k, gg in enumerate(st.rule.groups):
+        groups[f'cells{k}'] = gg.cells
+        groups[f'N{k}'] = gg.values
+        groups[f'W{k}'] = gg.weights
+        groups[f'order{k}'] = gg.order
+    save('p2', shape=grid.shape, lengths=grid.lengths, origin=grid.origin, spacing=grid.spacing,
+         volume=grid.volume, X=X, x=x, ngroups=len(st.rule.groups), base=st.base, phi=st.phi,
+         coef=coef, force_q=force_q, u0=fields[0], u1=fields[1], u2=fields[2],
+         v0=vel[0], v1=vel[1], v2=vel[2], gathered=gathered, rhs=rhs, **groups)
+
+
+def mg3d():
+    from math import pi
+    grid = MACGrid((8, 12, 16), (2., 3., 4.))
+    options = MGOptions(smooth=3)
+    ref = GeometricMultigrid(grid, options=options)
+    xyz = grid.coordinates()
+    exact = torch.cos(pi * xyz[..., 0] / 2) * torch.cos(2 * pi * xyz[..., 1] / 3) * torch.cos(pi * xyz[..., 2] / 4)
+    exact -= exact.mean()
+    rhs = negative_laplacian(exact, grid.spacing)
+    start = .1 * exact
+    with torch.no_grad():
+        cyc = ref._cycle(0, start, rhs)
+    p, info = ref.solve(rhs, start)
+    k = TensorKernels()
+    g = torch.Generator().manual_seed(3)
+    pp = torch.randn(grid.shape, generator=g)
+    rr = torch.randn(grid.shape, generator=g)
+    res = torch.empty_like(pp)
+    k.residual(pp, rr, res, grid.spacing)
+    sm = torch.empty_like(pp)
+    k.smooth(pp, rr, ref.diagonals[0], sm, grid.spacing)
+    coarse = torch.empty(tuple(n // 2 for n in grid.shape))
+    k.restrict(pp, coarse)
+    rres = torch.empty_like(coarse)
+    k.residual_restrict(pp, rr, rres, grid.spacing)
+    pro = pp.clone()
+    k.prolong_add(coarse, pro)
+    # 64^3-style five level solve on a random mean-zero RHS
+    grid2 = MACGrid((16, 16, 32), (1., 1., 2.))
+    mg2 = GeometricMultigrid(grid2)
+    r2 = torch.randn(grid2.shape, generator=g)
+    r2 -= r2.mean()
+    p2, info2 = mg2.solve(r2)
+    save('mg3d', shape=grid.shape, lengths=grid.lengths, spacing=grid.spacing, smooth=3,
+         rhs=rhs, start=start, cycle=cyc, solution=p, cycles=info['cycles'], diag0=ref.diagonals[0],
+         coarse_inverse=ref.coarse_inverse, pp=pp, rr=rr, residual=res, smoothed=sm, restricted=coarse,
+         residual_restricted=rres, prolonged=pro,
+         shape2=grid2.shape, lengths2=grid2.lengths, rhs2=r2, solution2=p2, cycles2=info2['cycles'],
+         residual2=info2['residual_norm'])
+
+
+def mg2d():
+    g = torch.Generator().manual_seed(13)
+    grid = ChannelGrid((32, 16), (2., 1.))
+    mg = ChannelMultigrid(grid, fused=False)
+    rhs = torch.randn(grid.shape, generator=g)
+    start = .1 * torch.randn(grid.shape, generator=g)
+    with torch.no_grad():
+        cyc = mg._cycle(0, start, rhs)
+    p, info = mg.solve(rhs)
+    k = ChannelKernels()
+    pp = torch.randn(grid.shape, generator=g)
+    res = torch.empty_like(pp)
+    k.residual(pp, rhs, res, grid.spacing)
+    sm = torch.empty_like(pp)
+    k.smooth(pp, rhs, mg.diagonals[0], sm, grid.spacing)
+    rres = torch.empty(tuple(n // 2 for n in grid.shape))
+    k.residual_restrict(pp, rhs, rres, grid.spacing)
+    pro = pp.clone()
+    k.prolong_add(rres, pro)
+    big = ChannelGrid((256, 64), (8., 1.61))
+    mgb = ChannelMultigrid(big, fused=False)
+    rb = torch.randn(big.shape, generator=g)
+    pb, infob = mgb.solve(rb)
+    save('mg2d', shape=grid.shape, lengths=grid.lengths, spacing=grid.spacing, rhs=rhs, start=start,
+         cycle=cyc, solution=p, cycles=info['cycles'], diag0=mg.diagonals[0], inverse=mg.inverse,
+         pp=pp, residual=res, smoothed=sm, residual_restricted=rres, prolonged=pro,
+         shape_b=big.shape, lengths_b=big.lengths, rhs_b=rb, solution_b=pb, cycles_b=infob['cycles'])
+
+
+def quadrature():
+    arrays = {}
+    like = torch.zeros(1)
+    for n in range(2, 9):
+        q, w = gaussian_tetra_rule(n, like, 'conical')
+        N, _ = tabulate(q)
+        arrays[f'q{n}'], arrays[f'w{n}'], arrays[f'N{n}'] = q, w, N
+    save('quadrature', **arrays)
+
+
+if __name__ == '__main__':
+    peskin()
+    compact3d()
+    transfer2d()
+    p2()
+    mg3d()
+    mg2d()
+    quadrature()
