@@ -1,0 +1,176 @@
+"""ctypes binding of ``libafsi_b200.so`` (the C-ABI in ``include/afsi_b200.h``).
+
+PyTorch supplies device memory and the current CUDA stream; every compute call
+goes to the native library.  There is no CPU or PyTorch fallback: a missing
+library or a CPU tensor raises.
+"""
+import ctypes
+import threading
+from pathlib import Path
+import torch
+
+LIB_PATH = Path(__file__).resolve().parent / 'libafsi_b200.so'
+
+F32, F64 = 0, 1
+OK, ERR_ARG, ERR_CUDA = 0, 1, 2
+FLAG_SUPPORT, FLAG_INDEX, FLAG_OVERFLOW = 1, 2, 4
+PHI_CLAMPED, PHI_RADICAL = 0, 1
+BC_NEUMANN, BC_CHANNEL, BC_PERIODIC = 0, 1, 2
+MAX_LEVELS = 12
+
+_lock = threading.Lock()
+_lib = None
+
+c_void_p, c_int64, c_int32, c_double = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_double
+P_I64 = ctypes.POINTER(ctypes.c_int64)
+P_F64 = ctypes.POINTER(ctypes.c_double)
+
+
+class MGLevel(ctypes.Structure):
+    _fields_ = [('shape', ctypes.c_int64 * 3), ('h2', ctypes.c_double * 3), ('inv_h2', ctypes.c_double * 3),
+                ('p', c_void_p), ('ping', c_void_p), ('rhs', c_void_p)]
+
+
+class MGPlan(ctypes.Structure):
+    _fields_ = [('dim', c_int32), ('bc', c_int32), ('levels', c_int32), ('smooth', c_int32),
+                ('dtype', c_int32), ('coarse_dtype', c_int32), ('level', MGLevel * MAX_LEVELS),
+                ('coarse_inverse', c_void_p), ('scratch', c_void_p)]
+
+
+# name -> argtypes (restype int32 unless listed in _RESTYPES)
+_SIGNATURES = {
+    'afsi_b200_last_error': [],
+    'afsi_b200_version': [],
+    'afsi_b200_launch_count': [],
+    'afsi_b200_compact_prepare': [c_void_p, c_int64, c_int32, P_F64, P_F64, P_F64, P_I64, c_int32, c_void_p,
+                                  c_void_p, c_void_p, c_int32, c_void_p],
+    'afsi_b200_indexed_prepare2d': [c_void_p, c_int64, c_int64, c_int64, c_double, c_double, c_double, c_double,
+                                    c_void_p, c_void_p, c_void_p, c_int32, c_void_p],
+    'afsi_b200_p2_prepare': [c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, P_F64, P_F64, P_F64,
+                             c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int32, c_void_p],
+    'afsi_b200_indexed_gather': [c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_int64, c_int64, c_void_p,
+                                 c_void_p, c_int32, c_void_p],
+    'afsi_b200_indexed_spread': [c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_int64, c_int64, c_double,
+                                 c_void_p, c_void_p, c_int32, c_void_p],
+    'afsi_b200_compact_gather': [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_int64, c_int64, c_void_p,
+                                 c_void_p, c_int32, c_void_p],
+    'afsi_b200_compact_spread': [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_int64, c_int64, c_double,
+                                 c_void_p, c_void_p, c_int32, c_void_p],
+    'afsi_b200_p2_spread': [c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
+                            c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_int64, c_double,
+                            c_void_p, c_int32, c_void_p],
+    'afsi_b200_p2_gather_assemble': [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_int64,
+                                     c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int64, c_int64,
+                                     c_int64, c_int64, c_void_p, c_int32, c_void_p],
+    'afsi_b200_p2_gather_local': [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
+                                  c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int64, c_int64, c_int64,
+                                  c_void_p, c_int32, c_void_p],
+    'afsi_b200_node_reduce': [c_void_p, c_int64, c_void_p, c_void_p, c_int64, c_void_p, c_int32, c_void_p,
+                              c_int32, c_void_p],
+    'afsi_b200_mg_smooth': [c_void_p, c_void_p, c_void_p, P_I64, P_F64, P_F64, c_int32, c_int32, c_int32,
+                            c_void_p],
+    'afsi_b200_mg_residual': [c_void_p, c_void_p, c_void_p, P_I64, P_F64, c_int32, c_int32, c_int32, c_void_p],
+    'afsi_b200_mg_restrict': [c_void_p, c_void_p, P_I64, c_int32, c_int32, c_void_p],
+    'afsi_b200_mg_residual_restrict': [c_void_p, c_void_p, c_void_p, P_I64, P_F64, c_int32, c_int32, c_int32,
+                                       c_void_p],
+    'afsi_b200_mg_prolong_add': [c_void_p, c_void_p, P_I64, c_int32, c_int32, c_int32, c_void_p],
+    'afsi_b200_mg_scratch_bytes': [ctypes.POINTER(MGPlan)],
+    'afsi_b200_mg_vcycles': [ctypes.POINTER(MGPlan), c_int32, c_void_p],
+    'afsi_b200_mg_residual_norm': [ctypes.POINTER(MGPlan), c_void_p, c_void_p],
+    'afsi_b200_vector_stats': [c_void_p, c_int64, c_void_p, c_void_p, c_int32, c_void_p],
+    'afsi_b200_subtract_mean': [c_void_p, c_int64, c_void_p, c_int32, c_void_p],
+}
+_RESTYPES = {'afsi_b200_last_error': ctypes.c_char_p, 'afsi_b200_mg_scratch_bytes': ctypes.c_int64,
+             'afsi_b200_launch_count': ctypes.c_int64}
+
+
+def exported_symbols():
+    """Names every build of the library must export (declared in the header)."""
+    return tuple(_SIGNATURES)
+
+
+def load():
+    """Load (building first if absent) and return the ctypes library."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not LIB_PATH.exists():
+                from .build import build
+                build()
+            lib = ctypes.CDLL(str(LIB_PATH))
+            for name, args in _SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.argtypes = args
+                fn.restype = _RESTYPES.get(name, ctypes.c_int32)
+            _lib = lib
+    return _lib
+
+
+def call(name, *args):
+    """Invoke an entry point; raise RuntimeError on a host status != 0."""
+    lib = load()
+    rc = getattr(lib, name)(*args)
+    if rc != OK:
+        msg = lib.afsi_b200_last_error().decode(errors='replace')
+        raise RuntimeError(f'{name}: {msg}' if msg else f'{name} failed with status {rc}')
+    return rc
+
+
+def dtype_code(dtype):
+    if dtype == torch.float64:
+        return F64
+    if dtype == torch.float32:
+        return F32
+    raise ValueError('IB/MG kernels support float32/float64')
+
+
+def ptr(t):
+    return None if t is None else t.data_ptr()
+
+
+def stream(device=None):
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def doubles(values):
+    values = [float(v) for v in values]
+    return (ctypes.c_double * len(values))(*values)
+
+
+def int64s(values):
+    values = [int(v) for v in values]
+    return (ctypes.c_int64 * len(values))(*values)
+
+
+def require_cuda(tensor):
+    """Native kernels only: CPU tensors are rejected, never handled on the CPU."""
+    if not torch.is_tensor(tensor) or not tensor.is_cuda:
+        raise ValueError('the B200 backend requires CUDA tensors; there is no CPU fallback')
+    load()
+
+
+_status = {}
+
+
+def status_word(device):
+    """Per-device int32 status word that kernels OR their AFSI_FLAG_* bits into."""
+    key = torch.device(device).index if torch.device(device).index is not None else torch.cuda.current_device()
+    word = _status.get(key)
+    if word is None:
+        word = torch.zeros((), dtype=torch.int32, device=torch.device('cuda', key))
+        _status[key] = word
+    return word
+
+
+_replayed = [0]
+
+
+def launch_count():
+    """Native kernel launches so far, including those replayed from captured graphs."""
+    return int(load().afsi_b200_launch_count()) + _replayed[0]
+
+
+def count_replay(launches):
+    _replayed[0] += int(launches)

@@ -1,0 +1,285 @@
+// Binning and IB_4 weight tables (compact 3D, reflected 2D, P2 quadrature).
+//
+// One thread per point: the point's coordinates are read once and all of its
+// lattices and axes are produced from registers, so the only HBM traffic is
+// the point read and the table write.  Arithmetic follows the reference
+// operation order (library built with --fmad=false, IEEE division and sqrt),
+// which makes the integer bases bit-exact and the weights equal to rounding.
+#include "common.cuh"
+
+namespace afsi {
+
+// Clamped two-branch Peskin kernel, afsi_torch/ib.py:57-67.
+template <class T>
+__device__ __forceinline__ T peskin_clamped(T d) {
+    const T r = fabs(d);
+    const T a = r < T(1) ? r : T(1);
+    const T b = r < T(1) ? T(1) : (r < T(2) ? r : T(2));
+    const T inner = (T(3) - T(2) * a + sqrt(T(1) + T(4) * a - T(4) * (a * a))) / T(8);
+    const T outer = (T(5) - T(2) * b - sqrt(T(-7) + T(12) * b - T(4) * (b * b))) / T(8);
+    return r < T(1) ? inner : (r < T(2) ? outer : T(0));
+}
+
+// Shared-radical weights for f in [0,1), mac/csrc/p2_transfer.cu:36-43.
+template <class T>
+__device__ __forceinline__ void peskin_radical(T f, T w[4]) {
+    const T rad = sqrt(T(1) + T(4) * f - T(4) * (f * f));
+    w[0] = (T(3) - T(2) * f - rad) / T(8);
+    w[1] = (T(3) - T(2) * f + rad) / T(8);
+    w[2] = (T(1) + T(2) * f + rad) / T(8);
+    w[3] = (T(1) + T(2) * f - rad) / T(8);
+}
+
+template <class T>
+__device__ __forceinline__ void store4(T* dst, const T w[4]);
+template <>
+__device__ __forceinline__ void store4<double>(double* dst, const double w[4]) {
+    reinterpret_cast<double2*>(dst)[0] = make_double2(w[0], w[1]);
+    reinterpret_cast<double2*>(dst)[1] = make_double2(w[2], w[3]);
+}
+template <>
+__device__ __forceinline__ void store4<float>(float* dst, const float w[4]) {
+    *reinterpret_cast<float4*>(dst) = make_float4(w[0], w[1], w[2], w[3]);
+}
+
+template <class T>
+struct CompactParams {
+    T origins[3][3];
+    T spacing[3];
+    T grid_origin[3];
+    T limits[3];
+    int lattices;
+    int form;
+};
+
+template <class T>
+__global__ void __launch_bounds__(256) compact_prepare_kernel(const T* __restrict__ points, int64_t count,
+                                                              CompactParams<T> prm, int64_t* __restrict__ base,
+                                                              T* __restrict__ phi, int32_t* status) {
+    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= count) return;
+    T x[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) x[a] = points[p * 3 + a];
+    bool valid = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const T s = (x[a] - prm.grid_origin[a]) / prm.spacing[a];
+        valid = valid && isfinite(s) && s >= T(2) && s < prm.limits[a];
+    }
+    if (!valid) flag(status, AFSI_FLAG_SUPPORT);
+    for (int l = 0; l < prm.lattices; ++l) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const T scaled = (x[a] - prm.origins[l][a]) / prm.spacing[a];
+            const T lo = floor(scaled - T(1));
+            const int64_t lower = static_cast<int64_t>(lo);
+            const int64_t row = (l * count + p) * 3 + a;
+            base[row] = lower;
+            T w[4];
+            if (prm.form == AFSI_PHI_RADICAL) {
+                peskin_radical(scaled - T(lower) - T(1), w);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) w[k] = peskin_clamped(scaled - T(lower + k));
+            }
+            store4(phi + row * 4, w);
+        }
+    }
+}
+
+template <class T>
+struct Prepare2dParams {
+    T hx, hy;
+    T xmin, xmax, ymin, ymax;
+    int64_t ny;
+};
+
+// Reflected 4x4 stencils of u (faces (nx+1,ny)) and v (faces (nx,ny+1)),
+// mac2d/transfer.py:61-81.  Offsets k=i*4+j, j (y) fastest.
+template <class T>
+__global__ void __launch_bounds__(256) prepare2d_kernel(const T* __restrict__ points, int64_t count,
+                                                        Prepare2dParams<T> prm, int64_t* __restrict__ ids,
+                                                        T* __restrict__ weights, int32_t* status) {
+    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= count) return;
+    const T px = points[p * 2], py = points[p * 2 + 1];
+    const bool valid = isfinite(px) && isfinite(py) && px >= prm.xmin && px <= prm.xmax &&
+                       py >= prm.ymin && py <= prm.ymax;
+    if (!valid) flag(status, AFSI_FLAG_SUPPORT);
+    const int64_t ny = prm.ny;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        const T ox = prm.hx * (c == 0 ? T(0) : T(.5));
+        const T oy = prm.hy * (c == 1 ? T(0) : T(.5));
+        const T sx = (px - ox) / prm.hx, sy = (py - oy) / prm.hy;
+        const int64_t bx = static_cast<int64_t>(floor(sx - T(1)));
+        const int64_t by = static_cast<int64_t>(floor(sy - T(1)));
+        const int64_t face_ny = ny + (c == 1);
+        T wx[4], wy[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            wx[k] = peskin_clamped(sx - T(bx + k));
+            wy[k] = peskin_clamped(sy - T(by + k));
+        }
+        int64_t* out_ids = ids + (c * count + p) * 16;
+        T* out_w = weights + (c * count + p) * 16;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int64_t y = by + j;
+                bool outside;
+                int64_t r;
+                if (c == 0) {
+                    outside = y < 0 || y >= ny;
+                    r = y < 0 ? -y - 1 : (y >= ny ? 2 * ny - y - 1 : y);
+                } else {
+                    outside = y < 0 || y > ny;
+                    r = y < 0 ? -y : (y > ny ? 2 * ny - y : y);
+                }
+                const T w = wx[i] * wy[j];
+                out_ids[i * 4 + j] = (bx + i) * face_ny + r;
+                out_w[i * 4 + j] = outside ? -w : w;
+            }
+        }
+    }
+}
+
+template <class T>
+struct P2Params {
+    T origin[3], spacing[3], limits[3];
+    int64_t nodes, elements, nq, total, offset;
+};
+
+// P2 positions + shared tables, mac/csrc/p2_transfer.cu:12-45.  One thread per
+// quadrature point (element-major, q fastest); each axis has its own validity
+// as in the reference, and an invalid axis is binned from scaled=0.
+template <class T>
+__global__ void __launch_bounds__(256) p2_prepare_kernel(const T* __restrict__ x, const int64_t* __restrict__ cells,
+                                                         const T* __restrict__ N, P2Params<T> prm,
+                                                         int64_t* __restrict__ base, T* __restrict__ phi,
+                                                         int32_t* status) {
+    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= prm.elements * prm.nq) return;
+    const int64_t e = p / prm.nq, q = p % prm.nq;
+    int64_t node[10];
+    bool ok = true;
+#pragma unroll
+    for (int a = 0; a < 10; ++a) {
+        node[a] = cells[e * 10 + a];
+        ok = ok && node[a] >= 0 && node[a] < prm.nodes;
+    }
+    if (!ok) {
+        flag(status, AFSI_FLAG_INDEX);
+        return;
+    }
+    T pos[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int a = 0; a < 10; ++a) {
+        const T n = N[q * 10 + a];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) pos[d] += n * x[node[a] * 3 + d];
+    }
+    const int64_t row0 = prm.offset + p;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const T physical = (pos[a] - prm.origin[a]) / prm.spacing[a];
+        const bool valid = isfinite(physical) && physical >= T(2) && physical < prm.limits[a];
+        if (!valid) flag(status, AFSI_FLAG_SUPPORT);
+#pragma unroll
+        for (int lattice = 0; lattice < 2; ++lattice) {
+            const T start = lattice ? prm.origin[a] + T(.5) * prm.spacing[a] : prm.origin[a];
+            const T scaled = valid ? (pos[a] - start) / prm.spacing[a] : T(0);
+            const int64_t lower = static_cast<int64_t>(floor(scaled - T(1)));
+            T w[4];
+            peskin_radical(scaled - T(lower) - T(1), w);
+            const int64_t row = (lattice * prm.total + row0) * 3 + a;
+            base[row] = lower;
+            store4(phi + row * 4, w);
+        }
+    }
+}
+
+}  // namespace afsi
+
+using namespace afsi;
+
+extern "C" int32_t afsi_b200_compact_prepare(const void* points, int64_t count, int32_t lattices,
+                                             const double* origins, const double* spacing,
+                                             const double* grid_origin, const int64_t* shape,
+                                             int32_t phi_form, int64_t* base, void* phi, int32_t* status,
+                                             int32_t dtype, afsi_stream_t stream) {
+    AFSI_REQUIRE(count >= 0, "negative point count");
+    AFSI_REQUIRE(lattices >= 1 && lattices <= 3, "lattices must be 1..3");
+    AFSI_REQUIRE(origins && spacing && grid_origin && shape, "null host parameter array");
+    AFSI_REQUIRE(phi_form == AFSI_PHI_CLAMPED || phi_form == AFSI_PHI_RADICAL, "unknown phi form");
+    if (count == 0) return AFSI_OK;
+    AFSI_REQUIRE(points && base && phi, "null device pointer");
+    AFSI_DISPATCH(dtype, {
+        CompactParams<T> prm;
+        for (int l = 0; l < 3; ++l)
+            for (int a = 0; a < 3; ++a) prm.origins[l][a] = T(l < lattices ? origins[l * 3 + a] : 0.0);
+        for (int a = 0; a < 3; ++a) {
+            AFSI_REQUIRE(spacing[a] > 0 && shape[a] > 0, "invalid grid spacing/shape");
+            prm.spacing[a] = T(spacing[a]);
+            prm.grid_origin[a] = T(grid_origin[a]);
+            prm.limits[a] = T(shape[a]) - T(2);
+        }
+        prm.lattices = lattices;
+        prm.form = phi_form;
+        compact_prepare_kernel<T><<<blocks_for(count, 256), 256, 0, stream>>>(
+            static_cast<const T*>(points), count, prm, base, static_cast<T*>(phi), status);
+    });
+    return launched("compact_prepare");
+}
+
+extern "C" int32_t afsi_b200_indexed_prepare2d(const void* points, int64_t count, int64_t nx, int64_t ny,
+                                               double hx, double hy, double lx, double ly, int64_t* ids,
+                                               void* weights, int32_t* status, int32_t dtype,
+                                               afsi_stream_t stream) {
+    AFSI_REQUIRE(count >= 0 && nx > 0 && ny > 0 && hx > 0 && hy > 0, "invalid 2D grid or point count");
+    if (count == 0) return AFSI_OK;
+    AFSI_REQUIRE(points && ids && weights, "null device pointer");
+    AFSI_DISPATCH(dtype, {
+        Prepare2dParams<T> prm;
+        prm.hx = T(hx);
+        prm.hy = T(hy);
+        prm.xmin = T(2 * hx);
+        prm.xmax = T(lx - 2 * hx);
+        prm.ymin = T(-hy);
+        prm.ymax = T(ly + hy);
+        prm.ny = ny;
+        prepare2d_kernel<T><<<blocks_for(count, 256), 256, 0, stream>>>(
+            static_cast<const T*>(points), count, prm, ids, static_cast<T*>(weights), status);
+    });
+    return launched("indexed_prepare2d");
+}
+
+extern "C" int32_t afsi_b200_p2_prepare(const void* x, int64_t nodes, const int64_t* cells, int64_t elements,
+                                        const void* N, int64_t nq, const double* origin, const double* spacing,
+                                        const double* limits, int64_t* base, void* phi, int64_t total,
+                                        int64_t offset, int32_t* status, int32_t dtype, afsi_stream_t stream) {
+    AFSI_REQUIRE(elements >= 0 && nq > 0 && nodes >= 0, "invalid P2 group sizes");
+    AFSI_REQUIRE(offset >= 0 && offset <= total && elements * nq <= total - offset,
+                 "P2 IB group exceeds table bounds");
+    AFSI_REQUIRE(origin && spacing && limits, "null host parameter array");
+    if (elements == 0) return AFSI_OK;
+    AFSI_REQUIRE(x && cells && N && base && phi, "null device pointer");
+    AFSI_DISPATCH(dtype, {
+        P2Params<T> prm;
+        for (int a = 0; a < 3; ++a) {
+            prm.origin[a] = T(origin[a]);
+            prm.spacing[a] = T(spacing[a]);
+            prm.limits[a] = T(limits[a]);
+        }
+        prm.nodes = nodes;
+        prm.elements = elements;
+        prm.nq = nq;
+        prm.total = total;
+        prm.offset = offset;
+        p2_prepare_kernel<T><<<blocks_for(elements * nq, 256), 256, 0, stream>>>(
+            static_cast<const T*>(x), cells, static_cast<const T*>(N), prm, base, static_cast<T*>(phi), status);
+    });
+    return launched("p2_prepare");
+}

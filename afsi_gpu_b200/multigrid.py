@@ -1,0 +1,344 @@
+"""MAC geometric multigrid on the B200 kernels.
+
+``GeometricMultigrid`` keeps the constructor and ``solve`` contract of
+``afsi_torch/mac/multigrid.py:24-172`` (closed-box Neumann pressure, mean-zero
+gauge) and ``ChannelMultigrid`` that of ``afsi_torch/mac2d/multigrid.py:16-134``
+(inlet/outlet channel).  ``ChannelMultigrid(grid)`` with ``grid.periodic`` solves
+the periodic-in-x / no-slip-in-y pressure problem, which has no reference
+solver: same V-cycle, x-wrapped stencils, the mean-zero gauge and the rank-one
+coarse inverse of the 3D solver.
+
+``B200Kernels`` is the kernel object the reference workspaces call
+(``smooth/residual/restrict/residual_restrict/prolong_add``,
+``mac/_triton_mg.py:121-151``, ``mac2d/_triton_mg.py:78-100``).  Its ``smooth``
+rebuilds the operator diagonal inside the kernel (the reference passes exactly
+that diagonal), so no diagonal array is read.
+
+The solve loop mirrors ``_solve_workspace``: start metrics (finiteness, mean,
+norms) on the device with one host read, then blocks of ``check_every`` fused
+V-cycles (optionally replayed as captured CUDA graphs) with one residual-norm
+read per block.  Results are returned as fresh tensors, never workspace aliases.
+"""
+import ctypes
+from dataclasses import dataclass
+from math import isfinite, prod
+import torch
+from . import _lib
+from ._lib import call, ptr, stream, dtype_code
+
+
+@dataclass(frozen=True)
+class MGOptions:
+    """``mac/multigrid.py:9-21``."""
+    rtol: float = 1e-10
+    atol: float = 1e-12
+    max_cycles: int = 100
+    smooth: int = 4
+    check_every: int = 2
+
+    def __post_init__(self):
+        if (any(not isfinite(x) or x < 0 for x in (self.rtol, self.atol)) or
+                self.rtol + self.atol == 0 or any(type(n) is not int or n < 1 for n in
+                                                  (self.max_cycles, self.smooth, self.check_every))):
+            raise ValueError('invalid multigrid options')
+
+
+def _h2(spacing):
+    return [h * h for h in spacing]
+
+
+def _ih2(spacing):
+    return [1 / h ** 2 for h in spacing]
+
+
+class B200Kernels:
+    """Kernel object for one boundary condition (3D Neumann or a 2D channel)."""
+
+    def __init__(self, bc='neumann'):
+        self.bc = {'neumann': _lib.BC_NEUMANN, 'channel': _lib.BC_CHANNEL, 'periodic': _lib.BC_PERIODIC}[bc]
+        self.dim = 3 if bc == 'neumann' else 2
+        self.name = 'b200' if bc == 'neumann' else f'b200-{bc}'
+
+    def _shape(self, t):
+        if t.dim() != self.dim:
+            raise ValueError(f'expected a {self.dim}D pressure field')
+        return _lib.int64s(list(t.shape) + [1] * (3 - self.dim))
+
+    @staticmethod
+    def _check(*ts):
+        for t in ts:
+            _lib.require_cuda(t)
+            if not t.is_contiguous():
+                raise ValueError('multigrid kernels need contiguous tensors')
+
+    def smooth(self, p, rhs, diagonal, out, spacing):
+        self._check(p, rhs, out)
+        call('afsi_b200_mg_smooth', ptr(p), ptr(rhs), ptr(out), self._shape(p), _lib.doubles(_h2(spacing)),
+             _lib.doubles(_ih2(spacing)), self.dim, self.bc, dtype_code(p.dtype), stream(p.device))
+
+    def residual(self, p, rhs, out, spacing):
+        self._check(p, rhs, out)
+        call('afsi_b200_mg_residual', ptr(p), ptr(rhs), ptr(out), self._shape(p), _lib.doubles(_h2(spacing)),
+             self.dim, self.bc, dtype_code(p.dtype), stream(p.device))
+
+    def restrict(self, fine, out):
+        self._check(fine, out)
+        call('afsi_b200_mg_restrict', ptr(fine), ptr(out), self._shape(fine), self.dim, dtype_code(fine.dtype),
+             stream(fine.device))
+
+    def residual_restrict(self, p, rhs, out, spacing):
+        self._check(p, rhs, out)
+        call('afsi_b200_mg_residual_restrict', ptr(p), ptr(rhs), ptr(out), self._shape(p),
+             _lib.doubles(_h2(spacing)), self.dim, self.bc, dtype_code(p.dtype), stream(p.device))
+
+    def prolong_add(self, coarse, fine):
+        self._check(coarse, fine)
+        call('afsi_b200_mg_prolong_add', ptr(coarse), ptr(fine), self._shape(fine), self.dim, self.bc,
+             dtype_code(fine.dtype), stream(fine.device))
+
+
+def _levels(shape, spacing):
+    """Coarsening rule of ``mac/multigrid.py:35-48``."""
+    shapes, spacings = [], []
+    shape, spacing = tuple(shape), tuple(spacing)
+    while True:
+        shapes.append(shape)
+        spacings.append(spacing)
+        if min(shape) <= 4 or any(n % 2 for n in shape):
+            break
+        shape = tuple(n // 2 for n in shape)
+        spacing = tuple(2 * h for h in spacing)
+    if prod(shape) > 512:
+        raise ValueError('MAC dimensions must coarsen to <=512 cells; use powers of two')
+    return shapes, spacings
+
+
+def _coarse_matrix(shape, spacing, bc):
+    """Dense coarsest operator (float64, CPU): -Δ with the level's BC, plus
+    11ᵀ/n when singular (``mac/multigrid.py:49-59``, ``mac2d/multigrid.py:41-45``)."""
+    n = prod(shape)
+    ids = torch.arange(n).reshape(shape)
+    A = torch.zeros((n, n), dtype=torch.float64)
+    dim = len(shape)
+    for c, h in enumerate(spacing):
+        w = 1 / h ** 2
+        if bc == 'periodic' and c == 0:
+            a = ids.reshape(-1)
+            b = torch.roll(ids, -1, 0).reshape(-1)
+        else:
+            sl_a = [slice(None)] * dim
+            sl_b = [slice(None)] * dim
+            sl_a[c] = slice(None, -1)
+            sl_b[c] = slice(1, None)
+            a, b = ids[tuple(sl_a)].reshape(-1), ids[tuple(sl_b)].reshape(-1)
+        for row, col, val in ((a, a, w), (b, b, w), (a, b, -w), (b, a, -w)):
+            A.index_put_((row, col), torch.full(row.shape, val, dtype=torch.float64), accumulate=True)
+    if bc == 'channel':
+        last = ids[-1].reshape(-1)
+        A.index_put_((last, last), torch.full(last.shape, 2 / spacing[0] ** 2, dtype=torch.float64),
+                     accumulate=True)
+    else:
+        A += 1. / n
+    return A
+
+
+class _Workspace:
+    """Fixed-address level buffers, reduction scratch and the native plan."""
+
+    def __init__(self, shapes, spacings, bc, dtype, device, smooth, coarse_dtype):
+        self.p = [torch.zeros(s, device=device, dtype=dtype) for s in shapes]
+        self.ping = [torch.zeros(s, device=device, dtype=dtype) for s in shapes]
+        self.rhs = [torch.zeros(s, device=device, dtype=dtype) for s in shapes]
+        bcode = {'neumann': _lib.BC_NEUMANN, 'channel': _lib.BC_CHANNEL, 'periodic': _lib.BC_PERIODIC}[bc]
+        plan = _lib.MGPlan()
+        plan.dim = len(shapes[0])
+        plan.bc = bcode
+        plan.levels = len(shapes)
+        plan.smooth = smooth
+        plan.dtype = dtype_code(dtype)
+        plan.coarse_dtype = dtype_code(coarse_dtype)
+        for l, (s, h) in enumerate(zip(shapes, spacings)):
+            L = plan.level[l]
+            dims = list(s) + [1] * (3 - len(s))
+            hh = list(h) + [1.] * (3 - len(h))
+            for a in range(3):
+                L.shape[a] = dims[a]
+                L.h2[a] = hh[a] * hh[a]
+                L.inv_h2[a] = 1 / hh[a] ** 2
+            L.p, L.ping, L.rhs = ptr(self.p[l]), ptr(self.ping[l]), ptr(self.rhs[l])
+        nbytes = _lib.load().afsi_b200_mg_scratch_bytes(ctypes.byref(plan))
+        self.scratch = torch.zeros(int(nbytes), device=device, dtype=torch.uint8)
+        plan.scratch = ptr(self.scratch)
+        self.plan = plan
+        self.stats = torch.zeros(12, device=device, dtype=torch.float64)
+        self.norm = torch.zeros(1, device=device, dtype=torch.float64)
+        self.stat_scratch = torch.zeros(4096 * 8 * 4 + 64, device=device, dtype=torch.uint8)
+        self.allocated_bytes = sum(t.numel() * t.element_size()
+                                   for group in (self.p, self.ping, self.rhs) for t in group)
+
+    def set_coarse(self, inverse):
+        self.coarse_inverse = inverse
+        self.plan.coarse_inverse = ptr(inverse)
+
+    def vcycles(self, count):
+        call('afsi_b200_mg_vcycles', ctypes.byref(self.plan), count, stream(self.p[0].device))
+
+    def residual_norm(self):
+        call('afsi_b200_mg_residual_norm', ctypes.byref(self.plan), ptr(self.norm), stream(self.p[0].device))
+        return self.norm[0]
+
+    def vector_stats(self, x, out):
+        call('afsi_b200_vector_stats', ptr(x), x.numel(), ptr(out), ptr(self.stat_scratch), dtype_code(x.dtype),
+             stream(x.device))
+
+    def subtract_mean(self, x, stats):
+        call('afsi_b200_subtract_mean', ptr(x), x.numel(), ptr(stats), dtype_code(x.dtype), stream(x.device))
+
+
+class _Solver:
+    bc = 'neumann'
+
+    def __init__(self, grid, *, device='cuda', dtype=torch.float64, options=None, backend='b200-graph',
+                 coarse_dtype=None):
+        if backend not in ('b200', 'b200-graph'):
+            raise ValueError('pressure backend must be b200 or b200-graph')
+        device = torch.device(device)
+        if device.type != 'cuda':
+            raise ValueError('the B200 multigrid requires a CUDA device; there is no CPU fallback')
+        _lib.load()
+        self.options = MGOptions() if options is None else options
+        self.grid = grid
+        self.shapes, self.spacings = _levels(grid.shape, grid.spacing)
+        self.dtype = dtype
+        self.coarse_dtype = dtype if coarse_dtype is None else coarse_dtype
+        A = _coarse_matrix(self.shapes[-1], self.spacings[-1], self.bc)
+        self.coarse_inverse = torch.linalg.inv(A).to(device=device, dtype=self.coarse_dtype)
+        self.kernels = B200Kernels(self.bc)
+        self.workspace = _Workspace(self.shapes, self.spacings, self.bc, dtype, device, self.options.smooth,
+                                    self.coarse_dtype)
+        self.workspace.set_coarse(self.coarse_inverse)
+        self.backend = self.kernels.name + ('-graph' if backend == 'b200-graph' else '')
+        self.graphs = {}
+        if backend == 'b200-graph':
+            self._capture()
+
+    @property
+    def singular(self):
+        return self.bc != 'channel'
+
+    # -- execution
+    def _capture(self):
+        w = self.workspace
+        device = w.p[0].device
+        with torch.cuda.device(device):
+            s = torch.cuda.Stream(device=device)
+            s.wait_stream(torch.cuda.current_stream(device))
+            with torch.cuda.stream(s):
+                for _ in range(2):
+                    w.vcycles(self.options.check_every)
+            torch.cuda.current_stream(device).wait_stream(s)
+            self.graph_launches = {}
+            for count in range(1, self.options.check_every + 1):
+                g = torch.cuda.CUDAGraph()
+                before = _lib.launch_count()
+                with torch.cuda.graph(g, stream=s):
+                    w.vcycles(count)
+                self.graph_launches[count] = _lib.launch_count() - before
+                self.graphs[count] = g
+            torch.cuda.current_stream(device).wait_stream(s)
+            for t in (*w.p, *w.ping, *w.rhs):
+                t.zero_()
+
+    def advance(self, count):
+        if self.graphs:
+            self.graphs[count].replay()
+            _lib.count_replay(self.graph_launches[count])
+        else:
+            self.workspace.vcycles(count)
+        return self.workspace.p[0]
+
+    def cycle(self):
+        """One V-cycle on the workspace iterate (for parity checks)."""
+        self.workspace.vcycles(1)
+        return self.workspace.p[0]
+
+    def initialize(self, p, rhs):
+        self.workspace.p[0].copy_(p)
+        self.workspace.rhs[0].copy_(rhs)
+
+    def residual_norm(self):
+        return self.workspace.residual_norm()
+
+    # -- solve
+    def _start(self, rhs, initial):
+        """Copy in, gauge-shift (singular BCs) and measure; one host read.
+
+        Returns raw-rhs (sum, sum|x|, finite), p finite, ||rhs|| after the
+        shift and the initial residual norm (``_start_metrics``,
+        ``mac/multigrid.py:68-73``)."""
+        w = self.workspace
+        w.rhs[0].copy_(rhs)
+        w.p[0].zero_() if initial is None else w.p[0].copy_(initial)
+        st = w.stats
+        w.vector_stats(w.rhs[0], st[0:4])
+        w.vector_stats(w.p[0], st[4:8])
+        if self.singular:
+            w.subtract_mean(w.rhs[0], st[0:4])
+            w.subtract_mean(w.p[0], st[4:8])
+            w.vector_stats(w.rhs[0], st[8:12])
+        else:
+            st[8:12].copy_(st[0:4])
+        norm = w.residual_norm()
+        v = torch.cat((st, norm)).tolist()
+        return dict(rhs_sum=v[0], rhs_abs=v[1], rhs_finite=v[3], p_finite=v[7], rhs_sq=v[10], residual=v[12])
+
+    def solve(self, rhs, initial=None, *, rtol=None):
+        rtol = self.options.rtol if rtol is None else rtol
+        if not isfinite(rtol) or rtol < 0:
+            raise ValueError('invalid multigrid solve tolerance')
+        if rhs.shape != self.shapes[0] or rhs.device != self.workspace.p[0].device or rhs.dtype != self.dtype:
+            raise ValueError('invalid pressure RHS')
+        if initial is not None and (initial.shape != rhs.shape or initial.device != rhs.device
+                                    or initial.dtype != rhs.dtype):
+            raise ValueError('invalid initial pressure')
+        w = self.workspace
+        m = self._start(rhs, initial)
+        n = rhs.numel()
+        if self.singular:
+            if not m['rhs_finite']:
+                raise ValueError('invalid pressure RHS')
+            if abs(m['rhs_sum'] / n) > 1e-12 + 1e-10 * (m['rhs_abs'] / n):
+                raise ValueError('incompatible Neumann pressure RHS: net flux must vanish')
+            if not m['p_finite']:
+                raise ValueError('invalid initial pressure')
+        elif not (m['rhs_finite'] and m['p_finite']):
+            raise ValueError('finite pressure RHS/initial guess required')
+        rhs_norm, residual = m['rhs_sq'] ** .5, m['residual']
+        if not isfinite(rhs_norm) or not isfinite(residual):
+            raise RuntimeError('nonfinite multigrid residual or RHS norm')
+        tol = max(self.options.atol, rtol * rhs_norm)
+        cycle = 0
+        while residual > tol and cycle < self.options.max_cycles:
+            count = min(self.options.check_every, self.options.max_cycles - cycle)
+            self.advance(count)
+            cycle += count
+            residual = self.residual_norm().item()
+            if not isfinite(residual):
+                raise RuntimeError('nonfinite multigrid residual')
+        if residual > tol:
+            raise RuntimeError(f'pressure multigrid did not converge: {residual:g} > {tol:g}')
+        return w.p[0].clone(), dict(cycles=cycle, residual_norm=residual, tolerance=tol, backend=self.backend)
+
+
+class GeometricMultigrid(_Solver):
+    """Closed-box 3D pressure V-cycle solver (``mac/multigrid.py:24-172``)."""
+    bc = 'neumann'
+
+
+class ChannelMultigrid(_Solver):
+    """2D channel (``mac2d/multigrid.py:16-134``) or, with ``grid.periodic``,
+    the periodic-x / Neumann-y problem."""
+
+    def __init__(self, grid, **kwargs):
+        self.bc = 'periodic' if getattr(grid, 'periodic', False) else 'channel'
+        super().__init__(grid, **kwargs)

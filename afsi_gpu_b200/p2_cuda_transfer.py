@@ -1,0 +1,195 @@
+"""P2 quadrature IB transfer on the B200 kernels.
+
+Module functions keep the signatures of ``afsi_torch/mac/p2_cuda_transfer.py``
+(``prepare(transfer, x, rule, *, buffers=None)``, ``spread(transfer,
+coefficient, stencil)``, ``assemble_velocity(transfer, velocity, stencil)``)
+and the semantics of the ``p2_prepare_ / p2_spread_ / p2_gather_assemble_``
+operators (``mac/csrc/p2_transfer.cpp:66-74``): shared face/centre tables
+(2,T,3)/(2,T,3,4), one launch per quadrature group, spreads accumulate into
+fresh zeroed fields, the nodal right-hand side accumulates into zeros, and a
+support violation raises ``ValueError`` after the prepare.
+
+``P2Transfer`` supplies what those functions read from the reference
+``AdaptiveFETransfer`` (grid, origin/spacing/limits, diagonal, rule) without
+the consistent-mass solve, which is outside this hot path.  Its
+``deterministic=True`` mode assembles through element-local sums and a fixed
+node CSR instead of atomics (bitwise reproducible ``assemble_velocity``).
+"""
+from dataclasses import dataclass
+import torch
+from . import _lib
+from ._lib import call, ptr, stream, dtype_code
+from .quadrature import RuleBuilder, InteractionRule
+
+
+@dataclass(frozen=True)
+class SharedAdaptiveStencil:
+    base: torch.Tensor   # (2,T,3) int64: lattice 0 = faces, 1 = centres
+    phi: torch.Tensor    # (2,T,3,4)
+    rule: InteractionRule
+    layout = 'shared'
+
+    @property
+    def storage_bytes(self):
+        return self.base.numel() * self.base.element_size() + self.phi.numel() * self.phi.element_size()
+
+    def expanded(self):
+        """Per-component (3,T,3)/(3,T,3,4) tables (``mac/shared_stencil.py:13-19``)."""
+        base = torch.stack([torch.stack([self.base[int(a != c), :, a] for a in range(3)], -1) for c in range(3)])
+        phi = torch.stack([torch.stack([self.phi[int(a != c), :, a, :] for a in range(3)], 1) for c in range(3)])
+        return base, phi
+
+
+class P2Transfer:
+    """Grid/quadrature state of the P2 CUDA transfer (no mass solve)."""
+
+    def __init__(self, grid, X, cells, *, point_density=2., max_order=8, max_points=12000000,
+                 deterministic=False):
+        if cells.dim() != 2 or cells.shape[1] != 10:
+            raise ValueError('P2 transfer requires ten-node tetrahedra')
+        _lib.require_cuda(X)
+        self.grid = grid
+        self.node_count = X.shape[0]
+        self.cells = cells.contiguous()
+        cast = X.new_tensor
+        self.origin, self.spacing = cast(grid.origin), cast(grid.spacing)
+        self.limits = cast(grid.shape) - 2
+        self.diagonal = torch.zeros((X.shape[0], 3), device=X.device, dtype=X.dtype)  # rhs template
+        self.rules = RuleBuilder(X, self.cells, grid, point_density=point_density, max_order=max_order,
+                                 max_points=max_points)
+        self.deterministic = deterministic
+        self._csr = None
+
+    def rule(self, x):
+        return self.rules(x)
+
+    def prepare(self, x, *, buffers=None):
+        rule = self.rule(x)
+        base, phi = prepare(self, x, rule, buffers=buffers)
+        return SharedAdaptiveStencil(base, phi, rule)
+
+    def spread(self, coefficient, stencil):
+        return spread(self, coefficient, stencil)
+
+    def assemble_velocity(self, velocity, stencil):
+        if self.deterministic:
+            return assemble_velocity_deterministic(self, velocity, stencil)
+        return assemble_velocity(self, velocity, stencil)
+
+    def node_csr(self, rule):
+        """node -> (element*10+a) CSR over the rule's group order (built once per rule)."""
+        if self._csr is not None and self._csr[0] is rule:
+            return self._csr[1:]
+        slots, offset = [], 0
+        for g in rule.groups:
+            slots.append(g.cells.reshape(-1))
+        flat = torch.cat(slots)
+        order = torch.argsort(flat, stable=True)
+        counts = torch.bincount(flat, minlength=self.node_count)
+        crow = torch.zeros(self.node_count + 1, dtype=torch.int64, device=flat.device)
+        crow[1:] = torch.cumsum(counts, 0)
+        self._csr = (rule, crow, order.contiguous())
+        return crow, order
+
+
+def _tables_ok(base, phi, total, x):
+    return (base.shape == (2, total, 3) and phi.shape == (2, total, 3, 4) and base.dtype == torch.int64 and
+            phi.dtype == x.dtype and base.device == x.device and phi.device == x.device and
+            base.is_contiguous() and phi.is_contiguous())
+
+
+def prepare(transfer, x, rule, *, buffers=None):
+    """``p2_cuda_transfer.prepare`` (``:18-39``): positions and shared tables
+    of every group; ``ValueError`` when a point's support leaves the grid."""
+    _lib.require_cuda(x)
+    x = x.contiguous()
+    total = rule.point_count
+    if buffers is None:
+        base = torch.empty((2, total, 3), device=x.device, dtype=torch.int64)
+        phi = x.new_empty((2, total, 3, 4))
+    else:
+        base, phi = buffers
+        if not _tables_ok(base, phi, total, x):
+            raise ValueError('invalid P2 stencil buffers')
+    word = _lib.status_word(x.device)
+    word.zero_()
+    g = transfer.grid
+    limits = [n - 2 for n in g.shape]
+    offset = 0
+    for group in rule.groups:
+        call('afsi_b200_p2_prepare', ptr(x), x.shape[0], ptr(group.cells), group.cells.shape[0], ptr(group.values),
+             group.values.shape[0], _lib.doubles(g.origin), _lib.doubles(g.spacing), _lib.doubles(limits),
+             ptr(base), ptr(phi), total, offset, ptr(word), dtype_code(x.dtype), stream(x.device))
+        offset += group.weights.numel()
+    flags = int(word.item())
+    if flags:
+        word.zero_()
+        if flags & _lib.FLAG_INDEX:
+            raise RuntimeError('P2 connectivity outside the node range')
+        raise ValueError('MAC IB support reaches a wall or is nonfinite; enlarge/refine the fluid box')
+    return base, phi
+
+
+def spread(transfer, coefficient, stencil):
+    """``p2_cuda_transfer.spread`` (``:42-49``): nodal coefficients -> MAC face
+    fields, F_q = (N·coef)·W spread with weight/volume."""
+    _lib.require_cuda(coefficient)
+    coefficient = coefficient.contiguous()
+    g = transfer.grid
+    fields = g.zeros(device=coefficient.device, dtype=coefficient.dtype)
+    word = _lib.status_word(coefficient.device)
+    offset = 0
+    for group in stencil.rule.groups:
+        call('afsi_b200_p2_spread', ptr(coefficient), coefficient.shape[0], ptr(group.cells), group.cells.shape[0],
+             ptr(group.values), group.values.shape[0], ptr(group.weights), ptr(stencil.base), ptr(stencil.phi),
+             stencil.base.shape[1], offset, *(ptr(f) for f in fields), *g.shape, float(g.volume), ptr(word),
+             dtype_code(coefficient.dtype), stream(coefficient.device))
+        offset += group.weights.numel()
+    return fields
+
+
+def _velocity(transfer, velocity):
+    transfer.grid.check_velocity(velocity)
+    _lib.require_cuda(velocity[0])
+    return tuple(v.contiguous() for v in velocity)
+
+
+def assemble_velocity(transfer, velocity, stencil):
+    """``p2_cuda_transfer.assemble_velocity`` (``:52-60``): MAC velocity ->
+    nodal right-hand side rhs[a] = Σ_q N[q,a] W U(x_q)."""
+    velocity = _velocity(transfer, velocity)
+    rhs = torch.zeros_like(transfer.diagonal)
+    word = _lib.status_word(rhs.device)
+    g = transfer.grid
+    offset = 0
+    for group in stencil.rule.groups:
+        call('afsi_b200_p2_gather_assemble', *(ptr(v) for v in velocity), ptr(group.cells), group.cells.shape[0],
+             ptr(group.values), group.values.shape[0], ptr(group.weights), ptr(stencil.base), ptr(stencil.phi),
+             stencil.base.shape[1], offset, ptr(rhs), rhs.shape[0], *g.shape, ptr(word), dtype_code(rhs.dtype),
+             stream(rhs.device))
+        offset += group.weights.numel()
+    return rhs
+
+
+def assemble_velocity_deterministic(transfer, velocity, stencil):
+    """Same result as :func:`assemble_velocity`, bitwise reproducible: element
+    sums are written without atomics, then reduced per node in CSR order."""
+    velocity = _velocity(transfer, velocity)
+    rule = stencil.rule
+    elements = sum(grp.cells.shape[0] for grp in rule.groups)
+    local = torch.empty((elements, 10, 3), device=velocity[0].device, dtype=velocity[0].dtype)
+    word = _lib.status_word(local.device)
+    g = transfer.grid
+    offset, first = 0, 0
+    for group in rule.groups:
+        call('afsi_b200_p2_gather_local', *(ptr(v) for v in velocity), ptr(group.cells), group.cells.shape[0],
+             ptr(group.values), group.values.shape[0], ptr(group.weights), ptr(stencil.base), ptr(stencil.phi),
+             stencil.base.shape[1], offset, local[first:].data_ptr(), *g.shape, ptr(word), dtype_code(local.dtype),
+             stream(local.device))
+        offset += group.weights.numel()
+        first += group.cells.shape[0]
+    crow, slot = transfer.node_csr(rule)
+    rhs = torch.empty_like(transfer.diagonal)
+    call('afsi_b200_node_reduce', ptr(local), elements * 10, ptr(crow), ptr(slot), rhs.shape[0], ptr(rhs), 0,
+         ptr(word), dtype_code(rhs.dtype), stream(rhs.device))
+    return rhs

@@ -1,0 +1,364 @@
+"""Benchmark: IB transfer + MG V-cycle steps/s on the 3D P2 FP64 configuration.
+
+Workload (one step, FP64, 64^3 MAC grid on the unit cube):
+  P2 prepare (positions + shared Peskin tables) -> P2 spread of nodal forces
+  -> P2 gather-assemble of a face velocity -> multigrid pressure solve of a
+  mean-zero random right-hand side to 1e-10 relative residual (zero start).
+Structure: truncated prolate-spheroid P2 shell (inner/outer semi-axes
+0.25/0.32 by 0.15/0.22) of 38,400 elements, adaptive conical interaction
+quadrature at point density 2 (order 4 everywhere: 2,457,600 points).
+Inputs are seeded synthetic data; the 590 MB of stencil tables exceed the
+126 MB L2, so every step streams from HBM (no explicit L2 flush needed).
+
+``--impl b200`` (default) times the CUDA path; ``--impl reference`` times the
+CPU restatement of the reference algorithm (the oracle) on this host.  With
+``--gpus N`` under torchrun every rank runs an independent replica (the path
+does not shard); the reported value is the whole-job steps/s from the slowest
+rank.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SHELL = dict(nr=3, ntheta=40, nphi=64)
+GRID = dict(shape=(64, 64, 64), lengths=(1., 1., 1.))
+METRIC = 'IB transfer+MG V-cycle steps/s (P2 prepare+spread+interpolate+pressure MG solve, FP64)'
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='b200', choices=('b200', 'reference'))
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    return ap.parse_args()
+
+
+def workload():
+    from afsi_gpu_b200 import synthetic
+    from afsi_gpu_b200.grid import MACGrid
+    grid = MACGrid(GRID['shape'], GRID['lengths'])
+    X, cells = synthetic.p2_shell(**SHELL)
+    rng = np.random.default_rng(12)
+    coef = rng.standard_normal(X.shape)
+    vel = [v.numpy() for v in synthetic.fourier_velocity3d(grid, seed=3)]
+    rhs = synthetic.mean_free_normal(grid.shape, seed=4).numpy()
+    return grid, X, cells, coef, vel, rhs
+
+
+# ------------------------------------------------------------------- clocks
+
+class Clocks:
+    QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = Path(os.environ.get('TMPDIR', '/tmp')) / f'afsi_clocks_{os.getpid()}.csv'
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.index}', f'--query-gpu={self.QUERY}',
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=open(self.path, 'w'), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(', ') for r in self.path.read_text().strip().splitlines() if r.strip()]
+        except OSError:
+            return None
+        rows = [r for r in rows if len(r) >= 9]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.strip().lower() == 'active'})
+        return dict(sm_mhz=float(np.median(sm)) if sm else None,
+                    sm_max_mhz=float(rows[0][2]) if rows[0][2].replace('.', '').isdigit() else None,
+                    reasons=reasons, samples=len(rows))
+
+
+# ----------------------------------------------------------------- the step
+
+class Step:
+    """Device-resident inputs; one call = one hot-path step."""
+
+    def __init__(self, grid, X, cells, coef, vel, rhs, device):
+        from afsi_gpu_b200 import p2_cuda_transfer as p2t
+        from afsi_gpu_b200.multigrid import GeometricMultigrid
+        self.p2t = p2t
+        self.grid = grid
+        self.x = torch.as_tensor(X, device=device)
+        self.cells = torch.as_tensor(cells, device=device)
+        self.coef = torch.as_tensor(coef, device=device)
+        self.vel = tuple(torch.as_tensor(v, device=device) for v in vel)
+        self.rhs = torch.as_tensor(rhs, device=device)
+        self.tr = p2t.P2Transfer(grid, self.x, self.cells)
+        self.mg = GeometricMultigrid(grid, device=device, backend='b200-graph')
+        self.events = None
+        self.cycles = []
+
+    def __call__(self, x=None, coef=None, vel=None, rhs=None, timing=None):
+        x = self.x if x is None else x
+        st = self.tr.prepare(x)
+        ev = timing
+        if ev is not None:
+            ev[0].record()
+        fields = self.p2t.spread(self.tr, self.coef if coef is None else coef, st)
+        if ev is not None:
+            ev[1].record()
+        nodal = self.p2t.assemble_velocity(self.tr, self.vel if vel is None else vel, st)
+        if ev is not None:
+            ev[2].record()
+        p, info = self.mg.solve(self.rhs if rhs is None else rhs)
+        self.cycles.append(info['cycles'])
+        return st, fields, nodal, p
+
+
+def algorithmic_bytes(points, elements, nodes, faces, s=8):
+    """Bytes a launch must move at minimum (SURVEY-style accounting per unit).
+
+    Tables: base (2,P,3) int64 + phi (2,P,3,4) = 48 + 24*s per point.
+    spread: tables + W (s/pt) + cells (80/elem) + nodal coef gathered per
+    element (10*3*s) + face write (s/face).  gather: same reads with the face
+    field read instead of written, plus the nodal rhs written (3*s/node)."""
+    tables = points * (48 + 24 * s)
+    common = tables + points * s + elements * (80 + 30 * s)
+    return dict(prepare=tables + elements * 80 + nodes * 3 * s,
+                spread=common + faces * s,
+                gather=common + faces * s + nodes * 3 * s)
+
+
+def mg_bytes_per_cycle(shapes, smooth=4, s=8):
+    """Σ_l N_l·s·(6·smooth + 10.25): Jacobi read p,rhs / write p per sweep,
+    gauge passes, residual-restrict and prolong-add (SURVEY §8d formula)."""
+    return sum(np.prod(sh) * s * (6 * smooth + 10.25) for sh in shapes[:-1])
+
+
+def load_traffic():
+    path = ROOT / 'profiles' / 'traffic.json'
+    try:
+        return json.loads(path.read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def peaks():
+    try:
+        return json.loads((ROOT / 'MEASURED_PEAKS.json').read_text()), 'measured'
+    except (OSError, ValueError):
+        return dict(hbm_gbs=6650.0), 'fallback'
+
+
+# ----------------------------------------------------------- cpu baselines
+
+def cpu_step_time(grid, X, cells, coef, vel, rhs, fraction=0.05):
+    """Oracle (NumPy port of the reference algorithm) on a bounded sample:
+    the first `fraction` of the elements for the transfers (time scaled by the
+    point ratio) and the full 64^3 multigrid solve."""
+    from oracle import ib, mg
+    from afsi_gpu_b200.quadrature import conical_rule, tabulate_p2, reference_determinants
+    E = cells.shape[0]
+    Es = max(1, int(E * fraction))
+    sub = cells[:Es]
+    q, w = conical_rule(4)
+    N = tabulate_p2(q)
+    W = reference_determinants(torch.as_tensor(X), torch.as_tensor(sub)).numpy()[:, None] * w
+    t0 = time.perf_counter()
+    base, phi, _ = ib.p2_prepare(X, [(sub, N)], grid.origin, grid.spacing, grid.shape)
+    ib.p2_spread(coef, [(sub, N, W)], base, phi, grid.shape, grid.volume)
+    ib.p2_gather_assemble(vel, [(sub, N, W)], base, phi, grid.shape, X.shape[0])
+    t1 = time.perf_counter()
+    h = mg.Hierarchy(grid.shape, grid.spacing, 'neumann')
+    mg.solve(h, rhs)
+    t2 = time.perf_counter()
+    transfer = (t1 - t0) * (E / Es)
+    return transfer + (t2 - t1), dict(transfer_s=transfer, mg_s=t2 - t1, elements_sampled=Es, elements=E)
+
+
+# --------------------------------------------------------------------- main
+
+def dist_setup(args):
+    if args.gpus > 1 or 'RANK' in os.environ:
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = 'nccl' if args.impl == 'b200' else 'gloo'
+        if args.impl == 'b200':
+            torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
+        return dist, dist.get_rank(), dist.get_world_size()
+    return None, 0, 1
+
+
+def run_reference(args):
+    dist, rank, world = dist_setup(args)
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    grid, X, cells, coef, vel, rhs = workload()
+    cores = 1
+    times = []
+    for i in range(args.warmup + args.steps):
+        dt, info = cpu_step_time(grid, X, cells, coef, vel, rhs, fraction=0.02)
+        if i >= args.warmup:
+            times.append(dt)
+    step = float(np.mean(times))
+    sample = (f'oracle (NumPy restatement of the reference CPU path): P2 prepare/spread/gather-assemble on '
+              f'{info["elements_sampled"]} of {info["elements"]} elements, time scaled by elements; '
+              f'full 64^3 MG solve; {args.steps} steps after {args.warmup} warm-up')
+    value = 1.0 / step
+    line = dict(metric=METRIC, value=value, unit='steps/s', impl='reference', n_gpus=args.gpus, steps=args.steps,
+                warmup=args.warmup, ms_per_step=step * 1e3, higher_is_better=True, scaling='weak',
+                vs_baseline=None, dtype='f64', data='synthetic',
+                config=dict(workload='3D P2 shell 38400 elements / 2457600 points, 64^3 MAC, FP64'),
+                cpu_baseline=dict(value=value, unit='steps/s', cores=cores, kind='port', sample=sample),
+                e2e=dict(value=value, unit='steps/s', h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_b200(args):
+    dist, rank, world = dist_setup(args)
+    device = torch.device('cuda', torch.cuda.current_device())
+    from afsi_gpu_b200 import _lib
+    _lib.load()
+    grid, X, cells, coef, vel, rhs = workload()
+    step = Step(grid, X, cells, coef, vel, rhs, device)
+    stream = torch.cuda.current_stream(device)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    spread_ms, gather_ms = [], []
+    launches0 = _lib.launch_count()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(device.index) as clocks:
+        barrier()
+        start.record(stream)
+        for _ in range(args.steps):
+            step(timing=ev)
+            spread_ms.append((ev[0], ev[1]))
+            gather_ms.append((ev[1], ev[2]))
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        stop.record(stream)
+        barrier()
+    launches = _lib.launch_count() - launches0
+    elapsed = start.elapsed_time(stop) / 1e3
+    if dist:
+        t = torch.tensor([elapsed], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = t.item()
+    spread_t = float(np.mean([a.elapsed_time(b) for a, b in spread_ms])) / 1e3
+    gather_t = float(np.mean([a.elapsed_time(b) for a, b in gather_ms])) / 1e3
+
+    # end to end through the public API with pinned host buffers
+    host = dict(x=torch.as_tensor(X).pin_memory(), coef=torch.as_tensor(coef).pin_memory(),
+                vel=tuple(torch.as_tensor(v).pin_memory() for v in vel),
+                rhs=torch.as_tensor(rhs).pin_memory())
+    outs = None
+    h2d = (host['x'].numel() + host['coef'].numel() + sum(v.numel() for v in host['vel'])
+           + host['rhs'].numel()) * 8
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    e2e_steps = max(3, args.steps // 2)
+    d2h = 0
+    for _ in range(e2e_steps):
+        x = host['x'].to(device, non_blocking=True)
+        c = host['coef'].to(device, non_blocking=True)
+        v = tuple(a.to(device, non_blocking=True) for a in host['vel'])
+        r = host['rhs'].to(device, non_blocking=True)
+        st, fields, nodal, p = step(x, c, v, r)
+        outs = [f.to('cpu', non_blocking=True) for f in fields] + [nodal.to('cpu', non_blocking=True),
+                                                                  p.to('cpu', non_blocking=True)]
+        d2h = sum(o.numel() for o in outs) * 8
+    e1.record(stream)
+    barrier()
+    e2e_elapsed = e0.elapsed_time(e1) / 1e3
+    if dist:
+        t = torch.tensor([e2e_elapsed], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_elapsed = t.item()
+
+    if rank == 0:
+        pk, pk_kind = peaks()
+        P = step.tr.rule(step.x).point_count
+        faces = sum(np.prod(grid.face_shape(c)) for c in range(3))
+        ab = algorithmic_bytes(P, cells.shape[0], X.shape[0], faces)
+        dominant, dt = ('p2_spread', spread_t) if spread_t >= gather_t else ('p2_gather_assemble', gather_t)
+        byte_key = 'spread' if dominant == 'p2_spread' else 'gather'
+        achieved = ab[byte_key] / dt / 1e9
+        traffic = load_traffic().get(dominant)
+        cpu = None
+        if not args.no_cpu_baseline:
+            cpu_t, info = cpu_step_time(grid, X, cells, coef, vel, rhs, fraction=0.05)
+            cpu = dict(value=1 / cpu_t, unit='steps/s', cores=1, kind='port',
+                       sample=(f'oracle (NumPy restatement) on {info["elements_sampled"]} of {info["elements"]} '
+                               f'elements for the transfers (scaled by element count) + full 64^3 MG solve'))
+        line = dict(
+            metric=METRIC, value=world * args.steps / elapsed, unit='steps/s', n_gpus=world, steps=args.steps,
+            warmup=args.warmup, ms_per_step=elapsed / args.steps * 1e3, higher_is_better=True, scaling='weak',
+            vs_baseline=None, dtype='f64', data='synthetic',
+            config=dict(workload='3D P2 shell 38400 elements / 2457600 points, 64^3 MAC, FP64',
+                        grid=list(GRID['shape']), elements=int(cells.shape[0]), points=int(P),
+                        mg='Neumann V-cycles to 1e-10, Jacobi 2/3 x4, graph-replayed, cycles per solve '
+                           f'{sorted(set(step.cycles))}',
+                        l2='inputs larger than L2 (590 MB of stencil tables per step)',
+                        parallelism=f'replicas x{world}'),
+            roofline=dict(bound='hbm', kernel=dominant, achieved=achieved, peak=pk['hbm_gbs'], unit='GB/s',
+                          frac=achieved / pk['hbm_gbs'], peak_kind=pk_kind,
+                          traffic=(traffic * 1.0 if traffic else None),
+                          algorithmic_bytes=ab[byte_key], launch_ms=dt * 1e3,
+                          phases_ms=dict(spread=spread_t * 1e3, gather_assemble=gather_t * 1e3)),
+            e2e=dict(value=world * e2e_steps / e2e_elapsed, unit='steps/s', h2d_bytes_per_step=int(h2d),
+                     d2h_bytes_per_step=int(d2h)),
+            gpu_launches=int(launches),
+            clocks=clocks.summary(),
+            cpu_baseline=cpu)
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == 'reference':
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,225 @@
+/*
+ * afsi_b200.h — C-ABI of the B200 (sm_100a) IB-transfer and MAC-multigrid kernels.
+ *
+ * Every entry point takes raw device pointers, element counts, a dtype code
+ * and a CUDA stream, launches asynchronously on that stream and returns a
+ * host status (AFSI_OK or an AFSI_ERR_* code; afsi_b200_last_error() gives
+ * the message of the calling thread's last failure).  Data-dependent faults
+ * found on the device (support leaving the grid, a stencil index outside the
+ * grid, a non-finite value) never trap: the kernel ORs an AFSI_FLAG_* bit
+ * into the caller's device word `status` and skips the access.
+ *
+ * No entry point allocates, frees or synchronises, so every one may be
+ * recorded into a CUDA graph.  Layouts are row-major, contiguous, z (or y in
+ * 2D) fastest, exactly as the reference tensors.
+ *
+ * Reference interfaces replaced (paths inside afsi-torch 0.28.0,
+ * src/afsi_torch/):
+ *   indexed_gather / indexed_spread     mac/csrc/transfer.cpp:48-57
+ *   compact_gather / compact_spread     mac/csrc/transfer.cpp:50-51
+ *   p2_prepare_ / p2_spread_ /
+ *   p2_gather_assemble_                 mac/csrc/p2_transfer.cpp:66-74
+ *   compact prepare (_prepare)          mac/compact_transfer.py:21-26
+ *   2D reflected prepare (_prepare)     mac2d/transfer.py:61-81
+ *   MG kernel objects smooth / residual / restrict / residual_restrict /
+ *   prolong_add                          mac/_triton_mg.py:121-151,
+ *                                        mac2d/_triton_mg.py:78-100
+ *   V-cycle block + residual norm       mac/mg_workspace.py:85-133,
+ *                                        mac2d/mg_workspace.py:45-106
+ */
+#ifndef AFSI_B200_H
+#define AFSI_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* afsi_stream_t; /* same object as cudaStream_t */
+
+/* dtype codes */
+#define AFSI_F32 0
+#define AFSI_F64 1
+
+/* host status */
+#define AFSI_OK 0
+#define AFSI_ERR_ARG 1     /* invalid argument (shape, size, null pointer, dtype) */
+#define AFSI_ERR_CUDA 2    /* the CUDA runtime reported an error */
+
+/* device status bits (OR-ed into *status; the caller zeroes it) */
+#define AFSI_FLAG_SUPPORT 1  /* a point's 4-point support leaves the grid, or it is non-finite */
+#define AFSI_FLAG_INDEX 2    /* a stencil table addressed outside the grid/node range */
+#define AFSI_FLAG_OVERFLOW 4 /* a bounded table or buffer overflowed */
+
+/* Peskin weight forms: clamped two-branch kernel (ib.py:57-67, the torch
+ * path) or the shared radical (mac/csrc/p2_transfer.cu:36-43). */
+#define AFSI_PHI_CLAMPED 0
+#define AFSI_PHI_RADICAL 1
+
+const char* afsi_b200_last_error(void);
+int32_t afsi_b200_version(void);
+/* Kernels this process has launched through the library (graph replays excluded). */
+int64_t afsi_b200_launch_count(void);
+
+/* ------------------------------------------------------------------ prepare */
+
+/* Binning + 1D weights on `lattices` staggered lattices
+ * (mac/compact_transfer.py:21-26; shared face/centre tables of
+ * mac/shared_stencil.py:8-19 when lattices==2).
+ *   points (P,3); origins (lattices,3) and spacing (3) host arrays;
+ *   base (lattices,P,3) int64; phi (lattices,P,3,4).
+ * The support test of compact_transfer.py:94-96 (2 <= (x-grid_origin)/h <
+ * shape-2, finite) is fused: a failing point sets AFSI_FLAG_SUPPORT. */
+int32_t afsi_b200_compact_prepare(const void* points, int64_t count, int32_t lattices,
+    const double* origins, const double* spacing, const double* grid_origin,
+    const int64_t* shape, int32_t phi_form, int64_t* base, void* phi,
+    int32_t* status, int32_t dtype, afsi_stream_t stream);
+
+/* 2D reflected 4x4 stencils of both velocity components (mac2d/transfer.py:61-81).
+ *   points (P,2); ids (2,P,16) int64; weights (2,P,16).
+ * The support screen of mac2d/transfer.py:97-101 is fused (AFSI_FLAG_SUPPORT). */
+int32_t afsi_b200_indexed_prepare2d(const void* points, int64_t count, int64_t nx, int64_t ny,
+    double hx, double hy, double lx, double ly, int64_t* ids, void* weights,
+    int32_t* status, int32_t dtype, afsi_stream_t stream);
+
+/* P2 quadrature-point positions and shared face/centre tables for one
+ * quadrature group (p2_prepare_, mac/csrc/p2_transfer.cpp:55-63 and
+ * p2_transfer.cu:12-45).
+ *   x (nodes,3); cells (elements,10) int64; N (nq,10);
+ *   origin/spacing/limits host arrays (3); base (2,total,3); phi (2,total,3,4);
+ *   rows offset..offset+elements*nq are written. */
+int32_t afsi_b200_p2_prepare(const void* x, int64_t nodes, const int64_t* cells, int64_t elements,
+    const void* N, int64_t nq, const double* origin, const double* spacing, const double* limits,
+    int64_t* base, void* phi, int64_t total, int64_t offset, int32_t* status,
+    int32_t dtype, afsi_stream_t stream);
+
+/* ----------------------------------------------------------------- transfer */
+
+/* out[p,c] = sum_k field[ids[p,k],c]*w[p,k]   (indexed_gather) */
+int32_t afsi_b200_indexed_gather(const void* field, int64_t nodes, int64_t components,
+    const int64_t* ids, const void* weights, int64_t points, int64_t neighbors,
+    void* out, int32_t* status, int32_t dtype, afsi_stream_t stream);
+
+/* out[ids[p,k],c] += (field[p,c]*w[p,k])/volume   (indexed_spread).
+ * `out` (size,components) is accumulated into; zero it first for the
+ * reference's fresh-output semantics. */
+int32_t afsi_b200_indexed_spread(const void* field, int64_t points, int64_t components,
+    const int64_t* ids, const void* weights, int64_t neighbors, int64_t size, double volume,
+    void* out, int32_t* status, int32_t dtype, afsi_stream_t stream);
+
+/* One component of the separable 3D transfer (compact_gather):
+ * out[p] = sum_{ijk} field[(x*ny+y)*nz+z]*(phi_x[i]*phi_y[j])*phi_z[k].
+ *   base (P,3) int64, phi (P,3,4); nx,ny,nz = this component's face shape. */
+int32_t afsi_b200_compact_gather(const void* field, const int64_t* base, const void* phi,
+    int64_t points, int64_t nx, int64_t ny, int64_t nz, void* out,
+    int32_t* status, int32_t dtype, afsi_stream_t stream);
+
+/* One component of compact_spread, accumulating (w*f)/volume into `out`. */
+int32_t afsi_b200_compact_spread(const void* field, const int64_t* base, const void* phi,
+    int64_t points, int64_t nx, int64_t ny, int64_t nz, double volume, void* out,
+    int32_t* status, int32_t dtype, afsi_stream_t stream);
+
+/* P2 fused spread of one quadrature group (p2_spread_): for element e and
+ * point q, F = (sum_a N[q,a]*value[cells[e,a]])*W[e,q], spread with the shared
+ * tables rows offset+e*nq+q into the three MAC face arrays (accumulated).
+ * nx,ny,nz are cell counts. */
+int32_t afsi_b200_p2_spread(const void* value, int64_t nodes, const int64_t* cells, int64_t elements,
+    const void* N, int64_t nq, const void* W, const int64_t* base, const void* phi,
+    int64_t total, int64_t offset, void* u0, void* u1, void* u2,
+    int64_t nx, int64_t ny, int64_t nz, double volume, int32_t* status,
+    int32_t dtype, afsi_stream_t stream);
+
+/* P2 fused gather + FE assembly of one group (p2_gather_assemble_):
+ * rhs[cells[e,a],c] += sum_q N[q,a]*W[e,q]*U_c(q), accumulated atomically. */
+int32_t afsi_b200_p2_gather_assemble(const void* u0, const void* u1, const void* u2,
+    const int64_t* cells, int64_t elements, const void* N, int64_t nq, const void* W,
+    const int64_t* base, const void* phi, int64_t total, int64_t offset, void* rhs, int64_t nodes,
+    int64_t nx, int64_t ny, int64_t nz, int32_t* status, int32_t dtype, afsi_stream_t stream);
+
+/* Deterministic form of the assembly: element-local sums are written to
+ * local (elements,10,3) in a fixed order (no atomics); afsi_b200_node_reduce
+ * then sums them per node through a node->(element,slot) CSR. */
+int32_t afsi_b200_p2_gather_local(const void* u0, const void* u1, const void* u2,
+    const int64_t* cells, int64_t elements, const void* N, int64_t nq, const void* W,
+    const int64_t* base, const void* phi, int64_t total, int64_t offset, void* local,
+    int64_t nx, int64_t ny, int64_t nz, int32_t* status, int32_t dtype, afsi_stream_t stream);
+
+/* rhs[n,:] (+)= sum_{k in crow[n]..crow[n+1]} local[slot[k],:] for 3 components,
+ * slot = element*10+a; accumulate!=0 adds to rhs, else overwrites. */
+int32_t afsi_b200_node_reduce(const void* local, int64_t slots, const int64_t* crow,
+    const int64_t* slot, int64_t nodes, void* rhs, int32_t accumulate,
+    int32_t* status, int32_t dtype, afsi_stream_t stream);
+
+/* --------------------------------------------------------------- multigrid */
+
+/* Boundary conditions of the pressure operator */
+#define AFSI_BC_NEUMANN 0  /* closed box (mac/grid.py:86-93), singular, mean-zero gauge */
+#define AFSI_BC_CHANNEL 1  /* 2D inlet/outlet channel (mac2d/grid.py:61-71), p=0 outlet */
+#define AFSI_BC_PERIODIC 2 /* 2D periodic in x, Neumann walls in y, mean-zero gauge */
+
+/* Elementwise MG kernels on one level (the kernel-object interface of
+ * mac/_triton_mg.py:121-151 and mac2d/_triton_mg.py:78-100).
+ * shape = (nx,ny,nz) cells (nz=1 for 2D); h2 = h*h per axis;
+ * inv_h2 = 1/h**2 per axis (the diagonal terms). */
+int32_t afsi_b200_mg_smooth(const void* p, const void* rhs, void* out, const int64_t* shape,
+    const double* h2, const double* inv_h2, int32_t dim, int32_t bc, int32_t dtype,
+    afsi_stream_t stream);
+int32_t afsi_b200_mg_residual(const void* p, const void* rhs, void* out, const int64_t* shape,
+    const double* h2, int32_t dim, int32_t bc, int32_t dtype, afsi_stream_t stream);
+/* coarse = mean of the 2^dim children of fine; shape = fine shape */
+int32_t afsi_b200_mg_restrict(const void* fine, void* coarse, const int64_t* shape, int32_t dim,
+    int32_t dtype, afsi_stream_t stream);
+int32_t afsi_b200_mg_residual_restrict(const void* p, const void* rhs, void* coarse,
+    const int64_t* shape, const double* h2, int32_t dim, int32_t bc, int32_t dtype,
+    afsi_stream_t stream);
+/* fine += prolong(coarse); shape = fine shape */
+int32_t afsi_b200_mg_prolong_add(const void* coarse, void* fine, const int64_t* shape, int32_t dim,
+    int32_t bc, int32_t dtype, afsi_stream_t stream);
+
+#define AFSI_MG_MAX_LEVELS 12
+
+typedef struct afsi_mg_level {
+    int64_t shape[3];   /* cells per axis; shape[2]==1 in 2D */
+    double h2[3];       /* h*h */
+    double inv_h2[3];   /* 1/h**2 */
+    void* p;            /* canonical iterate */
+    void* ping;         /* Jacobi partner buffer */
+    void* rhs;          /* right-hand side */
+} afsi_mg_level;
+
+typedef struct afsi_mg_plan {
+    int32_t dim;           /* 2 or 3 */
+    int32_t bc;            /* AFSI_BC_* */
+    int32_t levels;        /* number of levels, finest first */
+    int32_t smooth;        /* Jacobi sweeps before and after the correction */
+    int32_t dtype;         /* dtype of p/ping/rhs */
+    int32_t coarse_dtype;  /* dtype of coarse_inverse */
+    afsi_mg_level level[AFSI_MG_MAX_LEVELS];
+    const void* coarse_inverse;  /* (n,n), n = cells on the coarsest level */
+    void* scratch;         /* reduction scratch, afsi_b200_mg_scratch_bytes() */
+} afsi_mg_plan;
+
+/* Bytes of device scratch (zero-initialised once by the caller) a plan needs. */
+int64_t afsi_b200_mg_scratch_bytes(const afsi_mg_plan* plan);
+
+/* `cycles` V-cycles on level 0 (mac/mg_workspace.py:85-102,
+ * mac2d/mg_workspace.py:53-62): weighted Jacobi (omega=2/3), residual
+ * restriction, recursive correction, dense coarsest solve, prolongation.
+ * p[0] and rhs[0] are read and p[0] is updated in place. */
+int32_t afsi_b200_mg_vcycles(const afsi_mg_plan* plan, int32_t cycles, afsi_stream_t stream);
+
+/* norm_out (device double) = || rhs[0] - A p[0] ||_2 (deterministic). */
+int32_t afsi_b200_mg_residual_norm(const afsi_mg_plan* plan, double* norm_out, afsi_stream_t stream);
+
+/* stats_out (device double[4]) = {sum(x), sum(|x|), sum(x^2), all finite ? 1 : 0}
+ * over n values (deterministic order). */
+int32_t afsi_b200_vector_stats(const void* x, int64_t n, double* stats_out, void* scratch,
+    int32_t dtype, afsi_stream_t stream);
+/* x -= mean, mean = stats[0]/n computed on the device. */
+int32_t afsi_b200_subtract_mean(void* x, int64_t n, const double* stats, int32_t dtype,
+    afsi_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

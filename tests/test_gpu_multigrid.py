@@ -1,0 +1,186 @@
+"""CUDA multigrid against the reference fixtures and the oracle (B200).
+
+Tolerances follow the reference's own tests
+(``tests/test_mac_multigrid_fused.py:13-86``, ``tests/test_valve_execution.py:13-41``):
+level kernels 2e-12 (FP64) / 2e-5 (FP32), one V-cycle 2e-11, solves 2e-8.
+"""
+import numpy as np
+import pytest
+import torch
+from conftest import golden
+from oracle import mg as oracle
+from afsi_gpu_b200 import synthetic
+from afsi_gpu_b200.grid import MACGrid, ChannelGrid
+from afsi_gpu_b200.multigrid import B200Kernels, GeometricMultigrid, ChannelMultigrid, MGOptions
+
+pytestmark = pytest.mark.gpu
+DEV = 'cuda'
+
+
+def t(a, dtype=torch.float64):
+    return torch.as_tensor(np.asarray(a), device=DEV, dtype=dtype)
+
+
+def close(actual, expected, rtol, atol):
+    np.testing.assert_allclose(actual.detach().cpu().double().numpy(), np.asarray(expected), rtol=rtol, atol=atol)
+
+
+@pytest.mark.parametrize('dtype', [torch.float64, torch.float32])
+def test_3d_level_kernels_match_reference_fixture(dtype):
+    g = golden('mg3d')
+    spacing = tuple(float(x) for x in g['spacing'])
+    k = B200Kernels('neumann')
+    pp, rr = t(g['pp'], dtype), t(g['rr'], dtype)
+    out = torch.full_like(pp, float('nan'))
+    tol = (0, 0) if dtype == torch.float64 else (2e-5, 2e-5)
+    scale = float(np.abs(g['residual']).max())
+    k.residual(pp, rr, out, spacing)
+    close(out, g['residual'], tol[0], tol[1] * scale)
+    k.smooth(pp, rr, None, out, spacing)
+    close(out, g['smoothed'], tol[0], tol[1] * scale)
+    coarse = torch.empty(tuple(n // 2 for n in g['pp'].shape), device=DEV, dtype=dtype)
+    k.restrict(pp, coarse)
+    close(coarse, g['restricted'], *tol)
+    k.residual_restrict(pp, rr, coarse, spacing)
+    close(coarse, g['residual_restricted'], tol[0], tol[1] * scale)
+    k.restrict(pp, coarse)
+    fine = pp.clone()
+    k.prolong_add(coarse, fine)
+    close(fine, g['prolonged'], 2e-15 if dtype == torch.float64 else 2e-5, 2e-15 if dtype == torch.float64 else 2e-5)
+    const = torch.full_like(pp, 7.)
+    k.residual(const, torch.zeros_like(pp), out, spacing)
+    assert out.abs().max().item() == 0
+
+
+def test_3d_single_block_cycle_and_solve_match_reference_fixture():
+    g = golden('mg3d')
+    grid = MACGrid(tuple(int(n) for n in g['shape']), tuple(float(x) for x in g['lengths']))
+    mg = GeometricMultigrid(grid, options=MGOptions(smooth=int(g['smooth'])), backend='b200')
+    rhs, start = g['rhs'], g['start']
+    mg.initialize(t(start), t(rhs - rhs.mean()))
+    cyc = mg.cycle().clone()
+    close(cyc, g['cycle'], 2e-11, 2e-12)
+    p, info = mg.solve(t(rhs), t(start))
+    assert info['cycles'] == int(g['cycles'])
+    close(p, g['solution'], 2e-8, 2e-9)
+
+
+@pytest.mark.parametrize('shape', [(32, 32, 32), (64, 64, 64), (16, 16, 32)])
+def test_3d_fused_cycle_matches_oracle(shape):
+    grid = MACGrid(shape, tuple(n / 32 for n in shape))
+    rng = np.random.default_rng(2)
+    rhs = rng.standard_normal(shape)
+    rhs -= rhs.mean()
+    start = .1 * rng.standard_normal(shape)
+    start -= start.mean()
+    for smooth in (4, 3):
+        h = oracle.Hierarchy(shape, grid.spacing, 'neumann')
+        ref = oracle.cycle(h, 0, start, rhs, smooth)
+        mg = GeometricMultigrid(grid, options=MGOptions(smooth=smooth), backend='b200')
+        mg.initialize(t(start), t(rhs))
+        got = mg.cycle()
+        close(got, ref, 2e-11, 2e-11 * np.abs(ref).max())
+
+
+def test_3d_solve_matches_reference_fixture_and_oracle_and_graphs():
+    g = golden('mg3d')
+    shape2 = tuple(int(n) for n in g['shape2'])
+    grid = MACGrid(shape2, tuple(float(x) for x in g['lengths2']))
+    for backend in ('b200', 'b200-graph'):
+        mg = GeometricMultigrid(grid, backend=backend)
+        p, info = mg.solve(t(g['rhs2']))
+        assert info['cycles'] == int(g['cycles2'])
+        close(p, g['solution2'], 2e-8, 2e-9)
+        assert info['residual_norm'] <= info['tolerance']
+    grid = MACGrid((64, 64, 64), (1., 1., 1.))
+    rhs = synthetic.mean_free_normal(grid.shape, seed=9).numpy()
+    ref, rinfo = oracle.solve(oracle.Hierarchy(grid.shape, grid.spacing, 'neumann'), rhs)
+    mg = GeometricMultigrid(grid, backend='b200-graph')
+    p, info = mg.solve(t(rhs))
+    assert info['cycles'] == rinfo['cycles']
+    close(p, ref, 2e-8, 2e-9 * np.abs(ref).max())
+
+
+def test_3d_solver_contract_errors_buffers_and_ownership():
+    grid = MACGrid((16, 16, 16), (1., 1., 1.))
+    mg = GeometricMultigrid(grid, backend='b200-graph')
+    rhs = t(synthetic.mean_free_normal(grid.shape, seed=1).numpy())
+    before = [x.data_ptr() for x in (*mg.workspace.p, *mg.workspace.ping, *mg.workspace.rhs)]
+    rhs_copy = rhs.clone()
+    p, _ = mg.solve(rhs)
+    p_copy = p.clone()
+    p2, _ = mg.solve(-rhs, p)
+    close(p2, (-p_copy).cpu().numpy(), 1e-7, 1e-8)
+    assert torch.equal(p, p_copy) and torch.equal(rhs, rhs_copy)
+    assert before == [x.data_ptr() for x in (*mg.workspace.p, *mg.workspace.ping, *mg.workspace.rhs)]
+    zero, info = mg.solve(torch.zeros_like(rhs))
+    assert info['cycles'] == 0 and zero.count_nonzero().item() == 0
+    with pytest.raises(ValueError, match='incompatible'):
+        mg.solve(torch.ones_like(rhs))
+    with pytest.raises(ValueError, match='invalid pressure RHS'):
+        mg.solve(torch.full_like(rhs, float('nan')))
+    with pytest.raises(ValueError, match='CUDA'):
+        GeometricMultigrid(grid, device='cpu')
+
+
+def test_channel_kernels_cycle_solve_match_reference_fixture():
+    g = golden('mg2d')
+    grid = ChannelGrid(tuple(int(n) for n in g['shape']), tuple(float(x) for x in g['lengths']))
+    k = B200Kernels('channel')
+    pp, rhs = t(g['pp']), t(g['rhs'])
+    out = torch.empty_like(pp)
+    k.residual(pp, rhs, out, grid.spacing)
+    close(out, g['residual'], 0, 0)
+    k.smooth(pp, rhs, None, out, grid.spacing)
+    close(out, g['smoothed'], 0, 0)
+    coarse = torch.empty(tuple(n // 2 for n in grid.shape), device=DEV, dtype=torch.float64)
+    k.residual_restrict(pp, rhs, coarse, grid.spacing)
+    close(coarse, g['residual_restricted'], 0, 0)
+    fine = pp.clone()
+    k.prolong_add(coarse, fine)
+    close(fine, g['prolonged'], 1e-14, 1e-13)
+    mg = ChannelMultigrid(grid, backend='b200')
+    mg.initialize(t(g['start']), rhs)
+    close(mg.cycle(), g['cycle'], 2e-12, 2e-13)
+    p, info = mg.solve(rhs)
+    assert info['cycles'] == int(g['cycles'])
+    close(p, g['solution'], 2e-8, 2e-9)
+    big = ChannelGrid(tuple(int(n) for n in g['shape_b']), tuple(float(x) for x in g['lengths_b']))
+    for backend in ('b200', 'b200-graph'):
+        mg = ChannelMultigrid(big, backend=backend)
+        p, info = mg.solve(t(g['rhs_b']))
+        assert info['cycles'] == int(g['cycles_b'])
+        close(p, g['solution_b'], 2e-8, 2e-9 * np.abs(g['solution_b']).max())
+
+
+@pytest.mark.parametrize('bc', ['channel', 'periodic'])
+def test_2d_fused_cycle_matches_oracle(bc):
+    shape = (256, 64)
+    grid = ChannelGrid(shape, (1., .25), periodic=bc == 'periodic')
+    rng = np.random.default_rng(3)
+    rhs = rng.standard_normal(shape)
+    if bc == 'periodic':
+        rhs -= rhs.mean()
+    start = .1 * rng.standard_normal(shape)
+    h = oracle.Hierarchy(shape, grid.spacing, bc)
+    if bc == 'periodic':
+        start -= start.mean()
+    ref = oracle.cycle(h, 0, start, rhs, 4)
+    mg = ChannelMultigrid(grid, backend='b200')
+    mg.initialize(t(start), t(rhs))
+    close(mg.cycle(), ref, 2e-11, 2e-11 * np.abs(ref).max())
+    pref, rinfo = oracle.solve(h, rhs)
+    p, info = ChannelMultigrid(grid, backend='b200-graph').solve(t(rhs))
+    assert info['cycles'] == rinfo['cycles']
+    close(p, pref, 2e-8, 2e-9 * np.abs(pref).max())
+
+
+def test_fp32_multigrid_converges_with_fp64_coarse_solve():
+    grid = MACGrid((64, 64, 64), (1., 1., 1.))
+    rhs = synthetic.mean_free_normal(grid.shape, seed=2)
+    mg = GeometricMultigrid(grid, dtype=torch.float32, coarse_dtype=torch.float64,
+                            options=MGOptions(rtol=1e-5), backend='b200-graph')
+    p, info = mg.solve(rhs.to(DEV, torch.float32))
+    ref, _ = oracle.solve(oracle.Hierarchy(grid.shape, grid.spacing, 'neumann'), rhs.numpy())
+    err = np.abs(p.double().cpu().numpy() - ref).max() / np.abs(ref).max()
+    assert info['residual_norm'] <= info['tolerance'] and err < 1e-4
