@@ -288,8 +288,8 @@ class _Solver:
             w.vector_stats(w.rhs[0], st[8:12])
         else:
             st[8:12].copy_(st[0:4])
-        norm = w.residual_norm()
-        v = torch.cat((st, norm)).tolist()
+        w.residual_norm()
+        v = torch.cat((st, w.norm)).tolist()
         return dict(rhs_sum=v[0], rhs_abs=v[1], rhs_finite=v[3], p_finite=v[7], rhs_sq=v[10], residual=v[12])
 
     def solve(self, rhs, initial=None, *, rtol=None):

@@ -202,6 +202,14 @@ def cpu_step_time(grid, X, cells, coef, vel, rhs, fraction=0.05):
 
 # --------------------------------------------------------------------- main
 
+def _json(o):
+    if isinstance(o, (np.integer,)):
+        return int(o)
+    if isinstance(o, (np.floating,)):
+        return float(o)
+    raise TypeError(type(o))
+
+
 def dist_setup(args):
     if args.gpus > 1 or 'RANK' in os.environ:
         import torch.distributed as dist
@@ -238,7 +246,7 @@ def run_reference(args):
                 config=dict(workload='3D P2 shell 38400 elements / 2457600 points, 64^3 MAC, FP64'),
                 cpu_baseline=dict(value=value, unit='steps/s', cores=cores, kind='port', sample=sample),
                 e2e=dict(value=value, unit='steps/s', h2d_bytes_per_step=0, d2h_bytes_per_step=0))
-    print(json.dumps(line))
+    print(json.dumps(line, default=_json))
     if dist:
         dist.destroy_process_group()
 
@@ -347,7 +355,7 @@ def run_b200(args):
             gpu_launches=int(launches),
             clocks=clocks.summary(),
             cpu_baseline=cpu)
-        print(json.dumps(line))
+        print(json.dumps(line, default=_json))
     if dist:
         dist.destroy_process_group()
 

@@ -217,15 +217,19 @@ def test_p2_raw_operators_match_reference_fixture():
     cuda_ib.check()
 
 
-@pytest.mark.parametrize('dtype', [torch.float64, torch.float32])
-def test_p2_shell_against_oracle(dtype):
-    """Synthetic shell (smaller than the benchmark): prepare bit-exact, spread and
+SMALL = dict(inner=(.125, .075, .075), outer=(.16, .11, .11))
+
+
+@pytest.mark.parametrize('dtype,n', [(torch.float64, 32), (torch.float32, 32), (torch.float64, 64)])
+def test_p2_shell_against_oracle(dtype, n):
+    """Half-size synthetic shell: 40k points in 2 quadrature groups on 32^3,
+    324k points in 5 groups on 64^3.  Prepare bit-exact (FP64), spread and
     gather-assemble within the parity bar."""
-    X, cells = synthetic.p2_shell(2, 12, 16)
-    grid = MACGrid((64, 64, 64), (1., 1., 1.))
+    X, cells = synthetic.p2_shell(2, 12, 16, **SMALL)
+    grid = MACGrid((n, n, n), (1., 1., 1.))
     npdt = np.float64 if dtype == torch.float64 else np.float32
     Xd = t(X.astype(npdt))
-    tr = p2t.P2Transfer(grid, Xd, t(cells))
+    tr = p2t.P2Transfer(grid, Xd, t(cells), max_order=22)
     st = tr.prepare(Xd)
     groups = [(gr.cells.cpu().numpy(), gr.values.cpu().numpy().astype(npdt)) for gr in st.rule.groups]
     ob, op, invalid = oracle.p2_prepare(X.astype(npdt), groups, grid.origin, grid.spacing, grid.shape)
@@ -254,9 +258,9 @@ def test_p2_shell_against_oracle(dtype):
 
 
 def test_p2_deterministic_assembly_is_bitwise_reproducible():
-    X, cells = synthetic.p2_shell(2, 12, 16)
-    grid = MACGrid((64, 64, 64), (1., 1., 1.))
-    tr = p2t.P2Transfer(grid, t(X), t(cells), deterministic=True)
+    X, cells = synthetic.p2_shell(2, 12, 16, **SMALL)
+    grid = MACGrid((32, 32, 32), (1., 1., 1.))
+    tr = p2t.P2Transfer(grid, t(X), t(cells), deterministic=True, max_order=22)
     st = tr.prepare(t(X))
     vel = tuple(v.to(DEV) for v in synthetic.fourier_velocity3d(grid, seed=4))
     a = tr.assemble_velocity(vel, st)
@@ -267,8 +271,8 @@ def test_p2_deterministic_assembly_is_bitwise_reproducible():
 
 
 def test_p2_support_violation_raises_value_error():
-    X, cells = synthetic.p2_shell(1, 6, 8)
-    grid = MACGrid((64, 64, 64), (1., 1., 1.))
-    tr = p2t.P2Transfer(grid, t(X), t(cells))
+    X, cells = synthetic.p2_shell(1, 8, 12, **SMALL)
+    grid = MACGrid((32, 32, 32), (1., 1., 1.))
+    tr = p2t.P2Transfer(grid, t(X), t(cells), max_order=22)
     with pytest.raises(ValueError, match='support'):
         tr.prepare(t(X) - .45)
