@@ -130,21 +130,26 @@ def prepare(transfer, x, rule, *, buffers=None):
     return base, phi
 
 
-def spread(transfer, coefficient, stencil):
+def spread(transfer, coefficient, stencil, *, events=None):
     """``p2_cuda_transfer.spread`` (``:42-49``): nodal coefficients -> MAC face
-    fields, F_q = (N·coef)·W spread with weight/volume."""
+    fields, F_q = (N·coef)·W spread with weight/volume.  ``events`` (two CUDA
+    events) bracket the native launches, excluding the output zero-fill."""
     _lib.require_cuda(coefficient)
     coefficient = coefficient.contiguous()
     g = transfer.grid
     fields = g.zeros(device=coefficient.device, dtype=coefficient.dtype)
     word = _lib.status_word(coefficient.device)
     offset = 0
+    if events is not None:
+        events[0].record()
     for group in stencil.rule.groups:
         call('afsi_b200_p2_spread', ptr(coefficient), coefficient.shape[0], ptr(group.cells), group.cells.shape[0],
              ptr(group.values), group.values.shape[0], ptr(group.weights), ptr(stencil.base), ptr(stencil.phi),
              stencil.base.shape[1], offset, *(ptr(f) for f in fields), *g.shape, float(g.volume), ptr(word),
              dtype_code(coefficient.dtype), stream(coefficient.device))
         offset += group.weights.numel()
+    if events is not None:
+        events[1].record()
     return fields
 
 
@@ -154,20 +159,25 @@ def _velocity(transfer, velocity):
     return tuple(v.contiguous() for v in velocity)
 
 
-def assemble_velocity(transfer, velocity, stencil):
+def assemble_velocity(transfer, velocity, stencil, *, events=None):
     """``p2_cuda_transfer.assemble_velocity`` (``:52-60``): MAC velocity ->
-    nodal right-hand side rhs[a] = Σ_q N[q,a] W U(x_q)."""
+    nodal right-hand side rhs[a] = Σ_q N[q,a] W U(x_q).  ``events`` bracket
+    the native launches."""
     velocity = _velocity(transfer, velocity)
     rhs = torch.zeros_like(transfer.diagonal)
     word = _lib.status_word(rhs.device)
     g = transfer.grid
     offset = 0
+    if events is not None:
+        events[0].record()
     for group in stencil.rule.groups:
         call('afsi_b200_p2_gather_assemble', *(ptr(v) for v in velocity), ptr(group.cells), group.cells.shape[0],
              ptr(group.values), group.values.shape[0], ptr(group.weights), ptr(stencil.base), ptr(stencil.phi),
              stencil.base.shape[1], offset, ptr(rhs), rhs.shape[0], *g.shape, ptr(word), dtype_code(rhs.dtype),
              stream(rhs.device))
         offset += group.weights.numel()
+    if events is not None:
+        events[1].record()
     return rhs
 
 

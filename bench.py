@@ -123,24 +123,31 @@ class Step:
         self.cycles = []
 
     def __call__(self, x=None, coef=None, vel=None, rhs=None, timing=None):
-        x = self.x if x is None else x
-        st = self.tr.prepare(x)
+        """timing: nine CUDA events: before prepare and after each of the four
+        phases, then the spread and gather-assemble kernels alone."""
         ev = timing
         if ev is not None:
             ev[0].record()
-        fields = self.p2t.spread(self.tr, self.coef if coef is None else coef, st)
+        st = self.tr.prepare(self.x if x is None else x)
         if ev is not None:
             ev[1].record()
-        nodal = self.p2t.assemble_velocity(self.tr, self.vel if vel is None else vel, st)
+        fields = self.p2t.spread(self.tr, self.coef if coef is None else coef, st,
+                                 events=None if ev is None else ev[5:7])
         if ev is not None:
             ev[2].record()
+        nodal = self.p2t.assemble_velocity(self.tr, self.vel if vel is None else vel, st,
+                                           events=None if ev is None else ev[7:9])
+        if ev is not None:
+            ev[3].record()
         p, info = self.mg.solve(self.rhs if rhs is None else rhs)
+        if ev is not None:
+            ev[4].record()
         self.cycles.append(info['cycles'])
         return st, fields, nodal, p
 
 
 def algorithmic_bytes(points, elements, nodes, faces, s=8):
-    """Bytes a launch must move at minimum (SURVEY-style accounting per unit).
+    """Bytes a launch must move at minimum, per unit of work.
 
     Tables: base (2,P,3) int64 + phi (2,P,3,4) = 48 + 24*s per point.
     spread: tables + W (s/pt) + cells (80/elem) + nodal coef gathered per
@@ -155,7 +162,7 @@ def algorithmic_bytes(points, elements, nodes, faces, s=8):
 
 def mg_bytes_per_cycle(shapes, smooth=4, s=8):
     """Σ_l N_l·s·(6·smooth + 10.25): Jacobi read p,rhs / write p per sweep,
-    gauge passes, residual-restrict and prolong-add (SURVEY §8d formula)."""
+    gauge passes, residual-restrict and prolong-add, per V-cycle."""
     return sum(np.prod(sh) * s * (6 * smooth + 10.25) for sh in shapes[:-1])
 
 
@@ -268,18 +275,16 @@ def run_b200(args):
     for _ in range(args.warmup):
         step()
     barrier()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-    spread_ms, gather_ms = [], []
+    phases = []
     launches0 = _lib.launch_count()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(device.index) as clocks:
         barrier()
         start.record(stream)
         for _ in range(args.steps):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(9)]
             step(timing=ev)
-            spread_ms.append((ev[0], ev[1]))
-            gather_ms.append((ev[1], ev[2]))
-            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            phases.append(ev)
         stop.record(stream)
         barrier()
     launches = _lib.launch_count() - launches0
@@ -288,8 +293,10 @@ def run_b200(args):
         t = torch.tensor([elapsed], device=device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed = t.item()
-    spread_t = float(np.mean([a.elapsed_time(b) for a, b in spread_ms])) / 1e3
-    gather_t = float(np.mean([a.elapsed_time(b) for a, b in gather_ms])) / 1e3
+    names = ('prepare', 'spread', 'gather_assemble', 'mg_solve')
+    phase_ms = {n: float(np.mean([ev[i].elapsed_time(ev[i + 1]) for ev in phases])) for i, n in enumerate(names)}
+    spread_t = float(np.mean([ev[5].elapsed_time(ev[6]) for ev in phases])) / 1e3
+    gather_t = float(np.mean([ev[7].elapsed_time(ev[8]) for ev in phases])) / 1e3
 
     # end to end through the public API with pinned host buffers
     host = dict(x=torch.as_tensor(X).pin_memory(), coef=torch.as_tensor(coef).pin_memory(),
@@ -349,7 +356,7 @@ def run_b200(args):
                           frac=achieved / pk['hbm_gbs'], peak_kind=pk_kind,
                           traffic=(traffic * 1.0 if traffic else None),
                           algorithmic_bytes=ab[byte_key], launch_ms=dt * 1e3,
-                          phases_ms=dict(spread=spread_t * 1e3, gather_assemble=gather_t * 1e3)),
+                          phases_ms=phase_ms),
             e2e=dict(value=world * e2e_steps / e2e_elapsed, unit='steps/s', h2d_bytes_per_step=int(h2d),
                      d2h_bytes_per_step=int(d2h)),
             gpu_launches=int(launches),
