@@ -77,11 +77,14 @@ _SIGNATURES = {
     'afsi_b200_mg_scratch_bytes': [ctypes.POINTER(MGPlan)],
     'afsi_b200_mg_vcycles': [ctypes.POINTER(MGPlan), c_int32, c_void_p],
     'afsi_b200_mg_residual_norm': [ctypes.POINTER(MGPlan), c_void_p, c_void_p],
+    'afsi_b200_mg_sync_bytes': [],
+    'afsi_b200_mg_persistent': [ctypes.POINTER(MGPlan), c_int32, c_int32, c_int32, c_double, c_void_p, c_void_p,
+                                c_void_p],
     'afsi_b200_vector_stats': [c_void_p, c_int64, c_void_p, c_void_p, c_int32, c_void_p],
     'afsi_b200_subtract_mean': [c_void_p, c_int64, c_void_p, c_int32, c_void_p],
 }
 _RESTYPES = {'afsi_b200_last_error': ctypes.c_char_p, 'afsi_b200_mg_scratch_bytes': ctypes.c_int64,
-             'afsi_b200_launch_count': ctypes.c_int64}
+             'afsi_b200_launch_count': ctypes.c_int64, 'afsi_b200_mg_sync_bytes': ctypes.c_int64}
 
 
 def exported_symbols():

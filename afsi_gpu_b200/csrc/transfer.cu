@@ -1,14 +1,14 @@
-// IB_4 spread / gather kernels: indexed (explicit ids), compact separable 3D
-// (one component), and the fused P2 element transfers.
+// IB_4 spread / gather kernels: indexed (explicit ids) and compact separable
+// 3D (one component), plus the C-ABI of the fused P2 element transfers whose
+// kernels live in p2.cu.
 //
-// Gather kernels are atomic-free and deterministic.  The compact and P2
-// gathers give each point a group of four lanes (one x-offset i per lane,
-// 16 (j,k) links each) so the L2-resident face field is read by four times
-// more threads in flight than points, and combine the lanes with shuffles.
-// Spreads add into the caller's pre-zeroed fields with fire-and-forget L2
-// reductions; the P2 kernels work one warp per element so the element's
-// nodal data are read once and shared by shuffles.
+// Gather kernels are atomic-free and deterministic.  The compact gather gives
+// each point a group of four lanes (one x-offset i per lane, 16 (j,k) links
+// each) so the L2-resident face field is read by four times more threads in
+// flight than points, and combines the lanes with shuffles.  Spreads add into
+// the caller's pre-zeroed fields with fire-and-forget L2 reductions.
 #include "common.cuh"
+#include "p2.cuh"
 
 namespace afsi {
 
@@ -101,186 +101,6 @@ __global__ void __launch_bounds__(256) compact_kernel(const T* __restrict__ f, c
         sum += __shfl_xor_sync(0xffffffffu, sum, 1);
         sum += __shfl_xor_sync(0xffffffffu, sum, 2);
         if (active && i == 0) out[p] = sum;
-    }
-}
-
-// --------------------------------------------------------------------- P2
-//
-// Shared tables: base (2,total,3), phi (2,total,3,4); component c reads the
-// face lattice (0) along axis c and the centre lattice (1) elsewhere
-// (mac/shared_stencil.py:8-19).  Face shapes: component c has n_c+1 faces
-// along axis c.
-
-struct P2Grid {
-    int64_t nx, ny, nz, total, offset, nq, nodes, elements;
-};
-
-// Per point: load the six 1D tables needed by component c.
-template <class T>
-__device__ __forceinline__ void p2_axis(const int64_t* base, const T* phi, int64_t total, int64_t row, int c,
-                                        int a, int64_t& b, const T*& w) {
-    const int64_t r = ((int64_t(a != c) * total) + row) * 3 + a;
-    b = base[r];
-    w = phi + r * 4;
-}
-
-// Warp per element, eight points in flight (four lanes each, lane i = x-offset).
-template <class T>
-__global__ void __launch_bounds__(256) p2_spread_kernel(const T* __restrict__ value, const int64_t* __restrict__ cells,
-                                                        const T* __restrict__ N, const T* __restrict__ W,
-                                                        const int64_t* __restrict__ base, const T* __restrict__ phi,
-                                                        T* __restrict__ u0, T* __restrict__ u1, T* __restrict__ u2,
-                                                        P2Grid g, T volume, int32_t* status) {
-    const int lane = threadIdx.x & 31;
-    const int64_t e = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    if (e >= g.elements) return;
-    const int slot = lane >> 2, i = lane & 3;
-    // lane l<30 holds value[cells[e,l/3], l%3]
-    int64_t node = lane < 10 ? cells[e * 10 + lane] : 0;
-    const bool bad = lane < 10 && (node < 0 || node >= g.nodes);
-    if (__any_sync(0xffffffffu, bad)) {
-        if (lane == 0) flag(status, AFSI_FLAG_INDEX);
-        return;
-    }
-    const int64_t mine = __shfl_sync(0xffffffffu, node, lane < 30 ? lane / 3 : 0);
-    const T coef = lane < 30 ? value[mine * 3 + lane % 3] : T(0);
-    T* fields[3] = {u0, u1, u2};
-    const int64_t ext[3][3] = {{g.nx + 1, g.ny, g.nz}, {g.nx, g.ny + 1, g.nz}, {g.nx, g.ny, g.nz + 1}};
-    for (int64_t q0 = 0; q0 < g.nq; q0 += 8) {
-        const int64_t q = q0 + slot;
-        const bool active = q < g.nq;
-        const int64_t qq = active ? q : 0;
-        T F[3] = {T(0), T(0), T(0)};
-#pragma unroll
-        for (int a = 0; a < 10; ++a) {
-            const T n = N[qq * 10 + a];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) F[c] += n * __shfl_sync(0xffffffffu, coef, a * 3 + c);
-        }
-        if (!active) continue;
-        const T wq = W[e * g.nq + q];
-        const int64_t row = g.offset + e * g.nq + q;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const T force = F[c] * wq;
-            int64_t bx, by, bz;
-            const T *wx, *wy, *wz;
-            p2_axis(base, phi, g.total, row, c, 0, bx, wx);
-            p2_axis(base, phi, g.total, row, c, 1, by, wy);
-            p2_axis(base, phi, g.total, row, c, 2, bz, wz);
-            if (!box_inside(bx, by, bz, ext[c][0], ext[c][1], ext[c][2])) {
-                if (i == 0) flag(status, AFSI_FLAG_INDEX);
-                continue;
-            }
-            const T px = wx[i];
-            T* dst0 = fields[c] + ((bx + i) * ext[c][1] + by) * ext[c][2] + bz;
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const T wxy = px * wy[j];
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    atomicAdd(dst0 + j * ext[c][2] + k, ((wxy * wz[k]) * force) / volume);
-            }
-        }
-    }
-}
-
-// Warp per element: U_c(q) by four-lane gather, then the element's 30 nodal
-// sums accumulated in registers (lane i holds nodes a = i, i+4, i+8) and
-// reduced over the eight point slots with shuffles.  Local mode writes the
-// element sums (no atomics); otherwise they are added to rhs.
-template <class T, bool Local>
-__global__ void __launch_bounds__(256) p2_gather_kernel(const T* __restrict__ u0, const T* __restrict__ u1,
-                                                        const T* __restrict__ u2, const int64_t* __restrict__ cells,
-                                                        const T* __restrict__ N, const T* __restrict__ W,
-                                                        const int64_t* __restrict__ base, const T* __restrict__ phi,
-                                                        T* __restrict__ out, P2Grid g, int32_t* status) {
-    const int lane = threadIdx.x & 31;
-    const int64_t e = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    if (e >= g.elements) return;
-    const int slot = lane >> 2, i = lane & 3;
-    const int64_t node = lane < 10 ? cells[e * 10 + lane] : 0;
-    const bool bad = lane < 10 && (node < 0 || node >= g.nodes);
-    if (__any_sync(0xffffffffu, bad)) {
-        if (lane == 0) flag(status, AFSI_FLAG_INDEX);
-        return;
-    }
-    const T* fields[3] = {u0, u1, u2};
-    const int64_t ext[3][3] = {{g.nx + 1, g.ny, g.nz}, {g.nx, g.ny + 1, g.nz}, {g.nx, g.ny, g.nz + 1}};
-    T acc[3][3];  // [node slot m (a=i+4m)][component]
-#pragma unroll
-    for (int m = 0; m < 3; ++m)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) acc[m][c] = T(0);
-    for (int64_t q0 = 0; q0 < g.nq; q0 += 8) {
-        const int64_t q = q0 + slot;
-        const bool active = q < g.nq;
-        const int64_t row = g.offset + e * g.nq + (active ? q : 0);
-        T U[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            T s = T(0);
-            int64_t bx, by, bz;
-            const T *wx, *wy, *wz;
-            p2_axis(base, phi, g.total, row, c, 0, bx, wx);
-            p2_axis(base, phi, g.total, row, c, 1, by, wy);
-            p2_axis(base, phi, g.total, row, c, 2, bz, wz);
-            if (active) {
-                if (!box_inside(bx, by, bz, ext[c][0], ext[c][1], ext[c][2])) {
-                    if (i == 0) flag(status, AFSI_FLAG_INDEX);
-                } else {
-                    const T px = wx[i];
-                    const T* src = fields[c] + ((bx + i) * ext[c][1] + by) * ext[c][2] + bz;
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const T wxy = px * wy[j];
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) s = fma(src[j * ext[c][2] + k], wxy * wz[k], s);
-                    }
-                }
-            }
-            s += __shfl_xor_sync(0xffffffffu, s, 1);
-            s += __shfl_xor_sync(0xffffffffu, s, 2);
-            U[c] = s;
-        }
-        if (active) {
-            const T wq = W[e * g.nq + q];
-#pragma unroll
-            for (int m = 0; m < 3; ++m) {
-                const int a = i + 4 * m;
-                if (a < 10) {
-                    const T nw = N[q * 10 + a] * wq;
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) acc[m][c] = fma(nw, U[c], acc[m][c]);
-                }
-            }
-        }
-    }
-    // reduce over the eight point slots (lanes i, i+4, ..., i+28)
-#pragma unroll
-    for (int m = 0; m < 3; ++m)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            T v = acc[m][c];
-            v += __shfl_xor_sync(0xffffffffu, v, 4);
-            v += __shfl_xor_sync(0xffffffffu, v, 8);
-            v += __shfl_xor_sync(0xffffffffu, v, 16);
-            acc[m][c] = v;
-        }
-    // node ids of a = i+4m live in lane a; fetch them with full-warp shuffles
-#pragma unroll
-    for (int m = 0; m < 3; ++m) {
-        const int a = i + 4 * m;
-        const int64_t nd = __shfl_sync(0xffffffffu, node, a < 10 ? a : 0);
-        if (slot == 0 && a < 10) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                if (Local)
-                    out[(e * 10 + a) * 3 + c] = acc[m][c];
-                else
-                    atomicAdd(out + nd * 3 + c, acc[m][c]);
-            }
-        }
     }
 }
 
@@ -401,14 +221,14 @@ extern "C" int32_t afsi_b200_p2_spread(const void* value, int64_t nodes, const i
     AFSI_REQUIRE(isfinite(volume) && volume > 0, "invalid P2 MAC grid");
     if (elements == 0) return AFSI_OK;
     AFSI_REQUIRE(value && cells && N && W && base && phi && u0 && u1 && u2, "null device pointer");
-    P2Grid g{nx, ny, nz, total, offset, nq, nodes, elements};
+    P2Dims g{nx, ny, nz, total, offset, nq, nodes, elements};
     AFSI_DISPATCH(dtype, {
-        p2_spread_kernel<T><<<blocks_for(elements * 32, 256), 256, 0, stream>>>(
-            static_cast<const T*>(value), cells, static_cast<const T*>(N), static_cast<const T*>(W), base,
-            static_cast<const T*>(phi), static_cast<T*>(u0), static_cast<T*>(u1), static_cast<T*>(u2), g, T(volume),
-            status);
+        return launch_spread_staged<T>(static_cast<const T*>(value), cells, static_cast<const T*>(N),
+                                       static_cast<const T*>(W), base, static_cast<const T*>(phi),
+                                       static_cast<T*>(u0), static_cast<T*>(u1), static_cast<T*>(u2), g, T(volume),
+                                       status, staged_blocks(elements), stream);
     });
-    return launched("p2_spread");
+    return AFSI_OK;
 }
 
 template <bool Local>
@@ -420,14 +240,14 @@ static int32_t p2_gather(const void* u0, const void* u1, const void* u2, const i
     if (rc) return rc;
     if (elements == 0) return AFSI_OK;
     AFSI_REQUIRE(u0 && u1 && u2 && cells && N && W && base && phi && out, "null device pointer");
-    P2Grid g{nx, ny, nz, total, offset, nq, nodes, elements};
+    P2Dims g{nx, ny, nz, total, offset, nq, nodes, elements};
     AFSI_DISPATCH(dtype, {
-        p2_gather_kernel<T, Local><<<blocks_for(elements * 32, 256), 256, 0, stream>>>(
-            static_cast<const T*>(u0), static_cast<const T*>(u1), static_cast<const T*>(u2), cells,
-            static_cast<const T*>(N), static_cast<const T*>(W), base, static_cast<const T*>(phi),
-            static_cast<T*>(out), g, status);
+        return launch_gather_staged<T, Local>(static_cast<const T*>(u0), static_cast<const T*>(u1),
+                                              static_cast<const T*>(u2), cells, static_cast<const T*>(N),
+                                              static_cast<const T*>(W), base, static_cast<const T*>(phi),
+                                              static_cast<T*>(out), g, status, staged_blocks(elements), stream);
     });
-    return launched(Local ? "p2_gather_local" : "p2_gather_assemble");
+    return AFSI_OK;
 }
 
 extern "C" int32_t afsi_b200_p2_gather_assemble(const void* u0, const void* u1, const void* u2,

@@ -170,6 +170,8 @@ class _Workspace:
         self.scratch = torch.zeros(int(nbytes), device=device, dtype=torch.uint8)
         plan.scratch = ptr(self.scratch)
         self.plan = plan
+        self.sync = torch.zeros(int(_lib.load().afsi_b200_mg_sync_bytes()), device=device, dtype=torch.uint8)
+        self.info = torch.zeros(3, device=device, dtype=torch.float64)
         self.stats = torch.zeros(12, device=device, dtype=torch.float64)
         self.norm = torch.zeros(1, device=device, dtype=torch.float64)
         self.stat_scratch = torch.zeros(4096 * 8 * 4 + 64, device=device, dtype=torch.uint8)
@@ -182,6 +184,13 @@ class _Workspace:
 
     def vcycles(self, count):
         call('afsi_b200_mg_vcycles', ctypes.byref(self.plan), count, stream(self.p[0].device))
+
+    def persistent(self, cycles, *, tol=None, check_every=1):
+        """`cycles` V-cycles in one cooperative launch; with `tol`, stop on the
+        device once the residual norm is <= tol (checked every `check_every`)."""
+        call('afsi_b200_mg_persistent', ctypes.byref(self.plan), int(cycles), 0 if tol is None else 1,
+             int(check_every), 0. if tol is None else float(tol), ptr(self.info), ptr(self.sync),
+             stream(self.p[0].device))
 
     def residual_norm(self):
         call('afsi_b200_mg_residual_norm', ctypes.byref(self.plan), ptr(self.norm), stream(self.p[0].device))
@@ -200,8 +209,8 @@ class _Solver:
 
     def __init__(self, grid, *, device='cuda', dtype=torch.float64, options=None, backend='b200-graph',
                  coarse_dtype=None):
-        if backend not in ('b200', 'b200-graph'):
-            raise ValueError('pressure backend must be b200 or b200-graph')
+        if backend not in ('b200', 'b200-graph', 'b200-persistent'):
+            raise ValueError('pressure backend must be b200, b200-graph or b200-persistent')
         device = torch.device(device)
         if device.type != 'cuda':
             raise ValueError('the B200 multigrid requires a CUDA device; there is no CPU fallback')
@@ -217,7 +226,8 @@ class _Solver:
         self.workspace = _Workspace(self.shapes, self.spacings, self.bc, dtype, device, self.options.smooth,
                                     self.coarse_dtype)
         self.workspace.set_coarse(self.coarse_inverse)
-        self.backend = self.kernels.name + ('-graph' if backend == 'b200-graph' else '')
+        self.backend = self.kernels.name + {'b200': '', 'b200-graph': '-graph', 'b200-persistent': '-persistent'}[backend]
+        self.persistent = backend == 'b200-persistent'
         self.graphs = {}
         if backend == 'b200-graph':
             self._capture()
@@ -250,6 +260,9 @@ class _Solver:
                 t.zero_()
 
     def advance(self, count):
+        if self.persistent:
+            self.workspace.persistent(count)
+            return self.workspace.p[0]
         if self.graphs:
             self.graphs[count].replay()
             _lib.count_replay(self.graph_launches[count])
@@ -318,6 +331,15 @@ class _Solver:
             raise RuntimeError('nonfinite multigrid residual or RHS norm')
         tol = max(self.options.atol, rtol * rhs_norm)
         cycle = 0
+        if self.persistent and residual > tol:
+            # whole loop on the device: same check schedule, one host read
+            w.persistent(self.options.max_cycles, tol=tol, check_every=self.options.check_every)
+            cycle, residual, failed = w.info.tolist()
+            cycle = int(cycle)
+            if failed:
+                raise RuntimeError('persistent multigrid barrier timed out')
+            if not isfinite(residual):
+                raise RuntimeError('nonfinite multigrid residual')
         while residual > tol and cycle < self.options.max_cycles:
             count = min(self.options.check_every, self.options.max_cycles - cycle)
             self.advance(count)

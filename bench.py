@@ -348,7 +348,7 @@ def run_b200(args):
             vs_baseline=None, dtype='f64', data='synthetic',
             config=dict(workload='3D P2 shell 38400 elements / 2457600 points, 64^3 MAC, FP64',
                         grid=list(GRID['shape']), elements=int(cells.shape[0]), points=int(P),
-                        mg='Neumann V-cycles to 1e-10, Jacobi 2/3 x4, graph-replayed, cycles per solve '
+                        mg='Neumann V-cycles to 1e-10, Jacobi 2/3 x4, graph-replayed blocks of 2, cycles per solve '
                            f'{sorted(set(step.cycles))}',
                         l2='inputs larger than L2 (590 MB of stencil tables per step)',
                         parallelism=f'replicas x{world}'),

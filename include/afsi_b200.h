@@ -208,6 +208,19 @@ int64_t afsi_b200_mg_scratch_bytes(const afsi_mg_plan* plan);
  * p[0] and rhs[0] are read and p[0] is updated in place. */
 int32_t afsi_b200_mg_vcycles(const afsi_mg_plan* plan, int32_t cycles, afsi_stream_t stream);
 
+/* Persistent form of the above: all cycles in one cooperative launch (one
+ * 1024-thread block per SM, grid barriers with a clock-bounded wait).
+ * solve == 0: run `cycles` V-cycles.  solve != 0: run V-cycles until the
+ * residual norm ||rhs[0] - A p[0]|| is <= tol, checked on the device after
+ * every `check_every` cycles and after the last of at most `cycles`
+ * (mac/multigrid.py:88-97); info (device double[3]) receives {cycles run,
+ * last residual norm or -1 if unchecked, 0 or 1 if a barrier timed out}.
+ * sync_scratch: afsi_b200_mg_sync_bytes() zero-initialised device bytes,
+ * private to one stream at a time. */
+int64_t afsi_b200_mg_sync_bytes(void);
+int32_t afsi_b200_mg_persistent(const afsi_mg_plan* plan, int32_t cycles, int32_t solve, int32_t check_every,
+    double tol, double* info, void* sync_scratch, afsi_stream_t stream);
+
 /* norm_out (device double) = || rhs[0] - A p[0] ||_2 (deterministic). */
 int32_t afsi_b200_mg_residual_norm(const afsi_mg_plan* plan, double* norm_out, afsi_stream_t stream);
 

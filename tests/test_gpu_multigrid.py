@@ -65,7 +65,7 @@ def test_3d_single_block_cycle_and_solve_match_reference_fixture():
     close(p, g['solution'], 2e-8, 2e-9)
 
 
-@pytest.mark.parametrize('shape', [(32, 32, 32), (64, 64, 64), (16, 16, 32)])
+@pytest.mark.parametrize('shape', [(32, 32, 32), (64, 64, 64), (16, 16, 32), (8, 12, 16)])
 def test_3d_fused_cycle_matches_oracle(shape):
     grid = MACGrid(shape, tuple(n / 32 for n in shape))
     rng = np.random.default_rng(2)
@@ -80,13 +80,22 @@ def test_3d_fused_cycle_matches_oracle(shape):
         mg.initialize(t(start), t(rhs))
         got = mg.cycle()
         close(got, ref, 2e-11, 2e-11 * np.abs(ref).max())
+        pm = GeometricMultigrid(grid, options=MGOptions(smooth=smooth), backend='b200-persistent')
+        pm.initialize(t(start), t(rhs))
+        close(pm.advance(1), ref, 2e-11, 2e-11 * np.abs(ref).max())
+        # two cycles in one launch equal two single launches
+        pm.initialize(t(start), t(rhs))
+        two = pm.advance(2).clone()
+        mg.initialize(t(start), t(rhs))
+        mg.cycle()
+        close(two, mg.cycle().cpu().numpy(), 1e-13, 1e-13 * np.abs(ref).max())
 
 
 def test_3d_solve_matches_reference_fixture_and_oracle_and_graphs():
     g = golden('mg3d')
     shape2 = tuple(int(n) for n in g['shape2'])
     grid = MACGrid(shape2, tuple(float(x) for x in g['lengths2']))
-    for backend in ('b200', 'b200-graph'):
+    for backend in ('b200', 'b200-graph', 'b200-persistent'):
         mg = GeometricMultigrid(grid, backend=backend)
         p, info = mg.solve(t(g['rhs2']))
         assert info['cycles'] == int(g['cycles2'])
@@ -95,10 +104,11 @@ def test_3d_solve_matches_reference_fixture_and_oracle_and_graphs():
     grid = MACGrid((64, 64, 64), (1., 1., 1.))
     rhs = synthetic.mean_free_normal(grid.shape, seed=9).numpy()
     ref, rinfo = oracle.solve(oracle.Hierarchy(grid.shape, grid.spacing, 'neumann'), rhs)
-    mg = GeometricMultigrid(grid, backend='b200-graph')
-    p, info = mg.solve(t(rhs))
-    assert info['cycles'] == rinfo['cycles']
-    close(p, ref, 2e-8, 2e-9 * np.abs(ref).max())
+    for backend in ('b200-graph', 'b200-persistent'):
+        mg = GeometricMultigrid(grid, backend=backend)
+        p, info = mg.solve(t(rhs))
+        assert info['cycles'] == rinfo['cycles']
+        close(p, ref, 2e-8, 2e-9 * np.abs(ref).max())
 
 
 def test_3d_solver_contract_errors_buffers_and_ownership():
@@ -146,7 +156,7 @@ def test_channel_kernels_cycle_solve_match_reference_fixture():
     assert info['cycles'] == int(g['cycles'])
     close(p, g['solution'], 2e-8, 2e-9)
     big = ChannelGrid(tuple(int(n) for n in g['shape_b']), tuple(float(x) for x in g['lengths_b']))
-    for backend in ('b200', 'b200-graph'):
+    for backend in ('b200', 'b200-graph', 'b200-persistent'):
         mg = ChannelMultigrid(big, backend=backend)
         p, info = mg.solve(t(g['rhs_b']))
         assert info['cycles'] == int(g['cycles_b'])
@@ -170,9 +180,13 @@ def test_2d_fused_cycle_matches_oracle(bc):
     mg.initialize(t(start), t(rhs))
     close(mg.cycle(), ref, 2e-11, 2e-11 * np.abs(ref).max())
     pref, rinfo = oracle.solve(h, rhs)
-    p, info = ChannelMultigrid(grid, backend='b200-graph').solve(t(rhs))
-    assert info['cycles'] == rinfo['cycles']
-    close(p, pref, 2e-8, 2e-9 * np.abs(pref).max())
+    for backend in ('b200-graph', 'b200-persistent'):
+        p, info = ChannelMultigrid(grid, backend=backend).solve(t(rhs))
+        assert info['cycles'] == rinfo['cycles']
+        close(p, pref, 2e-8, 2e-9 * np.abs(pref).max())
+    mg = ChannelMultigrid(grid, backend='b200-persistent')
+    mg.initialize(t(start), t(rhs))
+    close(mg.advance(1), ref, 2e-11, 2e-11 * np.abs(ref).max())
 
 
 def test_fp32_multigrid_converges_with_fp64_coarse_solve():
