@@ -1,0 +1,70 @@
+"""Switch an installed afsi-torch onto the B200 kernels.
+
+``install()`` rebinds, in place, the functions the reference resolves at call
+time:
+
+* ``afsi_torch.mac.cuda_ib.{build, require_cuda, indexed_gather,
+  indexed_spread, compact_gather, compact_spread}`` (``mac/cuda_ib.py:38-90``);
+* ``afsi_torch.mac.p2_cuda_transfer.{prepare, spread, assemble_velocity}``
+  (``mac/p2_cuda_transfer.py:18-60``), which ``AdaptiveFETransfer`` imports
+  inside its methods;
+* the CUDA kernel objects of the multigrid workspaces: ``MGWorkspace`` and
+  ``ChannelWorkspace`` import ``TritonKernels`` from ``mac._triton_mg`` /
+  ``mac2d._triton_mg`` when they are built (``mac/mg_workspace.py:36-47``,
+  ``mac2d/mg_workspace.py:28-40``); those modules are replaced by shims whose
+  ``TritonKernels`` is the B200 kernel object.
+
+Nothing is copied from the reference; the P1 CSR contraction operators are
+left untouched.  ``uninstall()`` restores the originals.
+"""
+import sys
+import types
+
+_saved = {}
+
+
+def _shim(name, bc):
+    from .multigrid import B200Kernels
+
+    def factory():
+        return B200Kernels(bc)
+
+    module = types.ModuleType(name)
+    module.TritonKernels = factory
+    module.__doc__ = f'B200 kernel objects standing in for {name}'
+    return module
+
+
+def install():
+    """Point afsi_torch's CUDA IB operators and MG kernel objects at this library."""
+    import afsi_torch.mac.cuda_ib as ref_ib
+    import afsi_torch.mac.p2_cuda_transfer as ref_p2
+    from . import cuda_ib, p2_cuda_transfer
+    for name in ('build', 'require_cuda', 'indexed_gather', 'indexed_spread', 'compact_gather', 'compact_spread'):
+        _saved.setdefault(('cuda_ib', name), getattr(ref_ib, name))
+        setattr(ref_ib, name, getattr(cuda_ib, name))
+    for name in ('prepare', 'spread', 'assemble_velocity'):
+        _saved.setdefault(('p2', name), getattr(ref_p2, name))
+        setattr(ref_p2, name, getattr(p2_cuda_transfer, name))
+    for module, bc in (('afsi_torch.mac._triton_mg', 'neumann'), ('afsi_torch.mac2d._triton_mg', 'channel')):
+        _saved.setdefault(('module', module), sys.modules.get(module))
+        sys.modules[module] = _shim(module, bc)
+        parent, _, leaf = module.rpartition('.')
+        if parent in sys.modules:
+            setattr(sys.modules[parent], leaf, sys.modules[module])
+
+
+def uninstall():
+    import afsi_torch.mac.cuda_ib as ref_ib
+    import afsi_torch.mac.p2_cuda_transfer as ref_p2
+    for (kind, name), value in list(_saved.items()):
+        if kind == 'cuda_ib':
+            setattr(ref_ib, name, value)
+        elif kind == 'p2':
+            setattr(ref_p2, name, value)
+        else:
+            if value is None:
+                sys.modules.pop(name, None)
+            else:
+                sys.modules[name] = value
+    _saved.clear()

@@ -1,0 +1,39 @@
+"""The drop-in switch rebinds afsi-torch's call targets (CPU; needs the reference source)."""
+import os
+import sys
+import pytest
+
+REF = os.environ.get('AFSI_TORCH_SRC', '/root/reference/src')
+
+
+@pytest.fixture
+def afsi_torch():
+    if not os.path.isdir(os.path.join(REF, 'afsi_torch')):
+        pytest.skip('afsi-torch source not available')
+    sys.path.insert(0, REF)
+    try:
+        import afsi_torch.mac.cuda_ib  # noqa: F401
+        yield
+    finally:
+        sys.path.remove(REF)
+
+
+def test_install_rebinds_ib_operators_and_mg_kernels(afsi_torch):
+    import afsi_torch.mac.cuda_ib as ref_ib
+    import afsi_torch.mac.p2_cuda_transfer as ref_p2
+    from afsi_gpu_b200 import dropin, cuda_ib, p2_cuda_transfer
+    from afsi_gpu_b200.multigrid import B200Kernels
+    original = ref_ib.compact_gather
+    dropin.install()
+    try:
+        assert ref_ib.compact_gather is cuda_ib.compact_gather
+        assert ref_ib.indexed_spread is cuda_ib.indexed_spread
+        assert ref_p2.assemble_velocity is p2_cuda_transfer.assemble_velocity
+        from afsi_torch.mac._triton_mg import TritonKernels
+        k = TritonKernels()
+        assert isinstance(k, B200Kernels) and k.dim == 3
+        from afsi_torch.mac2d._triton_mg import TritonKernels as Channel
+        assert Channel().dim == 2
+    finally:
+        dropin.uninstall()
+    assert ref_ib.compact_gather is original
