@@ -77,6 +77,8 @@ _SIGNATURES = {
     'afsi_b200_mg_scratch_bytes': [ctypes.POINTER(MGPlan)],
     'afsi_b200_mg_vcycles': [ctypes.POINTER(MGPlan), c_int32, c_void_p],
     'afsi_b200_mg_residual_norm': [ctypes.POINTER(MGPlan), c_void_p, c_void_p],
+    'afsi_b200_mg_residual_norm_noalloc': [c_void_p, c_void_p, P_I64, P_F64, c_int32, c_int32, c_void_p, c_int32,
+                                           c_void_p],
     'afsi_b200_mg_sync_bytes': [],
     'afsi_b200_mg_persistent': [ctypes.POINTER(MGPlan), c_int32, c_int32, c_int32, c_double, c_void_p, c_void_p,
                                 c_void_p],

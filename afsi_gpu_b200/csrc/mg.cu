@@ -34,6 +34,7 @@
 //  * every level with at most kCoarseCells cells, the dense coarsest solve
 //    included, runs inside one thread block in shared memory.
 #include <algorithm>
+#include <atomic>
 #include "mg_ops.cuh"
 
 namespace afsi {
@@ -636,4 +637,90 @@ extern "C" int32_t afsi_b200_mg_prolong_add(const void* coarse, void* fine, cons
         });
     });
     return launched("mg_prolong_add");
+}
+
+// ---- residual norm without any device allocation ----
+//
+// Some callers cannot allocate device memory at the moment they need a
+// residual norm: a solver driven from inside a region where the CUDA
+// allocator must not be called (for example while a CUDA graph is being
+// captured, where cudaMalloc would break the capture), a host application that
+// hands this library only its own fixed buffers (a Fortran/C code with a
+// preallocated pool, a real-time loop that forbids allocation after start-up),
+// or an embedding that has no PyTorch caching allocator to lend scratch.
+// afsi_b200_mg_residual_norm needs caller-provided reduction scratch; this
+// variant keeps its per-block partial sums in a file-scope device array
+// instead, so the caller passes only the inputs and the output.
+//
+// The array is sized for kNoAllocBlocks blocks (4096 partial sums plus a
+// result and a completion counter, about 32 KB); every GPU that loads the
+// library holds it until the process exits.  Grids whose launch needs more
+// blocks are rejected.  All calls share the one array: calls that overlap on
+// the GPU (different streams, no ordering between them) race and must not be
+// issued.
+
+namespace {
+
+constexpr int kNoAllocBlocks = 4096;
+
+struct NoAllocScratch {
+    double partial[kNoAllocBlocks];
+    double result;
+    unsigned int counter;
+};
+
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+// Device address of g_noalloc_scratch per device (the host-side symbol is only
+// a stand-in; the address is looked up once per device, with it current).
+std::atomic<NoAllocScratch*> g_noalloc_address[64];
+
+int32_t noalloc_scratch(NoAllocScratch** out) {
+    int device = 0;
+    cudaError_t err = cudaGetDevice(&device);
+    if (err != cudaSuccess) return fail(AFSI_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(err));
+    AFSI_REQUIRE(device >= 0 && device < 64, "device index %d out of range", device);
+    NoAllocScratch* p = g_noalloc_address[device].load(std::memory_order_acquire);
+    if (!p) {
+        void* addr = nullptr;
+        err = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+        if (err != cudaSuccess)
+            return fail(AFSI_ERR_CUDA, "cudaGetSymbolAddress(no-allocation scratch): %s", cudaGetErrorString(err));
+        p = static_cast<NoAllocScratch*>(addr);
+        g_noalloc_address[device].store(p, std::memory_order_release);
+    }
+    *out = p;
+    return AFSI_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t afsi_b200_mg_residual_norm_noalloc(const void* p, const void* rhs, const int64_t* shape,
+                                                      const double* h2, int32_t dim, int32_t bc, double* norm_out,
+                                                      int32_t dtype, afsi_stream_t stream) {
+    int32_t rc = check_bc(dim, bc);
+    if (rc || (rc = check_shape(shape, dim))) return rc;
+    AFSI_REQUIRE(p && rhs && h2 && norm_out, "null argument");
+    AFSI_REQUIRE(dtype == AFSI_F32 || dtype == AFSI_F64, "unsupported dtype code %d", (int)dtype);
+    const double one[3] = {1, 1, 1};
+    const Geometry probe = launch_for(make_level<double>(shape, h2, one, dim), bc);
+    AFSI_REQUIRE(probe.blocks <= kNoAllocBlocks,
+                 "grid needs %lld blocks; the no-allocation residual norm serves at most %d "
+                 "(use afsi_b200_mg_residual_norm with caller scratch)",
+                 (long long)probe.blocks, kNoAllocBlocks);
+    NoAllocScratch* scratch = nullptr;
+    if ((rc = noalloc_scratch(&scratch))) return rc;
+    // the completion counter must start at zero for every call
+    cudaError_t err = cudaMemsetAsync(&scratch->counter, 0, sizeof(unsigned int), stream);
+    if (err != cudaSuccess) return fail(AFSI_ERR_CUDA, "clearing no-allocation scratch: %s", cudaGetErrorString(err));
+    const Site site{scratch->partial, &scratch->counter, &scratch->result};
+    AFSI_BC_DISPATCH(bc, {
+        AFSI_DISPATCH(dtype, {
+            Lv<T> L = make_level<T>(shape, h2, one, dim);
+            const Geometry g = launch_for(L, BC);
+            residual_norm_kernel<BC, true, T><<<g.grid, g.block, 0, stream>>>(
+                static_cast<const T*>(p), static_cast<const T*>(rhs), L, site, norm_out);
+        });
+    });
+    return launched("mg_residual_norm_noalloc");
 }

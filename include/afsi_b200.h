@@ -224,6 +224,17 @@ int32_t afsi_b200_mg_persistent(const afsi_mg_plan* plan, int32_t cycles, int32_
 /* norm_out (device double) = || rhs[0] - A p[0] ||_2 (deterministic). */
 int32_t afsi_b200_mg_residual_norm(const afsi_mg_plan* plan, double* norm_out, afsi_stream_t stream);
 
+/* Same norm as afsi_b200_mg_residual_norm for one level (p, rhs of `shape`),
+ * for callers that cannot allocate device memory.  No counterpart in the
+ * reference (it always has PyTorch allocate).  Allocates nothing: its
+ * reduction scratch is a 32 KB file-scope device array, so grids needing more
+ * than 4096 reduction blocks (e.g. 256^3) are rejected with AFSI_ERR_ARG.  The
+ * first call on a device looks the array's address up (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  Every call shares the
+ * array: calls that overlap on the GPU race. */
+int32_t afsi_b200_mg_residual_norm_noalloc(const void* p, const void* rhs, const int64_t* shape,
+    const double* h2, int32_t dim, int32_t bc, double* norm_out, int32_t dtype, afsi_stream_t stream);
+
 /* stats_out (device double[4]) = {sum(x), sum(|x|), sum(x^2), all finite ? 1 : 0}
  * over n values (deterministic order). */
 int32_t afsi_b200_vector_stats(const void* x, int64_t n, double* stats_out, void* scratch,

@@ -1,0 +1,62 @@
+"""The no-allocation residual norm agrees with the scratch-using one (B200).
+
+``afsi_b200_mg_residual_norm_noalloc`` exists for callers that cannot allocate
+device memory when they need a residual norm: code that runs while a CUDA graph
+is being captured, host applications that hand the library only their own
+preallocated buffers, or embeddings without a caching allocator.  It keeps its
+reduction scratch in a fixed device array inside the library instead of in
+caller-provided memory.  This file is collected last so that a run stopping at
+the first failure has already run every other test.
+"""
+import ctypes
+import numpy as np
+import pytest
+import torch
+from afsi_gpu_b200 import _lib, synthetic
+from afsi_gpu_b200.grid import MACGrid, ChannelGrid
+from afsi_gpu_b200.multigrid import GeometricMultigrid, ChannelMultigrid
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc_norm(p, rhs, spacing, bc):
+    dim = p.dim()
+    out = torch.full((1,), float('nan'), device=p.device, dtype=torch.float64)
+    shape = list(p.shape) + [1] * (3 - dim)
+    h2 = [h * h for h in spacing] + [1.] * (3 - dim)
+    _lib.call('afsi_b200_mg_residual_norm_noalloc', p.data_ptr(), rhs.data_ptr(), _lib.int64s(shape),
+              _lib.doubles(h2), dim, bc, out.data_ptr(), _lib.dtype_code(p.dtype), _lib.stream(p.device))
+    return out[0]
+
+
+def _scratch_norm(solver, p, rhs):
+    solver.initialize(p, rhs)
+    return solver.residual_norm().clone()
+
+
+@pytest.mark.parametrize('dtype', [torch.float64, torch.float32])
+def test_noalloc_residual_norm_matches_scratch_version_twice_in_a_row(dtype):
+    grid = MACGrid((64, 48, 32), (1., .75, .5))
+    mg = GeometricMultigrid(grid, dtype=dtype, backend='b200')
+    rng = np.random.default_rng(21)
+    for trial in range(2):  # the shared array keeps the last call's contents
+        p = torch.as_tensor(rng.standard_normal(grid.shape), device='cuda', dtype=dtype)
+        rhs = torch.as_tensor(rng.standard_normal(grid.shape), device='cuda', dtype=dtype)
+        got = _noalloc_norm(p, rhs, grid.spacing, _lib.BC_NEUMANN)
+        ref = _scratch_norm(mg, p, rhs)
+        torch.testing.assert_close(got, ref, rtol=1e-13, atol=0)
+        assert got.item() > 0
+
+
+def test_noalloc_residual_norm_2d_channel_and_rejects_large_grids():
+    grid = ChannelGrid((256, 64), (8., 1.61))
+    mg = ChannelMultigrid(grid, backend='b200')
+    rng = np.random.default_rng(22)
+    for trial in range(2):
+        p = torch.as_tensor(rng.standard_normal(grid.shape), device='cuda')
+        rhs = torch.as_tensor(rng.standard_normal(grid.shape), device='cuda')
+        got = _noalloc_norm(p, rhs, grid.spacing, _lib.BC_CHANNEL)
+        torch.testing.assert_close(got, _scratch_norm(mg, p, rhs), rtol=1e-13, atol=0)
+    big = torch.zeros((256, 256, 256), device='cuda')
+    with pytest.raises(RuntimeError, match='at most 4096'):
+        _noalloc_norm(big, big, (1 / 256,) * 3, _lib.BC_NEUMANN)
