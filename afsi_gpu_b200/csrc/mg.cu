@@ -48,12 +48,10 @@ template <int BC, bool Exact, class T>
 __global__ void __launch_bounds__(kThreads) sweep_kernel(const T* __restrict__ p, T* __restrict__ rhs, T* __restrict__ out,
                                                          Lv<T> L, const double* p_sum, const double* rhs_sum,
                                                          Site emit, int fix_rhs, int do_emit) {
-    int x, y, z;
-    const bool mine = my_cell<BC>(L, x, y, z);
     double local = 0.0;
-    if (mine) {
-        const T m = T(site_mean(p_sum, L.n));
-        const T mr = T(site_mean(rhs_sum, L.n));
+    const T m = T(site_mean(p_sum, L.n));
+    const T mr = T(site_mean(rhs_sum, L.n));
+    for_my_cells<BC>(L, [&](int x, int y, int z) {
         const int64_t i = index_of(x, y, z, L);
         T r = rhs[i];
         if (fix_rhs) {
@@ -69,8 +67,8 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(const T* __restrict__ p
             v = T(0) + (omega<T>() * r) / diag_at<BC>(x, y, z, L);
         }
         out[i] = v;
-        local = double(v);
-    }
+        local += double(v);
+    });
     if (do_emit) site_finish(emit, local);
 }
 
@@ -80,15 +78,13 @@ template <int BC, bool Exact, class T>
 __global__ void __launch_bounds__(kThreads) residual_restrict_kernel(const T* __restrict__ p, const T* __restrict__ rhs,
                                                                      T* __restrict__ coarse, Lv<T> L, Lv<T> C,
                                                                      const double* p_sum, Site emit, int do_emit) {
-    int cx, cy, cz;
-    const bool mine = my_cell<BC>(C, cx, cy, cz);
     double local = 0.0;
-    if (mine) {
-        const T m = T(site_mean(p_sum, L.n));
+    const T m = T(site_mean(p_sum, L.n));
+    for_my_cells<BC>(C, [&](int cx, int cy, int cz) {
         const T v = restrict_residual_at<BC, Exact>(p, rhs, cx, cy, cz, L, m);
         coarse[index_of(cx, cy, cz, C)] = v;
-        local = double(v);
-    }
+        local += double(v);
+    });
     if (do_emit) site_finish(emit, local);
 }
 
@@ -96,11 +92,11 @@ __global__ void __launch_bounds__(kThreads) residual_restrict_kernel(const T* __
 template <int BC, class T>
 __global__ void __launch_bounds__(kThreads) prolong_kernel(const T* src, const T* __restrict__ corr, T* dst, Lv<T> L,
                                                            Lv<T> C, const double* src_sum, const double* corr_sum) {
-    int x, y, z;
-    if (!my_cell<BC>(L, x, y, z)) return;
     const T ms = T(site_mean(src_sum, L.n)), mc = T(site_mean(corr_sum, C.n));
-    const int64_t i = index_of(x, y, z, L);
-    dst[i] = (src[i] - ms) + prolong_at<BC>(corr, x, y, z, C, mc);
+    for_my_cells<BC>(L, [&](int x, int y, int z) {
+        const int64_t i = index_of(x, y, z, L);
+        dst[i] = (src[i] - ms) + prolong_at<BC>(corr, x, y, z, C, mc);
+    });
 }
 
 // dst = src - sum/n (or a copy when sum is null); flat grid-stride.
@@ -114,32 +110,30 @@ __global__ void __launch_bounds__(kThreads) shift_kernel(const T* src, T* dst, i
 template <int BC, bool Exact, class T>
 __global__ void __launch_bounds__(kThreads) residual_kernel(const T* __restrict__ p, const T* __restrict__ rhs,
                                                             T* __restrict__ out, Lv<T> L) {
-    int x, y, z;
-    if (!my_cell<BC>(L, x, y, z)) return;
-    const int64_t i = index_of(x, y, z, L);
-    const T pc = p[i];
-    out[i] = rhs[i] - neg_lap<BC, Exact>(p, i, x, y, z, L, T(0), pc);
+    for_my_cells<BC>(L, [&](int x, int y, int z) {
+        const int64_t i = index_of(x, y, z, L);
+        const T pc = p[i];
+        out[i] = rhs[i] - neg_lap<BC, Exact>(p, i, x, y, z, L, T(0), pc);
+    });
 }
 
 template <int BC, bool Exact, class T>
 __global__ void __launch_bounds__(kThreads) residual_norm_kernel(const T* __restrict__ p, const T* __restrict__ rhs,
                                                                  Lv<T> L, Site s, double* norm_out) {
-    int x, y, z;
     double local = 0.0;
-    if (my_cell<BC>(L, x, y, z)) {
+    for_my_cells<BC>(L, [&](int x, int y, int z) {
         const int64_t i = index_of(x, y, z, L);
         const T pc = p[i];
         const T r = rhs[i] - neg_lap<BC, Exact>(p, i, x, y, z, L, T(0), pc);
-        local = double(r) * double(r);
-    }
+        local += double(r) * double(r);
+    });
     site_finish(s, local, norm_out);
 }
 
 template <int BC, class T>
 __global__ void __launch_bounds__(kThreads) restrict_kernel(const T* __restrict__ fine, T* __restrict__ coarse,
                                                             Lv<T> L, Lv<T> C) {
-    int cx, cy, cz;
-    if (!my_cell<BC>(C, cx, cy, cz)) return;
+    for_my_cells<BC>(C, [&](int cx, int cy, int cz) {
     T v;
     if (BC == AFSI_BC_NEUMANN) {
         const int64_t j = index_of(2 * cx, 2 * cy, 2 * cz, L);
@@ -158,6 +152,7 @@ __global__ void __launch_bounds__(kThreads) restrict_kernel(const T* __restrict_
         v = ((fine[j] + fine[j + 1]) + fine[j + L.ny] + fine[j + L.ny + 1]) * T(.25);
     }
     coarse[index_of(cx, cy, cz, C)] = v;
+    });
 }
 
 // sum, sum|x|, sum x^2, finite flag over a flat vector
@@ -231,7 +226,11 @@ Geometry launch_for(const Lv<T>& L, int bc) {
     while (by > 1 && (by >> 1) >= mid && bx * (by >> 1) >= 32) by >>= 1;
     Geometry g;
     g.block = dim3(bx, by, 1);
-    g.grid = dim3((fast + bx - 1) / bx, (mid + by - 1) / by, slow);
+    const int gx = (fast + bx - 1) / bx, gy = (mid + by - 1) / by;
+    // cap the blocks (x slabs are strided inside the kernel) so that the
+    // completion counter of a reducing launch sees at most ~600 arrivals
+    const int cap = std::max(1, 592 / std::max(1, gx * gy));
+    g.grid = dim3(gx, gy, std::min(slow, cap));
     g.blocks = int64_t(g.grid.x) * g.grid.y * g.grid.z;
     return g;
 }
@@ -352,7 +351,7 @@ struct Runner {
         cl.last = plan->levels - 1;
         int64_t cells = 0;
         for (int k = l; k < plan->levels; ++k) cells += lv[k].n;
-        const size_t bytes = size_t(cells) * 3 * sizeof(T);
+        const size_t bytes = (size_t(cells) * 3 + 64 * size_t(plan->levels - l)) * sizeof(T);
         static bool configured = false;  // once per instantiation, before any graph capture of it
         if (!configured) {
             cudaFuncSetAttribute(coarse_kernel<BC, T, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024);
@@ -467,7 +466,7 @@ int32_t run_plan(const afsi_mg_plan* plan, int cycles, cudaStream_t stream) {
     for (int l = 0; l < plan->levels; ++l) {
         int64_t cells = 0;
         for (int k = l; k < plan->levels; ++k) cells += r.lv[k].n;
-        if (r.lv[l].n <= kCoarseCells && cells * 3 * int64_t(sizeof(T)) <= 200 * 1024) {
+        if (r.lv[l].n <= kCoarseCells && (cells * 3 + 64 * (plan->levels - l)) * int64_t(sizeof(T)) <= 200 * 1024) {
             r.first_coarse = l;
             break;
         }
@@ -655,7 +654,8 @@ extern "C" int32_t afsi_b200_mg_prolong_add(const void* coarse, void* fine, cons
 // The array is sized for kNoAllocBlocks blocks (4096 partial sums plus a
 // result and a completion counter, about 32 KB); every GPU that loads the
 // library holds it until the process exits.  Grids whose launch needs more
-// blocks are rejected.  All calls share the one array: calls that overlap on
+// blocks (2D grids above about 2^20 cells, 3D grids whose y-z section exceeds
+// about 2^20 cells) are rejected.  All calls share the one array: calls that overlap on
 // the GPU (different streams, no ordering between them) race and must not be
 // issued.
 

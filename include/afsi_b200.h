@@ -227,8 +227,10 @@ int32_t afsi_b200_mg_residual_norm(const afsi_mg_plan* plan, double* norm_out, a
 /* Same norm as afsi_b200_mg_residual_norm for one level (p, rhs of `shape`),
  * for callers that cannot allocate device memory.  No counterpart in the
  * reference (it always has PyTorch allocate).  Allocates nothing: its
- * reduction scratch is a 32 KB file-scope device array, so grids needing more
- * than 4096 reduction blocks (e.g. 256^3) are rejected with AFSI_ERR_ARG.  The
+ * reduction scratch is a 32 KB file-scope device array, so grids whose launch
+ * needs more than 4096 reduction blocks are rejected with AFSI_ERR_ARG (2D
+ * grids above about 2^20 cells; 3D grids whose y-z section exceeds about 2^20
+ * cells).  The
  * first call on a device looks the array's address up (cudaGetSymbolAddress);
  * make that first call before any stream capture.  Every call shares the
  * array: calls that overlap on the GPU race. */

@@ -57,6 +57,6 @@ def test_noalloc_residual_norm_2d_channel_and_rejects_large_grids():
         rhs = torch.as_tensor(rng.standard_normal(grid.shape), device='cuda')
         got = _noalloc_norm(p, rhs, grid.spacing, _lib.BC_CHANNEL)
         torch.testing.assert_close(got, _scratch_norm(mg, p, rhs), rtol=1e-13, atol=0)
-    big = torch.zeros((256, 256, 256), device='cuda')
+    big = torch.zeros((2048, 4096), device='cuda')  # 2^23 cells: 32768 reduction blocks
     with pytest.raises(RuntimeError, match='at most 4096'):
-        _noalloc_norm(big, big, (1 / 256,) * 3, _lib.BC_NEUMANN)
+        _noalloc_norm(big, big, (1 / 2048, 1 / 4096), _lib.BC_CHANNEL)
