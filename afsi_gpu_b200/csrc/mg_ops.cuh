@@ -91,22 +91,19 @@ __device__ __forceinline__ int64_t index_of(int x, int y, int z, const Lv<T>& L)
     return (int64_t(x) * L.ny + y) * L.nz + z;
 }
 
-// Cell of this thread in the 3D launch geometry (see launch_for); false if
-// the thread is padding.
-template <int BC, class T>
-__device__ __forceinline__ bool my_cell(const Lv<T>& L, int& x, int& y, int& z) {
+// Cells of this thread in the launch geometry of launch_for: the block covers
+// the two fastest axes; in 3D the grid's z dimension strides over x slabs
+// (the grid is capped, so one block may own several slabs).  f(x, y, z).
+template <int BC, class T, class F>
+__device__ __forceinline__ void for_my_cells(const Lv<T>& L, F f) {
     const int fast = blockIdx.x * blockDim.x + threadIdx.x;
     const int mid = blockIdx.y * blockDim.y + threadIdx.y;
     if (BC == AFSI_BC_NEUMANN) {
-        z = fast;
-        y = mid;
-        x = blockIdx.z;
-        return z < L.nz && y < L.ny;
+        if (fast >= L.nz || mid >= L.ny) return;
+        for (int x = blockIdx.z; x < L.nx; x += gridDim.z) f(x, mid, fast);
+    } else {
+        if (fast < L.ny && mid < L.nx) f(mid, fast, 0);
     }
-    y = fast;
-    x = mid;
-    z = 0;
-    return y < L.ny && x < L.nx;
 }
 
 // Coordinates of flat index i (single-block code only; 32-bit division).
@@ -238,6 +235,16 @@ __device__ __forceinline__ T prolong_at(const T* __restrict__ c, int x, int y, i
 }
 
 // ----------------------------------------------------------- coarse block
+//
+// All levels from `first` down run inside one thread block in shared memory.
+// The block works with fast arithmetic and, to keep the single SM busy,
+// without integer or floating-point division in the inner loops:
+//  * cell coordinates come from shifts when a level's extents are powers of
+//    two (division otherwise);
+//  * the Jacobi update multiplies by a reciprocal diagonal looked up in a
+//    per-level table of the 64 boundary classes (first/last cell per axis),
+//    built once per launch;
+//  * the dense coarsest solve is warp-cooperative (lanes over a row).
 
 template <class T>
 struct CoarseLevels {
@@ -245,7 +252,6 @@ struct CoarseLevels {
     int first, last;  // level indices handled here
 };
 
-// Block-wide mean (deterministic) of smem array a[0..n).
 template <class T>
 __device__ T block_mean(const T* a, int n, double* red) {
     double v = 0.0;
@@ -257,15 +263,62 @@ __device__ T block_mean(const T* a, int n, double* red) {
     return T(bcast);
 }
 
+template <class T>
+struct FastCoords {
+    int lz, ly, mz, my;
+    bool pow2;
+    __device__ void init(const Lv<T>& L) {
+        pow2 = !(L.nz & (L.nz - 1)) && !(L.ny & (L.ny - 1));
+        lz = __ffs(L.nz) - 1;
+        ly = __ffs(L.ny) - 1;
+        mz = L.nz - 1;
+        my = L.ny - 1;
+    }
+    __device__ __forceinline__ void get(int i, const Lv<T>& L, int& x, int& y, int& z) const {
+        if (pow2) {
+            z = i & mz;
+            y = (i >> lz) & my;
+            x = i >> (lz + ly);
+        } else {
+            coords32(i, L, x, y, z);
+        }
+    }
+};
+
+__device__ __forceinline__ int boundary_class(int x, int y, int z, int nx, int ny, int nz) {
+    return (x == 0) | ((x == nx - 1) << 1) | ((y == 0) << 2) | ((y == ny - 1) << 3) | ((z == 0) << 4) |
+           ((z == nz - 1) << 5);
+}
+
+// 1/diag for each of the 64 boundary classes of level L (diag_at order).
 template <int BC, class T>
-__device__ void block_smooth(T*& cur, T*& oth, const T* R, const Lv<T>& L, int smooth) {
+__device__ void reciprocal_table(const Lv<T>& L, T* table) {
+    for (int k = threadIdx.x; k < 64; k += blockDim.x) {
+        const int x = (k & 1) ? 0 : ((k & 2) ? L.nx - 1 : (L.nx > 2 ? 1 : 0));
+        const int y = (k & 4) ? 0 : ((k & 8) ? L.ny - 1 : (L.ny > 2 ? 1 : 0));
+        const int z = (k & 16) ? 0 : ((k & 32) ? L.nz - 1 : (L.nz > 2 ? 1 : 0));
+        // classes that cannot occur (first and last both set on an axis longer
+        // than one cell) get an unused value
+        table[k] = T(1) / diag_at<BC>(x, y, z, L);
+    }
+}
+
+template <int BC, class T>
+__device__ __forceinline__ T jacobi_at(const T* __restrict__ cur, const T* __restrict__ R, int i, int x, int y, int z,
+                                       const Lv<T>& L, const T* rdiag) {
+    const T pc = cur[i];
+    const T a = neg_lap<BC, false>(cur, i, x, y, z, L, T(0), pc);
+    return pc + (omega<T>() * (R[i] - a)) * rdiag[boundary_class(x, y, z, L.nx, L.ny, L.nz)];
+}
+
+template <int BC, class T>
+__device__ void block_smooth(T*& cur, T*& oth, const T* R, const Lv<T>& L, const FastCoords<T>& fc, const T* rdiag,
+                             int smooth) {
     for (int s = 0; s < smooth; ++s) {
         for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
             int x, y, z;
-            coords32(i, L, x, y, z);
-            const T pc = cur[i];
-            const T a = neg_lap<BC, false>(cur, i, x, y, z, L, T(0), pc);
-            oth[i] = pc + (omega<T>() * (R[i] - a)) / diag_at<BC>(x, y, z, L);
+            fc.get(i, L, x, y, z);
+            oth[i] = jacobi_at<BC>(cur, R, i, x, y, z, L, rdiag);
         }
         __syncthreads();
         T* t = cur;
@@ -277,90 +330,109 @@ __device__ void block_smooth(T*& cur, T*& oth, const T* R, const Lv<T>& L, int s
 // Levels first..last of one V-cycle in one CTA (fast arithmetic).  rhs of
 // level `first` comes from global memory (shifted by rhs_sum/n); p[first]
 // starts from p_global (first==0) or zero; the final p[first] is written to
-// p_out.
+// p_out.  smem holds, per level, p, its Jacobi partner and rhs, then the
+// reciprocal-diagonal tables.
 template <int BC, class T, class TC>
 __device__ void coarse_cycle(T* smem, const T* __restrict__ rhs_global, const double* rhs_sum, const T* p_global,
                              T* p_out, const TC* __restrict__ cinv, const CoarseLevels<T>& cl, int smooth) {
     __shared__ double red[32];
     constexpr bool singular = BC != AFSI_BC_CHANNEL;
-    T* P[AFSI_MG_MAX_LEVELS];
-    T* Q[AFSI_MG_MAX_LEVELS];
-    T* R[AFSI_MG_MAX_LEVELS];
-    {
-        T* cur = smem;
-        for (int l = cl.first; l <= cl.last; ++l) {
-            const int64_t n = cl.lv[l].n;
-            P[l] = cur;
-            Q[l] = cur + n;
-            R[l] = cur + 2 * n;
-            cur += 3 * n;
-        }
-    }
-    const int f = cl.first;
+    const int f = cl.first, last = cl.last;
+    // layout: [P_f Q_f R_f][P_f+1 ...]...[tables]
+    auto level_base = [&](int l) {
+        int64_t off = 0;
+        for (int k = f; k < l; ++k) off += 3 * cl.lv[k].n;
+        return smem + off;
+    };
+    T* tables = level_base(last + 1);
+    for (int l = f; l <= last; ++l) reciprocal_table<BC>(cl.lv[l], tables + 64 * (l - f));
     {
         const T mr = T(site_mean(rhs_sum, cl.lv[f].n));
+        T* P = level_base(f);
+        T* R = P + 2 * cl.lv[f].n;
         for (int i = threadIdx.x; i < cl.lv[f].n; i += blockDim.x) {
-            R[f][i] = rhs_global[i] - mr;
-            P[f][i] = p_global ? p_global[i] : T(0);
+            R[i] = rhs_global[i] - mr;
+            P[i] = p_global ? p_global[i] : T(0);
         }
     }
     __syncthreads();
     // down
-    for (int l = f; l <= cl.last; ++l) {
+    for (int l = f; l < last; ++l) {
         const Lv<T>& L = cl.lv[l];
-        if (l == cl.last) {
-            // dense coarsest solve p = inv * rhs (mac/mg_workspace.py:86-90)
-            for (int r = threadIdx.x; r < L.n; r += blockDim.x) {
-                double s = 0.0;
-                for (int j = 0; j < L.n; ++j) s += double(cinv[int64_t(r) * L.n + j]) * double(R[l][j]);
-                P[l][r] = T(s);
-            }
-            __syncthreads();
-            if (singular) {
-                const T m = block_mean(P[l], int(L.n), red);
-                for (int i = threadIdx.x; i < L.n; i += blockDim.x) P[l][i] = P[l][i] - m;
-                __syncthreads();
-            }
-            break;
-        }
-        T* cur = P[l];
-        T* oth = Q[l];
-        block_smooth<BC>(cur, oth, R[l], L, smooth);
-        const T m = singular ? block_mean(cur, int(L.n), red) : T(0);
-        for (int i = threadIdx.x; i < L.n; i += blockDim.x) P[l][i] = cur[i] - m;
-        __syncthreads();
         const Lv<T>& C = cl.lv[l + 1];
+        T* P = level_base(l);
+        T* Q = P + L.n;
+        T* R = Q + L.n;
+        T* Pc = level_base(l + 1);
+        T* Rc = Pc + 2 * C.n;
+        FastCoords<T> fcL, fcC;
+        fcL.init(L);
+        fcC.init(C);
+        T* cur = P;
+        T* oth = Q;
+        block_smooth<BC>(cur, oth, R, L, fcL, tables + 64 * (l - f), smooth);
+        const T m = singular ? block_mean(cur, int(L.n), red) : T(0);
+        for (int i = threadIdx.x; i < L.n; i += blockDim.x) P[i] = cur[i] - m;
+        __syncthreads();
         for (int c = threadIdx.x; c < C.n; c += blockDim.x) {
             int cx, cy, cz;
-            coords32(c, C, cx, cy, cz);
-            R[l + 1][c] = restrict_residual_at<BC, false>(P[l], R[l], cx, cy, cz, L, T(0));
-            P[l + 1][c] = T(0);
+            fcC.get(c, C, cx, cy, cz);
+            Rc[c] = restrict_residual_at<BC, false>(P, R, cx, cy, cz, L, T(0));
+            Pc[c] = T(0);
         }
         __syncthreads();
         if (singular) {
-            const T mc = block_mean(R[l + 1], int(C.n), red);
-            for (int i = threadIdx.x; i < C.n; i += blockDim.x) R[l + 1][i] = R[l + 1][i] - mc;
+            const T mc = block_mean(Rc, int(C.n), red);
+            for (int i = threadIdx.x; i < C.n; i += blockDim.x) Rc[i] = Rc[i] - mc;
+            __syncthreads();
+        }
+    }
+    // dense coarsest solve p = inv * rhs (mac/mg_workspace.py:86-90), warp per row
+    {
+        const Lv<T>& L = cl.lv[last];
+        T* P = level_base(last);
+        T* R = P + 2 * L.n;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+        for (int r = warp; r < L.n; r += warps) {
+            double s = 0.0;
+            for (int j = lane; j < L.n; j += 32) s += double(cinv[int64_t(r) * L.n + j]) * double(R[j]);
+            s = warp_sum(s);
+            if (lane == 0) P[r] = T(s);
+        }
+        __syncthreads();
+        if (singular) {
+            const T m = block_mean(P, int(L.n), red);
+            for (int i = threadIdx.x; i < L.n; i += blockDim.x) P[i] = P[i] - m;
             __syncthreads();
         }
     }
     // up
-    for (int l = cl.last - 1; l >= f; --l) {
+    for (int l = last - 1; l >= f; --l) {
         const Lv<T>& L = cl.lv[l];
         const Lv<T>& C = cl.lv[l + 1];
+        T* P = level_base(l);
+        T* Q = P + L.n;
+        T* R = Q + L.n;
+        const T* Pc = level_base(l + 1);
+        FastCoords<T> fcL;
+        fcL.init(L);
         for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
             int x, y, z;
-            coords32(i, L, x, y, z);
-            P[l][i] = P[l][i] + prolong_at<BC>(P[l + 1], x, y, z, C, T(0));
+            fcL.get(i, L, x, y, z);
+            P[i] = P[i] + prolong_at<BC>(Pc, x, y, z, C, T(0));
         }
         __syncthreads();
-        T* cur = P[l];
-        T* oth = Q[l];
-        block_smooth<BC>(cur, oth, R[l], L, smooth);
+        T* cur = P;
+        T* oth = Q;
+        block_smooth<BC>(cur, oth, R, L, fcL, tables + 64 * (l - f), smooth);
         const T m = singular ? block_mean(cur, int(L.n), red) : T(0);
-        for (int i = threadIdx.x; i < L.n; i += blockDim.x) P[l][i] = cur[i] - m;
+        for (int i = threadIdx.x; i < L.n; i += blockDim.x) P[i] = cur[i] - m;
         __syncthreads();
     }
-    for (int i = threadIdx.x; i < cl.lv[f].n; i += blockDim.x) p_out[i] = P[f][i];
+    {
+        const T* P = level_base(f);
+        for (int i = threadIdx.x; i < cl.lv[f].n; i += blockDim.x) p_out[i] = P[i];
+    }
     __syncthreads();
 }
 

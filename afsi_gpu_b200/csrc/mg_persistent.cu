@@ -345,7 +345,7 @@ int32_t run_persistent(const afsi_mg_plan* plan, int cycles, int solve, int chec
     for (int l = 0; l < plan->levels; ++l) {
         int64_t cells = 0;
         for (int k = l; k < plan->levels; ++k) cells += a.lv[k].n;
-        if (a.lv[l].n <= kCoarseCells && cells * 3 * int64_t(sizeof(T)) <= 200 * 1024) {
+        if (a.lv[l].n <= kCoarseCells && (cells * 3 + 64 * (plan->levels - l)) * int64_t(sizeof(T)) <= 200 * 1024) {
             a.first_coarse = l;
             break;
         }
@@ -355,7 +355,7 @@ int32_t run_persistent(const afsi_mg_plan* plan, int cycles, int solve, int chec
     a.coarse.last = plan->levels - 1;
     int64_t cells = 0;
     for (int k = a.first_coarse; k < plan->levels; ++k) cells += a.lv[k].n;
-    const size_t smem = size_t(cells) * 3 * sizeof(T);
+    const size_t smem = (size_t(cells) * 3 + 64 * size_t(plan->levels - a.first_coarse)) * sizeof(T);
     a.cinv = static_cast<const TC*>(plan->coarse_inverse);
     a.solve = solve;
     a.cycles = cycles;
