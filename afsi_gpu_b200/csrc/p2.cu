@@ -1,21 +1,27 @@
 // P2 element transfers (spread, gather-assemble) for the B200.
 //
 // One warp owns one P2 element at a time (grid-stride over elements) and
-// works on two quadrature points at once: each half-warp takes one point and
-// its 16 lanes own the (i,j) columns of the point's 4x4x4 support, with the
-// four z links of a column handled by that lane.
+// works on four quadrature points at once: lane group g = lane>>3 takes one
+// point, and its eight lanes own (x offset i, y offsets 2jp..2jp+1) of the
+// point's 4x4x4 support with all four z links — eight links per lane and
+// component.
 //
-// Spread: the element's contributions are accumulated into a shared-memory
-// box covering all its supports.  Each half-warp has a private copy of the
-// box, so the adds are plain read-modify-writes with a fixed order (points
-// h, h+2, h+4, ... in half h): no atomics.  The two copies are summed and
-// flushed to the face arrays with one L2 reduction per non-zero face — about
-// 400 per element instead of 192 per point.
-// Gather: the face values of the box are staged in shared memory once per
-// element; each point reads its 64 links from there and the 16 lanes reduce
-// with four shuffles.  The nodal sums Σ_q N[q,a] W U(x_q) are accumulated in
-// registers and added to the right-hand side (or written per element for the
-// deterministic node reduction).
+// Spread: for each velocity component in turn, the element's contributions
+// are accumulated into a shared-memory box covering the supports of that
+// component.  Each lane group has a private copy of the box, so the adds are
+// plain read-modify-writes in a fixed order (points g, g+4, g+8, ... in group
+// g): no atomics.  The four copies are summed and flushed to the face array
+// with one L2 reduction per non-zero face — about 130 per element and
+// component instead of 64 per point.
+// Gather: the face values of the element's boxes are staged in shared memory
+// once per element; each point reads its 64 links per component from there
+// and the eight lanes of a group reduce with three shuffles.  The nodal sums
+// Σ_q N[q,a] W U(x_q) are accumulated in registers and added to the
+// right-hand side (or written per element for the deterministic node
+// reduction).
+// While a warp works on one element it asks L2 for the stencil rows of the
+// next element it will take (cp.async.bulk.prefetch.L2), so the table stream
+// from HBM does not wait on the warp's own loads.
 // Point forces F = (Σ_a N[q,a] value[a]) * W (mac/compact_transfer.py:29-35)
 // are computed once per point by a lanes-over-points pass; the spread
 // contribution is (φx·φy)·φz · (F/volume), one division per point instead of
@@ -31,14 +37,9 @@ namespace afsi {
 
 constexpr int kWarps = 4;       // warps per block
 constexpr int kChunk = 64;      // points whose forces are held at once
-template <class T> struct BoxCap { static constexpr int value = 5120 / sizeof(T); };  // per copy (640 doubles)
-
-template <class T>
-struct SpreadStage {
-    T f[3][kChunk];
-    T coef[32];
-    T copy[2][BoxCap<T>::value];
-};
+template <class T> struct BoxCap { static constexpr int value = 4608 / sizeof(T); };  // gather patch (576 doubles)
+constexpr int kCompCap = 224;     // spread: entries of one component's box per copy
+constexpr int kCompStride = 232;  // copy stride; the 8-entry pad puts the copies on different banks
 
 template <class T>
 struct GatherStage {
@@ -92,20 +93,61 @@ __device__ __forceinline__ void element_box(const int64_t* __restrict__ base, co
             bx.lo[c][a] = mn[c][a];
             bx.ext[c][a] = mx[c][a] - mn[c][a] + 4;
         }
-    bx.off[0] = 0;
+    bx.off[0] = 0;  // patch offsets, meaningful when box_fits holds
 #pragma unroll
-    for (int c = 0; c < 3; ++c) bx.off[c + 1] = bx.off[c] + bx.ext[c][0] * bx.ext[c][1] * bx.ext[c][2];
+    for (int c = 0; c < 3; ++c) bx.off[c + 1] = bx.off[c] + int(min(int64_t(bx.ext[c][0]) * bx.ext[c][1] * bx.ext[c][2], int64_t(1) << 20));
 }
 
-template <class T>
-__device__ __forceinline__ bool box_fits(const Box& bx, const P2Dims& g) {
-    const int64_t fe[3][3] = {{g.nx + 1, g.ny, g.nz}, {g.nx, g.ny + 1, g.nz}, {g.nx, g.ny, g.nz + 1}};
+__device__ __forceinline__ bool component_inside(const Box& bx, const P2Dims& g, int c) {
+    const int64_t fe[3] = {g.nx + (c == 0), g.ny + (c == 1), g.nz + (c == 2)};
     bool inside = true;
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
+    for (int a = 0; a < 3; ++a) inside = inside && bx.lo[c][a] >= 0 && int64_t(bx.lo[c][a]) + bx.ext[c][a] <= fe[a];
+    return inside;
+}
+
+__device__ __forceinline__ int64_t component_cells(const Box& bx, int c) {
+    return int64_t(bx.ext[c][0]) * bx.ext[c][1] * bx.ext[c][2];
+}
+
+// All three boxes lie in their face arrays and fit one gather patch.
+template <class T>
+__device__ __forceinline__ bool box_fits(const Box& bx, const P2Dims& g) {
+    int64_t cells = 0;
+    bool inside = true;
 #pragma unroll
-        for (int a = 0; a < 3; ++a) inside = inside && bx.lo[c][a] >= 0 && bx.lo[c][a] + bx.ext[c][a] <= fe[c][a];
-    return inside && bx.off[3] <= BoxCap<T>::value;
+    for (int c = 0; c < 3; ++c) {
+        inside = inside && component_inside(bx, g, c);
+        cells += component_cells(bx, c);
+    }
+    return inside && cells <= BoxCap<T>::value;
+}
+
+// Component c's box lies in its face array and fits one spread copy.
+__device__ __forceinline__ bool component_fits(const Box& bx, const P2Dims& g, int c) {
+    return component_inside(bx, g, c) && component_cells(bx, c) <= kCompCap;
+}
+
+// Ask L2 for [p, p+bytes) rounded inward to 16-byte boundaries.
+__device__ __forceinline__ void prefetch_l2(const void* p, int64_t bytes) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uintptr_t lo = (a + 15) & ~uintptr_t(15), hi = (a + uintptr_t(bytes)) & ~uintptr_t(15);
+    if (hi > lo && hi - lo < (uintptr_t(1) << 31))
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"(uint32_t(hi - lo)) : "memory");
+}
+
+// Lanes 0..4 of a warp prefetch the stencil rows and weights of element e.
+template <class T>
+__device__ __forceinline__ void prefetch_element(const int64_t* base, const T* phi, const T* W, const P2Dims& g,
+                                                 int64_t e, int lane) {
+    if (e >= g.elements || lane >= 5) return;
+    const int64_t row = g.offset + e * g.nq;
+    if (lane < 2)
+        prefetch_l2(base + (lane * g.total + row) * 3, g.nq * 3 * int64_t(sizeof(int64_t)));
+    else if (lane < 4)
+        prefetch_l2(phi + ((lane - 2) * g.total + row) * 12, g.nq * 12 * int64_t(sizeof(T)));
+    else
+        prefetch_l2(W + e * g.nq, g.nq * int64_t(sizeof(T)));
 }
 
 __device__ __forceinline__ int64_t face_index(const P2Dims& g, int c, int x, int y, int z) {
@@ -118,7 +160,59 @@ __device__ __forceinline__ bool point_inside(const P2Dims& g, int c, int x, int 
            z + 3 < g.nz + (c == 2);
 }
 
+// ------------------------------------------------------------------ lanes
+//
+// Lane layout: group g = lane>>3 takes one of four points in flight; within a
+// group, lane bits (i = (lane>>1)&3, jp = lane&1) own the x offset i and the
+// y offsets 2jp, 2jp+1 of the point's support, and all four z offsets: eight
+// links per component.  The z row of four weights is one 32-byte pair of
+// vector loads.
+
+template <class T> struct Pair;
+template <> struct Pair<double> { using type = double2; };
+template <> struct Pair<float> { using type = float2; };
+
+template <class T>
+__device__ __forceinline__ void load_row4(const T* __restrict__ w, T out[4]) {
+    using P = typename Pair<T>::type;
+    const P a = reinterpret_cast<const P*>(w)[0];
+    const P b = reinterpret_cast<const P*>(w)[1];
+    out[0] = a.x;
+    out[1] = a.y;
+    out[2] = b.x;
+    out[3] = b.y;
+}
+
+// One point's view for component c: support origin and the weights this lane needs.
+template <class T>
+struct PointView {
+    int gx, gy, gz;
+    T wx, wy0, wy1, wz[4];
+};
+
+template <class T>
+__device__ __forceinline__ void point_view(const int64_t* __restrict__ base, const T* __restrict__ phi, int64_t total,
+                                           int64_t row, int c, int li, int ljp, PointView<T>& v) {
+    const int64_t rx = table_row(total, row, c, 0), ry = table_row(total, row, c, 1), rz = table_row(total, row, c, 2);
+    v.gx = int(base[rx]);
+    v.gy = int(base[ry]);
+    v.gz = int(base[rz]);
+    v.wx = phi[rx * 4 + li];
+    using P = typename Pair<T>::type;
+    const P y = reinterpret_cast<const P*>(phi + ry * 4)[ljp];
+    v.wy0 = y.x;
+    v.wy1 = y.y;
+    load_row4(phi + rz * 4, v.wz);
+}
+
 // ------------------------------------------------------------------ spread
+
+template <class T>
+struct SpreadStage {
+    T f[kChunk];
+    T coef[32];
+    T copy[4][kCompStride];
+};
 
 template <class T>
 __global__ void __launch_bounds__(kWarps * 32) p2_spread_kernel(const T* __restrict__ value,
@@ -130,77 +224,75 @@ __global__ void __launch_bounds__(kWarps * 32) p2_spread_kernel(const T* __restr
                                                                 T volume, int32_t* status) {
     __shared__ SpreadStage<T> stage_all[kWarps];
     SpreadStage<T>& s = stage_all[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31, half = lane >> 4, li = (lane >> 2) & 3, lj = lane & 3;
+    const int lane = threadIdx.x & 31, grp = lane >> 3, li = (lane >> 1) & 3, ljp = lane & 1;
     const int64_t warps = int64_t(gridDim.x) * kWarps;
     T* fields[3] = {u0, u1, u2};
-    for (int64_t e = int64_t(blockIdx.x) * kWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
+    int64_t e = int64_t(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+    prefetch_element(base, phi, W, g, e, lane);
+    for (; e < g.elements; e += warps) {
+        prefetch_element(base, phi, W, g, e + warps, lane);
         const int64_t node = lane < 10 ? cells[e * 10 + lane] : 0;
         if (__any_sync(0xffffffffu, lane < 10 && (node < 0 || node >= g.nodes))) {
             if (lane == 0) flag(status, AFSI_FLAG_INDEX);
             continue;
         }
         const int64_t mine = __shfl_sync(0xffffffffu, node, lane < 30 ? lane / 3 : 0);
+        __syncwarp();
         if (lane < 30) s.coef[lane] = value[mine * 3 + lane % 3];
         Box bx;
         element_box(base, g, e, bx);
-        const bool fits = box_fits<T>(bx, g);
-        if (fits)
-            for (int t = lane; t < 2 * BoxCap<T>::value; t += 32) (&s.copy[0][0])[t] = T(0);
-        for (int64_t q0 = 0; q0 < g.nq; q0 += kChunk) {
-            const int n = int(g.nq - q0 < kChunk ? g.nq - q0 : kChunk);
+        T* copy = s.copy[grp];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {  // unrolled: the box and field of c stay in registers
+            const bool fits = component_fits(bx, g, c);
+            const int ey = bx.ext[c][1], ez = bx.ext[c][2];
             __syncwarp();
-            for (int q = lane; q < n; q += 32) {  // forces, lanes over points
-                T F[3] = {T(0), T(0), T(0)};
+            if (fits)
+                for (int t = lane; t < 4 * kCompStride; t += 32) (&s.copy[0][0])[t] = T(0);
+            for (int64_t q0 = 0; q0 < g.nq; q0 += kChunk) {
+                const int n = int(g.nq - q0 < kChunk ? g.nq - q0 : kChunk);
+                __syncwarp();
+                for (int q = lane; q < n; q += 32) {  // component c of the forces, lanes over points
+                    T F = T(0);
 #pragma unroll
-                for (int a = 0; a < 10; ++a) {
-                    const T nv = N[(q0 + q) * 10 + a];
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) F[c] += nv * s.coef[a * 3 + c];
+                    for (int a = 0; a < 10; ++a) F += N[(q0 + q) * 10 + a] * s.coef[a * 3 + c];
+                    s.f[q] = (F * W[e * g.nq + q0 + q]) / volume;
                 }
-                const T wq = W[e * g.nq + q0 + q];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) s.f[c][q] = (F[c] * wq) / volume;
-            }
-            __syncwarp();
-            T* copy = s.copy[half];
-            // unrolled so that several points' table loads are in flight per warp
-#pragma unroll 4
-            for (int q = half; q < n; q += 2) {
-                const int64_t row = g.offset + e * g.nq + q0 + q;
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const int64_t rx = table_row(g.total, row, c, 0), ry = table_row(g.total, row, c, 1),
-                                  rz = table_row(g.total, row, c, 2);
-                    const int gx = int(base[rx]), gy = int(base[ry]), gz = int(base[rz]);
-                    const T w = (phi[rx * 4 + li] * phi[ry * 4 + lj]);
-                    const T fq = s.f[c][q];
-                    T v[4];
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) v[k] = (w * phi[rz * 4 + k]) * fq;
+                __syncwarp();
+#pragma unroll 2
+                for (int q = grp; q < n; q += 4) {
+                    const int64_t row = g.offset + e * g.nq + q0 + q;
+                    PointView<T> v;
+                    point_view(base, phi, g.total, row, c, li, ljp, v);
+                    const T fq = s.f[q];
+                    const T w0 = (v.wx * v.wy0), w1 = (v.wx * v.wy1);
                     if (fits) {
-                        T* dst = copy + bx.off[c] +
-                                 ((gx - bx.lo[c][0] + li) * bx.ext[c][1] + (gy - bx.lo[c][1] + lj)) * bx.ext[c][2] +
-                                 (gz - bx.lo[c][2]);
+                        T* dst = copy + ((v.gx - bx.lo[c][0] + li) * ey + (v.gy - bx.lo[c][1] + 2 * ljp)) * ez +
+                                 (v.gz - bx.lo[c][2]);
+                        T* dst1 = dst + ez;
 #pragma unroll
-                        for (int k = 0; k < 4; ++k) dst[k] += v[k];
-                    } else if (point_inside(g, c, gx, gy, gz)) {
-                        T* dst = fields[c] + face_index(g, c, gx + li, gy + lj, gz);
+                        for (int k = 0; k < 4; ++k) {
+                            dst[k] += (w0 * v.wz[k]) * fq;
+                            dst1[k] += (w1 * v.wz[k]) * fq;
+                        }
+                    } else if (point_inside(g, c, v.gx, v.gy, v.gz)) {
+                        T* dst = fields[c] + face_index(g, c, v.gx + li, v.gy + 2 * ljp, v.gz);
+                        T* dst1 = fields[c] + face_index(g, c, v.gx + li, v.gy + 2 * ljp + 1, v.gz);
 #pragma unroll
-                        for (int k = 0; k < 4; ++k) atomicAdd(dst + k, v[k]);
-                    } else if ((lane & 15) == 0) {
+                        for (int k = 0; k < 4; ++k) {
+                            atomicAdd(dst + k, (w0 * v.wz[k]) * fq);
+                            atomicAdd(dst1 + k, (w1 * v.wz[k]) * fq);
+                        }
+                    } else if ((lane & 7) == 0) {
                         flag(status, AFSI_FLAG_INDEX);
                     }
                 }
             }
-        }
-        __syncwarp();
-        if (fits) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const int ey = bx.ext[c][1], ez = bx.ext[c][2];
+            __syncwarp();
+            if (fits) {
                 const int n = bx.ext[c][0] * ey * ez;
                 for (int t = lane; t < n; t += 32) {
-                    const T v = s.copy[0][bx.off[c] + t] + s.copy[1][bx.off[c] + t];
+                    const T v = ((s.copy[0][t] + s.copy[1][t]) + s.copy[2][t]) + s.copy[3][t];
                     if (v != T(0)) {
                         const int z = t % ez, r = t / ez;
                         atomicAdd(fields[c] + face_index(g, c, bx.lo[c][0] + r / ey, bx.lo[c][1] + r % ey,
@@ -225,10 +317,13 @@ __global__ void __launch_bounds__(kWarps * 32) p2_gather_kernel(const T* __restr
                                                                 P2Dims g, int32_t* status) {
     __shared__ GatherStage<T> stage_all[kWarps];
     GatherStage<T>& s = stage_all[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31, half = lane >> 4, li = (lane >> 2) & 3, lj = lane & 3;
+    const int lane = threadIdx.x & 31, grp = lane >> 3, li = (lane >> 1) & 3, ljp = lane & 1, sub = lane & 7;
     const int64_t warps = int64_t(gridDim.x) * kWarps;
     const T* fields[3] = {u0, u1, u2};
-    for (int64_t e = int64_t(blockIdx.x) * kWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
+    int64_t e = int64_t(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+    prefetch_element(base, phi, W, g, e, lane);
+    for (; e < g.elements; e += warps) {
+        prefetch_element(base, phi, W, g, e + warps, lane);
         const int64_t node = lane < 10 ? cells[e * 10 + lane] : 0;
         if (__any_sync(0xffffffffu, lane < 10 && (node < 0 || node >= g.nodes))) {
             if (lane == 0) flag(status, AFSI_FLAG_INDEX);
@@ -251,60 +346,83 @@ __global__ void __launch_bounds__(kWarps * 32) p2_gather_kernel(const T* __restr
             }
         }
         __syncwarp();
-        // lanes 0..9 of each half accumulate node a = lane&15 over that half's points
-        T acc[3] = {T(0), T(0), T(0)};
-        const int a_node = lane & 15;
-#pragma unroll 4
-        for (int64_t qb = 0; qb < g.nq; qb += 2) {
-            const int64_t q = qb + half;
+        // lane sub of each group accumulates nodes a = sub and sub+8 over the group's points
+        T acc[2][3] = {{T(0), T(0), T(0)}, {T(0), T(0), T(0)}};
+#pragma unroll 2
+        for (int64_t qb = 0; qb < g.nq; qb += 4) {
+            const int64_t q = qb + grp;
             const bool active = q < g.nq;
             const int64_t row = g.offset + e * g.nq + (active ? q : 0);
             T U[3];
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const int64_t rx = table_row(g.total, row, c, 0), ry = table_row(g.total, row, c, 1),
-                              rz = table_row(g.total, row, c, 2);
-                const int gx = int(base[rx]), gy = int(base[ry]), gz = int(base[rz]);
-                const T w = phi[rx * 4 + li] * phi[ry * 4 + lj];
-                T sum = T(0);
+                PointView<T> v;
+                point_view(base, phi, g.total, row, c, li, ljp, v);
+                T s0 = T(0), s1 = T(0);
                 if (active) {
+                    const T* src = nullptr;
+                    int64_t sy = 0;
                     if (fits) {
-                        const T* src = s.patch + bx.off[c] +
-                                       ((gx - bx.lo[c][0] + li) * bx.ext[c][1] + (gy - bx.lo[c][1] + lj)) *
-                                           bx.ext[c][2] +
-                                       (gz - bx.lo[c][2]);
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) sum = fma(src[k], phi[rz * 4 + k], sum);
-                    } else if (point_inside(g, c, gx, gy, gz)) {
-                        const T* src = fields[c] + face_index(g, c, gx + li, gy + lj, gz);
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) sum = fma(src[k], phi[rz * 4 + k], sum);
-                    } else if ((lane & 15) == 0) {
+                        src = s.patch + bx.off[c] +
+                              ((v.gx - bx.lo[c][0] + li) * bx.ext[c][1] + (v.gy - bx.lo[c][1] + 2 * ljp)) *
+                                  bx.ext[c][2] +
+                              (v.gz - bx.lo[c][2]);
+                        sy = bx.ext[c][2];
+                    } else if (point_inside(g, c, v.gx, v.gy, v.gz)) {
+                        src = fields[c] + face_index(g, c, v.gx + li, v.gy + 2 * ljp, v.gz);
+                        sy = g.nz + (c == 2);
+                    } else if (sub == 0) {
                         flag(status, AFSI_FLAG_INDEX);
                     }
-                }
-                sum *= w;
+                    if (src) {
 #pragma unroll
-                for (int d = 8; d; d >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, d);
+                        for (int k = 0; k < 4; ++k) {
+                            s0 = fma(src[k], v.wz[k], s0);
+                            s1 = fma(src[sy + k], v.wz[k], s1);
+                        }
+                    }
+                }
+                T sum = v.wx * (v.wy0 * s0 + v.wy1 * s1);
+                sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+                sum += __shfl_xor_sync(0xffffffffu, sum, 2);
+                sum += __shfl_xor_sync(0xffffffffu, sum, 4);
                 U[c] = sum;
             }
-            if (active && a_node < 10) {
-                const T nw = N[q * 10 + a_node] * W[e * g.nq + q];
+            if (active) {
+                const T wq = W[e * g.nq + q];
 #pragma unroll
-                for (int c = 0; c < 3; ++c) acc[c] = fma(nw, U[c], acc[c]);
+                for (int m = 0; m < 2; ++m) {
+                    const int a = sub + 8 * m;
+                    if (a < 10) {
+                        const T nw = N[q * 10 + a] * wq;
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) acc[m][c] = fma(nw, U[c], acc[m][c]);
+                    }
+                }
             }
         }
-        // combine the two halves: node a sums lane a and lane a+16
+        // combine the four groups: node a sums lanes sub, sub+8, sub+16, sub+24
 #pragma unroll
-        for (int c = 0; c < 3; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 16);
-        const int64_t nd = __shfl_sync(0xffffffffu, node, a_node < 10 ? a_node : 0);
-        if (lane < 10) {
+        for (int m = 0; m < 2; ++m)
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                if (Local)
-                    out[(e * 10 + lane) * 3 + c] = acc[c];
-                else
-                    atomicAdd(out + nd * 3 + c, acc[c]);
+                T v = acc[m][c];
+                v += __shfl_xor_sync(0xffffffffu, v, 8);
+                v += __shfl_xor_sync(0xffffffffu, v, 16);
+                acc[m][c] = v;
+            }
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+            const int a = sub + 8 * m;
+            const int64_t nd = __shfl_sync(0xffffffffu, node, a < 10 ? a : 0);
+            if (grp == 0 && a < 10) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    if (Local)
+                        out[(e * 10 + a) * 3 + c] = acc[m][c];
+                    else
+                        atomicAdd(out + nd * 3 + c, acc[m][c]);
+                }
             }
         }
         __syncwarp();
