@@ -201,6 +201,99 @@ __global__ void __launch_bounds__(256) p2_prepare_kernel(const T* __restrict__ x
     }
 }
 
+// Adaptive quadrature order of each P2 element (mac/adaptive_transfer.py:173-187):
+// ceil(density * D / dx), at least min_order, where D is the diameter of the
+// element's ten Bernstein control points (the four corners and, per edge
+// (i,j) of the tetrahedron, 2 x_mid - (x_i + x_j)/2).  The diameter is the
+// square root of the largest squared pair distance ((dx^2+dy^2)+dz^2); the
+// square root is monotone, so this equals the maximum of the pair norms.
+// The launch also counts the elements whose order differs from `last`,
+// the largest order, and a histogram of orders < bins, all into `summary`
+// (changed, max, flags, hist[bins]).  Nonfinite positions set
+// AFSI_FLAG_SUPPORT, node ids outside [0, nodes) AFSI_FLAG_INDEX; those
+// elements get order 0.
+// ends of tetrahedron edge k: (0,1) (0,2) (0,3) (1,2) (1,3) (2,3)
+__host__ __device__ constexpr int edge_from(int k) { return k < 3 ? 0 : k < 5 ? 1 : 2; }
+__host__ __device__ constexpr int edge_to(int k) { return k < 3 ? k + 1 : k < 5 ? k - 1 : 3; }
+constexpr int kOrderBins = 64;
+
+template <class T>
+__global__ void __launch_bounds__(256) p2_orders_kernel(const T* __restrict__ x, const int64_t* __restrict__ cells,
+                                                        int64_t elements, int64_t nodes, T dx, T density,
+                                                        int64_t min_order, int64_t* __restrict__ orders,
+                                                        const int64_t* __restrict__ last, int32_t* summary,
+                                                        int bins) {
+    __shared__ int hist[kOrderBins];
+    for (int t = threadIdx.x; t < kOrderBins; t += blockDim.x) hist[t] = 0;
+    __syncthreads();
+    const int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    int64_t order = 0;
+    bool changed = false;
+    int32_t flags = 0;
+    if (e < elements) {
+        int64_t node[10];
+        bool ok = true;
+#pragma unroll
+        for (int a = 0; a < 10; ++a) {
+            node[a] = cells[e * 10 + a];
+            ok = ok && node[a] >= 0 && node[a] < nodes;
+        }
+        if (!ok) {
+            flags |= AFSI_FLAG_INDEX;
+        } else {
+            T hull[10][3];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) hull[a][d] = x[node[a] * 3 + d];
+#pragma unroll
+            for (int k = 0; k < 6; ++k)
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    hull[4 + k][d] = T(2) * x[node[4 + k] * 3 + d] -
+                                     T(.5) * (hull[edge_from(k)][d] + hull[edge_to(k)][d]);
+            T best = T(0);
+            bool finite = true;
+#pragma unroll
+            for (int a = 0; a < 10; ++a)
+#pragma unroll
+                for (int b = a + 1; b < 10; ++b) {
+                    const T d0 = hull[a][0] - hull[b][0], d1 = hull[a][1] - hull[b][1], d2 = hull[a][2] - hull[b][2];
+                    const T s = (d0 * d0 + d1 * d1) + d2 * d2;
+                    finite = finite && isfinite(s);
+                    best = s > best ? s : best;
+                }
+            const T v = ceil(density * sqrt(best) / dx);
+            if (!finite || !isfinite(v)) {
+                flags |= AFSI_FLAG_SUPPORT;
+            } else {
+                const T capped = v < T(1e15) ? v : T(1e15);
+                order = int64_t(capped);
+                if (order < min_order) order = min_order;
+            }
+        }
+        orders[e] = order;
+        changed = last == nullptr || last[e] != order;
+        if (order < bins) atomicAdd(&hist[order], 1);
+    }
+    const int lane = threadIdx.x & 31;
+    const unsigned moved = __ballot_sync(0xffffffffu, changed);
+    int32_t top = int32_t(order < INT32_MAX ? order : INT32_MAX);
+#pragma unroll
+    for (int d = 16; d; d >>= 1) {
+        top = max(top, __shfl_xor_sync(0xffffffffu, top, d));
+        flags |= __shfl_xor_sync(0xffffffffu, flags, d);
+    }
+    if (lane == 0) {
+        if (moved) atomicAdd(&summary[0], __popc(moved));
+        if (top > 0) atomicMax(&summary[1], top);
+        if (flags) atomicOr(&summary[2], flags);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < bins; t += blockDim.x)
+        if (hist[t]) atomicAdd(&summary[3 + t], hist[t]);
+}
+
 }  // namespace afsi
 
 using namespace afsi;
@@ -282,4 +375,24 @@ extern "C" int32_t afsi_b200_p2_prepare(const void* x, int64_t nodes, const int6
             static_cast<const T*>(x), cells, static_cast<const T*>(N), prm, base, static_cast<T*>(phi), status);
     });
     return launched("p2_prepare");
+}
+
+extern "C" int32_t afsi_b200_p2_orders(const void* x, int64_t nodes, const int64_t* cells, int64_t elements,
+                                       double dx, double density, int64_t min_order, int64_t* orders,
+                                       const int64_t* last_orders, int32_t* summary, int32_t bins, int32_t dtype,
+                                       afsi_stream_t stream) {
+    AFSI_REQUIRE(elements >= 0 && nodes >= 0, "invalid P2 element or node count");
+    AFSI_REQUIRE(bins >= 1 && bins <= kOrderBins, "order histogram needs 1..%d bins, got %d", kOrderBins, bins);
+    AFSI_REQUIRE(dx > 0 && density > 0, "P2 orders need a positive spacing and point density");
+    AFSI_REQUIRE(summary, "null summary pointer");
+    if (cudaMemsetAsync(summary, 0, sizeof(int32_t) * (3 + bins), stream) != cudaSuccess)
+        return fail(AFSI_ERR_CUDA, "summary clear failed");
+    if (elements == 0) return AFSI_OK;
+    AFSI_REQUIRE(x && cells && orders, "null device pointer");
+    AFSI_DISPATCH(dtype, {
+        p2_orders_kernel<T><<<blocks_for(elements, 256), 256, 0, stream>>>(
+            static_cast<const T*>(x), cells, elements, nodes, T(dx), T(density), min_order, orders, last_orders,
+            summary, bins);
+    });
+    return launched("p2_orders");
 }

@@ -64,7 +64,25 @@ class P2Transfer:
         return self.rules(x)
 
     def prepare(self, x, *, buffers=None):
-        rule = self.rule(x)
+        """Rule + tables for positions ``x`` with one host read when the rule
+        is unchanged: the order kernel and a prepare with the cached rule are
+        queued together, then the order summary and the prepare's status word
+        come back in one copy.  A changed rule discards the speculative tables
+        and prepares again."""
+        _lib.require_cuda(x)
+        x = x.contiguous()
+        last = self.rules.last
+        orders, summary = self.rules.launch(x)
+        speculative = None
+        if last is not None:
+            base, phi = _tables(x, last.point_count, buffers)
+            _launch_prepare(self, x, last, base, phi, summary[-1:])
+            speculative = base, phi
+        counts = summary.cpu().tolist()
+        rule = self.rules.finish(x, orders, counts)
+        if speculative is not None and rule is last:
+            _raise_flags(counts[-1])
+            return SharedAdaptiveStencil(*speculative, rule)
         base, phi = prepare(self, x, rule, buffers=buffers)
         return SharedAdaptiveStencil(base, phi, rule)
 
@@ -98,35 +116,46 @@ def _tables_ok(base, phi, total, x):
             base.is_contiguous() and phi.is_contiguous())
 
 
-def prepare(transfer, x, rule, *, buffers=None):
-    """``p2_cuda_transfer.prepare`` (``:18-39``): positions and shared tables
-    of every group; ``ValueError`` when a point's support leaves the grid."""
-    _lib.require_cuda(x)
-    x = x.contiguous()
-    total = rule.point_count
+def _tables(x, total, buffers):
     if buffers is None:
-        base = torch.empty((2, total, 3), device=x.device, dtype=torch.int64)
-        phi = x.new_empty((2, total, 3, 4))
-    else:
-        base, phi = buffers
-        if not _tables_ok(base, phi, total, x):
-            raise ValueError('invalid P2 stencil buffers')
-    word = _lib.status_word(x.device)
-    word.zero_()
+        return (torch.empty((2, total, 3), device=x.device, dtype=torch.int64), x.new_empty((2, total, 3, 4)))
+    base, phi = buffers
+    if not _tables_ok(base, phi, total, x):
+        raise ValueError('invalid P2 stencil buffers')
+    return base, phi
+
+
+def _launch_prepare(transfer, x, rule, base, phi, word):
     g = transfer.grid
     limits = [n - 2 for n in g.shape]
     offset = 0
     for group in rule.groups:
         call('afsi_b200_p2_prepare', ptr(x), x.shape[0], ptr(group.cells), group.cells.shape[0], ptr(group.values),
              group.values.shape[0], _lib.doubles(g.origin), _lib.doubles(g.spacing), _lib.doubles(limits),
-             ptr(base), ptr(phi), total, offset, ptr(word), dtype_code(x.dtype), stream(x.device))
+             ptr(base), ptr(phi), rule.point_count, offset, ptr(word), dtype_code(x.dtype), stream(x.device))
         offset += group.weights.numel()
+
+
+def _raise_flags(flags):
+    if flags & _lib.FLAG_INDEX:
+        raise RuntimeError('P2 connectivity outside the node range')
+    if flags:
+        raise ValueError('MAC IB support reaches a wall or is nonfinite; enlarge/refine the fluid box')
+
+
+def prepare(transfer, x, rule, *, buffers=None):
+    """``p2_cuda_transfer.prepare`` (``:18-39``): positions and shared tables
+    of every group; ``ValueError`` when a point's support leaves the grid."""
+    _lib.require_cuda(x)
+    x = x.contiguous()
+    base, phi = _tables(x, rule.point_count, buffers)
+    word = _lib.status_word(x.device)
+    word.zero_()
+    _launch_prepare(transfer, x, rule, base, phi, word)
     flags = int(word.item())
     if flags:
         word.zero_()
-        if flags & _lib.FLAG_INDEX:
-            raise RuntimeError('P2 connectivity outside the node range')
-        raise ValueError('MAC IB support reaches a wall or is nonfinite; enlarge/refine the fluid box')
+        _raise_flags(flags)
     return base, phi
 
 

@@ -1,8 +1,10 @@
 """Adaptive interaction quadrature for P2 tetrahedra (host-side setup).
 
 Small reference tables are built on the CPU once per order, as in the
-reference; selecting orders and grouping cells runs as tensor ops on the
-device.  Follows ``afsi_torch/mac/adaptive_transfer.py:95-301``:
+reference.  The per-element orders, the comparison with the previous rule and
+the order histogram come from one native launch (``afsi_b200_p2_orders``);
+grouping cells, when the orders changed, runs as tensor ops on the device.
+Follows ``afsi_torch/mac/adaptive_transfer.py:95-301``:
 
 * Gaussian order per cell ``max(3, ceil(density * diam / dx_min))`` where diam
   is the diameter of the quadratic Bernstein hull of the P2 element
@@ -83,17 +85,6 @@ def reference_determinants(X, cells):
     return (D[..., 0, :] * torch.linalg.cross(D[..., 1, :], D[..., 2, :])).sum(-1).abs()
 
 
-def p2_orders(x, cells, dx, density):
-    """Per-cell order from the Bernstein hull diameter (adaptive_transfer.py:173-187)."""
-    nodes = x[cells]
-    e = torch.tensor(EDGES, device=x.device)
-    controls = 2 * nodes[:, 4:] - .5 * (nodes[:, e[:, 0]] + nodes[:, e[:, 1]])
-    hull = torch.cat((nodes[:, :4], controls), 1)
-    pairs = torch.triu_indices(10, 10, 1, device=x.device)
-    diam = torch.linalg.vector_norm(hull[:, pairs[0]] - hull[:, pairs[1]], dim=-1).amax(-1)
-    return torch.ceil(density * diam / dx).clamp_min(3).to(torch.int64)
-
-
 @dataclass(frozen=True)
 class QuadratureGroup:
     cells: torch.Tensor    # (E_g,10) int64
@@ -110,16 +101,24 @@ class InteractionRule:
 
 
 class RuleBuilder:
-    """Caches reference tables per order and builds grouped rules."""
+    """Caches reference tables per order and builds grouped rules
+    (``AdaptiveFETransfer._rule``, ``mac/adaptive_transfer.py:266-301``)."""
 
     def __init__(self, X, cells, grid, *, point_density=2., max_order=8, max_points=12000000):
+        from . import _lib
+        _lib.require_cuda(X)
         self.cells = cells
         self.grid = grid
         self.density = float(point_density)
         self.max_order, self.max_points = max_order, max_points
+        self.bins = max_order + 1
         self.determinants = reference_determinants(X, cells)
         self._tables = {}
         self._last = None
+
+    @property
+    def last(self):
+        return self._last
 
     def tables(self, order, like):
         if order not in self._tables:
@@ -128,13 +127,36 @@ class RuleBuilder:
                                    torch.as_tensor(w, dtype=like.dtype, device=like.device))
         return self._tables[order]
 
-    def __call__(self, x):
-        orders = p2_orders(x, self.cells, min(self.grid.spacing), self.density)
-        if self._last is not None and torch.equal(orders, self._last.orders):
+    def launch(self, x):
+        """Queue the order kernel; nothing is read back.  Returns the orders and
+        the int32 summary ``[changed, max, flags, hist[bins], spare]``; the
+        spare slot can take the status word of a following prepare."""
+        from . import _lib
+        x = x.contiguous()
+        E = self.cells.shape[0]
+        orders = torch.empty(E, dtype=torch.int64, device=x.device)
+        summary = torch.empty(4 + self.bins, dtype=torch.int32, device=x.device)
+        summary[-1:].zero_()
+        last = None if self._last is None else self._last.orders
+        _lib.call('afsi_b200_p2_orders', _lib.ptr(x), x.shape[0], _lib.ptr(self.cells), E,
+                  float(min(self.grid.spacing)), self.density, 3, _lib.ptr(orders),
+                  None if last is None else _lib.ptr(last), _lib.ptr(summary), self.bins,
+                  _lib.dtype_code(x.dtype), _lib.stream(x.device))
+        return orders, summary
+
+    def finish(self, x, orders, counts):
+        """Rule for ``orders`` given the host copy ``counts`` of the summary."""
+        from . import _lib
+        changed, top, flags = counts[0], counts[1], counts[2]
+        if flags & _lib.FLAG_INDEX:
+            raise RuntimeError('P2 connectivity outside the node range')
+        if flags & _lib.FLAG_SUPPORT:
+            raise ValueError('MAC IB support reaches a wall or is nonfinite; enlarge/refine the fluid box')
+        if self._last is not None and changed == 0:
             return self._last
-        hist = torch.bincount(orders).cpu().tolist()
-        if len(hist) - 1 > self.max_order:
-            raise ValueError(f'adaptive IB needs Gaussian order {len(hist) - 1}, exceeds max_order={self.max_order}')
+        if top > self.max_order:
+            raise ValueError(f'adaptive IB needs Gaussian order {top}, exceeds max_order={self.max_order}')
+        hist = counts[3:3 + self.bins]
         groups, total = [], 0
         for n, count in enumerate(hist):
             if not count:
@@ -148,6 +170,10 @@ class RuleBuilder:
             raise ValueError(f'adaptive IB needs {total} points, exceeds max_points={self.max_points}')
         self._last = InteractionRule(tuple(groups), orders, total)
         return self._last
+
+    def __call__(self, x):
+        orders, summary = self.launch(x)
+        return self.finish(x, orders, summary.cpu().tolist())
 
 
 def point_count_for(orders_histogram):

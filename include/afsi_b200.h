@@ -93,6 +93,23 @@ int32_t afsi_b200_p2_prepare(const void* x, int64_t nodes, const int64_t* cells,
     int64_t* base, void* phi, int64_t total, int64_t offset, int32_t* status,
     int32_t dtype, afsi_stream_t stream);
 
+/* Adaptive quadrature order per P2 element: ceil(density * D / dx), at least
+ * min_order, D the diameter of the element's Bernstein control points
+ * (_orders_p2, mac/adaptive_transfer.py:182-187, which the reference
+ * compiles with torch.compile and follows with torch.equal against the last
+ * rule's orders, :266-273).
+ *   x (nodes,3); cells (elements,10) int64; orders (elements) int64 out;
+ *   last_orders (elements) or NULL;
+ *   summary int32[3+bins], cleared here: [0] elements whose order differs
+ *   from last_orders (all when NULL), [1] largest order, [2] device flags
+ *   (AFSI_FLAG_INDEX: node id out of range, AFSI_FLAG_SUPPORT: nonfinite
+ *   position; such elements get order 0), [3+n] elements of order n < bins.
+ *   bins in [1, 64].  The flags slot may be passed on as the status word of a
+ *   following afsi_b200_p2_prepare so that one read covers both launches. */
+int32_t afsi_b200_p2_orders(const void* x, int64_t nodes, const int64_t* cells, int64_t elements,
+    double dx, double density, int64_t min_order, int64_t* orders, const int64_t* last_orders,
+    int32_t* summary, int32_t bins, int32_t dtype, afsi_stream_t stream);
+
 /* ----------------------------------------------------------------- transfer */
 
 /* out[p,c] = sum_k field[ids[p,k],c]*w[p,k]   (indexed_gather) */

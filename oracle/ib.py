@@ -292,3 +292,30 @@ def p2_gather_assemble(fields, groups, base, phi, shape, nodes):
         rhs += p2_assemble(U[off:off + n], c, N, W, nodes)
         off += n
     return rhs
+
+
+TET_EDGES = np.array([[0, 1], [0, 2], [0, 3], [1, 2], [1, 3], [2, 3]])
+
+
+def p2_orders(x, cells, dx, density, min_order=3):
+    """Adaptive quadrature order of each P2 element, ``_orders_p2`` in
+    ``mac/adaptive_transfer.py:173-187``: the Bernstein control points are the
+    four corners and ``2 x_mid - (x_i + x_j)/2`` per edge; the order is
+    ``ceil(density * diameter / dx)`` clamped below at 3."""
+    nodes = np.asarray(x)[np.asarray(cells)]
+    controls = 2 * nodes[:, 4:] - .5 * (nodes[:, TET_EDGES[:, 0]] + nodes[:, TET_EDGES[:, 1]])
+    hull = np.concatenate((nodes[:, :4], controls), 1)
+    a, b = np.triu_indices(10, 1)
+    d = hull[:, a] - hull[:, b]
+    squared = (d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1]) + d[..., 2] * d[..., 2]
+    diameter = np.sqrt(squared.max(-1))
+    return np.maximum(np.ceil(density * diameter / dx), min_order).astype(np.int64)
+
+
+def p1_orders(x, cells, dx, density, min_order=2):
+    """P1 element order, ``_orders`` in ``mac/adaptive_transfer.py:167-170``:
+    ``ceil(density * longest_edge / dx)`` clamped below at 2."""
+    nodes = np.asarray(x)[np.asarray(cells)]
+    d = nodes[:, TET_EDGES[:, 0]] - nodes[:, TET_EDGES[:, 1]]
+    squared = (d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1]) + d[..., 2] * d[..., 2]
+    return np.maximum(np.ceil(density * np.sqrt(squared.max(-1)) / dx), min_order).astype(np.int64)

@@ -27,7 +27,7 @@ from afsi_torch.mac2d.transfer import TriangleTransfer  # noqa: E402
 from afsi_torch.mac2d.multigrid import ChannelMultigrid  # noqa: E402
 from afsi_torch.mac2d.mg_workspace import TensorKernels as ChannelKernels  # noqa: E402
 from afsi_torch.mac.adaptive_transfer import (AdaptiveFETransfer, InteractionQuadratureOptions,  # noqa: E402
-                                              gaussian_tetra_rule)
+                                              gaussian_tetra_rule, _orders, _orders_p2)
 from afsi_torch.tetrahedron import reference_nodes, tabulate, promote_p1  # noqa: E402
 from afsi_torch.solid import prepare_p2  # noqa: E402
 
@@ -204,6 +204,19 @@ def mg2d():
          shape_b=big.shape, lengths_b=big.lengths, rhs_b=rb, solution_b=pb, cycles_b=infob['cycles'])
 
 
+def orders():
+    """Adaptive element orders (_orders_p2 / _orders) on seeded node clouds."""
+    g = torch.Generator().manual_seed(6)
+    x = torch.rand((300, 3), generator=g) * .3 + .2
+    cells = torch.randint(0, 300, (500, 10), generator=g)
+    edges = torch.tensor([[0, 1], [0, 2], [0, 3], [1, 2], [1, 3], [2, 3]])
+    arrays = dict(x=x, cells=cells, dx=np.array([.011, .037]), density=np.array([2., 3.5]))
+    for k, (dx, density) in enumerate(zip(arrays['dx'], arrays['density'])):
+        arrays[f'p2_{k}'] = _orders_p2(x, cells, edges, float(dx), float(density))
+        arrays[f'p1_{k}'] = _orders(x, cells[:, :4], edges, float(dx), float(density))
+    save('orders', **arrays)
+
+
 def quadrature():
     arrays = {}
     like = torch.zeros(1)
@@ -222,3 +235,4 @@ if __name__ == '__main__':
     mg3d()
     mg2d()
     quadrature()
+    orders()

@@ -10,7 +10,7 @@ import pytest
 import torch
 from conftest import golden
 from oracle import ib as oracle
-from afsi_gpu_b200 import cuda_ib, p2_cuda_transfer as p2t, synthetic
+from afsi_gpu_b200 import _lib, cuda_ib, p2_cuda_transfer as p2t, synthetic
 from afsi_gpu_b200.grid import MACGrid, ChannelGrid
 from afsi_gpu_b200.quadrature import InteractionRule, QuadratureGroup
 
@@ -276,3 +276,75 @@ def test_p2_support_violation_raises_value_error():
     tr = p2t.P2Transfer(grid, t(X), t(cells), max_order=22)
     with pytest.raises(ValueError, match='support'):
         tr.prepare(t(X) - .45)
+
+
+# ------------------------------------------------------------ adaptive orders
+
+def _orders(x, cells, dx, density, last=None, bins=64):
+    orders = torch.empty(cells.shape[0], dtype=torch.int64, device=DEV)
+    summary = torch.full((3 + bins,), -7, dtype=torch.int32, device=DEV)
+    _lib.call('afsi_b200_p2_orders', x.data_ptr(), x.shape[0], cells.data_ptr(), cells.shape[0], dx, density, 3,
+              orders.data_ptr(), None if last is None else last.data_ptr(), summary.data_ptr(), bins,
+              _lib.dtype_code(x.dtype), _lib.stream(x.device))
+    return orders, summary.cpu().tolist()
+
+
+def test_p2_orders_match_reference_fixture_and_count_changes():
+    g = golden('orders')
+    x, cells = t(g['x']), t(g['cells'])
+    for k, (dx, density) in enumerate(zip(g['dx'], g['density'])):
+        expected = g[f'p2_{k}']
+        np.testing.assert_array_equal(oracle.p2_orders(g['x'], g['cells'], dx, density), expected)
+        orders, summary = _orders(x, cells, float(dx), float(density))
+        np.testing.assert_array_equal(orders.cpu().numpy(), expected)
+        assert summary[0] == len(expected) and summary[1] == expected.max() and summary[2] == 0
+        hist = np.bincount(expected, minlength=64)[:64]
+        assert summary[3:] == hist.tolist()
+        again, summary = _orders(x, cells, float(dx), float(density), last=orders)
+        assert torch.equal(again, orders) and summary[0] == 0
+        moved = orders.clone()
+        moved[[3, 17, 400]] += 1
+        _, summary = _orders(x, cells, float(dx), float(density), last=moved)
+        assert summary[0] == 3
+    # orders at or above the bin count are left out of the histogram, not the maximum
+    orders, summary = _orders(x, cells, .011, 2., bins=8)
+    top = int(g['p2_0'].max())
+    assert summary[1] == top and sum(summary[3:]) == int((g['p2_0'] < 8).sum())
+
+
+def test_p2_orders_flag_bad_connectivity_and_nonfinite_nodes():
+    g = golden('orders')
+    x, cells = t(g['x']), t(g['cells'])
+    bad = cells.clone()
+    bad[5, 7] = x.shape[0]
+    orders, summary = _orders(x, bad, .011, 2.)
+    assert summary[2] == _lib.FLAG_INDEX and orders[5].item() == 0
+    assert orders[6].item() == int(g['p2_0'][6])
+    xn = x.clone()
+    xn[int(g['cells'][9, 0]), 1] = float('nan')
+    orders, summary = _orders(xn, cells, .011, 2.)
+    assert summary[2] == _lib.FLAG_SUPPORT and orders[9].item() == 0
+
+
+def test_p2_transfer_prepare_reuses_the_rule_and_rebuilds_on_change():
+    X, cells = synthetic.p2_shell(2, 12, 16, **SMALL)
+    grid = MACGrid((32, 32, 32), (1., 1., 1.))
+    tr = p2t.P2Transfer(grid, t(X), t(cells), max_order=22)
+    first = tr.prepare(t(X))
+    second = tr.prepare(t(X))  # speculative prepare with the cached rule
+    assert second.rule is first.rule
+    assert torch.equal(first.base, second.base) and torch.equal(first.phi, second.phi)
+    centre = X.mean(0)
+    Y = centre + 1.3 * (X - centre)  # larger elements: higher orders
+    third = tr.prepare(t(Y))
+    assert third.rule is not first.rule
+    orders = oracle.p2_orders(Y, cells, min(grid.spacing), 2.)
+    np.testing.assert_array_equal(third.rule.orders.cpu().numpy(), orders)
+    assert third.rule.point_count == sum(len(gr.weights[0]) * gr.cells.shape[0] for gr in third.rule.groups)
+    groups = [(gr.cells.cpu().numpy(), gr.values.cpu().numpy()) for gr in third.rule.groups]
+    ob, op, invalid = oracle.p2_prepare(Y, groups, grid.origin, grid.spacing, grid.shape)
+    assert invalid == 0
+    assert np.array_equal(third.base.cpu().numpy(), ob) and np.array_equal(third.phi.cpu().numpy(), op)
+    # a translation keeps the orders: the speculative prepare reports the wall
+    with pytest.raises(ValueError, match='support'):
+        tr.prepare(t(Y) - .45)

@@ -152,3 +152,10 @@ def test_periodic_restatement_converges_and_is_periodic():
     np.testing.assert_allclose(shifted, np.roll(p, 8, 0), rtol=1e-8, atol=1e-9)
     with pytest.raises(ValueError, match='incompatible'):
         mg.solve(h, np.ones(shape))
+
+
+def test_element_orders_match_reference():
+    g = golden('orders')
+    for k, (dx, density) in enumerate(zip(g['dx'], g['density'])):
+        np.testing.assert_array_equal(ib.p2_orders(g['x'], g['cells'], dx, density), g[f'p2_{k}'])
+        np.testing.assert_array_equal(ib.p1_orders(g['x'], g['cells'][:, :4], dx, density), g[f'p1_{k}'])
