@@ -1,31 +1,31 @@
 // P2 element transfers (spread, gather-assemble) for the B200.
 //
-// One warp owns one P2 element at a time (grid-stride over elements) and
-// works on four quadrature points at once: lane group g = lane>>3 takes one
-// point, and its eight lanes own (x offset i, y offsets 2jp..2jp+1) of the
-// point's 4x4x4 support with all four z links — eight links per lane and
-// component.
+// One warp owns one P2 element at a time (grid-stride over elements).
 //
 // Spread: for each velocity component in turn, the element's contributions
 // are accumulated into a shared-memory box covering the supports of that
-// component.  Each lane group has a private copy of the box, so the adds are
-// plain read-modify-writes in a fixed order (points g, g+4, g+8, ... in group
-// g): no atomics.  The four copies are summed and flushed to the face array
-// with one L2 reduction per non-zero face — about 130 per element and
-// component instead of 64 per point.
+// component.  The warp works on two quadrature points at once: each half-warp
+// takes one point and its 16 lanes own the (i,j) columns of the point's 4x4x4
+// support, with the four z links of a column handled by that lane.  Each
+// half-warp has a private copy of the box, so the adds are plain
+// read-modify-writes in a fixed order (points h, h+2, h+4, ... in half h): no
+// atomics.  The box strides are padded (y stride odd, x stride = 4 mod 8) so
+// that the 16 lanes of a half-warp always address 16 different 8-byte bank
+// pairs: the read-modify-writes are free of bank conflicts wherever the point
+// lies.  The two copies are summed and flushed to the face array with one L2
+// reduction per non-zero face — about 130 per element and component instead
+// of 64 per point.
 // Gather: the face values of the element's boxes are staged in shared memory
-// once per element; each point reads its 64 links per component from there
-// and the eight lanes of a group reduce with three shuffles.  The nodal sums
-// Σ_q N[q,a] W U(x_q) are accumulated in registers and added to the
+// once per element; four points are in flight per warp, lane group g =
+// lane>>3 taking one, its eight lanes owning (x offset i, y offsets
+// 2jp..2jp+1) with all four z links, reduced with three shuffles.  The nodal
+// sums Σ_q N[q,a] W U(x_q) are accumulated in registers and added to the
 // right-hand side (or written per element for the deterministic node
 // reduction).
-// While a warp works on one element it asks L2 for the stencil rows of the
-// next element it will take (cp.async.bulk.prefetch.L2), so the table stream
-// from HBM does not wait on the warp's own loads.
 // Point forces F = (Σ_a N[q,a] value[a]) * W (mac/compact_transfer.py:29-35)
-// are computed once per point by a lanes-over-points pass; the spread
-// contribution is (φx·φy)·φz · (F/volume), one division per point instead of
-// per link as in the reference kernel (one rounding of difference).
+// are computed once per point and component by a lanes-over-points pass; the
+// spread contribution is (φx·φy)·φz · (F/volume), one division per point
+// instead of per link as in the reference kernel (one rounding of difference).
 // An element whose box does not fit the shared-memory copies is processed
 // with direct L2 reductions / global loads, checking each point's support
 // against the grid (a point outside sets AFSI_FLAG_INDEX and is skipped).
@@ -38,8 +38,9 @@ namespace afsi {
 constexpr int kWarps = 4;       // warps per block
 constexpr int kChunk = 64;      // points whose forces are held at once
 template <class T> struct BoxCap { static constexpr int value = 4608 / sizeof(T); };  // gather patch (576 doubles)
-constexpr int kCompCap = 224;     // spread: entries of one component's box per copy
-constexpr int kCompStride = 232;  // copy stride; the 8-entry pad puts the copies on different banks
+constexpr int kSpreadCap = 288;   // spread: entries of one component's padded box per copy
+constexpr int kSpreadBlocks = 6;  // resident blocks per SM the spread is compiled for
+constexpr int kGatherBlocks = 6;  // same for the gather
 
 template <class T>
 struct GatherStage {
@@ -123,31 +124,19 @@ __device__ __forceinline__ bool box_fits(const Box& bx, const P2Dims& g) {
     return inside && cells <= BoxCap<T>::value;
 }
 
-// Component c's box lies in its face array and fits one spread copy.
-__device__ __forceinline__ bool component_fits(const Box& bx, const P2Dims& g, int c) {
-    return component_inside(bx, g, c) && component_cells(bx, c) <= kCompCap;
-}
-
-// Ask L2 for [p, p+bytes) rounded inward to 16-byte boundaries.
-__device__ __forceinline__ void prefetch_l2(const void* p, int64_t bytes) {
-    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
-    const uintptr_t lo = (a + 15) & ~uintptr_t(15), hi = (a + uintptr_t(bytes)) & ~uintptr_t(15);
-    if (hi > lo && hi - lo < (uintptr_t(1) << 31))
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"(uint32_t(hi - lo)) : "memory");
-}
-
-// Lanes 0..4 of a warp prefetch the stencil rows and weights of element e.
-template <class T>
-__device__ __forceinline__ void prefetch_element(const int64_t* base, const T* phi, const T* W, const P2Dims& g,
-                                                 int64_t e, int lane) {
-    if (e >= g.elements || lane >= 5) return;
-    const int64_t row = g.offset + e * g.nq;
-    if (lane < 2)
-        prefetch_l2(base + (lane * g.total + row) * 3, g.nq * 3 * int64_t(sizeof(int64_t)));
-    else if (lane < 4)
-        prefetch_l2(phi + ((lane - 2) * g.total + row) * 12, g.nq * 12 * int64_t(sizeof(T)));
-    else
-        prefetch_l2(W + e * g.nq, g.nq * int64_t(sizeof(T)));
+// Padded strides of component c's box in a spread copy: sy = ez|1 (odd) and
+// sx = 4 (mod 8), sx >= ey*sy.  Entry (x,y,z) sits at x*sx + y*sy + z, and the
+// offsets li*sx + lj*sy (li, lj in 0..3) are 16 distinct values mod 16: the
+// 16 lanes of a half-warp meet 16 different 8-byte bank pairs.  False when the
+// box leaves the face array or does not fit kSpreadCap entries.
+__device__ __forceinline__ bool spread_layout(const Box& bx, const P2Dims& g, int c, int& sx, int& sy) {
+    const int ey = bx.ext[c][1], ez = bx.ext[c][2];
+    sy = sx = 0;
+    if (!component_inside(bx, g, c) || ey > 64 || ez > 64) return false;
+    sy = ez | 1;
+    sx = ey * sy;
+    sx += (12 - (sx & 7)) & 7;
+    return int64_t(bx.ext[c][0]) * sx <= kSpreadCap;
 }
 
 __device__ __forceinline__ int64_t face_index(const P2Dims& g, int c, int x, int y, int z) {
@@ -162,7 +151,7 @@ __device__ __forceinline__ bool point_inside(const P2Dims& g, int c, int x, int 
 
 // ------------------------------------------------------------------ lanes
 //
-// Lane layout: group g = lane>>3 takes one of four points in flight; within a
+// Gather lane layout: group g = lane>>3 takes one of four points in flight; within a
 // group, lane bits (i = (lane>>1)&3, jp = lane&1) own the x offset i and the
 // y offsets 2jp, 2jp+1 of the point's support, and all four z offsets: eight
 // links per component.  The z row of four weights is one 32-byte pair of
@@ -211,26 +200,19 @@ template <class T>
 struct SpreadStage {
     T f[kChunk];
     T coef[32];
-    T copy[4][kCompStride];
+    T copy[2][kSpreadCap];
 };
 
 template <class T>
-__global__ void __launch_bounds__(kWarps * 32) p2_spread_kernel(const T* __restrict__ value,
-                                                                const int64_t* __restrict__ cells,
-                                                                const T* __restrict__ N, const T* __restrict__ W,
-                                                                const int64_t* __restrict__ base,
-                                                                const T* __restrict__ phi, T* __restrict__ u0,
-                                                                T* __restrict__ u1, T* __restrict__ u2, P2Dims g,
-                                                                T volume, int32_t* status) {
+__global__ void __launch_bounds__(kWarps * 32, kSpreadBlocks) p2_spread_kernel(
+    const T* __restrict__ value, const int64_t* __restrict__ cells, const T* __restrict__ N, const T* __restrict__ W,
+    const int64_t* __restrict__ base, const T* __restrict__ phi, T* __restrict__ u0, T* __restrict__ u1,
+    T* __restrict__ u2, P2Dims g, T volume, int32_t* status) {
     __shared__ SpreadStage<T> stage_all[kWarps];
     SpreadStage<T>& s = stage_all[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31, grp = lane >> 3, li = (lane >> 1) & 3, ljp = lane & 1;
+    const int lane = threadIdx.x & 31, half = lane >> 4, li = (lane >> 2) & 3, lj = lane & 3;
     const int64_t warps = int64_t(gridDim.x) * kWarps;
-    T* fields[3] = {u0, u1, u2};
-    int64_t e = int64_t(blockIdx.x) * kWarps + (threadIdx.x >> 5);
-    prefetch_element(base, phi, W, g, e, lane);
-    for (; e < g.elements; e += warps) {
-        prefetch_element(base, phi, W, g, e + warps, lane);
+    for (int64_t e = int64_t(blockIdx.x) * kWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
         const int64_t node = lane < 10 ? cells[e * 10 + lane] : 0;
         if (__any_sync(0xffffffffu, lane < 10 && (node < 0 || node >= g.nodes))) {
             if (lane == 0) flag(status, AFSI_FLAG_INDEX);
@@ -241,14 +223,15 @@ __global__ void __launch_bounds__(kWarps * 32) p2_spread_kernel(const T* __restr
         if (lane < 30) s.coef[lane] = value[mine * 3 + lane % 3];
         Box bx;
         element_box(base, g, e, bx);
-        T* copy = s.copy[grp];
+        T* copy = s.copy[half];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {  // unrolled: the box and field of c stay in registers
-            const bool fits = component_fits(bx, g, c);
-            const int ey = bx.ext[c][1], ez = bx.ext[c][2];
+            T* field = c == 0 ? u0 : c == 1 ? u1 : u2;
+            int sx, sy;
+            const bool fits = spread_layout(bx, g, c, sx, sy);
             __syncwarp();
             if (fits)
-                for (int t = lane; t < 4 * kCompStride; t += 32) (&s.copy[0][0])[t] = T(0);
+                for (int t = lane; t < 2 * kSpreadCap; t += 32) (&s.copy[0][0])[t] = T(0);
             for (int64_t q0 = 0; q0 < g.nq; q0 += kChunk) {
                 const int n = int(g.nq - q0 < kChunk ? g.nq - q0 : kChunk);
                 __syncwarp();
@@ -260,44 +243,39 @@ __global__ void __launch_bounds__(kWarps * 32) p2_spread_kernel(const T* __restr
                 }
                 __syncwarp();
 #pragma unroll 2
-                for (int q = grp; q < n; q += 4) {
+                for (int q = half; q < n; q += 2) {
                     const int64_t row = g.offset + e * g.nq + q0 + q;
-                    PointView<T> v;
-                    point_view(base, phi, g.total, row, c, li, ljp, v);
+                    const int64_t rx = table_row(g.total, row, c, 0), ry = table_row(g.total, row, c, 1),
+                                  rz = table_row(g.total, row, c, 2);
+                    const int gx = int(base[rx]), gy = int(base[ry]), gz = int(base[rz]);
+                    const T w = phi[rx * 4 + li] * phi[ry * 4 + lj];
+                    T wz[4];
+                    load_row4(phi + rz * 4, wz);
                     const T fq = s.f[q];
-                    const T w0 = (v.wx * v.wy0), w1 = (v.wx * v.wy1);
                     if (fits) {
-                        T* dst = copy + ((v.gx - bx.lo[c][0] + li) * ey + (v.gy - bx.lo[c][1] + 2 * ljp)) * ez +
-                                 (v.gz - bx.lo[c][2]);
-                        T* dst1 = dst + ez;
+                        T* dst = copy + (gx - bx.lo[c][0] + li) * sx + (gy - bx.lo[c][1] + lj) * sy +
+                                 (gz - bx.lo[c][2]);
 #pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            dst[k] += (w0 * v.wz[k]) * fq;
-                            dst1[k] += (w1 * v.wz[k]) * fq;
-                        }
-                    } else if (point_inside(g, c, v.gx, v.gy, v.gz)) {
-                        T* dst = fields[c] + face_index(g, c, v.gx + li, v.gy + 2 * ljp, v.gz);
-                        T* dst1 = fields[c] + face_index(g, c, v.gx + li, v.gy + 2 * ljp + 1, v.gz);
+                        for (int k = 0; k < 4; ++k) dst[k] += (w * wz[k]) * fq;
+                    } else if (point_inside(g, c, gx, gy, gz)) {
+                        T* dst = field + face_index(g, c, gx + li, gy + lj, gz);
 #pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            atomicAdd(dst + k, (w0 * v.wz[k]) * fq);
-                            atomicAdd(dst1 + k, (w1 * v.wz[k]) * fq);
-                        }
-                    } else if ((lane & 7) == 0) {
+                        for (int k = 0; k < 4; ++k) atomicAdd(dst + k, (w * wz[k]) * fq);
+                    } else if ((lane & 15) == 0) {
                         flag(status, AFSI_FLAG_INDEX);
                     }
                 }
             }
             __syncwarp();
             if (fits) {
+                const int ey = bx.ext[c][1], ez = bx.ext[c][2];
                 const int n = bx.ext[c][0] * ey * ez;
                 for (int t = lane; t < n; t += 32) {
-                    const T v = ((s.copy[0][t] + s.copy[1][t]) + s.copy[2][t]) + s.copy[3][t];
-                    if (v != T(0)) {
-                        const int z = t % ez, r = t / ez;
-                        atomicAdd(fields[c] + face_index(g, c, bx.lo[c][0] + r / ey, bx.lo[c][1] + r % ey,
-                                                         bx.lo[c][2] + z), v);
-                    }
+                    const int z = t % ez, r = t / ez, y = r % ey, x = r / ey;
+                    const int o = x * sx + y * sy + z;
+                    const T v = s.copy[0][o] + s.copy[1][o];
+                    if (v != T(0))
+                        atomicAdd(field + face_index(g, c, bx.lo[c][0] + x, bx.lo[c][1] + y, bx.lo[c][2] + z), v);
                 }
             }
         }
@@ -308,7 +286,7 @@ __global__ void __launch_bounds__(kWarps * 32) p2_spread_kernel(const T* __restr
 // ------------------------------------------------------------------ gather
 
 template <class T, bool Local>
-__global__ void __launch_bounds__(kWarps * 32) p2_gather_kernel(const T* __restrict__ u0, const T* __restrict__ u1,
+__global__ void __launch_bounds__(kWarps * 32, kGatherBlocks) p2_gather_kernel(const T* __restrict__ u0, const T* __restrict__ u1,
                                                                 const T* __restrict__ u2,
                                                                 const int64_t* __restrict__ cells,
                                                                 const T* __restrict__ N, const T* __restrict__ W,
@@ -320,10 +298,7 @@ __global__ void __launch_bounds__(kWarps * 32) p2_gather_kernel(const T* __restr
     const int lane = threadIdx.x & 31, grp = lane >> 3, li = (lane >> 1) & 3, ljp = lane & 1, sub = lane & 7;
     const int64_t warps = int64_t(gridDim.x) * kWarps;
     const T* fields[3] = {u0, u1, u2};
-    int64_t e = int64_t(blockIdx.x) * kWarps + (threadIdx.x >> 5);
-    prefetch_element(base, phi, W, g, e, lane);
-    for (; e < g.elements; e += warps) {
-        prefetch_element(base, phi, W, g, e + warps, lane);
+    for (int64_t e = int64_t(blockIdx.x) * kWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
         const int64_t node = lane < 10 ? cells[e * 10 + lane] : 0;
         if (__any_sync(0xffffffffu, lane < 10 && (node < 0 || node >= g.nodes))) {
             if (lane == 0) flag(status, AFSI_FLAG_INDEX);
