@@ -50,6 +50,10 @@ _SIGNATURES = {
                              c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int32, c_void_p],
     'afsi_b200_p2_orders': [c_void_p, c_int64, c_void_p, c_int64, ctypes.c_double, ctypes.c_double, c_int64,
                             c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p],
+    'afsi_b200_mg_solve_graph_create': [ctypes.POINTER(MGPlan), c_int32, c_int32, c_void_p, c_void_p,
+                                        ctypes.POINTER(c_void_p)],
+    'afsi_b200_mg_solve_graph_launch': [c_void_p, c_void_p],
+    'afsi_b200_mg_solve_graph_destroy': [c_void_p],
     'afsi_b200_indexed_gather': [c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_int64, c_int64, c_void_p,
                                  c_void_p, c_int32, c_void_p],
     'afsi_b200_indexed_spread': [c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_int64, c_int64, c_double,
@@ -181,3 +185,8 @@ def launch_count():
 
 def count_replay(launches):
     _replayed[0] += int(launches)
+
+
+def forget_launches(launches):
+    """Take back launches that were only captured into a graph, not run."""
+    _replayed[0] -= int(launches)

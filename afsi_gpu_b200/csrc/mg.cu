@@ -512,6 +512,115 @@ extern "C" int32_t afsi_b200_mg_residual_norm(const afsi_mg_plan* plan, double* 
     return launched("mg residual_norm");
 }
 
+// ------------------------------------------------------------ solve graph
+//
+// The solve loop of mac/multigrid.py:88-97 (check_every V-cycles, residual
+// norm, stop at tol or max_cycles) as one CUDA graph: a WHILE conditional
+// node whose body holds check_every V-cycles, the residual norm and a decide
+// kernel that updates the loop state and sets the condition.  One graph
+// launch replaces check_every-sized host round trips.  The body stops before
+// a block of check_every cycles would pass max_cycles; the caller runs any
+// tail on the host path.
+//
+// loop (device double[4]): [0] tol (written by the caller before each
+// launch), [1] cycles run, [2] last residual norm, [3] 1 when the norm was
+// nonfinite.
+
+namespace {
+
+__global__ void mg_decide_kernel(double* loop, const double* norm, int check_every, int max_cycles,
+                                 cudaGraphConditionalHandle handle) {
+    const double cycles = loop[1] + check_every;
+    const double r = *norm;
+    loop[1] = cycles;
+    loop[2] = r;
+    const bool finite = isfinite(r);
+    if (!finite) loop[3] = 1.0;
+    const bool again = finite && r > loop[0] && cycles + check_every <= max_cycles;
+    cudaGraphSetConditional(handle, again ? 1u : 0u);
+}
+
+struct SolveGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t capture = nullptr;
+};
+
+void release(SolveGraph* sg) {
+    if (!sg) return;
+    if (sg->exec) cudaGraphExecDestroy(sg->exec);
+    if (sg->graph) cudaGraphDestroy(sg->graph);
+    if (sg->capture) cudaStreamDestroy(sg->capture);
+    delete sg;
+}
+
+}  // namespace
+
+extern "C" int32_t afsi_b200_mg_solve_graph_create(const afsi_mg_plan* plan, int32_t check_every,
+                                                   int32_t max_cycles, double* loop, double* norm,
+                                                   void** graph_out) {
+    int32_t rc = validate_plan(plan);
+    if (rc) return rc;
+    AFSI_REQUIRE(graph_out && loop && norm, "null solve-graph argument");
+    AFSI_REQUIRE(check_every >= 1 && max_cycles >= check_every, "solve graph needs 1 <= check_every <= max_cycles");
+    AFSI_REQUIRE(plan->coarse_dtype == AFSI_F64 || plan->coarse_dtype == plan->dtype, "unsupported coarse dtype");
+    *graph_out = nullptr;
+    SolveGraph* sg = new SolveGraph;
+    cudaGraphConditionalHandle handle;
+    cudaGraphNodeParams np = {};
+    cudaGraphNode_t node;
+    if (cudaStreamCreateWithFlags(&sg->capture, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaGraphCreate(&sg->graph, 0) != cudaSuccess ||
+        cudaGraphConditionalHandleCreate(&handle, sg->graph, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+        release(sg);
+        return fail(AFSI_ERR_CUDA, "solve graph setup failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = handle;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    if (cudaGraphAddNode(&node, sg->graph, nullptr, 0, &np) != cudaSuccess) {
+        release(sg);
+        return fail(AFSI_ERR_CUDA, "solve graph conditional node failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(sg->capture, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+        cudaSuccess) {
+        release(sg);
+        return fail(AFSI_ERR_CUDA, "solve graph capture failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    rc = afsi_b200_mg_vcycles(plan, check_every, sg->capture);
+    if (!rc) rc = afsi_b200_mg_residual_norm(plan, norm, sg->capture);
+    if (!rc) {
+        mg_decide_kernel<<<1, 1, 0, sg->capture>>>(loop, norm, check_every, max_cycles, handle);
+        rc = launched("mg solve decide");
+    }
+    cudaGraph_t captured = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(sg->capture, &captured);
+    if (rc) {
+        release(sg);
+        return rc;
+    }
+    if (end != cudaSuccess || cudaGraphInstantiate(&sg->exec, sg->graph, 0) != cudaSuccess) {
+        release(sg);
+        return fail(AFSI_ERR_CUDA, "solve graph instantiation failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    *graph_out = sg;
+    return AFSI_OK;
+}
+
+extern "C" int32_t afsi_b200_mg_solve_graph_launch(void* graph, afsi_stream_t stream) {
+    AFSI_REQUIRE(graph, "null solve graph");
+    if (cudaGraphLaunch(static_cast<SolveGraph*>(graph)->exec, stream) != cudaSuccess)
+        return fail(AFSI_ERR_CUDA, "solve graph launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return AFSI_OK;
+}
+
+extern "C" int32_t afsi_b200_mg_solve_graph_destroy(void* graph) {
+    release(static_cast<SolveGraph*>(graph));
+    return AFSI_OK;
+}
+
 extern "C" int32_t afsi_b200_vector_stats(const void* x, int64_t n, double* stats_out, void* scratch, int32_t dtype,
                                           afsi_stream_t stream) {
     AFSI_REQUIRE(n > 0 && x && stats_out && scratch, "invalid stats arguments");

@@ -170,7 +170,7 @@ __device__ __forceinline__ void site_finish(const Site& s, double v, double* sqr
 template <int BC, bool Exact, class T>
 __device__ __forceinline__ T restrict_residual_at(const T* __restrict__ p, const T* __restrict__ rhs, int cx, int cy,
                                                   int cz, const Lv<T>& L, T m) {
-    if (BC == AFSI_BC_NEUMANN) {
+    if constexpr (BC == AFSI_BC_NEUMANN) {
         T v = T(0);
 #pragma unroll
         for (int a = 0; a < 2; ++a)
@@ -184,18 +184,19 @@ __device__ __forceinline__ T restrict_residual_at(const T* __restrict__ p, const
                     v = v + (rhs[i] - neg_lap<BC, Exact>(p, i, x, y, z, L, m, pc));
                 }
         return v * T(.125);
+    } else {
+        T r[4];
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                const int x = 2 * cx + a, y = 2 * cy + b;
+                const int64_t i = int64_t(x) * L.ny + y;
+                const T pc = p[i] - m;
+                r[a * 2 + b] = rhs[i] - neg_lap<BC, Exact>(p, i, x, y, 0, L, m, pc);
+            }
+        return ((r[0] + r[1]) + r[2] + r[3]) * T(.25);
     }
-    T r[4];
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b) {
-            const int x = 2 * cx + a, y = 2 * cy + b;
-            const int64_t i = int64_t(x) * L.ny + y;
-            const T pc = p[i] - m;
-            r[a * 2 + b] = rhs[i] - neg_lap<BC, Exact>(p, i, x, y, 0, L, m, pc);
-        }
-    return ((r[0] + r[1]) + r[2] + r[3]) * T(.25);
 }
 
 // Coarse value with the boundary ghosts of each BC (coarse lattice C).
@@ -237,13 +238,25 @@ __device__ __forceinline__ T prolong_at(const T* __restrict__ c, int x, int y, i
 // ----------------------------------------------------------- coarse block
 //
 // All levels from `first` down run inside one thread block in shared memory.
-// The block works with fast arithmetic and, to keep the single SM busy,
-// without integer or floating-point division in the inner loops:
+// The block works with fast arithmetic and keeps the single SM's instruction
+// count low:
 //  * cell coordinates come from shifts when a level's extents are powers of
 //    two (division otherwise);
-//  * the Jacobi update multiplies by a reciprocal diagonal looked up in a
-//    per-level table of the 64 boundary classes (first/last cell per axis),
-//    built once per launch;
+//  * the stencil is branch-free: a missing Neumann neighbour reads as the
+//    cell itself (zero flux), the channel outlet ghost as its negative, the
+//    periodic neighbour through the wrapped index; the axis terms are
+//    combined with fused multiply-adds;
+//  * the Jacobi update multiplies by omega/diag looked up in a per-level
+//    table of the 64 boundary classes (first/last cell per axis), built once
+//    per launch;
+//  * the mean-zero gauge of the singular operators is carried as pending
+//    shifts: the mean of a level's iterate is summed inside its last sweep
+//    (one barrier per reduction, every thread adds the 32 warp partials in the
+//    same order) and subtracted where the iterate is next read — in the
+//    prolongation, the next level's first sweep or the final copy — instead of
+//    in passes of their own.  A(p - m·1) = A p for these operators, so the
+//    restriction reads the unshifted iterate;
+//  * a zero initial iterate is folded into the first sweep;
 //  * the dense coarsest solve is warp-cooperative (lanes over a row).
 
 template <class T>
@@ -252,15 +265,19 @@ struct CoarseLevels {
     int first, last;  // level indices handled here
 };
 
-template <class T>
-__device__ T block_mean(const T* a, int n, double* red) {
-    double v = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) v += double(a[i]);
-    v = block_sum(v, red);
-    __shared__ double bcast;
-    if (threadIdx.x == 0) bcast = v / double(n);
+// Sum of v over the block, returned to every thread: one barrier.  Warp
+// partials go to red (32 slots); every thread adds them in slot order.  The
+// caller alternates between two red buffers so that a slot is rewritten only
+// after a later barrier.
+__device__ __forceinline__ double block_sum_all(double v, double* red) {
+#pragma unroll
+    for (int d = 16; d; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
     __syncthreads();
-    return T(bcast);
+    double t = 0.0;
+    const int warps = int(blockDim.x >> 5);
+    for (int w = 0; w < warps; ++w) t += red[w];
+    return t;
 }
 
 template <class T>
@@ -290,53 +307,129 @@ __device__ __forceinline__ int boundary_class(int x, int y, int z, int nx, int n
            ((z == nz - 1) << 5);
 }
 
-// 1/diag for each of the 64 boundary classes of level L (diag_at order).
+// omega/diag for each of the 64 boundary classes of level L (diag_at order).
 template <int BC, class T>
-__device__ void reciprocal_table(const Lv<T>& L, T* table) {
+__device__ void omega_table(const Lv<T>& L, T* table) {
     for (int k = threadIdx.x; k < 64; k += blockDim.x) {
         const int x = (k & 1) ? 0 : ((k & 2) ? L.nx - 1 : (L.nx > 2 ? 1 : 0));
         const int y = (k & 4) ? 0 : ((k & 8) ? L.ny - 1 : (L.ny > 2 ? 1 : 0));
         const int z = (k & 16) ? 0 : ((k & 32) ? L.nz - 1 : (L.nz > 2 ? 1 : 0));
         // classes that cannot occur (first and last both set on an axis longer
         // than one cell) get an unused value
-        table[k] = T(1) / diag_at<BC>(x, y, z, L);
+        table[k] = omega<T>() / diag_at<BC>(x, y, z, L);
     }
 }
 
+// (A p)_i of the block path, pc = p_i.
 template <int BC, class T>
-__device__ __forceinline__ T jacobi_at(const T* __restrict__ cur, const T* __restrict__ R, int i, int x, int y, int z,
-                                       const Lv<T>& L, const T* rdiag) {
-    const T pc = cur[i];
-    const T a = neg_lap<BC, false>(cur, i, x, y, z, L, T(0), pc);
-    return pc + (omega<T>() * (R[i] - a)) * rdiag[boundary_class(x, y, z, L.nx, L.ny, L.nz)];
+__device__ __forceinline__ T block_apply(const T* __restrict__ p, int i, int x, int y, int z, const Lv<T>& L, T pc) {
+    if (BC == AFSI_BC_NEUMANN) {
+        const int sx = L.ny * L.nz, sy = L.nz;
+        const T xm = x > 0 ? p[i - sx] : pc, xp = x + 1 < L.nx ? p[i + sx] : pc;
+        const T ym = y > 0 ? p[i - sy] : pc, yp = y + 1 < L.ny ? p[i + sy] : pc;
+        const T zm = z > 0 ? p[i - 1] : pc, zp = z + 1 < L.nz ? p[i + 1] : pc;
+        return __fma_rn((pc - xm) + (pc - xp), L.ih2[0],
+                        __fma_rn((pc - ym) + (pc - yp), L.ih2[1], ((pc - zm) + (pc - zp)) * L.ih2[2]));
+    } else {
+        const int sx = L.ny;
+        T xm, xp;
+        if (BC == AFSI_BC_CHANNEL) {
+            xm = x > 0 ? p[i - sx] : pc;
+            xp = x + 1 < L.nx ? p[i + sx] : -pc;  // outlet ghost: p = 0 on the face
+        } else {
+            xm = p[x > 0 ? i - sx : i + (L.nx - 1) * sx];
+            xp = p[x + 1 < L.nx ? i + sx : i - (L.nx - 1) * sx];
+        }
+        const T ym = y > 0 ? p[i - 1] : pc, yp = y + 1 < L.ny ? p[i + 1] : pc;
+        return __fma_rn((pc - xm) + (pc - xp), L.ih2[0], ((pc - ym) + (pc - yp)) * L.ih2[1]);
+    }
 }
 
+// Full-weighting restriction of the residual rhs - A p at coarse cell (cx,cy,cz).
 template <int BC, class T>
-__device__ void block_smooth(T*& cur, T*& oth, const T* R, const Lv<T>& L, const FastCoords<T>& fc, const T* rdiag,
-                             int smooth) {
+__device__ __forceinline__ T block_restrict(const T* __restrict__ p, const T* __restrict__ rhs, int cx, int cy, int cz,
+                                            const Lv<T>& L) {
+    if constexpr (BC == AFSI_BC_NEUMANN) {
+        T v = T(0);
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b)
+#pragma unroll
+                for (int d = 0; d < 2; ++d) {
+                    const int x = 2 * cx + a, y = 2 * cy + b, z = 2 * cz + d;
+                    const int i = (x * L.ny + y) * L.nz + z;
+                    v = v + (rhs[i] - block_apply<BC>(p, i, x, y, z, L, p[i]));
+                }
+        return v * T(.125);
+    } else {
+        T r[4];
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                const int x = 2 * cx + a, y = 2 * cy + b;
+                const int i = x * L.ny + y;
+                r[a * 2 + b] = rhs[i] - block_apply<BC>(p, i, x, y, 0, L, p[i]);
+            }
+        return ((r[0] + r[1]) + r[2] + r[3]) * T(.25);
+    }
+}
+
+// `smooth` Jacobi sweeps of level L in ping-pong buffers cur/oth.  zero: the
+// iterate starts at 0 (the first sweep reads no neighbours); rhs_shift: a
+// pending mean of R, subtracted in the first sweep and written back.
+// Returns the buffer of the final iterate; *mean gets its mean (singular BCs).
+template <int BC, class T>
+__device__ T* block_smooth(T* cur, T* oth, T* R, const Lv<T>& L, const FastCoords<T>& fc, const T* wrd, int smooth,
+                           bool zero, T rhs_shift, double (*red)[32], int& rt, T* mean) {
+    constexpr bool singular = BC != AFSI_BC_CHANNEL;
+    const int n = int(L.n);
     for (int s = 0; s < smooth; ++s) {
-        for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
+        const bool last = s == smooth - 1;
+        double acc = 0.0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
             int x, y, z;
             fc.get(i, L, x, y, z);
-            oth[i] = jacobi_at<BC>(cur, R, i, x, y, z, L, rdiag);
+            const T w = wrd[boundary_class(x, y, z, L.nx, L.ny, L.nz)];
+            T v;
+            if (s == 0 && zero) {
+                const T r = R[i] - rhs_shift;
+                if (rhs_shift != T(0)) R[i] = r;
+                v = r * w;
+            } else {
+                const T pc = cur[i];
+                v = __fma_rn(R[i] - block_apply<BC>(cur, i, x, y, z, L, pc), w, pc);
+            }
+            oth[i] = v;
+            if (last) acc += double(v);
         }
-        __syncthreads();
+        if (last && singular) {
+            *mean = T(block_sum_all(acc, red[rt]) / double(n));
+            rt ^= 1;
+        } else {
+            __syncthreads();
+        }
         T* t = cur;
         cur = oth;
         oth = t;
     }
+    if (!singular) *mean = T(0);
+    return cur;
 }
 
 // Levels first..last of one V-cycle in one CTA (fast arithmetic).  rhs of
 // level `first` comes from global memory (shifted by rhs_sum/n); p[first]
-// starts from p_global (first==0) or zero; the final p[first] is written to
-// p_out.  smem holds, per level, p, its Jacobi partner and rhs, then the
-// reciprocal-diagonal tables.
+// starts from p_global (first==0) or zero; the final p[first], mean removed
+// for the singular operators, is written to p_out.  smem holds, per level, p,
+// its Jacobi partner and rhs, then the omega/diag tables.
 template <int BC, class T, class TC>
 __device__ void coarse_cycle(T* smem, const T* __restrict__ rhs_global, const double* rhs_sum, const T* p_global,
                              T* p_out, const TC* __restrict__ cinv, const CoarseLevels<T>& cl, int smooth) {
-    __shared__ double red[32];
+    __shared__ double red[2][32];
+    __shared__ T down_mean[AFSI_MG_MAX_LEVELS];  // pending mean of each level's pre-smoothed iterate
     constexpr bool singular = BC != AFSI_BC_CHANNEL;
+    int rt = 0;
     const int f = cl.first, last = cl.last;
     // layout: [P_f Q_f R_f][P_f+1 ...]...[tables]
     auto level_base = [&](int l) {
@@ -345,94 +438,98 @@ __device__ void coarse_cycle(T* smem, const T* __restrict__ rhs_global, const do
         return smem + off;
     };
     T* tables = level_base(last + 1);
-    for (int l = f; l <= last; ++l) reciprocal_table<BC>(cl.lv[l], tables + 64 * (l - f));
+    for (int l = f; l <= last; ++l) omega_table<BC>(cl.lv[l], tables + 64 * (l - f));
     {
         const T mr = T(site_mean(rhs_sum, cl.lv[f].n));
         T* P = level_base(f);
         T* R = P + 2 * cl.lv[f].n;
         for (int i = threadIdx.x; i < cl.lv[f].n; i += blockDim.x) {
             R[i] = rhs_global[i] - mr;
-            P[i] = p_global ? p_global[i] : T(0);
+            if (p_global) P[i] = p_global[i];
         }
     }
     __syncthreads();
-    // down
+    // down: pre-smooth, restrict the residual; the restricted rhs mean is
+    // pending into the next level's first sweep
+    T rhs_shift = T(0);
     for (int l = f; l < last; ++l) {
         const Lv<T>& L = cl.lv[l];
         const Lv<T>& C = cl.lv[l + 1];
         T* P = level_base(l);
-        T* Q = P + L.n;
-        T* R = Q + L.n;
-        T* Pc = level_base(l + 1);
-        T* Rc = Pc + 2 * C.n;
+        T* R = P + 2 * L.n;
+        T* Rc = level_base(l + 1) + 2 * C.n;
         FastCoords<T> fcL, fcC;
         fcL.init(L);
         fcC.init(C);
-        T* cur = P;
-        T* oth = Q;
-        block_smooth<BC>(cur, oth, R, L, fcL, tables + 64 * (l - f), smooth);
-        const T m = singular ? block_mean(cur, int(L.n), red) : T(0);
-        for (int i = threadIdx.x; i < L.n; i += blockDim.x) P[i] = cur[i] - m;
-        __syncthreads();
+        T m;
+        const T* cur = block_smooth<BC>(P, P + L.n, R, L, fcL, tables + 64 * (l - f), smooth,
+                                        l > f || !p_global, rhs_shift, red, rt, &m);
+        if (threadIdx.x == 0) down_mean[l] = m;
+        double acc = 0.0;
         for (int c = threadIdx.x; c < C.n; c += blockDim.x) {
             int cx, cy, cz;
             fcC.get(c, C, cx, cy, cz);
-            Rc[c] = restrict_residual_at<BC, false>(P, R, cx, cy, cz, L, T(0));
-            Pc[c] = T(0);
+            const T v = block_restrict<BC>(cur, R, cx, cy, cz, L);
+            Rc[c] = v;
+            acc += double(v);
         }
-        __syncthreads();
         if (singular) {
-            const T mc = block_mean(Rc, int(C.n), red);
-            for (int i = threadIdx.x; i < C.n; i += blockDim.x) Rc[i] = Rc[i] - mc;
+            rhs_shift = T(block_sum_all(acc, red[rt]) / double(C.n));
+            rt ^= 1;
+        } else {
             __syncthreads();
         }
     }
-    // dense coarsest solve p = inv * rhs (mac/mg_workspace.py:86-90), warp per row
+    // dense coarsest solve p = inv * (rhs - shift) (mac/mg_workspace.py:86-90), warp per row
+    T coarse_shift;
     {
         const Lv<T>& L = cl.lv[last];
         T* P = level_base(last);
-        T* R = P + 2 * L.n;
+        const T* R = P + 2 * L.n;
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+        double acc = 0.0;
         for (int r = warp; r < L.n; r += warps) {
             double s = 0.0;
-            for (int j = lane; j < L.n; j += 32) s += double(cinv[int64_t(r) * L.n + j]) * double(R[j]);
+            for (int j = lane; j < L.n; j += 32) s += double(cinv[int64_t(r) * L.n + j]) * double(R[j] - rhs_shift);
             s = warp_sum(s);
-            if (lane == 0) P[r] = T(s);
+            const T v = T(s);
+            if (lane == 0) {
+                P[r] = v;
+                acc += double(v);
+            }
         }
-        __syncthreads();
         if (singular) {
-            const T m = block_mean(P, int(L.n), red);
-            for (int i = threadIdx.x; i < L.n; i += blockDim.x) P[i] = P[i] - m;
+            coarse_shift = T(block_sum_all(acc, red[rt]) / double(L.n));
+            rt ^= 1;
+        } else {
+            coarse_shift = T(0);
             __syncthreads();
         }
     }
-    // up
+    // up: add the prolonged correction to the shifted pre-smoothed iterate,
+    // post-smooth; the level's mean is pending into the level above
+    const T* corr = level_base(last);
     for (int l = last - 1; l >= f; --l) {
         const Lv<T>& L = cl.lv[l];
         const Lv<T>& C = cl.lv[l + 1];
         T* P = level_base(l);
         T* Q = P + L.n;
         T* R = Q + L.n;
-        const T* Pc = level_base(l + 1);
+        T* down = (smooth & 1) ? Q : P;  // where the pre-smoothing left the iterate
+        const T dm = down_mean[l];
         FastCoords<T> fcL;
         fcL.init(L);
         for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
             int x, y, z;
             fcL.get(i, L, x, y, z);
-            P[i] = P[i] + prolong_at<BC>(Pc, x, y, z, C, T(0));
+            P[i] = (down[i] - dm) + prolong_at<BC>(corr, x, y, z, C, coarse_shift);
         }
         __syncthreads();
-        T* cur = P;
-        T* oth = Q;
-        block_smooth<BC>(cur, oth, R, L, fcL, tables + 64 * (l - f), smooth);
-        const T m = singular ? block_mean(cur, int(L.n), red) : T(0);
-        for (int i = threadIdx.x; i < L.n; i += blockDim.x) P[i] = cur[i] - m;
-        __syncthreads();
+        T m;
+        corr = block_smooth<BC>(P, Q, R, L, fcL, tables + 64 * (l - f), smooth, false, T(0), red, rt, &m);
+        coarse_shift = m;
     }
-    {
-        const T* P = level_base(f);
-        for (int i = threadIdx.x; i < cl.lv[f].n; i += blockDim.x) p_out[i] = P[i];
-    }
+    for (int i = threadIdx.x; i < cl.lv[f].n; i += blockDim.x) p_out[i] = corr[i] - coarse_shift;
     __syncthreads();
 }
 

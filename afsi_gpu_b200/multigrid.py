@@ -254,10 +254,51 @@ class _Solver:
                 with torch.cuda.graph(g, stream=s):
                     w.vcycles(count)
                 self.graph_launches[count] = _lib.launch_count() - before
+                _lib.forget_launches(self.graph_launches[count])
                 self.graphs[count] = g
             torch.cuda.current_stream(device).wait_stream(s)
             for t in (*w.p, *w.ping, *w.rhs):
                 t.zero_()
+        self._capture_loop()
+
+    def _capture_loop(self):
+        """The host solve loop as one device graph (``afsi_b200_mg_solve_graph_create``):
+        blocks of ``check_every`` V-cycles with the residual check between them."""
+        w = self.workspace
+        self.loop_graph = None
+        if self.options.max_cycles < self.options.check_every:
+            return
+        self.loop = torch.zeros(4, dtype=torch.float64, device=w.p[0].device)
+        handle = ctypes.c_void_p()
+        before = _lib.launch_count()
+        with torch.cuda.device(w.p[0].device):
+            _lib.call('afsi_b200_mg_solve_graph_create', ctypes.byref(w.plan), self.options.check_every,
+                      self.options.max_cycles, _lib.ptr(self.loop), _lib.ptr(w.norm), ctypes.byref(handle))
+        self.loop_graph = handle.value
+        self.loop_body_launches = _lib.launch_count() - before
+        _lib.forget_launches(self.loop_body_launches)
+
+    def __del__(self):
+        graph = getattr(self, 'loop_graph', None)
+        if graph:
+            try:
+                _lib.call('afsi_b200_mg_solve_graph_destroy', graph)
+            except Exception:
+                pass
+            self.loop_graph = None
+
+    def _run_loop(self, tol):
+        """Device-side check loop from cycle 0; returns (cycles, residual)."""
+        lp = self.loop
+        lp.zero_()
+        lp[0].fill_(tol)
+        _lib.call('afsi_b200_mg_solve_graph_launch', self.loop_graph, _lib.stream(lp.device))
+        _, cycles, residual, nonfinite = lp.tolist()
+        cycles = int(cycles)
+        _lib.count_replay(cycles // self.options.check_every * self.loop_body_launches)
+        if nonfinite:
+            raise RuntimeError('nonfinite multigrid residual')
+        return cycles, residual
 
     def advance(self, count):
         if self.persistent:
@@ -340,6 +381,8 @@ class _Solver:
                 raise RuntimeError('persistent multigrid barrier timed out')
             if not isfinite(residual):
                 raise RuntimeError('nonfinite multigrid residual')
+        if getattr(self, 'loop_graph', None) and residual > tol:
+            cycle, residual = self._run_loop(tol)
         while residual > tol and cycle < self.options.max_cycles:
             count = min(self.options.check_every, self.options.max_cycles - cycle)
             self.advance(count)

@@ -234,6 +234,20 @@ int32_t afsi_b200_mg_vcycles(const afsi_mg_plan* plan, int32_t cycles, afsi_stre
  * last residual norm or -1 if unchecked, 0 or 1 if a barrier timed out}.
  * sync_scratch: afsi_b200_mg_sync_bytes() zero-initialised device bytes,
  * private to one stream at a time. */
+/* The solve loop (mac/multigrid.py:88-97) as one CUDA graph: a WHILE
+ * conditional node whose body runs check_every V-cycles, the residual norm
+ * into `norm` (device double) and a decide kernel on `loop` (device
+ * double[4]: [0] tol, written by the caller before each launch; [1] cycles
+ * run, reset by the caller; [2] last residual norm; [3] 1 if it was
+ * nonfinite).  The loop ends when the norm is <= tol, nonfinite, or another
+ * block of check_every cycles would pass max_cycles (the caller runs any
+ * remaining cycles itself).  Requires 1 <= check_every <= max_cycles.  The
+ * graph is captured on a private stream and launched on the caller's. */
+int32_t afsi_b200_mg_solve_graph_create(const afsi_mg_plan* plan, int32_t check_every, int32_t max_cycles,
+    double* loop, double* norm, void** graph_out);
+int32_t afsi_b200_mg_solve_graph_launch(void* graph, afsi_stream_t stream);
+int32_t afsi_b200_mg_solve_graph_destroy(void* graph);
+
 int64_t afsi_b200_mg_sync_bytes(void);
 int32_t afsi_b200_mg_persistent(const afsi_mg_plan* plan, int32_t cycles, int32_t solve, int32_t check_every,
     double tol, double* info, void* sync_scratch, afsi_stream_t stream);

@@ -198,3 +198,30 @@ def test_fp32_multigrid_converges_with_fp64_coarse_solve():
     ref, _ = oracle.solve(oracle.Hierarchy(grid.shape, grid.spacing, 'neumann'), rhs.numpy())
     err = np.abs(p.double().cpu().numpy() - ref).max() / np.abs(ref).max()
     assert info['residual_norm'] <= info['tolerance'] and err < 1e-4
+
+
+def test_device_solve_loop_follows_the_host_check_schedule():
+    """The graph backend's device-side loop (WHILE graph node) runs the same
+    cycles as the host loop: blocks of check_every with a residual check after
+    each, the tail past the last full block on the host; results bitwise equal."""
+    grid = MACGrid((32, 32, 32), (1., 1., 1.))
+    rhs = synthetic.mean_free_normal(grid.shape, seed=6).to(DEV)
+    hopeless = MGOptions(max_cycles=5, check_every=2, rtol=1e-300, atol=1e-300)
+    host = GeometricMultigrid(grid, options=hopeless, backend='b200')
+    dev = GeometricMultigrid(grid, options=hopeless, backend='b200-graph')
+    assert dev.loop_graph
+    for mg in (host, dev):
+        with pytest.raises(RuntimeError, match='did not converge'):
+            mg.solve(rhs)
+    assert torch.equal(host.workspace.p[0], dev.workspace.p[0])  # 5 cycles each
+    for check_every in (1, 3):
+        opts = MGOptions(check_every=check_every)
+        a, ia = GeometricMultigrid(grid, options=opts, backend='b200').solve(rhs)
+        b, ib = GeometricMultigrid(grid, options=opts, backend='b200-graph').solve(rhs)
+        assert ia['cycles'] == ib['cycles'] and ia['cycles'] % check_every == 0
+        assert torch.equal(a, b) and ia['residual_norm'] == ib['residual_norm']
+    cgrid = ChannelGrid((64, 16), (4., 1.))
+    crhs = torch.as_tensor(np.random.default_rng(3).standard_normal(cgrid.shape), device=DEV)
+    a, ia = ChannelMultigrid(cgrid, backend='b200').solve(crhs)
+    b, ib = ChannelMultigrid(cgrid, backend='b200-graph').solve(crhs)
+    assert ia['cycles'] == ib['cycles'] and torch.equal(a, b)
