@@ -266,17 +266,19 @@ struct CoarseLevels {
 };
 
 // Sum of v over the block, returned to every thread: one barrier.  Warp
-// partials go to red (32 slots); every thread adds them in slot order.  The
-// caller alternates between two red buffers so that a slot is rewritten only
-// after a later barrier.
+// partials go to red (32 slots); every warp then reduces the slots with the
+// same butterfly, so all threads get the same value.  The caller alternates
+// between two red buffers so that a slot is rewritten only after a later
+// barrier.
 __device__ __forceinline__ double block_sum_all(double v, double* red) {
 #pragma unroll
     for (int d = 16; d; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    const int lane = threadIdx.x & 31;
+    if (lane == 0) red[threadIdx.x >> 5] = v;
     __syncthreads();
-    double t = 0.0;
-    const int warps = int(blockDim.x >> 5);
-    for (int w = 0; w < warps; ++w) t += red[w];
+    double t = lane < int(blockDim.x >> 5) ? red[lane] : 0.0;
+#pragma unroll
+    for (int d = 16; d; d >>= 1) t += __shfl_xor_sync(0xffffffffu, t, d);
     return t;
 }
 
