@@ -30,6 +30,11 @@ from afsi_torch.mac.adaptive_transfer import (AdaptiveFETransfer, InteractionQua
                                               gaussian_tetra_rule, _orders, _orders_p2)
 from afsi_torch.tetrahedron import reference_nodes, tabulate, promote_p1  # noqa: E402
 from afsi_torch.solid import prepare_p2  # noqa: E402
+from afsi_torch.p1 import prepare_p1  # noqa: E402
+from afsi_torch.mac.adaptive_transfer import AdaptiveP1Transfer  # noqa: E402
+from afsi_torch.mac.assembled_transfer import AssembledP1Transfer  # noqa: E402
+from afsi_torch.mac.hash_transfer_assembly import hash_slot  # noqa: E402
+from afsi_torch.fluid.solvers import SolverOptions  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
 torch.set_default_dtype(torch.float64)
@@ -217,6 +222,66 @@ def orders():
     save('orders', **arrays)
 
 
+def kuhn_block(nx, ny, nz, h, origin, seed):
+    """Cube block cut into six Kuhn tetrahedra per cube, nodes jittered."""
+    g = torch.Generator().manual_seed(seed)
+    idx = torch.arange((nx + 1) * (ny + 1) * (nz + 1)).reshape(nx + 1, ny + 1, nz + 1)
+    grid = torch.stack(torch.meshgrid(*(torch.arange(n + 1.) for n in (nx, ny, nz)), indexing='ij'), -1)
+    X = grid.reshape(-1, 3) * h + torch.tensor(origin) + (torch.rand((idx.numel(), 3), generator=g) - .5) * .2 * h
+    cells = []
+    for i in range(nx):
+        for j in range(ny):
+            for k in range(nz):
+                for perm in ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)):
+                    v, path = [i, j, k], [int(idx[i, j, k])]
+                    for axis in perm:
+                        v[axis] += 1
+                        path.append(int(idx[v[0], v[1], v[2]]))
+                    cells.append(path)
+    return X, torch.tensor(cells)
+
+
+def p1csr():
+    """P1 CSR operators B_c (AssembledP1Transfer, coalesce backend) and the
+    SplitMix64 bucket of the hash assembly, on two P1 meshes."""
+    grid = MACGrid((12, 14, 16), (10., 12., 14.))
+    cases = dict(
+        pair=(torch.tensor([[4, 4, 4], [4.3, 4, 4], [4, 4.3, 4], [4, 4, 4.3], [4, 4, 2.6]]),
+              torch.tensor([[0, 1, 2, 3], [0, 2, 1, 4]])),
+        block=kuhn_block(4, 3, 3, .55, (3.2, 3.9, 4.6), seed=11))
+    X, cells = cases['block']
+    X[:, 0] = 3.2 + (X[:, 0] - 3.2) * (1 + .35 * (X[:, 0] - 3.2))  # stretched in x: several orders
+    arrays = dict(shape=grid.shape, lengths=grid.lengths, origin=grid.origin)
+    for name, (X, cells) in cases.items():
+        geometry = prepare_p1(X, cells, degree=2)
+        common = dict(quadrature_options=InteractionQuadratureOptions(mode='adaptive', stencil_backend='shared'),
+                      fused=False, options=SolverOptions(rtol=1e-12, atol=1e-13))
+        reference = AdaptiveP1Transfer(grid, geometry, **common)
+        assembled = AssembledP1Transfer(grid, geometry, chunk_entries=512, **common)
+        stencil = reference.prepare(X)
+        B = assembled.assemble_stencil(stencil)
+        arrays[f'{name}_X'] = X
+        arrays[f'{name}_cells'] = cells
+        if name == 'pair':
+            arrays[f'{name}_base'] = stencil.base
+            arrays[f'{name}_phi'] = stencil.phi
+        arrays[f'{name}_ngroups'] = len(stencil.rule.groups)
+        for k, gr in enumerate(stencil.rule.groups):
+            arrays[f'{name}_cells{k}'] = gr.cells
+            arrays[f'{name}_N{k}'] = gr.values
+            arrays[f'{name}_W{k}'] = gr.weights
+        for c, m in enumerate(B.gather):
+            arrays[f'{name}_crow{c}'] = m.crow_indices()
+            arrays[f'{name}_col{c}'] = m.col_indices()
+            arrays[f'{name}_val{c}'] = m.values()
+    keys = torch.cat((torch.arange(200), torch.arange(64) * 2147483649 + 4294967296,
+                      torch.randint(0, 2 ** 62, (64,), generator=torch.Generator().manual_seed(12))))
+    arrays['hash_keys'] = keys
+    for cap in (128, 4096, 1 << 20):
+        arrays[f'hash_slot_{cap}'] = torch.tensor([hash_slot(int(k), cap) for k in keys])
+    save('p1csr', **arrays)
+
+
 def quadrature():
     arrays = {}
     like = torch.zeros(1)
@@ -236,3 +301,4 @@ if __name__ == '__main__':
     mg2d()
     quadrature()
     orders()
+    p1csr()
