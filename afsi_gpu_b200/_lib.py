@@ -50,6 +50,24 @@ _SIGNATURES = {
                              c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int32, c_void_p],
     'afsi_b200_p2_orders': [c_void_p, c_int64, c_void_p, c_int64, ctypes.c_double, ctypes.c_double, c_int64,
                             c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p],
+    'afsi_b200_p1_prepare': [c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, P_F64, P_F64, P_F64,
+                             c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int32, c_void_p],
+    'afsi_b200_p1_orders': [c_void_p, c_int64, c_void_p, c_int64, ctypes.c_double, ctypes.c_double, c_int64,
+                            c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p],
+    'afsi_b200_p1_plan_scratch_bytes': [c_int64],
+    'afsi_b200_p1_component_plan': [c_void_p, c_int64, c_int64, c_int64, c_int64, c_int32, c_int32, c_void_p,
+                                    c_void_p, c_void_p, c_void_p, c_int64, c_void_p],
+    'afsi_b200_hash_contract': [c_void_p] * 11 + [c_int64] * 5 + [c_int64, c_int32, c_int64, c_int64, c_int64,
+                                                                    c_int32, c_int32, c_void_p],
+    'afsi_b200_cached_contract': [c_void_p] * 11 + [c_int64, c_void_p, c_void_p, c_void_p, c_int64] +
+                                 [c_int64] * 5 + [c_int32, c_int64, c_int64, c_int64, c_int32, c_int32, c_void_p],
+    'afsi_b200_hash_accumulate': [c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_int64, c_int32,
+                                  c_void_p],
+    'afsi_b200_hash_csr_scratch_bytes': [c_int64, c_int32],
+    'afsi_b200_hash_csr': [c_void_p, c_void_p, c_int64, c_int64, c_int64] + [c_void_p] * 8 + [c_int64, c_int32,
+                                                                                             c_void_p],
+    'afsi_b200_csr_spmv': [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int64, c_void_p, c_int64,
+                           ctypes.c_double, c_int32, c_void_p],
     'afsi_b200_mg_solve_graph_create': [ctypes.POINTER(MGPlan), c_int32, c_int32, c_void_p, c_void_p,
                                         ctypes.POINTER(c_void_p)],
     'afsi_b200_mg_solve_graph_launch': [c_void_p, c_void_p],
@@ -92,7 +110,8 @@ _SIGNATURES = {
     'afsi_b200_subtract_mean': [c_void_p, c_int64, c_void_p, c_int32, c_void_p],
 }
 _RESTYPES = {'afsi_b200_last_error': ctypes.c_char_p, 'afsi_b200_mg_scratch_bytes': ctypes.c_int64,
-             'afsi_b200_launch_count': ctypes.c_int64, 'afsi_b200_mg_sync_bytes': ctypes.c_int64}
+             'afsi_b200_launch_count': ctypes.c_int64, 'afsi_b200_mg_sync_bytes': ctypes.c_int64,
+             'afsi_b200_p1_plan_scratch_bytes': ctypes.c_int64, 'afsi_b200_hash_csr_scratch_bytes': ctypes.c_int64}
 
 
 def exported_symbols():

@@ -1,0 +1,523 @@
+// P1 CSR operators for the B200.
+//
+// For component c of a P1 interaction rule, B_c[node, face] = Σ over the
+// cells holding the node, Σ over the cell's quadrature points of
+// W·N[q,a]·φx·φy·φz, over the faces of the point's 4x4x4 support.  The
+// reference (mac/csrc/ib.cu:22-116) visits every face ("site") of each cell's
+// support box with one warp per site, its lanes over the cell's points, and
+// adds the four nodal sums into a hash keyed node·nf + face.
+//
+// Here one warp owns one cell: the cell's points are staged in shared memory
+// (relative bases, the three 4-weight rows, W and the four shape values), and
+// the lanes walk the box sites, each lane accumulating its site's four nodal
+// sums over the staged points in point order (no shuffles, no per-site binary
+// search).  The hash table semantics are the reference's, so a table built
+// here is interchangeable with one built there: SplitMix64 finaliser bucket
+// (mac/csrc/ib.cu:14-19), linear probing over at most 128 slots, a key
+// claimed with a 64-bit CAS on -1, the value added atomically, zero values
+// skipped, and the flag set to 1 on a negative key or a failed probe.  The
+// cached form only looks keys up and streams the misses out.
+//
+// hash -> CSR: empty slots become a sentinel just above the largest valid
+// key, the whole table is radix-sorted (CUB) on the bits the keys use, the
+// row boundaries come from one pass over the sorted keys, and the transpose
+// is a second sort on column-major keys.  No host synchronisation: the
+// number of entries and the validity flags land in a device info word.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+#include "common.cuh"
+
+namespace afsi {
+
+constexpr int kCellWarps = 4;        // warps per block in the contraction
+constexpr int64_t kFar = 1 << 20;    // larger than any box extent: marks a point outside every site
+
+__device__ __forceinline__ uint64_t hash_bucket(int64_t key, int64_t capacity) {
+    uint64_t h = uint64_t(key);
+    h = (h ^ (h >> 30)) * 0xbf58476d1ce4e5b9ull;
+    h = (h ^ (h >> 27)) * 0x94d049bb133111ebull;
+    return (h ^ (h >> 31)) & uint64_t(capacity - 1);
+}
+
+template <class T>
+struct Table {
+    int64_t* keys;
+    T* values;
+    int64_t capacity;
+    int32_t* flag;
+    // cached form: miss stream
+    int64_t* mkeys;
+    T* mvalues;
+    unsigned long long* mcount;
+    int64_t mcap;
+};
+
+template <class T, bool Cached>
+__device__ void table_add(int64_t key, T value, const Table<T>& t) {
+    if (value == T(0)) return;
+    if (key < 0) {
+        atomicExch(t.flag, 1);
+        return;
+    }
+    uint64_t slot = hash_bucket(key, t.capacity);
+    const uint64_t mask = uint64_t(t.capacity - 1);
+    for (int probe = 0; probe < 128; ++probe, slot = (slot + 1) & mask) {
+        int64_t previous;
+        if (Cached)  // the key table is immutable during a cached launch
+            previous = t.keys[slot];
+        else
+            previous = int64_t(atomicCAS(reinterpret_cast<unsigned long long*>(t.keys + slot), ~0ull,
+                                         static_cast<unsigned long long>(key)));
+        if (previous == key || (!Cached && previous == -1)) {
+            atomicAdd(t.values + slot, value);
+            return;
+        }
+        if (Cached && previous == -1) break;
+    }
+    if (Cached) {
+        const unsigned long long i = atomicAdd(t.mcount, 1ull);
+        if (i < static_cast<unsigned long long>(t.mcap)) {
+            t.mkeys[i] = key;
+            t.mvalues[i] = value;
+        }
+    } else {
+        atomicExch(t.flag, 1);
+    }
+}
+
+struct CellDims {
+    int64_t total, offset, cells, nq, count, ny, nz, nf, nx;
+    int c;
+    bool shared;
+};
+
+template <class T>
+struct CellStage {
+    T phi[32][3][4];
+    T w[32];
+    T n[32][4];
+    int d[32][3];
+};
+
+template <class T, bool Cached>
+__global__ void __launch_bounds__(kCellWarps * 32) contract_kernel(const int64_t* __restrict__ base,
+                                                                  const T* __restrict__ phi, const T* __restrict__ N,
+                                                                  const T* __restrict__ W,
+                                                                  const int64_t* __restrict__ cells,
+                                                                  const int64_t* __restrict__ low,
+                                                                  const int64_t* __restrict__ width,
+                                                                  const int64_t* __restrict__ prefix, Table<T> t,
+                                                                  CellDims g) {
+    __shared__ CellStage<T> stage_all[kCellWarps];
+    CellStage<T>& s = stage_all[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = int64_t(gridDim.x) * kCellWarps;
+    int lat[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) lat[a] = g.shared ? int(a != g.c) : g.c;
+    for (int64_t e = int64_t(blockIdx.x) * kCellWarps + (threadIdx.x >> 5); e < g.cells; e += warps) {
+        const int64_t first = prefix[e];
+        if (first >= g.count) continue;
+        const int64_t lx = low[e * 3], ly = low[e * 3 + 1], lz = low[e * 3 + 2];
+        const int64_t wx = width[e * 3], wy = width[e * 3 + 1], wz = width[e * 3 + 2];
+        const int64_t sites = prefix[e + 1] - first;
+        if (wx <= 0 || wy <= 0 || wz <= 0 || wx > kFar || wy > kFar || wz > kFar || sites != wx * wy * wz) {
+            if (lane == 0) atomicExch(t.flag, 1);  // malformed plan: nothing of this cell is added
+            continue;
+        }
+        int64_t node[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) node[a] = cells[e * 4 + a];
+        for (int64_t t0 = 0; t0 < sites; t0 += 32) {
+            const int64_t site = t0 + lane;
+            const int sz = int(site % wz), sy = int((site / wz) % wy), sx = int(site / (wy * wz));
+            T sums[4] = {T(0), T(0), T(0), T(0)};
+            for (int64_t q0 = 0; q0 < g.nq; q0 += 32) {
+                const int nj = int(g.nq - q0 < 32 ? g.nq - q0 : 32);
+                if (t0 == 0 || g.nq > 32) {  // with one chunk, staged once for the first batch of sites
+                    __syncwarp();
+                    if (lane < nj) {
+                        const int64_t row = g.offset + e * g.nq + q0 + lane;
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            const int64_t r = (int64_t(lat[a]) * g.total + row) * 3 + a;
+                            const int64_t lo = a == 0 ? lx : a == 1 ? ly : lz;
+                            const int64_t rel = base[r] - lo;
+                            s.d[lane][a] = int(rel < 0 || rel > kFar ? kFar : rel);
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) s.phi[lane][a][k] = phi[r * 4 + k];
+                        }
+                        s.w[lane] = W[e * g.nq + q0 + lane];
+#pragma unroll
+                        for (int a = 0; a < 4; ++a) s.n[lane][a] = N[(q0 + lane) * 4 + a];
+                    }
+                    __syncwarp();
+                }
+                for (int j = 0; j < nj; ++j) {
+                    const unsigned dx = unsigned(sx - s.d[j][0]), dy = unsigned(sy - s.d[j][1]),
+                                   dz = unsigned(sz - s.d[j][2]);
+                    if (dx < 4u && dy < 4u && dz < 4u) {
+                        const T k = ((s.phi[j][0][dx] * s.phi[j][1][dy]) * s.phi[j][2][dz]) * s.w[j];
+#pragma unroll
+                        for (int a = 0; a < 4; ++a) sums[a] += k * s.n[j][a];
+                    }
+                }
+            }
+            if (site < sites && first + site < g.count) {
+                const int64_t gx = lx + sx, gy = ly + sy, gz = lz + sz;
+                if (gx < 0 || gy < 0 || gz < 0 || gx >= g.nx || gy >= g.ny || gz >= g.nz) {
+                    atomicExch(t.flag, 1);
+                } else {
+                    const int64_t face = (gx * g.ny + gy) * g.nz + gz;
+#pragma unroll
+                    for (int a = 0; a < 4; ++a) table_add<T, Cached>(node[a] * g.nf + face, sums[a], t);
+                }
+            }
+        }
+    }
+}
+
+template <class T>
+__global__ void accumulate_kernel(const int64_t* __restrict__ in_keys, const T* __restrict__ in_values, int64_t n,
+                                  Table<T> t) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        table_add<T, false>(in_keys[i], in_values[i], t);
+}
+
+// low/width/size of every cell's support box for component c
+// (mac/hash_transfer_assembly.py:122-138).
+__global__ void plan_kernel(const int64_t* __restrict__ base, int64_t total, int64_t offset, int64_t cells,
+                            int64_t nq, int c, bool shared, int64_t* __restrict__ low, int64_t* __restrict__ width,
+                            int64_t* __restrict__ sizes) {
+    const int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= cells) return;
+    int64_t mn[3] = {INT64_MAX, INT64_MAX, INT64_MAX}, mx[3] = {INT64_MIN, INT64_MIN, INT64_MIN};
+    for (int64_t q = 0; q < nq; ++q) {
+        const int64_t row = offset + e * nq + q;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int lat = shared ? int(a != c) : c;
+            const int64_t b = base[(int64_t(lat) * total + row) * 3 + a];
+            mn[a] = b < mn[a] ? b : mn[a];
+            mx[a] = b > mx[a] ? b : mx[a];
+        }
+    }
+    int64_t size = 1;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int64_t w = nq > 0 ? mx[a] - mn[a] + 4 : 0;
+        low[e * 3 + a] = nq > 0 ? mn[a] : 0;
+        width[e * 3 + a] = w;
+        size *= w;
+    }
+    sizes[e] = size;
+}
+
+// Sort keys of the table: valid keys as they are, empty slots as the
+// sentinel (the number of valid keys); counts entries and flags keys outside
+// [0, sentinel) or nonfinite values (info[0] += entries, info[1] |= 1).
+template <class T>
+__global__ void table_keys_kernel(const int64_t* __restrict__ keys, const T* __restrict__ values, int64_t capacity,
+                                  uint64_t sentinel, uint64_t* __restrict__ out, unsigned long long* info) {
+    __shared__ unsigned long long block_count;
+    if (threadIdx.x == 0) block_count = 0;
+    __syncthreads();
+    unsigned long long mine = 0;
+    bool bad = false;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < capacity;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t k = keys[i];
+        if (k >= 0) {
+            ++mine;
+            bad = bad || uint64_t(k) >= sentinel || !isfinite(values[i]);
+            out[i] = uint64_t(k);
+        } else {
+            out[i] = sentinel;
+        }
+    }
+    atomicAdd(&block_count, mine);
+    if (bad) atomicOr(info + 1, 1ull);
+    __syncthreads();
+    if (threadIdx.x == 0 && block_count) atomicAdd(info, block_count);
+}
+
+// Row pointers from sorted keys (row = key / divisor, sentinel = end):
+// crow[r] = first index whose row >= r, for r = 0..rows.
+__global__ void row_pointers_kernel(const uint64_t* __restrict__ keys, int64_t n, uint64_t sentinel,
+                                    uint64_t divisor, int64_t rows, int64_t* __restrict__ crow,
+                                    int64_t* __restrict__ minor) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i <= n; i += int64_t(gridDim.x) * blockDim.x) {
+        const bool valid = i < n && keys[i] < sentinel;
+        const int64_t cur = valid ? int64_t(keys[i] / divisor) : rows;
+        const int64_t prev = i == 0 ? -1 : (keys[i - 1] < sentinel ? int64_t(keys[i - 1] / divisor) : rows);
+        for (int64_t r = prev + 1; r <= cur && r <= rows; ++r) crow[r] = i;
+        if (valid && minor) minor[i] = int64_t(keys[i] % divisor);
+    }
+}
+
+// Column-major keys (col·rows + row) of the sorted B entries; sentinel past nnz.
+__global__ void transpose_keys_kernel(const uint64_t* __restrict__ keys, int64_t n, uint64_t sentinel, uint64_t nf,
+                                      uint64_t rows, uint64_t* __restrict__ out) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const uint64_t k = keys[i];
+        out[i] = k < sentinel ? (k % nf) * rows + k / nf : sentinel;
+    }
+}
+
+// y[r·ys] = (Σ_j val[j]·x[col[j]·xs]) / divisor, L lanes per row.
+template <class T, int L>
+__global__ void csr_spmv_kernel(const int64_t* __restrict__ crow, const int64_t* __restrict__ col,
+                                const T* __restrict__ val, int64_t rows, const T* __restrict__ x, int64_t xs,
+                                T* __restrict__ y, int64_t ys, T divisor) {
+    const int64_t groups = int64_t(gridDim.x) * blockDim.x / L;
+    const int sub = threadIdx.x % L;
+    for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / L; r < rows + (groups - rows % groups) % groups;
+         r += groups) {
+        T s = T(0);
+        if (r < rows) {
+            const int64_t a = crow[r], b = crow[r + 1];
+            for (int64_t j = a + sub; j < b; j += L) s = fma(val[j], x[col[j] * xs], s);
+        }
+#pragma unroll
+        for (int d = L / 2; d; d >>= 1) s += __shfl_xor_sync(0xffffffffu, s, d);
+        if (r < rows && sub == 0) y[r * ys] = s / divisor;
+    }
+}
+
+inline int bit_length(uint64_t v) {
+    int b = 0;
+    while (v) {
+        ++b;
+        v >>= 1;
+    }
+    return b;
+}
+
+template <class T>
+size_t sort_temp_bytes(int64_t capacity) {
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, static_cast<const uint64_t*>(nullptr),
+                                    static_cast<uint64_t*>(nullptr), static_cast<const T*>(nullptr),
+                                    static_cast<T*>(nullptr), int64_t(capacity));
+    return bytes;
+}
+
+}  // namespace afsi
+
+using namespace afsi;
+
+namespace {
+
+bool power_of_two(int64_t n) { return n > 0 && !(n & (n - 1)); }
+
+template <class T>
+Table<T> make_table(int64_t* keys, void* values, int64_t capacity, int32_t* flag) {
+    Table<T> t;
+    t.keys = keys;
+    t.values = static_cast<T*>(values);
+    t.capacity = capacity;
+    t.flag = flag;
+    t.mkeys = nullptr;
+    t.mvalues = nullptr;
+    t.mcount = nullptr;
+    t.mcap = 0;
+    return t;
+}
+
+int32_t contract(const int64_t* base, const void* phi, const void* N, const void* W, const int64_t* cells,
+                 const int64_t* low, const int64_t* width, const int64_t* prefix, int64_t* keys, void* values,
+                 int32_t* flag, int64_t capacity, int64_t* mkeys, void* mvalues, int64_t* mcount, int64_t mcap,
+                 int64_t total, int64_t offset, int64_t elements, int64_t nq, int64_t count, int32_t component,
+                 int64_t ny, int64_t nz, int64_t nf, int32_t shared, int32_t dtype, afsi_stream_t stream,
+                 bool cached) {
+    AFSI_REQUIRE(power_of_two(capacity), "power-of-two hash capacity required");
+    AFSI_REQUIRE(elements >= 0 && nq > 0 && total >= 0, "invalid IB group sizes");
+    AFSI_REQUIRE(offset >= 0 && offset <= total && elements * nq <= total - offset, "IB group offset is out of range");
+    AFSI_REQUIRE(count >= 0 && (count == 0 || elements > 0) && component >= 0 && component < 3,
+                 "invalid IB site count or component");
+    AFSI_REQUIRE(ny > 0 && nz > 0 && nf > 0 && ny <= INT64_MAX / nz && nf % (ny * nz) == 0,
+                 "invalid IB face dimensions");
+    if (count == 0) return AFSI_OK;
+    AFSI_REQUIRE(base && phi && N && W && cells && low && width && prefix && keys && values && flag,
+                 "null device pointer");
+    AFSI_REQUIRE(!cached || (mkeys && mvalues && mcount && mcap >= 0), "invalid IB missing stream");
+    CellDims g;
+    g.total = total;
+    g.offset = offset;
+    g.cells = elements;
+    g.nq = nq;
+    g.count = count;
+    g.ny = ny;
+    g.nz = nz;
+    g.nf = nf;
+    g.nx = nf / (ny * nz);
+    g.c = component;
+    g.shared = shared != 0;
+    const int64_t want = (elements + kCellWarps - 1) / kCellWarps;
+    const unsigned blocks = unsigned(want < 65535 * 8 ? want : 65535 * 8);
+    AFSI_DISPATCH(dtype, {
+        Table<T> t = make_table<T>(keys, values, capacity, flag);
+        if (cached) {
+            t.mkeys = mkeys;
+            t.mvalues = static_cast<T*>(mvalues);
+            t.mcount = reinterpret_cast<unsigned long long*>(mcount);
+            t.mcap = mcap;
+            contract_kernel<T, true><<<blocks, kCellWarps * 32, 0, stream>>>(
+                base, static_cast<const T*>(phi), static_cast<const T*>(N), static_cast<const T*>(W), cells, low,
+                width, prefix, t, g);
+        } else {
+            contract_kernel<T, false><<<blocks, kCellWarps * 32, 0, stream>>>(
+                base, static_cast<const T*>(phi), static_cast<const T*>(N), static_cast<const T*>(W), cells, low,
+                width, prefix, t, g);
+        }
+    });
+    return launched(cached ? "cached_contract" : "hash_contract");
+}
+
+}  // namespace
+
+extern "C" int32_t afsi_b200_hash_contract(const int64_t* base, const void* phi, const void* N, const void* W,
+                                           const int64_t* cells, const int64_t* low, const int64_t* width,
+                                           const int64_t* prefix, int64_t* keys, void* values, int32_t* flag,
+                                           int64_t capacity, int64_t total, int64_t offset, int64_t elements,
+                                           int64_t nq, int64_t count, int32_t component, int64_t ny, int64_t nz,
+                                           int64_t nf, int32_t shared, int32_t dtype, afsi_stream_t stream) {
+    return contract(base, phi, N, W, cells, low, width, prefix, keys, values, flag, capacity, nullptr, nullptr,
+                    nullptr, 0, total, offset, elements, nq, count, component, ny, nz, nf, shared, dtype, stream,
+                    false);
+}
+
+extern "C" int32_t afsi_b200_cached_contract(const int64_t* base, const void* phi, const void* N, const void* W,
+                                             const int64_t* cells, const int64_t* low, const int64_t* width,
+                                             const int64_t* prefix, const int64_t* keys, void* values,
+                                             int32_t* flag, int64_t capacity, int64_t* missing_keys,
+                                             void* missing_values, int64_t* missing_count, int64_t missing_capacity,
+                                             int64_t total, int64_t offset, int64_t elements, int64_t nq,
+                                             int64_t count, int32_t component, int64_t ny, int64_t nz, int64_t nf,
+                                             int32_t shared, int32_t dtype, afsi_stream_t stream) {
+    return contract(base, phi, N, W, cells, low, width, prefix, const_cast<int64_t*>(keys), values, flag, capacity,
+                    missing_keys, missing_values, missing_count, missing_capacity, total, offset, elements, nq,
+                    count, component, ny, nz, nf, shared, dtype, stream, true);
+}
+
+extern "C" int32_t afsi_b200_hash_accumulate(const int64_t* input_keys, const void* input_values, int64_t count,
+                                             int64_t* keys, void* values, int32_t* flag, int64_t capacity,
+                                             int32_t dtype, afsi_stream_t stream) {
+    AFSI_REQUIRE(power_of_two(capacity), "power-of-two hash capacity required");
+    AFSI_REQUIRE(count >= 0, "negative entry count");
+    if (count == 0) return AFSI_OK;
+    AFSI_REQUIRE(input_keys && input_values && keys && values && flag, "null device pointer");
+    const int64_t want = (count + 255) / 256;
+    const unsigned blocks = unsigned(want < 65535 * 8 ? want : 65535 * 8);
+    AFSI_DISPATCH(dtype, {
+        accumulate_kernel<T><<<blocks, 256, 0, stream>>>(input_keys, static_cast<const T*>(input_values), count,
+                                                         make_table<T>(keys, values, capacity, flag));
+    });
+    return launched("hash_accumulate");
+}
+
+extern "C" int64_t afsi_b200_p1_plan_scratch_bytes(int64_t elements) {
+    size_t bytes = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, bytes, static_cast<const int64_t*>(nullptr),
+                                  static_cast<int64_t*>(nullptr), elements > 0 ? elements : 1);
+    return int64_t(bytes) + elements * 8 + 256;
+}
+
+extern "C" int32_t afsi_b200_p1_component_plan(const int64_t* base, int64_t total, int64_t offset,
+                                               int64_t elements, int64_t nq, int32_t component, int32_t shared,
+                                               int64_t* low, int64_t* width, int64_t* prefix, void* scratch,
+                                               int64_t scratch_bytes, afsi_stream_t stream) {
+    AFSI_REQUIRE(elements >= 0 && nq > 0 && component >= 0 && component < 3, "invalid IB plan arguments");
+    AFSI_REQUIRE(offset >= 0 && offset <= total && elements * nq <= total - offset, "IB group offset is out of range");
+    AFSI_REQUIRE(prefix, "null prefix");
+    if (cudaMemsetAsync(prefix, 0, sizeof(int64_t), stream) != cudaSuccess)
+        return fail(AFSI_ERR_CUDA, "prefix clear failed");
+    if (elements == 0) return AFSI_OK;
+    AFSI_REQUIRE(base && low && width && scratch, "null device pointer");
+    AFSI_REQUIRE(scratch_bytes >= afsi_b200_p1_plan_scratch_bytes(elements), "plan scratch too small");
+    int64_t* sizes = static_cast<int64_t*>(scratch);
+    void* temp = static_cast<unsigned char*>(scratch) + ((elements * 8 + 255) / 256) * 256;
+    size_t temp_bytes = size_t(scratch_bytes) - ((elements * 8 + 255) / 256) * 256;
+    plan_kernel<<<blocks_for(elements, 256), 256, 0, stream>>>(base, total, offset, elements, nq, component,
+                                                               shared != 0, low, width, sizes);
+    int32_t rc = launched("p1_component_plan");
+    if (rc) return rc;
+    if (cub::DeviceScan::InclusiveSum(temp, temp_bytes, sizes, prefix + 1, elements, stream) != cudaSuccess)
+        return fail(AFSI_ERR_CUDA, "box prefix scan failed");
+    return launched("p1_component_plan scan");
+}
+
+extern "C" int64_t afsi_b200_hash_csr_scratch_bytes(int64_t capacity, int32_t dtype) {
+    if (capacity <= 0) return 0;
+    size_t temp = dtype == AFSI_F32 ? sort_temp_bytes<float>(capacity) : sort_temp_bytes<double>(capacity);
+    return 2 * ((capacity * 8 + 255) / 256) * 256 + int64_t(temp) + 256;
+}
+
+extern "C" int32_t afsi_b200_hash_csr(const int64_t* keys, const void* values, int64_t capacity, int64_t rows,
+                                      int64_t nf, int64_t* crow, int64_t* col, void* val, int64_t* t_crow,
+                                      int64_t* t_col, void* t_val, int64_t* info, void* scratch,
+                                      int64_t scratch_bytes, int32_t dtype, afsi_stream_t stream) {
+    AFSI_REQUIRE(power_of_two(capacity), "power-of-two hash capacity required");
+    AFSI_REQUIRE(rows > 0 && nf > 0 && rows <= INT64_MAX / nf, "invalid CSR shape");
+    AFSI_REQUIRE(keys && values && crow && col && val && t_crow && t_col && t_val && info && scratch,
+                 "null device pointer");
+    AFSI_REQUIRE(scratch_bytes >= afsi_b200_hash_csr_scratch_bytes(capacity, dtype), "CSR scratch too small");
+    const uint64_t sentinel = uint64_t(rows) * uint64_t(nf);
+    const int end_bit = bit_length(sentinel);
+    const int64_t slab = ((capacity * 8 + 255) / 256) * 256;
+    uint64_t* ka = static_cast<uint64_t*>(scratch);
+    uint64_t* kb = reinterpret_cast<uint64_t*>(static_cast<unsigned char*>(scratch) + slab);
+    void* temp = static_cast<unsigned char*>(scratch) + 2 * slab;
+    size_t temp_bytes = size_t(scratch_bytes - 2 * slab);
+    if (cudaMemsetAsync(info, 0, 2 * sizeof(int64_t), stream) != cudaSuccess)
+        return fail(AFSI_ERR_CUDA, "info clear failed");
+    const unsigned grid = unsigned(capacity / 256 + 1 < 4096 ? capacity / 256 + 1 : 4096);
+    AFSI_DISPATCH(dtype, {
+        table_keys_kernel<T><<<grid, 256, 0, stream>>>(keys, static_cast<const T*>(values), capacity, sentinel, ka,
+                                                       reinterpret_cast<unsigned long long*>(info));
+        int32_t rc = launched("hash_csr keys");
+        if (rc) return rc;
+        if (cub::DeviceRadixSort::SortPairs(temp, temp_bytes, ka, kb, static_cast<const T*>(values),
+                                            static_cast<T*>(val), capacity, 0, end_bit, stream) != cudaSuccess)
+            return fail(AFSI_ERR_CUDA, "CSR key sort failed");
+        row_pointers_kernel<<<grid, 256, 0, stream>>>(kb, capacity, sentinel, uint64_t(nf), rows, crow, col);
+        transpose_keys_kernel<<<grid, 256, 0, stream>>>(kb, capacity, sentinel, uint64_t(nf), uint64_t(rows), ka);
+        if ((rc = launched("hash_csr rows"))) return rc;
+        if (cub::DeviceRadixSort::SortPairs(temp, temp_bytes, ka, kb, static_cast<const T*>(val),
+                                            static_cast<T*>(t_val), capacity, 0, end_bit, stream) != cudaSuccess)
+            return fail(AFSI_ERR_CUDA, "CSR transpose sort failed");
+        row_pointers_kernel<<<grid, 256, 0, stream>>>(kb, capacity, sentinel, uint64_t(rows), nf, t_crow, t_col);
+    });
+    return launched("hash_csr transpose");
+}
+
+extern "C" int32_t afsi_b200_csr_spmv(const int64_t* crow, const int64_t* col, const void* val, int64_t rows,
+                                      int64_t nnz, const void* x, int64_t x_stride, void* y, int64_t y_stride,
+                                      double divisor, int32_t dtype, afsi_stream_t stream) {
+    AFSI_REQUIRE(rows >= 0 && nnz >= 0 && x_stride > 0 && y_stride > 0 && divisor != 0.0, "invalid SpMV arguments");
+    if (rows == 0) return AFSI_OK;
+    AFSI_REQUIRE(crow && y && (nnz == 0 || (col && val && x)), "null device pointer");
+    const int64_t avg = nnz / rows;
+    AFSI_DISPATCH(dtype, {
+        const T* v = static_cast<const T*>(val);
+        const T* xv = static_cast<const T*>(x);
+        T* yv = static_cast<T*>(y);
+        if (avg >= 24) {
+            const int64_t want = (rows * 32 + 255) / 256;
+            const unsigned blocks = unsigned(want < 148 * 64 ? want : 148 * 64);
+            csr_spmv_kernel<T, 32><<<blocks, 256, 0, stream>>>(crow, col, v, rows, xv, x_stride, yv, y_stride,
+                                                               T(divisor));
+        } else if (avg >= 6) {
+            const int64_t want = (rows * 8 + 255) / 256;
+            const unsigned blocks = unsigned(want < 148 * 64 ? want : 148 * 64);
+            csr_spmv_kernel<T, 8><<<blocks, 256, 0, stream>>>(crow, col, v, rows, xv, x_stride, yv, y_stride,
+                                                              T(divisor));
+        } else {
+            const int64_t want = (rows * 4 + 255) / 256;
+            const unsigned blocks = unsigned(want < 148 * 64 ? want : 148 * 64);
+            csr_spmv_kernel<T, 4><<<blocks, 256, 0, stream>>>(crow, col, v, rows, xv, x_stride, yv, y_stride,
+                                                              T(divisor));
+        }
+    });
+    return launched("csr_spmv");
+}

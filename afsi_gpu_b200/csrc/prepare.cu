@@ -155,19 +155,19 @@ struct P2Params {
 // P2 positions + shared tables, mac/csrc/p2_transfer.cu:12-45.  One thread per
 // quadrature point (element-major, q fastest); each axis has its own validity
 // as in the reference, and an invalid axis is binned from scaled=0.
-template <class T>
-__global__ void __launch_bounds__(256) p2_prepare_kernel(const T* __restrict__ x, const int64_t* __restrict__ cells,
+template <class T, int NPC>
+__global__ void __launch_bounds__(256) fe_prepare_kernel(const T* __restrict__ x, const int64_t* __restrict__ cells,
                                                          const T* __restrict__ N, P2Params<T> prm,
                                                          int64_t* __restrict__ base, T* __restrict__ phi,
                                                          int32_t* status) {
     const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (p >= prm.elements * prm.nq) return;
     const int64_t e = p / prm.nq, q = p % prm.nq;
-    int64_t node[10];
+    int64_t node[NPC];
     bool ok = true;
 #pragma unroll
-    for (int a = 0; a < 10; ++a) {
-        node[a] = cells[e * 10 + a];
+    for (int a = 0; a < NPC; ++a) {
+        node[a] = cells[e * NPC + a];
         ok = ok && node[a] >= 0 && node[a] < prm.nodes;
     }
     if (!ok) {
@@ -176,8 +176,8 @@ __global__ void __launch_bounds__(256) p2_prepare_kernel(const T* __restrict__ x
     }
     T pos[3] = {T(0), T(0), T(0)};
 #pragma unroll
-    for (int a = 0; a < 10; ++a) {
-        const T n = N[q * 10 + a];
+    for (int a = 0; a < NPC; ++a) {
+        const T n = N[q * NPC + a];
 #pragma unroll
         for (int d = 0; d < 3; ++d) pos[d] += n * x[node[a] * 3 + d];
     }
@@ -201,14 +201,15 @@ __global__ void __launch_bounds__(256) p2_prepare_kernel(const T* __restrict__ x
     }
 }
 
-// Adaptive quadrature order of each P2 element (mac/adaptive_transfer.py:173-187):
-// ceil(density * D / dx), at least min_order, where D is the diameter of the
-// element's ten Bernstein control points (the four corners and, per edge
-// (i,j) of the tetrahedron, 2 x_mid - (x_i + x_j)/2).  The diameter is the
-// square root of the largest squared pair distance ((dx^2+dy^2)+dz^2); the
+// Adaptive quadrature order of each element (mac/adaptive_transfer.py:167-187):
+// ceil(density * D / dx), at least min_order.  P2 (NPC = 10): D is the
+// diameter of the element's ten Bernstein control points (the four corners
+// and, per edge (i,j) of the tetrahedron, 2 x_mid - (x_i + x_j)/2).  P1
+// (NPC = 4): D is the longest edge, the diameter of the four corners.  D is
+// the square root of the largest squared pair distance ((dx^2+dy^2)+dz^2); the
 // square root is monotone, so this equals the maximum of the pair norms.
-// The launch also counts the elements whose order differs from `last`,
-// the largest order, and a histogram of orders < bins, all into `summary`
+// The launch also counts the elements whose order differs from `last`, the
+// largest order, and a histogram of orders < bins, all into `summary`
 // (changed, max, flags, hist[bins]).  Nonfinite positions set
 // AFSI_FLAG_SUPPORT, node ids outside [0, nodes) AFSI_FLAG_INDEX; those
 // elements get order 0.
@@ -217,8 +218,8 @@ __host__ __device__ constexpr int edge_from(int k) { return k < 3 ? 0 : k < 5 ? 
 __host__ __device__ constexpr int edge_to(int k) { return k < 3 ? k + 1 : k < 5 ? k - 1 : 3; }
 constexpr int kOrderBins = 64;
 
-template <class T>
-__global__ void __launch_bounds__(256) p2_orders_kernel(const T* __restrict__ x, const int64_t* __restrict__ cells,
+template <class T, int NPC>
+__global__ void __launch_bounds__(256) fe_orders_kernel(const T* __restrict__ x, const int64_t* __restrict__ cells,
                                                         int64_t elements, int64_t nodes, T dx, T density,
                                                         int64_t min_order, int64_t* __restrict__ orders,
                                                         const int64_t* __restrict__ last, int32_t* summary,
@@ -231,23 +232,24 @@ __global__ void __launch_bounds__(256) p2_orders_kernel(const T* __restrict__ x,
     bool changed = false;
     int32_t flags = 0;
     if (e < elements) {
-        int64_t node[10];
+        int64_t node[NPC];
         bool ok = true;
 #pragma unroll
-        for (int a = 0; a < 10; ++a) {
-            node[a] = cells[e * 10 + a];
+        for (int a = 0; a < NPC; ++a) {
+            node[a] = cells[e * NPC + a];
             ok = ok && node[a] >= 0 && node[a] < nodes;
         }
         if (!ok) {
             flags |= AFSI_FLAG_INDEX;
         } else {
-            T hull[10][3];
+            constexpr int H = NPC == 10 ? 10 : 4;  // P2: corners + edge controls; P1: corners
+            T hull[H][3];
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) hull[a][d] = x[node[a] * 3 + d];
 #pragma unroll
-            for (int k = 0; k < 6; ++k)
+            for (int k = 0; k < H - 4; ++k)
 #pragma unroll
                 for (int d = 0; d < 3; ++d)
                     hull[4 + k][d] = T(2) * x[node[4 + k] * 3 + d] -
@@ -255,9 +257,9 @@ __global__ void __launch_bounds__(256) p2_orders_kernel(const T* __restrict__ x,
             T best = T(0);
             bool finite = true;
 #pragma unroll
-            for (int a = 0; a < 10; ++a)
+            for (int a = 0; a < H; ++a)
 #pragma unroll
-                for (int b = a + 1; b < 10; ++b) {
+                for (int b = a + 1; b < H; ++b) {
                     const T d0 = hull[a][0] - hull[b][0], d1 = hull[a][1] - hull[b][1], d2 = hull[a][2] - hull[b][2];
                     const T s = (d0 * d0 + d1 * d1) + d2 * d2;
                     finite = finite && isfinite(s);
@@ -349,13 +351,13 @@ extern "C" int32_t afsi_b200_indexed_prepare2d(const void* points, int64_t count
     return launched("indexed_prepare2d");
 }
 
-extern "C" int32_t afsi_b200_p2_prepare(const void* x, int64_t nodes, const int64_t* cells, int64_t elements,
-                                        const void* N, int64_t nq, const double* origin, const double* spacing,
-                                        const double* limits, int64_t* base, void* phi, int64_t total,
-                                        int64_t offset, int32_t* status, int32_t dtype, afsi_stream_t stream) {
-    AFSI_REQUIRE(elements >= 0 && nq > 0 && nodes >= 0, "invalid P2 group sizes");
-    AFSI_REQUIRE(offset >= 0 && offset <= total && elements * nq <= total - offset,
-                 "P2 IB group exceeds table bounds");
+template <int NPC>
+static int32_t fe_prepare(const void* x, int64_t nodes, const int64_t* cells, int64_t elements, const void* N,
+                          int64_t nq, const double* origin, const double* spacing, const double* limits,
+                          int64_t* base, void* phi, int64_t total, int64_t offset, int32_t* status, int32_t dtype,
+                          afsi_stream_t stream) {
+    AFSI_REQUIRE(elements >= 0 && nq > 0 && nodes >= 0, "invalid IB group sizes");
+    AFSI_REQUIRE(offset >= 0 && offset <= total && elements * nq <= total - offset, "IB group exceeds table bounds");
     AFSI_REQUIRE(origin && spacing && limits, "null host parameter array");
     if (elements == 0) return AFSI_OK;
     AFSI_REQUIRE(x && cells && N && base && phi, "null device pointer");
@@ -371,28 +373,60 @@ extern "C" int32_t afsi_b200_p2_prepare(const void* x, int64_t nodes, const int6
         prm.nq = nq;
         prm.total = total;
         prm.offset = offset;
-        p2_prepare_kernel<T><<<blocks_for(elements * nq, 256), 256, 0, stream>>>(
+        fe_prepare_kernel<T, NPC><<<blocks_for(elements * nq, 256), 256, 0, stream>>>(
             static_cast<const T*>(x), cells, static_cast<const T*>(N), prm, base, static_cast<T*>(phi), status);
     });
-    return launched("p2_prepare");
+    return launched(NPC == 10 ? "p2_prepare" : "p1_prepare");
 }
 
-extern "C" int32_t afsi_b200_p2_orders(const void* x, int64_t nodes, const int64_t* cells, int64_t elements,
-                                       double dx, double density, int64_t min_order, int64_t* orders,
-                                       const int64_t* last_orders, int32_t* summary, int32_t bins, int32_t dtype,
-                                       afsi_stream_t stream) {
-    AFSI_REQUIRE(elements >= 0 && nodes >= 0, "invalid P2 element or node count");
+extern "C" int32_t afsi_b200_p2_prepare(const void* x, int64_t nodes, const int64_t* cells, int64_t elements,
+                                        const void* N, int64_t nq, const double* origin, const double* spacing,
+                                        const double* limits, int64_t* base, void* phi, int64_t total,
+                                        int64_t offset, int32_t* status, int32_t dtype, afsi_stream_t stream) {
+    return fe_prepare<10>(x, nodes, cells, elements, N, nq, origin, spacing, limits, base, phi, total, offset, status,
+                          dtype, stream);
+}
+
+extern "C" int32_t afsi_b200_p1_prepare(const void* x, int64_t nodes, const int64_t* cells, int64_t elements,
+                                        const void* N, int64_t nq, const double* origin, const double* spacing,
+                                        const double* limits, int64_t* base, void* phi, int64_t total,
+                                        int64_t offset, int32_t* status, int32_t dtype, afsi_stream_t stream) {
+    return fe_prepare<4>(x, nodes, cells, elements, N, nq, origin, spacing, limits, base, phi, total, offset, status,
+                         dtype, stream);
+}
+
+template <int NPC>
+static int32_t fe_orders(const void* x, int64_t nodes, const int64_t* cells, int64_t elements, double dx,
+                         double density, int64_t min_order, int64_t* orders, const int64_t* last_orders,
+                         int32_t* summary, int32_t bins, int32_t dtype, afsi_stream_t stream) {
+    AFSI_REQUIRE(elements >= 0 && nodes >= 0, "invalid element or node count");
     AFSI_REQUIRE(bins >= 1 && bins <= kOrderBins, "order histogram needs 1..%d bins, got %d", kOrderBins, bins);
-    AFSI_REQUIRE(dx > 0 && density > 0, "P2 orders need a positive spacing and point density");
+    AFSI_REQUIRE(dx > 0 && density > 0, "element orders need a positive spacing and point density");
     AFSI_REQUIRE(summary, "null summary pointer");
     if (cudaMemsetAsync(summary, 0, sizeof(int32_t) * (3 + bins), stream) != cudaSuccess)
         return fail(AFSI_ERR_CUDA, "summary clear failed");
     if (elements == 0) return AFSI_OK;
     AFSI_REQUIRE(x && cells && orders, "null device pointer");
     AFSI_DISPATCH(dtype, {
-        p2_orders_kernel<T><<<blocks_for(elements, 256), 256, 0, stream>>>(
+        fe_orders_kernel<T, NPC><<<blocks_for(elements, 256), 256, 0, stream>>>(
             static_cast<const T*>(x), cells, elements, nodes, T(dx), T(density), min_order, orders, last_orders,
             summary, bins);
     });
-    return launched("p2_orders");
+    return launched(NPC == 10 ? "p2_orders" : "p1_orders");
+}
+
+extern "C" int32_t afsi_b200_p2_orders(const void* x, int64_t nodes, const int64_t* cells, int64_t elements,
+                                       double dx, double density, int64_t min_order, int64_t* orders,
+                                       const int64_t* last_orders, int32_t* summary, int32_t bins, int32_t dtype,
+                                       afsi_stream_t stream) {
+    return fe_orders<10>(x, nodes, cells, elements, dx, density, min_order, orders, last_orders, summary, bins, dtype,
+                         stream);
+}
+
+extern "C" int32_t afsi_b200_p1_orders(const void* x, int64_t nodes, const int64_t* cells, int64_t elements,
+                                       double dx, double density, int64_t min_order, int64_t* orders,
+                                       const int64_t* last_orders, int32_t* summary, int32_t bins, int32_t dtype,
+                                       afsi_stream_t stream) {
+    return fe_orders<4>(x, nodes, cells, elements, dx, density, min_order, orders, last_orders, summary, bins, dtype,
+                        stream);
 }

@@ -259,3 +259,15 @@ def gather2d(velocity, stencil):
     """``TriangleTransfer._gather`` CUDA branch (``mac2d/transfer.py:122-124``)."""
     return torch.cat([indexed_gather(u.reshape(-1, 1), ids, w)
                       for u, ids, w in zip(velocity, stencil.indices, stencil.weights)], -1)
+
+
+def contract(stencil, group, component, offset, low, width, prefix, count, face_shape, workspace, cache=None):
+    """``mac/cuda_ib.py:93-106``: P1 box-site contraction into the hash table."""
+    from .p1_csr import contract as _contract
+    _contract(stencil, group, component, offset, low, width, prefix, count, face_shape, workspace, cache)
+
+
+def hash_accumulate(keys, values, workspace):
+    """``mac/cuda_ib.py:109-112``: insert a (key, value) stream into the table."""
+    from .p1_csr import hash_accumulate as _accumulate
+    _accumulate(keys, values, workspace)

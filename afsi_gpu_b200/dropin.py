@@ -4,7 +4,9 @@
 time:
 
 * ``afsi_torch.mac.cuda_ib.{build, require_cuda, indexed_gather,
-  indexed_spread, compact_gather, compact_spread}`` (``mac/cuda_ib.py:38-90``);
+  indexed_spread, compact_gather, compact_spread, contract,
+  hash_accumulate}`` (``mac/cuda_ib.py:38-112``), which the P1 hash assembly
+  (``mac/hash_transfer_assembly.py:84-99``) imports at call time;
 * ``afsi_torch.mac.p2_cuda_transfer.{prepare, spread, assemble_velocity}``
   (``mac/p2_cuda_transfer.py:18-60``), which ``AdaptiveFETransfer`` imports
   inside its methods;
@@ -14,8 +16,7 @@ time:
   ``mac2d/mg_workspace.py:28-40``); those modules are replaced by shims whose
   ``TritonKernels`` is the B200 kernel object.
 
-Nothing is copied from the reference; the P1 CSR contraction operators are
-left untouched.  ``uninstall()`` restores the originals.
+Nothing is copied from the reference.  ``uninstall()`` restores the originals.
 """
 import sys
 import types
@@ -40,7 +41,8 @@ def install():
     import afsi_torch.mac.cuda_ib as ref_ib
     import afsi_torch.mac.p2_cuda_transfer as ref_p2
     from . import cuda_ib, p2_cuda_transfer
-    for name in ('build', 'require_cuda', 'indexed_gather', 'indexed_spread', 'compact_gather', 'compact_spread'):
+    for name in ('build', 'require_cuda', 'indexed_gather', 'indexed_spread', 'compact_gather', 'compact_spread',
+                 'contract', 'hash_accumulate'):
         _saved.setdefault(('cuda_ib', name), getattr(ref_ib, name))
         setattr(ref_ib, name, getattr(cuda_ib, name))
     for name in ('prepare', 'spread', 'assemble_velocity'):

@@ -1,4 +1,4 @@
-"""Adaptive interaction quadrature for P2 tetrahedra (host-side setup).
+"""Adaptive interaction quadrature for P1 and P2 tetrahedra (host-side setup).
 
 Small reference tables are built on the CPU once per order, as in the
 reference.  The per-element orders, the comparison with the previous rule and
@@ -107,11 +107,15 @@ class RuleBuilder:
     def __init__(self, X, cells, grid, *, point_density=2., max_order=8, max_points=12000000):
         from . import _lib
         _lib.require_cuda(X)
+        if cells.dim() != 2 or cells.shape[1] not in (4, 10):
+            raise ValueError('adaptive interaction rules need P1 (4-node) or P2 (10-node) tetrahedra')
         self.cells = cells
+        self.p2 = cells.shape[1] == 10
         self.grid = grid
         self.density = float(point_density)
         self.max_order, self.max_points = max_order, max_points
         self.bins = max_order + 1
+        self.min_order = 3 if self.p2 else 2   # _orders_p2 / _orders clamps (adaptive_transfer.py:167-187)
         self.determinants = reference_determinants(X, cells)
         self._tables = {}
         self._last = None
@@ -123,7 +127,8 @@ class RuleBuilder:
     def tables(self, order, like):
         if order not in self._tables:
             q, w = conical_rule(order)
-            self._tables[order] = (torch.as_tensor(tabulate_p2(q), dtype=like.dtype, device=like.device),
+            N = tabulate_p2(q) if self.p2 else np.concatenate((1 - q.sum(-1, keepdims=True), q), -1)
+            self._tables[order] = (torch.as_tensor(N, dtype=like.dtype, device=like.device),
                                    torch.as_tensor(w, dtype=like.dtype, device=like.device))
         return self._tables[order]
 
@@ -138,8 +143,9 @@ class RuleBuilder:
         summary = torch.empty(4 + self.bins, dtype=torch.int32, device=x.device)
         summary[-1:].zero_()
         last = None if self._last is None else self._last.orders
-        _lib.call('afsi_b200_p2_orders', _lib.ptr(x), x.shape[0], _lib.ptr(self.cells), E,
-                  float(min(self.grid.spacing)), self.density, 3, _lib.ptr(orders),
+        _lib.call('afsi_b200_p2_orders' if self.p2 else 'afsi_b200_p1_orders', _lib.ptr(x), x.shape[0],
+                  _lib.ptr(self.cells), E, float(min(self.grid.spacing)), self.density, self.min_order,
+                  _lib.ptr(orders),
                   None if last is None else _lib.ptr(last), _lib.ptr(summary), self.bins,
                   _lib.dtype_code(x.dtype), _lib.stream(x.device))
         return orders, summary

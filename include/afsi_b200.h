@@ -110,6 +110,81 @@ int32_t afsi_b200_p2_orders(const void* x, int64_t nodes, const int64_t* cells, 
     double dx, double density, int64_t min_order, int64_t* orders, const int64_t* last_orders,
     int32_t* summary, int32_t bins, int32_t dtype, afsi_stream_t stream);
 
+/* P1 counterparts of afsi_b200_p2_prepare / afsi_b200_p2_orders for 4-node
+ * cells: positions sum N[q,a]*x[cell_a] over the four nodes
+ * (mac/_triton_prepare.py:12-49); orders are ceil(density * longest edge /
+ * dx), callers pass min_order 2 (_orders, mac/adaptive_transfer.py:167-170).
+ * cells (elements,4); N (nq,4).  Same tables, status and summary contracts. */
+int32_t afsi_b200_p1_prepare(const void* x, int64_t nodes, const int64_t* cells, int64_t elements,
+    const void* N, int64_t nq, const double* origin, const double* spacing, const double* limits,
+    int64_t* base, void* phi, int64_t total, int64_t offset, int32_t* status,
+    int32_t dtype, afsi_stream_t stream);
+int32_t afsi_b200_p1_orders(const void* x, int64_t nodes, const int64_t* cells, int64_t elements,
+    double dx, double density, int64_t min_order, int64_t* orders, const int64_t* last_orders,
+    int32_t* summary, int32_t bins, int32_t dtype, afsi_stream_t stream);
+
+/* -------------------------------------------------------------- P1 CSR */
+
+/* Support box of every cell of one quadrature group for component c
+ * (component_plans, mac/hash_transfer_assembly.py:122-138): low (E,3) = min
+ * base, width (E,3) = max - min + 4, prefix (E+1) = exclusive scan of the
+ * box sizes (prefix[E] = the group's site count).  base is the (L,total,3)
+ * table; shared != 0 for the (2,T,3) face/centre layout (axis a of
+ * component c reads lattice a != c), else the (3,T,3) component layout.
+ * scratch: afsi_b200_p1_plan_scratch_bytes(E) device bytes. */
+int64_t afsi_b200_p1_plan_scratch_bytes(int64_t elements);
+int32_t afsi_b200_p1_component_plan(const int64_t* base, int64_t total, int64_t offset, int64_t elements,
+    int64_t nq, int32_t component, int32_t shared, int64_t* low, int64_t* width, int64_t* prefix,
+    void* scratch, int64_t scratch_bytes, afsi_stream_t stream);
+
+/* hash_contract_ (mac/csrc/ib.cpp:58-67, ib.cu:22-116): for each site of
+ * each cell's box, the four nodal sums sum_q W*N[q,a]*phi_x*phi_y*phi_z are
+ * added into the table (keys (capacity) int64, -1 = empty; values
+ * (capacity)) under key node*nf + face.  capacity is a power of two; the
+ * table's hashing and probing are the reference's (SplitMix64 bucket, linear
+ * probe, at most 128 slots), and *flag is set to 1 on a failed probe, a
+ * negative key, a site outside the face array or a malformed plan.  Only
+ * sites < count are visited.  N (nq,4), W (elements,nq), cells (elements,4),
+ * rows offset..offset+elements*nq of the tables. */
+int32_t afsi_b200_hash_contract(const int64_t* base, const void* phi, const void* N, const void* W,
+    const int64_t* cells, const int64_t* low, const int64_t* width, const int64_t* prefix,
+    int64_t* keys, void* values, int32_t* flag, int64_t capacity, int64_t total, int64_t offset,
+    int64_t elements, int64_t nq, int64_t count, int32_t component, int64_t ny, int64_t nz,
+    int64_t nf, int32_t shared, int32_t dtype, afsi_stream_t stream);
+/* cached_contract_ (mac/csrc/ib.cpp:69-81): keys are only looked up; a key
+ * not in the table is appended to the missing stream (missing_count, int64,
+ * counts every miss; entries past missing_capacity are not written). */
+int32_t afsi_b200_cached_contract(const int64_t* base, const void* phi, const void* N, const void* W,
+    const int64_t* cells, const int64_t* low, const int64_t* width, const int64_t* prefix,
+    const int64_t* keys, void* values, int32_t* flag, int64_t capacity, int64_t* missing_keys,
+    void* missing_values, int64_t* missing_count, int64_t missing_capacity, int64_t total,
+    int64_t offset, int64_t elements, int64_t nq, int64_t count, int32_t component, int64_t ny,
+    int64_t nz, int64_t nf, int32_t shared, int32_t dtype, afsi_stream_t stream);
+/* hash_accumulate_ (mac/csrc/ib.cpp:83-92): insert count (key, value) pairs. */
+int32_t afsi_b200_hash_accumulate(const int64_t* input_keys, const void* input_values, int64_t count,
+    int64_t* keys, void* values, int32_t* flag, int64_t capacity, int32_t dtype, afsi_stream_t stream);
+
+/* Table -> CSR of B (rows x nf, key = row*nf + col) and of its transpose
+ * (finish_component, mac/hash_transfer_assembly.py:105-119): crow (rows+1),
+ * col/val (capacity; the first nnz are B's entries, column-sorted rows),
+ * t_crow (nf+1), t_col/t_val (capacity; Bᵀ).  info (device int64[2]):
+ * [0] nnz, [1] 1 if a key lies outside [0, rows*nf) or a value is
+ * nonfinite.  No host synchronisation.  scratch:
+ * afsi_b200_hash_csr_scratch_bytes(capacity, dtype) device bytes. */
+int64_t afsi_b200_hash_csr_scratch_bytes(int64_t capacity, int32_t dtype);
+int32_t afsi_b200_hash_csr(const int64_t* keys, const void* values, int64_t capacity, int64_t rows, int64_t nf,
+    int64_t* crow, int64_t* col, void* val, int64_t* t_crow, int64_t* t_col, void* t_val, int64_t* info,
+    void* scratch, int64_t scratch_bytes, int32_t dtype, afsi_stream_t stream);
+
+/* y[r*y_stride] = (sum_j val[j] * x[col[j]*x_stride]) / divisor for the rows
+ * of a CSR matrix with nnz entries: the responses of the assembled P1
+ * transfer (AssembledP1Transfer.spread/interpolate,
+ * mac/assembled_transfer.py:195-212; torch.sparse.mm there).  Each row is
+ * summed in a fixed order: deterministic. */
+int32_t afsi_b200_csr_spmv(const int64_t* crow, const int64_t* col, const void* val, int64_t rows, int64_t nnz,
+    const void* x, int64_t x_stride, void* y, int64_t y_stride, double divisor, int32_t dtype,
+    afsi_stream_t stream);
+
 /* ----------------------------------------------------------------- transfer */
 
 /* out[p,c] = sum_k field[ids[p,k],c]*w[p,k]   (indexed_gather) */
