@@ -6,6 +6,9 @@ Three boundary conditions:
   ``mac/mg_workspace.py`` (mean-zero gauge, rank-one coarse fix).
 * ``channel2d``: 2D inlet/outlet channel, ``mac2d/multigrid.py`` (Dirichlet
   outlet ghost, no gauge).
+* ``dirichlet3d``: open box with zero pressure on the physical faces,
+  ``mac/dirichlet_mg.py`` and ``mac/open_boundary.py`` (no gauge, odd
+  extension in the prolongation).
 * ``periodic2d``: periodic in x, no-slip (Neumann pressure) in y.  The
   reference has no such solver; this restatement follows the channel V-cycle
   structure (``mac2d/multigrid.py:56-82``) with the Neumann gauge and the
@@ -110,6 +113,63 @@ def restrict2d(fine):
     return ((r00 + r01) + r10 + r11) * fine.dtype.type(.25)
 
 
+def neg_laplacian3d_dirichlet(p, spacing):
+    """``mac/open_boundary.py:14-24``: -div(grad p) with the boundary-face
+    gradient 2p/h (zero pressure half a cell outside), divergence summed over
+    axes in order (``mac/grid.py:70-71``)."""
+    out = None
+    for c, h in enumerate(spacing):
+        t = p.dtype.type(h)
+        first = [slice(None)] * 3
+        last = [slice(None)] * 3
+        first[c] = slice(0, 1)
+        last[c] = slice(-1, None)
+        g = np.concatenate((2 * p[tuple(first)] / t, np.diff(p, axis=c) / t, -2 * p[tuple(last)] / t), c)
+        d = np.diff(g, axis=c) / t
+        out = d if out is None else out + d
+    return -out
+
+
+def diagonal3d_dirichlet(shape, spacing, dtype=np.float64):
+    """``mac/open_boundary.py:47-52``: 2·Σh⁻² plus h⁻² on each boundary face."""
+    diag = np.full(shape, 2 * sum(h ** -2 for h in spacing), dtype=dtype)
+    for c, h in enumerate(spacing):
+        first = [slice(None)] * 3
+        last = [slice(None)] * 3
+        first[c] = slice(0, 1)
+        last[c] = slice(-1, None)
+        diag[tuple(first)] += dtype(h ** -2)
+        diag[tuple(last)] += dtype(h ** -2)
+    return diag
+
+
+def prolong3d_dirichlet(coarse):
+    """Odd extension by one ghost cell per side and axis, trilinear 2x
+    (``align_corners=False``), cropped to the interior
+    (``mac/dirichlet_mg.py:52-62``): fine i reads padded coarse i/2+3/4."""
+    padded = coarse
+    for c in range(3):
+        first = [slice(None)] * 3
+        last = [slice(None)] * 3
+        first[c] = slice(0, 1)
+        last[c] = slice(-1, None)
+        padded = np.concatenate((-padded[tuple(first)], padded, -padded[tuple(last)]), c)
+    def axis(n):
+        i = np.arange(n)
+        src = i / 2 + .75
+        i0 = np.floor(src).astype(np.int64)
+        l1 = src - i0
+        return i0, i0 + 1, 1 - l1, l1
+    dt = coarse.dtype
+    x0, x1, wx0, wx1 = axis(2 * coarse.shape[0])
+    y0, y1, wy0, wy1 = axis(2 * coarse.shape[1])
+    z0, z1, wz0, wz1 = axis(2 * coarse.shape[2])
+    wx0, wx1, wy0, wy1, wz0, wz1 = (w.astype(dt) for w in (wx0, wx1, wy0, wy1, wz0, wz1))
+    cz = padded[:, :, z0] * wz0 + padded[:, :, z1] * wz1
+    cy = cz[:, y0, :] * wy0[:, None] + cz[:, y1, :] * wy1[:, None]
+    return cy[x0] * wx0[:, None, None] + cy[x1] * wx1[:, None, None]
+
+
 def _axis_weights(n_fine, n_coarse):
     """Source index/weights of ``F.interpolate(..., align_corners=False)`` for 2x:
     ``src=max((i+.5)/2-.5,0)``, ``i1=i0+(i0<n-1)``."""
@@ -177,8 +237,11 @@ class Hierarchy:
         while True:
             self.shapes.append(shape)
             self.spacings.append(spacing)
-            self.diagonals.append(diagonal3d(shape, spacing, dtype) if self.dim == 3
-                                  else diagonal2d(shape, spacing, bc, dtype))
+            if bc == 'dirichlet':
+                self.diagonals.append(diagonal3d_dirichlet(shape, spacing, dtype))
+            else:
+                self.diagonals.append(diagonal3d(shape, spacing, dtype) if self.dim == 3
+                                      else diagonal2d(shape, spacing, bc, dtype))
             if min(shape) <= 4 or any(n % 2 for n in shape):
                 break
             shape = tuple(n // 2 for n in shape)
@@ -200,12 +263,16 @@ class Hierarchy:
 
     def apply(self, level, p):
         h = self.spacings[level]
+        if self.bc == 'dirichlet':
+            return neg_laplacian3d_dirichlet(p, h)
         return neg_laplacian3d(p, h) if self.dim == 3 else neg_laplacian2d(p, h, self.bc)
 
     def restrict(self, r):
         return restrict3d(r) if self.dim == 3 else restrict2d(r)
 
     def prolong(self, coarse, shape):
+        if self.bc == 'dirichlet':
+            return prolong3d_dirichlet(coarse)
         return prolong3d(coarse, shape) if self.dim == 3 else prolong2d(coarse, self.bc)
 
 

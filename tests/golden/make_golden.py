@@ -35,6 +35,8 @@ from afsi_torch.mac.adaptive_transfer import AdaptiveP1Transfer  # noqa: E402
 from afsi_torch.mac.assembled_transfer import AssembledP1Transfer  # noqa: E402
 from afsi_torch.mac.hash_transfer_assembly import hash_slot  # noqa: E402
 from afsi_torch.fluid.solvers import SolverOptions  # noqa: E402
+from afsi_torch.mac.dirichlet_mg import DirichletMultigrid  # noqa: E402
+from afsi_torch.mac.open_boundary import negative_laplacian as open_negative_laplacian  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
 torch.set_default_dtype(torch.float64)
@@ -282,6 +284,29 @@ def p1csr():
     save('p1csr', **arrays)
 
 
+def dirichlet():
+    """Open-box (zero face pressure) multigrid: operator, prolongation, one
+    V-cycle and solves of the reference DirichletMultigrid (torch backend)."""
+    g = torch.Generator().manual_seed(13)
+    grid = MACGrid((8, 16, 8), (3., 5., 4.))
+    solver = DirichletMultigrid(grid, backend='torch')
+    xyz = grid.coordinates()
+    exact = torch.sin(.7 * xyz[..., 0]) * torch.cos(.9 * xyz[..., 1]) + .4
+    rhs = open_negative_laplacian(exact, grid.spacing)
+    solution, info = solver.solve(rhs)
+    p = torch.randn(grid.shape, generator=g)
+    r = torch.randn(grid.shape, generator=g)
+    coarse = torch.randn((4, 8, 4), generator=g)
+    grid2 = MACGrid((16, 16, 32), (1., 1., 2.))
+    solver2 = DirichletMultigrid(grid2, backend='torch')
+    rhs2 = torch.randn(grid2.shape, generator=g)
+    solution2, info2 = solver2.solve(rhs2)
+    save('dirichlet', shape=grid.shape, lengths=grid.lengths, exact=exact, rhs=rhs, solution=solution,
+         cycles=info['cycles'], p=p, r=r, apply=open_negative_laplacian(p, grid.spacing),
+         cycle=solver.cycle(0, p, r), coarse=coarse, prolonged=solver.prolong(coarse, grid.shape),
+         shape2=grid2.shape, lengths2=grid2.lengths, rhs2=rhs2, solution2=solution2, cycles2=info2['cycles'])
+
+
 def quadrature():
     arrays = {}
     like = torch.zeros(1)
@@ -302,3 +327,4 @@ if __name__ == '__main__':
     quadrature()
     orders()
     p1csr()
+    dirichlet()

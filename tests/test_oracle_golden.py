@@ -210,3 +210,23 @@ def test_p1_hash_bucket_and_table_semantics():
     small = csr.HashTable(8)
     small.insert(np.arange(20), np.ones(20))
     assert small.flag == 1
+
+
+def test_dirichlet_multigrid_matches_reference():
+    g = golden('dirichlet')
+    shape = tuple(int(n) for n in g['shape'])
+    spacing = tuple(float(L) / n for L, n in zip(g['lengths'], shape))
+    np.testing.assert_allclose(mg.neg_laplacian3d_dirichlet(g['p'], spacing), g['apply'], rtol=1e-14, atol=1e-13)
+    np.testing.assert_allclose(mg.prolong3d_dirichlet(g['coarse']), g['prolonged'], rtol=1e-14, atol=1e-14)
+    h = mg.Hierarchy(shape, spacing, 'dirichlet')
+    assert not h.singular
+    np.testing.assert_allclose(mg.cycle(h, 0, g['p'], g['r'], 4), g['cycle'], rtol=1e-11, atol=1e-12)
+    p, info = mg.solve(h, g['rhs'])
+    assert info['cycles'] == int(g['cycles'])
+    np.testing.assert_allclose(p, g['solution'], rtol=1e-9, atol=1e-10)
+    np.testing.assert_allclose(p, g['exact'], rtol=1e-8, atol=1e-8)
+    shape2 = tuple(int(n) for n in g['shape2'])
+    spacing2 = tuple(float(L) / n for L, n in zip(g['lengths2'], shape2))
+    p2, info2 = mg.solve(mg.Hierarchy(shape2, spacing2, 'dirichlet'), g['rhs2'])
+    assert info2['cycles'] == int(g['cycles2'])
+    np.testing.assert_allclose(p2, g['solution2'], rtol=1e-9, atol=1e-10 * np.abs(g['solution2']).max())
