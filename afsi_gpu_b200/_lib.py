@@ -15,7 +15,7 @@ F32, F64 = 0, 1
 OK, ERR_ARG, ERR_CUDA = 0, 1, 2
 FLAG_SUPPORT, FLAG_INDEX, FLAG_OVERFLOW = 1, 2, 4
 PHI_CLAMPED, PHI_RADICAL = 0, 1
-BC_NEUMANN, BC_CHANNEL, BC_PERIODIC = 0, 1, 2
+BC_NEUMANN, BC_CHANNEL, BC_PERIODIC, BC_DIRICHLET = 0, 1, 2, 3
 MAX_LEVELS = 12
 
 _lock = threading.Lock()

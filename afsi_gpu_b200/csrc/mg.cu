@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(kThreads) restrict_kernel(const T* __restrict_
                                                             Lv<T> L, Lv<T> C) {
     for_my_cells<BC>(C, [&](int cx, int cy, int cz) {
     T v;
-    if (BC == AFSI_BC_NEUMANN) {
+    if (is3d(BC)) {
         const int64_t j = index_of(2 * cx, 2 * cy, 2 * cz, L);
         const int64_t sy = L.nz, sx = int64_t(L.ny) * L.nz;
         v = fine[j];
@@ -215,7 +215,7 @@ struct Geometry {
 // Block over the two fastest axes (z,y in 3D; y,x in 2D), grid z over x (3D).
 template <class T>
 Geometry launch_for(const Lv<T>& L, int bc) {
-    const bool three = bc == AFSI_BC_NEUMANN;
+    const bool three = is3d(bc);
     const int fast = three ? L.nz : L.ny;
     const int mid = three ? L.ny : L.nx;
     const int slow = three ? L.nx : 1;
@@ -265,7 +265,8 @@ Lv<T> coarser(const Lv<T>& L) {
 }
 
 int32_t check_bc(int32_t dim, int32_t bc) {
-    AFSI_REQUIRE((dim == 3 && bc == AFSI_BC_NEUMANN) || (dim == 2 && (bc == AFSI_BC_CHANNEL || bc == AFSI_BC_PERIODIC)),
+    AFSI_REQUIRE((dim == 3 && (bc == AFSI_BC_NEUMANN || bc == AFSI_BC_DIRICHLET)) ||
+                     (dim == 2 && (bc == AFSI_BC_CHANNEL || bc == AFSI_BC_PERIODIC)),
                  "unsupported dim/boundary combination (%d, %d)", dim, bc);
     return AFSI_OK;
 }
@@ -275,6 +276,7 @@ int32_t check_bc(int32_t dim, int32_t bc) {
     case AFSI_BC_NEUMANN: { constexpr int BC = AFSI_BC_NEUMANN; __VA_ARGS__; } break; \
     case AFSI_BC_CHANNEL: { constexpr int BC = AFSI_BC_CHANNEL; __VA_ARGS__; } break; \
     case AFSI_BC_PERIODIC: { constexpr int BC = AFSI_BC_PERIODIC; __VA_ARGS__; } break; \
+    case AFSI_BC_DIRICHLET: { constexpr int BC = AFSI_BC_DIRICHLET; __VA_ARGS__; } break; \
     default: return fail(AFSI_ERR_ARG, "unknown boundary condition %d", (int)(bc)); \
     }
 
@@ -342,7 +344,7 @@ struct Runner {
     T* P(int l) const { return static_cast<T*>(plan->level[l].p); }
     T* Q(int l) const { return static_cast<T*>(plan->level[l].ping); }
     T* R(int l) const { return static_cast<T*>(plan->level[l].rhs); }
-    static constexpr bool singular = BC != AFSI_BC_CHANNEL;
+    static constexpr bool singular = singular_bc(BC);
 
     int32_t coarse(int l, const double* rhs_sum, T** out) {
         CoarseLevels<T> cl;

@@ -11,6 +11,11 @@ constexpr int kThreads = 256;
 constexpr int kCoarseThreads = 1024;
 constexpr int64_t kCoarseCells = 4096;  // levels at or below this size run in one CTA
 
+// 3D levels (z fastest) for the closed and the open box; 2D (y fastest) otherwise.
+__host__ __device__ constexpr bool is3d(int bc) { return bc == AFSI_BC_NEUMANN || bc == AFSI_BC_DIRICHLET; }
+// Singular operators (constants in the null space): mean-zero gauge.
+__host__ __device__ constexpr bool singular_bc(int bc) { return bc == AFSI_BC_NEUMANN || bc == AFSI_BC_PERIODIC; }
+
 template <class T>
 struct Lv {
     int nx, ny, nz;  // cells per axis; nz == 1 in 2D (index x*ny + y)
@@ -28,7 +33,16 @@ struct Site {
 template <int BC, class T>
 __device__ __forceinline__ T diag_at(int x, int y, int z, const Lv<T>& L) {
     T d = T(0);
-    if (BC == AFSI_BC_NEUMANN) {
+    if (BC == AFSI_BC_DIRICHLET) {
+        // mac/open_boundary.py:47-52: 2·Σ h^-2, plus h^-2 on each boundary face
+        d = T(2) * ((L.ih2[0] + L.ih2[1]) + L.ih2[2]);
+        if (x == 0) d += L.ih2[0];
+        if (x == L.nx - 1) d += L.ih2[0];
+        if (y == 0) d += L.ih2[1];
+        if (y == L.ny - 1) d += L.ih2[1];
+        if (z == 0) d += L.ih2[2];
+        if (z == L.nz - 1) d += L.ih2[2];
+    } else if (BC == AFSI_BC_NEUMANN) {
         if (x < L.nx - 1) d += L.ih2[0];
         if (x > 0) d += L.ih2[0];
         if (y < L.ny - 1) d += L.ih2[1];
@@ -60,7 +74,16 @@ template <int BC, bool Exact, class T>
 __device__ __forceinline__ T neg_lap(const T* __restrict__ p, int64_t i, int x, int y, int z, const Lv<T>& L, T m,
                                      T pc) {
     T a = T(0);
-    if (BC == AFSI_BC_NEUMANN) {
+    if (BC == AFSI_BC_DIRICHLET) {
+        // zero pressure half a cell outside: the missing neighbour is the ghost -p
+        const int64_t sx = int64_t(L.ny) * L.nz, sy = L.nz;
+        a = x + 1 < L.nx ? a - scale<Exact>((p[i + sx] - m) - pc, L, 0) : a + scale<Exact>(pc + pc, L, 0);
+        a = x > 0 ? a + scale<Exact>(pc - (p[i - sx] - m), L, 0) : a + scale<Exact>(pc + pc, L, 0);
+        a = y + 1 < L.ny ? a - scale<Exact>((p[i + sy] - m) - pc, L, 1) : a + scale<Exact>(pc + pc, L, 1);
+        a = y > 0 ? a + scale<Exact>(pc - (p[i - sy] - m), L, 1) : a + scale<Exact>(pc + pc, L, 1);
+        a = z + 1 < L.nz ? a - scale<Exact>((p[i + 1] - m) - pc, L, 2) : a + scale<Exact>(pc + pc, L, 2);
+        a = z > 0 ? a + scale<Exact>(pc - (p[i - 1] - m), L, 2) : a + scale<Exact>(pc + pc, L, 2);
+    } else if (BC == AFSI_BC_NEUMANN) {
         const int64_t sx = int64_t(L.ny) * L.nz, sy = L.nz;
         if (x + 1 < L.nx) a = a - scale<Exact>((p[i + sx] - m) - pc, L, 0);
         if (x > 0) a = a + scale<Exact>(pc - (p[i - sx] - m), L, 0);
@@ -98,7 +121,7 @@ template <int BC, class T, class F>
 __device__ __forceinline__ void for_my_cells(const Lv<T>& L, F f) {
     const int fast = blockIdx.x * blockDim.x + threadIdx.x;
     const int mid = blockIdx.y * blockDim.y + threadIdx.y;
-    if (BC == AFSI_BC_NEUMANN) {
+    if (is3d(BC)) {
         if (fast >= L.nz || mid >= L.ny) return;
         for (int x = blockIdx.z; x < L.nx; x += gridDim.z) f(x, mid, fast);
     } else {
@@ -170,7 +193,7 @@ __device__ __forceinline__ void site_finish(const Site& s, double v, double* sqr
 template <int BC, bool Exact, class T>
 __device__ __forceinline__ T restrict_residual_at(const T* __restrict__ p, const T* __restrict__ rhs, int cx, int cy,
                                                   int cz, const Lv<T>& L, T m) {
-    if constexpr (BC == AFSI_BC_NEUMANN) {
+    if constexpr (is3d(BC)) {
         T v = T(0);
 #pragma unroll
         for (int a = 0; a < 2; ++a)
@@ -217,17 +240,25 @@ template <int BC, class T>
 __device__ __forceinline__ T prolong_at(const T* __restrict__ c, int x, int y, int z, const Lv<T>& C, T m) {
     const int ax = x / 2 - 1 + (x & 1), ay = y / 2 - 1 + (y & 1);
     const T wx = (x & 1) ? T(.25) : T(.75), wy = (y & 1) ? T(.25) : T(.75);
-    if (BC == AFSI_BC_NEUMANN) {
+    if (is3d(BC)) {
         const int az = z / 2 - 1 + (z & 1);
         const T wz = (z & 1) ? T(.25) : T(.75);
         const int x0 = ax < 0 ? 0 : ax, x1 = ax + 1 < C.nx - 1 ? ax + 1 : C.nx - 1;
         const int y0 = ay < 0 ? 0 : ay, y1 = ay + 1 < C.ny - 1 ? ay + 1 : C.ny - 1;
         const int z0 = az < 0 ? 0 : az, z1 = az + 1 < C.nz - 1 ? az + 1 : C.nz - 1;
-        auto at = [&](int i, int j, int k) { return c[index_of(i, j, k, C)] - m; };
-        const T c00 = at(x0, y0, z0) * (T(1) - wz) + at(x0, y0, z1) * wz;
-        const T c01 = at(x0, y1, z0) * (T(1) - wz) + at(x0, y1, z1) * wz;
-        const T c10 = at(x1, y0, z0) * (T(1) - wz) + at(x1, y0, z1) * wz;
-        const T c11 = at(x1, y1, z0) * (T(1) - wz) + at(x1, y1, z1) * wz;
+        // ghost one cell outside the coarse grid: the edge value (closed box)
+        // or its negative (open box, odd extension: mac/dirichlet_mg.py:52-62)
+        const bool odd = BC == AFSI_BC_DIRICHLET;
+        const bool gx0 = odd && ax < 0, gx1 = odd && ax + 1 > C.nx - 1, gy0 = odd && ay < 0,
+                   gy1 = odd && ay + 1 > C.ny - 1, gz0 = odd && az < 0, gz1 = odd && az + 1 > C.nz - 1;
+        auto at = [&](int i, int j, int k, bool fi, bool fj, bool fk) {
+            const T v = c[index_of(i, j, k, C)] - m;
+            return (fi != fj) != fk ? -v : v;  // one sign flip per ghost axis
+        };
+        const T c00 = at(x0, y0, z0, gx0, gy0, gz0) * (T(1) - wz) + at(x0, y0, z1, gx0, gy0, gz1) * wz;
+        const T c01 = at(x0, y1, z0, gx0, gy1, gz0) * (T(1) - wz) + at(x0, y1, z1, gx0, gy1, gz1) * wz;
+        const T c10 = at(x1, y0, z0, gx1, gy0, gz0) * (T(1) - wz) + at(x1, y0, z1, gx1, gy0, gz1) * wz;
+        const T c11 = at(x1, y1, z0, gx1, gy1, gz0) * (T(1) - wz) + at(x1, y1, z1, gx1, gy1, gz1) * wz;
         return (c00 * (T(1) - wy) + c01 * wy) * (T(1) - wx) + (c10 * (T(1) - wy) + c11 * wy) * wx;
     }
     const T c00 = coarse_at<BC>(c, ax, ay, C, m), c01 = coarse_at<BC>(c, ax, ay + 1, C, m);
@@ -325,11 +356,12 @@ __device__ void omega_table(const Lv<T>& L, T* table) {
 // (A p)_i of the block path, pc = p_i.
 template <int BC, class T>
 __device__ __forceinline__ T block_apply(const T* __restrict__ p, int i, int x, int y, int z, const Lv<T>& L, T pc) {
-    if (BC == AFSI_BC_NEUMANN) {
+    if (is3d(BC)) {
         const int sx = L.ny * L.nz, sy = L.nz;
-        const T xm = x > 0 ? p[i - sx] : pc, xp = x + 1 < L.nx ? p[i + sx] : pc;
-        const T ym = y > 0 ? p[i - sy] : pc, yp = y + 1 < L.ny ? p[i + sy] : pc;
-        const T zm = z > 0 ? p[i - 1] : pc, zp = z + 1 < L.nz ? p[i + 1] : pc;
+        const T g = BC == AFSI_BC_DIRICHLET ? -pc : pc;  // wall ghost: open box -p, closed box p
+        const T xm = x > 0 ? p[i - sx] : g, xp = x + 1 < L.nx ? p[i + sx] : g;
+        const T ym = y > 0 ? p[i - sy] : g, yp = y + 1 < L.ny ? p[i + sy] : g;
+        const T zm = z > 0 ? p[i - 1] : g, zp = z + 1 < L.nz ? p[i + 1] : g;
         return __fma_rn((pc - xm) + (pc - xp), L.ih2[0],
                         __fma_rn((pc - ym) + (pc - yp), L.ih2[1], ((pc - zm) + (pc - zp)) * L.ih2[2]));
     } else {
@@ -351,7 +383,7 @@ __device__ __forceinline__ T block_apply(const T* __restrict__ p, int i, int x, 
 template <int BC, class T>
 __device__ __forceinline__ T block_restrict(const T* __restrict__ p, const T* __restrict__ rhs, int cx, int cy, int cz,
                                             const Lv<T>& L) {
-    if constexpr (BC == AFSI_BC_NEUMANN) {
+    if constexpr (is3d(BC)) {
         T v = T(0);
 #pragma unroll
         for (int a = 0; a < 2; ++a)
@@ -385,7 +417,7 @@ __device__ __forceinline__ T block_restrict(const T* __restrict__ p, const T* __
 template <int BC, class T>
 __device__ T* block_smooth(T* cur, T* oth, T* R, const Lv<T>& L, const FastCoords<T>& fc, const T* wrd, int smooth,
                            bool zero, T rhs_shift, double (*red)[32], int& rt, T* mean) {
-    constexpr bool singular = BC != AFSI_BC_CHANNEL;
+    constexpr bool singular = singular_bc(BC);
     const int n = int(L.n);
     for (int s = 0; s < smooth; ++s) {
         const bool last = s == smooth - 1;
@@ -430,7 +462,7 @@ __device__ void coarse_cycle(T* smem, const T* __restrict__ rhs_global, const do
                              T* p_out, const TC* __restrict__ cinv, const CoarseLevels<T>& cl, int smooth) {
     __shared__ double red[2][32];
     __shared__ T down_mean[AFSI_MG_MAX_LEVELS];  // pending mean of each level's pre-smoothed iterate
-    constexpr bool singular = BC != AFSI_BC_CHANNEL;
+    constexpr bool singular = singular_bc(BC);
     int rt = 0;
     const int f = cl.first, last = cl.last;
     // layout: [P_f Q_f R_f][P_f+1 ...]...[tables]

@@ -126,7 +126,7 @@ __device__ __forceinline__ void for_cells(const Tiling& t, const Lv<T>& L, F f) 
         const int vx = v % t.gx, r = v / t.gx, vy = r % t.gy, vz = r / t.gy;
         const int fast = (vx << t.bxl) + tx, mid = (vy << t.byl) + ty, slow = (vz << t.bzl) + tz;
         int x, y, z;
-        if (BC == AFSI_BC_NEUMANN) {
+        if (is3d(BC)) {
             z = fast; y = mid; x = slow;
             if (z >= L.nz || y >= L.ny || x >= L.nx) continue;
         } else {
@@ -152,7 +152,7 @@ template <int BC, class T, class TC>
 __global__ void __launch_bounds__(kPThreads, 1) mg_persistent(PersistentArgs<T, TC> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[32];
-    constexpr bool singular = BC != AFSI_BC_CHANNEL;
+    constexpr bool singular = singular_bc(BC);
     const GridSync& gs = a.gs;
     const int fc = a.first_coarse;
     T* down[AFSI_MG_MAX_LEVELS];
@@ -301,7 +301,7 @@ int log2i(int v) {
 
 template <class T>
 Tiling tiling_for(const Lv<T>& L, int bc) {
-    const bool three = bc == AFSI_BC_NEUMANN;
+    const bool three = is3d(bc);
     const int fast = three ? L.nz : L.ny, mid = three ? L.ny : L.nx, slow = three ? L.nx : 1;
     Tiling t;
     t.bxl = std::min(5, log2i(fast));
@@ -393,7 +393,7 @@ int32_t run_persistent(const afsi_mg_plan* plan, int cycles, int solve, int chec
 
 int32_t check(const afsi_mg_plan* plan) {
     AFSI_REQUIRE(plan && plan->levels >= 1 && plan->levels <= AFSI_MG_MAX_LEVELS, "invalid plan");
-    AFSI_REQUIRE((plan->dim == 3 && plan->bc == AFSI_BC_NEUMANN) ||
+    AFSI_REQUIRE((plan->dim == 3 && (plan->bc == AFSI_BC_NEUMANN || plan->bc == AFSI_BC_DIRICHLET)) ||
                      (plan->dim == 2 && (plan->bc == AFSI_BC_CHANNEL || plan->bc == AFSI_BC_PERIODIC)),
                  "unsupported dim/boundary combination");
     AFSI_REQUIRE(plan->smooth >= 1 && plan->coarse_inverse, "invalid plan");
@@ -428,6 +428,7 @@ extern "C" int32_t afsi_b200_mg_persistent(const afsi_mg_plan* plan, int32_t cyc
         AFSI_PERSIST(AFSI_BC_NEUMANN)
         AFSI_PERSIST(AFSI_BC_CHANNEL)
         AFSI_PERSIST(AFSI_BC_PERIODIC)
+        AFSI_PERSIST(AFSI_BC_DIRICHLET)
 #undef AFSI_PERSIST
     default:
         return fail(AFSI_ERR_ARG, "unknown boundary condition");

@@ -47,16 +47,21 @@ def _h2(spacing):
     return [h * h for h in spacing]
 
 
+_BC_CODES = {'neumann': _lib.BC_NEUMANN, 'channel': _lib.BC_CHANNEL, 'periodic': _lib.BC_PERIODIC,
+             'dirichlet': _lib.BC_DIRICHLET}
+
+
 def _ih2(spacing):
     return [1 / h ** 2 for h in spacing]
 
 
 class B200Kernels:
-    """Kernel object for one boundary condition (3D Neumann or a 2D channel)."""
+    """Kernel object for one boundary condition (3D closed or open box, 2D
+    channel or periodic channel)."""
 
     def __init__(self, bc='neumann'):
-        self.bc = {'neumann': _lib.BC_NEUMANN, 'channel': _lib.BC_CHANNEL, 'periodic': _lib.BC_PERIODIC}[bc]
-        self.dim = 3 if bc == 'neumann' else 2
+        self.bc = _BC_CODES[bc]
+        self.dim = 3 if bc in ('neumann', 'dirichlet') else 2
         self.name = 'b200' if bc == 'neumann' else f'b200-{bc}'
 
     def _shape(self, t):
@@ -115,7 +120,8 @@ def _levels(shape, spacing):
 
 def _coarse_matrix(shape, spacing, bc):
     """Dense coarsest operator (float64, CPU): -Δ with the level's BC, plus
-    11ᵀ/n when singular (``mac/multigrid.py:49-59``, ``mac2d/multigrid.py:41-45``)."""
+    11ᵀ/n when singular (``mac/multigrid.py:49-59``, ``mac2d/multigrid.py:41-45``,
+    ``mac/dirichlet_mg.py:30-34``)."""
     n = prod(shape)
     ids = torch.arange(n).reshape(shape)
     A = torch.zeros((n, n), dtype=torch.float64)
@@ -137,6 +143,13 @@ def _coarse_matrix(shape, spacing, bc):
         last = ids[-1].reshape(-1)
         A.index_put_((last, last), torch.full(last.shape, 2 / spacing[0] ** 2, dtype=torch.float64),
                      accumulate=True)
+    elif bc == 'dirichlet':
+        # zero pressure half a cell outside every face (mac/open_boundary.py:14-24)
+        for c, h in enumerate(spacing):
+            for end in (0, -1):
+                face = ids.select(c, end).reshape(-1)
+                A.index_put_((face, face), torch.full(face.shape, 2 / h ** 2, dtype=torch.float64),
+                             accumulate=True)
     else:
         A += 1. / n
     return A
@@ -149,7 +162,7 @@ class _Workspace:
         self.p = [torch.zeros(s, device=device, dtype=dtype) for s in shapes]
         self.ping = [torch.zeros(s, device=device, dtype=dtype) for s in shapes]
         self.rhs = [torch.zeros(s, device=device, dtype=dtype) for s in shapes]
-        bcode = {'neumann': _lib.BC_NEUMANN, 'channel': _lib.BC_CHANNEL, 'periodic': _lib.BC_PERIODIC}[bc]
+        bcode = _BC_CODES[bc]
         plan = _lib.MGPlan()
         plan.dim = len(shapes[0])
         plan.bc = bcode
@@ -206,6 +219,12 @@ class _Workspace:
 
 class _Solver:
     bc = 'neumann'
+    # reference messages (mac/multigrid.py:125-172, mac2d/multigrid.py:85-111)
+    _bad_rhs = 'invalid pressure RHS'
+    _bad_initial = 'invalid initial pressure'
+    _nonfinite_input = 'finite pressure RHS/initial guess required'
+    _nonfinite_residual = 'nonfinite multigrid residual'
+    _not_converged = 'pressure multigrid did not converge'
 
     def __init__(self, grid, *, device='cuda', dtype=torch.float64, options=None, backend='b200-graph',
                  coarse_dtype=None):
@@ -234,7 +253,7 @@ class _Solver:
 
     @property
     def singular(self):
-        return self.bc != 'channel'
+        return self.bc in ('neumann', 'periodic')
 
     # -- execution
     def _capture(self):
@@ -297,7 +316,7 @@ class _Solver:
         cycles = int(cycles)
         _lib.count_replay(cycles // self.options.check_every * self.loop_body_launches)
         if nonfinite:
-            raise RuntimeError('nonfinite multigrid residual')
+            raise RuntimeError(self._nonfinite_residual)
         return cycles, residual
 
     def advance(self, count):
@@ -351,10 +370,10 @@ class _Solver:
         if not isfinite(rtol) or rtol < 0:
             raise ValueError('invalid multigrid solve tolerance')
         if rhs.shape != self.shapes[0] or rhs.device != self.workspace.p[0].device or rhs.dtype != self.dtype:
-            raise ValueError('invalid pressure RHS')
+            raise ValueError(self._bad_rhs)
         if initial is not None and (initial.shape != rhs.shape or initial.device != rhs.device
                                     or initial.dtype != rhs.dtype):
-            raise ValueError('invalid initial pressure')
+            raise ValueError(self._bad_initial)
         w = self.workspace
         m = self._start(rhs, initial)
         n = rhs.numel()
@@ -366,9 +385,11 @@ class _Solver:
             if not m['p_finite']:
                 raise ValueError('invalid initial pressure')
         elif not (m['rhs_finite'] and m['p_finite']):
-            raise ValueError('finite pressure RHS/initial guess required')
+            raise ValueError(self._nonfinite_input)
         rhs_norm, residual = m['rhs_sq'] ** .5, m['residual']
         if not isfinite(rhs_norm) or not isfinite(residual):
+            if self.bc == 'dirichlet':
+                raise ValueError(self._nonfinite_input)
             raise RuntimeError('nonfinite multigrid residual or RHS norm')
         tol = max(self.options.atol, rtol * rhs_norm)
         cycle = 0
@@ -389,15 +410,33 @@ class _Solver:
             cycle += count
             residual = self.residual_norm().item()
             if not isfinite(residual):
-                raise RuntimeError('nonfinite multigrid residual')
+                raise RuntimeError(self._nonfinite_residual)
         if residual > tol:
-            raise RuntimeError(f'pressure multigrid did not converge: {residual:g} > {tol:g}')
+            raise RuntimeError(f'{self._not_converged}: {residual:g} > {tol:g}')
         return w.p[0].clone(), dict(cycles=cycle, residual_norm=residual, tolerance=tol, backend=self.backend)
 
 
 class GeometricMultigrid(_Solver):
     """Closed-box 3D pressure V-cycle solver (``mac/multigrid.py:24-172``)."""
     bc = 'neumann'
+
+
+class DirichletMultigrid(_Solver):
+    """Open-box 3D pressure solver, zero pressure on the physical faces
+    (``mac/dirichlet_mg.py:10-123``): same V-cycle with the face ghost -p, odd
+    extension in the prolongation, no gauge.  ``backend`` also accepts the
+    reference's names ('torch', 'fused', 'workspace' run per-block launches,
+    'graph' the captured solve graph)."""
+    bc = 'dirichlet'
+    _bad_rhs = 'Dirichlet pressure RHS shape/dtype/device mismatch'
+    _bad_initial = 'invalid initial Dirichlet pressure'
+    _nonfinite_input = 'nonfinite Dirichlet pressure input'
+    _nonfinite_residual = 'nonfinite Dirichlet multigrid residual'
+    _not_converged = 'Dirichlet multigrid failed'
+
+    def __init__(self, grid, *, backend='b200-graph', **kwargs):
+        backend = {'torch': 'b200', 'fused': 'b200', 'workspace': 'b200', 'graph': 'b200-graph'}.get(backend, backend)
+        super().__init__(grid, backend=backend, **kwargs)
 
 
 class ChannelMultigrid(_Solver):

@@ -248,6 +248,7 @@ int32_t afsi_b200_node_reduce(const void* local, int64_t slots, const int64_t* c
 #define AFSI_BC_NEUMANN 0  /* closed box (mac/grid.py:86-93), singular, mean-zero gauge */
 #define AFSI_BC_CHANNEL 1  /* 2D inlet/outlet channel (mac2d/grid.py:61-71), p=0 outlet */
 #define AFSI_BC_PERIODIC 2 /* 2D periodic in x, Neumann walls in y, mean-zero gauge */
+#define AFSI_BC_DIRICHLET 3 /* 3D open box, p = 0 on the physical faces (mac/open_boundary.py:14-52) */
 
 /* Elementwise MG kernels on one level (the kernel-object interface of
  * mac/_triton_mg.py:121-151 and mac2d/_triton_mg.py:78-100).

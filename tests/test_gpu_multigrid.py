@@ -11,7 +11,7 @@ from conftest import golden
 from oracle import mg as oracle
 from afsi_gpu_b200 import synthetic
 from afsi_gpu_b200.grid import MACGrid, ChannelGrid
-from afsi_gpu_b200.multigrid import B200Kernels, GeometricMultigrid, ChannelMultigrid, MGOptions
+from afsi_gpu_b200.multigrid import B200Kernels, GeometricMultigrid, ChannelMultigrid, DirichletMultigrid, MGOptions
 
 pytestmark = pytest.mark.gpu
 DEV = 'cuda'
@@ -225,3 +225,52 @@ def test_device_solve_loop_follows_the_host_check_schedule():
     a, ia = ChannelMultigrid(cgrid, backend='b200').solve(crhs)
     b, ib = ChannelMultigrid(cgrid, backend='b200-graph').solve(crhs)
     assert ia['cycles'] == ib['cycles'] and torch.equal(a, b)
+
+
+def test_dirichlet_multigrid_matches_reference_fixture_and_oracle():
+    """Open box, zero face pressure (reference ``mac/dirichlet_mg.py``;
+    ``tests/test_paper_lv.py:74-86``): solves with the reference's cycle count,
+    the manufactured field to 1e-8, one V-cycle 2e-11, level kernels 2e-12."""
+    g = golden('dirichlet')
+    shape = tuple(int(n) for n in g['shape'])
+    grid = MACGrid(shape, tuple(float(x) for x in g['lengths']))
+    for backend in ('b200', 'b200-graph', 'b200-persistent', 'graph'):
+        solver = DirichletMultigrid(grid, backend=backend)
+        p, info = solver.solve(t(g['rhs']))
+        assert info['cycles'] == int(g['cycles'])
+        close(p, g['solution'], 2e-8, 2e-9)
+        close(p, g['exact'], 1e-8, 1e-8)
+        assert info['residual_norm'] <= info['tolerance']
+        saved = p.clone()
+        zero, zinfo = solver.solve(torch.zeros_like(p))
+        assert zinfo['cycles'] == 0 and torch.equal(zero, torch.zeros_like(p))
+        assert torch.equal(p, saved)  # returned solutions are owned copies
+    mg = DirichletMultigrid(grid, backend='b200')
+    mg.initialize(t(g['p']), t(g['r']))
+    close(mg.cycle(), g['cycle'], 2e-11, 2e-11 * np.abs(g['cycle']).max())
+    k = B200Kernels('dirichlet')
+    spacing = grid.spacing
+    out = torch.empty(shape, device=DEV, dtype=torch.float64)
+    k.residual(t(g['p']), t(g['r']), out, spacing)
+    close(out, g['r'] - g['apply'], 2e-12, 2e-12 * np.abs(g['apply']).max())
+    fine = torch.zeros(shape, device=DEV, dtype=torch.float64)
+    k.prolong_add(t(g['coarse']), fine)
+    close(fine, g['prolonged'], 1e-14, 1e-14)
+    h = oracle.Hierarchy(shape, spacing, 'dirichlet')
+    d = torch.empty(shape, device=DEV, dtype=torch.float64)
+    k.smooth(t(g['p']), t(g['r']), t(h.diagonals[0]), d, spacing)
+    ref = g['p'] + (2 / 3) * (g['r'] - g['apply']) / h.diagonals[0]
+    close(d, ref, 2e-12, 2e-12 * np.abs(ref).max())
+    shape2 = tuple(int(n) for n in g['shape2'])
+    grid2 = MACGrid(shape2, tuple(float(x) for x in g['lengths2']))
+    pref, rinfo = oracle.solve(oracle.Hierarchy(shape2, grid2.spacing, 'dirichlet'), g['rhs2'])
+    for backend in ('b200-graph', 'b200-persistent'):
+        p2, info2 = DirichletMultigrid(grid2, backend=backend).solve(t(g['rhs2']))
+        assert info2['cycles'] == rinfo['cycles'] == int(g['cycles2'])
+        close(p2, g['solution2'], 2e-8, 2e-9 * np.abs(g['solution2']).max())
+    with pytest.raises(ValueError, match='nonfinite Dirichlet pressure input'):
+        bad = t(g['rhs']).clone()
+        bad[0, 0, 0] = float('nan')
+        solver.solve(bad)
+    with pytest.raises(ValueError, match='shape/dtype/device mismatch'):
+        solver.solve(t(g['rhs']).float())
