@@ -209,14 +209,41 @@ def cpu_step_time(grid, X, cells, coef, vel, rhs, fraction=0.05):
     W = reference_determinants(torch.as_tensor(X), torch.as_tensor(sub)).numpy()[:, None] * w
     t0 = time.perf_counter()
     base, phi, _ = ib.p2_prepare(X, [(sub, N)], grid.origin, grid.spacing, grid.shape)
-    ib.p2_spread(coef, [(sub, N, W)], base, phi, grid.shape, grid.volume)
-    ib.p2_gather_assemble(vel, [(sub, N, W)], base, phi, grid.shape, X.shape[0])
+    fields = ib.p2_spread(coef, [(sub, N, W)], base, phi, grid.shape, grid.volume)
+    nodal = ib.p2_gather_assemble(vel, [(sub, N, W)], base, phi, grid.shape, X.shape[0])
     t1 = time.perf_counter()
     h = mg.Hierarchy(grid.shape, grid.spacing, 'neumann')
-    mg.solve(h, rhs)
+    p, info = mg.solve(h, rhs)
     t2 = time.perf_counter()
     transfer = (t1 - t0) * (E / Es)
-    return transfer + (t2 - t1), dict(transfer_s=transfer, mg_s=t2 - t1, elements_sampled=Es, elements=E)
+    outputs = dict(sub=sub, N=N, W=W, fields=fields, nodal=nodal, p=p, cycles=info['cycles'])
+    return transfer + (t2 - t1), dict(transfer_s=transfer, mg_s=t2 - t1, elements_sampled=Es, elements=E), outputs
+
+
+def oracle_errors(step, X, coef, vel, outputs, p_device):
+    """Relative errors (max |device - oracle| / max |oracle|) of the step's
+    outputs against the FP64 oracle: spread and gather-assemble on the
+    oracle's element sample (same cells, rule and weights), and the 64^3
+    pressure solve of the timed steps."""
+    from afsi_gpu_b200 import p2_cuda_transfer as p2t
+    from afsi_gpu_b200.quadrature import InteractionRule, QuadratureGroup
+    dev = step.x.device
+    group = QuadratureGroup(torch.as_tensor(outputs['sub'], device=dev),
+                            torch.as_tensor(outputs['N'], device=dev, dtype=torch.float64),
+                            torch.as_tensor(outputs['W'], device=dev, dtype=torch.float64), 4)
+    rule = InteractionRule((group,), None, group.weights.numel())
+    base, phi = p2t.prepare(step.tr, step.x, rule)
+    st = p2t.SharedAdaptiveStencil(base, phi, rule)
+    fields = p2t.spread(step.tr, step.coef, st)
+    nodal = p2t.assemble_velocity(step.tr, step.vel, st)
+
+    def rel(a, b):
+        b = np.asarray(b)
+        return float(np.abs(np.asarray(a).reshape(b.shape) - b).max() / max(np.abs(b).max(), 1e-300))
+    return dict(spread=max(rel(f.cpu().numpy(), o) for f, o in zip(fields, outputs['fields'])),
+                gather_assemble=rel(nodal.cpu().numpy(), outputs['nodal']),
+                mg_solve=rel(p_device, outputs['p']), mg_cycles_oracle=int(outputs['cycles']),
+                sample='spread/gather on the CPU-baseline element sample; MG on the full 64^3 solve')
 
 
 # --------------------------------------------------------------------- main
@@ -250,17 +277,18 @@ def run_reference(args):
     grid, X, cells, coef, vel, rhs = workload()
     cores = 1
     times = []
-    for i in range(args.warmup + args.steps):
-        dt, info = cpu_step_time(grid, X, cells, coef, vel, rhs, fraction=0.02)
-        if i >= args.warmup:
+    warm, timed = min(args.warmup, 1), min(args.steps, 30)  # about 1 s of CPU work per step
+    for i in range(warm + timed):
+        dt, info, _ = cpu_step_time(grid, X, cells, coef, vel, rhs, fraction=0.02)
+        if i >= warm:
             times.append(dt)
     step = float(np.mean(times))
     sample = (f'oracle (NumPy restatement of the reference CPU path): P2 prepare/spread/gather-assemble on '
               f'{info["elements_sampled"]} of {info["elements"]} elements, time scaled by elements; '
-              f'full 64^3 MG solve; {args.steps} steps after {args.warmup} warm-up')
+              f'full 64^3 MG solve; {timed} steps after {warm} warm-up')
     value = 1.0 / step
-    line = dict(metric=METRIC, value=value, unit='steps/s', impl='reference', n_gpus=args.gpus, steps=args.steps,
-                warmup=args.warmup, ms_per_step=step * 1e3, higher_is_better=True, scaling='weak',
+    line = dict(metric=METRIC, value=value, unit='steps/s', impl='reference', n_gpus=args.gpus, steps=timed,
+                warmup=warm, ms_per_step=step * 1e3, higher_is_better=True, scaling='weak',
                 vs_baseline=None, dtype='f64', data='synthetic',
                 config=dict(workload='3D P2 shell 38400 elements / 2457600 points, 64^3 MAC, FP64'),
                 cpu_baseline=dict(value=value, unit='steps/s', cores=cores, kind='port', sample=sample),
@@ -357,11 +385,14 @@ def run_b200(args):
         achieved = ab[byte_key] / dt / 1e9
         traffic = load_traffic().get(dominant)
         cpu = None
+        errors = None
         if not args.no_cpu_baseline:
-            cpu_t, info = cpu_step_time(grid, X, cells, coef, vel, rhs, fraction=0.05)
+            cpu_t, info, outputs = cpu_step_time(grid, X, cells, coef, vel, rhs, fraction=0.05)
             cpu = dict(value=1 / cpu_t, unit='steps/s', cores=1, kind='port',
                        sample=(f'oracle (NumPy restatement) on {info["elements_sampled"]} of {info["elements"]} '
                                f'elements for the transfers (scaled by element count) + full 64^3 MG solve'))
+            errors = oracle_errors(step, X, coef, vel, outputs, outs[-1].numpy())
+        step_ms = np.array([ev[0].elapsed_time(ev[4]) for ev in phases])
         line = dict(
             metric=METRIC, value=world * args.steps / elapsed, unit='steps/s', n_gpus=world, steps=args.steps,
             warmup=args.warmup, ms_per_step=elapsed / args.steps * 1e3, higher_is_better=True, scaling='weak',
@@ -381,6 +412,9 @@ def run_b200(args):
                      d2h_bytes_per_step=int(d2h)),
             gpu_launches=int(launches),
             clocks=clocks.summary(),
+            latency_ms=dict(p50=float(np.percentile(step_ms, 50)), p99=float(np.percentile(step_ms, 99)),
+                            mean=float(step_ms.mean())),
+            oracle_error=errors,
             cpu_baseline=cpu)
         print(json.dumps(line, default=_json))
     if dist:
