@@ -48,6 +48,7 @@ template <int BC, bool Exact, class T>
 __global__ void __launch_bounds__(kThreads) sweep_kernel(const T* __restrict__ p, T* __restrict__ rhs, T* __restrict__ out,
                                                          Lv<T> L, const double* p_sum, const double* rhs_sum,
                                                          Site emit, int fix_rhs, int do_emit) {
+    pdl_enter();
     double local = 0.0;
     const T m = T(site_mean(p_sum, L.n));
     const T mr = T(site_mean(rhs_sum, L.n));
@@ -78,6 +79,7 @@ template <int BC, bool Exact, class T>
 __global__ void __launch_bounds__(kThreads) residual_restrict_kernel(const T* __restrict__ p, const T* __restrict__ rhs,
                                                                      T* __restrict__ coarse, Lv<T> L, Lv<T> C,
                                                                      const double* p_sum, Site emit, int do_emit) {
+    pdl_enter();
     double local = 0.0;
     const T m = T(site_mean(p_sum, L.n));
     for_my_cells<BC>(C, [&](int cx, int cy, int cz) {
@@ -92,6 +94,7 @@ __global__ void __launch_bounds__(kThreads) residual_restrict_kernel(const T* __
 template <int BC, class T>
 __global__ void __launch_bounds__(kThreads) prolong_kernel(const T* src, const T* __restrict__ corr, T* dst, Lv<T> L,
                                                            Lv<T> C, const double* src_sum, const double* corr_sum) {
+    pdl_enter();
     const T ms = T(site_mean(src_sum, L.n)), mc = T(site_mean(corr_sum, C.n));
     for_my_cells<BC>(L, [&](int x, int y, int z) {
         const int64_t i = index_of(x, y, z, L);
@@ -102,6 +105,7 @@ __global__ void __launch_bounds__(kThreads) prolong_kernel(const T* src, const T
 // dst = src - sum/n (or a copy when sum is null); flat grid-stride.
 template <class T>
 __global__ void __launch_bounds__(kThreads) shift_kernel(const T* src, T* dst, int64_t n, const double* sum) {
+    pdl_enter();
     const T m = T(site_mean(sum, n));
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
         dst[i] = src[i] - m;
@@ -110,6 +114,7 @@ __global__ void __launch_bounds__(kThreads) shift_kernel(const T* src, T* dst, i
 template <int BC, bool Exact, class T>
 __global__ void __launch_bounds__(kThreads) residual_kernel(const T* __restrict__ p, const T* __restrict__ rhs,
                                                             T* __restrict__ out, Lv<T> L) {
+    pdl_enter();
     for_my_cells<BC>(L, [&](int x, int y, int z) {
         const int64_t i = index_of(x, y, z, L);
         const T pc = p[i];
@@ -120,6 +125,7 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(const T* __restrict_
 template <int BC, bool Exact, class T>
 __global__ void __launch_bounds__(kThreads) residual_norm_kernel(const T* __restrict__ p, const T* __restrict__ rhs,
                                                                  Lv<T> L, Site s, double* norm_out) {
+    pdl_enter();
     double local = 0.0;
     for_my_cells<BC>(L, [&](int x, int y, int z) {
         const int64_t i = index_of(x, y, z, L);
@@ -133,6 +139,7 @@ __global__ void __launch_bounds__(kThreads) residual_norm_kernel(const T* __rest
 template <int BC, class T>
 __global__ void __launch_bounds__(kThreads) restrict_kernel(const T* __restrict__ fine, T* __restrict__ coarse,
                                                             Lv<T> L, Lv<T> C) {
+    pdl_enter();
     for_my_cells<BC>(C, [&](int cx, int cy, int cz) {
     T v;
     if (is3d(BC)) {
@@ -159,6 +166,7 @@ __global__ void __launch_bounds__(kThreads) restrict_kernel(const T* __restrict_
 template <class T>
 __global__ void __launch_bounds__(kThreads) stats_kernel(const T* __restrict__ x, int64_t n, double* partial,
                                                          unsigned int* counter, double* out) {
+    pdl_enter();
     double s = 0.0, a = 0.0, q = 0.0, bad = 0.0;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
         const double v = double(x[i]);
@@ -197,6 +205,7 @@ template <int BC, class T, class TC>
 __global__ void __launch_bounds__(kCoarseThreads) coarse_kernel(const T* __restrict__ rhs_global, const double* rhs_sum,
                                                                const T* p_global, T* p_out, const TC* __restrict__ cinv,
                                                                CoarseLevels<T> cl, int smooth) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     coarse_cycle<BC, T, TC>(reinterpret_cast<T*>(smem_raw), rhs_global, rhs_sum, p_global, p_out, cinv, cl, smooth);
 }
@@ -206,6 +215,27 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_kernel(const T* __restr
 using namespace afsi;
 
 namespace {
+
+// Launch with programmatic stream serialisation: the kernel may begin
+// launching while its predecessor in the stream runs (both sides call
+// pdl_enter).  Captured graphs keep this as a programmatic edge.
+template <class... Params, class... Args>
+int32_t launch_pdl(const char* what, void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem,
+                   cudaStream_t stream, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    const cudaError_t err = cudaLaunchKernelEx(&cfg, kernel, static_cast<Params>(args)...);
+    if (err != cudaSuccess) return fail(AFSI_ERR_CUDA, "%s: %s", what, cudaGetErrorString(err));
+    return launched(what);
+}
 
 struct Geometry {
     dim3 grid, block;
@@ -359,11 +389,10 @@ struct Runner {
             cudaFuncSetAttribute(coarse_kernel<BC, T, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024);
             configured = true;
         }
-        coarse_kernel<BC, T, TC><<<1, kCoarseThreads, bytes, stream>>>(
-            R(l), rhs_sum, l == 0 ? P(0) : nullptr, P(l), static_cast<const TC*>(plan->coarse_inverse), cl,
-            plan->smooth);
         *out = P(l);
-        return launched("mg coarse block");
+        return launch_pdl("mg coarse block", coarse_kernel<BC, T, TC>, dim3(1), dim3(kCoarseThreads), bytes, stream,
+                          R(l), rhs_sum, l == 0 ? P(0) : nullptr, P(l), static_cast<const TC*>(plan->coarse_inverse),
+                          cl, plan->smooth);
     }
 
     // Returns the buffer holding the level's final iterate and the site whose
@@ -382,31 +411,33 @@ struct Runner {
         for (int s = 0; s < plan->smooth; ++s) {
             const bool first = s == 0;
             const bool last = s == plan->smooth - 1;
-            sweep_kernel<BC, false, T><<<g.grid, g.block, 0, stream>>>(
-                (first && l > 0) ? nullptr : cur, R(l), oth, L, nullptr,
-                (first && l > 0 && singular) ? st.s[l][2].result : nullptr, st.s[l][0],
-                (first && l > 0 && singular) ? 1 : 0, (last && singular) ? 1 : 0);
-            if ((rc = launched("mg sweep"))) return rc;
+            rc = launch_pdl("mg sweep", sweep_kernel<BC, false, T>, g.grid, g.block, 0, stream,
+                            (first && l > 0) ? nullptr : cur, R(l), oth, L, static_cast<const double*>(nullptr),
+                            (first && l > 0 && singular) ? st.s[l][2].result : nullptr, st.s[l][0],
+                            (first && l > 0 && singular) ? 1 : 0, (last && singular) ? 1 : 0);
+            if (rc) return rc;
             T* t = cur; cur = oth; oth = t;
         }
         const double* down_sum = singular ? st.s[l][0].result : nullptr;
         const Lv<T>& C = lv[l + 1];
         const Geometry gc = launch_for(C, BC);
-        residual_restrict_kernel<BC, false, T><<<gc.grid, gc.block, 0, stream>>>(
-            cur, R(l), R(l + 1), L, C, down_sum, st.s[l + 1][2], singular ? 1 : 0);
-        if ((rc = launched("mg residual_restrict"))) return rc;
+        rc = launch_pdl("mg residual_restrict", residual_restrict_kernel<BC, false, T>, gc.grid, gc.block, 0, stream,
+                        cur, R(l), R(l + 1), L, C, down_sum, st.s[l + 1][2], singular ? 1 : 0);
+        if (rc) return rc;
         T* corr;
         const double* corr_sum;
         if ((rc = level(l + 1, &corr, &corr_sum))) return rc;
-        prolong_kernel<BC, T><<<g.grid, g.block, 0, stream>>>(cur, corr, P(l), L, C, down_sum, corr_sum);
-        if ((rc = launched("mg prolong_add"))) return rc;
+        rc = launch_pdl("mg prolong_add", prolong_kernel<BC, T>, g.grid, g.block, 0, stream, cur,
+                        static_cast<const T*>(corr), P(l), L, C, down_sum, corr_sum);
+        if (rc) return rc;
         cur = P(l);
         oth = Q(l);
         for (int s = 0; s < plan->smooth; ++s) {
             const bool last = s == plan->smooth - 1;
-            sweep_kernel<BC, false, T><<<g.grid, g.block, 0, stream>>>(cur, R(l), oth, L, nullptr, nullptr,
-                                                                        st.s[l][1], 0, (last && singular) ? 1 : 0);
-            if ((rc = launched("mg sweep"))) return rc;
+            rc = launch_pdl("mg sweep", sweep_kernel<BC, false, T>, g.grid, g.block, 0, stream, cur, R(l), oth, L,
+                            static_cast<const double*>(nullptr), static_cast<const double*>(nullptr), st.s[l][1], 0,
+                            (last && singular) ? 1 : 0);
+            if (rc) return rc;
             T* t = cur; cur = oth; oth = t;
         }
         *out = cur;
@@ -421,8 +452,9 @@ struct Runner {
             int32_t rc = level(0, &out, &sum);
             if (rc) return rc;
             if (out != P(0) || sum) {
-                shift_kernel<T><<<flat_grid(lv[0].n), kThreads, 0, stream>>>(out, P(0), lv[0].n, sum);
-                if ((rc = launched("mg finalize"))) return rc;
+                rc = launch_pdl("mg finalize", shift_kernel<T>, dim3(flat_grid(lv[0].n)), dim3(kThreads), 0, stream,
+                                static_cast<const T*>(out), P(0), lv[0].n, sum);
+                if (rc) return rc;
             }
         }
         return AFSI_OK;
@@ -506,12 +538,12 @@ extern "C" int32_t afsi_b200_mg_residual_norm(const afsi_mg_plan* plan, double* 
         AFSI_DISPATCH(plan->dtype, {
             Lv<T> L = make_level<T>(plan->level[0].shape, plan->level[0].h2, plan->level[0].inv_h2, plan->dim);
             const Geometry g = launch_for(L, BC);
-            residual_norm_kernel<BC, true, T><<<g.grid, g.block, 0, stream>>>(
-                static_cast<const T*>(plan->level[0].p), static_cast<const T*>(plan->level[0].rhs), L, st.norm,
-                norm_out);
+            return launch_pdl("mg residual_norm", residual_norm_kernel<BC, true, T>, g.grid, g.block, 0, stream,
+                              static_cast<const T*>(plan->level[0].p), static_cast<const T*>(plan->level[0].rhs), L,
+                              st.norm, norm_out);
         });
     });
-    return launched("mg residual_norm");
+    return AFSI_OK;
 }
 
 // ------------------------------------------------------------ solve graph
@@ -532,6 +564,7 @@ namespace {
 
 __global__ void mg_decide_kernel(double* loop, const double* norm, int check_every, int max_cycles,
                                  cudaGraphConditionalHandle handle) {
+    pdl_enter();
     const double cycles = loop[1] + check_every;
     const double r = *norm;
     loop[1] = cycles;
@@ -594,8 +627,8 @@ extern "C" int32_t afsi_b200_mg_solve_graph_create(const afsi_mg_plan* plan, int
     rc = afsi_b200_mg_vcycles(plan, check_every, sg->capture);
     if (!rc) rc = afsi_b200_mg_residual_norm(plan, norm, sg->capture);
     if (!rc) {
-        mg_decide_kernel<<<1, 1, 0, sg->capture>>>(loop, norm, check_every, max_cycles, handle);
-        rc = launched("mg solve decide");
+        rc = launch_pdl("mg solve decide", mg_decide_kernel, dim3(1), dim3(1), 0, sg->capture, loop,
+                        static_cast<const double*>(norm), check_every, max_cycles, handle);
     }
     cudaGraph_t captured = nullptr;
     const cudaError_t end = cudaStreamEndCapture(sg->capture, &captured);
