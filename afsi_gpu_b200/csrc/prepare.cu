@@ -155,49 +155,79 @@ struct P2Params {
 // P2 positions + shared tables, mac/csrc/p2_transfer.cu:12-45.  One thread per
 // quadrature point (element-major, q fastest); each axis has its own validity
 // as in the reference, and an invalid axis is binned from scaled=0.
+template <class T> struct Vec16;
+template <> struct Vec16<double> { using type = double2; static constexpr int n = 2; };
+template <> struct Vec16<float> { using type = float4; static constexpr int n = 4; };
+
+constexpr int kPrepThreads = 128;
+
+// The tables of a block's points are staged in shared memory and written out
+// as two contiguous ranges per lattice (bases: 3 int64 per point, weights: 12
+// values per point) with coalesced stores, instead of 18 scattered stores per
+// point.  A point with a node id out of range flags AFSI_FLAG_INDEX and gets
+// zero tables.
 template <class T, int NPC>
-__global__ void __launch_bounds__(256) fe_prepare_kernel(const T* __restrict__ x, const int64_t* __restrict__ cells,
-                                                         const T* __restrict__ N, P2Params<T> prm,
-                                                         int64_t* __restrict__ base, T* __restrict__ phi,
-                                                         int32_t* status) {
-    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (p >= prm.elements * prm.nq) return;
-    const int64_t e = p / prm.nq, q = p % prm.nq;
-    int64_t node[NPC];
-    bool ok = true;
+__global__ void __launch_bounds__(kPrepThreads) fe_prepare_kernel(const T* __restrict__ x,
+                                                                  const int64_t* __restrict__ cells,
+                                                                  const T* __restrict__ N, P2Params<T> prm,
+                                                                  int64_t* __restrict__ base, T* __restrict__ phi,
+                                                                  int32_t* status) {
+    __shared__ __align__(16) T s_phi[2][kPrepThreads * 12];
+    __shared__ int64_t s_base[2][kPrepThreads * 3];
+    const int64_t first = int64_t(blockIdx.x) * kPrepThreads;
+    const int64_t points = prm.elements * prm.nq;
+    const int n = int(points - first < kPrepThreads ? points - first : kPrepThreads);
+    const int t = threadIdx.x;
+    if (t < n) {
+        const int64_t p = first + t;
+        const int64_t e = p / prm.nq, q = p % prm.nq;
+        int64_t node[NPC];
+        bool ok = true;
 #pragma unroll
-    for (int a = 0; a < NPC; ++a) {
-        node[a] = cells[e * NPC + a];
-        ok = ok && node[a] >= 0 && node[a] < prm.nodes;
-    }
-    if (!ok) {
-        flag(status, AFSI_FLAG_INDEX);
-        return;
-    }
-    T pos[3] = {T(0), T(0), T(0)};
-#pragma unroll
-    for (int a = 0; a < NPC; ++a) {
-        const T n = N[q * NPC + a];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) pos[d] += n * x[node[a] * 3 + d];
-    }
-    const int64_t row0 = prm.offset + p;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const T physical = (pos[a] - prm.origin[a]) / prm.spacing[a];
-        const bool valid = isfinite(physical) && physical >= T(2) && physical < prm.limits[a];
-        if (!valid) flag(status, AFSI_FLAG_SUPPORT);
-#pragma unroll
-        for (int lattice = 0; lattice < 2; ++lattice) {
-            const T start = lattice ? prm.origin[a] + T(.5) * prm.spacing[a] : prm.origin[a];
-            const T scaled = valid ? (pos[a] - start) / prm.spacing[a] : T(0);
-            const int64_t lower = static_cast<int64_t>(floor(scaled - T(1)));
-            T w[4];
-            peskin_radical(scaled - T(lower) - T(1), w);
-            const int64_t row = (lattice * prm.total + row0) * 3 + a;
-            base[row] = lower;
-            store4(phi + row * 4, w);
+        for (int a = 0; a < NPC; ++a) {
+            node[a] = cells[e * NPC + a];
+            ok = ok && node[a] >= 0 && node[a] < prm.nodes;
         }
+        T pos[3] = {T(0), T(0), T(0)};
+        if (ok) {
+#pragma unroll
+            for (int a = 0; a < NPC; ++a) {
+                const T nv = N[q * NPC + a];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) pos[d] += nv * x[node[a] * 3 + d];
+            }
+        } else {
+            flag(status, AFSI_FLAG_INDEX);
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const T physical = (pos[a] - prm.origin[a]) / prm.spacing[a];
+            const bool valid = ok && isfinite(physical) && physical >= T(2) && physical < prm.limits[a];
+            if (ok && !valid) flag(status, AFSI_FLAG_SUPPORT);
+#pragma unroll
+            for (int lattice = 0; lattice < 2; ++lattice) {
+                const T start = lattice ? prm.origin[a] + T(.5) * prm.spacing[a] : prm.origin[a];
+                const T scaled = valid ? (pos[a] - start) / prm.spacing[a] : T(0);
+                const int64_t lower = static_cast<int64_t>(floor(scaled - T(1)));
+                T w[4];
+                peskin_radical(scaled - T(lower) - T(1), w);
+                s_base[lattice][t * 3 + a] = ok ? lower : 0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) s_phi[lattice][(t * 3 + a) * 4 + k] = ok ? w[k] : T(0);
+            }
+        }
+    }
+    __syncthreads();
+    using V = typename Vec16<T>::type;
+    constexpr int per = Vec16<T>::n;
+#pragma unroll
+    for (int lattice = 0; lattice < 2; ++lattice) {
+        const int64_t row = (lattice * prm.total + prm.offset + first) * 3;
+        for (int i = t; i < n * 3; i += kPrepThreads) base[row + i] = s_base[lattice][i];
+        // weights start at row*4 values: a multiple of 12, so 16-byte aligned
+        V* dst = reinterpret_cast<V*>(phi + row * 4);
+        const V* src = reinterpret_cast<const V*>(s_phi[lattice]);
+        for (int i = t; i < n * 12 / per; i += kPrepThreads) dst[i] = src[i];
     }
 }
 
@@ -361,6 +391,7 @@ static int32_t fe_prepare(const void* x, int64_t nodes, const int64_t* cells, in
     AFSI_REQUIRE(origin && spacing && limits, "null host parameter array");
     if (elements == 0) return AFSI_OK;
     AFSI_REQUIRE(x && cells && N && base && phi, "null device pointer");
+    AFSI_REQUIRE(reinterpret_cast<uintptr_t>(phi) % 16 == 0, "IB weight table must be 16-byte aligned");
     AFSI_DISPATCH(dtype, {
         P2Params<T> prm;
         for (int a = 0; a < 3; ++a) {
@@ -373,7 +404,7 @@ static int32_t fe_prepare(const void* x, int64_t nodes, const int64_t* cells, in
         prm.nq = nq;
         prm.total = total;
         prm.offset = offset;
-        fe_prepare_kernel<T, NPC><<<blocks_for(elements * nq, 256), 256, 0, stream>>>(
+        fe_prepare_kernel<T, NPC><<<blocks_for(elements * nq, kPrepThreads), kPrepThreads, 0, stream>>>(
             static_cast<const T*>(x), cells, static_cast<const T*>(N), prm, base, static_cast<T*>(phi), status);
     });
     return launched(NPC == 10 ? "p2_prepare" : "p1_prepare");
