@@ -35,7 +35,7 @@
 //    included, runs inside one thread block in shared memory.
 #include <algorithm>
 #include <atomic>
-#include "mg_ops.cuh"
+#include "mg_cluster.cuh"
 
 namespace afsi {
 
@@ -198,6 +198,18 @@ __global__ void __launch_bounds__(kThreads) stats_kernel(const T* __restrict__ x
             *counter = 0u;
         }
     }
+}
+
+// Levels of one 3D V-cycle from `first` down, in one thread-block cluster
+// (cluster_cycle).
+template <int BC, class T, class TC>
+__global__ void __launch_bounds__(kCoarseThreads) cluster_kernel(const T* __restrict__ rhs_global,
+                                                                const double* rhs_sum, const T* p_global, T* p_out,
+                                                                const TC* __restrict__ cinv, ClusterLevels<T> cl,
+                                                                int smooth) {
+    pdl_enter();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cluster_cycle<BC, T, TC>(reinterpret_cast<T*>(smem_raw), rhs_global, rhs_sum, p_global, p_out, cinv, cl, smooth);
 }
 
 // Levels of one V-cycle from `first` down, in one CTA (coarse_cycle).
@@ -363,6 +375,8 @@ SiteTable sites_for(const afsi_mg_plan* plan) {
     return t;
 }
 
+constexpr int64_t kClusterCells = 512;  // cells per CTA of the first cluster level
+
 template <int BC, class T, class TC>
 struct Runner {
     const afsi_mg_plan* plan;
@@ -370,6 +384,10 @@ struct Runner {
     SiteTable st;
     Lv<T> lv[AFSI_MG_MAX_LEVELS];
     int first_coarse;
+    int first_cluster = AFSI_MG_MAX_LEVELS;  // levels from here run in the cluster kernel (3D)
+    int cluster_size = 0;
+    size_t cluster_bytes = 0;
+    ClusterLevels<T> ccl;
 
     T* P(int l) const { return static_cast<T*>(plan->level[l].p); }
     T* Q(int l) const { return static_cast<T*>(plan->level[l].ping); }
@@ -395,10 +413,120 @@ struct Runner {
                           cl, plan->smooth);
     }
 
+    int32_t cluster(int l, const double* rhs_sum, T** out) {
+        *out = P(l);
+        if constexpr (is3d(BC)) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(cluster_size);
+            cfg.blockDim = dim3(kCoarseThreads);
+            cfg.dynamicSmemBytes = cluster_bytes;
+            cfg.stream = stream;
+            cudaLaunchAttribute attr;
+            attr.id = cudaLaunchAttributeClusterDimension;
+            attr.val.clusterDim.x = cluster_size;
+            attr.val.clusterDim.y = 1;
+            attr.val.clusterDim.z = 1;
+            cfg.attrs = &attr;
+            cfg.numAttrs = 1;
+            const cudaError_t err =
+                cudaLaunchKernelEx(&cfg, cluster_kernel<BC, T, TC>, static_cast<const T*>(R(l)), rhs_sum,
+                                   static_cast<const T*>(l == 0 ? P(0) : nullptr), P(l),
+                                   static_cast<const TC*>(plan->coarse_inverse), ccl, plan->smooth);
+            if (err != cudaSuccess) return fail(AFSI_ERR_CUDA, "mg cluster block: %s", cudaGetErrorString(err));
+            return launched("mg cluster block");
+        } else {
+            return fail(AFSI_ERR_ARG, "cluster path is 3D only");
+        }
+    }
+
+    // Cluster plan for the 3D BCs: the first level whose x extent splits into
+    // 16 slabs of at most kClusterCells cells, distributed while nx is a
+    // multiple of 16 (at least 16), then replicated; used when it starts no
+    // coarser than the single-CTA block and leaves the coarsest level
+    // replicated.  Measured on the B200: a 16-CTA cluster beats the single CTA
+    // on 16^3 -> 4^3 (33 vs 38 us per cycle); with the 32^3 level inside
+    // (2048 cells per CTA) it loses to launched 32^3 kernels, and an 8-CTA
+    // cluster loses to the single CTA.
+    void plan_cluster() {
+        if constexpr (is3d(BC)) {
+            const int C = cluster_capacity();
+            if (C != kClusterMax) return;
+            const int last = plan->levels - 1;
+            for (int l = 0; l < last && l <= first_coarse; ++l) {
+                const Lv<T>& L = lv[l];
+                if (L.nx % C || L.nx < C || L.n / C > kClusterCells) continue;
+                int64_t off = 0;
+                bool distributed = true;
+                for (int k = l; k <= last; ++k) {
+                    ClusterLevel<T>& c = ccl.lv[k];
+                    c.L = lv[k];
+                    distributed = distributed && k < last && lv[k].nx % C == 0 && lv[k].nx >= C;
+                    c.ppc = distributed ? lv[k].nx / C : 0;
+                    c.cells = int(distributed ? lv[k].n / C : lv[k].n);
+                    c.off = int(off);
+                    off += 3 * int64_t(c.cells);
+                }
+                ccl.tables = int(off);
+                const size_t bytes = size_t(off + 64 * (last - l + 1)) * sizeof(T);
+                if (bytes > 200 * 1024) continue;
+                ccl.first = l;
+                ccl.last = last;
+                first_cluster = l;
+                cluster_size = C;
+                cluster_bytes = bytes;
+                return;
+            }
+        }
+    }
+
+    // Largest cluster (16, else 8) that this device runs with 1024-thread
+    // CTAs and 200 KB of shared memory each; 0 if none.  Queried once per
+    // instantiation, on the first (uncaptured) run.
+    static int cluster_capacity() {
+        static int capacity = -1;
+        if constexpr (is3d(BC)) {
+            if (capacity < 0) {
+                capacity = 0;
+                auto kernel = cluster_kernel<BC, T, TC>;
+                cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+                for (int C : {16, 8}) {
+                    if (C > 8 && cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                                     cudaSuccess) {
+                        cudaGetLastError();
+                        continue;
+                    }
+                    cudaLaunchConfig_t cfg = {};
+                    cfg.gridDim = dim3(C);
+                    cfg.blockDim = dim3(kCoarseThreads);
+                    cfg.dynamicSmemBytes = 200 * 1024;
+                    cudaLaunchAttribute attr;
+                    attr.id = cudaLaunchAttributeClusterDimension;
+                    attr.val.clusterDim.x = C;
+                    attr.val.clusterDim.y = 1;
+                    attr.val.clusterDim.z = 1;
+                    cfg.attrs = &attr;
+                    cfg.numAttrs = 1;
+                    int clusters = 0;
+                    if (cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg) == cudaSuccess && clusters > 0) {
+                        capacity = C;
+                        break;
+                    }
+                    cudaGetLastError();
+                }
+            }
+        }
+        return capacity < 0 ? 0 : capacity;
+    }
+
     // Returns the buffer holding the level's final iterate and the site whose
     // sum is its pending mean (nullptr: exact).
     int32_t level(int l, T** out, const double** out_sum) {
         int32_t rc;
+        if (l >= first_cluster) {
+            rc = cluster(l, (l > 0 && singular) ? st.s[l][2].result : nullptr, out);
+            *out_sum = nullptr;
+            return rc;
+        }
         if (l >= first_coarse) {
             rc = coarse(l, (l > 0 && singular) ? st.s[l][2].result : nullptr, out);
             *out_sum = nullptr;
@@ -505,6 +633,7 @@ int32_t run_plan(const afsi_mg_plan* plan, int cycles, cudaStream_t stream) {
             break;
         }
     }
+    r.plan_cluster();
     return r.cycles(cycles);
 }
 
