@@ -22,6 +22,9 @@
 // sums Σ_q N[q,a] W U(x_q) are accumulated in registers and added to the
 // right-hand side (or written per element for the deterministic node
 // reduction).
+// Rules of at most 64 points per element take a spread variant that stages the
+// element's stencil rows in shared memory with asynchronous copies first
+// (p2_spread_rows_kernel).
 // Point forces F = (Σ_a N[q,a] value[a]) * W (mac/compact_transfer.py:29-35)
 // are computed once per point and component by a lanes-over-points pass; the
 // spread contribution is (φx·φy)·φz · (F/volume), one division per point
@@ -283,6 +286,155 @@ __global__ void __launch_bounds__(kWarps * 32, kSpreadBlocks) p2_spread_kernel(
     }
 }
 
+// ------------------------------------------------------- spread, staged rows
+//
+// For rules of at most kRowPoints points per element (the common adaptive
+// orders) the element's stencil rows — both lattices' bases (3 int64 per
+// point) and weights (12 per point), about 15 KB for 64 points in FP64 — are
+// brought into shared memory with asynchronous copies (cp.async) in one go,
+// instead of one chain of dependent global loads per point, and the element's
+// boxes come from the staged bases.  The accumulation is the padded-box,
+// half-warp-per-point scheme of p2_spread_kernel.
+
+constexpr int kRowPoints = 64;
+constexpr int kRowWarps = 2;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+template <class T>
+struct RowStage {
+    T phi[2][kRowPoints * 12];
+    int64_t base[2][kRowPoints * 3];
+    T f[kRowPoints];
+    T coef[32];
+    T copy[2][kSpreadCap];
+};
+
+template <class T>
+__global__ void __launch_bounds__(kRowWarps * 32, 4) p2_spread_rows_kernel(
+    const T* __restrict__ value, const int64_t* __restrict__ cells, const T* __restrict__ N, const T* __restrict__ W,
+    const int64_t* __restrict__ base, const T* __restrict__ phi, T* __restrict__ u0, T* __restrict__ u1,
+    T* __restrict__ u2, P2Dims g, T volume, int32_t* status) {
+    __shared__ __align__(16) RowStage<T> stage_all[kRowWarps];
+    RowStage<T>& s = stage_all[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31, half = lane >> 4, li = (lane >> 2) & 3, lj = lane & 3;
+    const int64_t warps = int64_t(gridDim.x) * kRowWarps;
+    const int n = int(g.nq);
+    for (int64_t e = int64_t(blockIdx.x) * kRowWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
+        const int64_t node = lane < 10 ? cells[e * 10 + lane] : 0;
+        if (__any_sync(0xffffffffu, lane < 10 && (node < 0 || node >= g.nodes))) {
+            if (lane == 0) flag(status, AFSI_FLAG_INDEX);
+            continue;
+        }
+        __syncwarp();
+        const int64_t row0 = g.offset + e * g.nq;
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+            const unsigned char* src = reinterpret_cast<const unsigned char*>(phi + (int64_t(t) * g.total + row0) * 12);
+            for (int i = lane; i < n * 12 * int(sizeof(T)) / 16; i += 32)
+                cp_async16(reinterpret_cast<unsigned char*>(s.phi[t]) + i * 16, src + i * 16);
+            const int64_t* bsrc = base + (int64_t(t) * g.total + row0) * 3;
+            for (int i = lane; i < n * 3; i += 32) cp_async8(&s.base[t][i], bsrc + i);
+        }
+        const int64_t mine = __shfl_sync(0xffffffffu, node, lane < 30 ? lane / 3 : 0);
+        if (lane < 30) s.coef[lane] = value[mine * 3 + lane % 3];
+        cp_async_wait_all();
+        __syncwarp();
+        Box bx;
+        {
+            int mn[3][3], mx[3][3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    mn[c][a] = INT_MAX;
+                    mx[c][a] = INT_MIN;
+                }
+            for (int q = lane; q < n; q += 32) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        const int v = int(s.base[a != c][q * 3 + a]);
+                        mn[c][a] = min(mn[c][a], v);
+                        mx[c][a] = max(mx[c][a], v);
+                    }
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+#pragma unroll
+                    for (int d = 16; d; d >>= 1) {
+                        mn[c][a] = min(mn[c][a], __shfl_xor_sync(0xffffffffu, mn[c][a], d));
+                        mx[c][a] = max(mx[c][a], __shfl_xor_sync(0xffffffffu, mx[c][a], d));
+                    }
+                    bx.lo[c][a] = mn[c][a];
+                    bx.ext[c][a] = mx[c][a] - mn[c][a] + 4;
+                }
+        }
+        T* copy = s.copy[half];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {  // unrolled: the box, tables and field of c stay in registers
+            T* field = c == 0 ? u0 : c == 1 ? u1 : u2;
+            int sx, sy;
+            const bool fits = spread_layout(bx, g, c, sx, sy);
+            const int tx = c != 0, ty = c != 1, tz = c != 2;
+            __syncwarp();
+            if (fits)
+                for (int t = lane; t < 2 * kSpreadCap; t += 32) (&s.copy[0][0])[t] = T(0);
+            for (int q = lane; q < n; q += 32) {  // component c of the forces, lanes over points
+                T F = T(0);
+#pragma unroll
+                for (int a = 0; a < 10; ++a) F += N[q * 10 + a] * s.coef[a * 3 + c];
+                s.f[q] = (F * W[e * g.nq + q]) / volume;
+            }
+            __syncwarp();
+#pragma unroll 4
+            for (int q = half; q < n; q += 2) {
+                const int gx = int(s.base[tx][q * 3]), gy = int(s.base[ty][q * 3 + 1]),
+                          gz = int(s.base[tz][q * 3 + 2]);
+                const T w = s.phi[tx][q * 12 + li] * s.phi[ty][q * 12 + 4 + lj];
+                T wz[4];
+                load_row4(&s.phi[tz][q * 12 + 8], wz);
+                const T fq = s.f[q];
+                if (fits) {
+                    T* dst = copy + (gx - bx.lo[c][0] + li) * sx + (gy - bx.lo[c][1] + lj) * sy + (gz - bx.lo[c][2]);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) dst[k] += (w * wz[k]) * fq;
+                } else if (point_inside(g, c, gx, gy, gz)) {
+                    T* dst = field + face_index(g, c, gx + li, gy + lj, gz);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) atomicAdd(dst + k, (w * wz[k]) * fq);
+                } else if ((lane & 15) == 0) {
+                    flag(status, AFSI_FLAG_INDEX);
+                }
+            }
+            __syncwarp();
+            if (fits) {
+                const int ey = bx.ext[c][1], ez = bx.ext[c][2];
+                const int m = bx.ext[c][0] * ey * ez;
+                for (int t = lane; t < m; t += 32) {
+                    const int z = t % ez, r = t / ez, y = r % ey, x = r / ey;
+                    const int o = x * sx + y * sy + z;
+                    const T v = s.copy[0][o] + s.copy[1][o];
+                    if (v != T(0))
+                        atomicAdd(field + face_index(g, c, bx.lo[c][0] + x, bx.lo[c][1] + y, bx.lo[c][2] + z), v);
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // ------------------------------------------------------------------ gather
 
 template <class T, bool Local>
@@ -408,8 +560,14 @@ template <class T>
 int32_t launch_spread_staged(const T* value, const int64_t* cells, const T* N, const T* W, const int64_t* base,
                              const T* phi, T* u0, T* u1, T* u2, const P2Dims& g, T volume, int32_t* status,
                              int blocks, cudaStream_t stream) {
-    p2_spread_kernel<T><<<blocks, kWarps * 32, 0, stream>>>(value, cells, N, W, base, phi, u0, u1, u2, g, volume,
-                                                            status);
+    if (g.nq <= kRowPoints && reinterpret_cast<uintptr_t>(phi) % 16 == 0) {
+        const int64_t want = (g.elements + kRowWarps - 1) / kRowWarps;
+        p2_spread_rows_kernel<T><<<unsigned(want), kRowWarps * 32, 0, stream>>>(value, cells, N, W, base, phi, u0, u1,
+                                                                              u2, g, volume, status);
+    } else {
+        p2_spread_kernel<T><<<blocks, kWarps * 32, 0, stream>>>(value, cells, N, W, base, phi, u0, u1, u2, g, volume,
+                                                                status);
+    }
     return launched("p2_spread");
 }
 
