@@ -36,6 +36,8 @@ from afsi_torch.mac.assembled_transfer import AssembledP1Transfer  # noqa: E402
 from afsi_torch.mac.hash_transfer_assembly import hash_slot  # noqa: E402
 from afsi_torch.fluid.solvers import SolverOptions  # noqa: E402
 from afsi_torch.mac.dirichlet_mg import DirichletMultigrid  # noqa: E402
+from afsi_torch.mac.transfer import FETransfer  # noqa: E402
+from afsi_torch.mac.mass_solver import MassSolver  # noqa: E402
 from afsi_torch.mac.open_boundary import negative_laplacian as open_negative_laplacian  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
@@ -307,6 +309,32 @@ def dirichlet():
          shape2=grid2.shape, lengths2=grid2.lengths, rhs2=rhs2, solution2=solution2, cycles2=info2['cycles'])
 
 
+def mass():
+    """Consistent FE mass matrix of a P2 block mesh (FETransfer) and Jacobi-PCG
+    solves by the reference MassSolver: default schedule, warm start, and a
+    schedule with frequent checks and restarts."""
+    g = torch.Generator().manual_seed(14)
+    X1, c1 = kuhn_block(3, 2, 2, 1., (2., 2., 2.), seed=14)
+    X, cells = promote_p1(X1, c1)
+    geometry = prepare_p2(X, cells)
+    tr = FETransfer(MACGrid((12, 12, 12), (10., 10., 10.)), geometry)
+    mass = tr.mass
+    n = X.shape[0]
+    rhs = torch.randn((n, 3), generator=g)
+    initial = torch.randn((n, 3), generator=g) * .1
+    default = SolverOptions(rtol=1e-12, atol=1e-13, max_iterations=500, check_every=4)
+    busy = SolverOptions(rtol=1e-12, atol=1e-13, max_iterations=500, check_every=1, recompute_every=5)
+    out = dict(crow=mass.crow_indices(), col=mass.col_indices(), values=mass.values(),
+               diagonal=tr.diagonal[:, 0].contiguous(), rhs=rhs, initial=initial)
+    for name, opts, init in (('default', default, None), ('warm', default, initial), ('busy', busy, None)):
+        x, info = MassSolver(mass, tr.diagonal, opts).solve(rhs, init)
+        out[f'{name}_x'] = x
+        out[f'{name}_iterations'] = info.iterations
+        out[f'{name}_residual'] = info.residual_norm
+        out[f'{name}_tolerance'] = info.tolerance
+    save('mass', **out)
+
+
 def quadrature():
     arrays = {}
     like = torch.zeros(1)
@@ -328,3 +356,4 @@ if __name__ == '__main__':
     orders()
     p1csr()
     dirichlet()
+    mass()

@@ -230,3 +230,15 @@ def test_dirichlet_multigrid_matches_reference():
     p2, info2 = mg.solve(mg.Hierarchy(shape2, spacing2, 'dirichlet'), g['rhs2'])
     assert info2['cycles'] == int(g['cycles2'])
     np.testing.assert_allclose(p2, g['solution2'], rtol=1e-9, atol=1e-10 * np.abs(g['solution2']).max())
+
+
+def test_mass_pcg_matches_reference_solves():
+    from oracle import pcg
+    g = golden('mass')
+    opts = dict(default=dict(check_every=4), warm=dict(check_every=4), busy=dict(check_every=1, recompute_every=5))
+    for name, kw in opts.items():
+        x, it, res, tol = pcg.solve(g['crow'], g['col'], g['values'], g['diagonal'], g['rhs'],
+                                    g['initial'] if name == 'warm' else None, **kw)
+        assert it == int(g[f'{name}_iterations'])
+        assert res <= tol and abs(tol - float(g[f'{name}_tolerance'])) <= 1e-12 * tol
+        np.testing.assert_allclose(x, g[f'{name}_x'], rtol=1e-10, atol=1e-12 * np.abs(g[f'{name}_x']).max())
