@@ -37,6 +37,15 @@ class MGPlan(ctypes.Structure):
                 ('coarse_inverse', c_void_p), ('scratch', c_void_p)]
 
 
+class PCGPlan(ctypes.Structure):
+    _fields_ = [('crow', c_void_p), ('col', c_void_p), ('col32', c_void_p), ('val', c_void_p),
+                ('diagonal', c_void_p), ('rhs', c_void_p), ('initial', c_void_p), ('x', c_void_p), ('r', c_void_p),
+                ('d', c_void_p), ('Ad', c_void_p), ('state', c_void_p), ('scratch', c_void_p), ('rows', c_int64),
+                ('cols', c_int32), ('dtype', c_int32), ('max_iterations', c_int32), ('check_every', c_int32),
+                ('recompute_every', c_int32), ('diagonal_per_row', c_int32), ('rtol', ctypes.c_double),
+                ('atol', ctypes.c_double)]
+
+
 # name -> argtypes (restype int32 unless listed in _RESTYPES)
 _SIGNATURES = {
     'afsi_b200_last_error': [],
@@ -108,10 +117,17 @@ _SIGNATURES = {
                                 c_void_p],
     'afsi_b200_vector_stats': [c_void_p, c_int64, c_void_p, c_void_p, c_int32, c_void_p],
     'afsi_b200_subtract_mean': [c_void_p, c_int64, c_void_p, c_int32, c_void_p],
+    'afsi_b200_pcg_scratch_bytes': [],
+    'afsi_b200_pcg_begin': [ctypes.POINTER(PCGPlan), c_void_p],
+    'afsi_b200_pcg_iterations': [ctypes.POINTER(PCGPlan), c_int32, c_void_p],
+    'afsi_b200_pcg_graph_create': [ctypes.POINTER(PCGPlan), ctypes.POINTER(c_void_p)],
+    'afsi_b200_pcg_graph_launch': [c_void_p, c_void_p],
+    'afsi_b200_pcg_graph_destroy': [c_void_p],
 }
 _RESTYPES = {'afsi_b200_last_error': ctypes.c_char_p, 'afsi_b200_mg_scratch_bytes': ctypes.c_int64,
              'afsi_b200_launch_count': ctypes.c_int64, 'afsi_b200_mg_sync_bytes': ctypes.c_int64,
-             'afsi_b200_p1_plan_scratch_bytes': ctypes.c_int64, 'afsi_b200_hash_csr_scratch_bytes': ctypes.c_int64}
+             'afsi_b200_p1_plan_scratch_bytes': ctypes.c_int64, 'afsi_b200_hash_csr_scratch_bytes': ctypes.c_int64,
+             'afsi_b200_pcg_scratch_bytes': ctypes.c_int64}
 
 
 def exported_symbols():

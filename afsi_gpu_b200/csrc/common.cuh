@@ -81,6 +81,38 @@ __device__ __forceinline__ double sum_partials(const double* partial, int count,
     return block_sum(v, shared);
 }
 
+// Programmatic dependent launch (sm_90+): let the next kernel in the stream
+// begin launching now, then wait until every kernel this one depends on has
+// completed and its writes are visible.  The next kernel is launched only
+// after every block of this one has started, so waiting blocks never hold back
+// a kernel they depend on.  Both are no-ops for a launch without the
+// programmatic-serialization attribute.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+// Launch with programmatic stream serialisation: the kernel may begin
+// launching while its predecessor in the stream runs (both sides call
+// pdl_enter).  Captured graphs keep this as a programmatic edge.
+template <class... Params, class... Args>
+int32_t launch_pdl(const char* what, void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem,
+                   cudaStream_t stream, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    const cudaError_t err = cudaLaunchKernelEx(&cfg, kernel, static_cast<Params>(args)...);
+    if (err != cudaSuccess) return fail(AFSI_ERR_CUDA, "%s: %s", what, cudaGetErrorString(err));
+    return launched(what);
+}
+
 }  // namespace afsi
 
 #define AFSI_DISPATCH(dtype, ...)                                              \

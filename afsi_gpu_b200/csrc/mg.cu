@@ -228,27 +228,6 @@ using namespace afsi;
 
 namespace {
 
-// Launch with programmatic stream serialisation: the kernel may begin
-// launching while its predecessor in the stream runs (both sides call
-// pdl_enter).  Captured graphs keep this as a programmatic edge.
-template <class... Params, class... Args>
-int32_t launch_pdl(const char* what, void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem,
-                   cudaStream_t stream, Args... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = stream;
-    cudaLaunchAttribute attr;
-    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr.val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = &attr;
-    cfg.numAttrs = 1;
-    const cudaError_t err = cudaLaunchKernelEx(&cfg, kernel, static_cast<Params>(args)...);
-    if (err != cudaSuccess) return fail(AFSI_ERR_CUDA, "%s: %s", what, cudaGetErrorString(err));
-    return launched(what);
-}
-
 struct Geometry {
     dim3 grid, block;
     int64_t blocks;

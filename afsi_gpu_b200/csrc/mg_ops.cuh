@@ -16,17 +16,6 @@ __host__ __device__ constexpr bool is3d(int bc) { return bc == AFSI_BC_NEUMANN |
 // Singular operators (constants in the null space): mean-zero gauge.
 __host__ __device__ constexpr bool singular_bc(int bc) { return bc == AFSI_BC_NEUMANN || bc == AFSI_BC_PERIODIC; }
 
-// Programmatic dependent launch (sm_90+): let the next kernel in the stream
-// begin launching now, then wait until every kernel this one depends on has
-// completed and its writes are visible.  The next kernel is launched only
-// after every block of this one has started, so waiting blocks never hold back
-// a kernel they depend on.  Both are no-ops for a launch without the
-// programmatic-serialization attribute.
-__device__ __forceinline__ void pdl_enter() {
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-}
-
 template <class T>
 struct Lv {
     int nx, ny, nz;  // cells per axis; nz == 1 in 2D (index x*ny + y)

@@ -14,7 +14,12 @@ time:
   ``ChannelWorkspace`` import ``TritonKernels`` from ``mac._triton_mg`` /
   ``mac2d._triton_mg`` when they are built (``mac/mg_workspace.py:36-47``,
   ``mac2d/mg_workspace.py:28-40``); those modules are replaced by shims whose
-  ``TritonKernels`` is the B200 kernel object.
+  ``TritonKernels`` is the B200 kernel object;
+* the consistent-mass solvers: ``MassSolver`` as bound in
+  ``mac.compact_transfer`` and ``mac2d.transfer`` (imported there at module
+  load, ``mac/compact_transfer.py:7``, ``mac2d/transfer.py:10-11``),
+  ``GraphMassSolver`` in ``mac.mass_graph`` (imported at call time,
+  ``mac/compact_transfer.py:89``) and in ``mac2d.transfer``.
 
 Nothing is copied from the reference.  ``uninstall()`` restores the originals.
 """
@@ -48,6 +53,15 @@ def install():
     for name in ('prepare', 'spread', 'assemble_velocity'):
         _saved.setdefault(('p2', name), getattr(ref_p2, name))
         setattr(ref_p2, name, getattr(p2_cuda_transfer, name))
+    import importlib
+    from . import mass
+    for module, name in (('afsi_torch.mac.compact_transfer', 'MassSolver'),
+                         ('afsi_torch.mac.mass_graph', 'GraphMassSolver'),
+                         ('afsi_torch.mac2d.transfer', 'MassSolver'),
+                         ('afsi_torch.mac2d.transfer', 'GraphMassSolver')):
+        target = importlib.import_module(module)
+        _saved.setdefault(('attr', module, name), getattr(target, name))
+        setattr(target, name, getattr(mass, name))
     for module, bc in (('afsi_torch.mac._triton_mg', 'neumann'), ('afsi_torch.mac2d._triton_mg', 'channel')):
         _saved.setdefault(('module', module), sys.modules.get(module))
         sys.modules[module] = _shim(module, bc)
@@ -59,7 +73,12 @@ def install():
 def uninstall():
     import afsi_torch.mac.cuda_ib as ref_ib
     import afsi_torch.mac.p2_cuda_transfer as ref_p2
-    for (kind, name), value in list(_saved.items()):
+    import importlib
+    for key, value in list(_saved.items()):
+        if key[0] == 'attr':
+            setattr(importlib.import_module(key[1]), key[2], value)
+            continue
+        kind, name = key
         if kind == 'cuda_ib':
             setattr(ref_ib, name, value)
         elif kind == 'p2':

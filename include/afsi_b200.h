@@ -352,6 +352,68 @@ int32_t afsi_b200_vector_stats(const void* x, int64_t n, double* stats_out, void
 int32_t afsi_b200_subtract_mean(void* x, int64_t n, const double* stats, int32_t dtype,
     afsi_stream_t stream);
 
+/* ---- consistent-mass Jacobi-PCG ------------------------------------------
+ * Replaces MassSolver.solve / GraphMassSolver.solve (mac/mass_solver.py:39-103,
+ * mac/mass_graph.py:129-225): M x = rhs for a (rows, cols) block, M a CSR
+ * matrix, z = r/diag, one recurrence for all columns, the reference's
+ * breakdown guard, restart, check schedule and true-residual acceptance.  The
+ * checks run on the device; the caller reads `state` (device double
+ * [AFSI_PCG_STATE_SLOTS]) once when the solve has stopped. */
+#define AFSI_PCG_STATE_SLOTS 16
+#define AFSI_PCG_RESIDUAL 4    /* ||r|| of the recurrence after the latest iteration */
+#define AFSI_PCG_TOLERANCE 5   /* max(atol, rtol ||rhs||) */
+#define AFSI_PCG_BROKEN 7      /* 1 once the breakdown guard fired */
+#define AFSI_PCG_TRUE_NORM 9   /* ||rhs - M x|| of the latest true residual */
+#define AFSI_PCG_ITERATIONS 10
+#define AFSI_PCG_STATUS 11
+#define AFSI_PCG_RHS_NORM 12
+
+#define AFSI_PCG_RUNNING 0
+#define AFSI_PCG_CONVERGED 1      /* true residual <= tolerance */
+#define AFSI_PCG_BAD_INPUT 2      /* rhs or initial not finite */
+#define AFSI_PCG_BREAKDOWN 3      /* guard fired, seen at a check */
+#define AFSI_PCG_NONFINITE 4      /* nonfinite true residual */
+#define AFSI_PCG_NOT_CONVERGED 5  /* max_iterations reached */
+
+typedef struct afsi_pcg_plan {
+    const int64_t* crow;  /* [rows+1] */
+    const int64_t* col;   /* [nnz] int64 column indices, or NULL when col32 is given */
+    const int32_t* col32; /* [nnz] int32 column indices (rows < 2^31), or NULL */
+    const void* val;      /* [nnz] */
+    const void* diagonal; /* Jacobi diagonal: [rows] when diagonal_per_row, else [rows*cols] */
+    const void* rhs;      /* [rows*cols] */
+    const void* initial;  /* [rows*cols] initial guess (zeros for none) */
+    void* x;              /* [rows*cols] solution */
+    void* r;              /* [rows*cols] workspace */
+    void* d;
+    void* Ad;
+    double* state;        /* [AFSI_PCG_STATE_SLOTS] */
+    void* scratch;        /* afsi_b200_pcg_scratch_bytes(), zero-initialised once */
+    int64_t rows;
+    int32_t cols;         /* 1, 2 or 3 */
+    int32_t dtype;        /* AFSI_F32 or AFSI_F64, every array but crow/col/state */
+    int32_t max_iterations;
+    int32_t check_every;
+    int32_t recompute_every;
+    int32_t diagonal_per_row; /* 1: one diagonal value per row, shared by its columns */
+    double rtol;
+    double atol;
+} afsi_pcg_plan;
+
+int64_t afsi_b200_pcg_scratch_bytes(void);
+/* x = initial, ||rhs||, tolerance, finiteness, then r = rhs - M x and the
+ * first direction; stops (CONVERGED) when the initial guess already meets the
+ * tolerance. */
+int32_t afsi_b200_pcg_begin(const afsi_pcg_plan* plan, afsi_stream_t stream);
+/* `count` iterations (each: Ad = M d and the step, then the check or the
+ * direction update); no-ops once the status left RUNNING. */
+int32_t afsi_b200_pcg_iterations(const afsi_pcg_plan* plan, int32_t count, afsi_stream_t stream);
+/* The iteration loop as one CUDA graph (a WHILE node over one iteration);
+ * launch it after afsi_b200_pcg_begin on the same stream. */
+int32_t afsi_b200_pcg_graph_create(const afsi_pcg_plan* plan, void** graph_out);
+int32_t afsi_b200_pcg_graph_launch(void* graph, afsi_stream_t stream);
+int32_t afsi_b200_pcg_graph_destroy(void* graph);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,10 +17,15 @@ class PCGError(RuntimeError):
 
 
 def csr_mm(crow, col, val, v):
-    out = np.zeros((len(crow) - 1,) + v.shape[1:], dtype=np.result_type(val, v))
-    for r in range(len(crow) - 1):
-        s, e = crow[r], crow[r + 1]
-        out[r] = val[s:e] @ v[col[s:e]]
+    """M v for a CSR matrix (rows summed in column order, empty rows zero)."""
+    rows = len(crow) - 1
+    out = np.zeros((rows,) + v.shape[1:], dtype=np.result_type(val, v))
+    if len(col) == 0:
+        return out
+    shape = (-1,) + (1,) * (v.ndim - 1)
+    prod = np.asarray(val).reshape(shape) * v[col]
+    filled = crow[1:] > crow[:-1]
+    out[filled] = np.add.reduceat(prod, crow[:-1][filled], axis=0)
     return out
 
 

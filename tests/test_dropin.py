@@ -34,6 +34,14 @@ def test_install_rebinds_ib_operators_and_mg_kernels(afsi_torch):
         assert isinstance(k, B200Kernels) and k.dim == 3
         from afsi_torch.mac2d._triton_mg import TritonKernels as Channel
         assert Channel().dim == 2
+        import afsi_torch.mac.compact_transfer as ref_compact
+        import afsi_torch.mac.mass_graph as ref_graph
+        import afsi_torch.mac2d.transfer as ref_2d
+        from afsi_gpu_b200 import mass
+        assert ref_compact.MassSolver is mass.MassSolver and ref_graph.GraphMassSolver is mass.GraphMassSolver
+        assert ref_2d.MassSolver is mass.MassSolver and ref_2d.GraphMassSolver is mass.GraphMassSolver
     finally:
         dropin.uninstall()
     assert ref_ib.compact_gather is original
+    import afsi_torch.mac.mass_solver as ref_mass
+    assert ref_compact.MassSolver is ref_mass.MassSolver and ref_2d.MassSolver is ref_mass.MassSolver
