@@ -178,6 +178,56 @@ def mg_bytes_per_cycle(shapes, smooth=4, s=8):
     return sum(np.prod(sh) * s * (6 * smooth + 10.25) for sh in shapes[:-1])
 
 
+def mass_pcg_row(X, cells, device, peak_gbs, solves=20):
+    """Consistent-mass Jacobi-PCG (the solve inside every reference FE
+    spread/interpolate, mac/transfer.py:105-140) on the P2 mass matrix of the
+    bench mesh: its CSR pattern (every node pair of each element) does not
+    depend on the quadrature rule, so the rule here is the degree-4 Keast
+    rule.  The transfer's options (rtol 1e-12, atol 1e-13, check_every 4).
+
+    Bytes per iteration: the SpMV reads the matrix (int32 column + value per
+    entry, int64 row pointers), gathers d once and writes Ad; the update reads
+    x, d, r, Ad and the per-row diagonal and writes x, r; the direction reads
+    r, diagonal, d and writes d."""
+    from afsi_gpu_b200.mass import MassSolver, SolverOptions
+    from afsi_gpu_b200.quadrature import keast5, tabulate_p2, reference_determinants
+    q, w = keast5()
+    N = torch.as_tensor(tabulate_p2(q), device=device)
+    W = reference_determinants(torch.as_tensor(X), torch.as_tensor(cells)).to(device)[:, None] * \
+        torch.as_tensor(w, device=device)
+    c = torch.as_tensor(cells, device=device)
+    local = torch.einsum('eq,qa,qb->eab', W, N, N)
+    rows = X.shape[0]
+    ij = torch.stack((c[:, :, None].expand_as(local).reshape(-1), c[:, None, :].expand_as(local).reshape(-1)))
+    M = torch.sparse_coo_tensor(ij, local.reshape(-1), (rows, rows)).coalesce().to_sparse_csr()
+    diag = torch.zeros(rows, device=device, dtype=torch.float64).index_add(
+        0, c.reshape(-1), local.diagonal(dim1=-2, dim2=-1).reshape(-1))
+    solver = MassSolver(M, diag[:, None].expand(-1, 3),
+                        SolverOptions(rtol=1e-12, atol=1e-13, max_iterations=500, check_every=4))
+    g = torch.Generator(device=device).manual_seed(21)
+    rhs = torch.randn((rows, 3), device=device, dtype=torch.float64, generator=g)
+    for _ in range(3):
+        x, info = solver.solve(rhs)
+    stream = torch.cuda.current_stream(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(device)
+    e0.record(stream)
+    for _ in range(solves):
+        x, info = solver.solve(rhs)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    ms = e0.elapsed_time(e1) / solves
+    nnz = M.values().numel()
+    vec = rows * 3 * 8
+    per_it = nnz * 12 + (rows + 1) * 8 + 2 * vec + (7 * vec + rows * 8) + (4 * vec + rows * 8)
+    us_it = ms * 1e3 / max(info.iterations, 1)
+    gbs = per_it / (us_it * 1e-6) / 1e9
+    return dict(rows=rows, nnz=int(nnz), iterations=info.iterations, ms_per_solve=ms, us_per_iteration=us_it,
+                bytes_per_iteration=int(per_it), achieved_gbs=gbs, frac=gbs / peak_gbs,
+                residual=info.residual_norm, tolerance=info.tolerance,
+                note='one begin launch + one WHILE-loop graph launch per solve, one host read')
+
+
 def load_traffic():
     path = ROOT / 'profiles' / 'traffic.json'
     try:
@@ -392,6 +442,7 @@ def run_b200(args):
                        sample=(f'oracle (NumPy restatement) on {info["elements_sampled"]} of {info["elements"]} '
                                f'elements for the transfers (scaled by element count) + full 64^3 MG solve'))
             errors = oracle_errors(step, X, coef, vel, outputs, outs[-1].numpy())
+        mass = mass_pcg_row(X, cells, device, pk['hbm_gbs'])
         step_ms = np.array([ev[0].elapsed_time(ev[4]) for ev in phases])
         line = dict(
             metric=METRIC, value=world * args.steps / elapsed, unit='steps/s', n_gpus=world, steps=args.steps,
@@ -415,6 +466,7 @@ def run_b200(args):
             latency_ms=dict(p50=float(np.percentile(step_ms, 50)), p99=float(np.percentile(step_ms, 99)),
                             mean=float(step_ms.mean())),
             oracle_error=errors,
+            mass_pcg=mass,
             cpu_baseline=cpu)
         print(json.dumps(line, default=_json))
     if dist:
