@@ -117,6 +117,10 @@ _SIGNATURES = {
                                 c_void_p],
     'afsi_b200_vector_stats': [c_void_p, c_int64, c_void_p, c_void_p, c_int32, c_void_p],
     'afsi_b200_subtract_mean': [c_void_p, c_int64, c_void_p, c_int32, c_void_p],
+    'afsi_b200_mg_refine_scratch_bytes': [P_I64, c_int32, c_int32],
+    'afsi_b200_mg_refine_residual': [c_void_p, c_void_p, c_void_p, P_I64, P_F64, c_int32, c_int32, c_void_p, c_void_p,
+                                     c_void_p],
+    'afsi_b200_mg_refine_correct': [c_void_p, c_void_p, c_int64, c_void_p],
     'afsi_b200_pcg_scratch_bytes': [],
     'afsi_b200_pcg_begin': [ctypes.POINTER(PCGPlan), c_void_p],
     'afsi_b200_pcg_iterations': [ctypes.POINTER(PCGPlan), c_int32, c_void_p],
@@ -127,7 +131,7 @@ _SIGNATURES = {
 _RESTYPES = {'afsi_b200_last_error': ctypes.c_char_p, 'afsi_b200_mg_scratch_bytes': ctypes.c_int64,
              'afsi_b200_launch_count': ctypes.c_int64, 'afsi_b200_mg_sync_bytes': ctypes.c_int64,
              'afsi_b200_p1_plan_scratch_bytes': ctypes.c_int64, 'afsi_b200_hash_csr_scratch_bytes': ctypes.c_int64,
-             'afsi_b200_pcg_scratch_bytes': ctypes.c_int64}
+             'afsi_b200_pcg_scratch_bytes': ctypes.c_int64, 'afsi_b200_mg_refine_scratch_bytes': ctypes.c_int64}
 
 
 def exported_symbols():

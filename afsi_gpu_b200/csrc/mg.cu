@@ -222,6 +222,33 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_kernel(const T* __restr
     coarse_cycle<BC, T, TC>(reinterpret_cast<T*>(smem_raw), rhs_global, rhs_sum, p_global, p_out, cinv, cl, smooth);
 }
 
+// Iterative refinement (precision form): the residual of the FP64 iterate in
+// FP64, handed to the FP32 V-cycles as float, with the norm of the FP64
+// residual; then the FP32 correction added to the FP64 iterate.
+template <int BC>
+__global__ void __launch_bounds__(kThreads) refine_residual_kernel(const double* __restrict__ p,
+                                                                   const double* __restrict__ rhs,
+                                                                   float* __restrict__ out, Lv<double> L, Site s,
+                                                                   double* norm_out) {
+    pdl_enter();
+    double local = 0.0;
+    for_my_cells<BC>(L, [&](int x, int y, int z) {
+        const int64_t i = index_of(x, y, z, L);
+        const double pc = p[i];
+        const double r = rhs[i] - neg_lap<BC, true>(p, i, x, y, z, L, 0.0, pc);
+        out[i] = float(r);
+        local += r * r;
+    });
+    site_finish(s, local, norm_out);
+}
+
+__global__ void __launch_bounds__(kThreads) refine_correct_kernel(double* __restrict__ p, const float* __restrict__ e,
+                                                                  int64_t n) {
+    pdl_enter();
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        p[i] = p[i] + double(e[i]);
+}
+
 }  // namespace afsi
 
 using namespace afsi;
@@ -785,6 +812,41 @@ extern "C" int32_t afsi_b200_subtract_mean(void* x, int64_t n, const double* sta
                                                                stats);
     });
     return launched("subtract_mean");
+}
+
+// ---- iterative refinement (precision form) ----
+
+extern "C" int64_t afsi_b200_mg_refine_scratch_bytes(const int64_t* shape, int32_t dim, int32_t bc) {
+    if (check_bc(dim, bc) || check_shape(shape, dim)) return -1;
+    const double one[3] = {1, 1, 1};
+    const Geometry g = launch_for(make_level<double>(shape, one, one, dim), bc);
+    return g.blocks * 8 + 64;
+}
+
+extern "C" int32_t afsi_b200_mg_refine_residual(const double* p, const double* rhs, float* r32, const int64_t* shape,
+                                                const double* h2, int32_t dim, int32_t bc, double* norm_out,
+                                                void* scratch, afsi_stream_t stream) {
+    int32_t rc = check_bc(dim, bc);
+    if (rc || (rc = check_shape(shape, dim))) return rc;
+    AFSI_REQUIRE(p && rhs && r32 && h2 && norm_out && scratch, "null argument");
+    AFSI_REQUIRE(reinterpret_cast<uintptr_t>(scratch) % 16 == 0, "refinement scratch must be 16-byte aligned");
+    const double one[3] = {1, 1, 1};
+    Lv<double> L = make_level<double>(shape, h2, one, dim);
+    const Geometry g = launch_for(L, bc);
+    unsigned char* b = static_cast<unsigned char*>(scratch);
+    const Site site{reinterpret_cast<double*>(b), reinterpret_cast<unsigned int*>(b + g.blocks * 8 + 8),
+                    reinterpret_cast<double*>(b + g.blocks * 8)};
+    AFSI_BC_DISPATCH(bc, {
+        return launch_pdl("mg refine residual", refine_residual_kernel<BC>, g.grid, g.block, 0, stream, p, rhs, r32,
+                          L, site, norm_out);
+    });
+    return AFSI_OK;
+}
+
+extern "C" int32_t afsi_b200_mg_refine_correct(double* p, const float* e, int64_t n, afsi_stream_t stream) {
+    AFSI_REQUIRE(p && e && n > 0, "invalid refinement correction arguments");
+    return launch_pdl("mg refine correct", refine_correct_kernel, dim3(flat_grid(n)), dim3(kThreads), 0, stream, p,
+                      e, n);
 }
 
 // ---- standalone kernel-object entry points (exact arithmetic) ----

@@ -446,3 +446,132 @@ class ChannelMultigrid(_Solver):
     def __init__(self, grid, **kwargs):
         self.bc = 'periodic' if getattr(grid, 'periodic', False) else 'channel'
         super().__init__(grid, **kwargs)
+
+
+class RefinedMultigrid:
+    """Precision form of the pressure solve: FP32 V-cycles inside FP64
+    iterative refinement.
+
+    No counterpart in the reference, whose solvers are FP64 throughout
+    (``mac/multigrid.py:125-172``).  The iterate, the right-hand side, every
+    residual and the dense coarsest solve stay FP64; each refinement forms the
+    FP64 residual r = rhs - A p (``afsi_b200_mg_refine_residual``, the
+    reference operator), hands it to FP32 V-cycles as float, runs them until
+    the FP32 residual falls by ``inner_rtol`` (the device-side solve loop of
+    the FP32 solver) and adds the correction to p in FP64
+    (``afsi_b200_mg_refine_correct``).  It stops when the FP64 residual meets
+    ``max(atol, rtol ||rhs||)``, the FP64 solver's tolerance; the method differs
+    from the FP64 solver's (another cycle count), so results agree at the solve
+    tolerance, not bitwise.  Singular problems (Neumann, periodic) keep the
+    mean-zero gauge: the right-hand side and initial guess are shifted as in the
+    FP64 solver, each FP32 residual is shifted before its V-cycles, and the
+    final iterate is shifted once more in FP64.
+    """
+
+    def __init__(self, grid, *, bc=None, device='cuda', options=None, inner_rtol=1e-5, inner_cycles=40,
+                 max_refinements=8, backend='b200-graph'):
+        self.options = MGOptions() if options is None else options
+        if not 0 < inner_rtol < 1 or max_refinements < 1:
+            raise ValueError('refinement needs 0 < inner_rtol < 1 and max_refinements >= 1')
+        kind = bc or ('periodic' if getattr(grid, 'periodic', False) else
+                      'channel' if len(grid.shape) == 2 else 'neumann')
+        cls = {'neumann': GeometricMultigrid, 'dirichlet': DirichletMultigrid, 'channel': ChannelMultigrid,
+               'periodic': ChannelMultigrid}[kind]
+        inner_opts = MGOptions(rtol=inner_rtol, atol=0., max_cycles=inner_cycles, smooth=self.options.smooth,
+                               check_every=self.options.check_every)
+        self.inner = cls(grid, device=device, dtype=torch.float32, coarse_dtype=torch.float64, options=inner_opts,
+                         backend=backend)
+        self.bc = self.inner.bc
+        self.inner_rtol = inner_rtol
+        self.max_refinements = max_refinements
+        w = self.inner.workspace
+        self.shape = tuple(self.inner.shapes[0])
+        dev = w.p[0].device
+        self.p = torch.zeros(self.shape, device=dev, dtype=torch.float64)
+        self.rhs = torch.zeros_like(self.p)
+        self.stats = torch.zeros(8, device=dev, dtype=torch.float64)
+        self.norm = torch.zeros(1, device=dev, dtype=torch.float64)
+        self._shape = _lib.int64s(self.shape)
+        h = self.inner.spacings[0]
+        self._h2 = _lib.doubles([x * x for x in h])
+        self._dim = len(self.shape)
+        nbytes = _lib.load().afsi_b200_mg_refine_scratch_bytes(self._shape, self._dim, _BC_CODES[self.bc])
+        if nbytes < 0:
+            raise ValueError('grid not supported by the refinement kernels')
+        self.scratch = torch.zeros(int(nbytes), device=dev, dtype=torch.uint8)
+        self.backend = self.inner.backend + '-refined'
+
+    @property
+    def singular(self):
+        return self.bc in ('neumann', 'periodic')
+
+    def _residual(self):
+        """FP64 residual of self.p into the FP32 solver's rhs; its norm (one host read)."""
+        w = self.inner.workspace
+        call('afsi_b200_mg_refine_residual', ptr(self.p), ptr(self.rhs), ptr(w.rhs[0]), self._shape, self._h2,
+             self._dim, _BC_CODES[self.bc], ptr(self.norm), ptr(self.scratch), stream(self.p.device))
+        return self.norm.item()
+
+    def _inner_solve(self, norm):
+        """FP32 V-cycles on the residual from a zero start; returns the cycles run."""
+        inner, w = self.inner, self.inner.workspace
+        if self.singular:
+            w.vector_stats(w.rhs[0], w.stats[0:4])
+            w.subtract_mean(w.rhs[0], w.stats[0:4])
+        w.p[0].zero_()
+        tol = self.inner_rtol * norm
+        if getattr(inner, 'loop_graph', None):
+            cycles, residual = inner._run_loop(tol)
+        else:
+            cycles, residual = 0, float('inf')
+            while residual > tol and cycles + inner.options.check_every <= inner.options.max_cycles:
+                inner.advance(inner.options.check_every)
+                cycles += inner.options.check_every
+                residual = inner.residual_norm().item()
+        if not isfinite(residual):
+            raise RuntimeError('nonfinite multigrid residual in the FP32 correction')
+        call('afsi_b200_mg_refine_correct', ptr(self.p), ptr(w.p[0]), self.p.numel(), stream(self.p.device))
+        return cycles
+
+    @torch.no_grad()
+    def solve(self, rhs, initial=None, *, rtol=None):
+        rtol = self.options.rtol if rtol is None else rtol
+        if not isfinite(rtol) or rtol < 0:
+            raise ValueError('invalid multigrid solve tolerance')
+        if rhs.shape != self.shape or rhs.dtype != torch.float64 or rhs.device != self.p.device:
+            raise ValueError('refined pressure solve needs an FP64 right-hand side on the solver device')
+        if initial is not None and (initial.shape != self.shape or initial.dtype != torch.float64
+                                    or initial.device != self.p.device):
+            raise ValueError('invalid initial pressure')
+        w = self.inner.workspace
+        self.rhs.copy_(rhs)
+        self.p.zero_() if initial is None else self.p.copy_(initial)
+        w.vector_stats(self.rhs, self.stats[0:4])
+        w.vector_stats(self.p, self.stats[4:8])
+        raw = self.stats.tolist()
+        n = rhs.numel()
+        if not (raw[3] and raw[7]):
+            raise ValueError('finite pressure RHS/initial guess required')
+        if self.singular:
+            if abs(raw[0] / n) > 1e-12 + 1e-10 * (raw[1] / n):
+                raise ValueError('incompatible Neumann pressure RHS: net flux must vanish')
+            w.subtract_mean(self.rhs, self.stats[0:4])
+            w.subtract_mean(self.p, self.stats[4:8])
+            w.vector_stats(self.rhs, self.stats[0:4])
+        rhs_norm = self.stats[2].item() ** .5
+        tol = max(self.options.atol, rtol * rhs_norm)
+        cycles = refinements = 0
+        residual = self._residual()
+        while residual > tol and refinements < self.max_refinements and isfinite(residual):
+            cycles += self._inner_solve(residual)
+            refinements += 1
+            residual = self._residual()
+        if not isfinite(residual):
+            raise RuntimeError('nonfinite multigrid residual')
+        if residual > tol:
+            raise RuntimeError(f'refined pressure multigrid did not converge: {residual:g} > {tol:g}')
+        if self.singular:
+            w.vector_stats(self.p, self.stats[4:8])
+            w.subtract_mean(self.p, self.stats[4:8])
+        return self.p.clone(), dict(cycles=cycles, refinements=refinements, residual_norm=residual, tolerance=tol,
+                                    backend=self.backend)

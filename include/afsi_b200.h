@@ -344,6 +344,20 @@ int32_t afsi_b200_mg_residual_norm(const afsi_mg_plan* plan, double* norm_out, a
 int32_t afsi_b200_mg_residual_norm_noalloc(const void* p, const void* rhs, const int64_t* shape,
     const double* h2, int32_t dim, int32_t bc, double* norm_out, int32_t dtype, afsi_stream_t stream);
 
+/* Iterative refinement of an FP64 pressure solve by FP32 V-cycles (the
+ * precision form; no counterpart in the reference, whose solver is FP64
+ * throughout, mac/multigrid.py:125-172).
+ * afsi_b200_mg_refine_residual: r32 = float(rhs - A p) with the residual
+ * formed in FP64 by the reference's operator (mac/grid.py:86-93), and
+ * norm_out (device double) = ||rhs - A p||_2 of the FP64 residual
+ * (deterministic).  scratch: afsi_b200_mg_refine_scratch_bytes() device bytes,
+ * 16-byte aligned, zero-initialised once (-1 for an invalid shape).
+ * afsi_b200_mg_refine_correct: p += double(e) over n cells. */
+int64_t afsi_b200_mg_refine_scratch_bytes(const int64_t* shape, int32_t dim, int32_t bc);
+int32_t afsi_b200_mg_refine_residual(const double* p, const double* rhs, float* r32, const int64_t* shape,
+    const double* h2, int32_t dim, int32_t bc, double* norm_out, void* scratch, afsi_stream_t stream);
+int32_t afsi_b200_mg_refine_correct(double* p, const float* e, int64_t n, afsi_stream_t stream);
+
 /* stats_out (device double[4]) = {sum(x), sum(|x|), sum(x^2), all finite ? 1 : 0}
  * over n values (deterministic order). */
 int32_t afsi_b200_vector_stats(const void* x, int64_t n, double* stats_out, void* scratch,

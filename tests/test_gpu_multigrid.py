@@ -11,7 +11,8 @@ from conftest import golden
 from oracle import mg as oracle
 from afsi_gpu_b200 import synthetic
 from afsi_gpu_b200.grid import MACGrid, ChannelGrid
-from afsi_gpu_b200.multigrid import B200Kernels, GeometricMultigrid, ChannelMultigrid, DirichletMultigrid, MGOptions
+from afsi_gpu_b200.multigrid import (B200Kernels, GeometricMultigrid, ChannelMultigrid, DirichletMultigrid,
+                                     MGOptions, RefinedMultigrid)
 
 pytestmark = pytest.mark.gpu
 DEV = 'cuda'
@@ -274,3 +275,60 @@ def test_dirichlet_multigrid_matches_reference_fixture_and_oracle():
         solver.solve(bad)
     with pytest.raises(ValueError, match='shape/dtype/device mismatch'):
         solver.solve(t(g['rhs']).float())
+
+
+def _fp64_residual(solver_cls, grid, p, rhs, **kw):
+    """||rhs - A p|| by the FP64 solver's own residual kernel."""
+    mg = solver_cls(grid, backend='b200', **kw)
+    mg.initialize(p, rhs)
+    return mg.residual_norm().item()
+
+
+@pytest.mark.parametrize('case', ['neumann64', 'channel', 'periodic', 'dirichlet'])
+def test_refined_fp32_multigrid_reaches_fp64_tolerance(case):
+    """Precision form: FP32 V-cycles inside FP64 iterative refinement meet the
+    FP64 solver's tolerance (1e-10 relative) measured in FP64, and the
+    solution agrees with the FP64 oracle at the solve tolerance (2e-8, the
+    solve bar of the reference's tests)."""
+    if case == 'neumann64':
+        grid, bc, cls = MACGrid((64, 64, 64), (1., 1., 1.)), 'neumann', GeometricMultigrid
+        rhs = synthetic.mean_free_normal(grid.shape, seed=8).numpy()
+    elif case == 'dirichlet':
+        grid, bc, cls = MACGrid((32, 32, 32), (1., 1., 1.)), 'dirichlet', DirichletMultigrid
+        rhs = np.random.default_rng(9).standard_normal(grid.shape)
+    else:
+        grid = ChannelGrid((256, 64), (1., .25), periodic=case == 'periodic')
+        bc, cls = case, ChannelMultigrid
+        rhs = np.random.default_rng(10).standard_normal(grid.shape)
+        if case == 'periodic':
+            rhs -= rhs.mean()
+    refined = RefinedMultigrid(grid, bc=bc)
+    p, info = refined.solve(t(rhs))
+    assert p.dtype == torch.float64
+    assert info['refinements'] >= 1 and info['residual_norm'] <= info['tolerance']
+    rhs_shifted = rhs - rhs.mean() if bc in ('neumann', 'periodic') else rhs
+    assert abs(info['tolerance'] - max(1e-12, 1e-10 * np.linalg.norm(rhs_shifted))) <= 1e-12 * info['tolerance']
+    assert _fp64_residual(cls, grid, p, t(rhs_shifted)) <= info['tolerance'] * (1 + 1e-6)
+    pref, _ = oracle.solve(oracle.Hierarchy(grid.shape, grid.spacing, bc), rhs)
+    close(p, pref, 2e-8, 2e-8 * np.abs(pref).max())
+    if bc in ('neumann', 'periodic'):
+        assert abs(p.mean().item()) <= 1e-14 * p.abs().max().item()
+    # a second solve with the first as the initial guess needs no refinement
+    _, again = refined.solve(t(rhs), p)
+    assert again['refinements'] == 0
+
+
+def test_refined_multigrid_rejects_bad_input():
+    grid = MACGrid((32, 32, 32), (1., 1., 1.))
+    refined = RefinedMultigrid(grid)
+    rhs = synthetic.mean_free_normal(grid.shape, seed=1).to(DEV)
+    with pytest.raises(ValueError, match='FP64'):
+        refined.solve(rhs.float())
+    with pytest.raises(ValueError, match='incompatible Neumann'):
+        refined.solve(rhs + 1.0)
+    bad = rhs.clone()
+    bad[0, 0, 0] = float('nan')
+    with pytest.raises(ValueError, match='finite'):
+        refined.solve(bad)
+    p, info = refined.solve(rhs)
+    assert info['residual_norm'] <= info['tolerance']
