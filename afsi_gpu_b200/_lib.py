@@ -34,7 +34,7 @@ class MGLevel(ctypes.Structure):
 class MGPlan(ctypes.Structure):
     _fields_ = [('dim', c_int32), ('bc', c_int32), ('levels', c_int32), ('smooth', c_int32),
                 ('dtype', c_int32), ('coarse_dtype', c_int32), ('level', MGLevel * MAX_LEVELS),
-                ('coarse_inverse', c_void_p), ('scratch', c_void_p)]
+                ('coarse_inverse', c_void_p), ('scratch', c_void_p), ('smoother', c_int32)]
 
 
 class PCGPlan(ctypes.Structure):

@@ -222,6 +222,67 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_kernel(const T* __restr
     coarse_cycle<BC, T, TC>(reinterpret_cast<T*>(smem_raw), rhs_global, rhs_sum, p_global, p_out, cinv, cl, smooth);
 }
 
+// ---- red-black Gauss-Seidel V-cycle (selectable smoother) ----
+//
+// A method change beside the reference's weighted Jacobi (mac/multigrid.py:
+// 107-110): each sweep updates the cells with (x+y+z) even, then the odd ones,
+// in place with omega 1, p += (rhs - A p)/diag, so every update reads only
+// cells of the other colour (7- or 5-point stencil) and the half-sweep is
+// race-free.  Periodic x needs even extents for the colouring to wrap, which
+// the plan check enforces on every smoothed level.
+
+template <int BC, class T>
+__global__ void __launch_bounds__(kThreads) rb_kernel(T* p, const T* __restrict__ rhs, Lv<T> L, int color) {
+    pdl_enter();
+    for_my_cells<BC>(L, [&](int x, int y, int z) {
+        if (((x + y + z) & 1) != color) return;
+        const int64_t i = index_of(x, y, z, L);
+        const T pc = p[i];
+        const T a = neg_lap<BC, true>(p, i, x, y, z, L, T(0), pc);
+        p[i] = pc + (rhs[i] - a) / diag_at<BC>(x, y, z, L);
+    });
+}
+
+// Sum of a level into the site (for the mean gauge of singular problems).
+template <int BC, class T>
+__global__ void __launch_bounds__(kThreads) level_sum_kernel(const T* __restrict__ x, Lv<T> L, Site s) {
+    pdl_enter();
+    double local = 0.0;
+    for_my_cells<BC>(L, [&](int cx, int cy, int cz) { local += double(x[index_of(cx, cy, cz, L)]); });
+    site_finish(s, local);
+}
+
+// Coarsest level: p = inv (rhs) with the dense inverse of the (regularised)
+// operator, accumulated in TC; singular problems then subtract the mean of p
+// (summed in index order by thread 0: at most 512 cells).
+constexpr int kDenseThreads = 512;
+
+template <int BC, class T, class TC>
+__global__ void __launch_bounds__(kDenseThreads) rb_dense_kernel(const T* __restrict__ rhs, T* __restrict__ p,
+                                                                 const TC* __restrict__ inv, int n) {
+    pdl_enter();
+    __shared__ TC r[kDenseThreads];
+    __shared__ T out[kDenseThreads];
+    __shared__ double mean;
+    for (int i = threadIdx.x; i < n; i += kDenseThreads) r[i] = TC(rhs[i]);
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += kDenseThreads) {
+        TC acc = TC(0);
+        for (int j = 0; j < n; ++j) acc = fma(inv[int64_t(i) * n + j], r[j], acc);
+        out[i] = T(acc);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sum = 0.0;
+        if (singular_bc(BC))
+            for (int i = 0; i < n; ++i) sum += double(out[i]);
+        mean = sum / n;
+    }
+    __syncthreads();
+    const T m = T(mean);
+    for (int i = threadIdx.x; i < n; i += kDenseThreads) p[i] = out[i] - m;
+}
+
 // Iterative refinement (precision form): the residual of the FP64 iterate in
 // FP64, handed to the FP32 V-cycles as float, with the norm of the FP64
 // residual; then the FP32 correction added to the FP64 iterate.
@@ -617,6 +678,12 @@ int32_t validate_plan(const afsi_mg_plan* plan) {
     int64_t nc = 1;
     for (int a = 0; a < plan->dim; ++a) nc *= plan->level[plan->levels - 1].shape[a];
     AFSI_REQUIRE(nc <= 512, "coarsest level must have <= 512 cells");
+    AFSI_REQUIRE(plan->smoother == AFSI_MG_JACOBI || plan->smoother == AFSI_MG_RED_BLACK, "unknown smoother %d",
+                 int(plan->smoother));
+    if (plan->smoother == AFSI_MG_RED_BLACK && plan->bc == AFSI_BC_PERIODIC)
+        for (int l = 0; l + 1 < plan->levels; ++l)
+            AFSI_REQUIRE(plan->level[l].shape[0] % 2 == 0,
+                         "red-black smoothing with periodic x needs an even x extent on every smoothed level");
     return AFSI_OK;
 }
 
@@ -649,6 +716,96 @@ extern "C" int64_t afsi_b200_mg_scratch_bytes(const afsi_mg_plan* plan) {
     return int64_t(kSites) * site_bytes(partial_width(plan));
 }
 
+// V-cycles with the red-black smoother: per level `smooth` sweeps of two
+// half-sweeps before and after the coarse correction, the fused residual
+// restriction (coarse right-hand side shifted to mean zero for singular
+// problems), a zero coarse start, the dense coarsest solve and the
+// prolongation of mac/multigrid.py:112-123; the finest iterate is shifted to
+// mean zero after every cycle for singular problems.
+template <int BC, class T, class TC>
+struct RbRunner {
+    const afsi_mg_plan* plan;
+    cudaStream_t stream;
+    SiteTable st;
+    Lv<T> lv[AFSI_MG_MAX_LEVELS];
+    static constexpr bool singular = singular_bc(BC);
+
+    T* P(int l) const { return static_cast<T*>(plan->level[l].p); }
+    T* R(int l) const { return static_cast<T*>(plan->level[l].rhs); }
+
+    int32_t smooth(int l) {
+        const Geometry g = launch_for(lv[l], BC);
+        for (int k = 0; k < plan->smooth; ++k)
+            for (int color = 0; color < 2; ++color) {
+                const int32_t rc = launch_pdl("mg red-black sweep", rb_kernel<BC, T>, g.grid, g.block, 0, stream, P(l),
+                                              static_cast<const T*>(R(l)), lv[l], color);
+                if (rc) return rc;
+            }
+        return AFSI_OK;
+    }
+
+    int32_t shift_to_mean_zero(T* x, int l, const Site& site) {
+        const Geometry g = launch_for(lv[l], BC);
+        int32_t rc = launch_pdl("mg level sum", level_sum_kernel<BC, T>, g.grid, g.block, 0, stream,
+                                static_cast<const T*>(x), lv[l], site);
+        if (rc) return rc;
+        return launch_pdl("mg mean shift", shift_kernel<T>, dim3(flat_grid(lv[l].n)), dim3(kThreads), 0, stream,
+                          static_cast<const T*>(x), x, lv[l].n, static_cast<const double*>(site.result));
+    }
+
+    int32_t level(int l) {
+        const int last = plan->levels - 1;
+        int32_t rc;
+        if (l == last)
+            return launch_pdl("mg dense coarse solve", rb_dense_kernel<BC, T, TC>, dim3(1), dim3(kDenseThreads), 0,
+                              stream, static_cast<const T*>(R(l)), P(l),
+                              static_cast<const TC*>(plan->coarse_inverse), int(lv[l].n));
+        if ((rc = smooth(l))) return rc;
+        const Geometry gc = launch_for(lv[l + 1], BC);
+        rc = launch_pdl("mg residual restrict", residual_restrict_kernel<BC, true, T>, gc.grid, gc.block, 0, stream,
+                        static_cast<const T*>(P(l)), static_cast<const T*>(R(l)), R(l + 1), lv[l], lv[l + 1],
+                        static_cast<const double*>(nullptr), st.s[l + 1][2], int(singular));
+        if (rc) return rc;
+        if (singular) {
+            rc = launch_pdl("mg mean shift", shift_kernel<T>, dim3(flat_grid(lv[l + 1].n)), dim3(kThreads), 0, stream,
+                            static_cast<const T*>(R(l + 1)), R(l + 1), lv[l + 1].n,
+                            static_cast<const double*>(st.s[l + 1][2].result));
+            if (rc) return rc;
+        }
+        if (l + 1 < last) {
+            const cudaError_t err = cudaMemsetAsync(P(l + 1), 0, size_t(lv[l + 1].n) * sizeof(T), stream);
+            if (err != cudaSuccess) return fail(AFSI_ERR_CUDA, "mg zero start: %s", cudaGetErrorString(err));
+        }
+        if ((rc = level(l + 1))) return rc;
+        const Geometry g = launch_for(lv[l], BC);
+        rc = launch_pdl("mg prolong add", prolong_kernel<BC, T>, g.grid, g.block, 0, stream,
+                        static_cast<const T*>(P(l)), static_cast<const T*>(P(l + 1)), P(l), lv[l], lv[l + 1],
+                        static_cast<const double*>(nullptr), static_cast<const double*>(nullptr));
+        if (rc) return rc;
+        return smooth(l);
+    }
+
+    int32_t run(int cycles) {
+        for (int l = 0; l < plan->levels; ++l)
+            lv[l] = make_level<T>(plan->level[l].shape, plan->level[l].h2, plan->level[l].inv_h2, plan->dim);
+        for (int c = 0; c < cycles; ++c) {
+            int32_t rc = level(0);
+            if (!rc && singular) rc = shift_to_mean_zero(P(0), 0, st.s[0][0]);
+            if (rc) return rc;
+        }
+        return AFSI_OK;
+    }
+};
+
+template <int BC, class T, class TC>
+int32_t run_red_black(const afsi_mg_plan* plan, int cycles, cudaStream_t stream) {
+    RbRunner<BC, T, TC> r;
+    r.plan = plan;
+    r.stream = stream;
+    r.st = sites_for(plan);
+    return r.run(cycles);
+}
+
 extern "C" int32_t afsi_b200_mg_vcycles(const afsi_mg_plan* plan, int32_t cycles, afsi_stream_t stream) {
     int32_t rc = validate_plan(plan);
     if (rc) return rc;
@@ -656,6 +813,10 @@ extern "C" int32_t afsi_b200_mg_vcycles(const afsi_mg_plan* plan, int32_t cycles
     AFSI_REQUIRE(plan->coarse_dtype == AFSI_F64 || plan->coarse_dtype == plan->dtype, "unsupported coarse dtype");
     AFSI_BC_DISPATCH(plan->bc, {
         AFSI_DISPATCH(plan->dtype, {
+            if (plan->smoother == AFSI_MG_RED_BLACK) {
+                if (plan->coarse_dtype == AFSI_F64) return run_red_black<BC, T, double>(plan, cycles, stream);
+                return run_red_black<BC, T, T>(plan, cycles, stream);
+            }
             if (plan->coarse_dtype == AFSI_F64)
                 return run_plan<BC, T, double>(plan, cycles, stream);
             return run_plan<BC, T, T>(plan, cycles, stream);

@@ -413,6 +413,7 @@ extern "C" int32_t afsi_b200_mg_persistent(const afsi_mg_plan* plan, int32_t cyc
     if (rc) return rc;
     AFSI_REQUIRE(cycles >= 0 && check_every >= 1 && sync_scratch, "invalid persistent multigrid arguments");
     AFSI_REQUIRE(!solve || info, "solve mode needs an info buffer");
+    AFSI_REQUIRE(plan->smoother == AFSI_MG_JACOBI, "the persistent multigrid runs the Jacobi smoother only");
     if (cycles == 0) return AFSI_OK;
     AFSI_REQUIRE(plan->coarse_dtype == AFSI_F64 || plan->coarse_dtype == plan->dtype, "unsupported coarse dtype");
     switch (plan->bc) {

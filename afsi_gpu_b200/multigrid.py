@@ -227,9 +227,14 @@ class _Solver:
     _not_converged = 'pressure multigrid did not converge'
 
     def __init__(self, grid, *, device='cuda', dtype=torch.float64, options=None, backend='b200-graph',
-                 coarse_dtype=None):
+                 coarse_dtype=None, smoother='jacobi'):
         if backend not in ('b200', 'b200-graph', 'b200-persistent'):
             raise ValueError('pressure backend must be b200, b200-graph or b200-persistent')
+        if smoother not in ('jacobi', 'red-black'):
+            raise ValueError("smoother must be 'jacobi' (the reference's) or 'red-black'")
+        if smoother == 'red-black' and backend == 'b200-persistent':
+            raise ValueError('the persistent backend runs the Jacobi smoother only')
+        self.smoother = smoother
         device = torch.device(device)
         if device.type != 'cuda':
             raise ValueError('the B200 multigrid requires a CUDA device; there is no CPU fallback')
@@ -245,7 +250,10 @@ class _Solver:
         self.workspace = _Workspace(self.shapes, self.spacings, self.bc, dtype, device, self.options.smooth,
                                     self.coarse_dtype)
         self.workspace.set_coarse(self.coarse_inverse)
+        self.workspace.plan.smoother = 1 if smoother == 'red-black' else 0
         self.backend = self.kernels.name + {'b200': '', 'b200-graph': '-graph', 'b200-persistent': '-persistent'}[backend]
+        if smoother == 'red-black':
+            self.backend += '-red-black'
         self.persistent = backend == 'b200-persistent'
         self.graphs = {}
         if backend == 'b200-graph':
@@ -469,7 +477,7 @@ class RefinedMultigrid:
     """
 
     def __init__(self, grid, *, bc=None, device='cuda', options=None, inner_rtol=1e-5, inner_cycles=40,
-                 max_refinements=8, backend='b200-graph'):
+                 max_refinements=8, backend='b200-graph', smoother='jacobi'):
         self.options = MGOptions() if options is None else options
         if not 0 < inner_rtol < 1 or max_refinements < 1:
             raise ValueError('refinement needs 0 < inner_rtol < 1 and max_refinements >= 1')
@@ -480,7 +488,7 @@ class RefinedMultigrid:
         inner_opts = MGOptions(rtol=inner_rtol, atol=0., max_cycles=inner_cycles, smooth=self.options.smooth,
                                check_every=self.options.check_every)
         self.inner = cls(grid, device=device, dtype=torch.float32, coarse_dtype=torch.float64, options=inner_opts,
-                         backend=backend)
+                         backend=backend, smoother=smoother)
         self.bc = self.inner.bc
         self.inner_rtol = inner_rtol
         self.max_refinements = max_refinements

@@ -290,7 +290,19 @@ typedef struct afsi_mg_plan {
     afsi_mg_level level[AFSI_MG_MAX_LEVELS];
     const void* coarse_inverse;  /* (n,n), n = cells on the coarsest level */
     void* scratch;         /* reduction scratch, afsi_b200_mg_scratch_bytes() */
+    int32_t smoother;      /* AFSI_MG_JACOBI (the reference's) or AFSI_MG_RED_BLACK */
 } afsi_mg_plan;
+
+/* Smoothers.  AFSI_MG_JACOBI is the reference's weighted Jacobi (omega 2/3,
+ * mac/multigrid.py:107-110) with its mean gauge after every sweep.
+ * AFSI_MG_RED_BLACK is a method change with no counterpart in the reference:
+ * `smooth` red-black Gauss-Seidel sweeps (omega 1, in place) before and
+ * after the coarse correction, coarse right-hand sides shifted to mean zero,
+ * the finest iterate shifted to mean zero once per cycle (singular BCs); its
+ * solves agree with the Jacobi solves at the solve tolerance, not per cycle.
+ * The persistent entry point supports Jacobi only. */
+#define AFSI_MG_JACOBI 0
+#define AFSI_MG_RED_BLACK 1
 
 /* Bytes of device scratch (zero-initialised once by the caller) a plan needs. */
 int64_t afsi_b200_mg_scratch_bytes(const afsi_mg_plan* plan);

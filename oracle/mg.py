@@ -287,8 +287,30 @@ def smooth(h, level, p, rhs, sweeps):
     return p
 
 
-def cycle(h, level, p, rhs, sweeps):
-    """One V-cycle: ``mac/multigrid.py:112-123`` / ``mac2d/multigrid.py:67-83``."""
+def rb_smooth(h, level, p, rhs, sweeps):
+    """Red-black Gauss-Seidel sweeps (the selectable smoother of the B200
+    build; the reference has none): cells with an even index sum, then the
+    odd ones, p += (rhs - A p)/diag in place (omega 1)."""
+    color = np.indices(p.shape).sum(0) & 1
+    d = h.diagonals[level]
+    for _ in range(sweeps):
+        for c in (0, 1):
+            p = np.where(color == c, p + (rhs - h.apply(level, p)) / d, p)
+    return p
+
+
+def cycle(h, level, p, rhs, sweeps, smoother='jacobi'):
+    """One V-cycle: ``mac/multigrid.py:112-123`` / ``mac2d/multigrid.py:67-83``.
+
+    ``smoother='red-black'`` replaces the weighted Jacobi sweeps (and their
+    per-sweep mean gauge) by red-black Gauss-Seidel sweeps; singular problems
+    then shift the finest iterate to mean zero once, at the end of the cycle.
+    """
+    if smoother == 'red-black':
+        p = _rb_cycle(h, level, p, rhs, sweeps)
+        if level == 0 and h.singular:
+            p = p - p.mean(dtype=np.float64).astype(h.dtype)
+        return p
     if level == len(h.shapes) - 1:
         sol = (h.coarse_inverse.astype(np.float64) @ rhs.reshape(-1).astype(np.float64))
         sol = sol.astype(h.dtype).reshape(rhs.shape)
@@ -304,6 +326,22 @@ def cycle(h, level, p, rhs, sweeps):
     return smooth(h, level, p, rhs, sweeps) if h.singular else _plain_smooth(h, level, p, rhs, sweeps)
 
 
+def _rb_cycle(h, level, p, rhs, sweeps):
+    if level == len(h.shapes) - 1:
+        sol = (h.coarse_inverse.astype(np.float64) @ rhs.reshape(-1).astype(np.float64))
+        sol = sol.astype(h.dtype).reshape(rhs.shape)
+        if h.singular:
+            sol = sol - sol.mean(dtype=np.float64).astype(h.dtype)
+        return sol
+    p = rb_smooth(h, level, p, rhs, sweeps)
+    coarse = h.restrict(rhs - h.apply(level, p))
+    if h.singular:
+        coarse = coarse - coarse.mean(dtype=np.float64).astype(h.dtype)
+    corr = _rb_cycle(h, level + 1, np.zeros_like(coarse), coarse, sweeps)
+    p = p + h.prolong(corr, p.shape)
+    return rb_smooth(h, level, p, rhs, sweeps)
+
+
 def _plain_smooth(h, level, p, rhs, sweeps):
     w = h.dtype(OMEGA)
     for _ in range(sweeps):
@@ -311,7 +349,8 @@ def _plain_smooth(h, level, p, rhs, sweeps):
     return p
 
 
-def solve(h, rhs, initial=None, *, rtol=1e-10, atol=1e-12, max_cycles=100, sweeps=4, check_every=2):
+def solve(h, rhs, initial=None, *, rtol=1e-10, atol=1e-12, max_cycles=100, sweeps=4, check_every=2,
+          smoother='jacobi'):
     """Solve loop, ``mac/multigrid.py:125-172`` (singular) and
     ``mac2d/multigrid.py:85-111`` (channel).  Returns (p, info)."""
     rhs = np.asarray(rhs, dtype=h.dtype)
@@ -331,7 +370,7 @@ def solve(h, rhs, initial=None, *, rtol=1e-10, atol=1e-12, max_cycles=100, sweep
     if res <= tol:
         return p, dict(cycles=0, residual_norm=res, tolerance=tol)
     for k in range(1, max_cycles + 1):
-        p = cycle(h, 0, p, rhs, sweeps)
+        p = cycle(h, 0, p, rhs, sweeps, smoother)
         if k % check_every == 0 or k == max_cycles:
             res = float(np.linalg.norm((rhs - h.apply(0, p)).astype(np.float64)))
             if not isfinite(res):
