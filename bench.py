@@ -228,6 +228,43 @@ def mass_pcg_row(X, cells, device, peak_gbs, solves=20):
                 note='one begin launch + one WHILE-loop graph launch per solve, one host read')
 
 
+def mg_forms_row(grid, rhs, device, reps=10):
+    """The 64^3 pressure solve of the step in its other forms, each to the
+    same FP64 tolerance (rtol 1e-10): the reference's Jacobi smoother (the
+    step's solver), the red-black Gauss-Seidel smoother (2 sweeps), and the
+    precision form (FP32 V-cycles inside FP64 iterative refinement) with each
+    smoother.  CUDA events around `reps` solves; `max_rel_diff` is the largest
+    difference from the Jacobi FP64 solution over its largest value."""
+    from afsi_gpu_b200.multigrid import GeometricMultigrid, MGOptions, RefinedMultigrid
+    b = torch.as_tensor(rhs, device=device)
+    solvers = dict(
+        jacobi_fp64=GeometricMultigrid(grid, device=device, backend='b200-graph'),
+        red_black_fp64=GeometricMultigrid(grid, device=device, backend='b200-graph', smoother='red-black',
+                                          options=MGOptions(smooth=2)),
+        jacobi_fp32_refined=RefinedMultigrid(grid, device=device),
+        red_black_fp32_refined=RefinedMultigrid(grid, device=device, smoother='red-black',
+                                                options=MGOptions(smooth=2)))
+    stream = torch.cuda.current_stream(device)
+    out, base = {}, None
+    for name, mg in solvers.items():
+        for _ in range(2):
+            p, info = mg.solve(b)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        e0.record(stream)
+        for _ in range(reps):
+            p, info = mg.solve(b)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        if base is None:
+            base = p
+        out[name] = dict(ms_per_solve=e0.elapsed_time(e1) / reps, cycles=info['cycles'],
+                         refinements=info.get('refinements'), residual=info['residual_norm'],
+                         tolerance=info['tolerance'],
+                         max_rel_diff=float((p - base).abs().max() / base.abs().max()))
+    return out
+
+
 def load_traffic():
     path = ROOT / 'profiles' / 'traffic.json'
     try:
@@ -443,6 +480,7 @@ def run_b200(args):
                                f'elements for the transfers (scaled by element count) + full 64^3 MG solve'))
             errors = oracle_errors(step, X, coef, vel, outputs, outs[-1].numpy())
         mass = mass_pcg_row(X, cells, device, pk['hbm_gbs'])
+        forms = mg_forms_row(grid, rhs, device)
         step_ms = np.array([ev[0].elapsed_time(ev[4]) for ev in phases])
         line = dict(
             metric=METRIC, value=world * args.steps / elapsed, unit='steps/s', n_gpus=world, steps=args.steps,
@@ -467,6 +505,7 @@ def run_b200(args):
                             mean=float(step_ms.mean())),
             oracle_error=errors,
             mass_pcg=mass,
+            mg_forms=forms,
             cpu_baseline=cpu)
         print(json.dumps(line, default=_json))
     if dist:
