@@ -121,6 +121,12 @@ _SIGNATURES = {
     'afsi_b200_mg_refine_residual': [c_void_p, c_void_p, c_void_p, P_I64, P_F64, c_int32, c_int32, c_void_p, c_void_p,
                                      c_void_p],
     'afsi_b200_mg_refine_correct': [c_void_p, c_void_p, c_int64, c_void_p],
+    'afsi_b200_batch2d_prepare': [c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_int32,
+                                  c_void_p],
+    'afsi_b200_batch2d_spread': [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_void_p,
+                                 c_int64, c_int64, c_void_p, c_int32, c_void_p],
+    'afsi_b200_batch2d_gather': [c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_int64, c_void_p,
+                                 c_void_p, c_int32, c_void_p],
     'afsi_b200_pcg_scratch_bytes': [],
     'afsi_b200_pcg_begin': [ctypes.POINTER(PCGPlan), c_void_p],
     'afsi_b200_pcg_iterations': [ctypes.POINTER(PCGPlan), c_int32, c_void_p],

@@ -1,0 +1,275 @@
+"""Batching form: many independent 2D channel instances stepped together.
+
+No counterpart in the reference, which builds one ``TriangleTransfer``
+(``mac2d/transfer.py:19-127``) and one ``ChannelMultigrid``
+(``mac2d/multigrid.py:16-134``) per instance and steps instances one at a
+time.  Here a batch of instances with uneven grids and point counts is one
+step:
+
+* one launch each for the prepare, the spread and the gather of every
+  instance (``afsi_b200_batch2d_*``): points of all instances back to back,
+  face arrays back to back, batch-global stencil ids; positions and bases in
+  FP64, weights and transfers in ``transfer_dtype`` (FP32 in the precision
+  form);
+* a fixed number of V-cycles per instance on its own FP32 workspace (FP64
+  coarsest solve), the instances spread over ``streams`` capture streams so
+  that their small level kernels overlap on the device;
+* the whole step captured once as a CUDA graph and replayed.
+
+``autotune()`` chooses the schedule (stream count, instance order, smoother
+with the cycle count that reaches the requested FP32 residual reduction on
+every instance) by measuring graph replays, and keeps the fastest.
+"""
+from dataclasses import dataclass
+import numpy as np
+import torch
+from . import _lib
+from ._lib import call, ptr, dtype_code
+from .grid import ChannelGrid
+from .multigrid import ChannelMultigrid, MGOptions
+
+# afsi_batch2d_instance (include/afsi_b200.h)
+INSTANCE_DTYPE = np.dtype([('nx', '<i8'), ('ny', '<i8'), ('hx', '<f8'), ('hy', '<f8'), ('lx', '<f8'),
+                           ('ly', '<f8'), ('point_offset', '<i8'), ('point_count', '<i8'), ('u_offset', '<i8'),
+                           ('v_offset', '<i8')])
+
+
+def leaflet_points(grid, count, seed, dtype=np.float64):
+    """Two open leaflets, one hinged on each wall, as strips of points: a
+    stand-in for the quadrature points of two P2 triangle strips."""
+    rng = np.random.default_rng(seed)
+    Lx, Ly = grid.lengths
+    hx, hy = grid.spacing
+    out = []
+    for k, n in enumerate((count // 2, count - count // 2)):
+        s = rng.uniform(0., 1., n)                # position along the leaflet
+        t = rng.uniform(-.25, .25, n) * hx        # across the strip
+        x0 = Lx * (.35 + .1 * k)
+        y = (.02 + .4 * s) * Ly if k == 0 else (.98 - .4 * s) * Ly
+        x = x0 + .08 * Lx * s * s + t
+        out.append(np.stack((x, y), -1))
+    return np.concatenate(out).astype(dtype)
+
+
+@dataclass
+class Schedule:
+    streams: int = 4
+    order: str = 'largest-first'
+    smoother: str = 'jacobi'
+    cycles: int = 6
+
+
+class BatchedChannels:
+    """A batch of independent 2D channel instances (grids, points, forces,
+    face velocities, pressure right-hand sides), stepped together."""
+
+    def __init__(self, grids, points, forces, velocities, pressures, *, device='cuda',
+                 transfer_dtype=torch.float32, mg_dtype=torch.float32, schedule=None):
+        if not (len(grids) == len(points) == len(forces) == len(velocities) == len(pressures)) or not grids:
+            raise ValueError('one grid, point set, force set, velocity and pressure RHS per instance')
+        if len(grids) > 1024:
+            raise ValueError('at most 1024 instances per batch')
+        device = torch.device(device)
+        if device.type != 'cuda':
+            raise ValueError('the batched form requires a CUDA device; there is no CPU fallback')
+        _lib.load()
+        self.device, self.grids = device, list(grids)
+        self.transfer_dtype, self.mg_dtype = transfer_dtype, mg_dtype
+        self.schedule = schedule or Schedule()
+        counts = [int(len(p)) for p in points]
+        self.point_offsets = np.concatenate(([0], np.cumsum(counts))).astype(np.int64)
+        nu = [(g.shape[0] + 1) * g.shape[1] for g in grids]
+        nv = [g.shape[0] * (g.shape[1] + 1) for g in grids]
+        self.u_offsets = np.concatenate(([0], np.cumsum(nu))).astype(np.int64)
+        self.v_offsets = np.concatenate(([0], np.cumsum(nv))).astype(np.int64)
+        table = np.zeros(len(grids), INSTANCE_DTYPE)
+        for i, g in enumerate(grids):
+            table[i] = (g.shape[0], g.shape[1], g.spacing[0], g.spacing[1], g.lengths[0], g.lengths[1],
+                        self.point_offsets[i], counts[i], self.u_offsets[i], self.v_offsets[i])
+        self.table = torch.as_tensor(table.view(np.uint8), device=device)
+        self.total = int(self.point_offsets[-1])
+        self.nu, self.nv = int(self.u_offsets[-1]), int(self.v_offsets[-1])
+        as_t = lambda a, dt: torch.as_tensor(np.asarray(a), device=device, dtype=dt)
+        self.x = torch.cat([as_t(p, torch.float64) for p in points]).contiguous()
+        self.force = torch.cat([as_t(f, transfer_dtype) for f in forces]).contiguous()
+        self.u_in = torch.cat([as_t(v[0], transfer_dtype).reshape(-1) for v in velocities])
+        self.v_in = torch.cat([as_t(v[1], transfer_dtype).reshape(-1) for v in velocities])
+        self.rhs = [as_t(r, mg_dtype) for r in pressures]
+        self.ids = torch.empty((2, self.total, 16), device=device, dtype=torch.int64)
+        self.weights = torch.empty((2, self.total, 16), device=device, dtype=transfer_dtype)
+        self.u = torch.zeros(self.nu, device=device, dtype=transfer_dtype)
+        self.v = torch.zeros(self.nv, device=device, dtype=transfer_dtype)
+        self.gathered = torch.empty((self.total, 2), device=device, dtype=transfer_dtype)
+        self.status = torch.zeros(1, device=device, dtype=torch.int32)
+        self._solvers = {}
+        self.graph = None
+
+    # -- pieces of the step
+    def solvers(self, smoother):
+        """One FP32 workspace per instance and smoother (built once)."""
+        if smoother not in self._solvers:
+            opts = MGOptions(smooth=2 if smoother == 'red-black' else 4)
+            self._solvers[smoother] = [ChannelMultigrid(g, device=self.device, dtype=self.mg_dtype,
+                                                        coarse_dtype=torch.float64, backend='b200',
+                                                        smoother=smoother, options=opts) for g in self.grids]
+        return self._solvers[smoother]
+
+    def transfers(self, stream):
+        s = stream.cuda_stream
+        code = dtype_code(self.transfer_dtype)
+        n = len(self.grids)
+        call('afsi_b200_batch2d_prepare', ptr(self.x), self.total, ptr(self.table), n, ptr(self.ids),
+             ptr(self.weights), ptr(self.status), code, s)
+        self.u.zero_()
+        self.v.zero_()
+        call('afsi_b200_batch2d_spread', ptr(self.force), ptr(self.ids), ptr(self.weights), self.total,
+             ptr(self.table), n, ptr(self.u), ptr(self.v), self.nu, self.nv, ptr(self.status), code, s)
+        call('afsi_b200_batch2d_gather', ptr(self.u_in), ptr(self.v_in), self.nu, self.nv, ptr(self.ids),
+             ptr(self.weights), self.total, ptr(self.gathered), ptr(self.status), code, s)
+
+    def cycles(self, index, schedule):
+        mg = self.solvers(schedule.smoother)[index]
+        w = mg.workspace
+        w.rhs[0].copy_(self.rhs[index])
+        w.p[0].zero_()
+        w.vcycles(schedule.cycles)
+
+    def order(self, schedule):
+        idx = list(range(len(self.grids)))
+        if schedule.order == 'largest-first':
+            idx.sort(key=lambda i: -(self.grids[i].shape[0] * self.grids[i].shape[1]))
+        return idx
+
+    def run(self, schedule=None):
+        """The step on the current stream with a fork/join over `streams`
+        side streams (eager, or inside a capture)."""
+        schedule = schedule or self.schedule
+        main = torch.cuda.current_stream(self.device)
+        self.transfers(main)
+        side = [torch.cuda.Stream(device=self.device) for _ in range(schedule.streams)]
+        for s in side:
+            s.wait_stream(main)
+        for k, i in enumerate(self.order(schedule)):
+            with torch.cuda.stream(side[k % len(side)]):
+                self.cycles(i, schedule)
+        for s in side:
+            main.wait_stream(s)
+
+    def capture(self, schedule=None):
+        schedule = schedule or self.schedule
+        self.solvers(schedule.smoother)
+        with torch.cuda.device(self.device):
+            warm = torch.cuda.Stream(device=self.device)
+            warm.wait_stream(torch.cuda.current_stream(self.device))
+            with torch.cuda.stream(warm):
+                self.run(schedule)
+            torch.cuda.current_stream(self.device).wait_stream(warm)
+            g = torch.cuda.CUDAGraph()
+            before = _lib.launch_count()
+            with torch.cuda.graph(g):
+                self.run(schedule)
+            launches = _lib.launch_count() - before
+            _lib.forget_launches(launches)
+        return g, launches
+
+    def use(self, schedule):
+        self.schedule = schedule
+        self.graph, self.graph_launches = self.capture(schedule)
+
+    def replay(self):
+        if self.graph is None:
+            self.use(self.schedule)
+        self.graph.replay()
+        _lib.count_replay(self.graph_launches)
+
+    # -- results and checks
+    def fields(self, i):
+        g = self.grids[i]
+        u = self.u[self.u_offsets[i]:self.u_offsets[i + 1]].view(g.face_shape(0))
+        v = self.v[self.v_offsets[i]:self.v_offsets[i + 1]].view(g.face_shape(1))
+        return u, v
+
+    def velocities(self, i):
+        return self.gathered[self.point_offsets[i]:self.point_offsets[i + 1]]
+
+    def pressure(self, i, smoother=None):
+        return self.solvers(smoother or self.schedule.smoother)[i].workspace.p[0]
+
+    def residual_reduction(self, smoother=None):
+        """||rhs - A p|| / ||rhs|| per instance after the last step (FP32 workspaces)."""
+        out = []
+        for i, mg in enumerate(self.solvers(smoother or self.schedule.smoother)):
+            out.append(mg.residual_norm().item() / max(self.rhs[i].double().norm().item(), 1e-300))
+        return out
+
+    def check(self):
+        word = int(self.status.item())
+        self.status.zero_()
+        if word & _lib.FLAG_SUPPORT:
+            raise ValueError('valve IB points leave the channel support region')
+        if word & _lib.FLAG_INDEX:
+            raise RuntimeError('batched stencil index outside its instance')
+
+    # -- autotuner
+    def autotune(self, *, target=1e-4, streams=(1, 4, 8, 16), orders=('given', 'largest-first'),
+                 smoothers=('jacobi', 'red-black'), max_cycles=12, replays=5):
+        """Fastest schedule whose V-cycles reduce every instance's FP32
+        residual by `target`: for each smoother the smallest cycle count that
+        meets the target (measured), then every (streams, order) measured by
+        CUDA-event timing of graph replays.  Returns (schedule, table)."""
+        table = []
+        best = None
+        for smoother in smoothers:
+            cycles = None
+            for c in range(1, max_cycles + 1):
+                self.run(Schedule(streams=1, order='given', smoother=smoother, cycles=c))
+                torch.cuda.synchronize(self.device)
+                if max(self.residual_reduction(smoother)) <= target:
+                    cycles = c
+                    break
+            if cycles is None:
+                continue
+            for s in streams:
+                for order in orders:
+                    sch = Schedule(streams=s, order=order, smoother=smoother, cycles=cycles)
+                    g, launches = self.capture(sch)
+                    g.replay()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    torch.cuda.synchronize(self.device)
+                    e0.record()
+                    for _ in range(replays):
+                        g.replay()
+                    e1.record()
+                    torch.cuda.synchronize(self.device)
+                    ms = e0.elapsed_time(e1) / replays
+                    table.append(dict(streams=s, order=order, smoother=smoother, cycles=cycles, ms=ms,
+                                      launches=launches))
+                    if best is None or ms < best[0]:
+                        best = (ms, sch)
+                    del g
+        if best is None:
+            raise RuntimeError(f'no smoother reaches the residual reduction {target:g} in {max_cycles} cycles')
+        self.use(best[1])
+        return best[1], table
+
+
+def seeded_batch(count=64, *, seed=0, shapes=((128, 32), (256, 64), (384, 96), (512, 128)),
+                 points=(5000, 40000), device='cuda', **kwargs):
+    """The batching workload: `count` instances with seeded grid sizes,
+    leaflet point counts in `points`, N(0,1) forces, seeded Fourier face
+    velocities and mean-free N(0,1) pressure right-hand sides; lengths
+    (4, 1) so that h is uniform per instance."""
+    from . import synthetic
+    rng = np.random.default_rng(seed)
+    grids, pts, forces, vels, rhs = [], [], [], [], []
+    for i in range(count):
+        nx, ny = shapes[int(rng.integers(len(shapes)))]
+        g = ChannelGrid((nx, ny), (4., 1.))
+        n = int(rng.integers(points[0], points[1] + 1))
+        grids.append(g)
+        pts.append(leaflet_points(g, n, seed=seed * 1000 + i))
+        forces.append(rng.standard_normal((n, 2)))
+        vels.append(tuple(t.numpy() for t in synthetic.fourier_velocity2d(g, seed=seed * 1000 + i)))
+        r = rng.standard_normal((nx, ny))
+        rhs.append(r - r.mean())
+    return BatchedChannels(grids, pts, forces, vels, rhs, device=device, **kwargs)

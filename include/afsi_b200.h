@@ -378,6 +378,32 @@ int32_t afsi_b200_vector_stats(const void* x, int64_t n, double* stats_out, void
 int32_t afsi_b200_subtract_mean(void* x, int64_t n, const double* stats, int32_t dtype,
     afsi_stream_t stream);
 
+/* ---- batched 2D transfers (the batching form) ------------------------------
+ * Many independent 2D channel instances (TriangleTransfer, mac2d/transfer.py:
+ * 61-127, one per instance in the reference) in one launch per operation.
+ * Points of all instances are stored back to back, and the u (nx+1, ny) and
+ * v (nx, ny+1) face arrays of all instances back to back; `instances` is a
+ * DEVICE array of `count` (1..1024) entries ordered by point_offset.  Ids are
+ * written batch-global (face offset of the instance included).  Positions,
+ * bases and weights are formed in FP64 (points are FP64) and the weights
+ * stored in weight_dtype; the spread divides by the instance's hx*hy and
+ * accumulates into pre-zeroed u / v; the gather writes (total, 2). */
+typedef struct afsi_batch2d_instance {
+    int64_t nx, ny;              /* cells */
+    double hx, hy, lx, ly;       /* spacing and lengths */
+    int64_t point_offset;        /* first point of the instance in the batch */
+    int64_t point_count;
+    int64_t u_offset, v_offset;  /* first u / v face of the instance in the batch arrays */
+} afsi_batch2d_instance;
+
+int32_t afsi_b200_batch2d_prepare(const double* points, int64_t total, const afsi_batch2d_instance* instances,
+    int32_t count, int64_t* ids, void* weights, int32_t* status, int32_t weight_dtype, afsi_stream_t stream);
+int32_t afsi_b200_batch2d_spread(const void* force, const int64_t* ids, const void* weights, int64_t total,
+    const afsi_batch2d_instance* instances, int32_t count, void* u, void* v, int64_t nu, int64_t nv,
+    int32_t* status, int32_t dtype, afsi_stream_t stream);
+int32_t afsi_b200_batch2d_gather(const void* u, const void* v, int64_t nu, int64_t nv, const int64_t* ids,
+    const void* weights, int64_t total, void* out, int32_t* status, int32_t dtype, afsi_stream_t stream);
+
 /* ---- consistent-mass Jacobi-PCG ------------------------------------------
  * Replaces MassSolver.solve / GraphMassSolver.solve (mac/mass_solver.py:39-103,
  * mac/mass_graph.py:129-225): M x = rhs for a (rows, cols) block, M a CSR

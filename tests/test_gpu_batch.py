@@ -1,0 +1,104 @@
+"""Batching form (afsi_gpu_b200.batch): many 2D channel instances per step.
+
+Per instance the batch must reproduce the single-instance operators: stencil
+ids and FP64 weights bit-exact against the oracle (``mac2d/transfer.py:61-81``),
+FP32 weights equal to the FP64 weights rounded once; spreads and gathers
+1e-12 of the field scale in FP64 (the single-instance bar) and 2e-6 in FP32
+against the FP64 oracle; each instance's V-cycles bitwise equal to its own
+solver run alone; graph replay equal to the eager step.
+"""
+import numpy as np
+import pytest
+import torch
+from oracle import ib as oracle
+from afsi_gpu_b200.batch import BatchedChannels, Schedule, seeded_batch
+
+pytestmark = pytest.mark.gpu
+DEV = 'cuda'
+
+
+def _small(dtype, count=6, seed=4):
+    return seeded_batch(count, seed=seed, shapes=((128, 32), (256, 64), (384, 96)), points=(2000, 6000),
+                        device=DEV, transfer_dtype=dtype,
+                        schedule=Schedule(streams=3, order='largest-first', smoother='jacobi', cycles=3))
+
+
+def _host(b, i, name):
+    lo, hi = b.point_offsets[i], b.point_offsets[i + 1]
+    return getattr(b, name)[lo:hi].double().cpu().numpy()
+
+
+@pytest.mark.parametrize('dtype', [torch.float64, torch.float32])
+def test_batched_transfers_match_oracle_per_instance(dtype):
+    b = _small(dtype)
+    b.run()
+    torch.cuda.synchronize()
+    b.check()
+    tol = 1e-12 if dtype == torch.float64 else 2e-6
+    for i, g in enumerate(b.grids):
+        lo, hi = b.point_offsets[i], b.point_offsets[i + 1]
+        pts = b.x[lo:hi].cpu().numpy()
+        ids, w = oracle.prepare2d(pts, g.shape, g.spacing)
+        for c, off in enumerate((b.u_offsets[i], b.v_offsets[i])):
+            assert np.array_equal(b.ids[c, lo:hi].cpu().numpy(), ids[c] + off)
+            got_w = b.weights[c, lo:hi].cpu().numpy()
+            assert np.array_equal(got_w, w[c].astype(got_w.dtype))
+        force = b.force[lo:hi].double().cpu().numpy()
+        fields = b.fields(i)
+        vel = (b.u_in[b.u_offsets[i]:b.u_offsets[i + 1]], b.v_in[b.v_offsets[i]:b.v_offsets[i + 1]])
+        for c in range(2):
+            size = fields[c].numel()
+            ref = oracle.indexed_spread(force[:, c], ids[c], w[c], size, g.volume)
+            scale = np.abs(ref).max()
+            np.testing.assert_allclose(fields[c].reshape(-1).double().cpu().numpy(), ref, rtol=tol, atol=tol * scale)
+            ref = oracle.indexed_gather(vel[c].double().cpu().numpy(), ids[c], w[c])
+            np.testing.assert_allclose(b.velocities(i)[:, c].double().cpu().numpy(), ref, rtol=tol,
+                                       atol=tol * np.abs(ref).max())
+
+
+def test_batched_cycles_equal_each_instance_alone_and_graph_replay_equals_eager():
+    b = _small(torch.float32)
+    sch = b.schedule
+    b.run(sch)
+    torch.cuda.synchronize()
+    eager_p = [b.pressure(i).clone() for i in range(len(b.grids))]
+    eager_g = b.gathered.clone()
+    from afsi_gpu_b200.multigrid import ChannelMultigrid, MGOptions
+    for i, g in enumerate(b.grids):
+        alone = ChannelMultigrid(g, device=DEV, dtype=torch.float32, coarse_dtype=torch.float64, backend='b200',
+                                 options=MGOptions(smooth=4))
+        alone.initialize(torch.zeros_like(eager_p[i]), b.rhs[i])
+        p = alone.advance(sch.cycles)
+        assert torch.equal(p, eager_p[i])
+    reduction = b.residual_reduction()
+    assert max(reduction) < 1e-2
+    b.use(sch)  # captures (and so runs the step once more)
+    for i in range(len(b.grids)):
+        b.pressure(i).zero_()
+    b.gathered.zero_()
+    b.replay()
+    torch.cuda.synchronize()
+    b.check()
+    assert torch.equal(b.gathered, eager_g)
+    for i in range(len(b.grids)):
+        assert torch.equal(b.pressure(i), eager_p[i])
+
+
+def test_autotuner_picks_a_measured_schedule_meeting_the_target():
+    b = _small(torch.float32, count=8, seed=7)
+    schedule, table = b.autotune(target=1e-3, streams=(1, 4), max_cycles=10, replays=2)
+    best = min(table, key=lambda r: r['ms'])
+    assert (best['streams'], best['order'], best['smoother'], best['cycles']) == \
+        (schedule.streams, schedule.order, schedule.smoother, schedule.cycles)
+    assert {r['smoother'] for r in table} == {'jacobi', 'red-black'}
+    b.replay()
+    torch.cuda.synchronize()
+    assert max(b.residual_reduction()) <= 1e-3
+
+
+def test_batch_rejects_points_outside_their_channel():
+    b = _small(torch.float64, count=2)
+    b.x[0, 0] = -1.0
+    b.run()
+    with pytest.raises(ValueError, match='support'):
+        b.check()
