@@ -265,6 +265,101 @@ def mg_forms_row(grid, rhs, device, reps=10):
     return out
 
 
+def batch_form_row(device, count=64, replays=20):
+    """Batching form: 64 seeded 2D channel instances (grids 128x32 .. 512x128,
+    5k-40k leaflet points each, N(0,1) forces), FP32 transfers and V-cycles,
+    one captured graph per step with the autotuned schedule (fixed V-cycle
+    count reaching a 1e-4 FP32 residual reduction on every instance).  The
+    plain FP64 drop-in on the same GPU steps the same instances one at a time
+    through the single-instance API (prepare2d with its support check,
+    spread2d, gather2d, FP64 channel V-cycles, same cycle count).  Errors:
+    largest difference of the FP32 batch from the FP64 plain step over the
+    largest value, per output."""
+    from afsi_gpu_b200 import cuda_ib
+    from afsi_gpu_b200.batch import seeded_batch
+    from afsi_gpu_b200.multigrid import ChannelMultigrid, MGOptions
+    b = seeded_batch(count, seed=0, device=device)
+    schedule, table = b.autotune(target=1e-4)
+    stream = torch.cuda.current_stream(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b.replay()
+    torch.cuda.synchronize(device)
+    e0.record(stream)
+    for _ in range(replays):
+        b.replay()
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    ms = e0.elapsed_time(e1) / replays
+    b.check()
+    # plain FP64 drop-in, one instance at a time
+    opts = MGOptions(smooth=2 if schedule.smoother == 'red-black' else 4)
+    plain = [ChannelMultigrid(g, device=device, backend='b200', smoother=schedule.smoother, options=opts)
+             for g in b.grids]
+    x = [b.x[b.point_offsets[i]:b.point_offsets[i + 1]] for i in range(count)]
+    f = [b.force[b.point_offsets[i]:b.point_offsets[i + 1]].double() for i in range(count)]
+    vel = [(b.u_in[b.u_offsets[i]:b.u_offsets[i + 1]].double().view(g.face_shape(0)),
+            b.v_in[b.v_offsets[i]:b.v_offsets[i + 1]].double().view(g.face_shape(1)))
+           for i, g in enumerate(b.grids)]
+    rhs = [r.double() for r in b.rhs]
+
+    def plain_step():
+        out = []
+        for i, g in enumerate(b.grids):
+            st = cuda_ib.prepare2d(g, x[i])
+            fields = cuda_ib.spread2d(g, f[i], st)
+            gathered = cuda_ib.gather2d(vel[i], st)
+            mg = plain[i]
+            mg.initialize(torch.zeros_like(rhs[i]), rhs[i])
+            out.append((fields, gathered, mg.advance(schedule.cycles)))
+        return out
+
+    plain_step()
+    torch.cuda.synchronize(device)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    reps = 3
+    for _ in range(reps):
+        res = plain_step()
+    p1.record(stream)
+    torch.cuda.synchronize(device)
+    plain_ms = p0.elapsed_time(p1) / reps
+
+    def rel(a, ref):
+        return float((a.double() - ref).abs().max() / ref.abs().max())
+
+    err = dict(spread=max(max(rel(b.fields(i)[c], res[i][0][c]) for c in range(2)) for i in range(count)),
+               interpolate=max(rel(b.velocities(i), res[i][1]) for i in range(count)),
+               v_cycles=max(rel(b.pressure(i), res[i][2]) for i in range(count)))
+    return dict(instances=count, points=b.total, faces=b.nu + b.nv,
+                schedule=dict(streams=schedule.streams, order=schedule.order, smoother=schedule.smoother,
+                              cycles=schedule.cycles),
+                ms_per_batch_step=ms, instance_steps_per_s=count / (ms / 1e3),
+                plain_fp64_ms_per_batch=plain_ms, plain_fp64_instance_steps_per_s=count / (plain_ms / 1e3),
+                speedup_vs_plain_fp64=plain_ms / ms, error_vs_fp64=err,
+                max_residual_reduction=max(b.residual_reduction()), graph_launches=b.graph_launches,
+                autotune=table)
+
+
+def serving_form_row(device, count=400):
+    """Serving form: `count` requests of the serving mix (50% 2D 256x64 with
+    20k points, 35% 3D 32^3-64^3 with 50k-400k points, 15% 3D 96^3 with 800k
+    points; Poisson arrivals at 2000/s, seeded), each a full FP64 step
+    (prepare, spread, interpolate, pressure solve to 1e-10) on resident
+    states, admitted under a 150 GB budget.  8 worker slots (continuous
+    batching) against 1 slot (requests one at a time, the plain drop-in)."""
+    from afsi_gpu_b200.serving import Server, mix
+    reqs = mix(count, rate=2000., seed=0)
+    out = {}
+    for slots in (8, 1):
+        server = Server(device=device, slots=slots)
+        server.warm(reqs)
+        server.serve(reqs[:16])  # warm-up
+        report, _ = server.serve(reqs)
+        out[f'slots_{slots}'] = report
+    out['speedup_vs_one_slot'] = out['slots_8']['steps_per_s'] / out['slots_1']['steps_per_s']
+    return out
+
+
 def load_traffic():
     path = ROOT / 'profiles' / 'traffic.json'
     try:
@@ -481,6 +576,8 @@ def run_b200(args):
             errors = oracle_errors(step, X, coef, vel, outputs, outs[-1].numpy())
         mass = mass_pcg_row(X, cells, device, pk['hbm_gbs'])
         forms = mg_forms_row(grid, rhs, device)
+        batch = batch_form_row(device)
+        serving = serving_form_row(device)
         step_ms = np.array([ev[0].elapsed_time(ev[4]) for ev in phases])
         line = dict(
             metric=METRIC, value=world * args.steps / elapsed, unit='steps/s', n_gpus=world, steps=args.steps,
@@ -506,6 +603,8 @@ def run_b200(args):
             oracle_error=errors,
             mass_pcg=mass,
             mg_forms=forms,
+            batch_form=batch,
+            serving_form=serving,
             cpu_baseline=cpu)
         print(json.dumps(line, default=_json))
     if dist:
