@@ -357,6 +357,12 @@ def serving_form_row(device, count=400):
         report, _ = server.serve(reqs)
         out[f'slots_{slots}'] = report
     out['speedup_vs_one_slot'] = out['slots_8']['steps_per_s'] / out['slots_1']['steps_per_s']
+    # 2000 req/s saturates the GPU (latency is queueing); the same mix below
+    # saturation shows the step latency itself
+    rate = .5 * out['slots_8']['steps_per_s']
+    server = Server(device=device, slots=8)
+    report, _ = server.serve(mix(count // 2, rate=rate, seed=1))
+    out['slots_8_below_saturation'] = dict(report, arrival_rate=rate)
     return out
 
 
