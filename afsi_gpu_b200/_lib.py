@@ -127,6 +127,14 @@ _SIGNATURES = {
                                  c_int64, c_int64, c_void_p, c_int32, c_void_p],
     'afsi_b200_batch2d_gather': [c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_int64, c_void_p,
                                  c_void_p, c_int32, c_void_p],
+    'afsi_b200_stokes_partial_blocks': [P_I64],
+    'afsi_b200_helmholtz_initialize': [ctypes.POINTER(c_void_p), c_void_p, ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p), c_void_p, P_I64, P_F64, c_int32, c_void_p],
+    'afsi_b200_helmholtz_sweep': [ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p), c_void_p, P_I64, P_F64, c_int32, c_void_p],
+    'afsi_b200_stokes_start_partial': [ctypes.POINTER(c_void_p), c_void_p, c_void_p, P_I64, c_int32, c_void_p],
+    'afsi_b200_stokes_residual_partial': [ctypes.POINTER(c_void_p), c_void_p, ctypes.POINTER(c_void_p), c_void_p, c_void_p, c_void_p, P_I64, c_int32,
+                                          c_void_p],
+    'afsi_b200_pressure_input_partial': [c_void_p, c_void_p, c_int64, c_void_p, c_int32, c_void_p],
+    'afsi_b200_pressure_norm_partial': [c_void_p, c_void_p, c_void_p, c_void_p, P_I64, c_int32, c_void_p],
     'afsi_b200_pcg_scratch_bytes': [],
     'afsi_b200_pcg_begin': [ctypes.POINTER(PCGPlan), c_void_p],
     'afsi_b200_pcg_iterations': [ctypes.POINTER(PCGPlan), c_int32, c_void_p],
@@ -137,7 +145,8 @@ _SIGNATURES = {
 _RESTYPES = {'afsi_b200_last_error': ctypes.c_char_p, 'afsi_b200_mg_scratch_bytes': ctypes.c_int64,
              'afsi_b200_launch_count': ctypes.c_int64, 'afsi_b200_mg_sync_bytes': ctypes.c_int64,
              'afsi_b200_p1_plan_scratch_bytes': ctypes.c_int64, 'afsi_b200_hash_csr_scratch_bytes': ctypes.c_int64,
-             'afsi_b200_pcg_scratch_bytes': ctypes.c_int64, 'afsi_b200_mg_refine_scratch_bytes': ctypes.c_int64}
+             'afsi_b200_pcg_scratch_bytes': ctypes.c_int64, 'afsi_b200_mg_refine_scratch_bytes': ctypes.c_int64,
+             'afsi_b200_stokes_partial_blocks': ctypes.c_int64}
 
 
 def exported_symbols():
@@ -193,6 +202,11 @@ def stream(device=None):
 def doubles(values):
     values = [float(v) for v in values]
     return (ctypes.c_double * len(values))(*values)
+
+
+def pointers(tensors):
+    """Device pointers of three face arrays as a `void* const*` argument."""
+    return (c_void_p * 3)(*[t.data_ptr() for t in tensors])
 
 
 def int64s(values):

@@ -15,6 +15,11 @@ time:
   ``mac2d._triton_mg`` when they are built (``mac/mg_workspace.py:36-47``,
   ``mac2d/mg_workspace.py:28-40``); those modules are replaced by shims whose
   ``TritonKernels`` is the B200 kernel object;
+* the CN Helmholtz kernel object and the Stokes reductions, which
+  ``HelmholtzWorkspace`` and ``StokesWorkspace`` import when they are built or
+  measure (``mac/helmholtz.py:44-47``, ``mac/stokes_workspace.py:50,86,97``):
+  ``mac._triton_helmholtz`` and ``mac._triton_stokes`` are replaced by shims
+  holding the B200 ``HelmholtzKernels`` and partial functions;
 * the consistent-mass solvers: ``MassSolver`` as bound in
   ``mac.compact_transfer`` and ``mac2d.transfer`` (imported there at module
   load, ``mac/compact_transfer.py:7``, ``mac2d/transfer.py:10-11``),
@@ -62,6 +67,19 @@ def install():
         target = importlib.import_module(module)
         _saved.setdefault(('attr', module, name), getattr(target, name))
         setattr(target, name, getattr(mass, name))
+    from . import helmholtz
+    for module, names in (('afsi_torch.mac._triton_helmholtz', ('HelmholtzKernels',)),
+                          ('afsi_torch.mac._triton_stokes', ('start_partial', 'residual_partial',
+                                                            'pressure_input_partial', 'pressure_norm_partial'))):
+        _saved.setdefault(('module', module), sys.modules.get(module))
+        shim = types.ModuleType(module)
+        shim.__doc__ = f'B200 kernels standing in for {module}'
+        for name in names:
+            setattr(shim, name, getattr(helmholtz, name))
+        sys.modules[module] = shim
+        parent, _, leaf = module.rpartition('.')
+        if parent in sys.modules:
+            setattr(sys.modules[parent], leaf, shim)
     for module, bc in (('afsi_torch.mac._triton_mg', 'neumann'), ('afsi_torch.mac2d._triton_mg', 'channel')):
         _saved.setdefault(('module', module), sys.modules.get(module))
         sys.modules[module] = _shim(module, bc)

@@ -378,6 +378,45 @@ int32_t afsi_b200_vector_stats(const void* x, int64_t n, double* stats_out, void
 int32_t afsi_b200_subtract_mean(void* x, int64_t n, const double* stats, int32_t dtype,
     afsi_stream_t stream);
 
+/* ---- CN Helmholtz sweeps and Stokes residual reductions --------------------
+ * The kernels of the Stokes FGMRES preconditioner and its checks on the 3D MAC
+ * grid of `shape` cells (nx, ny, nz).  Face arrays come as three pointers
+ * (u (nx+1,ny,nz), v (nx,ny+1,nz), w (nx,ny,nz+1)), all in `dtype`.
+ * afsi_b200_helmholtz_initialize (HelmholtzKernels.initialize,
+ *   mac/_triton_helmholtz.py:6-31,64-70): rhs = b - param[1] G p on interior
+ *   component-normal faces (p may be NULL: no pressure term), 0 on the walls;
+ *   u = rhs / diag.  spacing: host double[3].
+ * afsi_b200_helmholtz_sweep (HelmholtzKernels.sweep, :34-61,72-77): out = u +
+ *   (rhs - u + param[0] L u)/diag with odd wall ghosts, 0 on the walls.
+ *   spacing_squared: host double[3].
+ * Stokes partials, one row per 256 cells (afsi_b200_stokes_partial_blocks):
+ * afsi_b200_stokes_start_partial (start_partial, mac/_triton_stokes.py:16-27):
+ *   out (blocks,3) = [sum b.b over the cells' low faces, sum p, all p finite];
+ * afsi_b200_stokes_residual_partial (residual_partial, :58-84): residual
+ *   (nx,ny,nz) = -coef[2] D u; out (blocks,2) = [sum |momentum residual|^2,
+ *   sum (D u)^2]; coefficients (device, 9) = [alpha, dt/rho, rho/dt, 1/h (3),
+ *   1/h^2 (3)] (mac/stokes_workspace.py:66-77);
+ * afsi_b200_pressure_input_partial (:106-114): out (blocks,5) = [sum rhs,
+ *   sum |rhs|, sum p, all rhs finite, all p finite] over n cells;
+ * afsi_b200_pressure_norm_partial (:117-132): out (blocks,2) = [sum rhs^2,
+ *   sum (rhs - A p)^2], A the Neumann operator; spacing_squared (device, 3). */
+int64_t afsi_b200_stokes_partial_blocks(const int64_t* shape);
+int32_t afsi_b200_helmholtz_initialize(const void* const* b, const void* p, const void* const* diag,
+    void* const* rhs, void* const* u, const void* param, const int64_t* shape, const double* spacing,
+    int32_t dtype, afsi_stream_t stream);
+int32_t afsi_b200_helmholtz_sweep(const void* const* u, const void* const* rhs, const void* const* diag,
+    void* const* out, const void* param, const int64_t* shape, const double* spacing_squared, int32_t dtype,
+    afsi_stream_t stream);
+int32_t afsi_b200_stokes_start_partial(const void* const* b, const void* p, void* out, const int64_t* shape,
+    int32_t dtype, afsi_stream_t stream);
+int32_t afsi_b200_stokes_residual_partial(const void* const* u, const void* p, const void* const* b,
+    void* residual, void* out, const void* coefficients, const int64_t* shape, int32_t dtype,
+    afsi_stream_t stream);
+int32_t afsi_b200_pressure_input_partial(const void* rhs, const void* p, int64_t n, void* out, int32_t dtype,
+    afsi_stream_t stream);
+int32_t afsi_b200_pressure_norm_partial(const void* rhs, const void* p, void* out, const void* spacing_squared,
+    const int64_t* shape, int32_t dtype, afsi_stream_t stream);
+
 /* ---- batched 2D transfers (the batching form) ------------------------------
  * Many independent 2D channel instances (TriangleTransfer, mac2d/transfer.py:
  * 61-127, one per instance in the reference) in one launch per operation.

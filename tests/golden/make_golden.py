@@ -345,6 +345,64 @@ def quadrature():
     save('quadrature', **arrays)
 
 
+def stokes():
+    """CN Helmholtz kernels (the reference's CPU kernel object) and the Stokes
+    residual / pressure metrics by the reference grid operators, on a small
+    anisotropic MAC grid with wall-free (zero normal wall) face fields."""
+    from afsi_torch.mac.helmholtz import TorchHelmholtzKernels
+    from afsi_torch.mac.grid import gradient, divergence, velocity_laplacian, zero_normal, slab
+    g = torch.Generator().manual_seed(15)
+    grid = MACGrid((10, 8, 6), (1.0, .9, .7))
+    faces = lambda: zero_normal(tuple(torch.randn(grid.face_shape(c), generator=g, dtype=torch.float64)
+                                      for c in range(3)))
+    b, u = faces(), faces()
+    p = torch.randn(grid.shape, generator=g, dtype=torch.float64)
+    alpha, scale = .013, .7
+    s2 = 2 * alpha * sum(1 / h ** 2 for h in grid.spacing)
+    diagonal = []
+    for c in range(3):
+        d = torch.full(grid.face_shape(c), 1 + s2, dtype=torch.float64)
+        for axis, h in enumerate(grid.spacing):
+            if axis != c:
+                d[slab(axis, 0, 1)] += alpha / h ** 2
+                d[slab(axis, -1, None)] += alpha / h ** 2
+        d[slab(c, 0, 1)] = 1.
+        d[slab(c, -1, None)] = 1.
+        diagonal.append(d)
+    k = TorchHelmholtzKernels()
+    params = torch.tensor([alpha, scale], dtype=torch.float64)
+    out = dict(shape=grid.shape, lengths=grid.lengths, alpha=alpha, scale=scale, p=p)
+    for c in range(3):
+        out[f'b{c}'], out[f'u{c}'], out[f'd{c}'] = b[c], u[c], diagonal[c]
+    for tag, pp in (('p', p), ('nop', None)):
+        rhs = tuple(torch.empty_like(v) for v in b)
+        first = tuple(torch.empty_like(v) for v in b)
+        k.initialize(b, pp, diagonal, rhs, first, params, grid)
+        second = tuple(torch.empty_like(v) for v in b)
+        cur, nxt = first, second
+        for c in range(3):
+            out[f'{tag}_rhs{c}'], out[f'{tag}_init{c}'] = rhs[c].clone(), first[c].clone()
+        for sweep in range(3):
+            k.sweep(cur, rhs, diagonal, nxt, params, grid)
+            cur, nxt = nxt, cur
+        for c in range(3):
+            out[f'{tag}_sweep3_{c}'] = cur[c]
+    # Stokes residual (StokesWorkspace.measure, CPU branch) with dt/rho = scale
+    gp = gradient(p, grid.spacing)
+    momentum = tuple(v - alpha * velocity_laplacian(v, c, grid.spacing) + scale * gq - r
+                     for c, (v, gq, r) in enumerate(zip(u, gp, b)))
+    div = divergence(u, grid.spacing)
+    out['norms'] = torch.stack((torch.sqrt(sum(v.square().sum() for v in momentum)), torch.linalg.vector_norm(div)))
+    out['residual'] = -(1 / scale) * div
+    out['start'] = torch.stack((torch.sqrt(sum(v.square().sum() for v in b)), p.mean(),
+                                torch.isfinite(p).all().double()))
+    rhs = torch.randn(grid.shape, generator=g, dtype=torch.float64)
+    out['prhs'] = rhs
+    out['pmetrics'] = torch.stack((rhs.sum(), rhs.abs().sum(), p.sum(), torch.linalg.vector_norm(rhs),
+                                   torch.linalg.vector_norm(rhs - negative_laplacian(p, grid.spacing))))
+    save('stokes', **out)
+
+
 if __name__ == '__main__':
     peskin()
     compact3d()
@@ -357,3 +415,4 @@ if __name__ == '__main__':
     p1csr()
     dirichlet()
     mass()
+    stokes()

@@ -40,6 +40,10 @@ def test_install_rebinds_ib_operators_and_mg_kernels(afsi_torch):
         from afsi_gpu_b200 import mass
         assert ref_compact.MassSolver is mass.MassSolver and ref_graph.GraphMassSolver is mass.GraphMassSolver
         assert ref_2d.MassSolver is mass.MassSolver and ref_2d.GraphMassSolver is mass.GraphMassSolver
+        from afsi_gpu_b200 import helmholtz
+        from afsi_torch.mac._triton_helmholtz import HelmholtzKernels as HK
+        from afsi_torch.mac._triton_stokes import residual_partial as rp
+        assert HK is helmholtz.HelmholtzKernels and rp is helmholtz.residual_partial
     finally:
         dropin.uninstall()
     assert ref_ib.compact_gather is original

@@ -1,0 +1,125 @@
+"""CN Helmholtz sweeps and Stokes residual reductions (csrc/stokes.cu) against
+the reference's CPU kernel object and grid operators (B200).
+
+Tolerances: Helmholtz fields bitwise in FP64 (the kernels keep the
+reference's operation order without contraction); FP32 2e-6 of the field
+scale. Reductions 1e-12 relative (block sums in another order; the blocked
+momentum residual multiplies by 1/h^2 as the reference's blocked kernel does,
+where its CPU branch divides by h^2).
+"""
+import numpy as np
+import pytest
+import torch
+from conftest import golden
+from oracle import stokes as ostokes
+from afsi_gpu_b200.grid import MACGrid
+from afsi_gpu_b200.helmholtz import (HelmholtzKernels, HelmholtzWorkspace, pressure_input_partial,
+                                     pressure_norm_partial, residual_partial, start_partial)
+
+pytestmark = pytest.mark.gpu
+DEV = 'cuda'
+
+
+def _case(dtype=torch.float64):
+    g = golden('stokes')
+    grid = MACGrid(tuple(int(n) for n in g['shape']), tuple(float(x) for x in g['lengths']))
+    t = lambda a: torch.as_tensor(np.asarray(a), device=DEV, dtype=dtype)
+    faces = lambda name: tuple(t(g[f'{name}{c}']) for c in range(3))
+    return g, grid, t, faces
+
+
+@pytest.mark.parametrize('dtype', [torch.float64, torch.float32])
+def test_helmholtz_kernels_match_reference(dtype):
+    g, grid, t, faces = _case(dtype)
+    k = HelmholtzKernels()
+    b, d = faces('b'), faces('d')
+    params = t([g['alpha'], g['scale']])
+    for tag, p in (('p', t(g['p'])), ('nop', None)):
+        rhs = tuple(torch.empty_like(v) for v in b)
+        cur = tuple(torch.empty_like(v) for v in b)
+        nxt = tuple(torch.empty_like(v) for v in b)
+        k.initialize(b, p, d, rhs, cur, params, grid)
+        for c in range(3):
+            for got, ref in ((rhs[c], g[f'{tag}_rhs{c}']), (cur[c], g[f'{tag}_init{c}'])):
+                if dtype == torch.float64:
+                    assert np.array_equal(got.cpu().numpy(), ref)
+                else:
+                    np.testing.assert_allclose(got.double().cpu().numpy(), ref, rtol=2e-6,
+                                               atol=2e-6 * np.abs(ref).max())
+        for _ in range(3):
+            k.sweep(cur, rhs, d, nxt, params, grid)
+            cur, nxt = nxt, cur
+        for c in range(3):
+            ref = g[f'{tag}_sweep3_{c}']
+            if dtype == torch.float64:
+                assert np.array_equal(cur[c].cpu().numpy(), ref)
+            else:
+                np.testing.assert_allclose(cur[c].double().cpu().numpy(), ref, rtol=2e-6,
+                                           atol=2e-6 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize('backend', ['graph', 'b200'])
+def test_helmholtz_workspace_solves_match_reference(backend):
+    g, grid, t, faces = _case()
+    ws = HelmholtzWorkspace(grid, faces('d'), backend=backend)
+    for _ in range(2):  # capture on the first solve, replay on the second
+        u = ws.solve(faces('b'), alpha=float(g['alpha']), count=3, pressure=t(g['p']),
+                     pressure_scale=float(g['scale']))
+        for c in range(3):
+            assert np.array_equal(u[c].cpu().numpy(), g[f'p_sweep3_{c}'])
+    u = ws.solve(faces('b'), alpha=float(g['alpha']), count=3)
+    for c in range(3):
+        assert np.array_equal(u[c].cpu().numpy(), g[f'nop_sweep3_{c}'])
+    assert ws.summary()['solves'] == 3
+    with pytest.raises(ValueError, match='positive fixed Helmholtz iteration count'):
+        ws.solve(faces('b'), alpha=.1, count=0)
+
+
+def test_stokes_partials_reduce_to_reference_metrics():
+    g, grid, t, faces = _case()
+    n = int(np.prod(grid.shape))
+    blocks = (n + 255) // 256
+    p = t(g['p'])
+    part = torch.empty((blocks, 3), device=DEV, dtype=torch.float64)
+    start_partial(faces('b'), p, part, grid.shape)
+    tot = part.sum(0)
+    got = torch.stack((tot[0].sqrt(), tot[1] / n, (part[:, 2].amin() > 0).double())).cpu().numpy()
+    np.testing.assert_allclose(got, g['start'], rtol=1e-12, atol=1e-15)
+    alpha, scale = float(g['alpha']), float(g['scale'])
+    coef = t([alpha, scale, 1 / scale, *(1 / h for h in grid.spacing), *(1 / (h * h) for h in grid.spacing)])
+    residual = torch.empty(grid.shape, device=DEV, dtype=torch.float64)
+    part2 = torch.empty((blocks, 2), device=DEV, dtype=torch.float64)
+    residual_partial(faces('u'), p, faces('b'), residual, part2, grid.shape, coef)
+    np.testing.assert_allclose(part2.sum(0).sqrt().cpu().numpy(), g['norms'], rtol=1e-12)
+    np.testing.assert_allclose(residual.cpu().numpy(), g['residual'], rtol=1e-12,
+                               atol=1e-12 * np.abs(g['residual']).max())
+    rhs = t(g['prhs'])
+    inputs = torch.empty((blocks, 5), device=DEV, dtype=torch.float64)
+    pressure_input_partial(rhs, p, inputs)
+    sums = inputs[:, :3].sum(0).cpu().numpy()
+    np.testing.assert_allclose(sums, g['pmetrics'][:3], rtol=1e-12, atol=1e-12)
+    assert inputs[:, 3:].amin().item() == 1
+    norms = torch.empty((blocks, 2), device=DEV, dtype=torch.float64)
+    pressure_norm_partial(rhs, p, norms, t([h * h for h in grid.spacing]))
+    np.testing.assert_allclose(norms.sum(0).sqrt().cpu().numpy(), g['pmetrics'][3:], rtol=1e-12)
+    bad = p.clone()
+    bad[1, 2, 3] = float('inf')
+    pressure_input_partial(rhs, bad, inputs)
+    assert inputs[:, 4].amin().item() == 0 and inputs[:, 3].amin().item() == 1
+
+
+def test_helmholtz_on_a_64_cube_against_the_oracle():
+    """A larger grid (several blocks per face lattice) against the oracle."""
+    grid = MACGrid((64, 48, 40), (1., .75, .625))
+    rng = np.random.default_rng(2)
+    b = ostokes.zero_normal([rng.standard_normal(grid.face_shape(c)) for c in range(3)])
+    d = [1.5 + rng.random(grid.face_shape(c)) for c in range(3)]
+    p = rng.standard_normal(grid.shape)
+    rhs_ref, u_ref = ostokes.helmholtz_initialize(b, p, d, .3, grid.spacing)
+    for _ in range(4):
+        u_ref = ostokes.helmholtz_sweep(u_ref, rhs_ref, d, .02, grid.spacing)
+    ws = HelmholtzWorkspace(grid, tuple(torch.as_tensor(x, device=DEV) for x in d))
+    u = ws.solve(tuple(torch.as_tensor(x, device=DEV) for x in b), alpha=.02, count=4,
+                 pressure=torch.as_tensor(p, device=DEV), pressure_scale=.3)
+    for c in range(3):
+        assert np.array_equal(u[c].cpu().numpy(), u_ref[c])

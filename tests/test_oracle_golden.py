@@ -242,3 +242,30 @@ def test_mass_pcg_matches_reference_solves():
         assert it == int(g[f'{name}_iterations'])
         assert res <= tol and abs(tol - float(g[f'{name}_tolerance'])) <= 1e-12 * tol
         np.testing.assert_allclose(x, g[f'{name}_x'], rtol=1e-10, atol=1e-12 * np.abs(g[f'{name}_x']).max())
+
+
+def test_stokes_oracle_matches_reference_kernels():
+    """oracle/stokes.py against the reference's CPU Helmholtz kernel object
+    (mac/helmholtz.py:14-28) and its Stokes / pressure reductions: Helmholtz
+    fields bitwise (same operation order), norms 1e-13 relative."""
+    from oracle import stokes
+    g = golden('stokes')
+    spacing = tuple(float(L) / int(n) for L, n in zip(g['lengths'], g['shape']))
+    b = [g[f'b{c}'] for c in range(3)]
+    d = [g[f'd{c}'] for c in range(3)]
+    u = [g[f'u{c}'] for c in range(3)]
+    for tag, p in (('p', g['p']), ('nop', None)):
+        rhs, cur = stokes.helmholtz_initialize(b, p, d, float(g['scale']), spacing)
+        for c in range(3):
+            assert np.array_equal(rhs[c], g[f'{tag}_rhs{c}']) and np.array_equal(cur[c], g[f'{tag}_init{c}'])
+        for _ in range(3):
+            cur = stokes.helmholtz_sweep(cur, rhs, d, float(g['alpha']), spacing)
+        for c in range(3):
+            assert np.array_equal(cur[c], g[f'{tag}_sweep3_{c}'])
+    norms, residual = stokes.stokes_measure(u, g['p'], b, float(g['alpha']), float(g['scale']), spacing)
+    np.testing.assert_allclose(norms, g['norms'], rtol=1e-13)
+    np.testing.assert_allclose(residual, g['residual'], rtol=1e-13, atol=1e-13 * np.abs(g['residual']).max())
+    np.testing.assert_allclose(stokes.stokes_start(b, g['p']), g['start'], rtol=1e-13, atol=1e-15)
+    m = stokes.pressure_metrics(g['prhs'], g['p'], spacing)
+    np.testing.assert_allclose(m[[0, 1, 2, 5, 6]], g['pmetrics'], rtol=1e-12, atol=1e-12)
+    assert m[3] == 1 and m[4] == 1
