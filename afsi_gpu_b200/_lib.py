@@ -127,6 +127,13 @@ _SIGNATURES = {
                                  c_int64, c_int64, c_void_p, c_int32, c_void_p],
     'afsi_b200_batch2d_gather': [c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_int64, c_void_p,
                                  c_void_p, c_int32, c_void_p],
+    'afsi_b200_cache_scratch_bytes': [c_int64] * 5,
+    'afsi_b200_cache_new_keys': [c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_int64, c_void_p, c_void_p,
+                                 c_void_p, c_void_p, c_int64, c_void_p],
+    'afsi_b200_cache_merge': [c_void_p, c_void_p, c_int64] + [c_void_p] * 4 + [c_int64, c_void_p, c_void_p, c_int64,
+                                                                             c_int64, c_int64] +
+                             [c_void_p] * 9 + [c_void_p, c_int64, c_int32, c_void_p],
+    'afsi_b200_cache_values': [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_int32, c_void_p],
     'afsi_b200_stokes_partial_blocks': [P_I64],
     'afsi_b200_helmholtz_initialize': [ctypes.POINTER(c_void_p), c_void_p, ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p), c_void_p, P_I64, P_F64, c_int32, c_void_p],
     'afsi_b200_helmholtz_sweep': [ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p), c_void_p, P_I64, P_F64, c_int32, c_void_p],
@@ -146,7 +153,7 @@ _RESTYPES = {'afsi_b200_last_error': ctypes.c_char_p, 'afsi_b200_mg_scratch_byte
              'afsi_b200_launch_count': ctypes.c_int64, 'afsi_b200_mg_sync_bytes': ctypes.c_int64,
              'afsi_b200_p1_plan_scratch_bytes': ctypes.c_int64, 'afsi_b200_hash_csr_scratch_bytes': ctypes.c_int64,
              'afsi_b200_pcg_scratch_bytes': ctypes.c_int64, 'afsi_b200_mg_refine_scratch_bytes': ctypes.c_int64,
-             'afsi_b200_stokes_partial_blocks': ctypes.c_int64}
+             'afsi_b200_stokes_partial_blocks': ctypes.c_int64, 'afsi_b200_cache_scratch_bytes': ctypes.c_int64}
 
 
 def exported_symbols():

@@ -25,6 +25,8 @@
 // number of entries and the validity flags land in a device info word.
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+#include <algorithm>
 #include "common.cuh"
 
 namespace afsi {
@@ -520,4 +522,400 @@ extern "C" int32_t afsi_b200_csr_spmv(const int64_t* crow, const int64_t* col, c
         }
     });
     return launched("csr_spmv");
+}
+
+// ------------------------------------------------------------ cached pattern
+//
+// finish_cached_component (mac/cached_transfer_assembly.py:97-175) on the
+// device.  A cached P1 transfer keeps, per component, the table slots of its
+// CSR entries in key order, the transpose order, and the row pointers of B and
+// B^T.  When new quadrature contributions miss the cached keys they are
+// inserted into the table and only the new keys are sorted and merged into
+// both orders: every old and new entry gets one merge position from a binary
+// search in the other (disjoint, individually sorted) array, as the reference
+// does with searchsorted, and the row pointers grow by the prefix counts of
+// the new rows and columns alone.  The first build is the same merge with no
+// old pattern and the table's occupied keys (with their slots) as the new keys.
+//
+// Two launches sequences with one host read between them (the reference
+// reads the number of new keys too):
+//   afsi_b200_cache_new_keys  sorted unique missing keys absent from the
+//                             pattern (or, with no pattern, the occupied table
+//                             keys with their slots) and their count;
+//   afsi_b200_cache_merge     the merged slots, transpose order, CSR indices,
+//                             values and transpose values.
+
+namespace afsi {
+
+__device__ __forceinline__ int64_t lower_bound(const int64_t* a, int64_t n, int64_t v) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (a[mid] < v)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int64_t upper_bound(const int64_t* a, int64_t n, int64_t v) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (a[mid] <= v)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void cache_gather_keys_kernel(const int64_t* __restrict__ table, const int64_t* __restrict__ slots,
+                                         int64_t n, int64_t* __restrict__ out) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        out[i] = table[slots[i]];
+}
+
+// flags[j] = sorted[j] is the first of its run and not an old key.
+__global__ void cache_flag_new_kernel(const int64_t* __restrict__ sorted, int64_t m, const int64_t* __restrict__ old,
+                                      int64_t nnz, uint8_t* __restrict__ flags) {
+    for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < m; j += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t k = sorted[j];
+        const bool first = j == 0 || sorted[j - 1] != k;
+        const int64_t at = lower_bound(old, nnz, k);
+        flags[j] = first && !(at < nnz && old[at] == k);
+    }
+}
+
+// Occupied table keys (others become `sentinel`, which sorts after every
+// key) with their slot indices; *count += occupied slots (one atomic per warp).
+__global__ void cache_occupied_kernel(const int64_t* __restrict__ table, int64_t capacity, int64_t sentinel,
+                                      int64_t* __restrict__ keys, int64_t* __restrict__ index,
+                                      unsigned long long* count) {
+    for (int64_t i0 = int64_t(blockIdx.x) * blockDim.x; i0 < capacity; i0 += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = i0 + threadIdx.x;
+        const bool occupied = i < capacity && table[i] >= 0;
+        if (i < capacity) {
+            keys[i] = occupied ? table[i] : sentinel;
+            index[i] = i;
+        }
+        const unsigned ballot = __ballot_sync(0xffffffffu, occupied);
+        if ((threadIdx.x & 31) == 0 && ballot) atomicAdd(count, (unsigned long long)__popc(ballot));
+    }
+}
+
+// Merge positions of the old and new keys; the merged keys and slots (new
+// slots from `new_slots`, or found in the table by linear probing).
+__global__ void cache_merge_keys_kernel(const int64_t* __restrict__ old_keys, const int64_t* __restrict__ old_slots,
+                                        int64_t nnz, const int64_t* __restrict__ new_keys,
+                                        const int64_t* __restrict__ new_slots, int64_t k,
+                                        const int64_t* __restrict__ table, int64_t capacity,
+                                        int64_t* __restrict__ keys_out, int64_t* __restrict__ slots_out,
+                                        int64_t* __restrict__ old_pos, int64_t* __restrict__ new_pos,
+                                        int32_t* status) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < nnz + k;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        if (t < nnz) {
+            const int64_t p = t + upper_bound(new_keys, k, old_keys[t]);
+            keys_out[p] = old_keys[t];
+            slots_out[p] = old_slots[t];
+            old_pos[t] = p;
+        } else {
+            const int64_t j = t - nnz, key = new_keys[j];
+            const int64_t p = j + lower_bound(old_keys, nnz, key);
+            int64_t slot = -1;
+            if (new_slots) {
+                slot = new_slots[j];
+            } else {
+                uint64_t s = hash_bucket(key, capacity);
+                for (int attempt = 0; attempt < 128; ++attempt) {  // the insertion probe bound
+                    if (table[s] == key) {
+                        slot = int64_t(s);
+                        break;
+                    }
+                    s = (s + 1) & uint64_t(capacity - 1);
+                }
+                if (slot < 0) {
+                    flag(status, AFSI_FLAG_OVERFLOW);
+                    slot = 0;
+                }
+            }
+            keys_out[p] = key;
+            slots_out[p] = slot;
+            new_pos[j] = p;
+        }
+    }
+}
+
+// counts[key / nf] += 1 (rows) and tcounts[key % nf] += 1 (columns).
+__global__ void cache_count_kernel(const int64_t* __restrict__ keys, int64_t k, int64_t nf, int64_t rows,
+                                   unsigned long long* __restrict__ counts, unsigned long long* __restrict__ tcounts,
+                                   int32_t* status) {
+    for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < k; j += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t key = keys[j];
+        if (key < 0 || key >= nf * rows) {
+            flag(status, AFSI_FLAG_INDEX);
+            continue;
+        }
+        atomicAdd(counts + key / nf, 1ull);
+        atomicAdd(tcounts + key % nf, 1ull);
+    }
+}
+
+// out[r] = base[r] + add[r] (base may be null).
+__global__ void cache_pointers_kernel(const int64_t* __restrict__ base, const int64_t* __restrict__ add, int64_t n,
+                                      int64_t* __restrict__ out) {
+    for (int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += int64_t(gridDim.x) * blockDim.x)
+        out[r] = (base ? base[r] : 0) + add[r];
+}
+
+// Reverse (column-major) keys col * rows + row: of the old entries in
+// transpose order, and of the new keys with their index.
+__global__ void cache_reverse_kernel(const int64_t* __restrict__ old_keys, const int64_t* __restrict__ old_order,
+                                     int64_t nnz, const int64_t* __restrict__ new_keys, int64_t k, int64_t nf,
+                                     int64_t rows, int64_t* __restrict__ old_rk, int64_t* __restrict__ new_rk,
+                                     int64_t* __restrict__ new_index) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < nnz + k;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        if (t < nnz) {
+            const int64_t key = old_keys[old_order[t]];
+            old_rk[t] = (key % nf) * rows + key / nf;
+        } else {
+            const int64_t j = t - nnz, key = new_keys[j];
+            new_rk[j] = (key % nf) * rows + key / nf;
+            new_index[j] = j;
+        }
+    }
+}
+
+__global__ void cache_merge_transpose_kernel(const int64_t* __restrict__ old_rk, const int64_t* __restrict__ old_order,
+                                             const int64_t* __restrict__ old_pos, int64_t nnz,
+                                             const int64_t* __restrict__ new_rk, const int64_t* __restrict__ new_order,
+                                             const int64_t* __restrict__ new_pos, int64_t k,
+                                             int64_t* __restrict__ order_out) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < nnz + k;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        if (t < nnz) {
+            order_out[t + upper_bound(new_rk, k, old_rk[t])] = old_pos[old_order[t]];
+        } else {
+            const int64_t q = t - nnz;
+            order_out[q + lower_bound(old_rk, nnz, new_rk[q])] = new_pos[new_order[q]];
+        }
+    }
+}
+
+template <class T>
+__global__ void cache_finish_kernel(const int64_t* __restrict__ keys, const int64_t* __restrict__ slots,
+                                    const int64_t* __restrict__ order, int64_t n, int64_t nf, int64_t rows,
+                                    const T* __restrict__ table_values, int64_t* __restrict__ columns,
+                                    int64_t* __restrict__ tcolumns, T* __restrict__ values, T* __restrict__ reverse,
+                                    int32_t* status) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t key = keys[i];
+        if (key < 0 || key >= nf * rows) flag(status, AFSI_FLAG_INDEX);
+        columns[i] = key % nf;
+        const T v = table_values[slots[i]];
+        if (!isfinite(v)) flag(status, AFSI_FLAG_SUPPORT);
+        values[i] = v;
+        const int64_t o = order[i];
+        tcolumns[i] = keys[o] / nf;
+        reverse[i] = table_values[slots[o]];
+    }
+}
+
+}  // namespace afsi
+
+namespace {
+
+unsigned cache_grid(int64_t n) {
+    const int64_t b = (n + 255) / 256;
+    return unsigned(b < 1 ? 1 : (b < 148 * 32 ? b : 148 * 32));
+}
+
+int key_bits(int64_t limit) {
+    int bits = 1;
+    while (bits < 63 && (int64_t(1) << bits) <= limit) ++bits;
+    return bits;
+}
+
+struct Carve {
+    unsigned char* base;
+    size_t used = 0, size;
+    template <class T>
+    T* take(int64_t n) {
+        used = (used + 255) & ~size_t(255);
+        T* p = reinterpret_cast<T*>(base + used);
+        used += size_t(n > 0 ? n : 1) * sizeof(T);
+        return p;
+    }
+};
+
+size_t cub_bytes(int64_t n_sort, int64_t n_scan) {
+    size_t a = 0, b = 0, c = 0, d = 0;
+    const int64_t ns = n_sort > 0 ? n_sort : 1, nc = n_scan > 0 ? n_scan : 1;
+    cub::DeviceRadixSort::SortPairs(nullptr, a, static_cast<const int64_t*>(nullptr), static_cast<int64_t*>(nullptr),
+                                    static_cast<const int64_t*>(nullptr), static_cast<int64_t*>(nullptr), ns);
+    cub::DeviceSelect::Flagged(nullptr, b, static_cast<const int64_t*>(nullptr), static_cast<const uint8_t*>(nullptr),
+                               static_cast<int64_t*>(nullptr), static_cast<int64_t*>(nullptr), ns);
+    cub::DeviceScan::ExclusiveSum(nullptr, c, static_cast<const unsigned long long*>(nullptr),
+                                  static_cast<unsigned long long*>(nullptr), nc);
+    cub::DeviceRadixSort::SortKeys(nullptr, d, static_cast<const int64_t*>(nullptr), static_cast<int64_t*>(nullptr),
+                                   ns);
+    return std::max(std::max(a, b), std::max(c, d));
+}
+
+}  // namespace
+
+extern "C" int64_t afsi_b200_cache_scratch_bytes(int64_t capacity, int64_t nnz_old, int64_t missing, int64_t rows,
+                                                 int64_t nf) {
+    if (capacity < 0 || nnz_old < 0 || missing < 0 || rows < 1 || nf < 1) return -1;
+    const int64_t k = std::max(missing, capacity);  // new keys: missing keys, or every occupied slot
+    const int64_t words = 2 * nnz_old + 8 * k + nnz_old + k + 2 * (rows + 1) + 2 * (nf + 1) + 2 * (nnz_old + k);
+    return words * 8 + k + 16 * 256 + int64_t(cub_bytes(k + nnz_old, std::max(rows, nf) + 1));
+}
+
+extern "C" int32_t afsi_b200_cache_new_keys(const int64_t* table_keys, int64_t capacity, const int64_t* old_slots,
+                                            int64_t nnz_old, const int64_t* missing_keys, int64_t missing,
+                                            int64_t limit, int64_t* new_keys, int64_t* new_slots, int64_t* count,
+                                            void* scratch, int64_t scratch_bytes, afsi_stream_t stream) {
+    AFSI_REQUIRE(table_keys && capacity > 0 && (capacity & (capacity - 1)) == 0 && new_keys && count && scratch,
+                 "invalid cached-pattern arguments");
+    AFSI_REQUIRE(nnz_old >= 0 && missing >= 0 && limit > 0, "invalid cached-pattern sizes");
+    Carve c{static_cast<unsigned char*>(scratch), 0, size_t(scratch_bytes)};
+    const int bits = key_bits(limit);
+    if (cudaMemsetAsync(count, 0, 8, stream) != cudaSuccess) return fail(AFSI_ERR_CUDA, "cached pattern: memset");
+    if (!old_slots) {
+        // first build: the occupied keys in key order with their slots; the
+        // first *count entries of new_keys / new_slots (capacity long) are them
+        AFSI_REQUIRE(new_slots, "a first build returns the slots of its keys");
+        int64_t* keys = c.take<int64_t>(capacity);
+        int64_t* index = c.take<int64_t>(capacity);
+        size_t temp_bytes = cub_bytes(capacity, 1);
+        void* temp = c.take<unsigned char>(int64_t(temp_bytes));
+        AFSI_REQUIRE(c.used <= c.size, "cached-pattern scratch too small");
+        cache_occupied_kernel<<<cache_grid(capacity), 256, 0, stream>>>(
+            table_keys, capacity, limit, keys, index, reinterpret_cast<unsigned long long*>(count));
+        int32_t rc = launched("cache occupied keys");
+        if (rc) return rc;
+        if (cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, new_keys, index, new_slots, capacity, 0, bits,
+                                            stream) != cudaSuccess)
+            return fail(AFSI_ERR_CUDA, "cached pattern: sort failed");
+        return launched("cache sort occupied keys");
+    }
+    AFSI_REQUIRE(missing_keys || missing == 0, "null missing keys");
+    if (missing == 0) return AFSI_OK;
+    int64_t* old_keys = c.take<int64_t>(nnz_old);
+    int64_t* sorted = c.take<int64_t>(missing);
+    uint8_t* flags = c.take<uint8_t>(missing);
+    size_t temp_bytes = cub_bytes(missing, 1);
+    void* temp = c.take<unsigned char>(int64_t(temp_bytes));
+    AFSI_REQUIRE(c.used <= c.size, "cached-pattern scratch too small");
+    if (nnz_old) cache_gather_keys_kernel<<<cache_grid(nnz_old), 256, 0, stream>>>(table_keys, old_slots, nnz_old, old_keys);
+    if (cub::DeviceRadixSort::SortKeys(temp, temp_bytes, missing_keys, sorted, missing, 0, bits, stream) !=
+        cudaSuccess)
+        return fail(AFSI_ERR_CUDA, "cached pattern: sort failed");
+    cache_flag_new_kernel<<<cache_grid(missing), 256, 0, stream>>>(sorted, missing, old_keys, nnz_old, flags);
+    if (cub::DeviceSelect::Flagged(temp, temp_bytes, sorted, flags, new_keys, count, missing, stream) != cudaSuccess)
+        return fail(AFSI_ERR_CUDA, "cached pattern: select failed");
+    return launched("cache new keys");
+}
+
+extern "C" int32_t afsi_b200_cache_merge(const int64_t* table_keys, const void* table_values, int64_t capacity,
+                                         const int64_t* old_slots, const int64_t* old_order, const int64_t* old_crow,
+                                         const int64_t* old_tcrow, int64_t nnz_old, const int64_t* new_keys,
+                                         const int64_t* new_slots, int64_t k, int64_t rows, int64_t nf,
+                                         int64_t* slots, int64_t* order, int64_t* crow, int64_t* columns,
+                                         int64_t* tcrow, int64_t* tcolumns, void* values, void* reverse,
+                                         int32_t* status, void* scratch, int64_t scratch_bytes, int32_t dtype,
+                                         afsi_stream_t stream) {
+    AFSI_REQUIRE(table_keys && table_values && capacity > 0 && (capacity & (capacity - 1)) == 0,
+                 "invalid cached-pattern table");
+    AFSI_REQUIRE(nnz_old >= 0 && k >= 0 && rows > 0 && nf > 0 && (nnz_old == 0 || (old_slots && old_order && old_crow &&
+                                                                                       old_tcrow)),
+                 "invalid cached pattern");
+    AFSI_REQUIRE(slots && order && crow && columns && tcrow && tcolumns && values && reverse && scratch &&
+                     (k == 0 || new_keys),
+                 "null cached-pattern output");
+    const int64_t n = nnz_old + k;
+    Carve c{static_cast<unsigned char*>(scratch), 0, size_t(scratch_bytes)};
+    int64_t* old_keys = c.take<int64_t>(nnz_old);
+    int64_t* old_rk = c.take<int64_t>(nnz_old);
+    int64_t* old_pos = c.take<int64_t>(nnz_old);
+    int64_t* new_pos = c.take<int64_t>(k);
+    int64_t* new_rk = c.take<int64_t>(k);
+    int64_t* new_rk_sorted = c.take<int64_t>(k);
+    int64_t* new_index = c.take<int64_t>(k);
+    int64_t* new_order = c.take<int64_t>(k);
+    int64_t* keys = c.take<int64_t>(n);
+    unsigned long long* counts = c.take<unsigned long long>(rows + 1);
+    unsigned long long* tcounts = c.take<unsigned long long>(nf + 1);
+    unsigned long long* scan = c.take<unsigned long long>(rows + 1);
+    unsigned long long* tscan = c.take<unsigned long long>(nf + 1);
+    size_t temp_bytes = cub_bytes(k, std::max(rows, nf) + 1);
+    void* temp = c.take<unsigned char>(int64_t(temp_bytes));
+    AFSI_REQUIRE(c.used <= c.size, "cached-pattern scratch too small");
+    const int bits = key_bits(nf * rows);
+    if (nnz_old)
+        cache_gather_keys_kernel<<<cache_grid(nnz_old), 256, 0, stream>>>(table_keys, old_slots, nnz_old, old_keys);
+    cache_merge_keys_kernel<<<cache_grid(n), 256, 0, stream>>>(old_keys, old_slots, nnz_old, new_keys, new_slots, k,
+                                                               table_keys, capacity, keys, slots, old_pos, new_pos,
+                                                               status);
+    // row pointers grow by the prefix counts of the new keys' rows / columns
+    if (cudaMemsetAsync(counts, 0, size_t(rows + 1) * 8, stream) != cudaSuccess ||
+        cudaMemsetAsync(tcounts, 0, size_t(nf + 1) * 8, stream) != cudaSuccess)
+        return fail(AFSI_ERR_CUDA, "cached pattern: memset");
+    cache_count_kernel<<<cache_grid(k), 256, 0, stream>>>(new_keys, k, nf, rows, counts, tcounts, status);
+    if (cub::DeviceScan::ExclusiveSum(temp, temp_bytes, counts, scan, rows + 1, stream) != cudaSuccess ||
+        cub::DeviceScan::ExclusiveSum(temp, temp_bytes, tcounts, tscan, nf + 1, stream) != cudaSuccess)
+        return fail(AFSI_ERR_CUDA, "cached pattern: scan failed");
+    cache_pointers_kernel<<<cache_grid(rows + 1), 256, 0, stream>>>(old_crow, reinterpret_cast<const int64_t*>(scan),
+                                                                     rows + 1, crow);
+    cache_pointers_kernel<<<cache_grid(nf + 1), 256, 0, stream>>>(old_tcrow, reinterpret_cast<const int64_t*>(tscan),
+                                                                   nf + 1, tcrow);
+    // transpose order: merge of the old reverse keys and the sorted new ones
+    cache_reverse_kernel<<<cache_grid(n), 256, 0, stream>>>(old_keys, old_order, nnz_old, new_keys, k, nf, rows,
+                                                            old_rk, new_rk, new_index);
+    if (k && cub::DeviceRadixSort::SortPairs(temp, temp_bytes, new_rk, new_rk_sorted, new_index, new_order, k, 0,
+                                             bits, stream) != cudaSuccess)
+        return fail(AFSI_ERR_CUDA, "cached pattern: sort failed");
+    cache_merge_transpose_kernel<<<cache_grid(n), 256, 0, stream>>>(old_rk, old_order, old_pos, nnz_old,
+                                                                    new_rk_sorted, new_order, new_pos, k, order);
+    AFSI_DISPATCH(dtype, {
+        cache_finish_kernel<T><<<cache_grid(n), 256, 0, stream>>>(keys, slots, order, n, nf, rows,
+                                                                  static_cast<const T*>(table_values), columns,
+                                                                  tcolumns, static_cast<T*>(values),
+                                                                  static_cast<T*>(reverse), status);
+    });
+    return launched("cache merge");
+}
+
+namespace afsi {
+
+template <class T>
+__global__ void cache_values_kernel(const T* __restrict__ table_values, const int64_t* __restrict__ slots,
+                                    const int64_t* __restrict__ order, int64_t n, T* __restrict__ values,
+                                    T* __restrict__ reverse, int32_t* status) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const T v = table_values[slots[i]];
+        if (!isfinite(v)) flag(status, AFSI_FLAG_SUPPORT);
+        values[i] = v;
+        reverse[i] = table_values[slots[order[i]]];
+    }
+}
+
+}  // namespace afsi
+
+extern "C" int32_t afsi_b200_cache_values(const void* table_values, const int64_t* slots, const int64_t* order,
+                                          int64_t n, void* values, void* reverse, int32_t* status, int32_t dtype,
+                                          afsi_stream_t stream) {
+    AFSI_REQUIRE(n >= 0, "negative entry count");
+    if (n == 0) return AFSI_OK;
+    AFSI_REQUIRE(table_values && slots && order && values && reverse, "null cached-pattern argument");
+    AFSI_DISPATCH(dtype, {
+        cache_values_kernel<T><<<cache_grid(n), 256, 0, stream>>>(static_cast<const T*>(table_values), slots, order,
+                                                                  n, static_cast<T*>(values),
+                                                                  static_cast<T*>(reverse), status);
+    });
+    return launched("cache values");
 }

@@ -20,6 +20,10 @@ time:
   measure (``mac/helmholtz.py:44-47``, ``mac/stokes_workspace.py:50,86,97``):
   ``mac._triton_helmholtz`` and ``mac._triton_stokes`` are replaced by shims
   holding the B200 ``HelmholtzKernels`` and partial functions;
+* the cached CSR pattern maintenance, ``finish_cached_component`` and
+  ``numeric_snapshot`` of ``mac.cached_transfer_assembly`` (called through
+  that module's globals by ``assemble_component_cached``, :186-280), with the
+  reference's ``PatternBudgetExceeded`` raised so that its handler applies;
 * the consistent-mass solvers: ``MassSolver`` as bound in
   ``mac.compact_transfer`` and ``mac2d.transfer`` (imported there at module
   load, ``mac/compact_transfer.py:7``, ``mac2d/transfer.py:10-11``),
@@ -67,7 +71,14 @@ def install():
         target = importlib.import_module(module)
         _saved.setdefault(('attr', module, name), getattr(target, name))
         setattr(target, name, getattr(mass, name))
-    from . import helmholtz
+    from . import helmholtz, p1_csr
+    import afsi_torch.mac.cached_transfer_assembly as ref_cached
+    for name in ('finish_cached_component', 'numeric_snapshot'):
+        _saved.setdefault(('attr', 'afsi_torch.mac.cached_transfer_assembly', name), getattr(ref_cached, name))
+        setattr(ref_cached, name, getattr(p1_csr, name))
+    # the reference's assembly catches its own budget exception class
+    _saved.setdefault(('attr', 'afsi_gpu_b200.p1_csr', 'PatternBudgetExceeded'), p1_csr.PatternBudgetExceeded)
+    p1_csr.PatternBudgetExceeded = ref_cached.PatternBudgetExceeded
     for module, names in (('afsi_torch.mac._triton_helmholtz', ('HelmholtzKernels',)),
                           ('afsi_torch.mac._triton_stokes', ('start_partial', 'residual_partial',
                                                             'pressure_input_partial', 'pressure_norm_partial'))):

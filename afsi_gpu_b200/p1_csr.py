@@ -340,3 +340,135 @@ class P1CSRTransfer:
                 out = u.new_empty((self.node_count, 3))
             B.matvec(u, out[:, c:], out_stride=3)
         return out
+
+
+# ------------------------------------------------------------ cached pattern
+
+class PatternBudgetExceeded(RuntimeError):
+    """``mac/cached_transfer_assembly.py:15-16``."""
+
+
+@dataclass
+class CSRPatternCache:
+    """The fields of ``CSRPatternCache`` (``mac/cached_transfer_assembly.py:19-69``)
+    that the pattern maintenance reads and writes."""
+    slots: torch.Tensor = None
+    transpose_order: torch.Tensor = None
+    crow: torch.Tensor = None
+    columns: torch.Tensor = None
+    transpose_crow: torch.Tensor = None
+    transpose_columns: torch.Tensor = None
+    missing_keys: torch.Tensor = None
+    missing_values: torch.Tensor = None
+    missing_count: torch.Tensor = None
+    missing_capacity: int = 0
+    rebuilds: int = 0
+    pattern_shape: tuple = None
+    last_sorted_keys: int = 0
+    total_sorted_keys: int = 0
+
+    @property
+    def nnz(self):
+        return 0 if self.slots is None else len(self.slots)
+
+
+def finish_cached_component(workspace, cache, node_count, shape, max_entries, *, missing=None):
+    """``finish_cached_component`` (``mac/cached_transfer_assembly.py:97-175``)
+    on the device: the first build from the occupied table keys, or the merge
+    of the keys of the miss stream (``missing`` of them) that the pattern
+    lacks into the slot order, the transpose order and both row-pointer
+    arrays (``afsi_b200_cache_new_keys`` then ``afsi_b200_cache_merge``; one
+    host read of the new-key count between them, as in the reference).
+    Works on the reference's workspace and cache objects or on the ones of
+    this module; returns (B, Bᵀ) as CSR tensors sharing the cache's indices."""
+    keys_t, values_t = workspace.keys, workspace.values
+    _lib.require_cuda(keys_t)
+    dev = keys_t.device
+    nf = prod(shape)
+    cap = int(workspace.capacity)
+    limit = nf * node_count
+    s = stream(dev)
+    lib = _lib.load()
+    if missing is None:
+        scratch = torch.empty(int(lib.afsi_b200_cache_scratch_bytes(cap, 0, 0, node_count, nf)), device=dev,
+                              dtype=torch.uint8)
+        sorted_keys = torch.empty(cap, device=dev, dtype=torch.int64)
+        sorted_slots = torch.empty(cap, device=dev, dtype=torch.int64)
+        count = torch.zeros(1, device=dev, dtype=torch.int64)
+        call('afsi_b200_cache_new_keys', ptr(keys_t), cap, None, 0, None, 0, limit, ptr(sorted_keys),
+             ptr(sorted_slots), ptr(count), ptr(scratch), scratch.numel(), s)
+        k = int(count.item())
+        if k > max_entries:
+            raise PatternBudgetExceeded('cached IB union exceeds entry budget')
+        new_keys, new_slots = sorted_keys[:k], sorted_slots[:k]
+        old = None
+        nnz_old = 0
+    else:
+        old_slots = cache.slots.to(torch.int64)
+        nnz_old = len(old_slots)
+        scratch = torch.empty(int(lib.afsi_b200_cache_scratch_bytes(cap, nnz_old, int(missing), node_count, nf)),
+                              device=dev, dtype=torch.uint8)
+        new_buf = torch.empty(max(int(missing), 1), device=dev, dtype=torch.int64)
+        count = torch.zeros(1, device=dev, dtype=torch.int64)
+        call('afsi_b200_cache_new_keys', ptr(keys_t), cap, ptr(old_slots), nnz_old, ptr(cache.missing_keys),
+             int(missing), limit, ptr(new_buf), None, ptr(count), ptr(scratch), scratch.numel(), s)
+        k = int(count.item())
+        if nnz_old + k > max_entries:
+            raise PatternBudgetExceeded('cached IB union exceeds entry budget')
+        if k == 0:
+            cache.last_sorted_keys = 0
+            return numeric_snapshot(workspace, cache, node_count, shape)
+        new_keys, new_slots = new_buf[:k], None
+        old = (old_slots, cache.transpose_order.to(torch.int64), cache.crow, cache.transpose_crow)
+    n = nnz_old + k
+    out = dict(slots=torch.empty(n, device=dev, dtype=torch.int64), order=torch.empty(n, device=dev, dtype=torch.int64),
+               crow=torch.empty(node_count + 1, device=dev, dtype=torch.int64),
+               columns=torch.empty(n, device=dev, dtype=torch.int64),
+               tcrow=torch.empty(nf + 1, device=dev, dtype=torch.int64),
+               tcolumns=torch.empty(n, device=dev, dtype=torch.int64),
+               values=torch.empty(n, device=dev, dtype=values_t.dtype),
+               reverse=torch.empty(n, device=dev, dtype=values_t.dtype))
+    status = torch.zeros(1, device=dev, dtype=torch.int32)
+    call('afsi_b200_cache_merge', ptr(keys_t), ptr(values_t), cap, *(ptr(t) for t in (old or (None,) * 4)), nnz_old,
+         ptr(new_keys), ptr(new_slots), k, node_count, nf, ptr(out['slots']), ptr(out['order']), ptr(out['crow']),
+         ptr(out['columns']), ptr(out['tcrow']), ptr(out['tcolumns']), ptr(out['values']), ptr(out['reverse']),
+         ptr(status), ptr(scratch), scratch.numel(), dtype_code(values_t.dtype), s)
+    word = int(status.item())
+    if word & _lib.FLAG_OVERFLOW:
+        raise RuntimeError('cached IB slot lookup failed after completed insertion')
+    if word & (_lib.FLAG_INDEX | _lib.FLAG_SUPPORT):
+        raise FloatingPointError('invalid cached IB entries: nonfinite values or out-of-range keys')
+    mapping = torch.int32 if max(cap, n) < 2 ** 31 else torch.int64
+    cache.slots, cache.transpose_order = out['slots'].to(mapping), out['order'].to(mapping)
+    cache.crow, cache.columns = out['crow'], out['columns']
+    cache.transpose_crow, cache.transpose_columns = out['tcrow'], out['tcolumns']
+    cache.pattern_shape = (node_count, *shape)
+    cache.last_sorted_keys = k
+    cache.total_sorted_keys += k
+    cache.rebuilds += 1
+    matrix = torch.sparse_csr_tensor(out['crow'], out['columns'], out['values'], (node_count, nf),
+                                     check_invariants=False)
+    transpose = torch.sparse_csr_tensor(out['tcrow'], out['tcolumns'], out['reverse'], (nf, node_count),
+                                        check_invariants=False)
+    return matrix, transpose
+
+
+def numeric_snapshot(workspace, cache, node_count, shape, *, validate=True, values=None):
+    """``numeric_snapshot`` (``mac/cached_transfer_assembly.py:161-175``): the
+    pattern's values read from the table in key and in transpose order."""
+    dev = workspace.keys.device
+    nf = prod(shape)
+    n = cache.nnz
+    slots = cache.slots.to(torch.int64)
+    order = cache.transpose_order.to(torch.int64)
+    vals = torch.empty(n, device=dev, dtype=workspace.values.dtype)
+    rev = torch.empty_like(vals)
+    status = torch.zeros(1, device=dev, dtype=torch.int32)
+    call('afsi_b200_cache_values', ptr(workspace.values), ptr(slots), ptr(order), n, ptr(vals), ptr(rev),
+         ptr(status), dtype_code(vals.dtype), stream(dev))
+    if validate and int(status.item()):
+        raise FloatingPointError('invalid cached IB entries: nonfinite values')
+    matrix = torch.sparse_csr_tensor(cache.crow, cache.columns, vals, (node_count, nf), check_invariants=False)
+    transpose = torch.sparse_csr_tensor(cache.transpose_crow, cache.transpose_columns, rev, (nf, node_count),
+                                        check_invariants=False)
+    return matrix, transpose

@@ -378,6 +378,37 @@ int32_t afsi_b200_vector_stats(const void* x, int64_t n, double* stats_out, void
 int32_t afsi_b200_subtract_mean(void* x, int64_t n, const double* stats, int32_t dtype,
     afsi_stream_t stream);
 
+/* ---- cached CSR pattern maintenance ----------------------------------------
+ * finish_cached_component / numeric_snapshot (mac/cached_transfer_assembly.py:
+ * 97-175) on the device.  A pattern is its table slots in key order, its
+ * transpose order and the row pointers of B (rows = nodes) and B^T (nf faces).
+ * afsi_b200_cache_new_keys: with old_slots == NULL (a first build) the
+ *   occupied table keys sorted with their slots into new_keys / new_slots
+ *   (capacity long; the first *count are the keys); otherwise the sorted
+ *   unique keys of missing_keys[0..missing) that the pattern's nnz_old keys
+ *   lack, into new_keys (*count of them).  limit = nodes * nf bounds the keys.
+ * afsi_b200_cache_merge: the pattern after adding the k sorted new keys
+ *   (new_slots given, or looked up in the table by linear probing, at most
+ *   128 slots; a failed lookup sets AFSI_FLAG_OVERFLOW): slots, transpose
+ *   order, crow (nodes+1), columns, tcrow (nf+1), transpose columns, values
+ *   and transpose values (nnz_old + k each); out-of-range keys set
+ *   AFSI_FLAG_INDEX, nonfinite values AFSI_FLAG_SUPPORT.  Old pattern arrays
+ *   may be NULL when nnz_old == 0.
+ * afsi_b200_cache_values: values and transpose values of an unchanged pattern.
+ * scratch: afsi_b200_cache_scratch_bytes(capacity, nnz_old, missing, nodes, nf). */
+int64_t afsi_b200_cache_scratch_bytes(int64_t capacity, int64_t nnz_old, int64_t missing, int64_t rows, int64_t nf);
+int32_t afsi_b200_cache_new_keys(const int64_t* table_keys, int64_t capacity, const int64_t* old_slots,
+    int64_t nnz_old, const int64_t* missing_keys, int64_t missing, int64_t limit, int64_t* new_keys,
+    int64_t* new_slots, int64_t* count, void* scratch, int64_t scratch_bytes, afsi_stream_t stream);
+int32_t afsi_b200_cache_merge(const int64_t* table_keys, const void* table_values, int64_t capacity,
+    const int64_t* old_slots, const int64_t* old_order, const int64_t* old_crow, const int64_t* old_tcrow,
+    int64_t nnz_old, const int64_t* new_keys, const int64_t* new_slots, int64_t k, int64_t rows, int64_t nf,
+    int64_t* slots, int64_t* order, int64_t* crow, int64_t* columns, int64_t* tcrow, int64_t* tcolumns,
+    void* values, void* reverse, int32_t* status, void* scratch, int64_t scratch_bytes, int32_t dtype,
+    afsi_stream_t stream);
+int32_t afsi_b200_cache_values(const void* table_values, const int64_t* slots, const int64_t* order, int64_t n,
+    void* values, void* reverse, int32_t* status, int32_t dtype, afsi_stream_t stream);
+
 /* ---- CN Helmholtz sweeps and Stokes residual reductions --------------------
  * The kernels of the Stokes FGMRES preconditioner and its checks on the 3D MAC
  * grid of `shape` cells (nx, ny, nz).  Face arrays come as three pointers

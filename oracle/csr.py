@@ -150,3 +150,55 @@ def csr_transpose(crow, col, val, ncols):
     t_crow = np.zeros(ncols + 1, dtype=np.int64)
     np.add.at(t_crow, col + 1, 1)
     return np.cumsum(t_crow), rows[order], val[order]
+
+
+def _pointers(idx, size):
+    counts = np.bincount(idx, minlength=size)
+    return np.concatenate(([0], np.cumsum(counts))).astype(np.int64)
+
+
+def finish_cached(table_keys, table_values, rows, nf, old=None, missing=None):
+    """``finish_cached_component`` (mac/cached_transfer_assembly.py:97-175):
+    returns dict(slots, order, crow, cols, tcrow, tcols, values, reverse, new)
+    for a first build (old None) or for the merge of `missing` keys into the
+    pattern `old` (a dict of the same fields)."""
+    table_keys = np.asarray(table_keys)
+    if old is None:
+        occupied = np.nonzero(table_keys >= 0)[0]
+        order = np.argsort(table_keys[occupied], kind='stable')
+        keys, slots = table_keys[occupied][order], occupied[order]
+        rws, cols = keys // nf, keys % nf
+        transpose = np.argsort(cols * rows + rws, kind='stable')
+        crow, tcrow = _pointers(rws, rows), _pointers(cols, nf)
+        new = len(keys)
+    else:
+        old_keys = table_keys[old['slots']]
+        new_keys = np.unique(np.asarray(missing))
+        at = np.searchsorted(old_keys, new_keys)
+        exists = (at < len(old_keys)) & (old_keys[np.minimum(at, len(old_keys) - 1)] == new_keys)
+        new_keys = new_keys[~exists]
+        old_pos = np.arange(len(old_keys)) + np.searchsorted(new_keys, old_keys, side='right')
+        new_pos = np.arange(len(new_keys)) + np.searchsorted(old_keys, new_keys)
+        n = len(old_keys) + len(new_keys)
+        keys = np.empty(n, np.int64)
+        keys[old_pos], keys[new_pos] = old_keys, new_keys
+        slots = np.empty(n, np.int64)
+        slots[old_pos] = old['slots']
+        slots[new_pos] = [int(np.nonzero(table_keys == k)[0][0]) for k in new_keys]
+        rws, cols = keys // nf, keys % nf
+        crow = old['crow'] + _pointers(new_keys // nf, rows)
+        tcrow = old['tcrow'] + _pointers(new_keys % nf, nf)
+        old_rev = old_keys[old['order']]
+        old_rev = old_rev % nf * rows + old_rev // nf
+        new_rev_keys = new_keys % nf * rows + new_keys // nf
+        new_rev_order = np.argsort(new_rev_keys, kind='stable')
+        new_rev = new_rev_keys[new_rev_order]
+        old_rpos = np.arange(len(old_rev)) + np.searchsorted(new_rev, old_rev, side='right')
+        new_rpos = np.arange(len(new_rev)) + np.searchsorted(old_rev, new_rev)
+        transpose = np.empty(n, np.int64)
+        transpose[old_rpos] = old_pos[old['order']]
+        transpose[new_rpos] = new_pos[new_rev_order]
+        new = len(new_keys)
+    values = np.asarray(table_values)[slots]
+    return dict(slots=slots, order=transpose, crow=crow, cols=cols, tcrow=tcrow, tcols=rws[transpose],
+                values=values, reverse=values[transpose], new=new)

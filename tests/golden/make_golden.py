@@ -403,6 +403,41 @@ def stokes():
     save('stokes', **out)
 
 
+def cached():
+    """Cached CSR pattern (mac/cached_transfer_assembly.py:97-175): a first
+    build from a filled hash table, then an extension by a miss stream that
+    holds new keys, keys already in the pattern and repeats."""
+    from afsi_torch.mac.hash_transfer_assembly import HashWorkspace, cpu_accumulate
+    from afsi_torch.mac.cached_transfer_assembly import CSRPatternCache, finish_cached_component
+    g = torch.Generator().manual_seed(16)
+    rows, shape = 40, (6, 5, 4)
+    nf = 6 * 5 * 4
+    ws = HashWorkspace()
+    ws.reset(1024, torch.zeros(1, dtype=torch.float64))
+    keys1 = torch.randint(0, rows * nf, (300,), generator=g)
+    cpu_accumulate(keys1, torch.randn(300, generator=g, dtype=torch.float64), ws)
+    cache = CSRPatternCache()
+    out = dict(rows=rows, shape=shape, capacity=ws.capacity, table1_keys=ws.keys.clone(),
+               table1_values=ws.values.clone())
+    m1, t1 = finish_cached_component(ws, cache, rows, shape, 10 ** 6)
+    out.update(slots1=cache.slots.to(torch.int64), order1=cache.transpose_order.to(torch.int64), crow1=cache.crow,
+               cols1=cache.columns, tcrow1=cache.transpose_crow, tcols1=cache.transpose_columns,
+               values1=m1.values(), reverse1=t1.values())
+    fresh = torch.randint(0, rows * nf, (60,), generator=g)
+    old = ws.keys[cache.slots.to(torch.int64)][torch.randint(0, cache.nnz, (30,), generator=g)]
+    missing = torch.cat((fresh, old, fresh[:10]))
+    vals = torch.randn(len(missing), generator=g, dtype=torch.float64)
+    cpu_accumulate(missing, vals, ws)
+    cache.scratch(len(missing), ws.values)
+    cache.missing_keys[:len(missing)] = missing
+    m2, t2 = finish_cached_component(ws, cache, rows, shape, 10 ** 6, missing=len(missing))
+    out.update(missing=missing, table2_keys=ws.keys.clone(), table2_values=ws.values.clone(),
+               slots2=cache.slots.to(torch.int64), order2=cache.transpose_order.to(torch.int64), crow2=cache.crow,
+               cols2=cache.columns, tcrow2=cache.transpose_crow, tcols2=cache.transpose_columns,
+               values2=m2.values(), reverse2=t2.values(), new_count=cache.last_sorted_keys)
+    save('cached', **out)
+
+
 if __name__ == '__main__':
     peskin()
     compact3d()
@@ -416,3 +451,4 @@ if __name__ == '__main__':
     dirichlet()
     mass()
     stokes()
+    cached()

@@ -44,6 +44,10 @@ def test_install_rebinds_ib_operators_and_mg_kernels(afsi_torch):
         from afsi_torch.mac._triton_helmholtz import HelmholtzKernels as HK
         from afsi_torch.mac._triton_stokes import residual_partial as rp
         assert HK is helmholtz.HelmholtzKernels and rp is helmholtz.residual_partial
+        import afsi_torch.mac.cached_transfer_assembly as ref_cached
+        from afsi_gpu_b200 import p1_csr
+        assert ref_cached.finish_cached_component is p1_csr.finish_cached_component
+        assert p1_csr.PatternBudgetExceeded is ref_cached.PatternBudgetExceeded
     finally:
         dropin.uninstall()
     assert ref_ib.compact_gather is original

@@ -214,3 +214,77 @@ def test_p1_fp32_operators_and_budget_errors():
     small = P1CSRTransfer(grid, X.double(), t(g['block_cells']), max_entries=8)
     with pytest.raises(RuntimeError, match='budget exceeded|probe/budget exceeded'):
         small.prepare(X.double())
+
+
+def _table(keys, values):
+    from afsi_gpu_b200.p1_csr import HashWorkspace
+    ws = HashWorkspace()
+    ws.capacity = len(keys)
+    ws.keys = t(keys, torch.int64)
+    ws.values = t(values)
+    ws.flag = torch.zeros((), device=DEV, dtype=torch.int32)
+    return ws
+
+
+def _pattern(cache, matrix, transpose):
+    return dict(slots=cache.slots.long().cpu().numpy(), order=cache.transpose_order.long().cpu().numpy(),
+                crow=cache.crow.cpu().numpy(), cols=cache.columns.cpu().numpy(),
+                tcrow=cache.transpose_crow.cpu().numpy(), tcols=cache.transpose_columns.cpu().numpy(),
+                values=matrix.values().cpu().numpy(), reverse=transpose.values().cpu().numpy())
+
+
+def test_cached_pattern_build_and_merge_match_reference():
+    """finish_cached_component on the device against the reference's own
+    first build and miss-stream merge (cached.npz): every index array exact,
+    values exact (they are read from the same table)."""
+    from afsi_gpu_b200.p1_csr import CSRPatternCache, finish_cached_component, numeric_snapshot
+    g = golden('cached')
+    rows, shape = int(g['rows']), tuple(int(n) for n in g['shape'])
+    cache = CSRPatternCache()
+    ws = _table(g['table1_keys'], g['table1_values'])
+    got = _pattern(cache, *finish_cached_component(ws, cache, rows, shape, 10 ** 6))
+    for k in got:
+        assert np.array_equal(got[k], g[f'{k}1']), k
+    ws2 = _table(g['table2_keys'], g['table2_values'])
+    cache.missing_keys = t(g['missing'], torch.int64)
+    got = _pattern(cache, *finish_cached_component(ws2, cache, rows, shape, 10 ** 6, missing=len(g['missing'])))
+    for k in got:
+        assert np.array_equal(got[k], g[f'{k}2']), k
+    assert cache.last_sorted_keys == int(g['new_count'])
+    m, tr = numeric_snapshot(ws2, cache, rows, shape)
+    assert np.array_equal(m.values().cpu().numpy(), g['values2'])
+    assert np.array_equal(tr.values().cpu().numpy(), g['reverse2'])
+    # nothing new: the snapshot path
+    cache.missing_keys = t(g['missing'][:20], torch.int64)
+    got = _pattern(cache, *finish_cached_component(ws2, cache, rows, shape, 10 ** 6, missing=20))
+    assert cache.last_sorted_keys == 0 and np.array_equal(got['slots'], g['slots2'])
+
+
+def test_cached_pattern_large_merge_against_oracle():
+    from afsi_gpu_b200.p1_csr import CSRPatternCache, HashWorkspace, finish_cached_component, hash_accumulate
+    rng = np.random.default_rng(9)
+    rows, shape = 5000, (24, 20, 16)
+    nf = int(np.prod(shape))
+    ws = HashWorkspace()
+    ws.reset(1 << 16, torch.zeros(1, device=DEV, dtype=torch.float64))
+    k1 = rng.integers(0, rows * nf, 20000)
+    hash_accumulate(t(k1, torch.int64), t(rng.standard_normal(len(k1))), ws)
+    assert int(ws.flag.item()) == 0
+    cache = CSRPatternCache()
+    finish_cached_component(ws, cache, rows, shape, 10 ** 7)
+    first = ocsr.finish_cached(ws.keys.cpu().numpy(), ws.values.cpu().numpy(), rows, nf)
+    assert np.array_equal(cache.slots.long().cpu().numpy(), first['slots'])
+    old_keys = ws.keys.cpu().numpy()[first['slots']]
+    k2 = np.concatenate((rng.integers(0, rows * nf, 4000), old_keys[rng.integers(0, len(old_keys), 2000)]))
+    hash_accumulate(t(k2, torch.int64), t(rng.standard_normal(len(k2))), ws)
+    cache.missing_keys = t(k2, torch.int64)
+    m, tr = finish_cached_component(ws, cache, rows, shape, 10 ** 7, missing=len(k2))
+    ref = ocsr.finish_cached(ws.keys.cpu().numpy(), ws.values.cpu().numpy(), rows, nf, old=first, missing=k2)
+    got = _pattern(cache, m, tr)
+    for k in got:
+        assert np.array_equal(got[k], ref[k]), k
+    # the merged pattern equals a first build of the same table
+    again = CSRPatternCache()
+    finish_cached_component(ws, again, rows, shape, 10 ** 7)
+    assert torch.equal(again.slots, cache.slots) and torch.equal(again.transpose_order, cache.transpose_order)
+    assert torch.equal(again.crow, cache.crow) and torch.equal(again.transpose_crow, cache.transpose_crow)

@@ -269,3 +269,19 @@ def test_stokes_oracle_matches_reference_kernels():
     m = stokes.pressure_metrics(g['prhs'], g['p'], spacing)
     np.testing.assert_allclose(m[[0, 1, 2, 5, 6]], g['pmetrics'], rtol=1e-12, atol=1e-12)
     assert m[3] == 1 and m[4] == 1
+
+
+def test_cached_pattern_oracle_matches_reference():
+    """oracle/csr.py:finish_cached against the reference's
+    finish_cached_component: a first build and a merge of a miss stream with
+    new, existing and repeated keys; every index array exact."""
+    from oracle import csr as ocsr
+    g = golden('cached')
+    rows, nf = int(g['rows']), int(np.prod(g['shape']))
+    first = ocsr.finish_cached(g['table1_keys'], g['table1_values'], rows, nf)
+    for k in ('slots', 'order', 'crow', 'cols', 'tcrow', 'tcols', 'values', 'reverse'):
+        assert np.array_equal(first[k], g[f'{k}1']), k
+    merged = ocsr.finish_cached(g['table2_keys'], g['table2_values'], rows, nf, old=first, missing=g['missing'])
+    for k in ('slots', 'order', 'crow', 'cols', 'tcrow', 'tcols', 'values', 'reverse'):
+        assert np.array_equal(merged[k], g[f'{k}2']), k
+    assert merged['new'] == int(g['new_count'])
