@@ -456,6 +456,34 @@ def dist_setup(args):
     return None, 0, 1
 
 
+_ORACLE = {}
+
+
+def _oracle_worker_init(X, coef, vel, shape, lengths, origin):
+    """Reference-arm worker set-up: the step's static inputs, the rule tables
+    and the oracle import, once per worker process."""
+    from afsi_gpu_b200.quadrature import conical_rule, tabulate_p2
+    torch.set_num_threads(1)  # one core per worker: the workers are the parallelism
+    q, w = conical_rule(4)
+    spacing = tuple(L / n for L, n in zip(lengths, shape))
+    _ORACLE.update(X=X, coef=coef, vel=vel, shape=shape, origin=origin, spacing=spacing,
+                   volume=float(np.prod(spacing)), N=tabulate_p2(q), w=w)
+
+
+def _oracle_transfer_chunk(cells):
+    """One worker's share of the reference arm: the oracle prepare, spread and
+    gather-assemble of a chunk of elements (top level, so that a spawn pool
+    can call it)."""
+    from oracle import ib
+    from afsi_gpu_b200.quadrature import reference_determinants
+    o = _ORACLE
+    W = reference_determinants(torch.as_tensor(o['X']), torch.as_tensor(cells)).numpy()[:, None] * o['w']
+    base, phi, _ = ib.p2_prepare(o['X'], [(cells, o['N'])], o['origin'], o['spacing'], o['shape'])
+    fields = ib.p2_spread(o['coef'], [(cells, o['N'], W)], base, phi, o['shape'], o['volume'])
+    nodal = ib.p2_gather_assemble(o['vel'], [(cells, o['N'], W)], base, phi, o['shape'], o['X'].shape[0])
+    return fields, nodal
+
+
 def run_reference(args):
     dist, rank, world = dist_setup(args)
     if rank != 0:
@@ -463,17 +491,50 @@ def run_reference(args):
             dist.destroy_process_group()
         return
     grid, X, cells, coef, vel, rhs = workload()
-    cores = 1
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    from oracle import mg
+    cores = max(1, len(os.sched_getaffinity(0)))
+    E = cells.shape[0]
     times = []
-    warm, timed = min(args.warmup, 1), min(args.steps, 30)  # about 1 s of CPU work per step
-    for i in range(warm + timed):
-        dt, info, _ = cpu_step_time(grid, X, cells, coef, vel, rhs, fraction=0.02)
-        if i >= warm:
-            times.append(dt)
+    warm, timed = min(args.warmup, 1), min(args.steps, 10)
+    init = (X, coef, vel, tuple(grid.shape), tuple(grid.lengths), tuple(grid.origin))
+    for var in ('OMP_NUM_THREADS', 'OPENBLAS_NUM_THREADS', 'MKL_NUM_THREADS'):
+        os.environ[var] = '1'  # inherited by the spawned workers
+    with ProcessPoolExecutor(max_workers=cores, mp_context=mp.get_context('spawn'), initializer=_oracle_worker_init,
+                             initargs=init) as pool:
+        list(pool.map(_oracle_transfer_chunk, [cells[:8]] * cores))  # start every worker, import the oracle
+        # use the worker count with the best element throughput on this host
+        # (hosts whose cores share memory bandwidth stop scaling early)
+        best = None
+        k = 1
+        while k <= cores:
+            t0 = time.perf_counter()
+            list(pool.map(_oracle_transfer_chunk, [cells[i * 512:(i + 1) * 512] for i in range(k)]))
+            rate = k * 512 / (time.perf_counter() - t0)
+            if best is None or rate > best[0]:
+                best = (rate, k)
+            k = k * 2 if k * 2 <= cores or k == cores else cores
+        workers = best[1]
+        Es = min(E, 512 * workers)  # element sample: 512 per worker, time scaled by E / Es
+        tasks = [cells[c] for c in np.array_split(np.arange(Es), workers)]
+        h = mg.Hierarchy(grid.shape, grid.spacing, 'neumann')
+        for i in range(warm + timed):
+            t0 = time.perf_counter()
+            parts = list(pool.map(_oracle_transfer_chunk, tasks))
+            fields = [sum(p[0][c] for p in parts) for c in range(3)]
+            nodal = sum(p[1] for p in parts)
+            t1 = time.perf_counter()
+            p, info = mg.solve(h, rhs)
+            t2 = time.perf_counter()
+            if i >= warm:
+                times.append((t1 - t0) * (E / Es) + (t2 - t1))
     step = float(np.mean(times))
     sample = (f'oracle (NumPy restatement of the reference CPU path): P2 prepare/spread/gather-assemble on '
-              f'{info["elements_sampled"]} of {info["elements"]} elements, time scaled by elements; '
-              f'full 64^3 MG solve; {timed} steps after {warm} warm-up')
+              f'{Es} of {E} elements split over {workers} worker processes (the fastest count of 1..{cores} '
+              f'host cores), time scaled by elements; full 64^3 MG solve in one process; {timed} steps after '
+              f'{warm} warm-up')
+    cores = workers
     value = 1.0 / step
     line = dict(metric=METRIC, value=value, unit='steps/s', impl='reference', n_gpus=args.gpus, steps=timed,
                 warmup=warm, ms_per_step=step * 1e3, higher_is_better=True, scaling='weak',
