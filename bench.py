@@ -42,6 +42,9 @@ def parse():
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='b200', choices=('b200', 'reference'))
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--rows', default='all', choices=('all', 'step'),
+                    help="'step': the headline step line only, without the mass-solve, MG-form, batching and "
+                         "serving rows (for profiler runs)")
     return ap.parse_args()
 
 
@@ -641,10 +644,11 @@ def run_b200(args):
                        sample=(f'oracle (NumPy restatement) on {info["elements_sampled"]} of {info["elements"]} '
                                f'elements for the transfers (scaled by element count) + full 64^3 MG solve'))
             errors = oracle_errors(step, X, coef, vel, outputs, outs[-1].numpy())
-        mass = mass_pcg_row(X, cells, device, pk['hbm_gbs'])
-        forms = mg_forms_row(grid, rhs, device)
-        batch = batch_form_row(device)
-        serving = serving_form_row(device)
+        extra = args.rows == 'all'
+        mass = mass_pcg_row(X, cells, device, pk['hbm_gbs']) if extra else None
+        forms = mg_forms_row(grid, rhs, device) if extra else None
+        batch = batch_form_row(device) if extra else None
+        serving = serving_form_row(device) if extra else None
         step_ms = np.array([ev[0].elapsed_time(ev[4]) for ev in phases])
         line = dict(
             metric=METRIC, value=world * args.steps / elapsed, unit='steps/s', n_gpus=world, steps=args.steps,
