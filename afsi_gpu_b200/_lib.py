@@ -59,6 +59,8 @@ _SIGNATURES = {
                              c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int32, c_void_p],
     'afsi_b200_p2_orders': [c_void_p, c_int64, c_void_p, c_int64, ctypes.c_double, ctypes.c_double, c_int64,
                             c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p],
+    'afsi_b200_fe_prepare_mixed': [c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, P_F64, P_F64,
+                                   P_F64, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int32, c_void_p],
     'afsi_b200_p1_prepare': [c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, P_F64, P_F64, P_F64,
                              c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int32, c_void_p],
     'afsi_b200_p1_orders': [c_void_p, c_int64, c_void_p, c_int64, ctypes.c_double, ctypes.c_double, c_int64,

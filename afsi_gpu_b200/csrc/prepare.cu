@@ -145,14 +145,15 @@ constexpr int kPrepThreads = 128;
 // as two contiguous ranges per lattice (bases: 3 int64 per point, weights: 12
 // values per point) with coalesced stores, instead of 18 scattered stores per
 // point.  A point with a node id out of range flags AFSI_FLAG_INDEX and gets
-// zero tables.
-template <class T, int NPC>
+// zero tables.  Positions, bases and weights are computed in T; the weights
+// are stored in TW (T, or float beside FP64 positions in the precision form).
+template <class T, int NPC, class TW = T>
 __global__ void __launch_bounds__(kPrepThreads) fe_prepare_kernel(const T* __restrict__ x,
                                                                   const int64_t* __restrict__ cells,
                                                                   const T* __restrict__ N, P2Params<T> prm,
-                                                                  int64_t* __restrict__ base, T* __restrict__ phi,
+                                                                  int64_t* __restrict__ base, TW* __restrict__ phi,
                                                                   int32_t* status) {
-    __shared__ __align__(16) T s_phi[2][kPrepThreads * 12];
+    __shared__ __align__(16) TW s_phi[2][kPrepThreads * 12];
     __shared__ int64_t s_base[2][kPrepThreads * 3];
     const int64_t first = int64_t(blockIdx.x) * kPrepThreads;
     const int64_t points = prm.elements * prm.nq;
@@ -193,13 +194,13 @@ __global__ void __launch_bounds__(kPrepThreads) fe_prepare_kernel(const T* __res
                 peskin_radical(scaled - T(lower) - T(1), w);
                 s_base[lattice][t * 3 + a] = ok ? lower : 0;
 #pragma unroll
-                for (int k = 0; k < 4; ++k) s_phi[lattice][(t * 3 + a) * 4 + k] = ok ? w[k] : T(0);
+                for (int k = 0; k < 4; ++k) s_phi[lattice][(t * 3 + a) * 4 + k] = ok ? TW(w[k]) : TW(0);
             }
         }
     }
     __syncthreads();
-    using V = typename Vec16<T>::type;
-    constexpr int per = Vec16<T>::n;
+    using V = typename Vec16<TW>::type;
+    constexpr int per = Vec16<TW>::n;
 #pragma unroll
     for (int lattice = 0; lattice < 2; ++lattice) {
         const int64_t row = (lattice * prm.total + prm.offset + first) * 3;
@@ -365,7 +366,10 @@ template <int NPC>
 static int32_t fe_prepare(const void* x, int64_t nodes, const int64_t* cells, int64_t elements, const void* N,
                           int64_t nq, const double* origin, const double* spacing, const double* limits,
                           int64_t* base, void* phi, int64_t total, int64_t offset, int32_t* status, int32_t dtype,
-                          afsi_stream_t stream) {
+                          afsi_stream_t stream, int32_t weight_dtype = -1) {
+    if (weight_dtype < 0) weight_dtype = dtype;
+    AFSI_REQUIRE(weight_dtype == dtype || (dtype == AFSI_F64 && weight_dtype == AFSI_F32),
+                 "weights may be stored in FP32 beside FP64 positions only");
     AFSI_REQUIRE(elements >= 0 && nq > 0 && nodes >= 0, "invalid IB group sizes");
     AFSI_REQUIRE(offset >= 0 && offset <= total && elements * nq <= total - offset, "IB group exceeds table bounds");
     AFSI_REQUIRE(origin && spacing && limits, "null host parameter array");
@@ -384,8 +388,15 @@ static int32_t fe_prepare(const void* x, int64_t nodes, const int64_t* cells, in
         prm.nq = nq;
         prm.total = total;
         prm.offset = offset;
-        fe_prepare_kernel<T, NPC><<<blocks_for(elements * nq, kPrepThreads), kPrepThreads, 0, stream>>>(
-            static_cast<const T*>(x), cells, static_cast<const T*>(N), prm, base, static_cast<T*>(phi), status);
+        if (weight_dtype != dtype) {
+            if constexpr (sizeof(T) == 8)
+                fe_prepare_kernel<T, NPC, float><<<blocks_for(elements * nq, kPrepThreads), kPrepThreads, 0, stream>>>(
+                    static_cast<const T*>(x), cells, static_cast<const T*>(N), prm, base, static_cast<float*>(phi),
+                    status);
+        } else {
+            fe_prepare_kernel<T, NPC><<<blocks_for(elements * nq, kPrepThreads), kPrepThreads, 0, stream>>>(
+                static_cast<const T*>(x), cells, static_cast<const T*>(N), prm, base, static_cast<T*>(phi), status);
+        }
     });
     return launched(NPC == 10 ? "p2_prepare" : "p1_prepare");
 }
@@ -396,6 +407,19 @@ extern "C" int32_t afsi_b200_p2_prepare(const void* x, int64_t nodes, const int6
                                         int64_t offset, int32_t* status, int32_t dtype, afsi_stream_t stream) {
     return fe_prepare<10>(x, nodes, cells, elements, N, nq, origin, spacing, limits, base, phi, total, offset, status,
                           dtype, stream);
+}
+
+extern "C" int32_t afsi_b200_fe_prepare_mixed(int32_t nodes_per_cell, const double* x, int64_t nodes,
+                                              const int64_t* cells, int64_t elements, const double* N, int64_t nq,
+                                              const double* origin, const double* spacing, const double* limits,
+                                              int64_t* base, void* phi, int64_t total, int64_t offset,
+                                              int32_t* status, int32_t weight_dtype, afsi_stream_t stream) {
+    AFSI_REQUIRE(nodes_per_cell == 10 || nodes_per_cell == 4, "nodes per cell must be 10 (P2) or 4 (P1)");
+    if (nodes_per_cell == 10)
+        return fe_prepare<10>(x, nodes, cells, elements, N, nq, origin, spacing, limits, base, phi, total, offset,
+                              status, AFSI_F64, stream, weight_dtype);
+    return fe_prepare<4>(x, nodes, cells, elements, N, nq, origin, spacing, limits, base, phi, total, offset, status,
+                         AFSI_F64, stream, weight_dtype);
 }
 
 extern "C" int32_t afsi_b200_p1_prepare(const void* x, int64_t nodes, const int64_t* cells, int64_t elements,

@@ -14,6 +14,10 @@ support violation raises ``ValueError`` after the prepare.
 the consistent-mass solve, which is outside this hot path.  Its
 ``deterministic=True`` mode assembles through element-local sums and a fixed
 node CSR instead of atomics (bitwise reproducible ``assemble_velocity``).
+``transfer_dtype=torch.float32`` beside FP64 positions is the precision form:
+positions, bases and weights are formed in FP64 (``afsi_b200_fe_prepare_mixed``,
+so the bases are the FP64 bases), the weight tables, rule tables and the
+transfers are FP32.
 """
 from dataclasses import dataclass
 import torch
@@ -44,7 +48,7 @@ class P2Transfer:
     """Grid/quadrature state of the P2 CUDA transfer (no mass solve)."""
 
     def __init__(self, grid, X, cells, *, point_density=2., max_order=8, max_points=12000000,
-                 deterministic=False):
+                 deterministic=False, transfer_dtype=None):
         if cells.dim() != 2 or cells.shape[1] != 10:
             raise ValueError('P2 transfer requires ten-node tetrahedra')
         _lib.require_cuda(X)
@@ -54,7 +58,11 @@ class P2Transfer:
         cast = X.new_tensor
         self.origin, self.spacing = cast(grid.origin), cast(grid.spacing)
         self.limits = cast(grid.shape) - 2
-        self.diagonal = torch.zeros((X.shape[0], 3), device=X.device, dtype=X.dtype)  # rhs template
+        self.transfer_dtype = X.dtype if transfer_dtype is None else transfer_dtype
+        if self.transfer_dtype != X.dtype and not (X.dtype == torch.float64 and self.transfer_dtype == torch.float32):
+            raise ValueError('FP32 transfers are supported beside FP64 positions only')
+        self.diagonal = torch.zeros((X.shape[0], 3), device=X.device, dtype=self.transfer_dtype)  # rhs template
+        self._cast = None
         self.rules = RuleBuilder(X, self.cells, grid, point_density=point_density, max_order=max_order,
                                  max_points=max_points)
         self.deterministic = deterministic
@@ -75,7 +83,7 @@ class P2Transfer:
         orders, summary = self.rules.launch(x)
         speculative = None
         if last is not None:
-            base, phi = _tables(x, last.point_count, buffers)
+            base, phi = _tables(x, last.point_count, buffers, self.transfer_dtype)
             _launch_prepare(self, x, last, base, phi, summary[-1:])
             speculative = base, phi
         counts = summary.cpu().tolist()
@@ -94,6 +102,16 @@ class P2Transfer:
             return assemble_velocity_deterministic(self, velocity, stencil)
         return assemble_velocity(self, velocity, stencil)
 
+    def group_tables(self, rule):
+        """(values N, weights W) of every group of `rule` in the transfer dtype
+        (the rule's own tensors, or FP32 copies made once per rule)."""
+        if self.transfer_dtype == rule.groups[0].weights.dtype:
+            return [(g.values, g.weights) for g in rule.groups]
+        if self._cast is None or self._cast[0] is not rule:
+            self._cast = (rule, [(g.values.to(self.transfer_dtype).contiguous(),
+                                  g.weights.to(self.transfer_dtype).contiguous()) for g in rule.groups])
+        return self._cast[1]
+
     def node_csr(self, rule):
         """node -> (element*10+a) CSR over the rule's group order (built once per rule)."""
         if self._csr is not None and self._csr[0] is rule:
@@ -110,17 +128,19 @@ class P2Transfer:
         return crow, order
 
 
-def _tables_ok(base, phi, total, x):
+def _tables_ok(base, phi, total, x, dtype):
     return (base.shape == (2, total, 3) and phi.shape == (2, total, 3, 4) and base.dtype == torch.int64 and
-            phi.dtype == x.dtype and base.device == x.device and phi.device == x.device and
+            phi.dtype == dtype and base.device == x.device and phi.device == x.device and
             base.is_contiguous() and phi.is_contiguous())
 
 
-def _tables(x, total, buffers):
+def _tables(x, total, buffers, dtype=None):
+    dtype = x.dtype if dtype is None else dtype
     if buffers is None:
-        return (torch.empty((2, total, 3), device=x.device, dtype=torch.int64), x.new_empty((2, total, 3, 4)))
+        return (torch.empty((2, total, 3), device=x.device, dtype=torch.int64),
+                torch.empty((2, total, 3, 4), device=x.device, dtype=dtype))
     base, phi = buffers
-    if not _tables_ok(base, phi, total, x):
+    if not _tables_ok(base, phi, total, x, dtype):
         raise ValueError('invalid P2 stencil buffers')
     return base, phi
 
@@ -129,10 +149,18 @@ def _launch_prepare(transfer, x, rule, base, phi, word):
     g = transfer.grid
     limits = [n - 2 for n in g.shape]
     offset = 0
+    mixed = phi.dtype != x.dtype
     for group in rule.groups:
-        call('afsi_b200_p2_prepare', ptr(x), x.shape[0], ptr(group.cells), group.cells.shape[0], ptr(group.values),
-             group.values.shape[0], _lib.doubles(g.origin), _lib.doubles(g.spacing), _lib.doubles(limits),
-             ptr(base), ptr(phi), rule.point_count, offset, ptr(word), dtype_code(x.dtype), stream(x.device))
+        if mixed:
+            call('afsi_b200_fe_prepare_mixed', 10, ptr(x), x.shape[0], ptr(group.cells), group.cells.shape[0],
+                 ptr(group.values), group.values.shape[0], _lib.doubles(g.origin), _lib.doubles(g.spacing),
+                 _lib.doubles(limits), ptr(base), ptr(phi), rule.point_count, offset, ptr(word),
+                 dtype_code(phi.dtype), stream(x.device))
+        else:
+            call('afsi_b200_p2_prepare', ptr(x), x.shape[0], ptr(group.cells), group.cells.shape[0],
+                 ptr(group.values), group.values.shape[0], _lib.doubles(g.origin), _lib.doubles(g.spacing),
+                 _lib.doubles(limits), ptr(base), ptr(phi), rule.point_count, offset, ptr(word),
+                 dtype_code(x.dtype), stream(x.device))
         offset += group.weights.numel()
 
 
@@ -148,7 +176,7 @@ def prepare(transfer, x, rule, *, buffers=None):
     of every group; ``ValueError`` when a point's support leaves the grid."""
     _lib.require_cuda(x)
     x = x.contiguous()
-    base, phi = _tables(x, rule.point_count, buffers)
+    base, phi = _tables(x, rule.point_count, buffers, getattr(transfer, 'transfer_dtype', x.dtype))
     word = _lib.status_word(x.device)
     word.zero_()
     _launch_prepare(transfer, x, rule, base, phi, word)
@@ -165,21 +193,31 @@ def spread(transfer, coefficient, stencil, *, events=None):
     events) bracket the native launches, excluding the output zero-fill."""
     _lib.require_cuda(coefficient)
     coefficient = coefficient.contiguous()
+    if coefficient.dtype != stencil.phi.dtype:
+        raise ValueError('P2 spread coefficient dtype must match the stencil weights')
     g = transfer.grid
     fields = g.zeros(device=coefficient.device, dtype=coefficient.dtype)
     word = _lib.status_word(coefficient.device)
     offset = 0
     if events is not None:
         events[0].record()
-    for group in stencil.rule.groups:
+    for group, (values, weights) in zip(stencil.rule.groups, _group_tables(transfer, stencil.rule)):
         call('afsi_b200_p2_spread', ptr(coefficient), coefficient.shape[0], ptr(group.cells), group.cells.shape[0],
-             ptr(group.values), group.values.shape[0], ptr(group.weights), ptr(stencil.base), ptr(stencil.phi),
+             ptr(values), values.shape[0], ptr(weights), ptr(stencil.base), ptr(stencil.phi),
              stencil.base.shape[1], offset, *(ptr(f) for f in fields), *g.shape, float(g.volume), ptr(word),
              dtype_code(coefficient.dtype), stream(coefficient.device))
         offset += group.weights.numel()
     if events is not None:
         events[1].record()
     return fields
+
+
+def _group_tables(transfer, rule):
+    """Rule tables in the transfer's dtype (the reference's transfer objects
+    have no precision form: their own tables)."""
+    if hasattr(transfer, 'group_tables'):
+        return transfer.group_tables(rule)
+    return [(g.values, g.weights) for g in rule.groups]
 
 
 def _velocity(transfer, velocity):
@@ -193,15 +231,17 @@ def assemble_velocity(transfer, velocity, stencil, *, events=None):
     nodal right-hand side rhs[a] = Σ_q N[q,a] W U(x_q).  ``events`` bracket
     the native launches."""
     velocity = _velocity(transfer, velocity)
+    if velocity[0].dtype != stencil.phi.dtype:
+        raise ValueError('P2 velocity dtype must match the stencil weights')
     rhs = torch.zeros_like(transfer.diagonal)
     word = _lib.status_word(rhs.device)
     g = transfer.grid
     offset = 0
     if events is not None:
         events[0].record()
-    for group in stencil.rule.groups:
+    for group, (values, weights) in zip(stencil.rule.groups, _group_tables(transfer, stencil.rule)):
         call('afsi_b200_p2_gather_assemble', *(ptr(v) for v in velocity), ptr(group.cells), group.cells.shape[0],
-             ptr(group.values), group.values.shape[0], ptr(group.weights), ptr(stencil.base), ptr(stencil.phi),
+             ptr(values), values.shape[0], ptr(weights), ptr(stencil.base), ptr(stencil.phi),
              stencil.base.shape[1], offset, ptr(rhs), rhs.shape[0], *g.shape, ptr(word), dtype_code(rhs.dtype),
              stream(rhs.device))
         offset += group.weights.numel()
@@ -220,9 +260,9 @@ def assemble_velocity_deterministic(transfer, velocity, stencil):
     word = _lib.status_word(local.device)
     g = transfer.grid
     offset, first = 0, 0
-    for group in rule.groups:
+    for group, (values, weights) in zip(rule.groups, _group_tables(transfer, rule)):
         call('afsi_b200_p2_gather_local', *(ptr(v) for v in velocity), ptr(group.cells), group.cells.shape[0],
-             ptr(group.values), group.values.shape[0], ptr(group.weights), ptr(stencil.base), ptr(stencil.phi),
+             ptr(values), values.shape[0], ptr(weights), ptr(stencil.base), ptr(stencil.phi),
              stencil.base.shape[1], offset, local[first:].data_ptr(), *g.shape, ptr(word), dtype_code(local.dtype),
              stream(local.device))
         offset += group.weights.numel()

@@ -369,6 +369,61 @@ def serving_form_row(device, count=400):
     return out
 
 
+def precision_form_row(grid, X, cells, coef, vel, rhs, device, steps=20):
+    """Precision form of the step on the bench workload: FP64 positions and
+    bases, FP32 weight tables and transfers, and the pressure solve as FP32
+    V-cycles inside FP64 iterative refinement to the FP64 tolerance.  CUDA
+    events around `steps` steps; errors are the largest differences from the
+    FP64 step's outputs over their largest values."""
+    from afsi_gpu_b200 import p2_cuda_transfer as p2t
+    from afsi_gpu_b200.multigrid import GeometricMultigrid, RefinedMultigrid
+    x = torch.as_tensor(X, device=device)
+    c64 = torch.as_tensor(coef, device=device)
+    v64 = tuple(torch.as_tensor(v, device=device) for v in vel)
+    r64 = torch.as_tensor(rhs, device=device)
+    tr64 = p2t.P2Transfer(grid, x, torch.as_tensor(cells, device=device))
+    tr32 = p2t.P2Transfer(grid, x, torch.as_tensor(cells, device=device), transfer_dtype=torch.float32)
+    mg64 = GeometricMultigrid(grid, device=device, backend='b200-graph')
+    mg32 = RefinedMultigrid(grid, device=device)
+    c32, v32 = c64.float(), tuple(v.float() for v in v64)
+
+    def step(tr, mg, c, v):
+        st = tr.prepare(x)
+        return tr.spread(c, st), tr.assemble_velocity(v, st), mg.solve(r64)
+
+    ref = step(tr64, mg64, c64, v64)
+    stream = torch.cuda.current_stream(device)
+
+    def timed(mg):
+        for _ in range(3):
+            out = step(tr32, mg, c32, v32)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        e0.record(stream)
+        for _ in range(steps):
+            out = step(tr32, mg, c32, v32)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        return out, e0.elapsed_time(e1) / steps
+
+    def rel(a, b):
+        return float((a.double() - b.double()).abs().max() / b.double().abs().max())
+
+    rows = {}
+    for name, mg in (('fp32_transfers_refined_mg', mg32), ('fp32_transfers_fp64_mg', mg64)):
+        out, ms = timed(mg)
+        info = out[2][1]
+        rows[name] = dict(steps_per_s=1e3 / ms, ms_per_step=ms, transfer_dtype='f32', positions='f64',
+                          mg=(f"FP32 V-cycles in FP64 refinement, {info['refinements']} refinements, "
+                              f"{info['cycles']} FP32 cycles" if 'refinements' in info else
+                              f"FP64 V-cycles, {info['cycles']} cycles"),
+                          residual=info['residual_norm'], tolerance=info['tolerance'],
+                          error_vs_fp64=dict(spread=max(rel(a, b) for a, b in zip(out[0], ref[0])),
+                                             gather_assemble=rel(out[1], ref[1]),
+                                             pressure=rel(out[2][0], ref[2][0])))
+    return rows
+
+
 def load_traffic():
     path = ROOT / 'profiles' / 'traffic.json'
     try:
@@ -647,6 +702,7 @@ def run_b200(args):
         extra = args.rows == 'all'
         mass = mass_pcg_row(X, cells, device, pk['hbm_gbs']) if extra else None
         forms = mg_forms_row(grid, rhs, device) if extra else None
+        precision = precision_form_row(grid, X, cells, coef, vel, rhs, device) if extra else None
         batch = batch_form_row(device) if extra else None
         serving = serving_form_row(device) if extra else None
         step_ms = np.array([ev[0].elapsed_time(ev[4]) for ev in phases])
@@ -674,6 +730,7 @@ def run_b200(args):
             oracle_error=errors,
             mass_pcg=mass,
             mg_forms=forms,
+            precision_form=precision,
             batch_form=batch,
             serving_form=serving,
             cpu_baseline=cpu)

@@ -93,6 +93,17 @@ int32_t afsi_b200_p2_prepare(const void* x, int64_t nodes, const int64_t* cells,
     int64_t* base, void* phi, int64_t total, int64_t offset, int32_t* status,
     int32_t dtype, afsi_stream_t stream);
 
+/* Precision form of the P2 / P1 prepares (nodes_per_cell 10 or 4): positions,
+ * bases and weights formed in FP64 from FP64 x and N exactly as
+ * afsi_b200_p2_prepare / afsi_b200_p1_prepare do, the weights stored in
+ * weight_dtype (AFSI_F32: the rounded FP64 weights), so the bases are the
+ * FP64 bases.  No counterpart in the reference (its tables take the
+ * positions' dtype). */
+int32_t afsi_b200_fe_prepare_mixed(int32_t nodes_per_cell, const double* x, int64_t nodes, const int64_t* cells,
+    int64_t elements, const double* N, int64_t nq, const double* origin, const double* spacing,
+    const double* limits, int64_t* base, void* phi, int64_t total, int64_t offset, int32_t* status,
+    int32_t weight_dtype, afsi_stream_t stream);
+
 /* Adaptive quadrature order per P2 element: ceil(density * D / dx), at least
  * min_order, D the diameter of the element's Bernstein control points
  * (_orders_p2, mac/adaptive_transfer.py:182-187, which the reference

@@ -257,6 +257,36 @@ def test_p2_shell_against_oracle(dtype, n):
     cuda_ib.check()
 
 
+def test_p2_precision_form_fp32_transfers_with_fp64_positions():
+    """Precision form: FP64 positions and bases (bit-exact with the FP64
+    oracle), weights the FP64 weights rounded once to FP32, FP32 spread and
+    gather-assemble within 3e-6 of the field scale of the FP64 oracle."""
+    X, cells = synthetic.p2_shell(2, 12, 16, **SMALL)
+    grid = MACGrid((64, 64, 64), (1., 1., 1.))
+    tr = p2t.P2Transfer(grid, t(X), t(cells), max_order=22, transfer_dtype=torch.float32)
+    st = tr.prepare(t(X))
+    groups = [(gr.cells.cpu().numpy(), gr.values.cpu().numpy()) for gr in st.rule.groups]
+    ob, op, invalid = oracle.p2_prepare(X, groups, grid.origin, grid.spacing, grid.shape)
+    assert invalid == 0 and st.phi.dtype == torch.float32
+    assert np.array_equal(st.base.cpu().numpy(), ob)
+    assert np.array_equal(st.phi.cpu().numpy(), op.astype(np.float32))
+    st2 = tr.prepare(t(X))  # the speculative (rule reused) path keeps the precision form
+    assert st2.phi.dtype == torch.float32 and torch.equal(st2.phi, st.phi)
+    full = [(gr.cells.cpu().numpy(), gr.values.cpu().numpy(), gr.weights.cpu().numpy()) for gr in st.rule.groups]
+    coef = np.random.default_rng(8).standard_normal((X.shape[0], 3))
+    fields = tr.spread(t(coef, torch.float32), st)
+    ref = oracle.p2_spread(coef, full, ob, op, grid.shape, grid.volume)
+    for c in range(3):
+        assert fields[c].dtype == torch.float32
+        close(fields[c].reshape(-1).double(), ref[c], **scaled_tol(ref[c], 3e-6))
+    vel = synthetic.fourier_velocity3d(grid, seed=1)
+    rhs = tr.assemble_velocity(tuple(v.to(DEV, torch.float32) for v in vel), st)
+    ref = oracle.p2_gather_assemble([v.numpy() for v in vel], full, ob, op, grid.shape, X.shape[0])
+    close(rhs.double(), ref, **scaled_tol(ref, 3e-6))
+    with pytest.raises(ValueError, match='dtype must match'):
+        tr.spread(t(coef), st)
+
+
 def test_p2_deterministic_assembly_is_bitwise_reproducible():
     X, cells = synthetic.p2_shell(2, 12, 16, **SMALL)
     grid = MACGrid((32, 32, 32), (1., 1., 1.))
