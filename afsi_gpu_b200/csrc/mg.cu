@@ -222,6 +222,16 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_kernel(const T* __restr
     coarse_cycle<BC, T, TC>(reinterpret_cast<T*>(smem_raw), rhs_global, rhs_sum, p_global, p_out, cinv, cl, smooth);
 }
 
+template <int BC, class T, class TC>
+__global__ void __launch_bounds__(kCoarseThreads) coarse_rb_kernel(const T* __restrict__ rhs_global,
+                                                                  const T* p_global, T* p_out,
+                                                                  const TC* __restrict__ cinv, CoarseLevels<T> cl,
+                                                                  int smooth) {
+    pdl_enter();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    coarse_cycle_rb<BC, T, TC>(reinterpret_cast<T*>(smem_raw), rhs_global, p_global, p_out, cinv, cl, smooth);
+}
+
 // ---- red-black Gauss-Seidel V-cycle (selectable smoother) ----
 //
 // A method change beside the reference's weighted Jacobi (mac/multigrid.py:
@@ -728,7 +738,27 @@ struct RbRunner {
     cudaStream_t stream;
     SiteTable st;
     Lv<T> lv[AFSI_MG_MAX_LEVELS];
+    int first_coarse;  // levels from here run in one CTA (coarse_rb_kernel)
     static constexpr bool singular = singular_bc(BC);
+
+    int32_t coarse(int l) {
+        CoarseLevels<T> cl;
+        for (int k = 0; k < plan->levels; ++k) cl.lv[k] = lv[k];
+        cl.first = l;
+        cl.last = plan->levels - 1;
+        int64_t cells = 0;
+        for (int k = l; k < plan->levels; ++k) cells += lv[k].n;
+        const size_t bytes = (size_t(cells) * 3 + 64 * size_t(plan->levels - l)) * sizeof(T);
+        static bool configured = false;  // once per instantiation, before any graph capture of it
+        if (!configured) {
+            cudaFuncSetAttribute(coarse_rb_kernel<BC, T, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 210 * 1024);
+            configured = true;
+        }
+        return launch_pdl("mg red-black coarse block", coarse_rb_kernel<BC, T, TC>, dim3(1), dim3(kCoarseThreads),
+                          bytes, stream, static_cast<const T*>(R(l)), static_cast<const T*>(l == 0 ? P(0) : nullptr),
+                          P(l), static_cast<const TC*>(plan->coarse_inverse), cl, plan->smooth);
+    }
 
     T* P(int l) const { return static_cast<T*>(plan->level[l].p); }
     T* R(int l) const { return static_cast<T*>(plan->level[l].rhs); }
@@ -756,6 +786,7 @@ struct RbRunner {
     int32_t level(int l) {
         const int last = plan->levels - 1;
         int32_t rc;
+        if (l == first_coarse && l < last) return coarse(l);
         if (l == last)
             return launch_pdl("mg dense coarse solve", rb_dense_kernel<BC, T, TC>, dim3(1), dim3(kDenseThreads), 0,
                               stream, static_cast<const T*>(R(l)), P(l),
@@ -772,7 +803,7 @@ struct RbRunner {
                             static_cast<const double*>(st.s[l + 1][2].result));
             if (rc) return rc;
         }
-        if (l + 1 < last) {
+        if (l + 1 < last && l + 1 != first_coarse) {
             const cudaError_t err = cudaMemsetAsync(P(l + 1), 0, size_t(lv[l + 1].n) * sizeof(T), stream);
             if (err != cudaSuccess) return fail(AFSI_ERR_CUDA, "mg zero start: %s", cudaGetErrorString(err));
         }
@@ -788,6 +819,16 @@ struct RbRunner {
     int32_t run(int cycles) {
         for (int l = 0; l < plan->levels; ++l)
             lv[l] = make_level<T>(plan->level[l].shape, plan->level[l].h2, plan->level[l].inv_h2, plan->dim);
+        // first level whose three arrays, with every coarser level's, fit one CTA's shared memory
+        first_coarse = plan->levels - 1;
+        for (int l = 0; l < plan->levels; ++l) {
+            int64_t cells = 0;
+            for (int k = l; k < plan->levels; ++k) cells += lv[k].n;
+            if (lv[l].n <= kCoarseCells && (cells * 3 + 64 * (plan->levels - l)) * int64_t(sizeof(T)) <= 200 * 1024) {
+                first_coarse = l;
+                break;
+            }
+        }
         for (int c = 0; c < cycles; ++c) {
             int32_t rc = level(0);
             if (!rc && singular) rc = shift_to_mean_zero(P(0), 0, st.s[0][0]);

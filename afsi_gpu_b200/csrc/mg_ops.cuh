@@ -567,4 +567,119 @@ __device__ void coarse_cycle(T* smem, const T* __restrict__ rhs_global, const do
     __syncthreads();
 }
 
+// Red-black Gauss-Seidel sweeps of level L in place (omega 1): cells with
+// (x+y+z) even, then odd, p += (R - A p)/diag (fast block arithmetic).
+template <int BC, class T>
+__device__ void block_smooth_rb(T* P, const T* R, const Lv<T>& L, const FastCoords<T>& fc, int smooth) {
+    const int n = int(L.n);
+    for (int s = 0; s < smooth; ++s) {
+        for (int color = 0; color < 2; ++color) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                int x, y, z;
+                fc.get(i, L, x, y, z);
+                if (((x + y + z) & 1) != color) continue;
+                const T pc = P[i];
+                P[i] = pc + (R[i] - block_apply<BC>(P, i, x, y, z, L, pc)) / diag_at<BC>(x, y, z, L);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Levels first..last of one red-black V-cycle in one CTA: rhs of level
+// `first` from global memory (already mean-free for singular problems), p
+// from p_global or zero; coarse right-hand sides shifted to mean zero, zero
+// coarse starts, the dense coarsest solve (mean removed for singular
+// problems), prolongation and post-smoothing; the final p[first] goes to p_out.
+template <int BC, class T, class TC>
+__device__ void coarse_cycle_rb(T* smem, const T* __restrict__ rhs_global, const T* p_global, T* p_out,
+                                const TC* __restrict__ cinv, const CoarseLevels<T>& cl, int smooth) {
+    __shared__ double red[2][32];
+    constexpr bool singular = singular_bc(BC);
+    int rt = 0;
+    const int f = cl.first, last = cl.last;
+    auto level_base = [&](int l) {
+        int64_t off = 0;
+        for (int k = f; k < l; ++k) off += 3 * cl.lv[k].n;
+        return smem + off;
+    };
+    {
+        T* P = level_base(f);
+        T* R = P + 2 * cl.lv[f].n;
+        for (int i = threadIdx.x; i < cl.lv[f].n; i += blockDim.x) {
+            R[i] = rhs_global[i];
+            P[i] = p_global ? p_global[i] : T(0);
+        }
+    }
+    __syncthreads();
+    for (int l = f; l < last; ++l) {
+        const Lv<T>& L = cl.lv[l];
+        const Lv<T>& C = cl.lv[l + 1];
+        T* P = level_base(l);
+        const T* R = P + 2 * L.n;
+        T* Pc = level_base(l + 1);
+        T* Rc = Pc + 2 * C.n;
+        FastCoords<T> fcL, fcC;
+        fcL.init(L);
+        fcC.init(C);
+        block_smooth_rb<BC>(P, R, L, fcL, smooth);
+        double acc = 0.0;
+        for (int c = threadIdx.x; c < C.n; c += blockDim.x) {
+            int cx, cy, cz;
+            fcC.get(c, C, cx, cy, cz);
+            const T v = block_restrict<BC>(P, R, cx, cy, cz, L);
+            Rc[c] = v;
+            Pc[c] = T(0);
+            acc += double(v);
+        }
+        if (singular) {
+            const T m = T(block_sum_all(acc, red[rt]) / double(C.n));
+            rt ^= 1;
+            for (int c = threadIdx.x; c < C.n; c += blockDim.x) Rc[c] = Rc[c] - m;
+        }
+        __syncthreads();
+    }
+    {
+        const Lv<T>& L = cl.lv[last];
+        T* P = level_base(last);
+        const T* R = P + 2 * L.n;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+        double acc = 0.0;
+        for (int r = warp; r < L.n; r += warps) {
+            double s = 0.0;
+            for (int j = lane; j < L.n; j += 32) s += double(cinv[int64_t(r) * L.n + j]) * double(R[j]);
+            s = warp_sum(s);
+            if (lane == 0) {
+                P[r] = T(s);
+                acc += double(T(s));
+            }
+        }
+        if (singular) {
+            const T m = T(block_sum_all(acc, red[rt]) / double(L.n));
+            rt ^= 1;
+            for (int r = threadIdx.x; r < L.n; r += blockDim.x) P[r] = P[r] - m;
+        }
+        __syncthreads();
+    }
+    for (int l = last - 1; l >= f; --l) {
+        const Lv<T>& L = cl.lv[l];
+        const Lv<T>& C = cl.lv[l + 1];
+        T* P = level_base(l);
+        const T* R = P + 2 * L.n;
+        const T* corr = level_base(l + 1);
+        FastCoords<T> fcL;
+        fcL.init(L);
+        for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
+            int x, y, z;
+            fcL.get(i, L, x, y, z);
+            P[i] = P[i] + prolong_at<BC>(corr, x, y, z, C, T(0));
+        }
+        __syncthreads();
+        block_smooth_rb<BC>(P, R, L, fcL, smooth);
+    }
+    const T* P = level_base(f);
+    for (int i = threadIdx.x; i < cl.lv[f].n; i += blockDim.x) p_out[i] = P[i];
+    __syncthreads();
+}
+
 }  // namespace afsi
