@@ -234,11 +234,14 @@ _status = {}
 
 
 def status_word(device):
-    """Per-device int32 status word that kernels OR their AFSI_FLAG_* bits into."""
-    key = torch.device(device).index if torch.device(device).index is not None else torch.cuda.current_device()
+    """Int32 status word that kernels OR their AFSI_FLAG_* bits into, one per
+    device and current stream, so that work on different streams (threads of
+    a server, say) never clears or reads another's flags."""
+    index = torch.device(device).index if torch.device(device).index is not None else torch.cuda.current_device()
+    key = (index, torch.cuda.current_stream(index).cuda_stream)
     word = _status.get(key)
     if word is None:
-        word = torch.zeros((), dtype=torch.int32, device=torch.device('cuda', key))
+        word = torch.zeros((), dtype=torch.int32, device=torch.device('cuda', index))
         _status[key] = word
     return word
 
