@@ -61,6 +61,13 @@ _SIGNATURES = {
                             c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p],
     'afsi_b200_fe_prepare_mixed': [c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, P_F64, P_F64,
                                    P_F64, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int32, c_void_p],
+    'afsi_b200_det_plan_bytes': [c_int64, c_int64, c_int64, c_int64, c_int32],
+    'afsi_b200_det_plan': [c_void_p, c_int64, c_int64, c_int64, c_int64, c_void_p, c_int64, c_void_p, c_int32,
+                           c_void_p],
+    'afsi_b200_det_spread': [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_int64, c_int64, c_void_p, c_int64,
+                             c_void_p, c_void_p, c_void_p, c_int32, c_void_p],
+    'afsi_b200_p2_point_forces': [c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_int64,
+                                  ctypes.c_double, c_void_p, c_void_p, c_int32, c_void_p],
     'afsi_b200_p1_prepare': [c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, P_F64, P_F64, P_F64,
                              c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int32, c_void_p],
     'afsi_b200_p1_orders': [c_void_p, c_int64, c_void_p, c_int64, ctypes.c_double, ctypes.c_double, c_int64,
@@ -155,7 +162,8 @@ _RESTYPES = {'afsi_b200_last_error': ctypes.c_char_p, 'afsi_b200_mg_scratch_byte
              'afsi_b200_launch_count': ctypes.c_int64, 'afsi_b200_mg_sync_bytes': ctypes.c_int64,
              'afsi_b200_p1_plan_scratch_bytes': ctypes.c_int64, 'afsi_b200_hash_csr_scratch_bytes': ctypes.c_int64,
              'afsi_b200_pcg_scratch_bytes': ctypes.c_int64, 'afsi_b200_mg_refine_scratch_bytes': ctypes.c_int64,
-             'afsi_b200_stokes_partial_blocks': ctypes.c_int64, 'afsi_b200_cache_scratch_bytes': ctypes.c_int64}
+             'afsi_b200_stokes_partial_blocks': ctypes.c_int64, 'afsi_b200_cache_scratch_bytes': ctypes.c_int64,
+             'afsi_b200_det_plan_bytes': ctypes.c_int64}
 
 
 def exported_symbols():

@@ -95,7 +95,32 @@ class P2Transfer:
         return SharedAdaptiveStencil(base, phi, rule)
 
     def spread(self, coefficient, stencil):
+        if self.deterministic:
+            return spread_deterministic(self, coefficient, stencil)
         return spread(self, coefficient, stencil)
+
+    def det_plan(self, stencil):
+        """Tile-sorted rows of `stencil` for the deterministic spread (built once per stencil)."""
+        key = (stencil.base.data_ptr(), stencil.base.shape[1], stencil.phi.dtype)
+        if getattr(self, '_det', None) is not None and self._det[0] == key:
+            return self._det[1]
+        g = self.grid
+        total = stencil.base.shape[1]
+        code = dtype_code(stencil.phi.dtype)
+        n = _lib.load().afsi_b200_det_plan_bytes(total, *g.shape, code)
+        if n < 0:
+            raise ValueError('stencil too large for the deterministic spread')
+        plan = torch.empty(int(n), device=stencil.base.device, dtype=torch.uint8)
+        word = _lib.status_word(plan.device)
+        word.zero_()
+        call('afsi_b200_det_plan', ptr(stencil.base), total, *g.shape, ptr(plan), plan.numel(), ptr(word), code,
+             stream(plan.device))
+        flags = int(word.item())
+        if flags:
+            word.zero_()
+            raise RuntimeError('P2 stencil support outside the MAC face arrays')
+        self._det = (key, plan)
+        return plan
 
     def assemble_velocity(self, velocity, stencil):
         if self.deterministic:
@@ -218,6 +243,33 @@ def _group_tables(transfer, rule):
     if hasattr(transfer, 'group_tables'):
         return transfer.group_tables(rule)
     return [(g.values, g.weights) for g in rule.groups]
+
+
+def spread_deterministic(transfer, coefficient, stencil):
+    """:func:`spread` without atomics and bitwise reproducible: point forces
+    (``afsi_b200_p2_point_forces``), then the tile-sorted deterministic spread
+    (``afsi_b200_det_spread``) over the stencil's plan."""
+    _lib.require_cuda(coefficient)
+    coefficient = coefficient.contiguous()
+    if coefficient.dtype != stencil.phi.dtype:
+        raise ValueError('P2 spread coefficient dtype must match the stencil weights')
+    g = transfer.grid
+    total = stencil.base.shape[1]
+    plan = transfer.det_plan(stencil)
+    force = torch.empty((total, 3), device=coefficient.device, dtype=coefficient.dtype)
+    word = _lib.status_word(coefficient.device)
+    code = dtype_code(coefficient.dtype)
+    s = stream(coefficient.device)
+    offset = 0
+    for group, (values, weights) in zip(stencil.rule.groups, _group_tables(transfer, stencil.rule)):
+        call('afsi_b200_p2_point_forces', ptr(coefficient), coefficient.shape[0], ptr(group.cells),
+             group.cells.shape[0], ptr(values), values.shape[0], ptr(weights), total, offset, float(g.volume),
+             ptr(force), ptr(word), code, s)
+        offset += group.weights.numel()
+    fields = g.zeros(device=coefficient.device, dtype=coefficient.dtype)
+    call('afsi_b200_det_spread', ptr(force), ptr(stencil.base), ptr(stencil.phi), total, *g.shape, ptr(plan),
+         plan.numel(), *(ptr(f) for f in fields), code, s)
+    return fields
 
 
 def _velocity(transfer, velocity):

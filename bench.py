@@ -424,6 +424,36 @@ def precision_form_row(grid, X, cells, coef, vel, rhs, device, steps=20):
     return rows
 
 
+def deterministic_row(step, coef, device, reps=10):
+    """The P2 spread of the step in its deterministic mode (tile-sorted,
+    atomic-free, bitwise reproducible) beside the atomic spread: CUDA events
+    around `reps` spreads each (the plan is built once per stencil, outside
+    the timing), and the largest difference between the two."""
+    from afsi_gpu_b200 import p2_cuda_transfer as p2t
+    tr = step.tr
+    st = tr.prepare(step.x)
+    c = torch.as_tensor(coef, device=device)
+    det = p2t.P2Transfer(step.grid, step.x, step.cells, deterministic=True)
+    det.rules = tr.rules
+    a = tr.spread(c, st)
+    d = det.spread(c, st)
+    again = det.spread(c, st)
+    stream = torch.cuda.current_stream(device)
+    out = {}
+    for name, fn in (('atomic', lambda: tr.spread(c, st)), ('deterministic', lambda: det.spread(c, st))):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        out[f'{name}_ms'] = e0.elapsed_time(e1) / reps
+    out['bitwise_reproducible'] = all(torch.equal(x, y) for x, y in zip(d, again))
+    out['max_rel_diff_vs_atomic'] = max(float((x - y).abs().max() / y.abs().max()) for x, y in zip(d, a))
+    return out
+
+
 def load_traffic():
     path = ROOT / 'profiles' / 'traffic.json'
     try:
@@ -703,6 +733,7 @@ def run_b200(args):
         mass = mass_pcg_row(X, cells, device, pk['hbm_gbs']) if extra else None
         forms = mg_forms_row(grid, rhs, device) if extra else None
         precision = precision_form_row(grid, X, cells, coef, vel, rhs, device) if extra else None
+        deterministic = deterministic_row(step, coef, device) if extra else None
         batch = batch_form_row(device) if extra else None
         serving = serving_form_row(device) if extra else None
         step_ms = np.array([ev[0].elapsed_time(ev[4]) for ev in phases])
@@ -731,6 +762,7 @@ def run_b200(args):
             mass_pcg=mass,
             mg_forms=forms,
             precision_form=precision,
+            deterministic_spread=deterministic,
             batch_form=batch,
             serving_form=serving,
             cpu_baseline=cpu)

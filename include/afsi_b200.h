@@ -104,6 +104,30 @@ int32_t afsi_b200_fe_prepare_mixed(int32_t nodes_per_cell, const double* x, int6
     const double* limits, int64_t* base, void* phi, int64_t total, int64_t offset, int32_t* status,
     int32_t weight_dtype, afsi_stream_t stream);
 
+/* Deterministic, atomic-free spread over the shared (2,T,3)/(2,T,3,4)
+ * tables (no counterpart in the reference, whose spreads add atomically).
+ * afsi_b200_det_plan (once per stencil): each row's support is binned by
+ *   its owning 8x8x8 face tile per component and the rows sorted by tile
+ *   (stable); rows whose support leaves the face array flag AFSI_FLAG_INDEX
+ *   and are left out.  plan: afsi_b200_det_plan_bytes() device bytes.
+ * afsi_b200_det_spread: u_c += the spread of force[:, c] (force (T,3), one
+ *   value per table row, already multiplied by W / volume): per tile, the
+ *   rows in sorted order into per-warp shared-memory boxes summed in warp
+ *   order, then every face adds the covering tiles' boxes in a fixed order.
+ *   Bitwise reproducible; equal to the atomic spreads to rounding.
+ * afsi_b200_p2_point_forces: force rows offset..offset+elements*nq of one
+ *   P2 group, (sum_a N[q,a] value[cell_a]) * W[e,q] / volume as the P2
+ *   spread forms them (p2_spread_, mac/csrc/p2_transfer.cu:98-188). */
+int64_t afsi_b200_det_plan_bytes(int64_t total, int64_t nx, int64_t ny, int64_t nz, int32_t dtype);
+int32_t afsi_b200_det_plan(const int64_t* base, int64_t total, int64_t nx, int64_t ny, int64_t nz, void* plan,
+    int64_t plan_bytes, int32_t* status, int32_t dtype, afsi_stream_t stream);
+int32_t afsi_b200_det_spread(const void* force, const int64_t* base, const void* phi, int64_t total, int64_t nx,
+    int64_t ny, int64_t nz, void* plan, int64_t plan_bytes, void* u0, void* u1, void* u2, int32_t dtype,
+    afsi_stream_t stream);
+int32_t afsi_b200_p2_point_forces(const void* value, int64_t nodes, const int64_t* cells, int64_t elements,
+    const void* N, int64_t nq, const void* W, int64_t total, int64_t offset, double volume, void* force,
+    int32_t* status, int32_t dtype, afsi_stream_t stream);
+
 /* Adaptive quadrature order per P2 element: ceil(density * D / dx), at least
  * min_order, D the diameter of the element's Bernstein control points
  * (_orders_p2, mac/adaptive_transfer.py:182-187, which the reference

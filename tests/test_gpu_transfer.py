@@ -287,6 +287,32 @@ def test_p2_precision_form_fp32_transfers_with_fp64_positions():
         tr.spread(t(coef), st)
 
 
+@pytest.mark.parametrize('dtype', [torch.float64, torch.float32])
+def test_p2_deterministic_spread_is_reproducible_and_matches(dtype):
+    """Tile-sorted, atomic-free spread: bitwise equal over repeated runs,
+    equal to the atomic spread and to the FP64 oracle within the parity bar
+    (1e-12 FP64; 3e-6 for FP32 transfers beside FP64 positions)."""
+    X, cells = synthetic.p2_shell(2, 12, 16, **SMALL)
+    grid = MACGrid((64, 64, 64), (1., 1., 1.))
+    kw = dict(max_order=22, transfer_dtype=dtype)
+    det = p2t.P2Transfer(grid, t(X), t(cells), deterministic=True, **kw)
+    atomic = p2t.P2Transfer(grid, t(X), t(cells), **kw)
+    st = det.prepare(t(X))
+    coef = np.random.default_rng(11).standard_normal((X.shape[0], 3))
+    c = t(coef, dtype)
+    first = det.spread(c, st)
+    second = det.spread(c, st)
+    reference = atomic.spread(c, st)
+    groups = [(gr.cells.cpu().numpy(), gr.values.cpu().numpy(), gr.weights.cpu().numpy()) for gr in st.rule.groups]
+    ob, op, _ = oracle.p2_prepare(X, [(g[0], g[1]) for g in groups], grid.origin, grid.spacing, grid.shape)
+    ref = oracle.p2_spread(coef, groups, ob, op, grid.shape, grid.volume)
+    tol = 1e-12 if dtype == torch.float64 else 3e-6
+    for k in range(3):
+        assert torch.equal(first[k], second[k])
+        close(first[k].double(), reference[k].double().cpu().numpy(), **scaled_tol(reference[k].double().cpu().numpy(), tol))
+        close(first[k].reshape(-1).double(), ref[k], **scaled_tol(ref[k], tol))
+
+
 def test_p2_deterministic_assembly_is_bitwise_reproducible():
     X, cells = synthetic.p2_shell(2, 12, 16, **SMALL)
     grid = MACGrid((32, 32, 32), (1., 1., 1.))
