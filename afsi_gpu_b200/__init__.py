@@ -7,10 +7,17 @@ through the C-ABI of ``include/afsi_b200.h``.
 Modules
 -------
 cuda_ib            drop-in for ``afsi_torch.mac.cuda_ib`` (+ binning kernels)
-p2_cuda_transfer   drop-in for ``afsi_torch.mac.p2_cuda_transfer`` (+ P2Transfer)
-multigrid          GeometricMultigrid / ChannelMultigrid / B200Kernels / MGOptions
+p2_cuda_transfer   drop-in for ``afsi_torch.mac.p2_cuda_transfer`` (+ P2Transfer, FP32
+                   and deterministic modes)
+p1_csr             P1 hash contraction to CSR, cached-pattern maintenance, P1CSRTransfer
+multigrid          GeometricMultigrid / ChannelMultigrid / DirichletMultigrid / RefinedMultigrid /
+                   B200Kernels / MGOptions (Jacobi or red-black smoothing)
+mass               consistent-mass Jacobi-PCG (MassSolver / GraphMassSolver)
+helmholtz          CN Helmholtz kernels and workspace, Stokes residual reductions
+batch              batching form: many 2D instances per step, autotuned schedule
+serving            serving form: continuous-batching request loop
 grid               MACGrid / ChannelGrid
-quadrature         adaptive conical P2 interaction rules
+quadrature         adaptive conical P2 / P1 interaction rules
 synthetic          seeded inputs of the benchmark configurations
 dropin             switch an installed ``afsi_torch`` onto these kernels
 """

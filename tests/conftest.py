@@ -1,5 +1,4 @@
 """Shared pytest configuration: the ``gpu`` marker and fixture loading."""
-import os
 import sys
 from pathlib import Path
 import numpy as np

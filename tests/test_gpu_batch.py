@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 import torch
 from oracle import ib as oracle
-from afsi_gpu_b200.batch import BatchedChannels, Schedule, seeded_batch
+from afsi_gpu_b200.batch import Schedule, seeded_batch
 
 pytestmark = pytest.mark.gpu
 DEV = 'cuda'
@@ -21,11 +21,6 @@ def _small(dtype, count=6, seed=4):
     return seeded_batch(count, seed=seed, shapes=((128, 32), (256, 64), (384, 96)), points=(2000, 6000),
                         device=DEV, transfer_dtype=dtype,
                         schedule=Schedule(streams=3, order='largest-first', smoother='jacobi', cycles=3))
-
-
-def _host(b, i, name):
-    lo, hi = b.point_offsets[i], b.point_offsets[i + 1]
-    return getattr(b, name)[lo:hi].double().cpu().numpy()
 
 
 @pytest.mark.parametrize('dtype', [torch.float64, torch.float32])

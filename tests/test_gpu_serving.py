@@ -5,7 +5,6 @@ pressure solves and interpolated velocities are bitwise equal (deterministic
 kernels, same inputs), spread fields equal to 1e-12 of their scale (the
 spread's L2 atomics may add in another order).
 """
-import numpy as np
 import pytest
 import torch
 from afsi_gpu_b200.serving import Request, Server, mix, request_bytes
