@@ -130,6 +130,9 @@ _SIGNATURES = {
     'afsi_b200_mg_refine_residual': [c_void_p, c_void_p, c_void_p, P_I64, P_F64, c_int32, c_int32, c_void_p, c_void_p,
                                      c_void_p],
     'afsi_b200_mg_refine_correct': [c_void_p, c_void_p, c_int64, c_void_p],
+    'afsi_b200_mg_batch_table_bytes': [c_void_p, c_int32],
+    'afsi_b200_mg_batch_table': [c_void_p, c_int32, c_void_p, c_void_p, c_int64],
+    'afsi_b200_mg_batch_vcycles': [c_void_p, c_int32, c_void_p, c_int32, c_int32, c_void_p],
     'afsi_b200_batch2d_prepare': [c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_int32,
                                   c_void_p],
     'afsi_b200_batch2d_spread': [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_void_p,
@@ -159,6 +162,7 @@ _SIGNATURES = {
     'afsi_b200_pcg_graph_destroy': [c_void_p],
 }
 _RESTYPES = {'afsi_b200_last_error': ctypes.c_char_p, 'afsi_b200_mg_scratch_bytes': ctypes.c_int64,
+             'afsi_b200_mg_batch_table_bytes': ctypes.c_int64,
              'afsi_b200_launch_count': ctypes.c_int64, 'afsi_b200_mg_sync_bytes': ctypes.c_int64,
              'afsi_b200_p1_plan_scratch_bytes': ctypes.c_int64, 'afsi_b200_hash_csr_scratch_bytes': ctypes.c_int64,
              'afsi_b200_pcg_scratch_bytes': ctypes.c_int64, 'afsi_b200_mg_refine_scratch_bytes': ctypes.c_int64,

@@ -12,14 +12,19 @@ step:
   FP64, weights and transfers in ``transfer_dtype`` (FP32 in the precision
   form);
 * a fixed number of V-cycles per instance on its own FP32 workspace (FP64
-  coarsest solve), the instances spread over ``streams`` capture streams so
-  that their small level kernels overlap on the device;
+  coarsest solve), either batched (``vcycles='batched'``, Jacobi: one launch
+  per level operation for all instances and one launch for all their
+  single-CTA coarse levels, ``afsi_b200_mg_batch_vcycles``) or per instance
+  with the instances spread over ``streams`` capture streams so that their
+  small level kernels overlap on the device;
 * the whole step captured once as a CUDA graph and replayed.
 
-``autotune()`` chooses the schedule (stream count, instance order, smoother
-with the cycle count that reaches the requested FP32 residual reduction on
-every instance) by measuring graph replays, and keeps the fastest.
+``autotune()`` chooses the schedule (batched or per-instance V-cycles, stream
+count, instance order, smoother with the cycle count that reaches the
+requested FP32 residual reduction on every instance) by measuring graph
+replays, and keeps the fastest.
 """
+import ctypes
 from dataclasses import dataclass
 import numpy as np
 import torch
@@ -57,6 +62,49 @@ class Schedule:
     order: str = 'largest-first'
     smoother: str = 'jacobi'
     cycles: int = 6
+    vcycles: str = 'streams'   # 'streams' (per instance over side streams) or 'batched' (Jacobi only)
+
+
+class BatchedVCycles:
+    """Jacobi V-cycles of many channel solvers advanced together
+    (``afsi_b200_mg_batch_vcycles``): per cycle one launch per level operation
+    and depth for all instances, one launch for all single-CTA coarse levels.
+    Each solver's iterates are bitwise those of its own ``advance``.  `sources`
+    (one right-hand side per solver, optional) are copied into the solvers'
+    finest right-hand sides when a run starts."""
+
+    def __init__(self, solvers, sources=None):
+        if not solvers:
+            raise ValueError('no solvers')
+        lib = _lib.load()
+        self.solvers = list(solvers)
+        self.count = len(self.solvers)
+        plans = [mg.workspace.plan for mg in self.solvers]
+        self._plans = (ctypes.POINTER(_lib.MGPlan) * self.count)(*[ctypes.pointer(p) for p in plans])
+        self._sources = None
+        if sources is not None:
+            if len(sources) != self.count:
+                raise ValueError('one right-hand side per solver')
+            for mg, r in zip(self.solvers, sources):
+                w = mg.workspace.rhs[0]
+                if r.shape != w.shape or r.dtype != w.dtype or r.device != w.device or not r.is_contiguous():
+                    raise ValueError("each source must be a contiguous tensor like its solver's right-hand side")
+            self._keep = list(sources)
+            self._sources = (ctypes.c_void_p * self.count)(*[ptr(r) for r in sources])
+        nbytes = lib.afsi_b200_mg_batch_table_bytes(self._plans, self.count)
+        if nbytes < 0:
+            raise ValueError(f'batched V-cycles: {lib.afsi_b200_last_error().decode(errors="replace")}')
+        host = np.zeros(int(nbytes), np.uint8)
+        call('afsi_b200_mg_batch_table', self._plans, self.count, self._sources, host.ctypes.data, int(nbytes))
+        self.table = torch.as_tensor(host).to(self.solvers[0].workspace.p[0].device)
+
+    def run(self, cycles, *, start=True):
+        """`cycles` V-cycles of every solver on the current stream; with
+        `start`, from a zero iterate with the sources as right-hand sides."""
+        if start and self._sources is None:
+            raise ValueError('a start needs right-hand-side sources')
+        call('afsi_b200_mg_batch_vcycles', self._plans, self.count, ptr(self.table), int(cycles), int(start),
+             torch.cuda.current_stream(self.table.device).cuda_stream)
 
 
 class BatchedChannels:
@@ -102,6 +150,7 @@ class BatchedChannels:
         self.gathered = torch.empty((self.total, 2), device=device, dtype=transfer_dtype)
         self.status = torch.zeros(1, device=device, dtype=torch.int32)
         self._solvers = {}
+        self._batched = None
         self.graph = None
 
     # -- pieces of the step
@@ -134,6 +183,12 @@ class BatchedChannels:
         w.p[0].zero_()
         w.vcycles(schedule.cycles)
 
+    def batched(self):
+        """The batched Jacobi V-cycles over the Jacobi workspaces (built once)."""
+        if self._batched is None:
+            self._batched = BatchedVCycles(self.solvers('jacobi'), self.rhs)
+        return self._batched
+
     def order(self, schedule):
         idx = list(range(len(self.grids)))
         if schedule.order == 'largest-first':
@@ -146,6 +201,13 @@ class BatchedChannels:
         schedule = schedule or self.schedule
         main = torch.cuda.current_stream(self.device)
         self.transfers(main)
+        if schedule.vcycles == 'batched':
+            if schedule.smoother != 'jacobi':
+                raise ValueError('batched V-cycles use the Jacobi smoother')
+            self.batched().run(schedule.cycles)
+            return
+        if schedule.vcycles != 'streams':
+            raise ValueError(f'unknown V-cycle schedule {schedule.vcycles!r}')
         side = [torch.cuda.Stream(device=self.device) for _ in range(schedule.streams)]
         for s in side:
             s.wait_stream(main)
@@ -158,6 +220,8 @@ class BatchedChannels:
     def capture(self, schedule=None):
         schedule = schedule or self.schedule
         self.solvers(schedule.smoother)
+        if schedule.vcycles == 'batched':
+            self.batched()
         with torch.cuda.device(self.device):
             warm = torch.cuda.Stream(device=self.device)
             warm.wait_stream(torch.cuda.current_stream(self.device))
@@ -215,8 +279,9 @@ class BatchedChannels:
                  smoothers=('jacobi', 'red-black'), max_cycles=12, replays=5):
         """Fastest schedule whose V-cycles reduce every instance's FP32
         residual by `target`: for each smoother the smallest cycle count that
-        meets the target (measured), then every (streams, order) measured by
-        CUDA-event timing of graph replays.  Returns (schedule, table)."""
+        meets the target (measured), then every (streams, order) and, for
+        Jacobi, the batched V-cycles, measured by CUDA-event timing of graph
+        replays.  Returns (schedule, table)."""
         table = []
         best = None
         for smoother in smoothers:
@@ -229,24 +294,27 @@ class BatchedChannels:
                     break
             if cycles is None:
                 continue
-            for s in streams:
-                for order in orders:
-                    sch = Schedule(streams=s, order=order, smoother=smoother, cycles=cycles)
-                    g, launches = self.capture(sch)
+            candidates = [Schedule(streams=s, order=order, smoother=smoother, cycles=cycles)
+                          for s in streams for order in orders]
+            if smoother == 'jacobi':
+                candidates.append(Schedule(streams=1, order='given', smoother=smoother, cycles=cycles,
+                                           vcycles='batched'))
+            for sch in candidates:
+                g, launches = self.capture(sch)
+                g.replay()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize(self.device)
+                e0.record()
+                for _ in range(replays):
                     g.replay()
-                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                    torch.cuda.synchronize(self.device)
-                    e0.record()
-                    for _ in range(replays):
-                        g.replay()
-                    e1.record()
-                    torch.cuda.synchronize(self.device)
-                    ms = e0.elapsed_time(e1) / replays
-                    table.append(dict(streams=s, order=order, smoother=smoother, cycles=cycles, ms=ms,
-                                      launches=launches))
-                    if best is None or ms < best[0]:
-                        best = (ms, sch)
-                    del g
+                e1.record()
+                torch.cuda.synchronize(self.device)
+                ms = e0.elapsed_time(e1) / replays
+                table.append(dict(streams=sch.streams, order=sch.order, smoother=smoother, cycles=cycles,
+                                  vcycles=sch.vcycles, ms=ms, launches=launches))
+                if best is None or ms < best[0]:
+                    best = (ms, sch)
+                del g
         if best is None:
             raise RuntimeError(f'no smoother reaches the residual reduction {target:g} in {max_cycles} cycles')
         self.use(best[1])

@@ -35,6 +35,8 @@
 //    included, runs inside one thread block in shared memory.
 #include <algorithm>
 #include <atomic>
+#include <cstring>
+#include <vector>
 #include "mg_cluster.cuh"
 
 namespace afsi {
@@ -697,6 +699,26 @@ int32_t validate_plan(const afsi_mg_plan* plan) {
     return AFSI_OK;
 }
 
+// First level that fits the single-block path: at most kCoarseCells cells,
+// and shared memory for 3 arrays of it and of every coarser level plus the
+// per-level tables.
+template <class T>
+int coarse_start(const Lv<T>* lv, int levels) {
+    for (int l = 0; l < levels; ++l) {
+        int64_t cells = 0;
+        for (int k = l; k < levels; ++k) cells += lv[k].n;
+        if (lv[l].n <= kCoarseCells && (cells * 3 + 64 * (levels - l)) * int64_t(sizeof(T)) <= 200 * 1024) return l;
+    }
+    return levels - 1;
+}
+
+template <class T>
+size_t coarse_smem_bytes(const Lv<T>* lv, int first, int levels) {
+    int64_t cells = 0;
+    for (int k = first; k < levels; ++k) cells += lv[k].n;
+    return (size_t(cells) * 3 + 64 * size_t(levels - first)) * sizeof(T);
+}
+
 template <int BC, class T, class TC>
 int32_t run_plan(const afsi_mg_plan* plan, int cycles, cudaStream_t stream) {
     Runner<BC, T, TC> r;
@@ -705,17 +727,7 @@ int32_t run_plan(const afsi_mg_plan* plan, int cycles, cudaStream_t stream) {
     r.st = sites_for(plan);
     for (int l = 0; l < plan->levels; ++l)
         r.lv[l] = make_level<T>(plan->level[l].shape, plan->level[l].h2, plan->level[l].inv_h2, plan->dim);
-    // first level that fits the single-block path (shared memory for 3 arrays
-    // of it and every coarser level)
-    r.first_coarse = plan->levels - 1;
-    for (int l = 0; l < plan->levels; ++l) {
-        int64_t cells = 0;
-        for (int k = l; k < plan->levels; ++k) cells += r.lv[k].n;
-        if (r.lv[l].n <= kCoarseCells && (cells * 3 + 64 * (plan->levels - l)) * int64_t(sizeof(T)) <= 200 * 1024) {
-            r.first_coarse = l;
-            break;
-        }
-    }
+    r.first_coarse = coarse_start(r.lv, plan->levels);
     r.plan_cluster();
     return r.cycles(cycles);
 }
@@ -819,16 +831,7 @@ struct RbRunner {
     int32_t run(int cycles) {
         for (int l = 0; l < plan->levels; ++l)
             lv[l] = make_level<T>(plan->level[l].shape, plan->level[l].h2, plan->level[l].inv_h2, plan->dim);
-        // first level whose three arrays, with every coarser level's, fit one CTA's shared memory
-        first_coarse = plan->levels - 1;
-        for (int l = 0; l < plan->levels; ++l) {
-            int64_t cells = 0;
-            for (int k = l; k < plan->levels; ++k) cells += lv[k].n;
-            if (lv[l].n <= kCoarseCells && (cells * 3 + 64 * (plan->levels - l)) * int64_t(sizeof(T)) <= 200 * 1024) {
-                first_coarse = l;
-                break;
-            }
-        }
+        first_coarse = coarse_start(lv, plan->levels);
         for (int c = 0; c < cycles; ++c) {
             int32_t rc = level(0);
             if (!rc && singular) rc = shift_to_mean_zero(P(0), 0, st.s[0][0]);
@@ -1239,4 +1242,431 @@ extern "C" int32_t afsi_b200_mg_residual_norm_noalloc(const void* p, const void*
         });
     });
     return launched("mg_residual_norm_noalloc");
+}
+
+// ---- batched V-cycles (batching form) ----
+//
+// Many independent channel plans advanced together.  Each level operation of
+// Runner (a Jacobi sweep, the residual restriction, the prolongation) runs
+// for every instance that has a launched level at that depth in ONE launch,
+// and the single-CTA coarse levels of all instances run in one launch with a
+// CTA per instance, so a cycle costs 2*smooth+2 launches per launched depth
+// plus one, whatever the instance count.  Each instance's sequence of
+// operations and every cell's arithmetic are Runner's (the same device
+// functions, compiled with --fmad=false), so the iterates are bitwise those
+// of afsi_b200_mg_vcycles on each plan alone.  Channel (non-singular) Jacobi
+// plans only: there are no gauge sites to batch.
+//
+// A launch over a depth covers its instances' levels in 8 x 32 cell tiles
+// (y fastest); a block map gives each block its instance entry and tile.
+
+namespace afsi {
+
+constexpr int kBatchTileY = 32, kBatchTileX = kThreads / kBatchTileY;
+constexpr int kBatchEntryBits = 11;  // block map word: entry << kBatchLocalBits | tile
+constexpr int kBatchLocalBits = 32 - kBatchEntryBits;
+
+template <class T>
+struct BatchLevel {
+    Lv<T> L, C;        // the level and its coarser level
+    T *p, *q, *r;      // iterate, Jacobi partner, right-hand side
+    T* rc;             // coarser right-hand side
+    const T* down;     // where the pre-smoothing leaves the iterate (p or q)
+    const T* corr;     // the coarser level's final iterate
+};
+
+template <class T, class TC>
+struct BatchCoarse {
+    CoarseLevels<T> cl;
+    const T* rhs;      // right-hand side of level cl.first
+    const T* p_start;  // initial iterate (level 0) or null (zero start)
+    T* p_out;
+    const TC* cinv;
+};
+
+template <class T>
+struct BatchStart {
+    const T* src;  // the instance's right-hand side, or null
+    T *r, *p;      // its finest rhs (copied into) and iterate (zeroed)
+    int nx, ny;
+};
+
+// This block's entry and tile.
+__device__ __forceinline__ int batch_entry(const uint32_t* __restrict__ map, int& tile) {
+    const uint32_t w = map[blockIdx.x];
+    tile = int(w & ((1u << kBatchLocalBits) - 1));
+    return int(w >> kBatchLocalBits);
+}
+
+// This thread's cell of the tile; false outside the nx x ny level.
+__device__ __forceinline__ bool batch_xy(int tile, int nx, int ny, int& x, int& y) {
+    const int gy = (ny + kBatchTileY - 1) / kBatchTileY;
+    y = (tile % gy) * kBatchTileY + int(threadIdx.x % kBatchTileY);
+    x = (tile / gy) * kBatchTileX + int(threadIdx.x / kBatchTileY);
+    return x < nx && y < ny;
+}
+
+// One Jacobi sweep of every entry: p -> q (odd == 0) or q -> p (odd == 1);
+// zero_in: the iterate is zero (first sweep below the finest level).  The
+// arithmetic of sweep_kernel with no pending shifts.
+template <int BC, class T>
+__global__ void __launch_bounds__(kThreads) batch_sweep_kernel(const BatchLevel<T>* __restrict__ lv,
+                                                               const uint32_t* __restrict__ map, int odd,
+                                                               int zero_in) {
+    pdl_enter();
+    int tile;
+    const BatchLevel<T>& e = lv[batch_entry(map, tile)];
+    const Lv<T> L = e.L;
+    int x, y;
+    if (!batch_xy(tile, L.nx, L.ny, x, y)) return;
+    const T* p = odd ? e.q : e.p;
+    T* out = odd ? e.p : e.q;
+    const int64_t i = index_of(x, y, 0, L);
+    const T r = e.r[i];
+    T v;
+    if (!zero_in) {
+        const T pc = p[i];
+        const T a = neg_lap<BC, false>(p, i, x, y, 0, L, T(0), pc);
+        v = pc + (omega<T>() * (r - a)) / diag_at<BC>(x, y, 0, L);
+    } else {
+        v = T(0) + (omega<T>() * r) / diag_at<BC>(x, y, 0, L);
+    }
+    out[i] = v;
+}
+
+// rc = restricted residual of the pre-smoothed iterate (residual_restrict_kernel).
+template <int BC, class T>
+__global__ void __launch_bounds__(kThreads) batch_restrict_kernel(const BatchLevel<T>* __restrict__ lv,
+                                                                  const uint32_t* __restrict__ map) {
+    pdl_enter();
+    int tile;
+    const BatchLevel<T>& e = lv[batch_entry(map, tile)];
+    const Lv<T> C = e.C;
+    int cx, cy;
+    if (!batch_xy(tile, C.nx, C.ny, cx, cy)) return;
+    const Lv<T> L = e.L;
+    e.rc[index_of(cx, cy, 0, C)] = restrict_residual_at<BC, false>(e.down, e.r, cx, cy, 0, L, T(0));
+}
+
+// p = down + P(corr) (prolong_kernel; down may be p itself, own cell only).
+template <int BC, class T>
+__global__ void __launch_bounds__(kThreads) batch_prolong_kernel(const BatchLevel<T>* __restrict__ lv,
+                                                                 const uint32_t* __restrict__ map) {
+    pdl_enter();
+    int tile;
+    const BatchLevel<T>& e = lv[batch_entry(map, tile)];
+    const Lv<T> L = e.L;
+    int x, y;
+    if (!batch_xy(tile, L.nx, L.ny, x, y)) return;
+    const Lv<T> C = e.C;
+    const int64_t i = index_of(x, y, 0, L);
+    e.p[i] = e.down[i] + prolong_at<BC>(e.corr, x, y, 0, C, T(0));
+}
+
+// p = q after an odd number of post-sweeps on the finest level (the finalize copy).
+template <class T>
+__global__ void __launch_bounds__(kThreads) batch_finalize_kernel(const BatchLevel<T>* __restrict__ lv,
+                                                                  const uint32_t* __restrict__ map) {
+    pdl_enter();
+    int tile;
+    const BatchLevel<T>& e = lv[batch_entry(map, tile)];
+    int x, y;
+    if (!batch_xy(tile, e.L.nx, e.L.ny, x, y)) return;
+    const int64_t i = index_of(x, y, 0, e.L);
+    e.p[i] = e.q[i];
+}
+
+// Cycle start of every instance: finest rhs = its source (when the table has
+// one), iterate = 0.
+template <class T>
+__global__ void __launch_bounds__(kThreads) batch_start_kernel(const BatchStart<T>* __restrict__ jobs,
+                                                               const uint32_t* __restrict__ map) {
+    pdl_enter();
+    int tile;
+    const BatchStart<T>& j = jobs[batch_entry(map, tile)];
+    int x, y;
+    if (!batch_xy(tile, j.nx, j.ny, x, y)) return;
+    const int64_t i = int64_t(x) * j.ny + y;
+    if (j.src) j.r[i] = j.src[i];
+    j.p[i] = T(0);
+}
+
+// The single-CTA levels of every instance, one CTA each (coarse_cycle).
+template <int BC, class T, class TC>
+__global__ void __launch_bounds__(kCoarseThreads) batch_coarse_kernel(const BatchCoarse<T, TC>* __restrict__ jobs,
+                                                                     int smooth) {
+    pdl_enter();
+    __shared__ CoarseLevels<T> cl;
+    static_assert(sizeof(CoarseLevels<T>) % 4 == 0, "word copy");
+    const BatchCoarse<T, TC>& j = jobs[blockIdx.x];
+    const unsigned* src = reinterpret_cast<const unsigned*>(&j.cl);
+    unsigned* dst = reinterpret_cast<unsigned*>(&cl);
+    for (int k = threadIdx.x; k < int(sizeof(cl) / 4); k += blockDim.x) dst[k] = src[k];
+    const T* rhs = j.rhs;
+    const T* p_start = j.p_start;
+    T* p_out = j.p_out;
+    const TC* cinv = j.cinv;
+    __syncthreads();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    coarse_cycle<BC, T, TC>(reinterpret_cast<T*>(smem_raw), rhs, nullptr, p_start, p_out, cinv, cl, smooth);
+}
+
+}  // namespace afsi
+
+namespace {
+
+constexpr int kBatchMaxInstances = 1 << kBatchEntryBits;
+
+int64_t align16(int64_t v) { return (v + 15) & ~int64_t(15); }
+
+// Table layout derived from the plans alone (so the cycles entry recomputes it).
+struct BatchLayout {
+    int depths = 0;  // launched depths: max over instances of the coarse start
+    int64_t entries[AFSI_MG_MAX_LEVELS] = {};
+    int64_t blocks_l[AFSI_MG_MAX_LEVELS] = {}, blocks_c[AFSI_MG_MAX_LEVELS] = {};
+    int64_t level_off[AFSI_MG_MAX_LEVELS] = {}, map_l_off[AFSI_MG_MAX_LEVELS] = {},
+            map_c_off[AFSI_MG_MAX_LEVELS] = {};
+    int64_t blocks_start = 0, start_off = 0, start_map_off = 0;
+    int64_t coarse_off = 0, bytes = 0;
+    size_t coarse_smem = 0;
+};
+
+int64_t tiles_of(int nx, int ny) {
+    return int64_t((ny + kBatchTileY - 1) / kBatchTileY) * ((nx + kBatchTileX - 1) / kBatchTileX);
+}
+
+int32_t validate_batch(const afsi_mg_plan* const* plans, int32_t count) {
+    AFSI_REQUIRE(plans && count >= 1 && count <= kBatchMaxInstances, "batch needs 1..%d plans", kBatchMaxInstances);
+    const afsi_mg_plan* a = plans[0];
+    AFSI_REQUIRE(a, "null plan 0");
+    for (int i = 0; i < count; ++i) {
+        const afsi_mg_plan* p = plans[i];
+        int32_t rc = validate_plan(p);
+        if (rc) return rc;
+        AFSI_REQUIRE(p->bc == AFSI_BC_CHANNEL && p->smoother == AFSI_MG_JACOBI,
+                     "batched V-cycles take channel plans with the Jacobi smoother (plan %d)", i);
+        AFSI_REQUIRE(p->smooth == a->smooth && p->dtype == a->dtype && p->coarse_dtype == a->coarse_dtype,
+                     "plan %d differs from plan 0 in smooth count or dtypes", i);
+        AFSI_REQUIRE(p->coarse_dtype == AFSI_F64 || p->coarse_dtype == p->dtype, "unsupported coarse dtype");
+    }
+    return AFSI_OK;
+}
+
+template <class T>
+void load_levels(const afsi_mg_plan* p, Lv<T>* lv) {
+    for (int l = 0; l < p->levels; ++l)
+        lv[l] = make_level<T>(p->level[l].shape, p->level[l].h2, p->level[l].inv_h2, p->dim);
+}
+
+// Layout, and with host != null the table itself.  Entries of a depth are the
+// instances (in plan order) with a launched level there; coarse jobs are
+// ordered by decreasing shared-memory size so that the largest start first.
+template <class T, class TC>
+int32_t batch_table(const afsi_mg_plan* const* plans, int count, const void* const* sources, BatchLayout& lay,
+                    unsigned char* host) {
+    std::vector<int> start(count);
+    std::vector<size_t> smem(count);
+    lay = BatchLayout();
+    for (int i = 0; i < count; ++i) {
+        Lv<T> lv[AFSI_MG_MAX_LEVELS];
+        load_levels<T>(plans[i], lv);
+        start[i] = coarse_start(lv, plans[i]->levels);
+        smem[i] = coarse_smem_bytes(lv, start[i], plans[i]->levels);
+        lay.depths = std::max(lay.depths, start[i]);
+        lay.coarse_smem = std::max(lay.coarse_smem, smem[i]);
+        AFSI_REQUIRE(tiles_of(lv[0].nx, lv[0].ny) < (int64_t(1) << kBatchLocalBits), "plan %d: level too large", i);
+        for (int d = 0; d < start[i]; ++d) {
+            lay.entries[d] += 1;
+            lay.blocks_l[d] += tiles_of(lv[d].nx, lv[d].ny);
+            lay.blocks_c[d] += tiles_of(lv[d + 1].nx, lv[d + 1].ny);
+        }
+        lay.blocks_start += tiles_of(lv[0].nx, lv[0].ny);
+    }
+    AFSI_REQUIRE(lay.blocks_start < (int64_t(1) << 31), "batch too large for one launch");
+    int64_t off = 0;
+    for (int d = 0; d < lay.depths; ++d) {
+        lay.level_off[d] = off;
+        off = align16(off + lay.entries[d] * int64_t(sizeof(BatchLevel<T>)));
+        lay.map_l_off[d] = off;
+        off = align16(off + lay.blocks_l[d] * 4);
+        lay.map_c_off[d] = off;
+        off = align16(off + lay.blocks_c[d] * 4);
+    }
+    lay.start_off = off;
+    off = align16(off + int64_t(count) * int64_t(sizeof(BatchStart<T>)));
+    lay.start_map_off = off;
+    off = align16(off + lay.blocks_start * 4);
+    lay.coarse_off = off;
+    off = align16(off + int64_t(count) * int64_t(sizeof(BatchCoarse<T, TC>)));
+    lay.bytes = off;
+    if (!host) return AFSI_OK;
+
+    std::memset(host, 0, size_t(lay.bytes));
+    auto word = [](int entry, int64_t tile) { return (uint32_t(entry) << kBatchLocalBits) | uint32_t(tile); };
+    int64_t fill[AFSI_MG_MAX_LEVELS] = {}, bl[AFSI_MG_MAX_LEVELS] = {}, bc[AFSI_MG_MAX_LEVELS] = {};
+    int64_t bs = 0;
+    for (int i = 0; i < count; ++i) {
+        const afsi_mg_plan* pl = plans[i];
+        Lv<T> lv[AFSI_MG_MAX_LEVELS];
+        load_levels<T>(pl, lv);
+        auto P = [&](int l) { return static_cast<T*>(pl->level[l].p); };
+        auto Q = [&](int l) { return static_cast<T*>(pl->level[l].ping); };
+        auto R = [&](int l) { return static_cast<T*>(pl->level[l].rhs); };
+        // the final iterate of level l: the coarse block writes p; launched
+        // levels end on p after an even number of post-sweeps, else on q
+        auto final_of = [&](int l) { return (l >= start[i] || pl->smooth % 2 == 0) ? P(l) : Q(l); };
+        for (int d = 0; d < start[i]; ++d) {
+            const int k = int(fill[d]++);
+            BatchLevel<T> e;
+            std::memset(&e, 0, sizeof(e));
+            e.L = lv[d];
+            e.C = lv[d + 1];
+            e.p = P(d);
+            e.q = Q(d);
+            e.r = R(d);
+            e.rc = R(d + 1);
+            e.down = pl->smooth % 2 == 0 ? P(d) : Q(d);
+            e.corr = final_of(d + 1);
+            std::memcpy(host + lay.level_off[d] + int64_t(k) * int64_t(sizeof(e)), &e, sizeof(e));
+            uint32_t* ml = reinterpret_cast<uint32_t*>(host + lay.map_l_off[d]);
+            for (int64_t t = 0; t < tiles_of(lv[d].nx, lv[d].ny); ++t) ml[bl[d]++] = word(k, t);
+            uint32_t* mc = reinterpret_cast<uint32_t*>(host + lay.map_c_off[d]);
+            for (int64_t t = 0; t < tiles_of(lv[d + 1].nx, lv[d + 1].ny); ++t) mc[bc[d]++] = word(k, t);
+        }
+        BatchStart<T> s;
+        std::memset(&s, 0, sizeof(s));
+        s.src = static_cast<const T*>(sources ? sources[i] : nullptr);
+        s.r = R(0);
+        s.p = P(0);
+        s.nx = lv[0].nx;
+        s.ny = lv[0].ny;
+        std::memcpy(host + lay.start_off + int64_t(i) * int64_t(sizeof(s)), &s, sizeof(s));
+        uint32_t* ms = reinterpret_cast<uint32_t*>(host + lay.start_map_off);
+        for (int64_t t = 0; t < tiles_of(lv[0].nx, lv[0].ny); ++t) ms[bs++] = word(i, t);
+    }
+    std::vector<int> order(count);
+    for (int i = 0; i < count; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return smem[a] > smem[b]; });
+    for (int k = 0; k < count; ++k) {
+        const int i = order[k];
+        const afsi_mg_plan* pl = plans[i];
+        BatchCoarse<T, TC> j;
+        std::memset(&j, 0, sizeof(j));
+        load_levels<T>(pl, j.cl.lv);
+        j.cl.first = start[i];
+        j.cl.last = pl->levels - 1;
+        j.rhs = static_cast<const T*>(pl->level[start[i]].rhs);
+        j.p_start = start[i] == 0 ? static_cast<const T*>(pl->level[0].p) : nullptr;
+        j.p_out = static_cast<T*>(pl->level[start[i]].p);
+        j.cinv = static_cast<const TC*>(pl->coarse_inverse);
+        std::memcpy(host + lay.coarse_off + int64_t(k) * int64_t(sizeof(j)), &j, sizeof(j));
+    }
+    return AFSI_OK;
+}
+
+template <class T, class TC>
+int32_t batch_cycles(const afsi_mg_plan* const* plans, int count, const unsigned char* table, int cycles, int start,
+                     cudaStream_t stream) {
+    constexpr int BC = AFSI_BC_CHANNEL;
+    BatchLayout lay;
+    int32_t rc = batch_table<T, TC>(plans, count, nullptr, lay, nullptr);
+    if (rc) return rc;
+    static bool configured = false;  // once per instantiation, before any graph capture of it
+    if (!configured) {
+        cudaFuncSetAttribute(batch_coarse_kernel<BC, T, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             210 * 1024);
+        configured = true;
+    }
+    const int smooth = plans[0]->smooth;
+    auto lv = [&](int d) { return reinterpret_cast<const BatchLevel<T>*>(table + lay.level_off[d]); };
+    auto ml = [&](int d) { return reinterpret_cast<const uint32_t*>(table + lay.map_l_off[d]); };
+    auto mc = [&](int d) { return reinterpret_cast<const uint32_t*>(table + lay.map_c_off[d]); };
+    const dim3 block(kThreads);
+    if (start) {
+        rc = launch_pdl("mg batch start", batch_start_kernel<T>, dim3(unsigned(lay.blocks_start)), block, 0, stream,
+                        reinterpret_cast<const BatchStart<T>*>(table + lay.start_off),
+                        reinterpret_cast<const uint32_t*>(table + lay.start_map_off));
+        if (rc) return rc;
+    }
+    for (int c = 0; c < cycles; ++c) {
+        for (int d = 0; d < lay.depths; ++d) {
+            const dim3 gl(unsigned(lay.blocks_l[d])), gc(unsigned(lay.blocks_c[d]));
+            for (int s = 0; s < smooth; ++s)
+                if ((rc = launch_pdl("mg batch sweep", batch_sweep_kernel<BC, T>, gl, block, 0, stream, lv(d), ml(d),
+                                     s & 1, (s == 0 && d > 0) ? 1 : 0)))
+                    return rc;
+            if ((rc = launch_pdl("mg batch residual_restrict", batch_restrict_kernel<BC, T>, gc, block, 0, stream,
+                                 lv(d), mc(d))))
+                return rc;
+        }
+        if ((rc = launch_pdl("mg batch coarse blocks", batch_coarse_kernel<BC, T, TC>, dim3(unsigned(count)),
+                             dim3(kCoarseThreads), lay.coarse_smem, stream,
+                             reinterpret_cast<const BatchCoarse<T, TC>*>(table + lay.coarse_off), smooth)))
+            return rc;
+        for (int d = lay.depths - 1; d >= 0; --d) {
+            const dim3 gl(unsigned(lay.blocks_l[d]));
+            if ((rc = launch_pdl("mg batch prolong_add", batch_prolong_kernel<BC, T>, gl, block, 0, stream, lv(d),
+                                 ml(d))))
+                return rc;
+            for (int s = 0; s < smooth; ++s)
+                if ((rc = launch_pdl("mg batch sweep", batch_sweep_kernel<BC, T>, gl, block, 0, stream, lv(d), ml(d),
+                                     s & 1, 0)))
+                    return rc;
+        }
+        if (lay.depths > 0 && smooth % 2 == 1 &&
+            (rc = launch_pdl("mg batch finalize", batch_finalize_kernel<T>, dim3(unsigned(lay.blocks_l[0])), block, 0,
+                             stream, lv(0), ml(0))))
+            return rc;
+    }
+    return AFSI_OK;
+}
+
+#define AFSI_BATCH_DISPATCH(plans, ...)      \
+    AFSI_DISPATCH((plans)[0]->dtype, {        \
+        if ((plans)[0]->coarse_dtype == AFSI_F64) { \
+            using TC = double;                \
+            __VA_ARGS__;                      \
+        } else {                              \
+            using TC = T;                     \
+            __VA_ARGS__;                      \
+        }                                     \
+    })
+
+}  // namespace
+
+extern "C" int64_t afsi_b200_mg_batch_table_bytes(const afsi_mg_plan* const* plans, int32_t count) {
+    if (validate_batch(plans, count)) return -1;
+    BatchLayout lay;
+    int32_t rc = AFSI_OK;
+    AFSI_BATCH_DISPATCH(plans, rc = batch_table<T, TC>(plans, count, nullptr, lay, nullptr));
+    return rc ? -1 : lay.bytes;
+}
+
+extern "C" int32_t afsi_b200_mg_batch_table(const afsi_mg_plan* const* plans, int32_t count,
+                                            const void* const* rhs_sources, void* host_table, int64_t bytes) {
+    int32_t rc = validate_batch(plans, count);
+    if (rc) return rc;
+    AFSI_REQUIRE(host_table, "null table");
+    if (rhs_sources)
+        for (int i = 0; i < count; ++i) AFSI_REQUIRE(rhs_sources[i], "null rhs source %d", i);
+    BatchLayout lay;
+    AFSI_BATCH_DISPATCH(plans, {
+        if ((rc = batch_table<T, TC>(plans, count, nullptr, lay, nullptr))) return rc;
+        AFSI_REQUIRE(bytes >= lay.bytes, "table needs %lld bytes", (long long)lay.bytes);
+        return batch_table<T, TC>(plans, count, rhs_sources, lay, static_cast<unsigned char*>(host_table));
+    });
+    return AFSI_OK;
+}
+
+extern "C" int32_t afsi_b200_mg_batch_vcycles(const afsi_mg_plan* const* plans, int32_t count, const void* table,
+                                              int32_t cycles, int32_t start, afsi_stream_t stream) {
+    int32_t rc = validate_batch(plans, count);
+    if (rc) return rc;
+    AFSI_REQUIRE(table && reinterpret_cast<uintptr_t>(table) % 16 == 0, "device table must be 16-byte aligned");
+    AFSI_REQUIRE(cycles >= 0, "negative cycle count");
+    AFSI_BATCH_DISPATCH(plans, {
+        return batch_cycles<T, TC>(plans, count, static_cast<const unsigned char*>(table), cycles, start ? 1 : 0,
+                                   static_cast<cudaStream_t>(stream));
+    });
+    return AFSI_OK;
 }

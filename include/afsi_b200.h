@@ -391,6 +391,28 @@ int32_t afsi_b200_mg_residual_norm(const afsi_mg_plan* plan, double* norm_out, a
 int32_t afsi_b200_mg_residual_norm_noalloc(const void* p, const void* rhs, const int64_t* shape,
     const double* h2, int32_t dim, int32_t bc, double* norm_out, int32_t dtype, afsi_stream_t stream);
 
+/* Batched V-cycles (the batching form; no counterpart in the reference, which
+ * steps one ChannelMultigrid per instance, mac2d/multigrid.py:16-134): `count`
+ * (1..2048) independent channel plans with the Jacobi smoother and the same
+ * smooth count, dtype and coarse dtype advance together, each level operation
+ * of all instances in one launch and the single-CTA coarse levels in one
+ * launch with a CTA per instance.  Every plan's iterates are bitwise those of
+ * afsi_b200_mg_vcycles on that plan alone.
+ * afsi_b200_mg_batch_table_bytes: size of the batch table (-1: invalid plans).
+ * afsi_b200_mg_batch_table: fills the table in HOST memory from the plans and,
+ *   optionally (else NULL), one right-hand-side source per plan (a device array
+ *   of the plan's finest shape and dtype); the caller copies it to a 16-byte
+ *   aligned device buffer once.  The table holds the plans' buffer addresses.
+ * afsi_b200_mg_batch_vcycles: `cycles` V-cycles of every plan; with start != 0
+ *   first zeroes each plan's finest iterate and copies its source, if the
+ *   table has sources, into its finest rhs.  `table` is the device copy, made
+ *   from the same plans. */
+int64_t afsi_b200_mg_batch_table_bytes(const afsi_mg_plan* const* plans, int32_t count);
+int32_t afsi_b200_mg_batch_table(const afsi_mg_plan* const* plans, int32_t count,
+    const void* const* rhs_sources, void* host_table, int64_t bytes);
+int32_t afsi_b200_mg_batch_vcycles(const afsi_mg_plan* const* plans, int32_t count, const void* table,
+    int32_t cycles, int32_t start, afsi_stream_t stream);
+
 /* Iterative refinement of an FP64 pressure solve by FP32 V-cycles (the
  * precision form; no counterpart in the reference, whose solver is FP64
  * throughout, mac/multigrid.py:125-172).

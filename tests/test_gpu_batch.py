@@ -4,7 +4,8 @@ Per instance the batch must reproduce the single-instance operators: stencil
 ids and FP64 weights bit-exact against the oracle (``mac2d/transfer.py:61-81``),
 FP32 weights equal to the FP64 weights rounded once; spreads and gathers
 1e-12 of the field scale in FP64 (the single-instance bar) and 2e-6 in FP32
-against the FP64 oracle; each instance's V-cycles bitwise equal to its own
+against the FP64 oracle; each instance's V-cycles, per instance over streams or batched
+(one launch per level operation for all instances), bitwise equal to its own
 solver run alone; graph replay equal to the eager step.
 """
 import numpy as np
@@ -17,10 +18,11 @@ pytestmark = pytest.mark.gpu
 DEV = 'cuda'
 
 
-def _small(dtype, count=6, seed=4):
-    return seeded_batch(count, seed=seed, shapes=((128, 32), (256, 64), (384, 96)), points=(2000, 6000),
-                        device=DEV, transfer_dtype=dtype,
-                        schedule=Schedule(streams=3, order='largest-first', smoother='jacobi', cycles=3))
+def _small(dtype, count=6, seed=4, vcycles='streams'):
+    return seeded_batch(count, seed=seed, shapes=((128, 32), (256, 64), (384, 96), (512, 128), (32, 8)),
+                        points=(2000, 6000), device=DEV, transfer_dtype=dtype,
+                        schedule=Schedule(streams=3, order='largest-first', smoother='jacobi', cycles=3,
+                                          vcycles=vcycles))
 
 
 @pytest.mark.parametrize('dtype', [torch.float64, torch.float32])
@@ -51,8 +53,9 @@ def test_batched_transfers_match_oracle_per_instance(dtype):
                                        atol=tol * np.abs(ref).max())
 
 
-def test_batched_cycles_equal_each_instance_alone_and_graph_replay_equals_eager():
-    b = _small(torch.float32)
+@pytest.mark.parametrize('vcycles', ['streams', 'batched'])
+def test_batched_cycles_equal_each_instance_alone_and_graph_replay_equals_eager(vcycles):
+    b = _small(torch.float32, count=9, vcycles=vcycles)
     sch = b.schedule
     b.run(sch)
     torch.cuda.synchronize()
@@ -86,6 +89,7 @@ def test_autotuner_picks_a_measured_schedule_meeting_the_target():
     assert (best['streams'], best['order'], best['smoother'], best['cycles']) == \
         (schedule.streams, schedule.order, schedule.smoother, schedule.cycles)
     assert {r['smoother'] for r in table} == {'jacobi', 'red-black'}
+    assert {r['vcycles'] for r in table} == {'streams', 'batched'}
     b.replay()
     torch.cuda.synchronize()
     assert max(b.residual_reduction()) <= 1e-3
@@ -97,3 +101,32 @@ def test_batch_rejects_points_outside_their_channel():
     b.run()
     with pytest.raises(ValueError, match='support'):
         b.check()
+
+
+@pytest.mark.parametrize('smooth', [3, 4])
+def test_batched_vcycles_match_each_solver_alone(smooth):
+    """Uneven grids (some wholly in one CTA, some with two launched levels),
+    an odd and an even sweep count; a started run then a continued one."""
+    from afsi_gpu_b200.batch import BatchedVCycles
+    from afsi_gpu_b200.grid import ChannelGrid
+    from afsi_gpu_b200.multigrid import ChannelMultigrid, MGOptions
+    shapes = [(512, 128), (64, 16), (256, 64), (32, 8), (384, 96)]
+    rng = np.random.default_rng(11)
+    grids = [ChannelGrid(s, (4., 1.)) for s in shapes]
+
+    def solver(g):
+        return ChannelMultigrid(g, device=DEV, dtype=torch.float32, coarse_dtype=torch.float64, backend='b200',
+                                options=MGOptions(smooth=smooth))
+    rhs = [torch.as_tensor(rng.standard_normal(s), dtype=torch.float32, device=DEV) for s in shapes]
+    batch = [solver(g) for g in grids]
+    for mg in batch:
+        mg.workspace.p[0].fill_(7.)   # the start must zero it
+    bv = BatchedVCycles(batch, rhs)
+    bv.run(2)
+    bv.run(1, start=False)
+    torch.cuda.synchronize()
+    for g, r, mg in zip(grids, rhs, batch):
+        alone = solver(g)
+        alone.initialize(torch.zeros_like(r), r)
+        p = alone.advance(3)
+        assert torch.equal(p, mg.workspace.p[0])
