@@ -13,6 +13,7 @@
 // (spread divided by the cell area, gather): positions, bases and weights are
 // formed in FP64 and the weights stored in the transfer type TW (float in
 // the precision form), so ids equal the single-instance FP64 ids exactly.
+#include <algorithm>
 #include "common.cuh"
 #include "peskin.cuh"
 
@@ -44,111 +45,199 @@ __device__ __forceinline__ void stage_firsts(const BatchTable& t, int64_t* s_fir
     __syncthreads();
 }
 
+constexpr int kPrepThreads = 256;
+constexpr int kStageRow = 17;  // int64 words per staged point row (16 taps + 1 pad against bank conflicts)
+
+// One thread per point.  A warp's 32 points own 32 consecutive rows of 16 ids
+// (and 16 weights) per component, so each warp stages its rows in shared
+// memory and writes them out as one contiguous run (coalesced stores).
 template <class TW>
-__global__ void __launch_bounds__(256) batch_prepare2d_kernel(const double* __restrict__ points, int64_t total,
-                                                              BatchTable t, int64_t* __restrict__ ids,
-                                                              TW* __restrict__ weights, int32_t* status) {
+__global__ void __launch_bounds__(kPrepThreads) batch_prepare2d_kernel(const double* __restrict__ points,
+                                                                       int64_t total, BatchTable t,
+                                                                       int64_t* __restrict__ ids,
+                                                                       TW* __restrict__ weights, int32_t* status) {
     __shared__ int64_t s_first[kMaxBatch];
+    __shared__ int64_t s_rows[kPrepThreads / 32][32 * kStageRow];
     stage_firsts(t, s_first);
-    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (p >= total) return;
-    const afsi_batch2d_instance I = t.inst[owner(s_first, t.count, p)];
-    const double px = points[p * 2], py = points[p * 2 + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t p0 = int64_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31);
+    if (p0 >= total) return;  // whole warp
+    const int n_valid = total - p0 < 32 ? int(total - p0) : 32;
+    const int64_t p = p0 + lane;
+    const bool live = lane < n_valid;
+    int64_t* row = s_rows[warp] + lane * kStageRow;
+    TW* wrow = reinterpret_cast<TW*>(s_rows[warp]) + lane * kStageRow;
+    afsi_batch2d_instance I{};
+    double px = 0.0, py = 0.0;
+    if (live) {
+        I = t.inst[owner(s_first, t.count, p)];
+        px = points[p * 2];
+        py = points[p * 2 + 1];
+        const bool valid = p < I.point_offset + I.point_count && isfinite(px) && isfinite(py) &&
+                           px >= 2 * I.hx && px <= I.lx - 2 * I.hx && py >= -I.hy && py <= I.ly + I.hy;
+        if (!valid) flag(status, AFSI_FLAG_SUPPORT);
+    }
     const double hx = I.hx, hy = I.hy;
-    const bool valid = p < I.point_offset + I.point_count && isfinite(px) && isfinite(py) && px >= 2 * hx &&
-                       px <= I.lx - 2 * hx && py >= -hy && py <= I.ly + hy;
-    if (!valid) flag(status, AFSI_FLAG_SUPPORT);
     const int64_t ny = I.ny;
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
-        const double ox = hx * (c == 0 ? 0.0 : .5);
-        const double oy = hy * (c == 1 ? 0.0 : .5);
-        const double sx = (px - ox) / hx, sy = (py - oy) / hy;
-        const int64_t bx = static_cast<int64_t>(floor(sx - 1.0));
-        const int64_t by = static_cast<int64_t>(floor(sy - 1.0));
-        const int64_t face_ny = ny + (c == 1);
-        const int64_t face_base = c == 0 ? I.u_offset : I.v_offset;
         double wx[4], wy[4];
+        int64_t bx = 0, by = 0;
+        if (live) {
+            const double ox = hx * (c == 0 ? 0.0 : .5);
+            const double oy = hy * (c == 1 ? 0.0 : .5);
+            const double sx = (px - ox) / hx, sy = (py - oy) / hy;
+            bx = static_cast<int64_t>(floor(sx - 1.0));
+            by = static_cast<int64_t>(floor(sy - 1.0));
+            const int64_t face_ny = ny + (c == 1);
+            const int64_t face_base = c == 0 ? I.u_offset : I.v_offset;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            wx[k] = peskin_clamped(sx - double(bx + k));
-            wy[k] = peskin_clamped(sy - double(by + k));
-        }
-        int64_t* out_ids = ids + (c * total + p) * 16;
-        TW* out_w = weights + (c * total + p) * 16;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int64_t y = by + j;
-                bool outside;
-                int64_t r;
-                if (c == 0) {
-                    outside = y < 0 || y >= ny;
-                    r = y < 0 ? -y - 1 : (y >= ny ? 2 * ny - y - 1 : y);
-                } else {
-                    outside = y < 0 || y > ny;
-                    r = y < 0 ? -y : (y > ny ? 2 * ny - y : y);
-                }
-                const double w = wx[i] * wy[j];
-                out_ids[i * 4 + j] = face_base + (bx + i) * face_ny + r;
-                out_w[i * 4 + j] = TW(outside ? -w : w);
+            for (int k = 0; k < 4; ++k) {
+                wx[k] = peskin_clamped(sx - double(bx + k));
+                wy[k] = peskin_clamped(sy - double(by + k));
             }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int64_t y = by + j;
+                    const int64_t r = c == 0 ? (y < 0 ? -y - 1 : (y >= ny ? 2 * ny - y - 1 : y))
+                                             : (y < 0 ? -y : (y > ny ? 2 * ny - y : y));
+                    row[i * 4 + j] = face_base + (bx + i) * face_ny + r;
+                }
         }
+        __syncwarp();
+        const int64_t out0 = (c * total + p0) * 16;
+        for (int k = lane; k < 16 * n_valid; k += 32) ids[out0 + k] = s_rows[warp][(k >> 4) * kStageRow + (k & 15)];
+        __syncwarp();
+        if (live) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int64_t y = by + j;
+                    const bool outside = c == 0 ? (y < 0 || y >= ny) : (y < 0 || y > ny);
+                    const double w = wx[i] * wy[j];
+                    wrow[i * 4 + j] = TW(outside ? -w : w);
+                }
+        }
+        __syncwarp();
+        const TW* sw = reinterpret_cast<const TW*>(s_rows[warp]);
+        for (int k = lane; k < 16 * n_valid; k += 32) weights[out0 + k] = sw[(k >> 4) * kStageRow + (k & 15)];
+        __syncwarp();
     }
 }
 
-// 16 lanes per (point, component): u_c[id] += F_c * w / (hx hy) of the point's instance.
+// Transfers: 16 lanes per (point, component) task, each lane one stencil
+// tap.  A 16-lane group takes kTaskUnroll consecutive tasks per iteration of
+// a grid-stride loop and issues all their loads before it uses them, so a
+// thread keeps several loads in flight; the grid is capped at a few blocks
+// per SM.
+constexpr int kTaskUnroll = 4;
+constexpr int kTransferThreads = 256;
+
+// u_c[id] += F_c * w / (hx hy) of the point's instance.
 template <class T>
-__global__ void __launch_bounds__(256) batch_spread2d_kernel(const T* __restrict__ force, const int64_t* __restrict__ ids,
-                                                             const T* __restrict__ w, int64_t total, BatchTable t,
-                                                             T* __restrict__ u, T* __restrict__ v, int64_t nu,
-                                                             int64_t nv, int32_t* status) {
+__global__ void __launch_bounds__(kTransferThreads) batch_spread2d_kernel(const T* __restrict__ force,
+                                                                          const int64_t* __restrict__ ids,
+                                                                          const T* __restrict__ w, int64_t total,
+                                                                          BatchTable t, T* __restrict__ u,
+                                                                          T* __restrict__ v, int64_t nu, int64_t nv,
+                                                                          int32_t* status) {
     __shared__ int64_t s_first[kMaxBatch];
     stage_firsts(t, s_first);
-    const int64_t task = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 16;
     const int sub = threadIdx.x % 16;
-    if (task >= total * 2) return;
-    const int64_t p = task >> 1;
-    const int c = int(task & 1);
-    const afsi_batch2d_instance& I = t.inst[owner(s_first, t.count, p)];
-    const T volume = T(I.hx * I.hy);
-    const int64_t j = ids[(c * total + p) * 16 + sub];
-    T* out = c == 0 ? u : v;
-    const int64_t lo = c == 0 ? I.u_offset : I.v_offset;
-    const int64_t hi = lo + (c == 0 ? (I.nx + 1) * I.ny : I.nx * (I.ny + 1));
-    if (j < lo || j >= hi || j >= (c == 0 ? nu : nv)) {
-        flag(status, AFSI_FLAG_INDEX);
-        return;
+    const int64_t tasks = total * 2;
+    const int64_t groups = (int64_t(gridDim.x) * blockDim.x) / 16;
+    for (int64_t g = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 16; g * kTaskUnroll < tasks; g += groups) {
+        int64_t j[kTaskUnroll];
+        T fw[kTaskUnroll];
+#pragma unroll
+        for (int k = 0; k < kTaskUnroll; ++k) {
+            const int64_t task = g * kTaskUnroll + k;
+            if (task < tasks) {
+                const int64_t p = task >> 1;
+                const int c = int(task & 1);
+                const int64_t row = (c * total + p) * 16 + sub;
+                j[k] = ids[row];
+                fw[k] = force[p * 2 + c] * w[row];
+            }
+        }
+        int64_t owner_p = -1;
+        int inst = 0;
+#pragma unroll
+        for (int k = 0; k < kTaskUnroll; ++k) {
+            const int64_t task = g * kTaskUnroll + k;
+            if (task >= tasks) break;
+            const int64_t p = task >> 1;
+            const int c = int(task & 1);
+            if (p != owner_p) {  // both components of a point share the lookup
+                inst = owner(s_first, t.count, p);
+                owner_p = p;
+            }
+            const afsi_batch2d_instance& I = t.inst[inst];
+            const T volume = T(I.hx * I.hy);
+            const int64_t lo = c == 0 ? I.u_offset : I.v_offset;
+            const int64_t hi = lo + (c == 0 ? (I.nx + 1) * I.ny : I.nx * (I.ny + 1));
+            if (j[k] < lo || j[k] >= hi || j[k] >= (c == 0 ? nu : nv)) {
+                flag(status, AFSI_FLAG_INDEX);
+                continue;
+            }
+            atomicAdd((c == 0 ? u : v) + j[k], fw[k] / volume);
+        }
     }
-    atomicAdd(out + j, (force[p * 2 + c] * w[(c * total + p) * 16 + sub]) / volume);
 }
 
-// 16 lanes per (point, component): U_c[p] = sum of u_c[id] * w (ids are
-// batch-global, so no instance lookup); xor-free shuffle tree as in the
-// single-instance gather.
+// U_c[p] = sum of u_c[id] * w (ids are batch-global, so no instance lookup);
+// the 16 taps summed by the shuffle tree of the single-instance gather.
 template <class T>
-__global__ void __launch_bounds__(256) batch_gather2d_kernel(const T* __restrict__ u, const T* __restrict__ v,
-                                                             const int64_t* __restrict__ ids, const T* __restrict__ w,
-                                                             int64_t total, int64_t nu, int64_t nv,
-                                                             T* __restrict__ out, int32_t* status) {
-    const int64_t task = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 16;
+__global__ void __launch_bounds__(kTransferThreads) batch_gather2d_kernel(const T* __restrict__ u,
+                                                                          const T* __restrict__ v,
+                                                                          const int64_t* __restrict__ ids,
+                                                                          const T* __restrict__ w, int64_t total,
+                                                                          int64_t nu, int64_t nv,
+                                                                          T* __restrict__ out, int32_t* status) {
     const int sub = threadIdx.x % 16;
-    const bool active = task < total * 2;
-    const int64_t p = active ? task >> 1 : 0;
-    const int c = int(task & 1);
-    T sum = T(0);
-    if (active) {
-        const int64_t j = ids[(c * total + p) * 16 + sub];
-        const int64_t n = c == 0 ? nu : nv;
-        if (j < 0 || j >= n)
-            flag(status, AFSI_FLAG_INDEX);
-        else
-            sum = (c == 0 ? u : v)[j] * w[(c * total + p) * 16 + sub];
-    }
+    const int64_t tasks = total * 2;
+    const int64_t groups = (int64_t(gridDim.x) * blockDim.x) / 16;
+    // uniform trip count per warp (both half-warps run every shuffle)
+    const int64_t first = (int64_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31)) / 16;
+    for (int64_t g0 = first; g0 * kTaskUnroll < tasks; g0 += groups) {
+        const int64_t g = g0 + (threadIdx.x & 16 ? 1 : 0);
+        int64_t j[kTaskUnroll];
+        T wt[kTaskUnroll];
 #pragma unroll
-    for (int d = 8; d; d >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, d, 16);
-    if (active && sub == 0) out[p * 2 + c] = sum;
+        for (int k = 0; k < kTaskUnroll; ++k) {
+            const int64_t task = g * kTaskUnroll + k;
+            j[k] = -1;
+            wt[k] = T(0);
+            if (task < tasks) {
+                const int64_t row = ((task & 1) * total + (task >> 1)) * 16 + sub;
+                j[k] = ids[row];
+                wt[k] = w[row];
+            }
+        }
+        T sum[kTaskUnroll];
+#pragma unroll
+        for (int k = 0; k < kTaskUnroll; ++k) {
+            const int64_t task = g * kTaskUnroll + k;
+            sum[k] = T(0);
+            if (task < tasks) {
+                const int c = int(task & 1);
+                if (j[k] < 0 || j[k] >= (c == 0 ? nu : nv))
+                    flag(status, AFSI_FLAG_INDEX);
+                else
+                    sum[k] = (c == 0 ? u : v)[j[k]] * wt[k];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kTaskUnroll; ++k) {
+#pragma unroll
+            for (int d = 8; d; d >>= 1) sum[k] += __shfl_down_sync(0xffffffffu, sum[k], d, 16);
+            const int64_t task = g * kTaskUnroll + k;
+            if (task < tasks && sub == 0) out[(task >> 1) * 2 + (task & 1)] = sum[k];
+        }
+    }
 }
 
 }  // namespace afsi
@@ -156,6 +245,21 @@ __global__ void __launch_bounds__(256) batch_gather2d_kernel(const T* __restrict
 using namespace afsi;
 
 namespace {
+
+// Blocks for a transfer over `total` points: one 16-lane group per
+// kTaskUnroll tasks, at most 8 blocks per SM (grid-stride beyond).
+unsigned transfer_blocks(int64_t total) {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    const int64_t groups = (total * 2 + kTaskUnroll - 1) / kTaskUnroll;
+    const int64_t blocks = (groups * 16 + kTransferThreads - 1) / kTransferThreads;
+    return unsigned(std::max<int64_t>(1, std::min<int64_t>(blocks, int64_t(sms) * 8)));
+}
 
 int32_t check_table(const afsi_batch2d_instance* inst, int32_t count) {
     AFSI_REQUIRE(inst && count >= 1 && count <= kMaxBatch, "batch needs 1..%d instances and a device table",
@@ -176,7 +280,7 @@ extern "C" int32_t afsi_b200_batch2d_prepare(const double* points, int64_t total
     AFSI_REQUIRE(points && ids && weights, "null device pointer");
     const BatchTable t{instances, count};
     AFSI_DISPATCH(weight_dtype, {
-        batch_prepare2d_kernel<T><<<blocks_for(total, 256), 256, 0, stream>>>(points, total, t, ids,
+        batch_prepare2d_kernel<T><<<blocks_for(total, kPrepThreads), kPrepThreads, 0, stream>>>(points, total, t, ids,
                                                                               static_cast<T*>(weights), status);
     });
     return launched("batch2d prepare");
@@ -193,7 +297,7 @@ extern "C" int32_t afsi_b200_batch2d_spread(const void* force, const int64_t* id
     AFSI_REQUIRE(force && ids && weights && u && v, "null device pointer");
     const BatchTable t{instances, count};
     AFSI_DISPATCH(dtype, {
-        batch_spread2d_kernel<T><<<blocks_for(total * 2 * 16, 256), 256, 0, stream>>>(
+        batch_spread2d_kernel<T><<<transfer_blocks(total), kTransferThreads, 0, stream>>>(
             static_cast<const T*>(force), ids, static_cast<const T*>(weights), total, t, static_cast<T*>(u),
             static_cast<T*>(v), nu, nv, status);
     });
@@ -207,7 +311,7 @@ extern "C" int32_t afsi_b200_batch2d_gather(const void* u, const void* v, int64_
     if (total == 0) return AFSI_OK;
     AFSI_REQUIRE(u && v && ids && weights && out, "null device pointer");
     AFSI_DISPATCH(dtype, {
-        batch_gather2d_kernel<T><<<blocks_for(total * 2 * 16, 256), 256, 0, stream>>>(
+        batch_gather2d_kernel<T><<<transfer_blocks(total), kTransferThreads, 0, stream>>>(
             static_cast<const T*>(u), static_cast<const T*>(v), ids, static_cast<const T*>(weights), total, nu, nv,
             static_cast<T*>(out), status);
     });
