@@ -348,9 +348,10 @@ Geometry launch_for(const Lv<T>& L, int bc) {
     Geometry g;
     g.block = dim3(bx, by, 1);
     const int gx = (fast + bx - 1) / bx, gy = (mid + by - 1) / by;
-    // cap the blocks (x slabs are strided inside the kernel) so that the
-    // completion counter of a reducing launch sees at most ~600 arrivals
-    const int cap = std::max(1, 592 / std::max(1, gx * gy));
+    // cap the blocks at 16 per SM of a B200 (x slabs beyond are strided inside
+    // the kernel), which bounds the arrivals at a reducing launch's completion
+    // counter; up to 64^3 every thread owns one cell
+    const int cap = std::max(1, 2368 / std::max(1, gx * gy));
     g.grid = dim3(gx, gy, std::min(slow, cap));
     g.blocks = int64_t(g.grid.x) * g.grid.y * g.grid.z;
     return g;
