@@ -1258,12 +1258,15 @@ extern "C" int32_t afsi_b200_mg_residual_norm_noalloc(const void* p, const void*
 // of afsi_b200_mg_vcycles on each plan alone.  Channel (non-singular) Jacobi
 // plans only: there are no gauge sites to batch.
 //
-// A launch over a depth covers its instances' levels in 8 x 32 cell tiles
-// (y fastest); a block map gives each block its instance entry and tile.
+// A launch over a depth covers its instances' levels in 32 x 32 cell tiles
+// (y fastest, four cells per thread); a block map gives each block its
+// instance entry and tile.
 
 namespace afsi {
 
-constexpr int kBatchTileY = 32, kBatchTileX = kThreads / kBatchTileY;
+constexpr int kBatchTileY = 32, kBatchTileX = 32;                // cells per tile (y fastest)
+constexpr int kBatchRowStep = kThreads / kBatchTileY;             // x rows apart of a thread's cells
+constexpr int kBatchRows = kBatchTileX / kBatchRowStep;           // cells per thread
 constexpr int kBatchEntryBits = 11;  // block map word: entry << kBatchLocalBits | tile
 constexpr int kBatchLocalBits = 32 - kBatchEntryBits;
 
@@ -1299,13 +1302,17 @@ __device__ __forceinline__ int batch_entry(const uint32_t* __restrict__ map, int
     return int(w >> kBatchLocalBits);
 }
 
-// This thread's cell of the tile; false outside the nx x ny level.
-__device__ __forceinline__ bool batch_xy(int tile, int nx, int ny, int& x, int& y) {
+// This thread's column y and first row x0 in the tile; its cells are
+// (x0 + m * kBatchRowStep, y), m < kBatchRows.
+__device__ __forceinline__ void batch_tile(int tile, int ny, int& x0, int& y) {
     const int gy = (ny + kBatchTileY - 1) / kBatchTileY;
     y = (tile % gy) * kBatchTileY + int(threadIdx.x % kBatchTileY);
-    x = (tile / gy) * kBatchTileX + int(threadIdx.x / kBatchTileY);
-    return x < nx && y < ny;
+    x0 = (tile / gy) * kBatchTileX + int(threadIdx.x / kBatchTileY);
 }
+
+// The kernels below compute all of a thread's cells before storing any, so
+// the loads of the cells are in flight together (the outputs never alias
+// another cell's inputs).
 
 // One Jacobi sweep of every entry: p -> q (odd == 0) or q -> p (odd == 1);
 // zero_in: the iterate is zero (first sweep below the finest level).  The
@@ -1318,21 +1325,33 @@ __global__ void __launch_bounds__(kThreads) batch_sweep_kernel(const BatchLevel<
     int tile;
     const BatchLevel<T>& e = lv[batch_entry(map, tile)];
     const Lv<T> L = e.L;
-    int x, y;
-    if (!batch_xy(tile, L.nx, L.ny, x, y)) return;
+    int x0, y;
+    batch_tile(tile, L.ny, x0, y);
+    if (y >= L.ny) return;
     const T* p = odd ? e.q : e.p;
     T* out = odd ? e.p : e.q;
-    const int64_t i = index_of(x, y, 0, L);
-    const T r = e.r[i];
-    T v;
-    if (!zero_in) {
-        const T pc = p[i];
-        const T a = neg_lap<BC, false>(p, i, x, y, 0, L, T(0), pc);
-        v = pc + (omega<T>() * (r - a)) / diag_at<BC>(x, y, 0, L);
-    } else {
-        v = T(0) + (omega<T>() * r) / diag_at<BC>(x, y, 0, L);
+    const T* rhs = e.r;
+    T v[kBatchRows];
+#pragma unroll
+    for (int m = 0; m < kBatchRows; ++m) {
+        const int x = x0 + m * kBatchRowStep;
+        if (x >= L.nx) break;
+        const int64_t i = index_of(x, y, 0, L);
+        const T r = rhs[i];
+        if (!zero_in) {
+            const T pc = p[i];
+            const T a = neg_lap<BC, false>(p, i, x, y, 0, L, T(0), pc);
+            v[m] = pc + (omega<T>() * (r - a)) / diag_at<BC>(x, y, 0, L);
+        } else {
+            v[m] = T(0) + (omega<T>() * r) / diag_at<BC>(x, y, 0, L);
+        }
     }
-    out[i] = v;
+#pragma unroll
+    for (int m = 0; m < kBatchRows; ++m) {
+        const int x = x0 + m * kBatchRowStep;
+        if (x >= L.nx) break;
+        out[index_of(x, y, 0, L)] = v[m];
+    }
 }
 
 // rc = restricted residual of the pre-smoothed iterate (residual_restrict_kernel).
@@ -1343,10 +1362,23 @@ __global__ void __launch_bounds__(kThreads) batch_restrict_kernel(const BatchLev
     int tile;
     const BatchLevel<T>& e = lv[batch_entry(map, tile)];
     const Lv<T> C = e.C;
-    int cx, cy;
-    if (!batch_xy(tile, C.nx, C.ny, cx, cy)) return;
+    int cx0, cy;
+    batch_tile(tile, C.ny, cx0, cy);
+    if (cy >= C.ny) return;
     const Lv<T> L = e.L;
-    e.rc[index_of(cx, cy, 0, C)] = restrict_residual_at<BC, false>(e.down, e.r, cx, cy, 0, L, T(0));
+    T v[kBatchRows];
+#pragma unroll
+    for (int m = 0; m < kBatchRows; ++m) {
+        const int cx = cx0 + m * kBatchRowStep;
+        if (cx >= C.nx) break;
+        v[m] = restrict_residual_at<BC, false>(e.down, e.r, cx, cy, 0, L, T(0));
+    }
+#pragma unroll
+    for (int m = 0; m < kBatchRows; ++m) {
+        const int cx = cx0 + m * kBatchRowStep;
+        if (cx >= C.nx) break;
+        e.rc[index_of(cx, cy, 0, C)] = v[m];
+    }
 }
 
 // p = down + P(corr) (prolong_kernel; down may be p itself, own cell only).
@@ -1357,11 +1389,23 @@ __global__ void __launch_bounds__(kThreads) batch_prolong_kernel(const BatchLeve
     int tile;
     const BatchLevel<T>& e = lv[batch_entry(map, tile)];
     const Lv<T> L = e.L;
-    int x, y;
-    if (!batch_xy(tile, L.nx, L.ny, x, y)) return;
+    int x0, y;
+    batch_tile(tile, L.ny, x0, y);
+    if (y >= L.ny) return;
     const Lv<T> C = e.C;
-    const int64_t i = index_of(x, y, 0, L);
-    e.p[i] = e.down[i] + prolong_at<BC>(e.corr, x, y, 0, C, T(0));
+    T v[kBatchRows];
+#pragma unroll
+    for (int m = 0; m < kBatchRows; ++m) {
+        const int x = x0 + m * kBatchRowStep;
+        if (x >= L.nx) break;
+        v[m] = e.down[index_of(x, y, 0, L)] + prolong_at<BC>(e.corr, x, y, 0, C, T(0));
+    }
+#pragma unroll
+    for (int m = 0; m < kBatchRows; ++m) {
+        const int x = x0 + m * kBatchRowStep;
+        if (x >= L.nx) break;
+        e.p[index_of(x, y, 0, L)] = v[m];
+    }
 }
 
 // p = q after an odd number of post-sweeps on the finest level (the finalize copy).
@@ -1371,10 +1415,16 @@ __global__ void __launch_bounds__(kThreads) batch_finalize_kernel(const BatchLev
     pdl_enter();
     int tile;
     const BatchLevel<T>& e = lv[batch_entry(map, tile)];
-    int x, y;
-    if (!batch_xy(tile, e.L.nx, e.L.ny, x, y)) return;
-    const int64_t i = index_of(x, y, 0, e.L);
-    e.p[i] = e.q[i];
+    int x0, y;
+    batch_tile(tile, e.L.ny, x0, y);
+    if (y >= e.L.ny) return;
+#pragma unroll
+    for (int m = 0; m < kBatchRows; ++m) {
+        const int x = x0 + m * kBatchRowStep;
+        if (x >= e.L.nx) break;
+        const int64_t i = index_of(x, y, 0, e.L);
+        e.p[i] = e.q[i];
+    }
 }
 
 // Cycle start of every instance: finest rhs = its source (when the table has
@@ -1385,11 +1435,17 @@ __global__ void __launch_bounds__(kThreads) batch_start_kernel(const BatchStart<
     pdl_enter();
     int tile;
     const BatchStart<T>& j = jobs[batch_entry(map, tile)];
-    int x, y;
-    if (!batch_xy(tile, j.nx, j.ny, x, y)) return;
-    const int64_t i = int64_t(x) * j.ny + y;
-    if (j.src) j.r[i] = j.src[i];
-    j.p[i] = T(0);
+    int x0, y;
+    batch_tile(tile, j.ny, x0, y);
+    if (y >= j.ny) return;
+#pragma unroll
+    for (int m = 0; m < kBatchRows; ++m) {
+        const int x = x0 + m * kBatchRowStep;
+        if (x >= j.nx) break;
+        const int64_t i = int64_t(x) * j.ny + y;
+        if (j.src) j.r[i] = j.src[i];
+        j.p[i] = T(0);
+    }
 }
 
 // The single-CTA levels of every instance, one CTA each (coarse_cycle).

@@ -15,7 +15,7 @@ import pytest
 from afsi_gpu_b200 import _lib
 from afsi_gpu_b200.multigrid import _levels
 
-TILE_Y, TILE_X, LOCAL_BITS = 32, 8, 21
+TILE_Y, TILE_X, LOCAL_BITS = 32, 32, 21
 LV = np.dtype([('nx', '<i4'), ('ny', '<i4'), ('nz', '<i4'), ('pad', '<i4'), ('n', '<i8'), ('h2', '<f4', 3),
                ('ih2', '<f4', 3)])
 LEVEL = np.dtype([('L', LV), ('C', LV), ('p', '<u8'), ('q', '<u8'), ('r', '<u8'), ('rc', '<u8'), ('down', '<u8'),
