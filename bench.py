@@ -271,8 +271,9 @@ def mg_forms_row(grid, rhs, device, reps=10):
 def batch_form_row(device, count=64, replays=20):
     """Batching form: 64 seeded 2D channel instances (grids 128x32 .. 512x128,
     5k-40k leaflet points each, N(0,1) forces), FP32 transfers and V-cycles,
-    one captured graph per step with the autotuned schedule (fixed V-cycle
-    count reaching a 1e-4 FP32 residual reduction on every instance).  The
+    one captured graph per step with the autotuned schedule (batched or
+    per-instance V-cycles; fixed V-cycle count reaching a 1e-4 FP32 residual
+    reduction on every instance).  The
     plain FP64 drop-in on the same GPU steps the same instances one at a time
     through the single-instance API (prepare2d with its support check,
     spread2d, gather2d, FP64 channel V-cycles, same cycle count).  Errors:
@@ -335,7 +336,7 @@ def batch_form_row(device, count=64, replays=20):
                v_cycles=max(rel(b.pressure(i), res[i][2]) for i in range(count)))
     return dict(instances=count, points=b.total, faces=b.nu + b.nv,
                 schedule=dict(streams=schedule.streams, order=schedule.order, smoother=schedule.smoother,
-                              cycles=schedule.cycles),
+                              cycles=schedule.cycles, vcycles=schedule.vcycles),
                 ms_per_batch_step=ms, instance_steps_per_s=count / (ms / 1e3),
                 plain_fp64_ms_per_batch=plain_ms, plain_fp64_instance_steps_per_s=count / (plain_ms / 1e3),
                 speedup_vs_plain_fp64=plain_ms / ms, error_vs_fp64=err,
