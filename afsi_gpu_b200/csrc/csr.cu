@@ -243,17 +243,33 @@ __global__ void table_keys_kernel(const int64_t* __restrict__ keys, const T* __r
     if (threadIdx.x == 0 && block_count) atomicAdd(info, block_count);
 }
 
-// Row pointers from sorted keys (row = key / divisor, sentinel = end):
-// crow[r] = first index whose row >= r, for r = 0..rows.
-__global__ void row_pointers_kernel(const uint64_t* __restrict__ keys, int64_t n, uint64_t sentinel,
-                                    uint64_t divisor, int64_t rows, int64_t* __restrict__ crow,
-                                    int64_t* __restrict__ minor) {
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i <= n; i += int64_t(gridDim.x) * blockDim.x) {
-        const bool valid = i < n && keys[i] < sentinel;
-        const int64_t cur = valid ? int64_t(keys[i] / divisor) : rows;
-        const int64_t prev = i == 0 ? -1 : (keys[i - 1] < sentinel ? int64_t(keys[i - 1] / divisor) : rows);
-        for (int64_t r = prev + 1; r <= cur && r <= rows; ++r) crow[r] = i;
-        if (valid && minor) minor[i] = int64_t(keys[i] % divisor);
+// Row pointers from sorted keys (row = key / divisor; sentinel and larger
+// keys count as row `rows`): crow[r] = first index whose row >= r, i.e. the
+// first key >= r * divisor, for r = 0..rows, one binary search per row (rows
+// without entries cost no more than others, however long the run of them).
+__global__ void row_pointers_kernel(const uint64_t* __restrict__ keys, int64_t n, uint64_t divisor, int64_t rows,
+                                    int64_t* __restrict__ crow) {
+    for (int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; r <= rows;
+         r += int64_t(gridDim.x) * blockDim.x) {
+        const uint64_t target = uint64_t(r) * divisor;
+        int64_t lo = 0, hi = n;
+        while (lo < hi) {
+            const int64_t mid = lo + ((hi - lo) >> 1);
+            if (__ldg(keys + mid) < target)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        crow[r] = lo;
+    }
+}
+
+// minor[i] = key % divisor (the column) of every entry below the sentinel.
+__global__ void minor_kernel(const uint64_t* __restrict__ keys, int64_t n, uint64_t sentinel, uint64_t divisor,
+                             int64_t* __restrict__ minor) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const uint64_t k = keys[i];
+        if (k < sentinel) minor[i] = int64_t(k % divisor);
     }
 }
 
@@ -449,6 +465,9 @@ extern "C" int32_t afsi_b200_p1_component_plan(const int64_t* base, int64_t tota
     return launched("p1_component_plan scan");
 }
 
+// Blocks for one thread per row pointer (rows + 1 of them), at most 4096.
+static unsigned rows_grid(int64_t rows) { return unsigned(rows / 256 + 1 < 4096 ? rows / 256 + 1 : 4096); }
+
 extern "C" int64_t afsi_b200_hash_csr_scratch_bytes(int64_t capacity, int32_t dtype) {
     if (capacity <= 0) return 0;
     size_t temp = dtype == AFSI_F32 ? sort_temp_bytes<float>(capacity) : sort_temp_bytes<double>(capacity);
@@ -482,13 +501,15 @@ extern "C" int32_t afsi_b200_hash_csr(const int64_t* keys, const void* values, i
         if (cub::DeviceRadixSort::SortPairs(temp, temp_bytes, ka, kb, static_cast<const T*>(values),
                                             static_cast<T*>(val), capacity, 0, end_bit, stream) != cudaSuccess)
             return fail(AFSI_ERR_CUDA, "CSR key sort failed");
-        row_pointers_kernel<<<grid, 256, 0, stream>>>(kb, capacity, sentinel, uint64_t(nf), rows, crow, col);
+        row_pointers_kernel<<<rows_grid(rows), 256, 0, stream>>>(kb, capacity, uint64_t(nf), rows, crow);
+        minor_kernel<<<grid, 256, 0, stream>>>(kb, capacity, sentinel, uint64_t(nf), col);
         transpose_keys_kernel<<<grid, 256, 0, stream>>>(kb, capacity, sentinel, uint64_t(nf), uint64_t(rows), ka);
         if ((rc = launched("hash_csr rows"))) return rc;
         if (cub::DeviceRadixSort::SortPairs(temp, temp_bytes, ka, kb, static_cast<const T*>(val),
                                             static_cast<T*>(t_val), capacity, 0, end_bit, stream) != cudaSuccess)
             return fail(AFSI_ERR_CUDA, "CSR transpose sort failed");
-        row_pointers_kernel<<<grid, 256, 0, stream>>>(kb, capacity, sentinel, uint64_t(rows), nf, t_crow, t_col);
+        row_pointers_kernel<<<rows_grid(nf), 256, 0, stream>>>(kb, capacity, uint64_t(rows), nf, t_crow);
+        minor_kernel<<<grid, 256, 0, stream>>>(kb, capacity, sentinel, uint64_t(rows), t_col);
     });
     return launched("hash_csr transpose");
 }

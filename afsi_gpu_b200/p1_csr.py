@@ -160,12 +160,17 @@ class P1CSRTransfer:
     ``interpolate_rhs`` apply the operators."""
 
     def __init__(self, grid, X, cells, *, point_density=2., max_order=8, max_points=12000000,
-                 max_entries=32000000):
+                 max_entries=32000000, transfer_dtype=None):
         if cells.dim() != 2 or cells.shape[1] != 4:
             raise ValueError('P1 CSR transfer requires four-node tetrahedra')
         if type(max_entries) is not int or max_entries < 1:
             raise ValueError('positive CSR entry budget required')
         _lib.require_cuda(X)
+        # precision form: FP64 positions, tables and contraction; the assembled
+        # operator values stored once per prepare in FP32 and applied in FP32
+        self.transfer_dtype = X.dtype if transfer_dtype is None else transfer_dtype
+        if self.transfer_dtype != X.dtype and not (X.dtype == torch.float64 and self.transfer_dtype == torch.float32):
+            raise ValueError('FP32 transfers are supported beside FP64 positions only')
         self.grid = grid
         self.node_count = X.shape[0]
         self.cells = cells.contiguous()
@@ -312,7 +317,16 @@ class P1CSRTransfer:
                                      contraction_backend='cuda', builder='b200-cell-warp+device-hash+radix-csr'))
 
     def prepare(self, x):
-        return self.assemble_stencil(self.prepare_tables(x))
+        st = self.assemble_stencil(self.prepare_tables(x))
+        if st.gather[0].val.dtype == self.transfer_dtype:
+            return st
+        cast = lambda ops: tuple(CSR(a.crow, a.col, a.val.to(self.transfer_dtype), a.shape) for a in ops)
+        return AssembledStencil(cast(st.gather), cast(st.spread), st.rule,
+                                dict(st.assembly, transfer_dtype=str(self.transfer_dtype).replace('torch.', '')))
+
+    def _check_dtype(self, t, stencil):
+        if t.dtype != stencil.gather[0].val.dtype:
+            raise ValueError(f'P1 CSR transfer in {stencil.gather[0].val.dtype} got {t.dtype} data')
 
     # -- responses
     def spread(self, coefficient, stencil):
@@ -322,6 +336,7 @@ class P1CSRTransfer:
         coefficient = coefficient.contiguous()
         if coefficient.shape != (self.node_count, 3):
             raise ValueError('P1 CSR spread expects nodal coefficients (N,3)')
+        self._check_dtype(coefficient, stencil)
         out = []
         for c, BT in enumerate(stencil.spread):
             field = coefficient.new_empty(self.grid.face_shape(c))
@@ -335,6 +350,7 @@ class P1CSRTransfer:
         out = None
         for c, (B, u) in enumerate(zip(stencil.gather, velocity)):
             _lib.require_cuda(u)
+            self._check_dtype(u, stencil)
             u = u.contiguous()
             if out is None:
                 out = u.new_empty((self.node_count, 3))

@@ -425,6 +425,78 @@ def precision_form_row(grid, X, cells, coef, vel, rhs, device, steps=20):
     return rows
 
 
+P1_SHELL = dict(nr=2, ntheta=80, nphi=160, outer=(.224, .154, .154), inner=(.214, .144, .144))
+
+
+def precision_p1_row(device, steps=3):
+    """The precision form on its own configuration: 128^3 MAC grid, a thin P1
+    tetrahedral prolate shell (128,000 elements, about 1.22 M adaptive
+    interaction points at density 2), seeded uniform nodal forces in [-1, 1],
+    a seeded Fourier face velocity and a mean-free N(0,1) pressure RHS.  A step
+    is the P1 prepare and CSR assembly (positions, tables and contraction in
+    FP64), the spread and the interpolate, and the pressure solve to the FP64
+    tolerance.  Plain: FP64 operators and FP64 V-cycles.  Precision form: the
+    assembled operator values rounded to FP32, FP32 spread / interpolate, and
+    FP32 V-cycles inside FP64 iterative refinement.  CUDA events around
+    `steps` steps of each after one untimed step; errors are the largest
+    differences from the FP64 step's outputs over their largest values."""
+    from afsi_gpu_b200 import synthetic
+    from afsi_gpu_b200.grid import MACGrid
+    from afsi_gpu_b200.multigrid import GeometricMultigrid, RefinedMultigrid
+    from afsi_gpu_b200.p1_csr import P1CSRTransfer
+    grid = MACGrid((128, 128, 128), (1., 1., 1.))
+    X, cells = synthetic.prolate_shell(**P1_SHELL)
+    rng = np.random.default_rng(21)
+    x = torch.as_tensor(X, device=device)
+    cells_t = torch.as_tensor(cells, device=device)
+    c64 = torch.as_tensor(rng.uniform(-1., 1., (X.shape[0], 3)), device=device)
+    v64 = tuple(v.to(device) for v in synthetic.fourier_velocity3d(grid, seed=21))
+    r64 = synthetic.mean_free_normal(grid.shape, seed=21).to(device)
+    budget = dict(max_entries=400_000_000)
+    tr64 = P1CSRTransfer(grid, x, cells_t, **budget)
+    tr32 = P1CSRTransfer(grid, x, cells_t, transfer_dtype=torch.float32, **budget)
+    mg64 = GeometricMultigrid(grid, device=device, backend='b200-graph')
+    mg32 = RefinedMultigrid(grid, device=device)
+    c32, v32 = c64.float(), tuple(v.float() for v in v64)
+    stream = torch.cuda.current_stream(device)
+
+    def step(tr, mg, c, v):
+        st = tr.prepare(x)
+        return tr.spread(c, st), tr.interpolate_rhs(v, st), mg.solve(r64), st
+
+    def timed(*args):
+        out = step(*args)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        e0.record(stream)
+        for _ in range(steps):
+            out = step(*args)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        return out, e0.elapsed_time(e1) / steps
+
+    def rel(a, b):
+        return float((a.double() - b.double()).abs().max() / b.double().abs().max())
+
+    ref, ms64 = timed(tr64, mg64, c64, v64)
+    out, ms32 = timed(tr32, mg32, c32, v32)
+    info64, info32 = ref[2][1], out[2][1]
+    return dict(workload=(f'128^3 MAC, P1 prolate shell {cells.shape[0]} elements / '
+                          f'{ref[3].rule.point_count} points, uniform [-1,1] forces'),
+                points=int(ref[3].rule.point_count), elements=int(cells.shape[0]),
+                csr_nnz=int(ref[3].assembly['total_nnz']),
+                plain_fp64=dict(steps_per_s=1e3 / ms64, ms_per_step=ms64, cycles=info64['cycles'],
+                                residual=info64['residual_norm'], tolerance=info64['tolerance']),
+                precision_form=dict(steps_per_s=1e3 / ms32, ms_per_step=ms32, transfer_dtype='f32',
+                                    positions='f64',
+                                    mg=(f"FP32 V-cycles in FP64 refinement, {info32['refinements']} refinements, "
+                                        f"{info32['cycles']} FP32 cycles"),
+                                    residual=info32['residual_norm'], tolerance=info32['tolerance']),
+                speedup_vs_plain_fp64=ms64 / ms32,
+                error_vs_fp64=dict(spread=max(rel(a, b) for a, b in zip(out[0], ref[0])),
+                                   interpolate=rel(out[1], ref[1]), pressure=rel(out[2][0], ref[2][0])))
+
+
 def deterministic_row(step, coef, device, reps=10):
     """The P2 spread of the step in its deterministic mode (tile-sorted,
     atomic-free, bitwise reproducible) beside the atomic spread: CUDA events
@@ -734,6 +806,8 @@ def run_b200(args):
         mass = mass_pcg_row(X, cells, device, pk['hbm_gbs']) if extra else None
         forms = mg_forms_row(grid, rhs, device) if extra else None
         precision = precision_form_row(grid, X, cells, coef, vel, rhs, device) if extra else None
+        if extra:
+            precision['p1_128'] = precision_p1_row(device)
         deterministic = deterministic_row(step, coef, device) if extra else None
         batch = batch_form_row(device) if extra else None
         serving = serving_form_row(device) if extra else None

@@ -216,6 +216,41 @@ def test_p1_fp32_operators_and_budget_errors():
         small.prepare(X.double())
 
 
+def test_p1_precision_form_fp32_transfers_beside_fp64_positions():
+    """transfer_dtype=float32 with FP64 positions: rule, tables and contraction
+    in FP64, the operator values rounded once to FP32 (equal to the FP64
+    values cast), spread and interpolate in FP32 within 2e-6 of the field
+    scale of the FP64 oracle; FP64 data is refused."""
+    g = golden('p1csr')
+    grid = _grid(g)
+    Xn, cells = g['block_X'], g['block_cells']
+    tr64 = P1CSRTransfer(grid, t(Xn), t(cells))
+    tr32 = P1CSRTransfer(grid, t(Xn), t(cells), transfer_dtype=torch.float32)
+    A64, A32 = tr64.prepare(t(Xn)), tr32.prepare(t(Xn))
+    assert A32.assembly['transfer_dtype'] == 'float32'
+    for a, b in zip(A32.gather + A32.spread, A64.gather + A64.spread):
+        assert a.val.dtype == torch.float32 and torch.equal(a.val, b.val.float())
+        assert torch.equal(a.col, b.col) and torch.equal(a.crow, b.crow)
+    rng = np.random.default_rng(9)
+    coef = rng.uniform(-1, 1, (Xn.shape[0], 3))
+    vel = [rng.standard_normal(grid.face_shape(c)) for c in range(3)]
+    fields = tr32.spread(t(coef, torch.float32), A32)
+    rhs = tr32.interpolate_rhs(tuple(t(v, torch.float32) for v in vel), A32)
+    groups = [(gr.cells.cpu().numpy(), gr.values.cpu().numpy(), gr.weights.cpu().numpy()) for gr in A64.rule.groups]
+    base, phi, _ = oib.p2_prepare(Xn, [(c, N) for c, N, _ in groups], grid.origin, grid.spacing, grid.shape)
+    for c in range(3):
+        fs = grid.face_shape(c)
+        _, _, (crow, col, val) = ocsr.assemble(base, phi, groups, c, fs, Xn.shape[0])
+        tcrow, tcol, tval = ocsr.csr_transpose(crow, col, val, int(np.prod(fs)))
+        expect = ocsr.csr_matvec(tcrow, tcol, tval, coef[:, c]) / grid.volume
+        got = fields[c].reshape(-1).double().cpu().numpy()
+        np.testing.assert_allclose(got, expect, rtol=0, atol=2e-6 * np.abs(expect).max())
+        r = ocsr.csr_matvec(crow, col, val, vel[c].reshape(-1))
+        np.testing.assert_allclose(rhs[:, c].double().cpu().numpy(), r, rtol=0, atol=2e-6 * np.abs(r).max())
+    with pytest.raises(ValueError, match='float64'):
+        tr32.spread(t(coef), A32)
+
+
 def _table(keys, values):
     from afsi_gpu_b200.p1_csr import HashWorkspace
     ws = HashWorkspace()
