@@ -42,6 +42,27 @@ constexpr int kWarps = 4;       // warps per block
 constexpr int kChunk = 64;      // points whose forces are held at once
 template <class T> struct BoxCap { static constexpr int value = 4608 / sizeof(T); };  // gather patch (576 doubles)
 constexpr int kSpreadCap = 288;   // spread: entries of one component's padded box per copy
+
+// f(t, x, y, z) for the cells t = lane, lane + 32, ... of an ex x ey x ez box
+// (z fastest); the coordinates advance by mixed-radix addition of 32 (one
+// carry per axis at most) instead of two divisions per cell.
+template <class F>
+__device__ __forceinline__ void box_walk(int lane, int ex, int ey, int ez, F f) {
+    const int n = ex * ey * ez;
+    if (lane >= n) return;
+    const int qz = 32 % ez, q = 32 / ez, qy = q % ey, qx = q / ey;
+    int z = lane % ez, r = lane / ez, y = r % ey, x = r / ey;
+    for (int t = lane; t < n; t += 32) {
+        f(t, x, y, z);
+        z += qz;
+        int carry = z >= ez ? 1 : 0;
+        z -= carry * ez;
+        y += qy + carry;
+        carry = y >= ey ? 1 : 0;
+        y -= carry * ey;
+        x += qx + carry;
+    }
+}
 constexpr int kSpreadBlocks = 6;  // resident blocks per SM the spread is compiled for
 constexpr int kGatherBlocks = 6;  // same for the gather
 
@@ -271,15 +292,12 @@ __global__ void __launch_bounds__(kWarps * 32, kSpreadBlocks) p2_spread_kernel(
             }
             __syncwarp();
             if (fits) {
-                const int ey = bx.ext[c][1], ez = bx.ext[c][2];
-                const int n = bx.ext[c][0] * ey * ez;
-                for (int t = lane; t < n; t += 32) {
-                    const int z = t % ez, r = t / ez, y = r % ey, x = r / ey;
+                box_walk(lane, bx.ext[c][0], bx.ext[c][1], bx.ext[c][2], [&](int, int x, int y, int z) {
                     const int o = x * sx + y * sy + z;
                     const T v = s.copy[0][o] + s.copy[1][o];
                     if (v != T(0))
                         atomicAdd(field + face_index(g, c, bx.lo[c][0] + x, bx.lo[c][1] + y, bx.lo[c][2] + z), v);
-                }
+                });
             }
         }
         __syncwarp();
@@ -420,15 +438,12 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) p2_spread_rows_kernel(
             }
             __syncwarp();
             if (fits) {
-                const int ey = bx.ext[c][1], ez = bx.ext[c][2];
-                const int m = bx.ext[c][0] * ey * ez;
-                for (int t = lane; t < m; t += 32) {
-                    const int z = t % ez, r = t / ez, y = r % ey, x = r / ey;
+                box_walk(lane, bx.ext[c][0], bx.ext[c][1], bx.ext[c][2], [&](int, int x, int y, int z) {
                     const int o = x * sx + y * sy + z;
                     const T v = s.copy[0][o] + s.copy[1][o];
                     if (v != T(0))
                         atomicAdd(field + face_index(g, c, bx.lo[c][0] + x, bx.lo[c][1] + y, bx.lo[c][2] + z), v);
-                }
+                });
             }
         }
         __syncwarp();
@@ -463,13 +478,10 @@ __global__ void __launch_bounds__(kWarps * 32, kGatherBlocks) p2_gather_kernel(c
         if (fits) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const int ey = bx.ext[c][1], ez = bx.ext[c][2];
-                const int n = bx.ext[c][0] * ey * ez;
-                for (int t = lane; t < n; t += 32) {
-                    const int z = t % ez, r = t / ez;
-                    s.patch[bx.off[c] + t] =
-                        fields[c][face_index(g, c, bx.lo[c][0] + r / ey, bx.lo[c][1] + r % ey, bx.lo[c][2] + z)];
-                }
+                box_walk(lane, bx.ext[c][0], bx.ext[c][1], bx.ext[c][2], [&](int t, int x, int y, int z) {
+                    s.patch[bx.off[c] + t] = fields[c][face_index(g, c, bx.lo[c][0] + x, bx.lo[c][1] + y,
+                                                                  bx.lo[c][2] + z)];
+                });
             }
         }
         __syncwarp();
