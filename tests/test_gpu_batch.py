@@ -130,3 +130,43 @@ def test_batched_vcycles_match_each_solver_alone(smooth):
         alone.initialize(torch.zeros_like(r), r)
         p = alone.advance(3)
         assert torch.equal(p, mg.workspace.p[0])
+
+
+@pytest.mark.parametrize('shapes', [[(256, 64)], [(32, 8), (64, 16), (16, 4)], [(512, 128), (8, 4), (384, 96)]])
+def test_batched_vcycles_fp64_single_and_coarse_only_batches(shapes):
+    """FP64 workspaces with FP64 coarsest solves; a batch of one; a batch
+    whose instances all run wholly in one CTA (no launched level); a mix of
+    two launched levels with a tiny instance."""
+    from afsi_gpu_b200.batch import BatchedVCycles
+    from afsi_gpu_b200.grid import ChannelGrid
+    from afsi_gpu_b200.multigrid import ChannelMultigrid
+    rng = np.random.default_rng(len(shapes))
+    grids = [ChannelGrid(s, (4., 1.)) for s in shapes]
+
+    def solver(g):
+        return ChannelMultigrid(g, device=DEV, dtype=torch.float64, backend='b200')
+    rhs = [torch.as_tensor(rng.standard_normal(s), device=DEV) for s in shapes]
+    batch = [solver(g) for g in grids]
+    bv = BatchedVCycles(batch, rhs)
+    bv.run(3)
+    torch.cuda.synchronize()
+    for g, r, mg in zip(grids, rhs, batch):
+        alone = solver(g)
+        alone.initialize(torch.zeros_like(r), r)
+        assert torch.equal(alone.advance(3), mg.workspace.p[0])
+
+
+def test_batched_vcycles_reject_what_they_do_not_batch():
+    from afsi_gpu_b200.batch import BatchedVCycles
+    from afsi_gpu_b200.grid import ChannelGrid
+    from afsi_gpu_b200.multigrid import ChannelMultigrid
+    g = ChannelGrid((64, 16), (4., 1.))
+    a = ChannelMultigrid(g, device=DEV, dtype=torch.float32, coarse_dtype=torch.float64, backend='b200')
+    b = ChannelMultigrid(g, device=DEV, dtype=torch.float64, backend='b200')
+    rb = ChannelMultigrid(g, device=DEV, dtype=torch.float32, coarse_dtype=torch.float64, backend='b200',
+                          smoother='red-black')
+    for pair in ((a, b), (a, rb)):
+        with pytest.raises(ValueError, match='batched V-cycles'):
+            BatchedVCycles(list(pair))
+    with pytest.raises(ValueError, match='sources'):
+        BatchedVCycles([a]).run(1)
