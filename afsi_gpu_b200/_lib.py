@@ -133,6 +133,7 @@ _SIGNATURES = {
     'afsi_b200_mg_batch_table_bytes': [c_void_p, c_int32],
     'afsi_b200_mg_batch_table': [c_void_p, c_int32, c_void_p, c_void_p, c_int64],
     'afsi_b200_mg_batch_vcycles': [c_void_p, c_int32, c_void_p, c_int32, c_int32, c_void_p],
+    'afsi_b200_mg_batch_persistent': [c_void_p, c_int32, c_void_p, c_int32, c_int32, c_void_p, c_void_p],
     'afsi_b200_batch2d_prepare': [c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_int32,
                                   c_void_p],
     'afsi_b200_batch2d_spread': [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_void_p,

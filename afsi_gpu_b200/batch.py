@@ -62,7 +62,7 @@ class Schedule:
     order: str = 'largest-first'
     smoother: str = 'jacobi'
     cycles: int = 6
-    vcycles: str = 'streams'   # 'streams' (per instance over side streams) or 'batched' (Jacobi only)
+    vcycles: str = 'streams'   # 'streams' (per instance over side streams), 'batched' or 'persistent' (Jacobi)
 
 
 class BatchedVCycles:
@@ -96,15 +96,29 @@ class BatchedVCycles:
             raise ValueError(f'batched V-cycles: {lib.afsi_b200_last_error().decode(errors="replace")}')
         host = np.zeros(int(nbytes), np.uint8)
         call('afsi_b200_mg_batch_table', self._plans, self.count, self._sources, host.ctypes.data, int(nbytes))
-        self.table = torch.as_tensor(host).to(self.solvers[0].workspace.p[0].device)
+        device = self.solvers[0].workspace.p[0].device
+        self.table = torch.as_tensor(host).to(device)
+        self.sync = torch.zeros(int(lib.afsi_b200_mg_sync_bytes()), dtype=torch.uint8, device=device)
 
-    def run(self, cycles, *, start=True):
+    def run(self, cycles, *, start=True, persistent=False):
         """`cycles` V-cycles of every solver on the current stream; with
-        `start`, from a zero iterate with the sources as right-hand sides."""
+        `start`, from a zero iterate with the sources as right-hand sides.
+        persistent: all of it in one cooperative launch
+        (``afsi_b200_mg_batch_persistent``) instead of one launch per level
+        operation; the results are the same bit for bit."""
         if start and self._sources is None:
             raise ValueError('a start needs right-hand-side sources')
-        call('afsi_b200_mg_batch_vcycles', self._plans, self.count, ptr(self.table), int(cycles), int(start),
-             torch.cuda.current_stream(self.table.device).cuda_stream)
+        s = torch.cuda.current_stream(self.table.device).cuda_stream
+        if persistent:
+            call('afsi_b200_mg_batch_persistent', self._plans, self.count, ptr(self.table), int(cycles), int(start),
+                 ptr(self.sync), s)
+        else:
+            call('afsi_b200_mg_batch_vcycles', self._plans, self.count, ptr(self.table), int(cycles), int(start), s)
+
+    def check(self):
+        """Raise if a grid barrier of a persistent run timed out."""
+        if int(self.sync[8:12].view(torch.int32).item()):
+            raise RuntimeError('persistent batched V-cycles: a grid barrier timed out')
 
 
 class BatchedChannels:
@@ -201,10 +215,10 @@ class BatchedChannels:
         schedule = schedule or self.schedule
         main = torch.cuda.current_stream(self.device)
         self.transfers(main)
-        if schedule.vcycles == 'batched':
+        if schedule.vcycles in ('batched', 'persistent'):
             if schedule.smoother != 'jacobi':
                 raise ValueError('batched V-cycles use the Jacobi smoother')
-            self.batched().run(schedule.cycles)
+            self.batched().run(schedule.cycles, persistent=schedule.vcycles == 'persistent')
             return
         if schedule.vcycles != 'streams':
             raise ValueError(f'unknown V-cycle schedule {schedule.vcycles!r}')
@@ -220,7 +234,7 @@ class BatchedChannels:
     def capture(self, schedule=None):
         schedule = schedule or self.schedule
         self.solvers(schedule.smoother)
-        if schedule.vcycles == 'batched':
+        if schedule.vcycles in ('batched', 'persistent'):
             self.batched()
         with torch.cuda.device(self.device):
             warm = torch.cuda.Stream(device=self.device)
@@ -267,6 +281,8 @@ class BatchedChannels:
         return out
 
     def check(self):
+        if self._batched is not None:
+            self._batched.check()
         word = int(self.status.item())
         self.status.zero_()
         if word & _lib.FLAG_SUPPORT:
@@ -297,8 +313,8 @@ class BatchedChannels:
             candidates = [Schedule(streams=s, order=order, smoother=smoother, cycles=cycles)
                           for s in streams for order in orders]
             if smoother == 'jacobi':
-                candidates.append(Schedule(streams=1, order='given', smoother=smoother, cycles=cycles,
-                                           vcycles='batched'))
+                candidates += [Schedule(streams=1, order='given', smoother=smoother, cycles=cycles, vcycles=v)
+                               for v in ('batched', 'persistent')]
             for sch in candidates:
                 g, launches = self.capture(sch)
                 g.replay()
@@ -350,7 +366,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=main.__doc__)
     ap.add_argument('--instances', type=int, default=64)
     ap.add_argument('--seed', type=int, default=0)
-    ap.add_argument('--vcycles', choices=('batched', 'streams'), default='batched')
+    ap.add_argument('--vcycles', choices=('batched', 'persistent', 'streams'), default='batched')
     ap.add_argument('--smoother', choices=('jacobi', 'red-black'), default='jacobi')
     ap.add_argument('--streams', type=int, default=16)
     ap.add_argument('--cycles', type=int, default=4)

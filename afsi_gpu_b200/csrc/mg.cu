@@ -1295,38 +1295,33 @@ struct BatchStart {
     int nx, ny;
 };
 
-// This block's entry and tile.
-__device__ __forceinline__ int batch_entry(const uint32_t* __restrict__ map, int& tile) {
-    const uint32_t w = map[blockIdx.x];
+// Entry and tile of a block map word.
+__device__ __forceinline__ int batch_word(uint32_t w, int& tile) {
     tile = int(w & ((1u << kBatchLocalBits) - 1));
     return int(w >> kBatchLocalBits);
 }
 
-// This thread's column y and first row x0 in the tile; its cells are
-// (x0 + m * kBatchRowStep, y), m < kBatchRows.
-__device__ __forceinline__ void batch_tile(int tile, int ny, int& x0, int& y) {
+// Column y and first row x0 of thread `tid` (of kThreads) in the tile; its
+// cells are (x0 + m * kBatchRowStep, y), m < kBatchRows.
+__device__ __forceinline__ void batch_tile(int tile, int ny, int tid, int& x0, int& y) {
     const int gy = (ny + kBatchTileY - 1) / kBatchTileY;
-    y = (tile % gy) * kBatchTileY + int(threadIdx.x % kBatchTileY);
-    x0 = (tile / gy) * kBatchTileX + int(threadIdx.x / kBatchTileY);
+    y = (tile % gy) * kBatchTileY + tid % kBatchTileY;
+    x0 = (tile / gy) * kBatchTileX + tid / kBatchTileY;
 }
 
-// The kernels below compute all of a thread's cells before storing any, so
-// the loads of the cells are in flight together (the outputs never alias
-// another cell's inputs).
+// The tile operations below compute all of a thread's cells before storing
+// any, so the loads of the cells are in flight together (the outputs never
+// alias another cell's inputs).  They are shared by the per-operation
+// launches and the persistent kernel.
 
-// One Jacobi sweep of every entry: p -> q (odd == 0) or q -> p (odd == 1);
+// One Jacobi sweep of an entry's tile: p -> q (odd == 0) or q -> p (odd == 1);
 // zero_in: the iterate is zero (first sweep below the finest level).  The
 // arithmetic of sweep_kernel with no pending shifts.
 template <int BC, class T>
-__global__ void __launch_bounds__(kThreads) batch_sweep_kernel(const BatchLevel<T>* __restrict__ lv,
-                                                               const uint32_t* __restrict__ map, int odd,
-                                                               int zero_in) {
-    pdl_enter();
-    int tile;
-    const BatchLevel<T>& e = lv[batch_entry(map, tile)];
+__device__ __forceinline__ void sweep_tile(const BatchLevel<T>& e, int tile, int tid, int odd, int zero_in) {
     const Lv<T> L = e.L;
     int x0, y;
-    batch_tile(tile, L.ny, x0, y);
+    batch_tile(tile, L.ny, tid, x0, y);
     if (y >= L.ny) return;
     const T* p = odd ? e.q : e.p;
     T* out = odd ? e.p : e.q;
@@ -1356,14 +1351,10 @@ __global__ void __launch_bounds__(kThreads) batch_sweep_kernel(const BatchLevel<
 
 // rc = restricted residual of the pre-smoothed iterate (residual_restrict_kernel).
 template <int BC, class T>
-__global__ void __launch_bounds__(kThreads) batch_restrict_kernel(const BatchLevel<T>* __restrict__ lv,
-                                                                  const uint32_t* __restrict__ map) {
-    pdl_enter();
-    int tile;
-    const BatchLevel<T>& e = lv[batch_entry(map, tile)];
+__device__ __forceinline__ void restrict_tile(const BatchLevel<T>& e, int tile, int tid) {
     const Lv<T> C = e.C;
     int cx0, cy;
-    batch_tile(tile, C.ny, cx0, cy);
+    batch_tile(tile, C.ny, tid, cx0, cy);
     if (cy >= C.ny) return;
     const Lv<T> L = e.L;
     T v[kBatchRows];
@@ -1383,14 +1374,10 @@ __global__ void __launch_bounds__(kThreads) batch_restrict_kernel(const BatchLev
 
 // p = down + P(corr) (prolong_kernel; down may be p itself, own cell only).
 template <int BC, class T>
-__global__ void __launch_bounds__(kThreads) batch_prolong_kernel(const BatchLevel<T>* __restrict__ lv,
-                                                                 const uint32_t* __restrict__ map) {
-    pdl_enter();
-    int tile;
-    const BatchLevel<T>& e = lv[batch_entry(map, tile)];
+__device__ __forceinline__ void prolong_tile(const BatchLevel<T>& e, int tile, int tid) {
     const Lv<T> L = e.L;
     int x0, y;
-    batch_tile(tile, L.ny, x0, y);
+    batch_tile(tile, L.ny, tid, x0, y);
     if (y >= L.ny) return;
     const Lv<T> C = e.C;
     T v[kBatchRows];
@@ -1410,13 +1397,9 @@ __global__ void __launch_bounds__(kThreads) batch_prolong_kernel(const BatchLeve
 
 // p = q after an odd number of post-sweeps on the finest level (the finalize copy).
 template <class T>
-__global__ void __launch_bounds__(kThreads) batch_finalize_kernel(const BatchLevel<T>* __restrict__ lv,
-                                                                  const uint32_t* __restrict__ map) {
-    pdl_enter();
-    int tile;
-    const BatchLevel<T>& e = lv[batch_entry(map, tile)];
+__device__ __forceinline__ void finalize_tile(const BatchLevel<T>& e, int tile, int tid) {
     int x0, y;
-    batch_tile(tile, e.L.ny, x0, y);
+    batch_tile(tile, e.L.ny, tid, x0, y);
     if (y >= e.L.ny) return;
 #pragma unroll
     for (int m = 0; m < kBatchRows; ++m) {
@@ -1427,16 +1410,12 @@ __global__ void __launch_bounds__(kThreads) batch_finalize_kernel(const BatchLev
     }
 }
 
-// Cycle start of every instance: finest rhs = its source (when the table has
+// Cycle start of an instance: finest rhs = its source (when the table has
 // one), iterate = 0.
 template <class T>
-__global__ void __launch_bounds__(kThreads) batch_start_kernel(const BatchStart<T>* __restrict__ jobs,
-                                                               const uint32_t* __restrict__ map) {
-    pdl_enter();
-    int tile;
-    const BatchStart<T>& j = jobs[batch_entry(map, tile)];
+__device__ __forceinline__ void start_tile(const BatchStart<T>& j, int tile, int tid) {
     int x0, y;
-    batch_tile(tile, j.ny, x0, y);
+    batch_tile(tile, j.ny, tid, x0, y);
     if (y >= j.ny) return;
 #pragma unroll
     for (int m = 0; m < kBatchRows; ++m) {
@@ -1446,6 +1425,52 @@ __global__ void __launch_bounds__(kThreads) batch_start_kernel(const BatchStart<
         if (j.src) j.r[i] = j.src[i];
         j.p[i] = T(0);
     }
+}
+
+template <int BC, class T>
+__global__ void __launch_bounds__(kThreads) batch_sweep_kernel(const BatchLevel<T>* __restrict__ lv,
+                                                               const uint32_t* __restrict__ map, int odd,
+                                                               int zero_in) {
+    pdl_enter();
+    int tile;
+    const int ent = batch_word(map[blockIdx.x], tile);
+    sweep_tile<BC>(lv[ent], tile, threadIdx.x, odd, zero_in);
+}
+
+template <int BC, class T>
+__global__ void __launch_bounds__(kThreads) batch_restrict_kernel(const BatchLevel<T>* __restrict__ lv,
+                                                                  const uint32_t* __restrict__ map) {
+    pdl_enter();
+    int tile;
+    const int ent = batch_word(map[blockIdx.x], tile);
+    restrict_tile<BC>(lv[ent], tile, threadIdx.x);
+}
+
+template <int BC, class T>
+__global__ void __launch_bounds__(kThreads) batch_prolong_kernel(const BatchLevel<T>* __restrict__ lv,
+                                                                 const uint32_t* __restrict__ map) {
+    pdl_enter();
+    int tile;
+    const int ent = batch_word(map[blockIdx.x], tile);
+    prolong_tile<BC>(lv[ent], tile, threadIdx.x);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) batch_finalize_kernel(const BatchLevel<T>* __restrict__ lv,
+                                                                  const uint32_t* __restrict__ map) {
+    pdl_enter();
+    int tile;
+    const int ent = batch_word(map[blockIdx.x], tile);
+    finalize_tile(lv[ent], tile, threadIdx.x);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) batch_start_kernel(const BatchStart<T>* __restrict__ jobs,
+                                                               const uint32_t* __restrict__ map) {
+    pdl_enter();
+    int tile;
+    const int ent = batch_word(map[blockIdx.x], tile);
+    start_tile(jobs[ent], tile, threadIdx.x);
 }
 
 // The single-CTA levels of every instance, one CTA each (coarse_cycle).
@@ -1466,6 +1491,91 @@ __global__ void __launch_bounds__(kCoarseThreads) batch_coarse_kernel(const Batc
     __syncthreads();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     coarse_cycle<BC, T, TC>(reinterpret_cast<T*>(smem_raw), rhs, nullptr, p_start, p_out, cinv, cl, smooth);
+}
+
+// ---- persistent batched V-cycles: every level operation of every cycle in
+// one cooperative launch, the launches of batch_cycles replaced by grid
+// barriers (bounded waits; a timed-out barrier sets the error word and the
+// kernel returns).  Each 1024-thread CTA works as four 256-thread virtual
+// blocks over the block maps; the coarse jobs go to CTAs in turn.
+
+constexpr int kBatchPThreads = 1024;
+constexpr int kBatchVirtual = kBatchPThreads / kThreads;
+
+template <class T, class TC>
+struct BatchPersistArgs {
+    const unsigned char* table;
+    int64_t level_off[AFSI_MG_MAX_LEVELS], map_l_off[AFSI_MG_MAX_LEVELS], map_c_off[AFSI_MG_MAX_LEVELS];
+    int64_t blocks_l[AFSI_MG_MAX_LEVELS], blocks_c[AFSI_MG_MAX_LEVELS];
+    int64_t start_off, start_map_off, blocks_start, coarse_off;
+    int depths, smooth, count, cycles, start;
+    GridSync gs;
+};
+
+template <int BC, class T, class TC>
+__global__ void __launch_bounds__(kBatchPThreads, 1) batch_persistent_kernel(BatchPersistArgs<T, TC> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ CoarseLevels<T> cl;
+    const int tid = threadIdx.x % kThreads;
+    const int64_t vb0 = int64_t(blockIdx.x) * kBatchVirtual + threadIdx.x / kThreads;
+    const int64_t vstride = int64_t(gridDim.x) * kBatchVirtual;
+    auto lv = [&](int d) { return reinterpret_cast<const BatchLevel<T>*>(a.table + a.level_off[d]); };
+    auto ml = [&](int d) { return reinterpret_cast<const uint32_t*>(a.table + a.map_l_off[d]); };
+    auto mc = [&](int d) { return reinterpret_cast<const uint32_t*>(a.table + a.map_c_off[d]); };
+    // f(entry, tile) for the blocks of a map, virtual block by virtual block
+    auto over = [&](int64_t blocks, const uint32_t* map, auto f) {
+        for (int64_t b = vb0; b < blocks; b += vstride) {
+            int tile;
+            const int ent = batch_word(map[b], tile);
+            f(ent, tile);
+        }
+    };
+    bool ok = true;
+    if (a.start) {
+        const BatchStart<T>* jobs = reinterpret_cast<const BatchStart<T>*>(a.table + a.start_off);
+        over(a.blocks_start, reinterpret_cast<const uint32_t*>(a.table + a.start_map_off),
+             [&](int ent, int tile) { start_tile(jobs[ent], tile, tid); });
+        ok = grid_sync(a.gs, 0.0, nullptr);
+    }
+    for (int c = 0; c < a.cycles && ok; ++c) {
+        for (int d = 0; d < a.depths && ok; ++d) {
+            const BatchLevel<T>* L = lv(d);
+            for (int s = 0; s < a.smooth && ok; ++s) {
+                const int zero = (s == 0 && d > 0) ? 1 : 0;
+                over(a.blocks_l[d], ml(d), [&](int ent, int tile) { sweep_tile<BC>(L[ent], tile, tid, s & 1, zero); });
+                ok = grid_sync(a.gs, 0.0, nullptr);
+            }
+            if (!ok) break;
+            over(a.blocks_c[d], mc(d), [&](int ent, int tile) { restrict_tile<BC>(L[ent], tile, tid); });
+            ok = grid_sync(a.gs, 0.0, nullptr);
+        }
+        if (!ok) break;
+        const BatchCoarse<T, TC>* jobs = reinterpret_cast<const BatchCoarse<T, TC>*>(a.table + a.coarse_off);
+        for (int j = blockIdx.x; j < a.count; j += gridDim.x) {
+            const unsigned* src = reinterpret_cast<const unsigned*>(&jobs[j].cl);
+            unsigned* dst = reinterpret_cast<unsigned*>(&cl);
+            for (int k = threadIdx.x; k < int(sizeof(cl) / 4); k += blockDim.x) dst[k] = src[k];
+            __syncthreads();
+            coarse_cycle<BC, T, TC>(reinterpret_cast<T*>(smem_raw), jobs[j].rhs, nullptr, jobs[j].p_start,
+                                    jobs[j].p_out, jobs[j].cinv, cl, a.smooth);
+            __syncthreads();
+        }
+        ok = grid_sync(a.gs, 0.0, nullptr);
+        for (int d = a.depths - 1; d >= 0 && ok; --d) {
+            const BatchLevel<T>* L = lv(d);
+            over(a.blocks_l[d], ml(d), [&](int ent, int tile) { prolong_tile<BC>(L[ent], tile, tid); });
+            ok = grid_sync(a.gs, 0.0, nullptr);
+            for (int s = 0; s < a.smooth && ok; ++s) {
+                over(a.blocks_l[d], ml(d), [&](int ent, int tile) { sweep_tile<BC>(L[ent], tile, tid, s & 1, 0); });
+                ok = grid_sync(a.gs, 0.0, nullptr);
+            }
+        }
+        if (ok && a.depths > 0 && a.smooth % 2 == 1) {
+            const BatchLevel<T>* L = lv(0);
+            over(a.blocks_l[0], ml(0), [&](int ent, int tile) { finalize_tile(L[ent], tile, tid); });
+            ok = grid_sync(a.gs, 0.0, nullptr);
+        }
+    }
 }
 
 }  // namespace afsi
@@ -1678,6 +1788,69 @@ int32_t batch_cycles(const afsi_mg_plan* const* plans, int count, const unsigned
     return AFSI_OK;
 }
 
+// The persistent form of batch_cycles: one cooperative launch, one CTA per
+// SM; `sync` is afsi_b200_mg_sync_bytes() of zero-initialised barrier words
+// (its error word is cleared here).
+template <class T, class TC>
+int32_t batch_persistent(const afsi_mg_plan* const* plans, int count, const unsigned char* table, int cycles,
+                         int start, void* sync, cudaStream_t stream) {
+    constexpr int BC = AFSI_BC_CHANNEL;
+    BatchLayout lay;
+    int32_t rc = batch_table<T, TC>(plans, count, nullptr, lay, nullptr);
+    if (rc) return rc;
+    BatchPersistArgs<T, TC> a;
+    a.table = table;
+    for (int d = 0; d < AFSI_MG_MAX_LEVELS; ++d) {
+        a.level_off[d] = lay.level_off[d];
+        a.map_l_off[d] = lay.map_l_off[d];
+        a.map_c_off[d] = lay.map_c_off[d];
+        a.blocks_l[d] = lay.blocks_l[d];
+        a.blocks_c[d] = lay.blocks_c[d];
+    }
+    a.start_off = lay.start_off;
+    a.start_map_off = lay.start_map_off;
+    a.blocks_start = lay.blocks_start;
+    a.coarse_off = lay.coarse_off;
+    a.depths = lay.depths;
+    a.smooth = plans[0]->smooth;
+    a.count = count;
+    a.cycles = cycles;
+    a.start = start;
+    unsigned char* b = static_cast<unsigned char*>(sync);
+    a.gs.count = reinterpret_cast<unsigned int*>(b);
+    a.gs.gen = reinterpret_cast<unsigned int*>(b + 4);
+    a.gs.error = reinterpret_cast<int*>(b + 8);
+    a.gs.slot = reinterpret_cast<double*>(b + 64);
+    a.gs.partial = reinterpret_cast<double*>(b + 64 + 8 * (AFSI_MG_MAX_LEVELS * 3 + 8));
+    auto kernel = batch_persistent_kernel<BC, T, TC>;
+    static int per_sm = -1;  // once per instantiation, before any graph capture of it
+    if (per_sm < 0) {
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBatchPThreads, 200 * 1024);
+    }
+    int device = 0, sms = 0;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    AFSI_REQUIRE(per_sm >= 1 && sms >= 1 && sms <= 4096, "persistent batched V-cycles do not fit on this device");
+    // counter, generation and error word start from zero (a run whose barrier
+    // timed out may have left the counter part-way)
+    if (cudaMemsetAsync(sync, 0, 12, stream) != cudaSuccess)
+        return fail(AFSI_ERR_CUDA, "clearing the barrier words failed");
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(sms);
+    cfg.blockDim = dim3(kBatchPThreads);
+    cfg.dynamicSmemBytes = lay.coarse_smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeCooperative;
+    attr.val.cooperative = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    const cudaError_t err = cudaLaunchKernelEx(&cfg, kernel, a);
+    if (err != cudaSuccess) return fail(AFSI_ERR_CUDA, "persistent batched V-cycles: %s", cudaGetErrorString(err));
+    return launched("mg batch persistent");
+}
+
 #define AFSI_BATCH_DISPATCH(plans, ...)      \
     AFSI_DISPATCH((plans)[0]->dtype, {        \
         if ((plans)[0]->coarse_dtype == AFSI_F64) { \
@@ -1724,6 +1897,21 @@ extern "C" int32_t afsi_b200_mg_batch_vcycles(const afsi_mg_plan* const* plans, 
     AFSI_BATCH_DISPATCH(plans, {
         return batch_cycles<T, TC>(plans, count, static_cast<const unsigned char*>(table), cycles, start ? 1 : 0,
                                    static_cast<cudaStream_t>(stream));
+    });
+    return AFSI_OK;
+}
+
+extern "C" int32_t afsi_b200_mg_batch_persistent(const afsi_mg_plan* const* plans, int32_t count, const void* table,
+                                                 int32_t cycles, int32_t start, void* sync_scratch,
+                                                 afsi_stream_t stream) {
+    int32_t rc = validate_batch(plans, count);
+    if (rc) return rc;
+    AFSI_REQUIRE(table && reinterpret_cast<uintptr_t>(table) % 16 == 0, "device table must be 16-byte aligned");
+    AFSI_REQUIRE(sync_scratch, "null barrier scratch");
+    AFSI_REQUIRE(cycles >= 0, "negative cycle count");
+    AFSI_BATCH_DISPATCH(plans, {
+        return batch_persistent<T, TC>(plans, count, static_cast<const unsigned char*>(table), cycles, start ? 1 : 0,
+                                       sync_scratch, static_cast<cudaStream_t>(stream));
     });
     return AFSI_OK;
 }

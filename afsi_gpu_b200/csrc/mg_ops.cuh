@@ -30,6 +30,76 @@ struct Site {
     double* result;
 };
 
+// Grid barrier of a cooperative launch (every block resident): arrival
+// counter, generation word, error word (a barrier that waits longer than
+// about a second sets it, and every later barrier returns at once), one
+// partial per block and reduction result slots.
+struct GridSync {
+    unsigned int* count;
+    unsigned int* gen;
+    int* error;
+    double* partial;  // one per block
+    double* slot;     // reduction results: [level*3 + {0: p down, 1: p up, 2: rhs}], [kNormSlot]
+};
+
+
+// Barrier with an optional deterministic sum of one double per block
+// (valid in thread 0).  Returns false if any barrier of this launch failed.
+__device__ inline bool grid_sync(const GridSync& g, double v, double* slot) {
+    __shared__ int s_ok;
+    __shared__ bool s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_last = false;
+        const int failed = *reinterpret_cast<volatile int*>(g.error);
+        if (failed) {
+            s_ok = 0;
+        } else {
+            const unsigned my_gen = *reinterpret_cast<volatile unsigned*>(g.gen);
+            if (slot) g.partial[blockIdx.x] = v;
+            __threadfence();
+            const unsigned arrived = atomicAdd(g.count, 1u);
+            if (arrived == gridDim.x - 1) {
+                s_last = true;  // release after the reduction below
+            } else {
+                const long long t0 = clock64();
+                while (*reinterpret_cast<volatile unsigned*>(g.gen) == my_gen) {
+                    if (clock64() - t0 > 2000000000LL) {
+                        atomicOr(g.error, 1);
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
+            s_ok = 1;
+        }
+    }
+    __syncthreads();
+    if (s_last) {
+        if (threadIdx.x < 32) {
+            double t = 0.0;
+            if (slot)
+                for (unsigned i = threadIdx.x; i < gridDim.x; i += 32) t += __ldcg(g.partial + i);
+            t = warp_sum(t);
+            if (threadIdx.x == 0) {
+                if (slot) *slot = t;
+                *g.count = 0u;
+                __threadfence();
+                atomicAdd(g.gen, 1u);
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (*reinterpret_cast<volatile int*>(g.error)) s_ok = 0;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+__device__ __forceinline__ double read_mean(const double* slot, int64_t n) { return __ldcg(slot) / double(n); }
+
 template <int BC, class T>
 __device__ __forceinline__ T diag_at(int x, int y, int z, const Lv<T>& L) {
     T d = T(0);

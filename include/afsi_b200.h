@@ -412,6 +412,15 @@ int32_t afsi_b200_mg_batch_table(const afsi_mg_plan* const* plans, int32_t count
     const void* const* rhs_sources, void* host_table, int64_t bytes);
 int32_t afsi_b200_mg_batch_vcycles(const afsi_mg_plan* const* plans, int32_t count, const void* table,
     int32_t cycles, int32_t start, afsi_stream_t stream);
+/* The same V-cycles in one cooperative launch (one 1024-thread CTA per SM,
+ * grid barriers between the level operations, coarse jobs taken by the CTAs
+ * in turn), bitwise equal to afsi_b200_mg_batch_vcycles.  sync_scratch:
+ * afsi_b200_mg_sync_bytes() zero-initialised device bytes, one per concurrent
+ * run; a barrier that waits longer than about a second sets the int32 error
+ * word at byte offset 8 and the kernel returns; every call first clears the
+ * counter, generation and error words (bytes 0-11). */
+int32_t afsi_b200_mg_batch_persistent(const afsi_mg_plan* const* plans, int32_t count, const void* table,
+    int32_t cycles, int32_t start, void* sync_scratch, afsi_stream_t stream);
 
 /* Iterative refinement of an FP64 pressure solve by FP32 V-cycles (the
  * precision form; no counterpart in the reference, whose solver is FP64

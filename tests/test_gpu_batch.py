@@ -53,7 +53,7 @@ def test_batched_transfers_match_oracle_per_instance(dtype):
                                        atol=tol * np.abs(ref).max())
 
 
-@pytest.mark.parametrize('vcycles', ['streams', 'batched'])
+@pytest.mark.parametrize('vcycles', ['streams', 'batched', 'persistent'])
 def test_batched_cycles_equal_each_instance_alone_and_graph_replay_equals_eager(vcycles):
     b = _small(torch.float32, count=9, vcycles=vcycles)
     sch = b.schedule
@@ -89,7 +89,7 @@ def test_autotuner_picks_a_measured_schedule_meeting_the_target():
     assert (best['streams'], best['order'], best['smoother'], best['cycles']) == \
         (schedule.streams, schedule.order, schedule.smoother, schedule.cycles)
     assert {r['smoother'] for r in table} == {'jacobi', 'red-black'}
-    assert {r['vcycles'] for r in table} == {'streams', 'batched'}
+    assert {r['vcycles'] for r in table} == {'streams', 'batched', 'persistent'}
     b.replay()
     torch.cuda.synchronize()
     assert max(b.residual_reduction()) <= 1e-3
@@ -103,8 +103,9 @@ def test_batch_rejects_points_outside_their_channel():
         b.check()
 
 
+@pytest.mark.parametrize('persistent', [False, True])
 @pytest.mark.parametrize('smooth', [3, 4])
-def test_batched_vcycles_match_each_solver_alone(smooth):
+def test_batched_vcycles_match_each_solver_alone(smooth, persistent):
     """Uneven grids (some wholly in one CTA, some with two launched levels),
     an odd and an even sweep count; a started run then a continued one."""
     from afsi_gpu_b200.batch import BatchedVCycles
@@ -122,9 +123,10 @@ def test_batched_vcycles_match_each_solver_alone(smooth):
     for mg in batch:
         mg.workspace.p[0].fill_(7.)   # the start must zero it
     bv = BatchedVCycles(batch, rhs)
-    bv.run(2)
-    bv.run(1, start=False)
+    bv.run(2, persistent=persistent)
+    bv.run(1, start=False, persistent=persistent)
     torch.cuda.synchronize()
+    bv.check()
     for g, r, mg in zip(grids, rhs, batch):
         alone = solver(g)
         alone.initialize(torch.zeros_like(r), r)
@@ -149,7 +151,13 @@ def test_batched_vcycles_fp64_single_and_coarse_only_batches(shapes):
     batch = [solver(g) for g in grids]
     bv = BatchedVCycles(batch, rhs)
     bv.run(3)
+    again = [solver(g) for g in grids]
+    pv = BatchedVCycles(again, rhs)
+    pv.run(3, persistent=True)
     torch.cuda.synchronize()
+    pv.check()
+    for a, b in zip(batch, again):
+        assert torch.equal(a.workspace.p[0], b.workspace.p[0])
     for g, r, mg in zip(grids, rhs, batch):
         alone = solver(g)
         alone.initialize(torch.zeros_like(r), r)
