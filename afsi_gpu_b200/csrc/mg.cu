@@ -1535,7 +1535,7 @@ __global__ void __launch_bounds__(kBatchPThreads, 1) batch_persistent_kernel(Bat
         const BatchStart<T>* jobs = reinterpret_cast<const BatchStart<T>*>(a.table + a.start_off);
         over(a.blocks_start, reinterpret_cast<const uint32_t*>(a.table + a.start_map_off),
              [&](int ent, int tile) { start_tile(jobs[ent], tile, tid); });
-        ok = grid_sync(a.gs, 0.0, nullptr);
+        ok = grid_barrier(a.gs);
     }
     for (int c = 0; c < a.cycles && ok; ++c) {
         for (int d = 0; d < a.depths && ok; ++d) {
@@ -1543,11 +1543,11 @@ __global__ void __launch_bounds__(kBatchPThreads, 1) batch_persistent_kernel(Bat
             for (int s = 0; s < a.smooth && ok; ++s) {
                 const int zero = (s == 0 && d > 0) ? 1 : 0;
                 over(a.blocks_l[d], ml(d), [&](int ent, int tile) { sweep_tile<BC>(L[ent], tile, tid, s & 1, zero); });
-                ok = grid_sync(a.gs, 0.0, nullptr);
+                ok = grid_barrier(a.gs);
             }
             if (!ok) break;
             over(a.blocks_c[d], mc(d), [&](int ent, int tile) { restrict_tile<BC>(L[ent], tile, tid); });
-            ok = grid_sync(a.gs, 0.0, nullptr);
+            ok = grid_barrier(a.gs);
         }
         if (!ok) break;
         const BatchCoarse<T, TC>* jobs = reinterpret_cast<const BatchCoarse<T, TC>*>(a.table + a.coarse_off);
@@ -1560,20 +1560,20 @@ __global__ void __launch_bounds__(kBatchPThreads, 1) batch_persistent_kernel(Bat
                                     jobs[j].p_out, jobs[j].cinv, cl, a.smooth);
             __syncthreads();
         }
-        ok = grid_sync(a.gs, 0.0, nullptr);
+        ok = grid_barrier(a.gs);
         for (int d = a.depths - 1; d >= 0 && ok; --d) {
             const BatchLevel<T>* L = lv(d);
             over(a.blocks_l[d], ml(d), [&](int ent, int tile) { prolong_tile<BC>(L[ent], tile, tid); });
-            ok = grid_sync(a.gs, 0.0, nullptr);
+            ok = grid_barrier(a.gs);
             for (int s = 0; s < a.smooth && ok; ++s) {
                 over(a.blocks_l[d], ml(d), [&](int ent, int tile) { sweep_tile<BC>(L[ent], tile, tid, s & 1, 0); });
-                ok = grid_sync(a.gs, 0.0, nullptr);
+                ok = grid_barrier(a.gs);
             }
         }
         if (ok && a.depths > 0 && a.smooth % 2 == 1) {
             const BatchLevel<T>* L = lv(0);
             over(a.blocks_l[0], ml(0), [&](int ent, int tile) { finalize_tile(L[ent], tile, tid); });
-            ok = grid_sync(a.gs, 0.0, nullptr);
+            ok = grid_barrier(a.gs);
         }
     }
 }

@@ -100,6 +100,44 @@ __device__ inline bool grid_sync(const GridSync& g, double v, double* slot) {
 
 __device__ __forceinline__ double read_mean(const double* slot, int64_t n) { return __ldcg(slot) / double(n); }
 
+// Grid barrier without a reduction: the block's threads meet at the CTA
+// barrier, then thread 0 arrives with an acquire-release add on the counter;
+// the last block to arrive resets the counter and releases the generation
+// word, the others spin on it with acquire loads (bounded as grid_sync).  The
+// release by thread 0 is cumulative over the writes its CTA barrier ordered
+// before it, so every block's writes are visible to every block afterwards.
+// Returns false if any barrier of the launch failed.
+__device__ inline bool grid_barrier(const GridSync& g) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        unsigned gen0, arrived;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(gen0) : "l"(g.gen) : "memory");
+        asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(g.count) : "memory");
+        if (arrived == gridDim.x - 1) {
+            asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(g.count) : "memory");
+            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(g.gen) : "memory");
+        } else {
+            const long long t0 = clock64();
+            unsigned gen;
+            do {
+                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(gen) : "l"(g.gen) : "memory");
+                if (gen == gen0 && clock64() - t0 > 2000000000LL) {
+                    atomicOr(g.error, 1);
+                    break;
+                }
+            } while (gen == gen0);
+        }
+        int err;
+        asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(err) : "l"(g.error) : "memory");
+        if (err) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
 template <int BC, class T>
 __device__ __forceinline__ T diag_at(int x, int y, int z, const Lv<T>& L) {
     T d = T(0);
