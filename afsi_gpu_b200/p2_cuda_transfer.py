@@ -26,6 +26,19 @@ from ._lib import call, ptr, stream, dtype_code
 from .quadrature import RuleBuilder, InteractionRule
 
 
+@dataclass
+class DeferredStencil:
+    """Tables prepared with the cached rule before the rule was checked
+    (``P2Transfer.prepare_deferred``): ``stencil`` is usable at once;
+    ``P2Transfer.confirm`` settles it."""
+    stencil: 'SharedAdaptiveStencil'
+    x: torch.Tensor
+    orders: torch.Tensor
+    summary: torch.Tensor   # pinned host copy of the order summary and status word
+    ready: torch.cuda.Event
+    buffers: tuple = None
+
+
 @dataclass(frozen=True)
 class SharedAdaptiveStencil:
     base: torch.Tensor   # (2,T,3) int64: lattice 0 = faces, 1 = centres
@@ -92,6 +105,46 @@ class P2Transfer:
             _raise_flags(counts[-1])
             return SharedAdaptiveStencil(*speculative, rule)
         base, phi = prepare(self, x, rule, buffers=buffers)
+        return SharedAdaptiveStencil(base, phi, rule)
+
+    def prepare_deferred(self, x, *, buffers=None):
+        """Rule + tables with no host read (rule selection without host syncs):
+        the order kernel and a prepare with the cached rule are queued, and the
+        order summary with the prepare's status word is copied to pinned host
+        memory behind them.  The returned ``DeferredStencil.stencil`` is used
+        at once; ``confirm`` checks it later, typically after the step's own
+        host read, when the copy has long landed.  The first call has no
+        cached rule and prepares synchronously (already confirmed)."""
+        _lib.require_cuda(x)
+        x = x.contiguous()
+        last = self.rules.last
+        if last is None:
+            st = self.prepare(x, buffers=buffers)
+            return DeferredStencil(st, x, None, None, None, buffers)
+        orders, summary = self.rules.launch(x)
+        base, phi = _tables(x, last.point_count, buffers, self.transfer_dtype)
+        _launch_prepare(self, x, last, base, phi, summary[-1:])
+        host = torch.empty(summary.shape, dtype=summary.dtype, pin_memory=True)
+        host.copy_(summary, non_blocking=True)
+        ready = torch.cuda.Event()
+        ready.record(torch.cuda.current_stream(x.device))
+        return DeferredStencil(SharedAdaptiveStencil(base, phi, last), x, orders, host, ready, buffers)
+
+    def confirm(self, deferred):
+        """Settle a deferred prepare: its stencil when the orders did not
+        change (the common case; no work); a stencil prepared again,
+        synchronously, with the new rule when they did (the caller redoes the
+        transfers that used the old one); ``ValueError`` / ``RuntimeError``
+        for a support or connectivity violation, as ``prepare`` raises them."""
+        if deferred.summary is None:
+            return deferred.stencil
+        deferred.ready.synchronize()
+        counts = deferred.summary.tolist()
+        rule = self.rules.finish(deferred.x, deferred.orders, counts)
+        if rule is deferred.stencil.rule:
+            _raise_flags(counts[-1])
+            return deferred.stencil
+        base, phi = prepare(self, deferred.x, rule, buffers=deferred.buffers)
         return SharedAdaptiveStencil(base, phi, rule)
 
     def spread(self, coefficient, stencil):

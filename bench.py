@@ -143,20 +143,29 @@ class Step:
         ev = timing
         if ev is not None:
             ev[0].record()
-        st = self.tr.prepare(self.x if x is None else x)
+        # rule selection without a host read: the prepare runs with the cached
+        # rule and is confirmed after the solve's own host read; a changed rule
+        # (never on this workload) redoes the transfers
+        deferred = self.tr.prepare_deferred(self.x if x is None else x)
+        st = deferred.stencil
         if ev is not None:
             ev[1].record()
-        fields = self.p2t.spread(self.tr, self.coef if coef is None else coef, st,
-                                 events=None if ev is None else ev[5:7])
+        coef = self.coef if coef is None else coef
+        vel = self.vel if vel is None else vel
+        fields = self.p2t.spread(self.tr, coef, st, events=None if ev is None else ev[5:7])
         if ev is not None:
             ev[2].record()
-        nodal = self.p2t.assemble_velocity(self.tr, self.vel if vel is None else vel, st,
-                                           events=None if ev is None else ev[7:9])
+        nodal = self.p2t.assemble_velocity(self.tr, vel, st, events=None if ev is None else ev[7:9])
         if ev is not None:
             ev[3].record()
         p, info = self.mg.solve(self.rhs if rhs is None else rhs)
         if ev is not None:
             ev[4].record()
+        confirmed = self.tr.confirm(deferred)
+        if confirmed is not st:
+            st = confirmed
+            fields = self.p2t.spread(self.tr, coef, st)
+            nodal = self.p2t.assemble_velocity(self.tr, vel, st)
         self.cycles.append(info['cycles'])
         return st, fields, nodal, p
 

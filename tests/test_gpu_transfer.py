@@ -382,6 +382,36 @@ def test_p2_orders_flag_bad_connectivity_and_nonfinite_nodes():
     assert summary[2] == _lib.FLAG_SUPPORT and orders[9].item() == 0
 
 
+def test_p2_deferred_prepare_confirms_the_rule_after_the_fact():
+    """prepare_deferred reads nothing on the host: unchanged orders give the
+    speculative tables bitwise equal to a synchronous prepare and confirm
+    returns them as they are; changed orders make confirm prepare again with
+    the new rule (equal to a synchronous prepare); a support violation is
+    raised at confirm."""
+    X, cells = synthetic.p2_shell(2, 12, 16, **SMALL)
+    grid = MACGrid((32, 32, 32), (1., 1., 1.))
+    tr = p2t.P2Transfer(grid, t(X), t(cells), max_order=22)
+    ref = p2t.P2Transfer(grid, t(X), t(cells), max_order=22)
+    first = tr.prepare_deferred(t(X))  # no cached rule yet: synchronous
+    assert tr.confirm(first) is first.stencil
+    second = tr.prepare_deferred(t(X))
+    sync = ref.prepare(t(X))
+    assert torch.equal(second.stencil.base, sync.base) and torch.equal(second.stencil.phi, sync.phi)
+    assert tr.confirm(second) is second.stencil
+    centre = X.mean(0)
+    Y = centre + 1.3 * (X - centre)  # larger elements: higher orders
+    third = tr.prepare_deferred(t(Y))
+    assert third.stencil.rule is second.stencil.rule  # speculative, with the old rule
+    fixed = tr.confirm(third)
+    assert fixed.rule is not second.stencil.rule
+    again = ref.prepare(t(Y))
+    assert fixed.rule.point_count == again.rule.point_count
+    assert torch.equal(fixed.base, again.base) and torch.equal(fixed.phi, again.phi)
+    bad = tr.prepare_deferred(t(Y) - .45)  # a translation keeps the orders
+    with pytest.raises(ValueError, match='support'):
+        tr.confirm(bad)
+
+
 def test_p2_transfer_prepare_reuses_the_rule_and_rebuilds_on_change():
     X, cells = synthetic.p2_shell(2, 12, 16, **SMALL)
     grid = MACGrid((32, 32, 32), (1., 1., 1.))
