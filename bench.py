@@ -618,6 +618,20 @@ def _json(o):
     raise TypeError(type(o))
 
 
+def max_over_ranks(value, dist, device):
+    """The largest `value` over the ranks: a multi-GPU time is its slowest rank's."""
+    if not dist:
+        return value
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.item()
+
+
+def whole_job_rate(world, steps, elapsed):
+    """Steps per second of the whole job: every replica ran `steps` steps."""
+    return world * steps / elapsed
+
+
 def dist_setup(args):
     if args.gpus > 1 or 'RANK' in os.environ:
         import torch.distributed as dist
@@ -751,11 +765,7 @@ def run_b200(args):
         stop.record(stream)
         barrier()
     launches = _lib.launch_count() - launches0
-    elapsed = start.elapsed_time(stop) / 1e3
-    if dist:
-        t = torch.tensor([elapsed], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = t.item()
+    elapsed = max_over_ranks(start.elapsed_time(stop) / 1e3, dist, device)
     names = ('prepare', 'spread', 'gather_assemble', 'mg_solve')
     phase_ms = {n: float(np.mean([ev[i].elapsed_time(ev[i + 1]) for ev in phases])) for i, n in enumerate(names)}
     spread_t = float(np.mean([ev[5].elapsed_time(ev[6]) for ev in phases])) / 1e3
@@ -825,11 +835,7 @@ def run_b200(args):
     final = outs[(e2e_steps - 1) % 2]  # the last step's pinned results
     e1.record(stream)
     barrier()
-    e2e_elapsed = e0.elapsed_time(e1) / 1e3
-    if dist:
-        t = torch.tensor([e2e_elapsed], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_elapsed = t.item()
+    e2e_elapsed = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, device)
 
     if rank == 0:
         pk, pk_kind = peaks()
@@ -859,7 +865,7 @@ def run_b200(args):
         serving = serving_form_row(device) if extra else None
         step_ms = np.array([ev[0].elapsed_time(ev[4]) for ev in phases])
         line = dict(
-            metric=METRIC, value=world * args.steps / elapsed, unit='steps/s', n_gpus=world, steps=args.steps,
+            metric=METRIC, value=whole_job_rate(world, args.steps, elapsed), unit='steps/s', n_gpus=world, steps=args.steps,
             warmup=args.warmup, ms_per_step=elapsed / args.steps * 1e3, higher_is_better=True, scaling='weak',
             vs_baseline=None, dtype='f64', data='synthetic',
             config=dict(workload='3D P2 shell 38400 elements / 2457600 points, 64^3 MAC, FP64',
@@ -873,7 +879,7 @@ def run_b200(args):
                           traffic=(traffic * 1.0 if traffic else None),
                           algorithmic_bytes=ab[byte_key], launch_ms=dt * 1e3,
                           phases_ms=phase_ms),
-            e2e=dict(value=world * e2e_steps / e2e_elapsed, unit='steps/s', h2d_bytes_per_step=int(h2d),
+            e2e=dict(value=whole_job_rate(world, e2e_steps, e2e_elapsed), unit='steps/s', h2d_bytes_per_step=int(h2d),
                      d2h_bytes_per_step=int(d2h)),
             gpu_launches=int(launches),
             clocks=clocks.summary(),
