@@ -2,7 +2,7 @@
 
 Tolerances: integer tables (bases, stencil ids) bit-exact; FP64 weights within
 rounding of the reference torch path (its CPU sqrt is not correctly rounded);
-FP64 spread/gather 1e-12 relative (north-star parity bar); FP32 8e-5/3e-5
+FP64 spread/gather 1e-12 relative (the FP64 parity bar); FP32 8e-5/3e-5
 (``tests/test_p2_cuda_execution.py:38`` of the reference).
 """
 import numpy as np
