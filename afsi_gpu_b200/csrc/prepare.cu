@@ -76,53 +76,80 @@ struct Prepare2dParams {
 };
 
 // Reflected 4x4 stencils of u (faces (nx+1,ny)) and v (faces (nx,ny+1)),
-// mac2d/transfer.py:61-81.  Offsets k=i*4+j, j (y) fastest.
+// mac2d/transfer.py:61-81.  Offsets k=i*4+j, j (y) fastest.  One thread per
+// point; a warp's 32 points own 32 consecutive rows of 16 ids and 16 weights
+// per component, so each warp stages its rows in shared memory and writes
+// them as one contiguous run (coalesced stores).
+constexpr int kPrep2dThreads = 256;
+constexpr int kPrep2dRow = 17;  // int64 words per staged row (16 taps + 1 pad against bank conflicts)
+
 template <class T>
-__global__ void __launch_bounds__(256) prepare2d_kernel(const T* __restrict__ points, int64_t count,
-                                                        Prepare2dParams<T> prm, int64_t* __restrict__ ids,
-                                                        T* __restrict__ weights, int32_t* status) {
-    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (p >= count) return;
-    const T px = points[p * 2], py = points[p * 2 + 1];
-    const bool valid = isfinite(px) && isfinite(py) && px >= prm.xmin && px <= prm.xmax &&
-                       py >= prm.ymin && py <= prm.ymax;
-    if (!valid) flag(status, AFSI_FLAG_SUPPORT);
+__global__ void __launch_bounds__(kPrep2dThreads) prepare2d_kernel(const T* __restrict__ points, int64_t count,
+                                                                   Prepare2dParams<T> prm, int64_t* __restrict__ ids,
+                                                                   T* __restrict__ weights, int32_t* status) {
+    __shared__ int64_t s_rows[kPrep2dThreads / 32][32 * kPrep2dRow];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t p0 = int64_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31);
+    if (p0 >= count) return;  // whole warp
+    const int n_valid = count - p0 < 32 ? int(count - p0) : 32;
+    const int64_t p = p0 + lane;
+    const bool live = lane < n_valid;
+    int64_t* row = s_rows[warp] + lane * kPrep2dRow;
+    T* wrow = reinterpret_cast<T*>(s_rows[warp]) + lane * kPrep2dRow;
+    T px = T(0), py = T(0);
+    if (live) {
+        px = points[p * 2];
+        py = points[p * 2 + 1];
+        const bool valid = isfinite(px) && isfinite(py) && px >= prm.xmin && px <= prm.xmax && py >= prm.ymin &&
+                           py <= prm.ymax;
+        if (!valid) flag(status, AFSI_FLAG_SUPPORT);
+    }
     const int64_t ny = prm.ny;
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
-        const T ox = prm.hx * (c == 0 ? T(0) : T(.5));
-        const T oy = prm.hy * (c == 1 ? T(0) : T(.5));
-        const T sx = (px - ox) / prm.hx, sy = (py - oy) / prm.hy;
-        const int64_t bx = static_cast<int64_t>(floor(sx - T(1)));
-        const int64_t by = static_cast<int64_t>(floor(sy - T(1)));
-        const int64_t face_ny = ny + (c == 1);
         T wx[4], wy[4];
+        int64_t by = 0;
+        if (live) {
+            const T ox = prm.hx * (c == 0 ? T(0) : T(.5));
+            const T oy = prm.hy * (c == 1 ? T(0) : T(.5));
+            const T sx = (px - ox) / prm.hx, sy = (py - oy) / prm.hy;
+            const int64_t bx = static_cast<int64_t>(floor(sx - T(1)));
+            by = static_cast<int64_t>(floor(sy - T(1)));
+            const int64_t face_ny = ny + (c == 1);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            wx[k] = peskin_clamped(sx - T(bx + k));
-            wy[k] = peskin_clamped(sy - T(by + k));
-        }
-        int64_t* out_ids = ids + (c * count + p) * 16;
-        T* out_w = weights + (c * count + p) * 16;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int64_t y = by + j;
-                bool outside;
-                int64_t r;
-                if (c == 0) {
-                    outside = y < 0 || y >= ny;
-                    r = y < 0 ? -y - 1 : (y >= ny ? 2 * ny - y - 1 : y);
-                } else {
-                    outside = y < 0 || y > ny;
-                    r = y < 0 ? -y : (y > ny ? 2 * ny - y : y);
-                }
-                const T w = wx[i] * wy[j];
-                out_ids[i * 4 + j] = (bx + i) * face_ny + r;
-                out_w[i * 4 + j] = outside ? -w : w;
+            for (int k = 0; k < 4; ++k) {
+                wx[k] = peskin_clamped(sx - T(bx + k));
+                wy[k] = peskin_clamped(sy - T(by + k));
             }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int64_t y = by + j;
+                    const int64_t r = c == 0 ? (y < 0 ? -y - 1 : (y >= ny ? 2 * ny - y - 1 : y))
+                                             : (y < 0 ? -y : (y > ny ? 2 * ny - y : y));
+                    row[i * 4 + j] = (bx + i) * face_ny + r;
+                }
         }
+        __syncwarp();
+        const int64_t out0 = (c * count + p0) * 16;
+        for (int k = lane; k < 16 * n_valid; k += 32) ids[out0 + k] = s_rows[warp][(k >> 4) * kPrep2dRow + (k & 15)];
+        __syncwarp();
+        if (live) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int64_t y = by + j;
+                    const bool outside = c == 0 ? (y < 0 || y >= ny) : (y < 0 || y > ny);
+                    const T w = wx[i] * wy[j];
+                    wrow[i * 4 + j] = outside ? -w : w;
+                }
+        }
+        __syncwarp();
+        const T* sw = reinterpret_cast<const T*>(s_rows[warp]);
+        for (int k = lane; k < 16 * n_valid; k += 32) weights[out0 + k] = sw[(k >> 4) * kPrep2dRow + (k & 15)];
+        __syncwarp();
     }
 }
 
@@ -356,7 +383,7 @@ extern "C" int32_t afsi_b200_indexed_prepare2d(const void* points, int64_t count
         prm.ymin = T(-hy);
         prm.ymax = T(ly + hy);
         prm.ny = ny;
-        prepare2d_kernel<T><<<blocks_for(count, 256), 256, 0, stream>>>(
+        prepare2d_kernel<T><<<blocks_for(count, kPrep2dThreads), kPrep2dThreads, 0, stream>>>(
             static_cast<const T*>(points), count, prm, ids, static_cast<T*>(weights), status);
     });
     return launched("indexed_prepare2d");
