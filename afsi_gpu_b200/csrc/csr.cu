@@ -130,9 +130,13 @@ __global__ void __launch_bounds__(kCellWarps * 32) contract_kernel(const int64_t
         int64_t node[4];
 #pragma unroll
         for (int a = 0; a < 4; ++a) node[a] = cells[e * 4 + a];
+        // site -> (sx, sy, sz), z fastest, advanced by mixed-radix addition of
+        // 32 per batch (32-bit; the box extents are at most kFar)
+        const int iwz = int(wz), iwy = int(wy);
+        const int qz = 32 % iwz, qq = 32 / iwz, qy = qq % iwy, qx = qq / iwy;
+        int sz = lane % iwz, sy = (lane / iwz) % iwy, sx = (lane / iwz) / iwy;
         for (int64_t t0 = 0; t0 < sites; t0 += 32) {
             const int64_t site = t0 + lane;
-            const int sz = int(site % wz), sy = int((site / wz) % wy), sx = int(site / (wy * wz));
             T sums[4] = {T(0), T(0), T(0), T(0)};
             for (int64_t q0 = 0; q0 < g.nq; q0 += 32) {
                 const int nj = int(g.nq - q0 < 32 ? g.nq - q0 : 32);
@@ -175,6 +179,13 @@ __global__ void __launch_bounds__(kCellWarps * 32) contract_kernel(const int64_t
                     for (int a = 0; a < 4; ++a) table_add<T, Cached>(node[a] * g.nf + face, sums[a], t);
                 }
             }
+            sz += qz;
+            int carry = sz >= iwz ? 1 : 0;
+            sz -= carry * iwz;
+            sy += qy + carry;
+            carry = sy >= iwy ? 1 : 0;
+            sy -= carry * iwy;
+            sx += qx + carry;
         }
     }
 }
