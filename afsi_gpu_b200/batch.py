@@ -14,9 +14,11 @@ step:
 * a fixed number of V-cycles per instance on its own FP32 workspace (FP64
   coarsest solve), either batched (``vcycles='batched'``, Jacobi: one launch
   per level operation for all instances and one launch for all their
-  single-CTA coarse levels, ``afsi_b200_mg_batch_vcycles``) or per instance
-  with the instances spread over ``streams`` capture streams so that their
-  small level kernels overlap on the device;
+  single-CTA coarse levels, ``afsi_b200_mg_batch_vcycles``), the same in one
+  persistent cooperative launch (``vcycles='persistent'``,
+  ``afsi_b200_mg_batch_persistent``), or per instance with the instances
+  spread over ``streams`` capture streams so that their small level kernels
+  overlap on the device;
 * the whole step captured once as a CUDA graph and replayed.
 
 ``autotune()`` chooses the schedule (batched or per-instance V-cycles, stream
@@ -79,6 +81,9 @@ class BatchedVCycles:
         lib = _lib.load()
         self.solvers = list(solvers)
         self.count = len(self.solvers)
+        device = self.solvers[0].workspace.p[0].device
+        if any(mg.workspace.p[0].device != device for mg in self.solvers):
+            raise ValueError('batched V-cycles need every solver on one device')
         plans = [mg.workspace.plan for mg in self.solvers]
         self._plans = (ctypes.POINTER(_lib.MGPlan) * self.count)(*[ctypes.pointer(p) for p in plans])
         self._sources = None
@@ -96,7 +101,6 @@ class BatchedVCycles:
             raise ValueError(f'batched V-cycles: {lib.afsi_b200_last_error().decode(errors="replace")}')
         host = np.zeros(int(nbytes), np.uint8)
         call('afsi_b200_mg_batch_table', self._plans, self.count, self._sources, host.ctypes.data, int(nbytes))
-        device = self.solvers[0].workspace.p[0].device
         self.table = torch.as_tensor(host).to(device)
         self.sync = torch.zeros(int(lib.afsi_b200_mg_sync_bytes()), dtype=torch.uint8, device=device)
 
