@@ -42,9 +42,10 @@ def parse():
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='b200', choices=('b200', 'reference'))
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--rows', default='all', choices=('all', 'step'),
+    ap.add_argument('--rows', default='all', choices=('all', 'step', 'p1'),
                     help="'step': the headline step line only, without the mass-solve, MG-form, batching and "
-                         "serving rows (for profiler runs)")
+                         "serving rows (for profiler runs); 'p1': only the precision-form row on the 128^3 P1 "
+                         "configuration, printed as its own JSON object (for profiler runs)")
     return ap.parse_args()
 
 
@@ -906,6 +907,8 @@ def main():
     args = parse()
     if args.impl == 'reference':
         run_reference(args)
+    elif args.rows == 'p1':
+        print(json.dumps(precision_p1_row(torch.device('cuda', torch.cuda.current_device())), default=_json))
     else:
         run_b200(args)
 
