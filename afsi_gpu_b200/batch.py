@@ -361,41 +361,3 @@ def seeded_batch(count=64, *, seed=0, shapes=((128, 32), (256, 64), (384, 96), (
         r = rng.standard_normal((nx, ny))
         rhs.append(r - r.mean())
     return BatchedChannels(grids, pts, forces, vels, rhs, device=device, **kwargs)
-
-
-def main(argv=None):
-    """Time graph replays of the seeded batch under one schedule:
-    ``python -m afsi_gpu_b200.batch --instances 64 --vcycles batched``."""
-    import argparse
-    ap = argparse.ArgumentParser(description=main.__doc__)
-    ap.add_argument('--instances', type=int, default=64)
-    ap.add_argument('--seed', type=int, default=0)
-    ap.add_argument('--vcycles', choices=('batched', 'persistent', 'streams'), default='batched')
-    ap.add_argument('--smoother', choices=('jacobi', 'red-black'), default='jacobi')
-    ap.add_argument('--streams', type=int, default=16)
-    ap.add_argument('--cycles', type=int, default=4)
-    ap.add_argument('--warmup', type=int, default=3)
-    ap.add_argument('--replays', type=int, default=20)
-    args = ap.parse_args(argv)
-    dev = torch.device('cuda')
-    b = seeded_batch(args.instances, seed=args.seed, device=dev)
-    b.use(Schedule(streams=args.streams, order='largest-first', smoother=args.smoother, cycles=args.cycles,
-                   vcycles=args.vcycles))
-    for _ in range(args.warmup):
-        b.replay()
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.replays):
-        b.replay()
-    e1.record()
-    torch.cuda.synchronize(dev)
-    b.check()
-    ms = e0.elapsed_time(e1) / args.replays
-    print(f'{args.instances} instances, {b.total} points: {ms:.3f} ms per batch step, '
-          f'{args.instances / ms * 1e3:.0f} instance-steps/s, {b.graph_launches} launches per step, '
-          f'max residual reduction {max(b.residual_reduction()):.2e}')
-
-
-if __name__ == '__main__':
-    main()

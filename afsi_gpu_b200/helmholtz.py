@@ -5,10 +5,9 @@
 ``mac/helmholtz.py:44-47``): ``initialize(b, p, diagonal, rhs, u, parameters,
 grid)`` and ``sweep(u, rhs, diagonal, out, parameters, grid)`` with the same
 arguments, each one launch over the three face lattices.
-``HelmholtzWorkspace`` keeps the reference workspace's contract
-(``mac/helmholtz.py:31-121``): a fixed count of sweeps from the diagonal
-initial guess, optionally replayed from a captured CUDA graph (bounded LRU of
-four counts), owned results.
+``HelmholtzSolver`` runs a fixed-count solve (initialize plus sweeps) as one
+captured graph over staged inputs; the reference's own ``HelmholtzWorkspace``
+runs on ``HelmholtzKernels`` after ``dropin.install()``.
 
 The Stokes functions keep the signatures of ``mac/_triton_stokes.py``
 (``start_partial``, ``residual_partial``, ``pressure_input_partial``,
@@ -17,7 +16,6 @@ buffer, reduced by the caller (``mac/stokes_workspace.py``).
 
 CUDA only: CPU tensors are rejected.
 """
-from collections import OrderedDict
 import torch
 from . import _lib
 from ._lib import call, ptr, stream, dtype_code, pointers, int64s, doubles
@@ -49,89 +47,105 @@ class HelmholtzKernels:
              stream(u[0].device))
 
 
-class HelmholtzWorkspace:
-    """``mac/helmholtz.py:31-121`` on the B200 kernels: backend 'graph'
-    (captured sweep chains, the reference default) or 'b200' (launched)."""
+class HelmholtzSolver:
+    """Fixed-count CN Helmholtz solve on the B200 kernels.
 
-    def __init__(self, grid, diagonal, *, backend='graph', kernels=None):
-        backend = {'triton': 'b200'}.get(backend, backend)
-        if backend not in ('b200', 'graph'):
-            raise ValueError('invalid Helmholtz workspace backend')
-        _check_faces(diagonal, 'Helmholtz workspace')
-        self.grid, self.diagonal, self.backend = grid, diagonal, backend
-        self.rhs, self.first, self.second = [tuple(torch.empty_like(d) for d in diagonal) for _ in range(3)]
-        self.parameters = diagonal[0].new_zeros(2)
-        self._parameter_values = None
+    Solves (I - alpha L) u = b - pressure_scale * G p approximately, the way
+    the reference's CN flow does (``mac/cnab.py:176-192``): the initial guess
+    rhs/diagonal, then `count` Jacobi sweeps, wall-normal faces held at zero.
+
+    The design is this package's own.  `alpha` and `count` are fixed for the
+    solver's life (a CN flow changes them only with its time step).  The
+    right-hand side and the pressure are staged into the solver's own input
+    buffers (``inputs``), so with ``graph=True`` the whole chain (the
+    initialize launch and every sweep) is one CUDA graph per pressure mode,
+    captured on first use and replayed afterwards; ``graph=False`` launches
+    the same kernels.  A caller that fills ``inputs`` itself passes
+    ``staged=True`` and skips the copies.  Results are returned as fresh
+    tensors unless ``out`` is given.  One solver serves one stream at a time.
+    """
+
+    def __init__(self, grid, diagonal, alpha, count, *, graph=True, kernels=None):
+        if type(count) is not int or count < 1:
+            raise ValueError('the Helmholtz sweep count must be a positive integer')
+        diagonal = tuple(diagonal)
+        _check_faces(diagonal, 'Helmholtz solver')
+        grid.check_velocity(diagonal)
+        ref = diagonal[0]
+        self.grid, self.diagonal, self.count, self.alpha = grid, diagonal, count, float(alpha)
         self.kernels = kernels or HelmholtzKernels()
-        self.graphs = OrderedDict()
-        self._stream = None
-        self.solves = self.sweeps = self.graph_builds = 0
+        self.use_graph = bool(graph)
+        faces = lambda: tuple(torch.zeros_like(d) for d in diagonal)
+        self.inputs = faces()
+        self.pressure = torch.zeros(grid.shape, device=ref.device, dtype=ref.dtype)
+        self._rhs, self._ping, self._pong = faces(), faces(), faces()
+        self._param = torch.tensor([self.alpha, 0.], device=ref.device, dtype=ref.dtype)
+        self._scale = 0.
+        self._graphs = {}
+        self._launches = {}
+        self.calls = 0
 
-    def _block(self, count):
-        u, out = self.first, self.second
-        for _ in range(count):
-            self.kernels.sweep(u, self.rhs, self.diagonal, out, self.parameters, self.grid)
-            u, out = out, u
-        return u
+    @property
+    def result(self):
+        """The buffer the last sweep writes (ping after an even count)."""
+        return self._ping if self.count % 2 == 0 else self._pong
 
-    def _capture(self, count):
-        if len(self.graphs) >= 4:
-            self.graphs.popitem(last=False)
-        dev = self.parameters.device
-        with torch.cuda.device(dev):
-            s = torch.cuda.Stream(device=dev)
-            s.wait_stream(torch.cuda.current_stream(dev))
-            g = torch.cuda.CUDAGraph()
-            before = _lib.launch_count()
-            with torch.cuda.graph(g, stream=s):
-                self._block(count)
-            self.graph_launches = _lib.launch_count() - before
-            _lib.forget_launches(self.graph_launches)
-            torch.cuda.current_stream(dev).wait_stream(s)
-        self.graphs[count] = g
-        self.graph_builds += 1
+    def _chain(self, with_pressure):
+        self.kernels.initialize(self.inputs, self.pressure if with_pressure else None, self.diagonal, self._rhs,
+                                self._ping, self._param, self.grid)
+        src, dst = self._ping, self._pong
+        for _ in range(self.count):
+            self.kernels.sweep(src, self._rhs, self.diagonal, dst, self._param, self.grid)
+            src, dst = dst, src
+
+    def _graph(self, with_pressure):
+        if with_pressure not in self._graphs:
+            dev = self._param.device
+            with torch.cuda.device(dev):
+                side = torch.cuda.Stream(device=dev)
+                side.wait_stream(torch.cuda.current_stream(dev))
+                g = torch.cuda.CUDAGraph()
+                before = _lib.launch_count()
+                with torch.cuda.graph(g, stream=side):
+                    self._chain(with_pressure)
+                self._launches[with_pressure] = _lib.launch_count() - before
+                _lib.forget_launches(self._launches[with_pressure])
+                torch.cuda.current_stream(dev).wait_stream(side)
+            self._graphs[with_pressure] = g
+        return self._graphs[with_pressure]
 
     @torch.no_grad()
-    def solve(self, b, *, alpha, count, pressure=None, pressure_scale=0., owned=True):
-        self.grid.check_velocity(b)
-        if type(count) is not int or count < 1:
-            raise ValueError('positive fixed Helmholtz iteration count required')
-        if any(v.device != self.parameters.device or v.dtype != self.parameters.dtype for v in b):
-            raise ValueError('Helmholtz workspace dtype/device mismatch')
-        if pressure is not None and (pressure.shape != self.grid.shape or pressure.device != self.parameters.device
-                                     or pressure.dtype != self.parameters.dtype):
-            raise ValueError('Helmholtz pressure shape/device/dtype mismatch')
-        s = torch.cuda.current_stream(self.parameters.device).cuda_stream
-        if self._stream is not None and self._stream != s:
-            raise ValueError('Helmholtz workspace requires its original CUDA stream')
-        self._stream = s
-        with torch.cuda.device(self.parameters.device):
-            parameters = float(alpha), float(pressure_scale)
-            if parameters != self._parameter_values:
-                self.parameters[0].fill_(alpha)
-                self.parameters[1].fill_(pressure_scale)
-                self._parameter_values = parameters
-            b = tuple(v.contiguous() for v in b)
-            pressure = None if pressure is None else pressure.contiguous()
-            if self.backend == 'graph' and count not in self.graphs:
-                self._capture(count)
-            self.kernels.initialize(b, pressure, self.diagonal, self.rhs, self.first, self.parameters, self.grid)
-            if self.backend == 'graph':
-                self.graphs.move_to_end(count)
-                self.graphs[count].replay()
-                _lib.count_replay(self.graph_launches)
-                result = self.second if count % 2 else self.first
-            else:
-                result = self._block(count)
-            self.solves += 1
-            self.sweeps += count
-            return tuple(v.clone() for v in result) if owned else result
-
-    def summary(self):
-        return dict(backend=self.backend, solves=self.solves, sweeps=self.sweeps, graph_builds=self.graph_builds,
-                    cached_graphs=len(self.graphs),
-                    buffer_bytes=sum(v.numel() * v.element_size() for group in (self.rhs, self.first, self.second)
-                                     for v in group))
+    def solve(self, b=None, pressure=None, pressure_scale=0., *, staged=False, out=None):
+        """u for right-hand side `b` (face arrays) and, optionally, the pressure
+        term; with staged=True, `b` and `pressure` were written into
+        ``inputs`` / ``pressure`` already (pass pressure=True to use it)."""
+        with_pressure = pressure is not None and pressure is not False
+        if not staged:
+            self.grid.check_velocity(b)
+            ref = self.inputs[0]
+            if b[0].dtype != ref.dtype or b[0].device != ref.device:
+                raise ValueError('Helmholtz right-hand side dtype/device differs from the solver\'s')
+            for dst, src in zip(self.inputs, b):
+                dst.copy_(src)
+            if with_pressure:
+                if tuple(pressure.shape) != tuple(self.grid.shape) or pressure.dtype != ref.dtype:
+                    raise ValueError('Helmholtz pressure shape/dtype mismatch')
+                self.pressure.copy_(pressure)
+        if with_pressure and float(pressure_scale) != self._scale:
+            self._scale = float(pressure_scale)
+            self._param[1].fill_(self._scale)
+        if self.use_graph:
+            self._graph(with_pressure).replay()
+            _lib.count_replay(self._launches[with_pressure])
+        else:
+            self._chain(with_pressure)
+        self.calls += 1
+        res = self.result
+        if out is None:
+            return tuple(v.clone() for v in res)
+        for o, v in zip(out, res):
+            o.copy_(v)
+        return out
 
 
 # ------------------------------------------------------------------ Stokes

@@ -3,17 +3,21 @@
 Run from the repository root in a container where the reference source tree is
 available (it is not needed afterwards; the fixtures are committed):
 
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py [REFERENCE_SRC]
+    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py REFERENCE_SRC
 
-REFERENCE_SRC defaults to ``/root/reference/src``.  Every fixture is produced by
+REFERENCE_SRC is the reference's ``src`` directory (the argument, or the
+``AFSI_TORCH_SRC`` environment variable when no argument is given).  Every fixture is produced by
 the reference's own public functions or the CPU expressions its classes use;
 inputs are seeded.  Outputs are small ``.npz`` files next to this script.
 """
+import os
 import sys
 from pathlib import Path
 import numpy as np
 
-SRC = sys.argv[1] if len(sys.argv) > 1 else '/root/reference/src'
+SRC = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('AFSI_TORCH_SRC')
+if not SRC:
+    sys.exit('usage: make_golden.py REFERENCE_SRC  (or set AFSI_TORCH_SRC)')
 sys.path.insert(0, SRC)
 import torch  # noqa: E402
 from afsi_torch import ib  # noqa: E402

@@ -3,13 +3,14 @@ import os
 import sys
 import pytest
 
-REF = os.environ.get('AFSI_TORCH_SRC', '/root/reference/src')
+# the reference's src directory; the tests skip when it is not given
+REF = os.environ.get('AFSI_TORCH_SRC', '')
 
 
 @pytest.fixture
 def afsi_torch():
-    if not os.path.isdir(os.path.join(REF, 'afsi_torch')):
-        pytest.skip('afsi-torch source not available')
+    if not REF or not os.path.isdir(os.path.join(REF, 'afsi_torch')):
+        pytest.skip('afsi-torch source not available (set AFSI_TORCH_SRC)')
     sys.path.insert(0, REF)
     try:
         import afsi_torch.mac.cuda_ib  # noqa: F401

@@ -13,7 +13,7 @@ import torch
 from conftest import golden
 from oracle import stokes as ostokes
 from afsi_gpu_b200.grid import MACGrid
-from afsi_gpu_b200.helmholtz import (HelmholtzKernels, HelmholtzWorkspace, pressure_input_partial,
+from afsi_gpu_b200.helmholtz import (HelmholtzKernels, HelmholtzSolver, pressure_input_partial,
                                      pressure_norm_partial, residual_partial, start_partial)
 
 pytestmark = pytest.mark.gpu
@@ -58,21 +58,30 @@ def test_helmholtz_kernels_match_reference(dtype):
                                            atol=2e-6 * np.abs(ref).max())
 
 
-@pytest.mark.parametrize('backend', ['graph', 'b200'])
-def test_helmholtz_workspace_solves_match_reference(backend):
+@pytest.mark.parametrize('graph', [True, False])
+def test_helmholtz_solver_matches_reference(graph):
+    """Initialize + 3 sweeps through the solver (one captured graph per
+    pressure mode, or launched) equal the reference kernel object's chain."""
     g, grid, t, faces = _case()
-    ws = HelmholtzWorkspace(grid, faces('d'), backend=backend)
+    hs = HelmholtzSolver(grid, faces('d'), float(g['alpha']), 3, graph=graph)
     for _ in range(2):  # capture on the first solve, replay on the second
-        u = ws.solve(faces('b'), alpha=float(g['alpha']), count=3, pressure=t(g['p']),
-                     pressure_scale=float(g['scale']))
+        u = hs.solve(faces('b'), t(g['p']), float(g['scale']))
         for c in range(3):
             assert np.array_equal(u[c].cpu().numpy(), g[f'p_sweep3_{c}'])
-    u = ws.solve(faces('b'), alpha=float(g['alpha']), count=3)
+    u = hs.solve(faces('b'))
     for c in range(3):
         assert np.array_equal(u[c].cpu().numpy(), g[f'nop_sweep3_{c}'])
-    assert ws.summary()['solves'] == 3
-    with pytest.raises(ValueError, match='positive fixed Helmholtz iteration count'):
-        ws.solve(faces('b'), alpha=.1, count=0)
+    # staged inputs and a caller-owned output
+    for dst, src in zip(hs.inputs, faces('b')):
+        dst.copy_(src)
+    hs.pressure.copy_(t(g['p']))
+    out = tuple(torch.empty_like(v) for v in u)
+    hs.solve(pressure=True, pressure_scale=float(g['scale']), staged=True, out=out)
+    for c in range(3):
+        assert np.array_equal(out[c].cpu().numpy(), g[f'p_sweep3_{c}'])
+    assert hs.calls == 4
+    with pytest.raises(ValueError, match='sweep count'):
+        HelmholtzSolver(grid, faces('d'), .1, 0)
 
 
 def test_stokes_partials_reduce_to_reference_metrics():
@@ -118,8 +127,7 @@ def test_helmholtz_on_a_64_cube_against_the_oracle():
     rhs_ref, u_ref = ostokes.helmholtz_initialize(b, p, d, .3, grid.spacing)
     for _ in range(4):
         u_ref = ostokes.helmholtz_sweep(u_ref, rhs_ref, d, .02, grid.spacing)
-    ws = HelmholtzWorkspace(grid, tuple(torch.as_tensor(x, device=DEV) for x in d))
-    u = ws.solve(tuple(torch.as_tensor(x, device=DEV) for x in b), alpha=.02, count=4,
-                 pressure=torch.as_tensor(p, device=DEV), pressure_scale=.3)
+    hs = HelmholtzSolver(grid, tuple(torch.as_tensor(x, device=DEV) for x in d), .02, 4)
+    u = hs.solve(tuple(torch.as_tensor(x, device=DEV) for x in b), torch.as_tensor(p, device=DEV), .3)
     for c in range(3):
         assert np.array_equal(u[c].cpu().numpy(), u_ref[c])

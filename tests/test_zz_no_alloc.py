@@ -1,9 +1,10 @@
 """The no-allocation residual norm agrees with the scratch-using one (B200).
 
 ``afsi_b200_mg_residual_norm_noalloc`` exists for callers that cannot allocate
-device memory when they need a residual norm: code that runs while a CUDA graph
-is being captured, host applications that hand the library only their own
-preallocated buffers, or embeddings without a caching allocator.  It keeps its
+device memory when they need a residual norm: host applications that hand the
+library only their own preallocated buffers, embeddings without a caching
+allocator, or code that cannot afford the device synchronisation of a
+cudaMalloc.  It keeps its
 reduction scratch in a fixed device array inside the library instead of in
 caller-provided memory.  This file is collected last so that a run stopping at
 the first failure has already run every other test.
@@ -44,8 +45,8 @@ def test_noalloc_residual_norm_matches_scratch_version_twice_in_a_row(dtype):
         rhs = torch.as_tensor(rng.standard_normal(grid.shape), device='cuda', dtype=dtype)
         got = _noalloc_norm(p, rhs, grid.spacing, _lib.BC_NEUMANN)
         ref = _scratch_norm(mg, p, rhs)
-        torch.testing.assert_close(got, ref, rtol=1e-13, atol=0)
-        assert got.item() > 0
+        # same kernel, same launch geometry, same partial order: bitwise equal
+        assert got.item() == ref.item() > 0
 
 
 def test_noalloc_residual_norm_2d_channel_and_rejects_large_grids():
@@ -56,7 +57,7 @@ def test_noalloc_residual_norm_2d_channel_and_rejects_large_grids():
         p = torch.as_tensor(rng.standard_normal(grid.shape), device='cuda')
         rhs = torch.as_tensor(rng.standard_normal(grid.shape), device='cuda')
         got = _noalloc_norm(p, rhs, grid.spacing, _lib.BC_CHANNEL)
-        torch.testing.assert_close(got, _scratch_norm(mg, p, rhs), rtol=1e-13, atol=0)
+        assert got.item() == _scratch_norm(mg, p, rhs).item()
     big = torch.zeros((2048, 4096), device='cuda')  # 2^23 cells: 32768 reduction blocks
     with pytest.raises(RuntimeError, match='at most 4096'):
         _noalloc_norm(big, big, (1 / 2048, 1 / 4096), _lib.BC_CHANNEL)
