@@ -46,6 +46,11 @@ class PCGPlan(ctypes.Structure):
                 ('atol', ctypes.c_double)]
 
 
+class RefineInstance(ctypes.Structure):
+    _fields_ = [('nx', c_int64), ('ny', c_int64), ('h2', ctypes.c_double * 2), ('p', c_void_p), ('b', c_void_p),
+                ('r32', c_void_p), ('e32', c_void_p)]
+
+
 # name -> argtypes (restype int32 unless listed in _RESTYPES)
 _SIGNATURES = {
     'afsi_b200_last_error': [],
@@ -134,6 +139,15 @@ _SIGNATURES = {
     'afsi_b200_mg_batch_table': [c_void_p, c_int32, c_void_p, c_void_p, c_int64],
     'afsi_b200_mg_batch_vcycles': [c_void_p, c_int32, c_void_p, c_int32, c_int32, c_void_p],
     'afsi_b200_mg_batch_persistent': [c_void_p, c_int32, c_void_p, c_int32, c_int32, c_void_p, c_void_p],
+    'afsi_b200_batch_refine_bytes': [c_void_p, c_int32],
+    'afsi_b200_batch_refine_state_offset': [c_void_p, c_int32],
+    'afsi_b200_batch_refine_setup': [c_void_p, c_int32, c_void_p, c_int64],
+    'afsi_b200_batch_refine_start': [c_void_p, c_int32, c_void_p, c_double, c_double, c_int32, c_void_p],
+    'afsi_b200_batch_refine_step': [c_void_p, c_int32, c_void_p, c_double, c_double, c_int32, c_void_p],
+    'afsi_b200_batch_refine_graph_create': [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_int32, c_double,
+                                            c_double, c_int32, c_void_p],
+    'afsi_b200_batch_refine_graph_launch': [c_void_p, c_void_p],
+    'afsi_b200_batch_refine_graph_destroy': [c_void_p],
     'afsi_b200_batch2d_prepare': [c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_int32,
                                   c_void_p],
     'afsi_b200_batch2d_spread': [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_void_p,
@@ -163,7 +177,8 @@ _SIGNATURES = {
     'afsi_b200_pcg_graph_destroy': [c_void_p],
 }
 _RESTYPES = {'afsi_b200_last_error': ctypes.c_char_p, 'afsi_b200_mg_scratch_bytes': ctypes.c_int64,
-             'afsi_b200_mg_batch_table_bytes': ctypes.c_int64,
+             'afsi_b200_mg_batch_table_bytes': ctypes.c_int64, 'afsi_b200_batch_refine_bytes': ctypes.c_int64,
+             'afsi_b200_batch_refine_state_offset': ctypes.c_int64,
              'afsi_b200_launch_count': ctypes.c_int64, 'afsi_b200_mg_sync_bytes': ctypes.c_int64,
              'afsi_b200_p1_plan_scratch_bytes': ctypes.c_int64, 'afsi_b200_hash_csr_scratch_bytes': ctypes.c_int64,
              'afsi_b200_pcg_scratch_bytes': ctypes.c_int64, 'afsi_b200_mg_refine_scratch_bytes': ctypes.c_int64,

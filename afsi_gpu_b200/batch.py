@@ -19,7 +19,12 @@ step:
   ``afsi_b200_mg_batch_persistent``), or per instance with the instances
   spread over ``streams`` capture streams so that their small level kernels
   overlap on the device;
-* the whole step captured once as a CUDA graph and replayed.
+* the whole step captured once as a CUDA graph and replayed;
+* or, at the FP64 solve tolerance (``Schedule(refined=True)``): the pressure
+  kept in FP64 per instance, and batched FP32 V-cycles inside batched FP64
+  iterative refinement until every instance's FP64 residual meets
+  max(atol, rtol ||b||) (``BatchedRefinement``); the refinement loop runs on the
+  device as one graph with a WHILE node.
 
 ``autotune()`` chooses the schedule (batched or per-instance V-cycles, stream
 count, instance order, smoother with the cycle count that reaches the
@@ -65,6 +70,7 @@ class Schedule:
     smoother: str = 'jacobi'
     cycles: int = 6
     vcycles: str = 'streams'   # 'streams' (per instance over side streams), 'batched' or 'persistent' (Jacobi)
+    refined: bool = False      # FP64 refinement to the solve tolerance; `cycles` V-cycles per refinement
 
 
 class BatchedVCycles:
@@ -106,12 +112,10 @@ class BatchedVCycles:
 
     def run(self, cycles, *, start=True, persistent=False):
         """`cycles` V-cycles of every solver on the current stream; with
-        `start`, from a zero iterate with the sources as right-hand sides.
-        persistent: all of it in one cooperative launch
-        (``afsi_b200_mg_batch_persistent``) instead of one launch per level
-        operation; the results are the same bit for bit."""
-        if start and self._sources is None:
-            raise ValueError('a start needs right-hand-side sources')
+        `start`, from a zero iterate, with the sources (if this batch has
+        them) copied in as right-hand sides first.  persistent: all of it in
+        one cooperative launch (``afsi_b200_mg_batch_persistent``) instead of
+        one launch per level operation; the results are the same bit for bit."""
         s = torch.cuda.current_stream(self.table.device).cuda_stream
         if persistent:
             call('afsi_b200_mg_batch_persistent', self._plans, self.count, ptr(self.table), int(cycles), int(start),
@@ -123,6 +127,122 @@ class BatchedVCycles:
         """Raise if a grid barrier of a persistent run timed out."""
         if int(self.sync[8:12].view(torch.int32).item()):
             raise RuntimeError('persistent batched V-cycles: a grid barrier timed out')
+
+
+class BatchedRefinement:
+    """FP64 iterative refinement of many channel pressure solves around
+    batched FP32 V-cycles (``afsi_b200_batch_refine_*``).
+
+    Each instance keeps an FP64 iterate and right-hand side (views into two
+    batch arrays).  One refinement runs `cycles` batched Jacobi V-cycles of the
+    FP32 solvers from zero on the float of the FP64 residual, adds the
+    correction in FP64 and forms the new FP64 residual with the reference
+    operator and its norm per instance.  Refinements repeat on the device
+    until every instance meets its own tolerance max(atol, rtol ||b||), the
+    tolerance of the FP64 solver (``mac2d/multigrid.py:94-99``), or
+    `max_refinements` ran.  `run(cycles)` launches the whole loop (start plus
+    a WHILE node) as one graph; `state()` reads the outcome with one host read.
+    """
+
+    def __init__(self, solvers, rhs, *, rtol=1e-10, atol=1e-12, max_refinements=12):
+        self.solvers = list(solvers)
+        self.count = len(self.solvers)
+        if self.count != len(rhs) or not self.count:
+            raise ValueError('one FP64 right-hand side per solver')
+        lib = _lib.load()
+        w0 = self.solvers[0].workspace
+        device = w0.p[0].device
+        for mg in self.solvers:
+            w = mg.workspace
+            if w.p[0].dtype != torch.float32 or mg.bc != 'channel' or mg.smoother != 'jacobi':
+                raise ValueError('batched refinement takes FP32 Jacobi channel solvers')
+        sizes = [mg.workspace.p[0].numel() for mg in self.solvers]
+        self.offsets = np.concatenate(([0], np.cumsum(sizes))).astype(np.int64)
+        self.b = torch.cat([torch.as_tensor(r, device=device, dtype=torch.float64).reshape(-1) for r in rhs])
+        self.p = torch.zeros_like(self.b)
+        inst = (_lib.RefineInstance * self.count)()
+        for i, mg in enumerate(self.solvers):
+            w, (nx, ny) = mg.workspace, mg.shapes[0]
+            hx, hy = mg.spacings[0]
+            inst[i].nx, inst[i].ny = nx, ny
+            inst[i].h2[0], inst[i].h2[1] = hx * hx, hy * hy
+            lo = int(self.offsets[i])
+            inst[i].p = self.p.data_ptr() + lo * 8
+            inst[i].b = self.b.data_ptr() + lo * 8
+            inst[i].r32 = ptr(w.rhs[0])
+            inst[i].e32 = ptr(w.p[0])
+        self._inst = inst
+        nbytes = lib.afsi_b200_batch_refine_bytes(inst, self.count)
+        if nbytes < 0:
+            raise ValueError(f'batched refinement: {lib.afsi_b200_last_error().decode(errors="replace")}')
+        host = np.zeros(int(nbytes), np.uint8)
+        call('afsi_b200_batch_refine_setup', inst, self.count, host.ctypes.data, int(nbytes))
+        self.buffer = torch.as_tensor(host).to(device)
+        self._state_off = int(lib.afsi_b200_batch_refine_state_offset(inst, self.count))
+        self.vcycles = BatchedVCycles(self.solvers)   # table without sources: a start zeroes the iterates only
+        with torch.cuda.device(device):
+            self.vcycles.run(1, start=True)  # one eager run sets the kernels' attributes before any capture
+        self.rtol, self.atol, self.max_refinements = float(rtol), float(atol), int(max_refinements)
+        self._graphs = {}
+
+    def rhs(self, i):
+        return self.b[self.offsets[i]:self.offsets[i + 1]].view(self.solvers[i].shapes[0])
+
+    def pressure(self, i):
+        return self.p[self.offsets[i]:self.offsets[i + 1]].view(self.solvers[i].shapes[0])
+
+    def _graph(self, cycles):
+        if cycles not in self._graphs:
+            handle = ctypes.c_void_p()
+            before = _lib.launch_count()
+            with torch.cuda.device(self.buffer.device):
+                call('afsi_b200_batch_refine_graph_create', self._inst, self.count, ptr(self.buffer),
+                     self.vcycles._plans, ptr(self.vcycles.table), int(cycles), self.rtol, self.atol,
+                     self.max_refinements, ctypes.byref(handle))
+            captured = _lib.launch_count() - before  # start + body, captured only
+            _lib.forget_launches(captured)
+            self._graphs[cycles] = (handle.value, captured - 1)
+        return self._graphs[cycles]
+
+    def run(self, cycles):
+        """The refinement loop with `cycles` V-cycles per refinement on the current stream."""
+        graph, _ = self._graph(cycles)
+        call('afsi_b200_batch_refine_graph_launch', graph, torch.cuda.current_stream(self.buffer.device).cuda_stream)
+
+    def run_launched(self, cycles):
+        """The same loop driven from the host (one read per refinement), for checks."""
+        s = torch.cuda.current_stream(self.buffer.device).cuda_stream
+        args = (self._inst, self.count, ptr(self.buffer))
+        call('afsi_b200_batch_refine_start', *args, self.rtol, self.atol, self.max_refinements, s)
+        while True:
+            st = self.state()
+            if not st['unconverged'] or st['nonfinite'] or st['refinements'] >= self.max_refinements:
+                return st
+            self.vcycles.run(cycles, start=True)
+            call('afsi_b200_batch_refine_step', *args, self.rtol, self.atol, self.max_refinements, s)
+
+    def state(self):
+        """Outcome of the last run: per-instance residual norms, tolerances and
+        the refinement after which each first met its tolerance (-1: never)."""
+        n = self.count
+        words = self.buffer[self._state_off:self._state_off + (4 * n + 8) * 8].view(torch.float64).tolist()
+        loop = words[4 * n:]
+        return dict(norm=words[:n], tol=words[n:2 * n], rhs_norm=words[2 * n:3 * n],
+                    done_at=[int(v) for v in words[3 * n:4 * n]], refinements=int(loop[0]),
+                    unconverged=int(loop[1]), nonfinite=bool(loop[2]), worst_ratio=loop[3])
+
+    def launches(self, cycles):
+        """Native launches of one run: the start plus the body per refinement."""
+        _, body = self._graph(cycles)
+        return 1 + body * self.state()['refinements']
+
+    def __del__(self):
+        for graph, _ in getattr(self, '_graphs', {}).values():
+            try:
+                _lib.call('afsi_b200_batch_refine_graph_destroy', graph)
+            except Exception:
+                pass
+        self._graphs = {}
 
 
 class BatchedChannels:
@@ -161,6 +281,7 @@ class BatchedChannels:
         self.u_in = torch.cat([as_t(v[0], transfer_dtype).reshape(-1) for v in velocities])
         self.v_in = torch.cat([as_t(v[1], transfer_dtype).reshape(-1) for v in velocities])
         self.rhs = [as_t(r, mg_dtype) for r in pressures]
+        self.rhs64 = [as_t(r, torch.float64) for r in pressures]
         self.ids = torch.empty((2, self.total, 16), device=device, dtype=torch.int64)
         self.weights = torch.empty((2, self.total, 16), device=device, dtype=transfer_dtype)
         self.u = torch.zeros(self.nu, device=device, dtype=transfer_dtype)
@@ -169,6 +290,7 @@ class BatchedChannels:
         self.status = torch.zeros(1, device=device, dtype=torch.int32)
         self._solvers = {}
         self._batched = None
+        self._refinement = None
         self.graph = None
 
     # -- pieces of the step
@@ -207,6 +329,14 @@ class BatchedChannels:
             self._batched = BatchedVCycles(self.solvers('jacobi'), self.rhs)
         return self._batched
 
+    def refinement(self):
+        """FP64 refinement around the batched FP32 Jacobi V-cycles (built once)."""
+        if self._refinement is None:
+            if self.mg_dtype != torch.float32:
+                raise ValueError('the refined schedule runs FP32 V-cycles')
+            self._refinement = BatchedRefinement(self.solvers('jacobi'), self.rhs64)
+        return self._refinement
+
     def order(self, schedule):
         idx = list(range(len(self.grids)))
         if schedule.order == 'largest-first':
@@ -219,6 +349,9 @@ class BatchedChannels:
         schedule = schedule or self.schedule
         main = torch.cuda.current_stream(self.device)
         self.transfers(main)
+        if schedule.refined:
+            self.refinement().run(schedule.cycles)
+            return
         if schedule.vcycles in ('batched', 'persistent'):
             if schedule.smoother != 'jacobi':
                 raise ValueError('batched V-cycles use the Jacobi smoother')
@@ -236,10 +369,16 @@ class BatchedChannels:
             main.wait_stream(s)
 
     def capture(self, schedule=None):
+        """The step as a CUDA graph: everything, or with a refined schedule the
+        transfers only (the refinement loop is its own graph, launched after)."""
         schedule = schedule or self.schedule
         self.solvers(schedule.smoother)
-        if schedule.vcycles in ('batched', 'persistent'):
+        if schedule.refined:
+            self.refinement()._graph(schedule.cycles)
+        elif schedule.vcycles in ('batched', 'persistent'):
             self.batched()
+        step = (lambda: self.transfers(torch.cuda.current_stream(self.device))) if schedule.refined else \
+            (lambda: self.run(schedule))
         with torch.cuda.device(self.device):
             warm = torch.cuda.Stream(device=self.device)
             warm.wait_stream(torch.cuda.current_stream(self.device))
@@ -249,7 +388,7 @@ class BatchedChannels:
             g = torch.cuda.CUDAGraph()
             before = _lib.launch_count()
             with torch.cuda.graph(g):
-                self.run(schedule)
+                step()
             launches = _lib.launch_count() - before
             _lib.forget_launches(launches)
         return g, launches
@@ -263,6 +402,8 @@ class BatchedChannels:
             self.use(self.schedule)
         self.graph.replay()
         _lib.count_replay(self.graph_launches)
+        if self.schedule.refined:
+            self.refinement().run(self.schedule.cycles)
 
     # -- results and checks
     def fields(self, i):
@@ -275,7 +416,18 @@ class BatchedChannels:
         return self.gathered[self.point_offsets[i]:self.point_offsets[i + 1]]
 
     def pressure(self, i, smoother=None):
+        if self.schedule.refined and smoother is None:
+            return self.refinement().pressure(i)
         return self.solvers(smoother or self.schedule.smoother)[i].workspace.p[0]
+
+    def refined_report(self):
+        """Cycles-to-tolerance per instance of the last refined run (one host read)."""
+        st = self.refinement().state()
+        c = self.schedule.cycles
+        return dict(refinements=st['refinements'], unconverged=st['unconverged'], nonfinite=st['nonfinite'],
+                    worst_relative_residual=st['worst_ratio'],
+                    cycles_to_tolerance=[d * c if d >= 0 else None for d in st['done_at']],
+                    max_norm_over_tol=max(n / t for n, t in zip(st['norm'], st['tol'])))
 
     def residual_reduction(self, smoother=None):
         """||rhs - A p|| / ||rhs|| per instance after the last step (FP32 workspaces)."""
@@ -337,6 +489,38 @@ class BatchedChannels:
                 del g
         if best is None:
             raise RuntimeError(f'no smoother reaches the residual reduction {target:g} in {max_cycles} cycles')
+        self.use(best[1])
+        return best[1], table
+
+
+    def autotune_refined(self, *, cycles=(2, 3, 4, 5, 6, 8), replays=5):
+        """Fastest refined schedule: for each count of V-cycles per refinement,
+        one run to check that every instance meets its FP64 tolerance, then
+        CUDA-event timing of `replays` whole steps (transfers graph plus the
+        refinement loop); returns (schedule, table)."""
+        table, best = [], None
+        for c in cycles:
+            sch = Schedule(streams=1, order='given', smoother='jacobi', cycles=int(c), vcycles='batched',
+                           refined=True)
+            self.use(sch)
+            self.replay()
+            rep = self.refined_report()
+            row = dict(cycles_per_refinement=int(c), refinements=rep['refinements'],
+                       converged=rep['unconverged'] == 0 and not rep['nonfinite'])
+            if row['converged']:
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize(self.device)
+                e0.record()
+                for _ in range(replays):
+                    self.replay()
+                e1.record()
+                torch.cuda.synchronize(self.device)
+                row['ms'] = e0.elapsed_time(e1) / replays
+                if best is None or row['ms'] < best[0]:
+                    best = (row['ms'], sch)
+            table.append(row)
+        if best is None:
+            raise RuntimeError('no refined schedule met the FP64 tolerance on every instance')
         self.use(best[1])
         return best[1], table
 

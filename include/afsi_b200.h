@@ -423,6 +423,52 @@ int32_t afsi_b200_mg_batch_vcycles(const afsi_mg_plan* const* plans, int32_t cou
 int32_t afsi_b200_mg_batch_persistent(const afsi_mg_plan* const* plans, int32_t count, const void* table,
     int32_t cycles, int32_t start, void* sync_scratch, afsi_stream_t stream);
 
+/* Batched FP64 iterative refinement around the batched FP32 V-cycles (the
+ * batching form at the FP64 solve tolerance; no counterpart in the reference,
+ * which solves each channel instance alone in FP64 with ChannelMultigrid.solve,
+ * mac2d/multigrid.py:85-111).  An instance is an FP64 iterate p and right-hand
+ * side b on an nx x ny channel grid, and the finest right-hand side r32 and
+ * iterate e32 of its FP32 channel plan.  One refinement: FP32 V-cycles from
+ * zero on r32 give e32; p += double(e32); r = b - A p with the reference's
+ * FP64 operator (mac2d/grid.py:61-71); r32 = float(r); ||r|| per instance.
+ * Refinements repeat until every instance meets max(atol, rtol ||b||) (the
+ * FP64 solver's tolerance, mac2d/multigrid.py:94-99) or max_refinements (1..64)
+ * ran.  `buffer` is a device copy of the image afsi_b200_batch_refine_setup
+ * fills in host memory (16-byte aligned, afsi_b200_batch_refine_bytes long);
+ * after a run it holds, as doubles at afsi_b200_batch_refine_state_offset():
+ * norm[count], tol[count], rhs_norm[count], done_at[count] (refinements after
+ * which the instance first met its tolerance, -1 if never), then loop words
+ * {refinements run, instances unconverged, nonfinite flag, largest ||r||/||b||}.
+ * afsi_b200_batch_refine_start: p = 0, r32 = float(b), the norms and tolerances.
+ * afsi_b200_batch_refine_step: the correction and residual of one refinement
+ *   (the caller runs the V-cycles in between).
+ * afsi_b200_batch_refine_graph_create: the whole solve as one CUDA graph (the
+ *   start, then a WHILE node whose body is `cycles` batched V-cycles of `plans`
+ *   over `vcycle_table` (a table made without right-hand-side sources), the
+ *   correction and the residual); launched with .._graph_launch. */
+typedef struct afsi_refine_instance {
+    int64_t nx, ny;      /* cells */
+    double h2[2];        /* hx^2, hy^2 */
+    double* p;           /* FP64 iterate (written) */
+    const double* b;     /* FP64 right-hand side */
+    float* r32;          /* FP32 plan's finest right-hand side (written) */
+    const float* e32;    /* FP32 plan's finest iterate (the correction) */
+} afsi_refine_instance;
+
+int64_t afsi_b200_batch_refine_bytes(const afsi_refine_instance* instances, int32_t count);
+int64_t afsi_b200_batch_refine_state_offset(const afsi_refine_instance* instances, int32_t count);
+int32_t afsi_b200_batch_refine_setup(const afsi_refine_instance* instances, int32_t count, void* host_buffer,
+    int64_t bytes);
+int32_t afsi_b200_batch_refine_start(const afsi_refine_instance* instances, int32_t count, void* buffer,
+    double rtol, double atol, int32_t max_refinements, afsi_stream_t stream);
+int32_t afsi_b200_batch_refine_step(const afsi_refine_instance* instances, int32_t count, void* buffer,
+    double rtol, double atol, int32_t max_refinements, afsi_stream_t stream);
+int32_t afsi_b200_batch_refine_graph_create(const afsi_refine_instance* instances, int32_t count, void* buffer,
+    const afsi_mg_plan* const* plans, const void* vcycle_table, int32_t cycles, double rtol, double atol,
+    int32_t max_refinements, void** graph_out);
+int32_t afsi_b200_batch_refine_graph_launch(void* graph, afsi_stream_t stream);
+int32_t afsi_b200_batch_refine_graph_destroy(void* graph);
+
 /* Iterative refinement of an FP64 pressure solve by FP32 V-cycles (the
  * precision form; no counterpart in the reference, whose solver is FP64
  * throughout, mac/multigrid.py:125-172).

@@ -176,5 +176,68 @@ def test_batched_vcycles_reject_what_they_do_not_batch():
     for pair in ((a, b), (a, rb)):
         with pytest.raises(ValueError, match='batched V-cycles'):
             BatchedVCycles(list(pair))
-    with pytest.raises(ValueError, match='sources'):
-        BatchedVCycles([a]).run(1)
+    # a batch without right-hand-side sources starts from a zero iterate on
+    # the right-hand side already in the workspace (the refinement's use)
+    a.workspace.p[0].fill_(3.)
+    a.workspace.rhs[0].copy_(torch.randn(g.shape, device=DEV))
+    rhs = a.workspace.rhs[0].clone()
+    BatchedVCycles([a]).run(1)
+    alone = ChannelMultigrid(g, device=DEV, dtype=torch.float32, coarse_dtype=torch.float64, backend='b200')
+    alone.initialize(torch.zeros_like(rhs), rhs)
+    assert torch.equal(a.workspace.rhs[0], rhs) and torch.equal(a.workspace.p[0], alone.advance(1))
+
+
+def test_refined_batch_meets_the_fp64_tolerance_per_instance_against_the_oracle():
+    """The batching form at the FP64 bar: FP64 transfers and FP32 V-cycles in
+    batched FP64 refinement.  Every instance meets its own FP64 tolerance
+    (1e-10 relative residual), and every output is within 1e-8 (relative to
+    its largest value) of the FP64 oracle: the transfers of
+    ``mac2d/transfer.py:61-127`` and the channel solve of
+    ``mac2d/multigrid.py:85-111`` run to 1e-10.  The device loop (one graph)
+    equals the host-driven loop of the same kernels bit for bit."""
+    from oracle import mg as oracle_mg
+    b = seeded_batch(7, seed=5, shapes=((64, 16), (128, 32), (256, 64), (32, 8)), points=(800, 3000), device=DEV,
+                     transfer_dtype=torch.float64,
+                     schedule=Schedule(smoother='jacobi', cycles=4, vcycles='batched', refined=True))
+    b.replay()
+    torch.cuda.synchronize()
+    b.check()
+    rep = b.refined_report()
+    assert rep['unconverged'] == 0 and not rep['nonfinite'] and rep['max_norm_over_tol'] <= 1
+    assert all(c is not None and c > 0 for c in rep['cycles_to_tolerance'])
+    graph_p = b.refinement().p.clone()
+    for i, g in enumerate(b.grids):
+        lo, hi = b.point_offsets[i], b.point_offsets[i + 1]
+        ids, w = oracle.prepare2d(b.x[lo:hi].cpu().numpy(), g.shape, g.spacing)
+        force = b.force[lo:hi].cpu().numpy()
+        fields = b.fields(i)
+        vel = (b.u_in[b.u_offsets[i]:b.u_offsets[i + 1]], b.v_in[b.v_offsets[i]:b.v_offsets[i + 1]])
+        for c in range(2):
+            ref = oracle.indexed_spread(force[:, c], ids[c], w[c], fields[c].numel(), g.volume)
+            got = fields[c].reshape(-1).cpu().numpy()
+            assert np.abs(got - ref).max() <= 1e-8 * np.abs(ref).max()
+            ref = oracle.indexed_gather(vel[c].cpu().numpy(), ids[c], w[c])
+            got = b.velocities(i)[:, c].cpu().numpy()
+            assert np.abs(got - ref).max() <= 1e-8 * np.abs(ref).max()
+        rhs = b.rhs64[i].cpu().numpy()
+        pref, info = oracle_mg.solve(oracle_mg.Hierarchy(g.shape, g.spacing, 'channel'), rhs)
+        p = b.pressure(i).cpu().numpy()
+        assert np.abs(p - pref).max() <= 1e-8 * np.abs(pref).max(), i
+        res = np.linalg.norm(rhs - oracle_mg.Hierarchy(g.shape, g.spacing, 'channel').apply(0, p))
+        assert res <= 1e-10 * np.linalg.norm(rhs)
+    st = b.refinement().run_launched(4)
+    torch.cuda.synchronize()
+    assert st['unconverged'] == 0
+    assert torch.equal(b.refinement().p, graph_p)
+
+
+def test_refined_batch_stops_at_the_refinement_cap_without_hanging():
+    """A cap below what the tolerance needs ends the device loop with the
+    instances reported unconverged (the loop cannot run past the cap)."""
+    from afsi_gpu_b200.batch import BatchedRefinement
+    b = seeded_batch(3, seed=6, shapes=((128, 32),), points=(500, 800), device=DEV, transfer_dtype=torch.float64)
+    r = BatchedRefinement(b.solvers('jacobi'), b.rhs64, rtol=1e-14, atol=0., max_refinements=2)
+    r.run(1)
+    st = r.state()
+    assert st['refinements'] == 2 and st['unconverged'] == 3
+    assert all(d == -1 for d in st['done_at'])
