@@ -33,6 +33,7 @@ sys.path.insert(0, str(ROOT))
 SHELL = dict(nr=3, ntheta=40, nphi=64)
 GRID = dict(shape=(64, 64, 64), lengths=(1., 1., 1.))
 METRIC = 'IB transfer+MG V-cycle steps/s (P2 prepare+spread+interpolate+pressure MG solve, FP64)'
+WORKLOAD = '3D P2 shell 38400 elements / 2457600 points, 64^3 MAC, FP64'
 
 
 def parse():
@@ -42,10 +43,12 @@ def parse():
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='b200', choices=('b200', 'reference'))
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--rows', default='all', choices=('all', 'step', 'p1'),
+    ap.add_argument('--rows', default='all', choices=('all', 'step', 'p1', 'batch'),
                     help="'step': the headline step line only, without the mass-solve, MG-form, batching and "
                          "serving rows (for profiler runs); 'p1': only the precision-form row on the 128^3 P1 "
-                         "configuration, printed as its own JSON object (for profiler runs)")
+                         "configuration, printed as its own JSON object (for profiler runs); 'batch': only "
+                         "`--steps` replays of the refined batch step after `--warmup`, summarised as JSON "
+                         "(for profiler runs)")
     return ap.parse_args()
 
 
@@ -278,22 +281,7 @@ def mg_forms_row(grid, rhs, device, reps=10):
     return out
 
 
-def batch_form_row(device, count=64, replays=20):
-    """Batching form: 64 seeded 2D channel instances (grids 128x32 .. 512x128,
-    5k-40k leaflet points each, N(0,1) forces), FP32 transfers and V-cycles,
-    one captured graph per step with the autotuned schedule (batched or
-    per-instance V-cycles; fixed V-cycle count reaching a 1e-4 FP32 residual
-    reduction on every instance).  The
-    plain FP64 drop-in on the same GPU steps the same instances one at a time
-    through the single-instance API (prepare2d with its support check,
-    spread2d, gather2d, FP64 channel V-cycles, same cycle count).  Errors:
-    largest difference of the FP32 batch from the FP64 plain step over the
-    largest value, per output."""
-    from afsi_gpu_b200 import cuda_ib
-    from afsi_gpu_b200.batch import seeded_batch
-    from afsi_gpu_b200.multigrid import ChannelMultigrid, MGOptions
-    b = seeded_batch(count, seed=0, device=device)
-    schedule, table = b.autotune(target=1e-4)
+def _time_replays(b, replays, device):
     stream = torch.cuda.current_stream(device)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     b.replay()
@@ -303,18 +291,41 @@ def batch_form_row(device, count=64, replays=20):
         b.replay()
     e1.record(stream)
     torch.cuda.synchronize(device)
-    ms = e0.elapsed_time(e1) / replays
+    return e0.elapsed_time(e1) / replays
+
+
+def batch_form_row(device, count=64, replays=20, oracle_instances=6):
+    """Batching form at the FP64 bar: 64 seeded 2D channel instances (grids
+    128x32 .. 512x128, 5k-40k leaflet points each, N(0,1) forces).  One batch
+    step: one prepare, spread and gather launch for all instances (FP64
+    positions, weights and transfers; a captured graph), then the pressure of
+    every instance to its own 1e-10 relative residual: batched FP32 Jacobi
+    V-cycles inside batched FP64 iterative refinement, the loop on the device
+    (one graph, WHILE node), cycles per refinement chosen by the autotuner.
+    The plain FP64 drop-in on the same GPU steps the same instances one at a
+    time through the single-instance API: prepare2d with its support check,
+    spread2d, gather2d, and ChannelMultigrid.solve to 1e-10 (FP64 V-cycles,
+    graph-replayed blocks).  Both sides report cycles to tolerance.  Errors:
+    max |batch - plain| / max |plain| per output over all instances, and
+    against the FP64 oracle (transfers and the channel solve to 1e-10) on
+    `oracle_instances` instances.  The same step with FP32 weights and
+    transfers is reported beside it with its (larger) errors."""
+    from afsi_gpu_b200 import cuda_ib
+    from afsi_gpu_b200.batch import seeded_batch
+    from afsi_gpu_b200.multigrid import ChannelMultigrid
+    from oracle import ib as oib, mg as omg
+    b = seeded_batch(count, seed=0, device=device, transfer_dtype=torch.float64)
+    schedule, table = b.autotune_refined()
+    ms = _time_replays(b, replays, device)
     b.check()
-    # plain FP64 drop-in, one instance at a time
-    opts = MGOptions(smooth=2 if schedule.smoother == 'red-black' else 4)
-    plain = [ChannelMultigrid(g, device=device, backend='b200', smoother=schedule.smoother, options=opts)
-             for g in b.grids]
+    rep = b.refined_report()
+    launches = b.graph_launches + b.refinement().launches(schedule.cycles)
+    # plain FP64 drop-in, one instance at a time, each solved to its tolerance
+    plain = [ChannelMultigrid(g, device=device, backend='b200-graph') for g in b.grids]
     x = [b.x[b.point_offsets[i]:b.point_offsets[i + 1]] for i in range(count)]
-    f = [b.force[b.point_offsets[i]:b.point_offsets[i + 1]].double() for i in range(count)]
-    vel = [(b.u_in[b.u_offsets[i]:b.u_offsets[i + 1]].double().view(g.face_shape(0)),
-            b.v_in[b.v_offsets[i]:b.v_offsets[i + 1]].double().view(g.face_shape(1)))
-           for i, g in enumerate(b.grids)]
-    rhs = [r.double() for r in b.rhs]
+    f = [b.force[b.point_offsets[i]:b.point_offsets[i + 1]] for i in range(count)]
+    vel = [(b.u_in[b.u_offsets[i]:b.u_offsets[i + 1]].view(g.face_shape(0)),
+            b.v_in[b.v_offsets[i]:b.v_offsets[i + 1]].view(g.face_shape(1))) for i, g in enumerate(b.grids)]
 
     def plain_step():
         out = []
@@ -322,36 +333,123 @@ def batch_form_row(device, count=64, replays=20):
             st = cuda_ib.prepare2d(g, x[i])
             fields = cuda_ib.spread2d(g, f[i], st)
             gathered = cuda_ib.gather2d(vel[i], st)
-            mg = plain[i]
-            mg.initialize(torch.zeros_like(rhs[i]), rhs[i])
-            out.append((fields, gathered, mg.advance(schedule.cycles)))
+            p, info = plain[i].solve(b.rhs64[i])
+            out.append((fields, gathered, p, info['cycles']))
         return out
 
     plain_step()
+    stream = torch.cuda.current_stream(device)
     torch.cuda.synchronize(device)
     p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    p0.record(stream)
     reps = 3
+    p0.record(stream)
     for _ in range(reps):
         res = plain_step()
     p1.record(stream)
     torch.cuda.synchronize(device)
     plain_ms = p0.elapsed_time(p1) / reps
 
-    def rel(a, ref):
-        return float((a.double() - ref).abs().max() / ref.abs().max())
+    def vs_plain(bb):
+        return dict(spread=max(max(rel_err(bb.fields(i)[c].cpu(), res[i][0][c].cpu()) for c in range(2))
+                               for i in range(count)),
+                    interpolate=max(rel_err(bb.velocities(i).cpu(), res[i][1].cpu()) for i in range(count)),
+                    pressure=max(rel_err(bb.pressure(i).cpu(), res[i][2].cpu()) for i in range(count)))
 
-    err = dict(spread=max(max(rel(b.fields(i)[c], res[i][0][c]) for c in range(2)) for i in range(count)),
-               interpolate=max(rel(b.velocities(i), res[i][1]) for i in range(count)),
-               v_cycles=max(rel(b.pressure(i), res[i][2]) for i in range(count)))
+    err_plain = vs_plain(b)
+    # against the FP64 oracle on a few instances spread over the batch
+    picks = sorted(set(int(k) for k in np.linspace(0, count - 1, oracle_instances)))
+    eo = dict(spread=0., interpolate=0., pressure=0.)
+    for i in picks:
+        g = b.grids[i]
+        ids, w = oib.prepare2d(x[i].cpu().numpy(), g.shape, g.spacing)
+        ff, vv = f[i].cpu().numpy(), [v.cpu().numpy() for v in vel[i]]
+        for c in range(2):
+            eo['spread'] = max(eo['spread'], rel_err(b.fields(i)[c].reshape(-1).cpu(),
+                                                     oib.indexed_spread(ff[:, c], ids[c], w[c], vel[i][c].numel(),
+                                                                        g.volume)))
+            eo['interpolate'] = max(eo['interpolate'], rel_err(b.velocities(i)[:, c].cpu(),
+                                                               oib.indexed_gather(vv[c], ids[c], w[c])))
+        pref, _ = omg.solve(omg.Hierarchy(g.shape, g.spacing, 'channel'), b.rhs64[i].cpu().numpy())
+        eo['pressure'] = max(eo['pressure'], rel_err(b.pressure(i).cpu(), pref))
+    eo['instances'] = picks
+    # the FP32-transfer variant of the same step (does not meet 1e-8)
+    b32 = seeded_batch(count, seed=0, device=device, transfer_dtype=torch.float32)
+    s32, _ = b32.autotune_refined()
+    ms32 = _time_replays(b32, replays, device)
+    err32 = vs_plain(b32)
+    meets = max(err_plain.values()) <= 1e-8 and max(v for k, v in eo.items() if k != 'instances') <= 1e-8
     return dict(instances=count, points=b.total, faces=b.nu + b.nv,
-                schedule=dict(streams=schedule.streams, order=schedule.order, smoother=schedule.smoother,
-                              cycles=schedule.cycles, vcycles=schedule.vcycles),
+                form='FP64 transfers; batched FP32 V-cycles in batched FP64 refinement to 1e-10 per instance',
+                schedule=dict(cycles_per_refinement=schedule.cycles, refinements=rep['refinements'],
+                              vcycles=schedule.vcycles),
                 ms_per_batch_step=ms, instance_steps_per_s=count / (ms / 1e3),
+                cycles_to_tolerance=dict(batch=sorted(set(c for c in rep['cycles_to_tolerance'] if c is not None)),
+                                         plain_fp64=sorted(set(r[3] for r in res))),
+                unconverged=rep['unconverged'], worst_relative_residual=rep['worst_relative_residual'],
                 plain_fp64_ms_per_batch=plain_ms, plain_fp64_instance_steps_per_s=count / (plain_ms / 1e3),
-                speedup_vs_plain_fp64=plain_ms / ms, error_vs_fp64=err,
-                max_residual_reduction=max(b.residual_reduction()), graph_launches=b.graph_launches,
-                autotune=table)
+                speedup_vs_plain_fp64=plain_ms / ms, meets_1e_8=bool(meets),
+                error_vs_plain_fp64=err_plain, error_vs_fp64_oracle=eo,
+                launches_per_step=int(launches), autotune=table,
+                fp32_transfers=dict(ms_per_batch_step=ms32, speedup_vs_plain_fp64=plain_ms / ms32,
+                                    cycles_per_refinement=s32.cycles, error_vs_plain_fp64=err32,
+                                    meets_1e_8=bool(max(err32.values()) <= 1e-8)))
+
+
+def config1_row(device, steps=50, cpu_reps=5):
+    """Config 1, the plain method: 2D 256x64 MAC on a 1.0 x 0.25 box (h =
+    1/256), periodic in x with walls in y, FP64.  20,000 points on the
+    centred ellipse with semi-axes 0.3 and 0.1 and radial jitter U(-0.2h,
+    0.2h); N(0,1) point forces; a face velocity of 8 seeded Fourier modes; a
+    mean-free N(0,1) pressure right-hand side.  One step: the prepare with its
+    support screen, one IB_4 spread, one IB_4 interpolate and the multigrid
+    solve to 1e-10 relative residual.  GPU: CUDA events around `steps` steps
+    after 5 warm-up steps.  CPU: the oracle (NumPy, one process), median of
+    `cpu_reps` steps.  Errors against the oracle's outputs."""
+    from afsi_gpu_b200 import cuda_ib, synthetic
+    from afsi_gpu_b200.grid import ChannelGrid
+    from afsi_gpu_b200.multigrid import ChannelMultigrid
+    from oracle import ib as oib, mg as omg
+    grid = ChannelGrid((256, 64), (1., .25), periodic=True)
+    pts = synthetic.ellipse_points(20000, spacing=1 / 256, seed=3)
+    force = np.random.default_rng(5).standard_normal((20000, 2))
+    vel = [v.numpy() for v in synthetic.fourier_velocity2d(grid, seed=2)]
+    rhs = synthetic.mean_free_normal(grid.shape, seed=6).numpy()
+    x, fd = torch.as_tensor(pts, device=device), torch.as_tensor(force, device=device)
+    vd, rd = tuple(torch.as_tensor(v, device=device) for v in vel), torch.as_tensor(rhs, device=device)
+    mg = ChannelMultigrid(grid, device=device, backend='b200-graph')
+
+    def step():
+        st = cuda_ib.prepare2d(grid, x)
+        return cuda_ib.spread2d(grid, fd, st), cuda_ib.gather2d(vd, st), mg.solve(rd)
+
+    for _ in range(5):
+        out = step()
+    stream = torch.cuda.current_stream(device)
+    torch.cuda.synchronize(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        out = step()
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    ms = e0.elapsed_time(e1) / steps
+    h = omg.Hierarchy(grid.shape, grid.spacing, 'periodic')
+    times = []
+    for _ in range(cpu_reps):
+        t0 = time.perf_counter()
+        ids, w = oib.prepare2d(pts, grid.shape, grid.spacing)
+        sp = [oib.indexed_spread(force[:, c], ids[c], w[c], vel[c].size, grid.volume) for c in range(2)]
+        ga = np.stack([oib.indexed_gather(vel[c], ids[c], w[c]) for c in range(2)], -1)
+        pref, info = omg.solve(h, rhs)
+        times.append(time.perf_counter() - t0)
+    fields, gathered, (p, ginfo) = out
+    return dict(workload='2D 256x64 MAC (1.0 x 0.25), periodic x / walls y, 20,000 ellipse points, FP64',
+                steps_per_s=1e3 / ms, ms_per_step=ms, cycles=ginfo['cycles'], cycles_oracle=info['cycles'],
+                residual=ginfo['residual_norm'], tolerance=ginfo['tolerance'],
+                cpu_baseline=dict(steps_per_s=1 / float(np.median(times)), ms_per_step=float(np.median(times)) * 1e3,
+                                  cores=1, kind='port', sample=f'whole step, median of {cpu_reps}'),
+                error_vs_oracle=dict(spread=max(rel_err(fields[c].reshape(-1).cpu(), sp[c]) for c in range(2)),
+                                     interpolate=rel_err(gathered.cpu(), ga), pressure=rel_err(p.cpu(), pref)))
 
 
 def serving_form_row(device, count=400):
@@ -384,12 +482,15 @@ def serving_form_row(device, count=400):
     return out
 
 
-def precision_form_row(grid, X, cells, coef, vel, rhs, device, steps=20):
-    """Precision form of the step on the bench workload: FP64 positions and
-    bases, FP32 weight tables and transfers, and the pressure solve as FP32
-    V-cycles inside FP64 iterative refinement to the FP64 tolerance.  CUDA
-    events around `steps` steps; errors are the largest differences from the
-    FP64 step's outputs over their largest values."""
+def precision_form_row(grid, X, cells, coef, vel, rhs, device, oracle_out=None, steps=20):
+    """Precision forms of the step on the bench workload, each timed with CUDA
+    events around `steps` steps beside the plain FP64 step: FP64 positions and
+    bases always; weight tables and transfers in FP64 or FP32; the pressure
+    solve as FP64 V-cycles or as FP32 V-cycles inside FP64 iterative
+    refinement, always to the FP64 tolerance.  Errors are max |form - oracle| /
+    max |oracle| against the full-size FP64 oracle outputs (or, without them,
+    against the GPU FP64 step), and meets_1e_8 says whether every output is
+    within 1e-8."""
     from afsi_gpu_b200 import p2_cuda_transfer as p2t
     from afsi_gpu_b200.multigrid import GeometricMultigrid, RefinedMultigrid
     x = torch.as_tensor(X, device=device)
@@ -401,41 +502,51 @@ def precision_form_row(grid, X, cells, coef, vel, rhs, device, steps=20):
     mg64 = GeometricMultigrid(grid, device=device, backend='b200-graph')
     mg32 = RefinedMultigrid(grid, device=device)
     c32, v32 = c64.float(), tuple(v.float() for v in v64)
+    stream = torch.cuda.current_stream(device)
 
     def step(tr, mg, c, v):
         st = tr.prepare(x)
         return tr.spread(c, st), tr.assemble_velocity(v, st), mg.solve(r64)
 
-    ref = step(tr64, mg64, c64, v64)
-    stream = torch.cuda.current_stream(device)
-
-    def timed(mg):
+    def timed(*args):
         for _ in range(3):
-            out = step(tr32, mg, c32, v32)
+            out = step(*args)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize(device)
         e0.record(stream)
         for _ in range(steps):
-            out = step(tr32, mg, c32, v32)
+            out = step(*args)
         e1.record(stream)
         torch.cuda.synchronize(device)
         return out, e0.elapsed_time(e1) / steps
 
-    def rel(a, b):
-        return float((a.double() - b.double()).abs().max() / b.double().abs().max())
+    plain, plain_ms = timed(tr64, mg64, c64, v64)
+    if oracle_out is not None:
+        ref = ([np.asarray(f) for f in oracle_out['fields']], oracle_out['nodal'], oracle_out['p'])
+        against = 'full-size FP64 oracle'
+    else:
+        ref = ([f.cpu() for f in plain[0]], plain[1].cpu(), plain[2][0].cpu())
+        against = 'GPU FP64 step'
 
-    rows = {}
-    for name, mg in (('fp32_transfers_refined_mg', mg32), ('fp32_transfers_fp64_mg', mg64)):
-        out, ms = timed(mg)
+    def errors(out):
+        return dict(spread=max(rel_err(a.cpu(), b) for a, b in zip(out[0], ref[0])),
+                    gather_assemble=rel_err(out[1].cpu(), ref[1]), pressure=rel_err(out[2][0].cpu(), ref[2]))
+
+    rows = dict(plain_fp64=dict(steps_per_s=1e3 / plain_ms, ms_per_step=plain_ms, error_vs_oracle=errors(plain)))
+    for name, tr, mg, c, v in (('fp64_transfers_refined_mg', tr64, mg32, c64, v64),
+                               ('fp32_transfers_refined_mg', tr32, mg32, c32, v32),
+                               ('fp32_transfers_fp64_mg', tr32, mg64, c32, v32)):
+        out, ms = timed(tr, mg, c, v)
         info = out[2][1]
-        rows[name] = dict(steps_per_s=1e3 / ms, ms_per_step=ms, transfer_dtype='f32', positions='f64',
+        err = errors(out)
+        rows[name] = dict(steps_per_s=1e3 / ms, ms_per_step=ms, speedup_vs_plain_fp64=plain_ms / ms,
+                          transfer_dtype='f64' if tr is tr64 else 'f32', positions='f64',
                           mg=(f"FP32 V-cycles in FP64 refinement, {info['refinements']} refinements, "
                               f"{info['cycles']} FP32 cycles" if 'refinements' in info else
                               f"FP64 V-cycles, {info['cycles']} cycles"),
                           residual=info['residual_norm'], tolerance=info['tolerance'],
-                          error_vs_fp64=dict(spread=max(rel(a, b) for a, b in zip(out[0], ref[0])),
-                                             gather_assemble=rel(out[1], ref[1]),
-                                             pressure=rel(out[2][0], ref[2][0])))
+                          error_vs_oracle=err, meets_1e_8=bool(max(err.values()) <= 1e-8))
+    rows['errors_against'] = against
     return rows
 
 
@@ -493,26 +604,66 @@ def precision_p1_row(device, steps=5):
             ms.append(e0.elapsed_time(e1))
         return out, float(np.median(ms))
 
-    def rel(a, b):
-        return float((a.double() - b.double()).abs().max() / b.double().abs().max())
-
     ref, ms64 = timed(tr64, mg64, c64, v64)
     out, ms32 = timed(tr32, mg32, c32, v32)
     info64, info32 = ref[2][1], out[2][1]
+    oracle = p1_oracle_errors(grid, X, cells, c64, v64, r64, device, dict(plain_fp64=(ref[2][0], None),
+                                                                          precision_form=(out[2][0],
+                                                                                          torch.float32)))
     return dict(workload=(f'128^3 MAC, P1 prolate shell {cells.shape[0]} elements / '
                           f'{ref[3].rule.point_count} points, uniform [-1,1] forces'),
                 points=int(ref[3].rule.point_count), elements=int(cells.shape[0]),
                 csr_nnz=int(ref[3].assembly['total_nnz']),
                 plain_fp64=dict(steps_per_s=1e3 / ms64, ms_per_step=ms64, cycles=info64['cycles'],
-                                residual=info64['residual_norm'], tolerance=info64['tolerance']),
+                                residual=info64['residual_norm'], tolerance=info64['tolerance'],
+                                error_vs_oracle=oracle['plain_fp64']),
                 precision_form=dict(steps_per_s=1e3 / ms32, ms_per_step=ms32, transfer_dtype='f32',
                                     positions='f64',
                                     mg=(f"FP32 V-cycles in FP64 refinement, {info32['refinements']} refinements, "
                                         f"{info32['cycles']} FP32 cycles"),
-                                    residual=info32['residual_norm'], tolerance=info32['tolerance']),
-                speedup_vs_plain_fp64=ms64 / ms32,
-                error_vs_fp64=dict(spread=max(rel(a, b) for a, b in zip(out[0], ref[0])),
-                                   interpolate=rel(out[1], ref[1]), pressure=rel(out[2][0], ref[2][0])))
+                                    residual=info32['residual_norm'], tolerance=info32['tolerance'],
+                                    error_vs_oracle=oracle['precision_form']),
+                speedup_vs_plain_fp64=ms64 / ms32, oracle_sample=oracle['sample'])
+
+
+def p1_oracle_errors(grid, X, cells, coef, vel, rhs, device, forms, sample_elements=2000):
+    """Errors of the P1 forms against the FP64 oracle.  Transfers on an
+    element sample (every k-th element of the shell, so the sample spans it):
+    the form's transfer built on the sampled cells alone, its spread and
+    interpolate against the oracle's P1 quadrature transfer with the same rule
+    (x_q = N x, F_q = (N coef) W, spread over the shared tables, U_q gathered
+    and assembled with N W).  Pressure: the full 128^3 oracle solve to 1e-10.
+    forms: name -> (pressure from the timed step, transfer dtype or None)."""
+    from afsi_gpu_b200.p1_csr import P1CSRTransfer
+    from oracle import ib as oib, mg as omg
+    k = max(1, cells.shape[0] // sample_elements)
+    sub = np.ascontiguousarray(cells[::k][:sample_elements])
+    x = torch.as_tensor(X, device=device)
+    pref, _ = omg.solve(omg.Hierarchy(grid.shape, grid.spacing, 'neumann'), rhs.cpu().numpy())
+    coef_np = coef.cpu().numpy()
+    vel_np = [v.cpu().numpy() for v in vel]
+    out = dict(sample=f'transfers on {sub.shape[0]} of {cells.shape[0]} elements (every {k}th); '
+                      f'pressure on the full grid')
+    oracle_ref = None
+    for name, (p, dtype) in forms.items():
+        kw = {} if dtype is None else dict(transfer_dtype=dtype)
+        tr = P1CSRTransfer(grid, x, torch.as_tensor(sub, device=device), **kw)
+        st = tr.prepare(x)
+        cd = coef if dtype is None else coef.to(dtype)
+        vd = vel if dtype is None else tuple(v.to(dtype) for v in vel)
+        fields = tr.spread(cd, st)
+        nodal = tr.interpolate_rhs(vd, st)
+        if oracle_ref is None:
+            groups = [(g.cells.cpu().numpy(), g.values.cpu().numpy(), g.weights.cpu().numpy())
+                      for g in st.rule.groups]
+            base, phi, _ = oib.p2_prepare(X, [(c, N) for c, N, _ in groups], grid.origin, grid.spacing,
+                                          grid.shape)
+            oracle_ref = (oib.p2_spread(coef_np, groups, base, phi, grid.shape, grid.volume),
+                          oib.p2_gather_assemble(vel_np, groups, base, phi, grid.shape, X.shape[0]))
+        out[name] = dict(spread=max(rel_err(f.cpu(), o) for f, o in zip(fields, oracle_ref[0])),
+                         interpolate=rel_err(nodal.cpu(), oracle_ref[1]), pressure=rel_err(p.cpu(), pref))
+        out[name]['meets_1e_8'] = bool(max(out[name].values()) <= 1e-8)
+    return out
 
 
 def deterministic_row(step, coef, device, reps=10):
@@ -562,55 +713,99 @@ def peaks():
 
 # ----------------------------------------------------------- cpu baselines
 
-def cpu_step_time(grid, X, cells, coef, vel, rhs, fraction=0.05):
-    """Oracle (NumPy port of the reference algorithm) on a bounded sample:
-    the first `fraction` of the elements for the transfers (time scaled by the
-    point ratio) and the full 64^3 multigrid solve."""
-    from oracle import ib, mg
-    from afsi_gpu_b200.quadrature import conical_rule, tabulate_p2, reference_determinants
-    E = cells.shape[0]
-    Es = max(1, int(E * fraction))
-    sub = cells[:Es]
-    q, w = conical_rule(4)
-    N = tabulate_p2(q)
-    W = reference_determinants(torch.as_tensor(X), torch.as_tensor(sub)).numpy()[:, None] * w
-    t0 = time.perf_counter()
-    base, phi, _ = ib.p2_prepare(X, [(sub, N)], grid.origin, grid.spacing, grid.shape)
-    fields = ib.p2_spread(coef, [(sub, N, W)], base, phi, grid.shape, grid.volume)
-    nodal = ib.p2_gather_assemble(vel, [(sub, N, W)], base, phi, grid.shape, X.shape[0])
-    t1 = time.perf_counter()
-    h = mg.Hierarchy(grid.shape, grid.spacing, 'neumann')
-    p, info = mg.solve(h, rhs)
-    t2 = time.perf_counter()
-    transfer = (t1 - t0) * (E / Es)
-    outputs = dict(sub=sub, N=N, W=W, fields=fields, nodal=nodal, p=p, cycles=info['cycles'])
-    return transfer + (t2 - t1), dict(transfer_s=transfer, mg_s=t2 - t1, elements_sampled=Es, elements=E), outputs
+class OracleRun:
+    """The oracle (NumPy restatement of the reference's CPU path) on the WHOLE
+    bench workload per step: the P2 prepare, spread and gather-assemble of all
+    elements, split over a spawn pool of single-threaded worker processes (one
+    per host core), then the 64^3 multigrid solve in this process.  Used as the
+    reference arm, as the GPU arm's CPU baseline, and as the full-size oracle
+    the GPU outputs are checked against.  Nothing is sampled or scaled."""
+
+    def __init__(self, grid, X, cells, coef, vel, rhs, workers=None):
+        import multiprocessing as mp
+        from oracle import mg
+        self.workers = workers or max(1, len(os.sched_getaffinity(0)))
+        for var in ('OMP_NUM_THREADS', 'OPENBLAS_NUM_THREADS', 'MKL_NUM_THREADS'):
+            os.environ[var] = '1'  # inherited by the spawned workers
+        from multiprocessing import shared_memory
+        self.face_sizes = [int(np.prod(grid.face_shape(c))) for c in range(3)]
+        self.nodes = int(X.shape[0])
+        self.slot_floats = sum(self.face_sizes) + 3 * self.nodes
+        # one output slot per worker task, summed here (no result pickling)
+        self.shm = shared_memory.SharedMemory(create=True, size=self.workers * self.slot_floats * 8)
+        init = (X, coef, vel, tuple(grid.shape), tuple(grid.lengths), tuple(grid.origin), self.shm.name,
+                self.slot_floats)
+        # every worker is started up front (a spawn pool: no fork after CUDA)
+        self.pool = mp.get_context('spawn').Pool(self.workers, initializer=_oracle_worker_init, initargs=init)
+        self.pool.map(_oracle_transfer_chunk, [(k, cells[:8]) for k in range(self.workers)], chunksize=1)
+        self.tasks = [(k, cells[c]) for k, c in enumerate(np.array_split(np.arange(cells.shape[0]), self.workers))]
+        self.grid = grid
+        self.hierarchy = mg.Hierarchy(grid.shape, grid.spacing, 'neumann')
+        self.rhs = rhs
+        self.elements = int(cells.shape[0])
+
+    def step(self):
+        """One oracle step; returns (outputs, phase seconds, step seconds)."""
+        from oracle import mg
+        t0 = time.perf_counter()
+        parts = self.pool.map(_oracle_transfer_chunk, self.tasks, chunksize=1)
+        slots = np.ndarray((self.workers, self.slot_floats), dtype=np.float64, buffer=self.shm.buf)
+        total = slots.sum(0)
+        cut = np.cumsum([0] + self.face_sizes)
+        fields = [total[cut[c]:cut[c + 1]].reshape(self.grid.face_shape(c)) for c in range(3)]
+        nodal = total[cut[3]:].reshape(self.nodes, 3)
+        del slots
+        t1 = time.perf_counter()
+        p, info = mg.solve(self.hierarchy, self.rhs)
+        t2 = time.perf_counter()
+        worst = np.max(parts, axis=0)  # slowest worker per phase
+        phases = dict(prepare=float(worst[0]), spread=float(worst[1]), gather_assemble=float(worst[2]),
+                      transfers_wall=t1 - t0, mg_solve=t2 - t1)
+        return dict(fields=fields, nodal=nodal, p=p, cycles=info['cycles']), phases, t2 - t0
+
+    def run(self, steps, warmup):
+        times, phases, out = [], [], None
+        for i in range(warmup + steps):
+            out, ph, dt = self.step()
+            if i >= warmup:
+                times.append(dt)
+                phases.append(ph)
+        return out, times, phases
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+        self.shm.close()
+        self.shm.unlink()
+
+    def sample(self, steps, warmup):
+        return (f'oracle (NumPy restatement of the reference CPU path, FP64) on the whole workload every step: '
+                f'P2 prepare/spread/gather-assemble of all {self.elements} elements split over {self.workers} '
+                f'single-threaded worker processes, then the full 64^3 MG solve to 1e-10; {steps} steps after '
+                f'{warmup} warm-up, nothing scaled')
 
 
-def oracle_errors(step, X, coef, vel, outputs, p_device):
-    """Relative errors (max |device - oracle| / max |oracle|) of the step's
-    outputs against the FP64 oracle: spread and gather-assemble on the
-    oracle's element sample (same cells, rule and weights), and the 64^3
-    pressure solve of the timed steps."""
-    from afsi_gpu_b200 import p2_cuda_transfer as p2t
-    from afsi_gpu_b200.quadrature import InteractionRule, QuadratureGroup
-    dev = step.x.device
-    group = QuadratureGroup(torch.as_tensor(outputs['sub'], device=dev),
-                            torch.as_tensor(outputs['N'], device=dev, dtype=torch.float64),
-                            torch.as_tensor(outputs['W'], device=dev, dtype=torch.float64), 4)
-    rule = InteractionRule((group,), None, group.weights.numel())
-    base, phi = p2t.prepare(step.tr, step.x, rule)
-    st = p2t.SharedAdaptiveStencil(base, phi, rule)
-    fields = p2t.spread(step.tr, step.coef, st)
-    nodal = p2t.assemble_velocity(step.tr, step.vel, st)
+def phase_stats(phases):
+    """Median and p90 (ms) of each phase over the timed steps."""
+    out = {}
+    for k in phases[0]:
+        v = np.array([ph[k] for ph in phases]) * 1e3
+        out[k] = dict(median_ms=float(np.median(v)), p90_ms=float(np.percentile(v, 90)))
+    return out
 
-    def rel(a, b):
-        b = np.asarray(b)
-        return float(np.abs(np.asarray(a).reshape(b.shape) - b).max() / max(np.abs(b).max(), 1e-300))
-    return dict(spread=max(rel(f.cpu().numpy(), o) for f, o in zip(fields, outputs['fields'])),
-                gather_assemble=rel(nodal.cpu().numpy(), outputs['nodal']),
-                mg_solve=rel(p_device, outputs['p']), mg_cycles_oracle=int(outputs['cycles']),
-                sample='spread/gather on the CPU-baseline element sample; MG on the full 64^3 solve')
+
+def rel_err(a, b):
+    """max |a - b| / max |b| (FP64)."""
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    return float(np.abs(a.reshape(b.shape) - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def oracle_errors(outputs, fields, nodal, p):
+    """Errors of the GPU step's outputs against the full-size FP64 oracle."""
+    return dict(spread=max(rel_err(f, o) for f, o in zip(fields, outputs['fields'])),
+                gather_assemble=rel_err(nodal, outputs['nodal']), mg_solve=rel_err(p, outputs['p']),
+                mg_cycles_oracle=int(outputs['cycles']),
+                sample='all elements and points of the workload (no sample); max |gpu - oracle| / max |oracle|')
 
 
 # --------------------------------------------------------------------- main
@@ -652,29 +847,38 @@ def dist_setup(args):
 _ORACLE = {}
 
 
-def _oracle_worker_init(X, coef, vel, shape, lengths, origin):
-    """Reference-arm worker set-up: the step's static inputs, the rule tables
-    and the oracle import, once per worker process."""
+def _oracle_worker_init(X, coef, vel, shape, lengths, origin, shm_name, slot_floats):
+    """Reference-arm worker set-up: the step's static inputs, the rule tables,
+    the oracle import and the shared-memory output slots, once per worker."""
+    from multiprocessing import shared_memory
     from afsi_gpu_b200.quadrature import conical_rule, tabulate_p2
     torch.set_num_threads(1)  # one core per worker: the workers are the parallelism
     q, w = conical_rule(4)
     spacing = tuple(L / n for L, n in zip(lengths, shape))
+    shm = shared_memory.SharedMemory(name=shm_name)
     _ORACLE.update(X=X, coef=coef, vel=vel, shape=shape, origin=origin, spacing=spacing,
-                   volume=float(np.prod(spacing)), N=tabulate_p2(q), w=w)
+                   volume=float(np.prod(spacing)), N=tabulate_p2(q), w=w, shm=shm, slot_floats=slot_floats)
 
 
-def _oracle_transfer_chunk(cells):
-    """One worker's share of the reference arm: the oracle prepare, spread and
-    gather-assemble of a chunk of elements (top level, so that a spawn pool
-    can call it)."""
+def _oracle_transfer_chunk(task):
+    """One worker's share of an oracle step: the prepare, spread and
+    gather-assemble of a chunk of elements, written into output slot `slot`
+    of the shared block (top level, so that a spawn pool can call it)."""
     from oracle import ib
     from afsi_gpu_b200.quadrature import reference_determinants
+    slot, cells = task
     o = _ORACLE
+    t0 = time.perf_counter()
     W = reference_determinants(torch.as_tensor(o['X']), torch.as_tensor(cells)).numpy()[:, None] * o['w']
     base, phi, _ = ib.p2_prepare(o['X'], [(cells, o['N'])], o['origin'], o['spacing'], o['shape'])
+    t1 = time.perf_counter()
     fields = ib.p2_spread(o['coef'], [(cells, o['N'], W)], base, phi, o['shape'], o['volume'])
+    t2 = time.perf_counter()
     nodal = ib.p2_gather_assemble(o['vel'], [(cells, o['N'], W)], base, phi, o['shape'], o['X'].shape[0])
-    return fields, nodal
+    t3 = time.perf_counter()
+    out = np.ndarray((o['slot_floats'],), dtype=np.float64, buffer=o['shm'].buf, offset=slot * o['slot_floats'] * 8)
+    np.concatenate([f.reshape(-1) for f in fields] + [nodal.reshape(-1)], out=out)
+    return t1 - t0, t2 - t1, t3 - t2
 
 
 def run_reference(args):
@@ -684,56 +888,21 @@ def run_reference(args):
             dist.destroy_process_group()
         return
     grid, X, cells, coef, vel, rhs = workload()
-    import multiprocessing as mp
-    from concurrent.futures import ProcessPoolExecutor
-    from oracle import mg
-    cores = max(1, len(os.sched_getaffinity(0)))
-    E = cells.shape[0]
-    times = []
-    warm, timed = min(args.warmup, 1), min(args.steps, 10)
-    init = (X, coef, vel, tuple(grid.shape), tuple(grid.lengths), tuple(grid.origin))
-    for var in ('OMP_NUM_THREADS', 'OPENBLAS_NUM_THREADS', 'MKL_NUM_THREADS'):
-        os.environ[var] = '1'  # inherited by the spawned workers
-    with ProcessPoolExecutor(max_workers=cores, mp_context=mp.get_context('spawn'), initializer=_oracle_worker_init,
-                             initargs=init) as pool:
-        list(pool.map(_oracle_transfer_chunk, [cells[:8]] * cores))  # start every worker, import the oracle
-        # use the worker count with the best element throughput on this host
-        # (hosts whose cores share memory bandwidth stop scaling early)
-        best = None
-        k = 1
-        while k <= cores:
-            t0 = time.perf_counter()
-            list(pool.map(_oracle_transfer_chunk, [cells[i * 512:(i + 1) * 512] for i in range(k)]))
-            rate = k * 512 / (time.perf_counter() - t0)
-            if best is None or rate > best[0]:
-                best = (rate, k)
-            k = k * 2 if k * 2 <= cores or k == cores else cores
-        workers = best[1]
-        Es = min(E, 512 * workers)  # element sample: 512 per worker, time scaled by E / Es
-        tasks = [cells[c] for c in np.array_split(np.arange(Es), workers)]
-        h = mg.Hierarchy(grid.shape, grid.spacing, 'neumann')
-        for i in range(warm + timed):
-            t0 = time.perf_counter()
-            parts = list(pool.map(_oracle_transfer_chunk, tasks))
-            fields = [sum(p[0][c] for p in parts) for c in range(3)]
-            nodal = sum(p[1] for p in parts)
-            t1 = time.perf_counter()
-            p, info = mg.solve(h, rhs)
-            t2 = time.perf_counter()
-            if i >= warm:
-                times.append((t1 - t0) * (E / Es) + (t2 - t1))
+    run = OracleRun(grid, X, cells, coef, vel, rhs)
+    try:
+        _, times, phases = run.run(args.steps, args.warmup)
+    finally:
+        run.close()
     step = float(np.mean(times))
-    sample = (f'oracle (NumPy restatement of the reference CPU path): P2 prepare/spread/gather-assemble on '
-              f'{Es} of {E} elements split over {workers} worker processes (the fastest count of 1..{cores} '
-              f'host cores), time scaled by elements; full 64^3 MG solve in one process; {timed} steps after '
-              f'{warm} warm-up')
-    cores = workers
     value = 1.0 / step
-    line = dict(metric=METRIC, value=value, unit='steps/s', impl='reference', n_gpus=args.gpus, steps=timed,
-                warmup=warm, ms_per_step=step * 1e3, higher_is_better=True, scaling='weak',
-                vs_baseline=None, dtype='f64', data='synthetic',
-                config=dict(workload='3D P2 shell 38400 elements / 2457600 points, 64^3 MAC, FP64'),
-                cpu_baseline=dict(value=value, unit='steps/s', cores=cores, kind='port', sample=sample),
+    sample = run.sample(args.steps, args.warmup)
+    line = dict(metric=METRIC, value=value, unit='steps/s', impl='reference', n_gpus=args.gpus, steps=args.steps,
+                warmup=args.warmup, ms_per_step=step * 1e3, higher_is_better=True, scaling='weak',
+                vs_baseline=None, dtype='f64', data='synthetic', config=dict(workload=WORKLOAD),
+                latency_ms=dict(p50=float(np.percentile(times, 50)) * 1e3, p90=float(np.percentile(times, 90)) * 1e3,
+                                p99=float(np.percentile(times, 99)) * 1e3),
+                phases=phase_stats(phases),
+                cpu_baseline=dict(value=value, unit='steps/s', cores=run.workers, kind='port', sample=sample),
                 e2e=dict(value=value, unit='steps/s', h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line, default=_json))
     if dist:
@@ -853,27 +1022,34 @@ def run_b200(args):
         traffic = load_traffic().get(dominant)
         cpu = None
         errors = None
+        oracle_out = None
         if not args.no_cpu_baseline:
-            cpu_t, info, outputs = cpu_step_time(grid, X, cells, coef, vel, rhs, fraction=0.05)
-            cpu = dict(value=1 / cpu_t, unit='steps/s', cores=1, kind='port',
-                       sample=(f'oracle (NumPy restatement) on {info["elements_sampled"]} of {info["elements"]} '
-                               f'elements for the transfers (scaled by element count) + full 64^3 MG solve'))
-            errors = oracle_errors(step, X, coef, vel, outputs, final[-1].numpy())
+            # the reference arm's measurement on a bounded number of steps; its
+            # outputs are the full-size FP64 oracle for the error check
+            run = OracleRun(grid, X, cells, coef, vel, rhs)
+            try:
+                oracle_out, cpu_times, cpu_phases = run.run(2, 1)
+            finally:
+                run.close()
+            cpu = dict(value=1 / float(np.mean(cpu_times)), unit='steps/s', cores=run.workers, kind='port',
+                       sample=run.sample(2, 1), phases=phase_stats(cpu_phases))
+            errors = oracle_errors(oracle_out, [t.numpy() for t in final[:3]], final[3].numpy(), final[4].numpy())
         extra = args.rows == 'all'
         mass = mass_pcg_row(X, cells, device, pk['hbm_gbs']) if extra else None
         forms = mg_forms_row(grid, rhs, device) if extra else None
-        precision = precision_form_row(grid, X, cells, coef, vel, rhs, device) if extra else None
+        precision = precision_form_row(grid, X, cells, coef, vel, rhs, device, oracle_out) if extra else None
         if extra:
             precision['p1_128'] = precision_p1_row(device)
         deterministic = deterministic_row(step, coef, device) if extra else None
         batch = batch_form_row(device) if extra else None
+        config1 = config1_row(device) if extra else None
         serving = serving_form_row(device) if extra else None
         step_ms = np.array([ev[0].elapsed_time(ev[4]) for ev in phases])
         line = dict(
             metric=METRIC, value=whole_job_rate(world, args.steps, elapsed), unit='steps/s', n_gpus=world, steps=args.steps,
             warmup=args.warmup, ms_per_step=elapsed / args.steps * 1e3, higher_is_better=True, scaling='weak',
             vs_baseline=None, dtype='f64', data='synthetic',
-            config=dict(workload='3D P2 shell 38400 elements / 2457600 points, 64^3 MAC, FP64',
+            config=dict(workload=WORKLOAD,
                         grid=list(GRID['shape']), elements=int(cells.shape[0]), points=int(P),
                         mg='Neumann V-cycles to 1e-10, Jacobi 2/3 x4, graph-replayed blocks of 2, cycles per solve '
                            f'{sorted(set(step.cycles))}',
@@ -896,6 +1072,7 @@ def run_b200(args):
             precision_form=precision,
             deterministic_spread=deterministic,
             batch_form=batch,
+            config1=config1,
             serving_form=serving,
             cpu_baseline=cpu)
         print(json.dumps(line, default=_json))
@@ -903,10 +1080,27 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+def batch_only(args):
+    """Replays of the refined batch step (64 instances, FP64 transfers, 5
+    V-cycles per refinement) for profiler runs."""
+    from afsi_gpu_b200.batch import Schedule, seeded_batch
+    device = torch.device('cuda', torch.cuda.current_device())
+    b = seeded_batch(64, seed=0, device=device, transfer_dtype=torch.float64)
+    b.use(Schedule(streams=1, order='given', smoother='jacobi', cycles=5, vcycles='batched', refined=True))
+    for _ in range(args.warmup):
+        b.replay()
+    ms = _time_replays(b, args.steps, device)
+    rep = b.refined_report()
+    print(json.dumps(dict(ms_per_batch_step=ms, refinements=rep['refinements'], unconverged=rep['unconverged'],
+                          launches_per_step=b.graph_launches + b.refinement().launches(5))))
+
+
 def main():
     args = parse()
     if args.impl == 'reference':
         run_reference(args)
+    elif args.rows == 'batch':
+        batch_only(args)
     elif args.rows == 'p1':
         print(json.dumps(precision_p1_row(torch.device('cuda', torch.cuda.current_device())), default=_json))
     else:
