@@ -148,6 +148,13 @@ _SIGNATURES = {
                                             c_double, c_int32, c_void_p],
     'afsi_b200_batch_refine_graph_launch': [c_void_p, c_void_p],
     'afsi_b200_batch_refine_graph_destroy': [c_void_p],
+    'afsi_b200_stokes_packed_size': [P_I64],
+    'afsi_b200_stokes_precondition_scratch_bytes': [P_I64],
+    'afsi_b200_stokes_action': [c_void_p, c_void_p, P_I64, P_F64, c_double, c_double, c_int32, c_void_p],
+    'afsi_b200_stokes_precondition_rhs': [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, P_I64, P_F64, c_double,
+                                          c_int32, c_void_p],
+    'afsi_b200_stokes_precondition_result': [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, P_I64,
+                                             P_F64, c_double, c_double, c_int32, c_void_p],
     'afsi_b200_batch2d_prepare': [c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_int32,
                                   c_void_p],
     'afsi_b200_batch2d_spread': [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_void_p,
@@ -179,6 +186,8 @@ _SIGNATURES = {
 _RESTYPES = {'afsi_b200_last_error': ctypes.c_char_p, 'afsi_b200_mg_scratch_bytes': ctypes.c_int64,
              'afsi_b200_mg_batch_table_bytes': ctypes.c_int64, 'afsi_b200_batch_refine_bytes': ctypes.c_int64,
              'afsi_b200_batch_refine_state_offset': ctypes.c_int64,
+             'afsi_b200_stokes_packed_size': ctypes.c_int64,
+             'afsi_b200_stokes_precondition_scratch_bytes': ctypes.c_int64,
              'afsi_b200_launch_count': ctypes.c_int64, 'afsi_b200_mg_sync_bytes': ctypes.c_int64,
              'afsi_b200_p1_plan_scratch_bytes': ctypes.c_int64, 'afsi_b200_hash_csr_scratch_bytes': ctypes.c_int64,
              'afsi_b200_pcg_scratch_bytes': ctypes.c_int64, 'afsi_b200_mg_refine_scratch_bytes': ctypes.c_int64,

@@ -126,3 +126,25 @@ def mean_free_normal(shape, seed=0, dtype=torch.float64):
     g = torch.Generator().manual_seed(seed)
     r = torch.randn(shape, generator=g, dtype=torch.float64)
     return (r - r.mean()).to(dtype)
+
+
+def divergence_free_faces(grid, seed=0):
+    """Seeded face field with zero discrete divergence and zero wall-normal
+    flux: the discrete curl of random edge potentials that vanish on every
+    boundary edge (each potential lives on the cell edges along its axis)."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = grid.shape
+    hx, hy, hz = grid.spacing
+    pot = []
+    for shape in ((nx, ny + 1, nz + 1), (nx + 1, ny, nz + 1), (nx + 1, ny + 1, nz)):
+        a = rng.standard_normal(shape)
+        for axis, n in enumerate(shape):
+            if n != (nx, ny, nz)[axis]:  # node axes: clear both boundary planes
+                a[(slice(None),) * axis + (0,)] = 0.
+                a[(slice(None),) * axis + (n - 1,)] = 0.
+        pot.append(a)
+    ax, ay, az = pot
+    u = np.diff(az, axis=1) / hy - np.diff(ay, axis=2) / hz
+    v = np.diff(ax, axis=2) / hz - np.diff(az, axis=0) / hx
+    w = np.diff(ay, axis=0) / hx - np.diff(ax, axis=1) / hy
+    return tuple(torch.as_tensor(f) for f in (u, v, w))

@@ -395,6 +395,60 @@ def batch_form_row(device, count=64, replays=20, oracle_instances=6):
                                     meets_1e_8=bool(max(err32.values()) <= 1e-8)))
 
 
+STOKES = dict(dt=1e-3, rho=1., mu=.01)
+
+
+def stokes_row(grid, device, solves=5):
+    """Config 2's Stokes solve, timed as its own row: the CN saddle point
+    H u + (dt/rho) G p = b, D u = 0 on the 64^3 grid (dt 1e-3, rho 1, mu 0.01:
+    14 Helmholtz sweeps per solve), b a seeded divergence-free face field (the
+    discrete curl of random edge potentials), solved by MG-preconditioned
+    FGMRES to the reference's acceptance test (restart 20, preconditioner
+    multigrid to 0.01).  FP64, and the precision form (FP32 preconditioner
+    inside the FP64 FGMRES).  CUDA events around `solves` solves after one
+    warm-up solve; CPU: the oracle's FGMRES (NumPy, one process), one solve;
+    errors against the oracle's solution."""
+    from afsi_gpu_b200 import synthetic
+    from afsi_gpu_b200.stokes_fgmres import CNStokes
+    from oracle import stokes as ostokes, mg as omg
+    b = synthetic.divergence_free_faces(grid, seed=8)
+    bd = tuple(t.to(device) for t in b)
+    stream = torch.cuda.current_stream(device)
+    P = ostokes.StokesProblem(grid.shape, grid.spacing, STOKES['dt'], STOKES['rho'], STOKES['mu'],
+                              omg.Hierarchy(grid.shape, grid.spacing, 'neumann'))
+    t0 = time.perf_counter()
+    u_ref, p_ref, oinfo = ostokes.fgmres_solve(P, [t.numpy() for t in b])
+    cpu_s = time.perf_counter() - t0
+    out = dict(workload='64^3 MAC, CN saddle point, divergence-free seeded RHS, dt 1e-3 rho 1 mu 0.01',
+               cpu_baseline=dict(ms_per_solve=cpu_s * 1e3, cores=1, kind='port',
+                                 sample='one whole FGMRES solve of the oracle (NumPy restatement)',
+                                 iterations=oinfo['iterations'], poisson_solves=oinfo['poisson_solves']))
+    for precision in ('fp64', 'fp32-preconditioner'):
+        flow = CNStokes(grid, device=device, precision=precision, **STOKES)
+        res = flow.stokes(bd)
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(solves):
+            res = flow.stokes(bd)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        ms = e0.elapsed_time(e1) / solves
+        st, pr = res.diagnostics['stokes'], res.diagnostics['pressure']
+        err = dict(velocity=max(rel_err(res.velocity[c].cpu(), u_ref[c]) for c in range(3)),
+                   pressure=rel_err(res.pressure.cpu(), p_ref))
+        out[precision] = dict(ms_per_solve=ms, solves_per_s=1e3 / ms, iterations=st['iterations'],
+                              operator_actions=st['operator_actions'], poisson_solves=pr['poisson_solves'],
+                              v_cycles=pr['cycles'], helmholtz_sweeps_per_solve=st['helmholtz_iterations'],
+                              momentum=[st['momentum_residual'], st['momentum_tolerance']],
+                              divergence=[st['divergence_norm'], st['divergence_tolerance']],
+                              error_vs_oracle=err, meets_1e_8=bool(max(err.values()) <= 1e-8),
+                              speedup_vs_cpu_oracle=cpu_s * 1e3 / ms)
+    out['fp32-preconditioner']['speedup_vs_fp64'] = out['fp64']['ms_per_solve'] / \
+        out['fp32-preconditioner']['ms_per_solve']
+    return out
+
+
 def config1_row(device, steps=50, cpu_reps=5):
     """Config 1, the plain method: 2D 256x64 MAC on a 1.0 x 0.25 box (h =
     1/256), periodic in x with walls in y, FP64.  20,000 points on the
@@ -1043,6 +1097,7 @@ def run_b200(args):
         deterministic = deterministic_row(step, coef, device) if extra else None
         batch = batch_form_row(device) if extra else None
         config1 = config1_row(device) if extra else None
+        stokes = stokes_row(grid, device) if extra else None
         serving = serving_form_row(device) if extra else None
         step_ms = np.array([ev[0].elapsed_time(ev[4]) for ev in phases])
         line = dict(
@@ -1073,6 +1128,7 @@ def run_b200(args):
             deterministic_spread=deterministic,
             batch_form=batch,
             config1=config1,
+            stokes_fgmres=stokes,
             serving_form=serving,
             cpu_baseline=cpu)
         print(json.dumps(line, default=_json))

@@ -561,6 +561,32 @@ int32_t afsi_b200_pressure_input_partial(const void* rhs, const void* p, int64_t
 int32_t afsi_b200_pressure_norm_partial(const void* rhs, const void* p, void* out, const void* spacing_squared,
     const int64_t* shape, int32_t dtype, afsi_stream_t stream);
 
+/* ---- MG-preconditioned FGMRES for the CN saddle point -----------------------
+ * mac/stokes_fgmres.py:15-96: H u + (dt/rho) G p = b, D u = 0.  Krylov vectors
+ * are packed [u0 | u1 | u2 | q] (the three face arrays, then the cells; the
+ * reference's pack, stokes_fgmres.py:31-35); afsi_b200_stokes_packed_size gives
+ * the length (-1 for an invalid shape).
+ * afsi_b200_stokes_action: out = [(u - alpha L u) + h G q on interior faces, 0 on
+ *   each component's two wall faces; (-h) D u], the reference's action
+ *   (stokes_fgmres.py:36-43) with its operation order.  v and out distinct.
+ * afsi_b200_stokes_precondition_rhs: rhs = (-s)/h - D t for the Helmholtz
+ *   solution t (three face arrays) and the q-part s; *sum_out = sum(rhs)
+ *   (deterministic) for the caller's mean removal (stokes_fgmres.py:50-53).
+ * afsi_b200_stokes_precondition_result: out = [t - G phi; (phi + alpha rhs)/h],
+ *   *sum_out = sum of the q-part (stokes_fgmres.py:58-63).
+ * scratch: afsi_b200_stokes_precondition_scratch_bytes(shape) device bytes,
+ *   zero-initialised once, one stream at a time. */
+int64_t afsi_b200_stokes_packed_size(const int64_t* shape);
+int64_t afsi_b200_stokes_precondition_scratch_bytes(const int64_t* shape);
+int32_t afsi_b200_stokes_action(const void* v, void* out, const int64_t* shape, const double* spacing,
+    double alpha, double h, int32_t dtype, afsi_stream_t stream);
+int32_t afsi_b200_stokes_precondition_rhs(const void* const* tentative, const void* s, void* rhs,
+    double* sum_out, void* scratch, const int64_t* shape, const double* spacing, double h, int32_t dtype,
+    afsi_stream_t stream);
+int32_t afsi_b200_stokes_precondition_result(const void* const* tentative, const void* phi, const void* rhs,
+    void* out, double* sum_out, void* scratch, const int64_t* shape, const double* spacing, double alpha,
+    double h, int32_t dtype, afsi_stream_t stream);
+
 /* ---- batched 2D transfers (the batching form) ------------------------------
  * Many independent 2D channel instances (TriangleTransfer, mac2d/transfer.py:
  * 61-127, one per instance in the reference) in one launch per operation.

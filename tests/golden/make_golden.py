@@ -442,17 +442,86 @@ def cached():
     save('cached', **out)
 
 
+def curl_rhs(grid, seed):
+    """Seeded discrete curl of edge potentials that vanish on the boundary
+    edges: face fields with zero wall-normal flux and zero discrete divergence."""
+    g = torch.Generator().manual_seed(seed)
+    nx, ny, nz = grid.shape
+    hx, hy, hz = grid.spacing
+    Ax = torch.randn((nx, ny + 1, nz + 1), generator=g, dtype=torch.float64)
+    Ay = torch.randn((nx + 1, ny, nz + 1), generator=g, dtype=torch.float64)
+    Az = torch.randn((nx + 1, ny + 1, nz), generator=g, dtype=torch.float64)
+    for A, axes in ((Ax, (1, 2)), (Ay, (0, 2)), (Az, (0, 1))):
+        for a in axes:
+            A.index_fill_(a, torch.tensor([0, A.shape[a] - 1]), 0.)
+    u = torch.diff(Az, dim=1) / hy - torch.diff(Ay, dim=2) / hz
+    v = torch.diff(Ax, dim=2) / hz - torch.diff(Az, dim=0) / hx
+    w = torch.diff(Ay, dim=0) / hx - torch.diff(Ax, dim=1) / hy
+    return (u, v, w)
+
+
+def fgmres():
+    """The CN saddle-point solve by MG-preconditioned FGMRES
+    (mac/stokes_fgmres.py:15-96 with nonlinear.py gmres), from a zero and from
+    a random initial pressure, on a small anisotropic grid; plus one operator
+    action and one preconditioner application on a random packed vector, built
+    from the reference's own grid operators and flow methods exactly as the
+    solve's closures build them."""
+    from afsi_torch.mac.cnab import MACCNABFlow, CNABOptions
+    from afsi_torch.mac.grid import zero_normal, gradient, divergence
+    grid = MACGrid((16, 12, 10), (1.0, .9, .7))
+    dt, rho, mu = 1e-3, 1., .01
+    flow = MACCNABFlow(grid, dt=dt, rho=rho, mu=mu, cnab_options=CNABOptions(stokes_solver='fgmres',
+                                                                              advection='centered'))
+    g = torch.Generator().manual_seed(17)
+    b = curl_rhs(grid, 7)
+    b = tuple(v + 1e-3 * torch.randn(v.shape, generator=g, dtype=torch.float64) for v in b)
+    out = dict(shape=grid.shape, lengths=grid.lengths, dt=dt, rho=rho, mu=mu, alpha=flow.alpha,
+               helmholtz_iterations=flow.helmholtz_iterations)
+    for c in range(3):
+        out[f'b{c}'] = b[c]
+    p0 = torch.randn(grid.shape, generator=g, dtype=torch.float64)
+    out['p0'] = p0
+    for tag, initial in (('zero', None), ('warm', p0)):
+        res = flow.stokes(b, initial)
+        st, pr = res.diagnostics['stokes'], res.diagnostics['pressure']
+        for c in range(3):
+            out[f'{tag}_u{c}'] = res.velocity[c]
+        out[f'{tag}_p'] = res.pressure
+        out[f'{tag}_info'] = np.array([st['iterations'], st['operator_actions'], pr['poisson_solves'], pr['cycles'],
+                                       st['momentum_residual'], st['momentum_tolerance'], st['divergence_norm'],
+                                       st['divergence_tolerance']])
+    # one action and one preconditioner application (the solve's closures)
+    h = min(grid.spacing)
+    sizes = [grid.face_shape(c) for c in range(3)]
+    v = [torch.randn(s, generator=g, dtype=torch.float64) for s in sizes]
+    q = torch.randn(grid.shape, generator=g, dtype=torch.float64)
+    gp = gradient(q, grid.spacing)
+    hu = zero_normal(tuple(a - flow.alpha * l + h * gq for a, l, gq in zip(v, flow._lap(v), gp)))
+    for c in range(3):
+        out[f'v{c}'] = v[c]
+        out[f'action_u{c}'] = hu[c]
+    out['q'] = q
+    out['action_q'] = -h * divergence(v, grid.spacing)
+    tentative = flow._solve_helmholtz(tuple(v))
+    rhs = -q / h - divergence(tentative, grid.spacing)
+    rhs = rhs - rhs.mean()
+    phi, info = flow.pressure_solver.solve(rhs, rtol=flow.cnab_options.stokes_preconditioner_rtol)
+    grad = gradient(phi, grid.spacing)
+    for c in range(3):
+        out[f'pre_tentative{c}'] = tentative[c]
+        out[f'pre_u{c}'] = tentative[c] - grad[c]
+    qq = (phi + flow.alpha * rhs) / h
+    out['pre_rhs'] = rhs
+    out['pre_phi'] = phi
+    out['pre_q'] = qq - qq.mean()
+    out['pre_cycles'] = info['cycles']
+    save('fgmres', **out)
+
+
 if __name__ == '__main__':
-    peskin()
-    compact3d()
-    transfer2d()
-    p2()
-    mg3d()
-    mg2d()
-    quadrature()
-    orders()
-    p1csr()
-    dirichlet()
-    mass()
-    stokes()
-    cached()
+    # make_golden.py REFERENCE_SRC [fixture ...]: all fixtures, or the named ones
+    names = sys.argv[2:] or ['peskin', 'compact3d', 'transfer2d', 'p2', 'mg3d', 'mg2d', 'quadrature', 'orders',
+                             'p1csr', 'dirichlet', 'mass', 'stokes', 'cached', 'fgmres']
+    for name in names:
+        globals()[name]()

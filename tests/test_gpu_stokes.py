@@ -131,3 +131,85 @@ def test_helmholtz_on_a_64_cube_against_the_oracle():
     u = hs.solve(tuple(torch.as_tensor(x, device=DEV) for x in b), torch.as_tensor(p, device=DEV), .3)
     for c in range(3):
         assert np.array_equal(u[c].cpu().numpy(), u_ref[c])
+
+
+# --------------------------------------------------------------- FGMRES solve
+
+def _fgmres_case(precision='fp64'):
+    from afsi_gpu_b200.stokes_fgmres import CNStokes
+    z = golden('fgmres')
+    grid = MACGrid(tuple(int(n) for n in z['shape']), tuple(float(x) for x in z['lengths']))
+    flow = CNStokes(grid, dt=float(z['dt']), rho=float(z['rho']), mu=float(z['mu']), precision=precision)
+    return z, grid, flow
+
+
+def test_stokes_action_and_preconditioner_match_reference():
+    """The packed action kernel equals the reference's action (bitwise up to
+    the sign of zeros); the preconditioner (Helmholtz sweeps, the rhs kernel,
+    the multigrid solve to 0.01, the result kernel) within 1e-12."""
+    from afsi_gpu_b200.stokes_fgmres import _precondition
+    from afsi_gpu_b200 import _lib
+    z, grid, flow = _fgmres_case()
+    v = flow.pack(tuple(torch.as_tensor(z[f'v{c}'], device=DEV) for c in range(3)), torch.as_tensor(z['q'], device=DEV))
+    out = torch.empty_like(v)
+    _lib.call('afsi_b200_stokes_action', v.data_ptr(), out.data_ptr(), flow._shape, flow._spacing, flow.alpha,
+              min(grid.spacing), _lib.F64, _lib.stream())
+    u, q = flow.unpack(out)
+    for c in range(3):
+        assert np.array_equal(u[c].cpu().numpy(), z[f'action_u{c}'])
+    assert np.array_equal(q.cpu().numpy(), z['action_q'])
+    pre, cycles = _precondition(flow, v, min(grid.spacing))
+    u, q = flow.unpack(pre)
+    assert cycles == int(z['pre_cycles'])
+    for c in range(3):
+        ref = z[f'pre_u{c}']
+        np.testing.assert_allclose(u[c].cpu().numpy(), ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+    np.testing.assert_allclose(q.cpu().numpy(), z['pre_q'], rtol=0, atol=1e-12 * np.abs(z['pre_q']).max())
+
+
+@pytest.mark.parametrize('tag', ['zero', 'warm'])
+def test_fgmres_solve_matches_reference(tag):
+    """The whole CN saddle-point solve against the reference's: identical
+    iteration, action, Poisson-solve and V-cycle counts, velocity and pressure
+    within 1e-10 of the reference's largest values, accepted by the same
+    true-residual test."""
+    z, grid, flow = _fgmres_case()
+    b = tuple(torch.as_tensor(z[f'b{c}'], device=DEV) for c in range(3))
+    initial = None if tag == 'zero' else torch.as_tensor(z['p0'], device=DEV)
+    res = flow.stokes(b, initial)
+    st, pr = res.diagnostics['stokes'], res.diagnostics['pressure']
+    ref = z[f'{tag}_info']
+    assert [st['iterations'], st['operator_actions'], pr['poisson_solves'], pr['cycles']] == [int(v) for v in ref[:4]]
+    assert st['momentum_residual'] <= st['momentum_tolerance'] and st['divergence_norm'] <= st['divergence_tolerance']
+    np.testing.assert_allclose(st['momentum_tolerance'], ref[5], rtol=1e-12)
+    np.testing.assert_allclose(st['divergence_tolerance'], ref[7], rtol=1e-12)
+    for c in range(3):
+        r = z[f'{tag}_u{c}']
+        np.testing.assert_allclose(res.velocity[c].cpu().numpy(), r, rtol=0, atol=1e-10 * np.abs(r).max())
+    np.testing.assert_allclose(res.pressure.cpu().numpy(), z[f'{tag}_p'], rtol=0,
+                               atol=1e-10 * np.abs(z[f'{tag}_p']).max())
+
+
+def test_fgmres_precision_form_meets_the_fp64_acceptance_on_a_larger_grid():
+    """FP32 preconditioner (Helmholtz sweeps and V-cycles; FP64 coarsest
+    solve) inside the FP64 FGMRES: accepted by the FP64 true-residual test,
+    and within 1e-8 of the FP64 oracle's solve on a 32^3 grid."""
+    from afsi_gpu_b200.stokes_fgmres import CNStokes
+    from oracle import mg as omg
+    grid = MACGrid((32, 32, 32), (1., 1., 1.))
+    rng = np.random.default_rng(31)
+    b = [rng.standard_normal(grid.face_shape(c)) for c in range(3)]
+    P = ostokes.StokesProblem(grid.shape, grid.spacing, 1e-3, 1., .01, omg.Hierarchy(grid.shape, grid.spacing,
+                                                                                      'neumann'))
+    u_ref, p_ref, info = ostokes.fgmres_solve(P, b)
+    for precision in ('fp64', 'fp32-preconditioner'):
+        flow = CNStokes(grid, dt=1e-3, rho=1., mu=.01, precision=precision)
+        res = flow.stokes(tuple(torch.as_tensor(x, device=DEV) for x in b))
+        st = res.diagnostics['stokes']
+        assert st['momentum_residual'] <= st['momentum_tolerance']
+        assert st['divergence_norm'] <= st['divergence_tolerance']
+        if precision == 'fp64':
+            assert st['iterations'] == info['iterations']
+        for c in range(3):
+            assert np.abs(res.velocity[c].cpu().numpy() - u_ref[c]).max() <= 1e-8 * np.abs(u_ref[c]).max()
+        assert np.abs(res.pressure.cpu().numpy() - p_ref).max() <= 1e-8 * np.abs(p_ref).max()

@@ -285,3 +285,28 @@ def test_cached_pattern_oracle_matches_reference():
     for k in ('slots', 'order', 'crow', 'cols', 'tcrow', 'tcols', 'values', 'reverse'):
         assert np.array_equal(merged[k], g[f'{k}2']), k
     assert merged['new'] == int(g['new_count'])
+
+
+def test_fgmres_oracle_matches_reference_solves():
+    """The FGMRES restatement (oracle/stokes.py) reproduces the reference's
+    CN saddle-point solves (mac/stokes_fgmres.py:15-96): same iteration,
+    operator-action, Poisson-solve and V-cycle counts, solutions within 1e-14,
+    and the operator action bit for bit."""
+    from oracle import stokes as ostokes, mg as omg
+    z = golden('fgmres')
+    shape = tuple(int(n) for n in z['shape'])
+    spacing = tuple(float(L) / n for L, n in zip(z['lengths'], shape))
+    P = ostokes.StokesProblem(shape, spacing, float(z['dt']), float(z['rho']), float(z['mu']),
+                              omg.Hierarchy(shape, spacing, 'neumann'))
+    assert P.count == int(z['helmholtz_iterations'])
+    b = [z[f'b{c}'] for c in range(3)]
+    for tag, initial in (('zero', None), ('warm', z['p0'])):
+        u, p, info = ostokes.fgmres_solve(P, b, initial)
+        ref = z[f'{tag}_info']
+        assert [info['iterations'], info['operator_actions'], info['poisson_solves'], info['cycles']] == \
+            [int(v) for v in ref[:4]]
+        for c in range(3):
+            np.testing.assert_allclose(u[c], z[f'{tag}_u{c}'], rtol=0, atol=1e-14 * np.abs(z[f'{tag}_u{c}']).max())
+        np.testing.assert_allclose(p, z[f'{tag}_p'], rtol=0, atol=1e-14 * np.abs(z[f'{tag}_p']).max())
+    au, aq = P.unpack(P.action(P.pack([z[f'v{c}'] for c in range(3)], z['q'])))
+    assert all(np.array_equal(au[c], z[f'action_u{c}']) for c in range(3)) and np.array_equal(aq, z['action_q'])
