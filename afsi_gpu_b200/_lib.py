@@ -148,6 +148,15 @@ _SIGNATURES = {
                                             c_double, c_int32, c_void_p],
     'afsi_b200_batch_refine_graph_launch': [c_void_p, c_void_p],
     'afsi_b200_batch_refine_graph_destroy': [c_void_p],
+    'afsi_b200_fe_fused_spread': [c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p, c_int64,
+                                  c_void_p, c_void_p, P_F64, P_F64, P_F64, c_void_p, c_void_p, c_void_p, c_int64,
+                                  c_int64, c_int64, c_double, c_void_p, c_int32, c_int32, c_void_p],
+    'afsi_b200_fe_fused_gather': [c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p, c_int64,
+                                  c_void_p, c_void_p, c_void_p, c_void_p, P_F64, P_F64, P_F64, c_void_p, c_int64,
+                                  c_int64, c_int64, c_void_p, c_int32, c_int32, c_void_p],
+    'afsi_b200_fe_fused_gather_local': [c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p, c_int64,
+                                        c_void_p, c_void_p, c_void_p, c_void_p, P_F64, P_F64, P_F64, c_void_p,
+                                        c_int64, c_int64, c_int64, c_void_p, c_int32, c_int32, c_void_p],
     'afsi_b200_stokes_packed_size': [P_I64],
     'afsi_b200_stokes_precondition_scratch_bytes': [P_I64],
     'afsi_b200_stokes_action': [c_void_p, c_void_p, P_I64, P_F64, c_double, c_double, c_int32, c_void_p],

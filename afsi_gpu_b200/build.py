@@ -12,7 +12,7 @@ PACKAGE = Path(__file__).resolve().parent
 ROOT = PACKAGE.parent
 CSRC = PACKAGE / 'csrc'
 LIBRARY = PACKAGE / 'libafsi_b200.so'
-SOURCES = ('api.cu', 'prepare.cu', 'transfer.cu', 'p2.cu', 'mg.cu', 'mg_persistent.cu', 'csr.cu', 'mass.cu', 'batch.cu', 'stokes.cu', 'det_spread.cu', 'batch_refine.cu', 'fgmres.cu')
+SOURCES = ('api.cu', 'prepare.cu', 'transfer.cu', 'p2.cu', 'mg.cu', 'mg_persistent.cu', 'csr.cu', 'mass.cu', 'batch.cu', 'stokes.cu', 'det_spread.cu', 'batch_refine.cu', 'fgmres.cu', 'fe_fused.cu')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 FLAGS = ['-O3', '--fmad=false', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC,-O3',
          '--expt-relaxed-constexpr']

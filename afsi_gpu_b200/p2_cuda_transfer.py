@@ -18,6 +18,16 @@ node CSR instead of atomics (bitwise reproducible ``assemble_velocity``).
 positions, bases and weights are formed in FP64 (``afsi_b200_fe_prepare_mixed``,
 so the bases are the FP64 bases), the weight tables, rule tables and the
 transfers are FP32.
+
+Table-free form (``P2Transfer.prepare_table_free``, ``TableFreeStencil``): the
+rule only, no stencil tables; ``spread`` / ``assemble_velocity`` then form each
+point's position, bases and weights inside the transfer kernels
+(``afsi_b200_fe_fused_spread/_gather``) with the prepare's arithmetic, so the
+results equal the table-based ones up to the order of the atomic additions.
+Support and connectivity violations are flagged into the stencil's status
+word by the transfers and raised by ``confirm``.  ``P1Transfer`` is the
+matrix-free P1 element transfer (``mac/adaptive_cell.py:22-83``) on the same
+kernels with four-node cells.
 """
 from dataclasses import dataclass
 import torch
@@ -57,13 +67,28 @@ class SharedAdaptiveStencil:
         return base, phi
 
 
+@dataclass(frozen=True)
+class TableFreeStencil:
+    """A rule without stencil tables: the positions ``x`` it was built for,
+    the rule, and a device status word that the transfers OR their
+    AFSI_FLAG_* bits into (checked by ``P2Transfer.confirm`` / ``check``)."""
+    x: torch.Tensor
+    rule: InteractionRule
+    status: torch.Tensor
+    layout = 'table-free'
+
+    storage_bytes = 0
+
+
 class P2Transfer:
     """Grid/quadrature state of the P2 CUDA transfer (no mass solve)."""
 
+    nodes_per_cell = 10
+
     def __init__(self, grid, X, cells, *, point_density=2., max_order=8, max_points=12000000,
                  deterministic=False, transfer_dtype=None):
-        if cells.dim() != 2 or cells.shape[1] != 10:
-            raise ValueError('P2 transfer requires ten-node tetrahedra')
+        if cells.dim() != 2 or cells.shape[1] != self.nodes_per_cell:
+            raise ValueError(f'{type(self).__name__} requires {self.nodes_per_cell}-node tetrahedra')
         _lib.require_cuda(X)
         self.grid = grid
         self.node_count = X.shape[0]
@@ -130,12 +155,49 @@ class P2Transfer:
         ready.record(torch.cuda.current_stream(x.device))
         return DeferredStencil(SharedAdaptiveStencil(base, phi, last), x, orders, host, ready, buffers)
 
+    def prepare_table_free(self, x):
+        """The rule for positions ``x`` and no tables, with no host read: as
+        ``prepare_deferred``, the order kernel runs and its summary is copied
+        to pinned memory behind it, and the cached rule is used at once.
+        Returns a ``DeferredStencil`` whose ``stencil`` is a
+        ``TableFreeStencil``; ``confirm`` settles the rule and raises the
+        support / connectivity flags of the transfers that used it."""
+        _lib.require_cuda(x)
+        x = x.contiguous()
+        status = torch.zeros((), dtype=torch.int32, device=x.device)
+        last = self.rules.last
+        if last is None:
+            return DeferredStencil(TableFreeStencil(x, self.rules(x), status), x, None, None, None)
+        orders, summary = self.rules.launch(x)
+        host = torch.empty(summary.shape, dtype=summary.dtype, pin_memory=True)
+        host.copy_(summary, non_blocking=True)
+        ready = torch.cuda.Event()
+        ready.record(torch.cuda.current_stream(x.device))
+        return DeferredStencil(TableFreeStencil(x, last, status), x, orders, host, ready)
+
+    def check(self, stencil):
+        """Raise the flags a table-free stencil's transfers set (one host read)."""
+        flags = int(stencil.status.item())
+        if flags:
+            stencil.status.zero_()
+            _raise_flags(flags)
+
     def confirm(self, deferred):
         """Settle a deferred prepare: its stencil when the orders did not
         change (the common case; no work); a stencil prepared again,
         synchronously, with the new rule when they did (the caller redoes the
         transfers that used the old one); ``ValueError`` / ``RuntimeError``
         for a support or connectivity violation, as ``prepare`` raises them."""
+        if isinstance(deferred.stencil, TableFreeStencil):
+            st = deferred.stencil
+            if deferred.summary is not None:
+                deferred.ready.synchronize()
+                counts = deferred.summary.tolist()
+                rule = self.rules.finish(deferred.x, deferred.orders, counts)
+                if rule is not st.rule:
+                    return TableFreeStencil(st.x, rule, torch.zeros_like(st.status))
+            self.check(st)
+            return st
         if deferred.summary is None:
             return deferred.stencil
         deferred.ready.synchronize()
@@ -271,6 +333,8 @@ def spread(transfer, coefficient, stencil, *, events=None):
     events) bracket the native launches, excluding the output zero-fill."""
     _lib.require_cuda(coefficient)
     coefficient = coefficient.contiguous()
+    if isinstance(stencil, TableFreeStencil):
+        return _table_free_spread(transfer, coefficient, stencil, events)
     if coefficient.dtype != stencil.phi.dtype:
         raise ValueError('P2 spread coefficient dtype must match the stencil weights')
     g = transfer.grid
@@ -336,6 +400,8 @@ def assemble_velocity(transfer, velocity, stencil, *, events=None):
     nodal right-hand side rhs[a] = Σ_q N[q,a] W U(x_q).  ``events`` bracket
     the native launches."""
     velocity = _velocity(transfer, velocity)
+    if isinstance(stencil, TableFreeStencil):
+        return _table_free_assemble(transfer, velocity, stencil, events)
     if velocity[0].dtype != stencil.phi.dtype:
         raise ValueError('P2 velocity dtype must match the stencil weights')
     rhs = torch.zeros_like(transfer.diagonal)
@@ -377,3 +443,79 @@ def assemble_velocity_deterministic(transfer, velocity, stencil):
     call('afsi_b200_node_reduce', ptr(local), elements * 10, ptr(crow), ptr(slot), rhs.shape[0], ptr(rhs), 0,
          ptr(word), dtype_code(rhs.dtype), stream(rhs.device))
     return rhs
+
+
+# ------------------------------------------------------------ table-free form
+
+def _geometry(transfer):
+    g = transfer.grid
+    return _lib.doubles(g.origin), _lib.doubles(g.spacing), _lib.doubles([n - 2 for n in g.shape])
+
+
+def _table_free_spread(transfer, coefficient, stencil, events=None):
+    """Spread with the rows formed in the kernel (``afsi_b200_fe_fused_spread``)."""
+    x = stencil.x
+    if coefficient.dtype != transfer.transfer_dtype:
+        raise ValueError('spread coefficient dtype must match the transfer dtype')
+    g = transfer.grid
+    fields = g.zeros(device=coefficient.device, dtype=coefficient.dtype)
+    origin, spacing, limits = _geometry(transfer)
+    if events is not None:
+        events[0].record()
+    for group, (values, weights) in zip(stencil.rule.groups, _group_tables(transfer, stencil.rule)):
+        call('afsi_b200_fe_fused_spread', transfer.nodes_per_cell, ptr(x), x.shape[0], ptr(group.cells),
+             group.cells.shape[0], ptr(group.values), ptr(values), values.shape[0], ptr(weights), ptr(coefficient),
+             origin, spacing, limits, *(ptr(f) for f in fields), *g.shape, float(g.volume), ptr(stencil.status),
+             dtype_code(x.dtype), dtype_code(coefficient.dtype), stream(coefficient.device))
+    if events is not None:
+        events[1].record()
+    return fields
+
+
+def _table_free_assemble(transfer, velocity, stencil, events=None):
+    """Gather-assemble with the rows formed in the kernel (``afsi_b200_fe_fused_gather``)."""
+    x = stencil.x
+    if velocity[0].dtype != transfer.transfer_dtype:
+        raise ValueError('velocity dtype must match the transfer dtype')
+    rhs = torch.zeros_like(transfer.diagonal)
+    origin, spacing, limits = _geometry(transfer)
+    g = transfer.grid
+    if events is not None:
+        events[0].record()
+    for group, (values, weights) in zip(stencil.rule.groups, _group_tables(transfer, stencil.rule)):
+        call('afsi_b200_fe_fused_gather', transfer.nodes_per_cell, ptr(x), x.shape[0], ptr(group.cells),
+             group.cells.shape[0], ptr(group.values), ptr(values), values.shape[0], ptr(weights),
+             *(ptr(v) for v in velocity), origin, spacing, limits, ptr(rhs), *g.shape, ptr(stencil.status),
+             dtype_code(x.dtype), dtype_code(rhs.dtype), stream(rhs.device))
+    if events is not None:
+        events[1].record()
+    return rhs
+
+
+class P1Transfer(P2Transfer):
+    """Matrix-free P1 element transfer (the reference's ``AdaptiveP1Transfer``
+    CUDA execution, ``mac/adaptive_cell.py:22-83`` -> ``mac/_triton_adaptive.py:
+    25-128``, without the consistent-mass solve): the adaptive P1 rule
+    (``mac/adaptive_transfer.py`` ``_orders``), then spread and gather-assemble
+    of four-node elements with each point's position, bases and weights
+    formed in the kernel; no stencil tables and no assembled operator.
+    ``transfer_dtype=torch.float32`` beside FP64 positions keeps positions and
+    bases in FP64 and runs the weights and transfers in FP32."""
+    nodes_per_cell = 4
+
+    def prepare(self, x, **_):
+        """Rule for positions ``x`` (one host read when it changes); support and
+        connectivity violations are raised by ``check`` / ``confirm``."""
+        _lib.require_cuda(x)
+        x = x.contiguous()
+        return TableFreeStencil(x, self.rules(x), torch.zeros((), dtype=torch.int32, device=x.device))
+
+    prepare_deferred = P2Transfer.prepare_table_free
+
+    def spread(self, coefficient, stencil):
+        return spread(self, coefficient, stencil)
+
+    def assemble_velocity(self, velocity, stencil):
+        return assemble_velocity(self, velocity, stencil)
+
+    interpolate_rhs = assemble_velocity

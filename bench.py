@@ -608,23 +608,28 @@ P1_SHELL = dict(nr=2, ntheta=80, nphi=160, outer=(.224, .154, .154), inner=(.214
 
 
 def precision_p1_row(device, steps=5):
-    """The precision form on its own configuration: 128^3 MAC grid, a thin P1
-    tetrahedral prolate shell (128,000 elements, about 1.22 M adaptive
+    """Config 3 on its own configuration: 128^3 MAC grid, a thin P1
+    tetrahedral prolate shell (128,000 elements, about 1.1 M adaptive
     interaction points at density 2), seeded uniform nodal forces in [-1, 1],
     a seeded Fourier face velocity and a mean-free N(0,1) pressure RHS.  A step
-    is the P1 prepare and CSR assembly (positions, tables and contraction in
-    FP64), the spread and the interpolate, and the pressure solve to the FP64
-    tolerance.  Plain: FP64 operators and FP64 V-cycles.  Precision form: the
-    assembled operator values rounded to FP32, FP32 spread / interpolate, and
-    FP32 V-cycles inside FP64 iterative refinement.  CUDA events around each
-    of `steps` steps after one untimed step, the median step reported (the
-    assembly reads the host three times per step, so a busy host shows up as
-    outliers); errors are the largest differences from the FP64 step's
-    outputs over their largest values."""
+    is the P1 prepare, the spread, the interpolate and the pressure solve to
+    the FP64 tolerance (1e-10).  Forms:
+      csr_fp64:          the assembled-operator drop-in (CSR contraction and
+                         SpMVs, FP64) with FP64 V-cycles;
+      matrix_free_fp64:  the matrix-free element transfer (rows formed in the
+                         kernels, no operator, FP64) with FP64 V-cycles;
+      matrix_free_fp64_refined_mg: the same transfers, FP32 V-cycles inside FP64
+                         refinement (meets the FP64 bar);
+      precision_form:    matrix-free FP32 weights and transfers beside FP64
+                         positions, FP32 V-cycles inside FP64 refinement.
+    CUDA events around each of `steps` steps after one untimed step, the
+    median reported; errors against the FP64 oracle (transfers on an element
+    sample, the pressure on the full grid)."""
     from afsi_gpu_b200 import synthetic
     from afsi_gpu_b200.grid import MACGrid
     from afsi_gpu_b200.multigrid import GeometricMultigrid, RefinedMultigrid
     from afsi_gpu_b200.p1_csr import P1CSRTransfer
+    from afsi_gpu_b200.p2_cuda_transfer import P1Transfer
     grid = MACGrid((128, 128, 128), (1., 1., 1.))
     X, cells = synthetic.prolate_shell(**P1_SHELL)
     rng = np.random.default_rng(21)
@@ -633,19 +638,29 @@ def precision_p1_row(device, steps=5):
     c64 = torch.as_tensor(rng.uniform(-1., 1., (X.shape[0], 3)), device=device)
     v64 = tuple(v.to(device) for v in synthetic.fourier_velocity3d(grid, seed=21))
     r64 = synthetic.mean_free_normal(grid.shape, seed=21).to(device)
-    budget = dict(max_entries=400_000_000)
-    tr64 = P1CSRTransfer(grid, x, cells_t, **budget)
-    tr32 = P1CSRTransfer(grid, x, cells_t, transfer_dtype=torch.float32, **budget)
+    c32, v32 = c64.float(), tuple(v.float() for v in v64)
     mg64 = GeometricMultigrid(grid, device=device, backend='b200-graph')
     mg32 = RefinedMultigrid(grid, device=device)
-    c32, v32 = c64.float(), tuple(v.float() for v in v64)
     stream = torch.cuda.current_stream(device)
 
-    def step(tr, mg, c, v):
+    def csr_step(tr, mg, c, v):
         st = tr.prepare(x)
         return tr.spread(c, st), tr.interpolate_rhs(v, st), mg.solve(r64), st
 
-    def timed(*args):
+    def free_step(tr, mg, c, v):
+        # rule and support confirmed after the solve's own host read; a changed
+        # rule (never on this workload) redoes the transfers
+        deferred = tr.prepare_deferred(x)
+        st = deferred.stencil
+        f, r, p = tr.spread(c, st), tr.interpolate_rhs(v, st), mg.solve(r64)
+        confirmed = tr.confirm(deferred)
+        if confirmed is not st:
+            st = confirmed
+            f, r = tr.spread(c, st), tr.interpolate_rhs(v, st)
+            tr.check(st)
+        return f, r, p, st
+
+    def timed(step, *args):
         out = step(*args)
         torch.cuda.synchronize(device)
         ms = []
@@ -658,37 +673,54 @@ def precision_p1_row(device, steps=5):
             ms.append(e0.elapsed_time(e1))
         return out, float(np.median(ms))
 
-    ref, ms64 = timed(tr64, mg64, c64, v64)
-    out, ms32 = timed(tr32, mg32, c32, v32)
-    info64, info32 = ref[2][1], out[2][1]
-    oracle = p1_oracle_errors(grid, X, cells, c64, v64, r64, device, dict(plain_fp64=(ref[2][0], None),
-                                                                          precision_form=(out[2][0],
-                                                                                          torch.float32)))
+    budget = dict(max_entries=400_000_000)
+    forms = {}
+    csr, ms_csr = timed(csr_step, P1CSRTransfer(grid, x, cells_t, **budget), mg64, c64, v64)
+    forms['csr_fp64'] = (csr, ms_csr, None)
+    free64 = P1Transfer(grid, x, cells_t)
+    free32 = P1Transfer(grid, x, cells_t, transfer_dtype=torch.float32)
+    for name, tr, mg, c, v, dt in (('matrix_free_fp64', free64, mg64, c64, v64, None),
+                                   ('matrix_free_fp64_refined_mg', free64, mg32, c64, v64, None),
+                                   ('precision_form', free32, mg32, c32, v32, torch.float32)):
+        out, ms = timed(free_step, tr, mg, c, v)
+        forms[name] = (out, ms, dt)
+    oracle = p1_oracle_errors(grid, X, cells, c64, v64, r64, device,
+                              {name: (out[2][0], dt) for name, (out, _, dt) in forms.items()},
+                              transfer={'csr_fp64': 'csr'})
+    rows = {}
+    for name, (out, ms, dt) in forms.items():
+        info = out[2][1]
+        rows[name] = dict(steps_per_s=1e3 / ms, ms_per_step=ms, speedup_vs_csr_fp64=ms_csr / ms,
+                          transfer_dtype='f32' if dt is not None else 'f64',
+                          mg=(f"FP32 V-cycles in FP64 refinement, {info['refinements']} refinements, "
+                              f"{info['cycles']} FP32 cycles" if 'refinements' in info else
+                              f"FP64 V-cycles, {info['cycles']} cycles"),
+                          residual=info['residual_norm'], tolerance=info['tolerance'],
+                          error_vs_oracle=oracle[name])
+    rows['matrix_free_fp64']['speedup_vs_matrix_free_fp64'] = 1.
+    base = forms['matrix_free_fp64'][1]
+    for name in ('matrix_free_fp64_refined_mg', 'precision_form'):
+        rows[name]['speedup_vs_matrix_free_fp64'] = base / forms[name][1]
+    st = csr[3]
     return dict(workload=(f'128^3 MAC, P1 prolate shell {cells.shape[0]} elements / '
-                          f'{ref[3].rule.point_count} points, uniform [-1,1] forces'),
-                points=int(ref[3].rule.point_count), elements=int(cells.shape[0]),
-                csr_nnz=int(ref[3].assembly['total_nnz']),
-                plain_fp64=dict(steps_per_s=1e3 / ms64, ms_per_step=ms64, cycles=info64['cycles'],
-                                residual=info64['residual_norm'], tolerance=info64['tolerance'],
-                                error_vs_oracle=oracle['plain_fp64']),
-                precision_form=dict(steps_per_s=1e3 / ms32, ms_per_step=ms32, transfer_dtype='f32',
-                                    positions='f64',
-                                    mg=(f"FP32 V-cycles in FP64 refinement, {info32['refinements']} refinements, "
-                                        f"{info32['cycles']} FP32 cycles"),
-                                    residual=info32['residual_norm'], tolerance=info32['tolerance'],
-                                    error_vs_oracle=oracle['precision_form']),
-                speedup_vs_plain_fp64=ms64 / ms32, oracle_sample=oracle['sample'])
+                          f'{st.rule.point_count} points, uniform [-1,1] forces'),
+                points=int(st.rule.point_count), elements=int(cells.shape[0]),
+                csr_nnz=int(st.assembly['total_nnz']), oracle_sample=oracle['sample'], **rows)
 
 
-def p1_oracle_errors(grid, X, cells, coef, vel, rhs, device, forms, sample_elements=2000):
+def p1_oracle_errors(grid, X, cells, coef, vel, rhs, device, forms, sample_elements=2000, transfer=None):
     """Errors of the P1 forms against the FP64 oracle.  Transfers on an
     element sample (every k-th element of the shell, so the sample spans it):
     the form's transfer built on the sampled cells alone, its spread and
     interpolate against the oracle's P1 quadrature transfer with the same rule
     (x_q = N x, F_q = (N coef) W, spread over the shared tables, U_q gathered
     and assembled with N W).  Pressure: the full 128^3 oracle solve to 1e-10.
-    forms: name -> (pressure from the timed step, transfer dtype or None)."""
+    forms: name -> (pressure from the timed step, transfer dtype or None);
+    transfer: name -> 'csr' for the assembled-operator forms (default: the
+    matrix-free transfer)."""
     from afsi_gpu_b200.p1_csr import P1CSRTransfer
+    from afsi_gpu_b200.p2_cuda_transfer import P1Transfer
+    transfer = transfer or {}
     from oracle import ib as oib, mg as omg
     k = max(1, cells.shape[0] // sample_elements)
     sub = np.ascontiguousarray(cells[::k][:sample_elements])
@@ -701,7 +733,8 @@ def p1_oracle_errors(grid, X, cells, coef, vel, rhs, device, forms, sample_eleme
     oracle_ref = None
     for name, (p, dtype) in forms.items():
         kw = {} if dtype is None else dict(transfer_dtype=dtype)
-        tr = P1CSRTransfer(grid, x, torch.as_tensor(sub, device=device), **kw)
+        cls = P1CSRTransfer if transfer.get(name) == 'csr' else P1Transfer
+        tr = cls(grid, x, torch.as_tensor(sub, device=device), **kw)
         st = tr.prepare(x)
         cd = coef if dtype is None else coef.to(dtype)
         vd = vel if dtype is None else tuple(v.to(dtype) for v in vel)

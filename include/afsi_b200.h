@@ -561,6 +561,35 @@ int32_t afsi_b200_pressure_input_partial(const void* rhs, const void* p, int64_t
 int32_t afsi_b200_pressure_norm_partial(const void* rhs, const void* p, void* out, const void* spacing_squared,
     const int64_t* shape, int32_t dtype, afsi_stream_t stream);
 
+/* ---- table-free element transfers (P2 and matrix-free P1) --------------------
+ * The P2 spread / gather-assemble (mac/csrc/p2_transfer.cu:98-188) and the
+ * matrix-free P1 element transfer (mac/adaptive_cell.py:22-83,
+ * mac/_triton_adaptive.py:25-128) without stencil tables: each point's
+ * position x_q = sum_a N_pos[q,a] x[cell_a], its support check and its bases
+ * and IB_4 weights on both lattices are formed inside the transfer kernel
+ * with the arithmetic of afsi_b200_p2_prepare / afsi_b200_p1_prepare (bases
+ * bit-exact with their tables), so no (2,P,3) / (2,P,3,4) arrays exist.
+ * nodes_per_cell: 10 (P2) or 4 (P1).  x (nodes,3) and N_pos (nq,npc) in
+ * pos_dtype; N (nq,npc), W (elements,nq), value (nodes,3), the face arrays and
+ * rhs in dtype (FP64/FP64, FP64 positions with FP32 transfers, or FP32/FP32).
+ * limits = shape - 2 per axis.  Spread accumulates into u0/u1/u2 (pre-zeroed
+ * by the caller); gather adds into rhs (nodes,3), or writes per element
+ * (elements,npc,3) in the _local form.  A point whose support leaves the grid
+ * sets AFSI_FLAG_SUPPORT in *status and is skipped; an element with a node id
+ * outside [0, nodes) sets AFSI_FLAG_INDEX and is skipped. */
+int32_t afsi_b200_fe_fused_spread(int32_t nodes_per_cell, const void* x, int64_t nodes, const int64_t* cells,
+    int64_t elements, const void* N_pos, const void* N, int64_t nq, const void* W, const void* value,
+    const double* origin, const double* spacing, const double* limits, void* u0, void* u1, void* u2, int64_t nx,
+    int64_t ny, int64_t nz, double volume, int32_t* status, int32_t pos_dtype, int32_t dtype, afsi_stream_t stream);
+int32_t afsi_b200_fe_fused_gather(int32_t nodes_per_cell, const void* x, int64_t nodes, const int64_t* cells,
+    int64_t elements, const void* N_pos, const void* N, int64_t nq, const void* W, const void* u0, const void* u1,
+    const void* u2, const double* origin, const double* spacing, const double* limits, void* rhs, int64_t nx,
+    int64_t ny, int64_t nz, int32_t* status, int32_t pos_dtype, int32_t dtype, afsi_stream_t stream);
+int32_t afsi_b200_fe_fused_gather_local(int32_t nodes_per_cell, const void* x, int64_t nodes, const int64_t* cells,
+    int64_t elements, const void* N_pos, const void* N, int64_t nq, const void* W, const void* u0, const void* u1,
+    const void* u2, const double* origin, const double* spacing, const double* limits, void* local, int64_t nx,
+    int64_t ny, int64_t nz, int32_t* status, int32_t pos_dtype, int32_t dtype, afsi_stream_t stream);
+
 /* ---- MG-preconditioned FGMRES for the CN saddle point -----------------------
  * mac/stokes_fgmres.py:15-96: H u + (dt/rho) G p = b, D u = 0.  Krylov vectors
  * are packed [u0 | u1 | u2 | q] (the three face arrays, then the cells; the
