@@ -509,29 +509,48 @@ def config1_row(device, steps=50, cpu_reps=5):
 def serving_form_row(device, count=400):
     """Serving form: `count` requests of the serving mix (50% 2D 256x64 with
     20k points, 35% 3D 32^3-64^3 with 50k-400k points, 15% 3D 96^3 with 800k
-    points; Poisson arrivals at 2000/s, seeded), each a full FP64 step
-    (prepare, spread, interpolate, pressure solve to 1e-10) on resident
-    states, admitted under a 150 GB budget.  8 worker slots (continuous
-    batching) against 1 slot (requests one at a time, the plain drop-in)."""
-    from afsi_gpu_b200.serving import Request, Server, mix
-    reqs = mix(count, rate=2000., seed=0)
+    points; Poisson arrivals at 2000/s, seeded), each a full step to the FP64
+    tolerance on resident states: inputs (made before the clock starts, in
+    pinned host memory) copied in, prepare, spread, interpolate and pressure
+    solve, interpolated velocity and pressure copied back.  The server
+    admits under a 150 GB budget, batches the 2D requests that are waiting
+    when its 2D lane frees up (up to 8 per batch) and runs the 3D requests on
+    4 lanes with their own streams.  Both precisions (FP64 V-cycles; FP32
+    V-cycles inside FP64 refinement, batched for 2D), and the plain drop-in
+    serving one request at a time for comparison; then the refined form
+    below saturation (a quarter and a half of its saturated throughput)."""
+    from afsi_gpu_b200.serving import Request, Server, mix, with_inputs
+    reqs = with_inputs(mix(count, rate=2000., seed=0))
     out = {}
-    for slots in (8, 1):
-        server = Server(device=device, slots=slots)
+    for precision in ('fp64', 'fp32-refined'):
+        server = Server(device=device, slots=4, batch=8, precision=precision)
         server.warm(reqs)
         server.serve(reqs[:16])  # warm-up
         report, _ = server.serve(reqs)
-        out[f'slots_{slots}'] = report
-    out['speedup_vs_one_slot'] = out['slots_8']['steps_per_s'] / out['slots_1']['steps_per_s']
-    # 2000 req/s saturates the GPU (latency is queueing); the same mix at a
-    # quarter of the saturated throughput shows the step latency itself, and
-    # at half of it the knee where queueing starts
-    server = Server(device=device, slots=8)
+        out[precision] = report
+    one = Server(device=device, slots=1, batch=1, precision='fp64')
+    one.warm(reqs)
+    t0 = time.perf_counter()
+    for r in reqs:
+        one.alone(r)
+    wall = time.perf_counter() - t0
+    out['one_at_a_time_fp64'] = dict(requests=len(reqs), wall_s=wall, steps_per_s=len(reqs) / wall,
+                                     note='plain FP64 drop-in, each request alone, no batching or overlap')
+    out['speedup_fp32_refined_vs_one_at_a_time'] = out['fp32-refined']['steps_per_s'] / (len(reqs) / wall)
+    out['speedup_fp64_vs_one_at_a_time'] = out['fp64']['steps_per_s'] / (len(reqs) / wall)
+    # 2000 req/s saturates the GPU (latency there is queueing); the same mix
+    # at a quarter and a half of the refined form's saturated throughput shows
+    # the step latency itself and the knee where queueing starts
+    server = Server(device=device, slots=4, batch=8, precision='fp32-refined')
     below = mix(count // 2, rate=1., seed=1)
-    server.serve([Request(0., r.rid, r.kind, r.n, r.points, r.seed) for r in below[:16]])  # warm-up
-    for key, share in (('slots_8_below_saturation', .25), ('slots_8_half_saturation', .5)):
-        rate = share * out['slots_8']['steps_per_s']
-        report, _ = server.serve(mix(count // 2, rate=rate, seed=1))
+    made = with_inputs(below)
+    server.warm(made)
+    server.serve([Request(0., r.rid, r.kind, r.n, r.points, r.seed, r.inputs) for r in made[:16]])  # warm-up
+    for key, share in (('fp32_refined_quarter_saturation', .25), ('fp32_refined_half_saturation', .5)):
+        rate = share * out['fp32-refined']['steps_per_s']
+        timed = mix(count // 2, rate=rate, seed=1)
+        report, _ = server.serve([Request(t.arrival, r.rid, r.kind, r.n, r.points, r.seed, r.inputs)
+                                  for t, r in zip(timed, made)])
         out[key] = dict(report, arrival_rate=rate)
     return out
 

@@ -60,3 +60,17 @@ def test_leaflet_points_lie_inside_the_batched_support_region(shape):
 def test_forms_refuse_a_cpu_device():
     with pytest.raises(ValueError, match='CUDA'):
         Server(device='cpu')
+
+
+def test_request_inputs_are_made_once_and_seeded():
+    """Request inputs are host tensors made from the seed (the serving clock
+    never includes their generation): point and force shapes per kind, a
+    mean-free pressure right-hand side on the request's grid."""
+    from afsi_gpu_b200.serving import make_inputs, grid_of
+    for req in (Request(0., 0, '2d', 256, 3000, 7), Request(0., 1, '3d', 32, 2000, 8)):
+        a, b = make_inputs(req, pin=False), make_inputs(req, pin=False)
+        d = 2 if req.kind == '2d' else 3
+        assert a['points'].shape == (req.points, d) and a['force'].shape == (req.points, d)
+        assert tuple(a['rhs'].shape) == tuple(grid_of(req.kind, req.n).shape)
+        assert abs(float(a['rhs'].mean())) < 1e-12
+        assert all(np.array_equal(a[k].numpy(), b[k].numpy()) for k in a)
