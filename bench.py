@@ -43,12 +43,14 @@ def parse():
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='b200', choices=('b200', 'reference'))
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--rows', default='all', choices=('all', 'step', 'p1', 'batch'),
+    ap.add_argument('--rows', default='all', choices=('all', 'step', 'p1', 'batch', 'p1free', 'stokes'),
                     help="'step': the headline step line only, without the mass-solve, MG-form, batching and "
                          "serving rows (for profiler runs); 'p1': only the precision-form row on the 128^3 P1 "
                          "configuration, printed as its own JSON object (for profiler runs); 'batch': only "
                          "`--steps` replays of the refined batch step after `--warmup`, summarised as JSON "
-                         "(for profiler runs)")
+                         "(for profiler runs); 'p1free': `--steps` matrix-free P1 steps of the 128^3 "
+                         "configuration (FP64 transfers, FP64 V-cycles); 'stokes': `--steps` FGMRES Stokes "
+                         "solves of the 64^3 row (for profiler runs)")
     return ap.parse_args()
 
 
@@ -1203,12 +1205,62 @@ def batch_only(args):
                           launches_per_step=b.graph_launches + b.refinement().launches(5))))
 
 
+def p1free_only(args):
+    """Matrix-free P1 steps of the 128^3 configuration for profiler runs."""
+    from afsi_gpu_b200 import synthetic
+    from afsi_gpu_b200.grid import MACGrid
+    from afsi_gpu_b200.multigrid import GeometricMultigrid
+    from afsi_gpu_b200.p2_cuda_transfer import P1Transfer
+    device = torch.device('cuda', torch.cuda.current_device())
+    grid = MACGrid((128, 128, 128), (1., 1., 1.))
+    X, cells = synthetic.prolate_shell(**P1_SHELL)
+    rng = np.random.default_rng(21)
+    x = torch.as_tensor(X, device=device)
+    tr = P1Transfer(grid, x, torch.as_tensor(cells, device=device))
+    c = torch.as_tensor(rng.uniform(-1., 1., (X.shape[0], 3)), device=device)
+    v = tuple(t.to(device) for t in synthetic.fourier_velocity3d(grid, seed=21))
+    r = synthetic.mean_free_normal(grid.shape, seed=21).to(device)
+    mg = GeometricMultigrid(grid, device=device, backend='b200-graph')
+    st = tr.prepare(x)
+    for k in range(args.warmup + args.steps):
+        if k == args.warmup:
+            torch.cuda.synchronize(device)
+            t0 = time.perf_counter()
+        tr.spread(c, st), tr.interpolate_rhs(v, st), mg.solve(r)
+    torch.cuda.synchronize(device)
+    tr.check(st)
+    print(json.dumps(dict(points=st.rule.point_count, ms_per_step=(time.perf_counter() - t0) * 1e3 / max(args.steps, 1))))
+
+
+def stokes_only(args):
+    """FGMRES Stokes solves of the 64^3 row for profiler runs."""
+    from afsi_gpu_b200 import synthetic
+    from afsi_gpu_b200.grid import MACGrid
+    from afsi_gpu_b200.stokes_fgmres import CNStokes
+    device = torch.device('cuda', torch.cuda.current_device())
+    grid = MACGrid(GRID['shape'], GRID['lengths'])
+    b = tuple(t.to(device) for t in synthetic.divergence_free_faces(grid, seed=8))
+    flow = CNStokes(grid, device=device, **STOKES)
+    for k in range(args.warmup + args.steps):
+        if k == args.warmup:
+            torch.cuda.synchronize(device)
+            t0 = time.perf_counter()
+        res = flow.stokes(b)
+    torch.cuda.synchronize(device)
+    print(json.dumps(dict(iterations=res.diagnostics['stokes']['iterations'],
+                          ms_per_solve=(time.perf_counter() - t0) * 1e3 / max(args.steps, 1))))
+
+
 def main():
     args = parse()
     if args.impl == 'reference':
         run_reference(args)
     elif args.rows == 'batch':
         batch_only(args)
+    elif args.rows == 'p1free':
+        p1free_only(args)
+    elif args.rows == 'stokes':
+        stokes_only(args)
     elif args.rows == 'p1':
         print(json.dumps(precision_p1_row(torch.device('cuda', torch.cuda.current_device())), default=_json))
     else:
