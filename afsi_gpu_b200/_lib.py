@@ -13,7 +13,7 @@ LIB_PATH = Path(__file__).resolve().parent / 'libafsi_b200.so'
 
 F32, F64 = 0, 1
 OK, ERR_ARG, ERR_CUDA = 0, 1, 2
-FLAG_SUPPORT, FLAG_INDEX, FLAG_OVERFLOW = 1, 2, 4
+FLAG_SUPPORT, FLAG_INDEX, FLAG_OVERFLOW, FLAG_TIMEOUT = 1, 2, 4, 8
 PHI_CLAMPED, PHI_RADICAL = 0, 1
 BC_NEUMANN, BC_CHANNEL, BC_PERIODIC, BC_DIRICHLET = 0, 1, 2, 3
 MAX_LEVELS = 12

@@ -41,7 +41,10 @@ namespace {
 
 constexpr int kFSpreadWarps = 2;  // warps per spread block (about 19 KB of rows and boxes each)
 constexpr int kFGatherWarps = 4;  // warps per gather block
-constexpr int kFChunk = 64;       // points whose rows are held at once
+// Points whose rows are held at once: 64 for P2 (the common adaptive orders
+// have 15 or 64 points), 32 for P1 (orders 2 and 3 have 8 and 27 points), so a
+// P1 warp's staging is half the size and twice as many warps fit an SM.
+template <int NPC> struct FChunk { static constexpr int value = NPC == 10 ? 64 : 32; };
 constexpr int kFSpreadCap = 288;  // entries of one component's padded box per copy
 template <class T> struct FPatch { static constexpr int value = 4608 / sizeof(T); };
 
@@ -254,9 +257,9 @@ __device__ __forceinline__ bool stage_element(const TP* __restrict__ x, const in
 
 template <class TP, class T, int NPC>
 struct __align__(16) FSpreadStage {
-    T w[2][kFChunk * 12];    // rows of both lattices: axis a weights at q*12 + a*4
-    int b[2][kFChunk * 3];   // bases; b[0][q*3] == INT_MIN marks an invalid point
-    T f[kFChunk];
+    T w[2][FChunk<NPC>::value * 12];    // rows of both lattices: axis a weights at q*12 + a*4
+    int b[2][FChunk<NPC>::value * 3];   // bases; b[0][q*3] == INT_MIN marks an invalid point
+    T f[FChunk<NPC>::value];
     T coef[32];
     TP xs[32];
     T copy[2][kFSpreadCap];
@@ -296,7 +299,7 @@ __device__ __forceinline__ void fbox_walk(int lane, int ex, int ey, int ez, F f)
 template <class TP, class T, int NPC, class Stage>
 __device__ __forceinline__ bool element_rows_and_box(Stage& s, const TP* __restrict__ Npos, const FusedDims& g,
                                                      const Geo<TP>& geo, FBox& bx, int32_t* status) {
-    if (g.nq <= kFChunk) {
+    if (g.nq <= FChunk<NPC>::value) {
         if (fill_rows<TP, T, NPC>(Npos, s.xs, 0, int(g.nq), geo, s.w[0], s.w[1], s.b[0], s.b[1]) &&
             (threadIdx.x & 31) == 0)
             flag(status, AFSI_FLAG_SUPPORT);
@@ -315,7 +318,7 @@ __global__ void __launch_bounds__(kFSpreadWarps * 32) fused_spread_kernel(
     FSpreadStage<TP, T, NPC>& s = reinterpret_cast<FSpreadStage<TP, T, NPC>*>(fused_smem)[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31, half = lane >> 4, li = (lane >> 2) & 3, lj = lane & 3;
     const int64_t warps = int64_t(gridDim.x) * kFSpreadWarps;
-    const bool resident = g.nq <= kFChunk;
+    const bool resident = g.nq <= FChunk<NPC>::value;
     for (int64_t e = int64_t(blockIdx.x) * kFSpreadWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
         int64_t node;
         if (!stage_element<TP, T, NPC>(x, cells, value, e, g.nodes, s.xs, s.coef, node, status)) continue;
@@ -331,8 +334,8 @@ __global__ void __launch_bounds__(kFSpreadWarps * 32) fused_spread_kernel(
             __syncwarp();
             if (fits)
                 for (int t = lane; t < 2 * kFSpreadCap; t += 32) (&s.copy[0][0])[t] = T(0);
-            for (int64_t q0 = 0; q0 < g.nq; q0 += kFChunk) {
-                const int n = int(g.nq - q0 < kFChunk ? g.nq - q0 : kFChunk);
+            for (int64_t q0 = 0; q0 < g.nq; q0 += FChunk<NPC>::value) {
+                const int n = int(g.nq - q0 < FChunk<NPC>::value ? g.nq - q0 : FChunk<NPC>::value);
                 __syncwarp();
                 if (!resident) fill_rows<TP, T, NPC>(Npos, s.xs, q0, n, geo, s.w[0], s.w[1], s.b[0], s.b[1]);
                 for (int q = lane; q < n; q += 32) {  // component c of the forces, lanes over points
@@ -384,8 +387,8 @@ __global__ void __launch_bounds__(kFSpreadWarps * 32) fused_spread_kernel(
 
 template <class TP, class T, int NPC>
 struct __align__(16) FGatherStage {
-    T w[2][kFChunk * 12];    // both lattices' rows: axis a at q*12 + a*4
-    int b[2][kFChunk * 3];
+    T w[2][FChunk<NPC>::value * 12];    // both lattices' rows: axis a at q*12 + a*4
+    int b[2][FChunk<NPC>::value * 3];
     T patch[FPatch<T>::value];
     TP xs[32];
 };
@@ -399,7 +402,7 @@ __global__ void __launch_bounds__(kFGatherWarps * 32) fused_gather_kernel(
     FGatherStage<TP, T, NPC>& s = reinterpret_cast<FGatherStage<TP, T, NPC>*>(fused_smem)[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31, grp = lane >> 3, li = (lane >> 1) & 3, ljp = lane & 1, sub = lane & 7;
     const int64_t warps = int64_t(gridDim.x) * kFGatherWarps;
-    const bool resident = g.nq <= kFChunk;
+    const bool resident = g.nq <= FChunk<NPC>::value;
     const T* fields[3] = {u0, u1, u2};
     for (int64_t e = int64_t(blockIdx.x) * kFGatherWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
         int64_t node;
@@ -426,8 +429,8 @@ __global__ void __launch_bounds__(kFGatherWarps * 32) fused_gather_kernel(
                 });
         }
         T acc[2][3] = {{T(0), T(0), T(0)}, {T(0), T(0), T(0)}};
-        for (int64_t q0 = 0; q0 < g.nq && any; q0 += kFChunk) {
-            const int n = int(g.nq - q0 < kFChunk ? g.nq - q0 : kFChunk);
+        for (int64_t q0 = 0; q0 < g.nq && any; q0 += FChunk<NPC>::value) {
+            const int n = int(g.nq - q0 < FChunk<NPC>::value ? g.nq - q0 : FChunk<NPC>::value);
             if (!resident) {
                 __syncwarp();
                 fill_rows<TP, T, NPC>(Npos, s.xs, q0, n, geo, s.w[0], s.w[1], s.b[0], s.b[1]);

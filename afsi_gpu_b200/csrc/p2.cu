@@ -309,9 +309,13 @@ __global__ void __launch_bounds__(kWarps * 32, kSpreadBlocks) p2_spread_kernel(
 // For rules of at most kRowPoints points per element (the common adaptive
 // orders) the element's stencil rows — both lattices' bases (3 int64 per
 // point) and weights (12 per point), about 15 KB for 64 points in FP64 — are
-// brought into shared memory with asynchronous copies (cp.async) in one go,
-// instead of one chain of dependent global loads per point, and the element's
-// boxes come from the staged bases.  The accumulation is the padded-box,
+// contiguous in the tables, and are brought into shared memory by the bulk
+// copy engine (cp.async.bulk, one copy per lattice's weights and, when
+// 16-byte aligned, per lattice's bases), completing on a per-warp mbarrier,
+// instead of one chain of dependent global loads per point; the element's
+// boxes come from the staged bases.  The wait on the mbarrier is bounded by
+// a clock budget: a copy that does not complete flags AFSI_FLAG_TIMEOUT and
+// the element is skipped.  The accumulation is the padded-box,
 // half-warp-per-point scheme of p2_spread_kernel.
 
 constexpr int kRowPoints = 64;
@@ -327,13 +331,47 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// Bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from
+// global to this CTA's shared memory, completing on mbarrier `bar`.
+__device__ __forceinline__ void bulk_copy(void* smem, const void* gmem, unsigned bytes, unsigned long long* bar) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    const unsigned b = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(d), "l"(gmem), "r"(bytes), "r"(b) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+    const unsigned b = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(unsigned long long* bar, unsigned bytes) {
+    const unsigned b = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+}
+
+// Wait for phase `parity` of `bar` to complete, for at most about a second.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+    const unsigned b = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+    const long long t0 = clock64();
+    while (true) {
+        unsigned done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}" : "=r"(done) : "r"(b), "r"(parity) : "memory");
+        if (done) return true;
+        if (clock64() - t0 > 2000000000LL) return false;
+    }
+}
+
 template <class T>
-struct RowStage {
+struct __align__(16) RowStage {  // size a multiple of 16: every warp's copy targets start 16-byte aligned
     T phi[2][kRowPoints * 12];
     int64_t base[2][kRowPoints * 3];
     T f[kRowPoints];
     T coef[32];
     T copy[2][kSpreadCap];
+    unsigned long long bar;  // completion of this warp's bulk copies
 };
 
 template <class T>
@@ -346,6 +384,12 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) p2_spread_rows_kernel(
     const int lane = threadIdx.x & 31, half = lane >> 4, li = (lane >> 2) & 3, lj = lane & 3;
     const int64_t warps = int64_t(gridDim.x) * kRowWarps;
     const int n = int(g.nq);
+    // weights: n*12*sizeof(T) bytes per lattice, a multiple of 16 (n even for T=float)
+    const unsigned phi_bytes = unsigned(n * 12 * int(sizeof(T)));
+    const bool phi_bulk = phi_bytes % 16 == 0;
+    if (lane == 0) mbar_init(&s.bar);
+    __syncwarp();
+    unsigned parity = 0;
     for (int64_t e = int64_t(blockIdx.x) * kRowWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
         const int64_t node = lane < 10 ? cells[e * 10 + lane] : 0;
         if (__any_sync(0xffffffffu, lane < 10 && (node < 0 || node >= g.nodes))) {
@@ -354,17 +398,45 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) p2_spread_rows_kernel(
         }
         __syncwarp();
         const int64_t row0 = g.offset + e * g.nq;
+        // bases: bulk when both lattices' rows start 16-byte aligned (row0 and total even)
+        const bool base_bulk = ((row0 | g.total) & 1) == 0 && (n * 3 * 8) % 16 == 0 &&
+                               reinterpret_cast<uintptr_t>(base) % 16 == 0;
+        if (lane == 0) {
+            // order this warp's earlier shared-memory reads before the bulk writes
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            const unsigned bytes = (phi_bulk ? 2 * phi_bytes : 0) + (base_bulk ? 2 * unsigned(n * 3 * 8) : 0);
+            mbar_expect(&s.bar, bytes);
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                if (phi_bulk) bulk_copy(s.phi[t], phi + (int64_t(t) * g.total + row0) * 12, phi_bytes, &s.bar);
+                if (base_bulk)
+                    bulk_copy(s.base[t], base + (int64_t(t) * g.total + row0) * 3, unsigned(n * 3 * 8), &s.bar);
+            }
+        }
 #pragma unroll
         for (int t = 0; t < 2; ++t) {
-            const unsigned char* src = reinterpret_cast<const unsigned char*>(phi + (int64_t(t) * g.total + row0) * 12);
-            for (int i = lane; i < n * 12 * int(sizeof(T)) / 16; i += 32)
-                cp_async16(reinterpret_cast<unsigned char*>(s.phi[t]) + i * 16, src + i * 16);
-            const int64_t* bsrc = base + (int64_t(t) * g.total + row0) * 3;
-            for (int i = lane; i < n * 3; i += 32) cp_async8(&s.base[t][i], bsrc + i);
+            if (!phi_bulk) {
+                const unsigned char* src =
+                    reinterpret_cast<const unsigned char*>(phi + (int64_t(t) * g.total + row0) * 12);
+                for (int i = lane; i < n * 12 * int(sizeof(T)) / 8; i += 32)
+                    cp_async8(reinterpret_cast<unsigned char*>(s.phi[t]) + i * 8, src + i * 8);
+            }
+            if (!base_bulk) {
+                const int64_t* bsrc = base + (int64_t(t) * g.total + row0) * 3;
+                for (int i = lane; i < n * 3; i += 32) cp_async8(&s.base[t][i], bsrc + i);
+            }
         }
         const int64_t mine = __shfl_sync(0xffffffffu, node, lane < 30 ? lane / 3 : 0);
         if (lane < 30) s.coef[lane] = value[mine * 3 + lane % 3];
         cp_async_wait_all();
+        const bool arrived = mbar_wait(&s.bar, parity);
+        parity ^= 1u;
+        if (!__all_sync(0xffffffffu, arrived)) {
+            // a copy that never completed: flag it; this warp's later bulk copies
+            // would land in the same buffers, so the warp stops here
+            if (lane == 0) flag(status, AFSI_FLAG_TIMEOUT);
+            return;
+        }
         __syncwarp();
         Box bx;
         {

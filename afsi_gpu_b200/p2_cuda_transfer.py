@@ -305,6 +305,8 @@ def _launch_prepare(transfer, x, rule, base, phi, word):
 
 
 def _raise_flags(flags):
+    if flags & _lib.FLAG_TIMEOUT:
+        raise RuntimeError('a P2 transfer gave up waiting for its staged stencil rows')
     if flags & _lib.FLAG_INDEX:
         raise RuntimeError('P2 connectivity outside the node range')
     if flags:

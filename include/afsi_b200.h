@@ -50,6 +50,7 @@ typedef struct CUstream_st* afsi_stream_t; /* same object as cudaStream_t */
 #define AFSI_FLAG_SUPPORT 1  /* a point's 4-point support leaves the grid, or it is non-finite */
 #define AFSI_FLAG_INDEX 2    /* a stencil table addressed outside the grid/node range */
 #define AFSI_FLAG_OVERFLOW 4 /* a bounded table or buffer overflowed */
+#define AFSI_FLAG_TIMEOUT 8  /* a bounded wait for an asynchronous copy gave up (the work it fed was skipped) */
 
 /* Peskin weight forms: clamped two-branch kernel (ib.py:57-67, the torch
  * path) or the shared radical (mac/csrc/p2_transfer.cu:36-43). */
