@@ -46,10 +46,20 @@ namespace afsi {
 // out = p + (2/3)(rhs - A p)/diag, p read with shift m_p (p_in == nullptr: p=0).
 // fix_rhs: rhs -= mean(rhs) (pending from the restriction) and write it back.
 // emit: reduce sum(out) into the site.
+// Exact: the reference's operation order, (2/3)(rhs - A p) divided by the
+// diagonal; fast: the update p + (rhs - A p)(omega/diag) with omega/diag from a
+// 64-entry boundary-class table each block builds before waiting on its
+// predecessor (the single-CTA coarse levels use the same update).
 template <int BC, bool Exact, class T>
 __global__ void __launch_bounds__(kThreads) sweep_kernel(const T* __restrict__ p, T* __restrict__ rhs, T* __restrict__ out,
                                                          Lv<T> L, const double* p_sum, const double* rhs_sum,
                                                          Site emit, int fix_rhs, int do_emit) {
+    __shared__ T wtab[64];
+    if (!Exact) {
+        const unsigned t = thread_linear();
+        if (t < 64) wtab[t] = omega_of_class<BC>(int(t), L);
+        __syncthreads();
+    }
     pdl_enter();
     double local = 0.0;
     const T m = T(site_mean(p_sum, L.n));
@@ -62,12 +72,22 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(const T* __restrict__ p
             rhs[i] = r;
         }
         T v;
-        if (p) {
-            const T pc = p[i] - m;
-            const T a = neg_lap<BC, Exact>(p, i, x, y, z, L, m, pc);
-            v = pc + (omega<T>() * (r - a)) / diag_at<BC>(x, y, z, L);
+        if (Exact) {
+            if (p) {
+                const T pc = p[i] - m;
+                const T a = neg_lap<BC, Exact>(p, i, x, y, z, L, m, pc);
+                v = pc + (omega<T>() * (r - a)) / diag_at<BC>(x, y, z, L);
+            } else {
+                v = T(0) + (omega<T>() * r) / diag_at<BC>(x, y, z, L);
+            }
         } else {
-            v = T(0) + (omega<T>() * r) / diag_at<BC>(x, y, z, L);
+            const T w = wtab[boundary_class(x, y, z, L.nx, L.ny, L.nz)];
+            if (p) {
+                const T pc = p[i] - m;
+                v = jacobi_update(pc, r, neg_lap<BC, Exact>(p, i, x, y, z, L, m, pc), w);
+            } else {
+                v = r * w;
+            }
         }
         out[i] = v;
         local += double(v);
@@ -1272,6 +1292,7 @@ constexpr int kBatchLocalBits = 32 - kBatchEntryBits;
 
 template <class T>
 struct BatchLevel {
+    T w[64];           // omega/diag per boundary class of L (the fast sweep's table)
     Lv<T> L, C;        // the level and its coarser level
     T *p, *q, *r;      // iterate, Jacobi partner, right-hand side
     T* rc;             // coarser right-hand side
@@ -1333,12 +1354,12 @@ __device__ __forceinline__ void sweep_tile(const BatchLevel<T>& e, int tile, int
         if (x >= L.nx) break;
         const int64_t i = index_of(x, y, 0, L);
         const T r = rhs[i];
+        const T w = e.w[boundary_class(x, y, 0, L.nx, L.ny, L.nz)];
         if (!zero_in) {
             const T pc = p[i];
-            const T a = neg_lap<BC, false>(p, i, x, y, 0, L, T(0), pc);
-            v[m] = pc + (omega<T>() * (r - a)) / diag_at<BC>(x, y, 0, L);
+            v[m] = jacobi_update(pc, r, neg_lap<BC, false>(p, i, x, y, 0, L, T(0), pc), w);
         } else {
-            v[m] = T(0) + (omega<T>() * r) / diag_at<BC>(x, y, 0, L);
+            v[m] = r * w;
         }
     }
 #pragma unroll
@@ -1688,6 +1709,7 @@ int32_t batch_table(const afsi_mg_plan* const* plans, int count, const void* con
             std::memset(&e, 0, sizeof(e));
             e.L = lv[d];
             e.C = lv[d + 1];
+            for (int k = 0; k < 64; ++k) e.w[k] = omega_of_class<AFSI_BC_CHANNEL>(k, e.L);
             e.p = P(d);
             e.q = Q(d);
             e.r = R(d);

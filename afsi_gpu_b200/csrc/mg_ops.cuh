@@ -139,7 +139,7 @@ __device__ inline bool grid_barrier(const GridSync& g) {
 }
 
 template <int BC, class T>
-__device__ __forceinline__ T diag_at(int x, int y, int z, const Lv<T>& L) {
+__host__ __device__ __forceinline__ T diag_at(int x, int y, int z, const Lv<T>& L) {
     T d = T(0);
     if (BC == AFSI_BC_DIRICHLET) {
         // mac/open_boundary.py:47-52: 2·Σ h^-2, plus h^-2 on each boundary face
@@ -247,7 +247,7 @@ __device__ __forceinline__ void coords32(int i, const Lv<T>& L, int& x, int& y, 
 }
 
 template <class T>
-__device__ __forceinline__ T omega() { return T(2.0 / 3.0); }
+__host__ __device__ __forceinline__ T omega() { return T(2.0 / 3.0); }
 
 __device__ __forceinline__ double site_mean(const double* result, int64_t n) {
     return result ? *result / double(n) : 0.0;
@@ -443,23 +443,34 @@ struct FastCoords {
     }
 };
 
-__device__ __forceinline__ int boundary_class(int x, int y, int z, int nx, int ny, int nz) {
+__host__ __device__ __forceinline__ int boundary_class(int x, int y, int z, int nx, int ny, int nz) {
     return (x == 0) | ((x == nx - 1) << 1) | ((y == 0) << 2) | ((y == ny - 1) << 3) | ((z == 0) << 4) |
            ((z == nz - 1) << 5);
 }
 
-// omega/diag for each of the 64 boundary classes of level L (diag_at order).
+// omega/diag of boundary class k of level L (diag_at order, one IEEE
+// division), the same bits on the host and the device; classes that cannot
+// occur (first and last both set on an axis longer than one cell) get an
+// unused value.
+template <int BC, class T>
+__host__ __device__ __forceinline__ T omega_of_class(int k, const Lv<T>& L) {
+    const int x = (k & 1) ? 0 : ((k & 2) ? L.nx - 1 : (L.nx > 2 ? 1 : 0));
+    const int y = (k & 4) ? 0 : ((k & 8) ? L.ny - 1 : (L.ny > 2 ? 1 : 0));
+    const int z = (k & 16) ? 0 : ((k & 32) ? L.nz - 1 : (L.nz > 2 ? 1 : 0));
+    return omega<T>() / diag_at<BC>(x, y, z, L);
+}
+
+// omega/diag for each of the 64 boundary classes of level L.
 template <int BC, class T>
 __device__ void omega_table(const Lv<T>& L, T* table) {
-    for (int k = threadIdx.x; k < 64; k += blockDim.x) {
-        const int x = (k & 1) ? 0 : ((k & 2) ? L.nx - 1 : (L.nx > 2 ? 1 : 0));
-        const int y = (k & 4) ? 0 : ((k & 8) ? L.ny - 1 : (L.ny > 2 ? 1 : 0));
-        const int z = (k & 16) ? 0 : ((k & 32) ? L.nz - 1 : (L.nz > 2 ? 1 : 0));
-        // classes that cannot occur (first and last both set on an axis longer
-        // than one cell) get an unused value
-        table[k] = omega<T>() / diag_at<BC>(x, y, z, L);
-    }
+    for (int k = threadIdx.x; k < 64; k += blockDim.x) table[k] = omega_of_class<BC>(k, L);
 }
+
+// The weighted-Jacobi update of the fast arithmetic, shared by the launched,
+// batched and single-CTA sweeps: p + (rhs - A p) * (omega/diag) as one fused
+// multiply-add; from a zero iterate rhs * (omega/diag).
+template <class T>
+__device__ __forceinline__ T jacobi_update(T pc, T r, T a, T w) { return __fma_rn(r - a, w, pc); }
 
 // (A p)_i of the block path, pc = p_i.
 template <int BC, class T>
@@ -541,7 +552,7 @@ __device__ T* block_smooth(T* cur, T* oth, T* R, const Lv<T>& L, const FastCoord
                 v = r * w;
             } else {
                 const T pc = cur[i];
-                v = __fma_rn(R[i] - block_apply<BC>(cur, i, x, y, z, L, pc), w, pc);
+                v = jacobi_update(pc, R[i], block_apply<BC>(cur, i, x, y, z, L, pc), w);
             }
             oth[i] = v;
             if (last) acc += double(v);

@@ -18,8 +18,8 @@ from afsi_gpu_b200.multigrid import _levels
 TILE_Y, TILE_X, LOCAL_BITS = 32, 32, 21
 LV = np.dtype([('nx', '<i4'), ('ny', '<i4'), ('nz', '<i4'), ('pad', '<i4'), ('n', '<i8'), ('h2', '<f4', 3),
                ('ih2', '<f4', 3)])
-LEVEL = np.dtype([('L', LV), ('C', LV), ('p', '<u8'), ('q', '<u8'), ('r', '<u8'), ('rc', '<u8'), ('down', '<u8'),
-                  ('corr', '<u8')])
+LEVEL = np.dtype([('w', '<f4', 64), ('L', LV), ('C', LV), ('p', '<u8'), ('q', '<u8'), ('r', '<u8'), ('rc', '<u8'),
+                  ('down', '<u8'), ('corr', '<u8')])
 START = np.dtype([('src', '<u8'), ('r', '<u8'), ('p', '<u8'), ('nx', '<i4'), ('ny', '<i4')])
 COARSE = np.dtype([('lv', LV, _lib.MAX_LEVELS), ('first', '<i4'), ('last', '<i4'), ('rhs', '<u8'),
                    ('p_start', '<u8'), ('p_out', '<u8'), ('cinv', '<u8')])
@@ -101,6 +101,11 @@ def test_batch_table_covers_every_tile_once(smooth):
             P, Q = (lambda l: plan.level[l].p), (lambda l: plan.level[l].ping)
             e = lv[k]
             assert (e['L']['nx'], e['L']['ny'], e['L']['nz']) == (*shapes[d], 1)
+            # omega/diag of an interior cell (class 48: 2D, both z bits), the
+            # channel diagonal summed x then y in FP32, one division
+            ihx, ihy = e['L']['ih2'][0], e['L']['ih2'][1]
+            d_int = ((np.float32(0) + ihx + ihx) + ihy) + ihy
+            assert e['w'][48] == np.float32(2.0 / 3.0) / d_int
             assert (e['C']['nx'], e['C']['ny']) == shapes[d + 1] and e['C']['n'] == np.prod(shapes[d + 1])
             assert (e['p'], e['q'], e['r'], e['rc']) == (P(d), Q(d), plan.level[d].rhs, plan.level[d + 1].rhs)
             assert e['down'] == (P(d) if smooth % 2 == 0 else Q(d))
