@@ -18,35 +18,38 @@
 // Arithmetic: positions, validity, bases and weights use exactly the
 // operations of fe_prepare_kernel (prepare.cu) in the position type TP, so the
 // bases are bit-exact with the tables and the weights are the tables'
-// weights (rounded once to T in the precision form); the accumulation is the
-// staged-row kernels' (p2.cu), so a transfer equals the table-based one up to
-// the order of its global atomic additions.
+// weights (rounded once to T in the precision form).  Where the spacing of an
+// axis is a power of two, (x - start) / h is formed as (x - start) * (1/h),
+// which is the same correctly rounded value.
 //
-// Layout: one warp per element.  A first pass over the element's points
-// (lanes over points) forms the positions and the six (axis, lattice) bases
-// and reduces the element's support box per component.  Points are then
-// taken in chunks of 64: lanes over points form the rows a chunk needs in
-// shared memory (the spread: the three rows of one component and its
-// forces; the gather: all six rows); the accumulation half-warp per point
-// (spread, padded private boxes) or four points in flight (gather, staged face
-// patch) follows.  A point whose support leaves the grid sets
+// Layout: one warp per element, the three components in turn.  The element's
+// point positions are formed once (lanes over points, kept in shared memory
+// for rules of at most one chunk); per component, lanes over points form the
+// three weight rows the component reads (x, y, z: 12 values per point), its
+// support origins and, for the spread, its force factors; the warp reduces
+// the component's box.  The spread then accumulates runs of points with one
+// support origin in registers and adds each run to a padded shared-memory box
+// once (spread_runs, runs.cuh), flushed to the face array with one L2
+// reduction per non-zero face.  The gather stages the component's face patch
+// in the same padded layout, and four lane groups of eight walk contiguous
+// quarters of the points, reloading their eight patch values only when the
+// support origin changes.  A point whose support leaves the grid sets
 // AFSI_FLAG_SUPPORT and is skipped; an element with a node id outside
 // [0, nodes) sets AFSI_FLAG_INDEX and is skipped.
 #include <climits>
+#include <cmath>
 #include "common.cuh"
 #include "peskin.cuh"
+#include "runs.cuh"
 
 namespace afsi {
 namespace {
 
-constexpr int kFSpreadWarps = 2;  // warps per spread block (about 19 KB of rows and boxes each)
-constexpr int kFGatherWarps = 4;  // warps per gather block
+constexpr int kFWarps = 2;        // warps per block (spread and gather)
 // Points whose rows are held at once: 64 for P2 (the common adaptive orders
-// have 15 or 64 points), 32 for P1 (orders 2 and 3 have 8 and 27 points), so a
-// P1 warp's staging is half the size and twice as many warps fit an SM.
+// have 15 or 64 points), 32 for P1 (orders 2 and 3 have 8 and 27 points).
 template <int NPC> struct FChunk { static constexpr int value = NPC == 10 ? 64 : 32; };
-constexpr int kFSpreadCap = 288;  // entries of one component's padded box per copy
-template <class T> struct FPatch { static constexpr int value = 4608 / sizeof(T); };
+constexpr int kFBoxCap = 288;     // entries of one component's padded box (spread) or patch (gather)
 
 struct FusedDims {
     int64_t nx, ny, nz, nodes, elements, nq;
@@ -54,31 +57,32 @@ struct FusedDims {
 
 template <class TP>
 struct Geo {
-    TP origin[3], spacing[3], limits[3];
+    TP origin[3], spacing[3], limits[3], inv[3];
+    int pow2;  // bit a: spacing[a] is a power of two (inv[a] = 1 / spacing[a] exactly)
 };
 
+// One component's box: lower corner and extents of the supports.
 struct FBox {
-    int lo[3][3], ext[3][3], off[4];
+    int lo[3], ext[3];
 };
 
 template <class T> struct FPair;
 template <> struct FPair<double> { using type = double2; };
 template <> struct FPair<float> { using type = float2; };
 
-template <class TP, int NPC>
-struct ElementNodes {
-    TP x[NPC * 3];
-};
+// (x - start) / h on lattice l of axis a.
+template <class TP>
+__device__ __forceinline__ TP lattice_scaled(const Geo<TP>& geo, TP x, int a, int l) {
+    const TP start = l ? geo.origin[a] + TP(.5) * geo.spacing[a] : geo.origin[a];
+    return ((geo.pow2 >> a) & 1) ? (x - start) * geo.inv[a] : (x - start) / geo.spacing[a];
+}
 
-// Position of point q (fe_prepare_kernel: pos[d] += N[q,a] * x[a][d], a in
-// order, from zero), then per axis and lattice its base and, with w != null,
-// its four weights; the lattice-0 quotient (x - origin)/h is also the
-// prepare's support coordinate.  Returns the point's validity (every axis
-// finite with 2 <= (x - origin)/h < n - 2).
-template <class TP, class T, int NPC>
-__device__ __forceinline__ bool point_rows(const TP* __restrict__ Npos, const TP* xs, int64_t q, const Geo<TP>& geo,
-                                           int b[2][3], T* w0, T* w1) {
-    TP pos[3] = {TP(0), TP(0), TP(0)};
+// x_q = sum_a N[q,a] x[a] (fe_prepare_kernel: a in order, from zero) and its
+// validity (every axis finite with 2 <= (x - origin)/h < n - 2).
+template <class TP, int NPC>
+__device__ __forceinline__ bool point_position(const TP* __restrict__ Npos, const TP* xs, int64_t q,
+                                               const Geo<TP>& geo, TP pos[3]) {
+    pos[0] = pos[1] = pos[2] = TP(0);
 #pragma unroll
     for (int a = 0; a < NPC; ++a) {
         const TP nv = Npos[q * NPC + a];
@@ -88,147 +92,102 @@ __device__ __forceinline__ bool point_rows(const TP* __restrict__ Npos, const TP
     bool valid = true;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-#pragma unroll
-        for (int l = 0; l < 2; ++l) {
-            const TP start = l ? geo.origin[a] + TP(.5) * geo.spacing[a] : geo.origin[a];
-            const TP scaled = (pos[a] - start) / geo.spacing[a];
-            if (l == 0) valid = valid && isfinite(scaled) && scaled >= TP(2) && scaled < geo.limits[a];
-            const int64_t lower = static_cast<int64_t>(floor(scaled - TP(1)));
-            b[l][a] = int(lower);
-            T* w = l ? w1 : w0;
-            if (w) {
-                TP r[4];
-                peskin_radical(scaled - TP(lower) - TP(1), r);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) w[a * 4 + k] = T(r[k]);
-            }
-        }
+        const TP s0 = lattice_scaled(geo, pos[a], a, 0);
+        valid = valid && isfinite(s0) && s0 >= TP(2) && s0 < geo.limits[a];
     }
     return valid;
 }
 
-// Rows of points q0 .. q0+n-1 into shared memory (lanes over points):
-// w[l][q*12 + a*4 + k], b[l][q*3 + a]; an invalid point is marked by
-// b[0][q*3] = INT_MIN.  Returns true in every lane if any point was invalid.
-template <class TP, class T, int NPC>
-__device__ __forceinline__ bool fill_rows(const TP* __restrict__ Npos, const TP* xs, int64_t q0, int n,
-                                          const Geo<TP>& geo, T* w0, T* w1, int* b0, int* b1) {
-    bool bad = false;
-    for (int q = threadIdx.x & 31; q < n; q += 32) {
-        int b[2][3];
-        const bool valid = point_rows<TP, T, NPC>(Npos, xs, q0 + q, geo, b, &w0[q * 12], &w1[q * 12]);
+// Component c's support origins of a point (axis a on lattice a != c) and,
+// with w != null, its weight rows w[a*4 + k].
+template <class TP, class T>
+__device__ __forceinline__ void component_rows(const Geo<TP>& geo, const TP pos[3], int c, int b[3], T* w) {
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            b0[q * 3 + a] = b[0][a];
-            b1[q * 3 + a] = b[1][a];
-        }
-        if (!valid) {
-            b0[q * 3] = INT_MIN;
-            bad = true;
+    for (int a = 0; a < 3; ++a) {
+        const TP scaled = lattice_scaled(geo, pos[a], a, a != c);
+        const int64_t lower = static_cast<int64_t>(floor(scaled - TP(1)));
+        b[a] = int(lower);
+        if (w) {
+            TP r[4];
+            peskin_radical(scaled - TP(lower) - TP(1), r);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) w[a * 4 + k] = T(r[k]);
         }
     }
-    return __any_sync(0xffffffffu, bad);
 }
 
-__device__ __forceinline__ void box_init(int mn[3][3], int mx[3][3]) {
+__device__ __forceinline__ void bounds_init(int mn[3], int mx[3]) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            mn[c][a] = INT_MAX;
-            mx[c][a] = INT_MIN;
-        }
+    for (int a = 0; a < 3; ++a) {
+        mn[a] = INT_MAX;
+        mx[a] = INT_MIN;
+    }
 }
 
-__device__ __forceinline__ void box_add(int mn[3][3], int mx[3][3], const int b[2][3]) {
+__device__ __forceinline__ void bounds_add(int mn[3], int mx[3], const int b[3]) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const int v = b[a != c][a];
-            mn[c][a] = min(mn[c][a], v);
-            mx[c][a] = max(mx[c][a], v);
-        }
+    for (int a = 0; a < 3; ++a) {
+        mn[a] = min(mn[a], b[a]);
+        mx[a] = max(mx[a], b[a]);
+    }
 }
 
 // Warp-reduce the per-lane bounds into the box; false when no point was valid.
-__device__ __forceinline__ bool box_finish(int mn[3][3], int mx[3][3], FBox& bx) {
+__device__ __forceinline__ bool bounds_finish(int mn[3], int mx[3], FBox& bx) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
+    for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int d = 16; d; d >>= 1) {
-                mn[c][a] = min(mn[c][a], __shfl_xor_sync(0xffffffffu, mn[c][a], d));
-                mx[c][a] = max(mx[c][a], __shfl_xor_sync(0xffffffffu, mx[c][a], d));
-            }
-    if (mn[0][0] == INT_MAX) return false;  // no valid point
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            bx.lo[c][a] = mn[c][a];
-            bx.ext[c][a] = mx[c][a] - mn[c][a] + 4;
+        for (int d = 16; d; d >>= 1) {
+            mn[a] = min(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], d));
+            mx[a] = max(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], d));
         }
-    bx.off[0] = 0;
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
-        bx.off[c + 1] = bx.off[c] + int(min(int64_t(bx.ext[c][0]) * bx.ext[c][1] * bx.ext[c][2], int64_t(1) << 20));
-    return true;
-}
-
-// Box of the n rows held in shared memory.
-__device__ __forceinline__ bool box_from_rows(const int* b0, const int* b1, int n, FBox& bx) {
-    int mn[3][3], mx[3][3];
-    box_init(mn, mx);
-    for (int q = threadIdx.x & 31; q < n; q += 32) {
-        if (b0[q * 3] == INT_MIN) continue;
-        int b[2][3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            b[0][a] = b0[q * 3 + a];
-            b[1][a] = b1[q * 3 + a];
-        }
-        box_add(mn, mx, b);
+    for (int a = 0; a < 3; ++a) {
+        bx.lo[a] = mn[a];
+        bx.ext[a] = mx[a] == INT_MIN ? 0 : mx[a] - mn[a] + 4;
     }
-    return box_finish(mn, mx, bx);
-}
-
-// Box of all nq points, bases only (rules larger than one chunk); invalid
-// points set AFSI_FLAG_SUPPORT.
-template <class TP, class T, int NPC>
-__device__ __forceinline__ bool box_from_points(const TP* __restrict__ Npos, const TP* xs, int64_t nq,
-                                                const Geo<TP>& geo, FBox& bx, int32_t* status) {
-    int mn[3][3], mx[3][3];
-    box_init(mn, mx);
-    bool bad = false;
-    for (int64_t q = threadIdx.x & 31; q < nq; q += 32) {
-        int b[2][3];
-        if (!point_rows<TP, T, NPC>(Npos, xs, q, geo, b, nullptr, nullptr)) {
-            bad = true;
-            continue;
-        }
-        box_add(mn, mx, b);
-    }
-    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) flag(status, AFSI_FLAG_SUPPORT);
-    return box_finish(mn, mx, bx);
+    return mn[0] != INT_MAX;
 }
 
 __device__ __forceinline__ int64_t ffield_index(const FusedDims& g, int c, int x, int y, int z) {
     return (int64_t(x) * (g.ny + (c == 1)) + y) * (g.nz + (c == 2)) + z;
 }
 
-__device__ __forceinline__ bool fcomponent_inside(const FBox& bx, const FusedDims& g, int c) {
-    const int64_t fe[3] = {g.nx + (c == 0), g.ny + (c == 1), g.nz + (c == 2)};
-    bool inside = true;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) inside = inside && bx.lo[c][a] >= 0 && int64_t(bx.lo[c][a]) + bx.ext[c][a] <= fe[a];
-    return inside;
-}
-
 __device__ __forceinline__ bool fpoint_inside(const FusedDims& g, int c, int x, int y, int z) {
     return x >= 0 && y >= 0 && z >= 0 && x + 3 < g.nx + (c == 0) && y + 3 < g.ny + (c == 1) &&
            z + 3 < g.nz + (c == 2);
+}
+
+// Padded strides of component c's box; false when the box leaves the face
+// array or does not fit kFBoxCap entries (the element then takes the direct
+// L2 path).
+__device__ __forceinline__ bool fbox_layout(const FBox& bx, const FusedDims& g, int c, int& sx, int& sy) {
+    const int64_t fe[3] = {g.nx + (c == 0), g.ny + (c == 1), g.nz + (c == 2)};
+    bool inside = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) inside = inside && bx.lo[a] >= 0 && int64_t(bx.lo[a]) + bx.ext[a] <= fe[a];
+    sx = sy = 0;
+    if (!inside || bx.ext[1] > 64 || bx.ext[2] > 64) return false;
+    padded_strides(bx.ext[1], bx.ext[2], sx, sy);
+    return int64_t(bx.ext[0]) * sx <= kFBoxCap;
+}
+
+template <class F>
+__device__ __forceinline__ void fbox_walk(int lane, int ex, int ey, int ez, F f) {
+    const int n = ex * ey * ez;
+    if (lane >= n) return;
+    const int qz = 32 % ez, q = 32 / ez, qy = q % ey, qx = q / ey;
+    int z = lane % ez, r = lane / ez, y = r % ey, x = r / ey;
+    for (int t = lane; t < n; t += 32) {
+        f(x, y, z);
+        z += qz;
+        int carry = z >= ez ? 1 : 0;
+        z -= carry * ez;
+        y += qy + carry;
+        carry = y >= ey ? 1 : 0;
+        y -= carry * ey;
+        x += qx + carry;
+    }
 }
 
 // Stage the element's node positions (TP) and, optionally, its nodal values
@@ -253,129 +212,189 @@ __device__ __forceinline__ bool stage_element(const TP* __restrict__ x, const in
     return true;
 }
 
+// Per-warp shared memory of both kernels.
+template <class TP, class T, int NPC>
+struct __align__(16) FStage {
+    T w[FChunk<NPC>::value * 12];      // one component's rows: x at q*12, y at q*12+4, z at q*12+8
+    TP pos[FChunk<NPC>::value * 3];    // positions of a resident rule
+    int b[FChunk<NPC>::value * 3];     // support origins (absolute) of the component
+    int key[FChunk<NPC>::value];       // run keys in the box, -1 for an invalid point
+    T f[FChunk<NPC>::value];           // spread: force factors of the component
+    T box[kFBoxCap];                   // padded box
+    T coef[32];
+    TP xs[32];
+    int perm[FChunk<NPC>::value];      // points grouped by key (spread_element)
+    int rs[FChunk<NPC>::value + 1], rk[FChunk<NPC>::value];
+};
+
+// Positions of a resident rule (all nq <= chunk points) into s.pos; returns
+// the validity bits in every lane (bit q) and flags an invalid point.
+template <class TP, int NPC, class S>
+__device__ __forceinline__ unsigned long long resident_positions(S& s, const TP* __restrict__ Npos, int n,
+                                                                 const Geo<TP>& geo, int32_t* status) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long valid = 0;
+#pragma unroll
+    for (int j = 0; j < FChunk<NPC>::value / 32; ++j) {
+        const int q = lane + 32 * j;
+        bool v = false;
+        if (q < n) {
+            TP pos[3];
+            v = point_position<TP, NPC>(Npos, s.xs, q, geo, pos);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) s.pos[q * 3 + d] = pos[d];
+        }
+        valid |= static_cast<unsigned long long>(__ballot_sync(0xffffffffu, v)) << (32 * j);
+    }
+    const unsigned long long all = n >= 64 ? ~0ull : ((1ull << n) - 1);
+    if (valid != all && lane == 0) flag(status, AFSI_FLAG_SUPPORT);
+    __syncwarp();
+    return valid;
+}
+
+// Box of component c over all nq points (rules larger than one chunk),
+// support origins only; invalid points set AFSI_FLAG_SUPPORT.
+template <class TP, int NPC>
+__device__ __forceinline__ bool component_box_all(const TP* __restrict__ Npos, const TP* xs, int64_t nq,
+                                                  const Geo<TP>& geo, int c, FBox& bx, int32_t* status) {
+    int mn[3], mx[3];
+    bounds_init(mn, mx);
+    bool bad = false;
+    for (int64_t q = threadIdx.x & 31; q < nq; q += 32) {
+        TP pos[3];
+        if (!point_position<TP, NPC>(Npos, xs, q, geo, pos)) {
+            bad = true;
+            continue;
+        }
+        int b[3];
+        component_rows<TP, float>(geo, pos, c, b, nullptr);
+        bounds_add(mn, mx, b);
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) flag(status, AFSI_FLAG_SUPPORT);
+    return bounds_finish(mn, mx, bx);
+}
+
+// Rows pass of component c over points q0 .. q0+n-1 (lanes over points):
+// weight rows and absolute support origins into shared memory, the spread's
+// force factors when coef != null; the bounds of the valid points' origins
+// are added to mn/mx.  Invalid points get b[q*3] = INT_MIN.
+template <class TP, class T, int NPC>
+__device__ __forceinline__ void component_pass(FStage<TP, T, NPC>& s, const TP* __restrict__ Npos,
+                                               const T* __restrict__ N, const T* __restrict__ W, bool resident,
+                                               unsigned long long valid_bits, int64_t e, int64_t nq, int64_t q0,
+                                               int n, const Geo<TP>& geo, int c, const T* coef, T volume, int mn[3],
+                                               int mx[3]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll 1
+    for (int j = 0; j < FChunk<NPC>::value / 32; ++j) {
+        const int q = lane + 32 * j;
+        if (q >= n) continue;
+        TP pos[3];
+        bool v;
+        if (resident) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) pos[d] = s.pos[q * 3 + d];
+            v = (valid_bits >> q) & 1;
+        } else {
+            v = point_position<TP, NPC>(Npos, s.xs, q0 + q, geo, pos);
+        }
+        if (!v) {
+            s.b[q * 3] = INT_MIN;
+            continue;
+        }
+        int b[3];
+        component_rows<TP, T>(geo, pos, c, b, &s.w[q * 12]);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) s.b[q * 3 + a] = b[a];
+        bounds_add(mn, mx, b);
+        if (coef) {
+            T F = T(0);
+#pragma unroll
+            for (int a = 0; a < NPC; ++a) F += N[(q0 + q) * NPC + a] * coef[a * 3 + c];
+            s.f[q] = (F * W[e * nq + q0 + q]) / volume;
+        }
+    }
+}
+
+// Run keys of points 0..n-1 in box bx (-1 for invalid points, or all -1 when
+// the box does not fit).
+template <class TP, class T, int NPC>
+__device__ __forceinline__ void component_keys(FStage<TP, T, NPC>& s, int n, const FBox& bx, bool fits) {
+    for (int q = threadIdx.x & 31; q < n; q += 32) {
+        const int bx0 = s.b[q * 3];
+        s.key[q] = (fits && bx0 != INT_MIN)
+                       ? run_key(bx0 - bx.lo[0], s.b[q * 3 + 1] - bx.lo[1], s.b[q * 3 + 2] - bx.lo[2])
+                       : -1;
+    }
+}
+
 // ------------------------------------------------------------------ spread
 
 template <class TP, class T, int NPC>
-struct __align__(16) FSpreadStage {
-    T w[2][FChunk<NPC>::value * 12];    // rows of both lattices: axis a weights at q*12 + a*4
-    int b[2][FChunk<NPC>::value * 3];   // bases; b[0][q*3] == INT_MIN marks an invalid point
-    T f[FChunk<NPC>::value];
-    T coef[32];
-    TP xs[32];
-    T copy[2][kFSpreadCap];
-};
-
-// Padded strides of component c's box (p2.cu spread_layout).
-__device__ __forceinline__ bool fspread_layout(const FBox& bx, const FusedDims& g, int c, int& sx, int& sy) {
-    const int ey = bx.ext[c][1], ez = bx.ext[c][2];
-    sy = sx = 0;
-    if (!fcomponent_inside(bx, g, c) || ey > 64 || ez > 64) return false;
-    sy = ez | 1;
-    sx = ey * sy;
-    sx += (12 - (sx & 7)) & 7;
-    return int64_t(bx.ext[c][0]) * sx <= kFSpreadCap;
-}
-
-template <class F>
-__device__ __forceinline__ void fbox_walk(int lane, int ex, int ey, int ez, F f) {
-    const int n = ex * ey * ez;
-    if (lane >= n) return;
-    const int qz = 32 % ez, q = 32 / ez, qy = q % ey, qx = q / ey;
-    int z = lane % ez, r = lane / ez, y = r % ey, x = r / ey;
-    for (int t = lane; t < n; t += 32) {
-        f(t, x, y, z);
-        z += qz;
-        int carry = z >= ez ? 1 : 0;
-        z -= carry * ez;
-        y += qy + carry;
-        carry = y >= ey ? 1 : 0;
-        y -= carry * ey;
-        x += qx + carry;
-    }
-}
-
-// Element boxes: from the resident rows when the rule fits one chunk (the
-// rows are then formed once per element), else from a bases-only pass.
-template <class TP, class T, int NPC, class Stage>
-__device__ __forceinline__ bool element_rows_and_box(Stage& s, const TP* __restrict__ Npos, const FusedDims& g,
-                                                     const Geo<TP>& geo, FBox& bx, int32_t* status) {
-    if (g.nq <= FChunk<NPC>::value) {
-        if (fill_rows<TP, T, NPC>(Npos, s.xs, 0, int(g.nq), geo, s.w[0], s.w[1], s.b[0], s.b[1]) &&
-            (threadIdx.x & 31) == 0)
-            flag(status, AFSI_FLAG_SUPPORT);
-        __syncwarp();
-        return box_from_rows(s.b[0], s.b[1], int(g.nq), bx);
-    }
-    return box_from_points<TP, T, NPC>(Npos, s.xs, g.nq, geo, bx, status);
-}
-
-template <class TP, class T, int NPC>
-__global__ void __launch_bounds__(kFSpreadWarps * 32) fused_spread_kernel(
+__global__ void __launch_bounds__(kFWarps * 32, 8) fused_spread_kernel(
     const TP* __restrict__ x, const int64_t* __restrict__ cells, const TP* __restrict__ Npos,
     const T* __restrict__ N, const T* __restrict__ W, const T* __restrict__ value, Geo<TP> geo, T* __restrict__ u0,
     T* __restrict__ u1, T* __restrict__ u2, FusedDims g, T volume, int32_t* status) {
     extern __shared__ __align__(16) unsigned char fused_smem[];
-    FSpreadStage<TP, T, NPC>& s = reinterpret_cast<FSpreadStage<TP, T, NPC>*>(fused_smem)[threadIdx.x >> 5];
+    FStage<TP, T, NPC>& s = reinterpret_cast<FStage<TP, T, NPC>*>(fused_smem)[threadIdx.x >> 5];
+    constexpr int C = FChunk<NPC>::value;
     const int lane = threadIdx.x & 31, half = lane >> 4, li = (lane >> 2) & 3, lj = lane & 3;
-    const int64_t warps = int64_t(gridDim.x) * kFSpreadWarps;
-    const bool resident = g.nq <= FChunk<NPC>::value;
-    for (int64_t e = int64_t(blockIdx.x) * kFSpreadWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
+    const int64_t warps = int64_t(gridDim.x) * kFWarps;
+    const bool resident = g.nq <= C;
+    for (int64_t e = int64_t(blockIdx.x) * kFWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
         int64_t node;
         if (!stage_element<TP, T, NPC>(x, cells, value, e, g.nodes, s.xs, s.coef, node, status)) continue;
-        FBox bx;
-        if (!element_rows_and_box<TP, T, NPC>(s, Npos, g, geo, bx, status)) continue;
-        T* copy = s.copy[half];
-#pragma unroll
+        const unsigned long long valid =
+            resident ? resident_positions<TP, NPC>(s, Npos, int(g.nq), geo, status) : 0ull;
+#pragma unroll 1
         for (int c = 0; c < 3; ++c) {
             T* field = c == 0 ? u0 : c == 1 ? u1 : u2;
-            const int tx = c != 0, ty = c != 1, tz = c != 2;
-            int sx, sy;
-            const bool fits = fspread_layout(bx, g, c, sx, sy);
-            __syncwarp();
-            if (fits)
-                for (int t = lane; t < 2 * kFSpreadCap; t += 32) (&s.copy[0][0])[t] = T(0);
-            for (int64_t q0 = 0; q0 < g.nq; q0 += FChunk<NPC>::value) {
-                const int n = int(g.nq - q0 < FChunk<NPC>::value ? g.nq - q0 : FChunk<NPC>::value);
+            FBox bx;
+            bool any = true;
+            if (!resident) any = component_box_all<TP, NPC>(Npos, s.xs, g.nq, geo, c, bx, status);
+            int sx = 0, sy = 0;
+            bool fits = false;
+            for (int64_t q0 = 0; q0 < g.nq && any; q0 += C) {
+                const int n = int(g.nq - q0 < C ? g.nq - q0 : C);
                 __syncwarp();
-                if (!resident) fill_rows<TP, T, NPC>(Npos, s.xs, q0, n, geo, s.w[0], s.w[1], s.b[0], s.b[1]);
-                for (int q = lane; q < n; q += 32) {  // component c of the forces, lanes over points
-                    if (s.b[0][q * 3] == INT_MIN) continue;
-                    T F = T(0);
-#pragma unroll
-                    for (int a = 0; a < NPC; ++a) F += N[(q0 + q) * NPC + a] * s.coef[a * 3 + c];
-                    s.f[q] = (F * W[e * g.nq + q0 + q]) / volume;
+                int mn[3], mx[3];
+                bounds_init(mn, mx);
+                component_pass<TP, T, NPC>(s, Npos, N, W, resident, valid, e, g.nq, q0, n, geo, c, s.coef, volume,
+                                           mn, mx);
+                if (resident) {
+                    any = bounds_finish(mn, mx, bx);
+                    if (!any) break;
+                }
+                if (q0 == 0) {
+                    fits = fbox_layout(bx, g, c, sx, sy);
+                    if (fits)
+                        for (int t = lane; t < kFBoxCap; t += 32) s.box[t] = T(0);
                 }
                 __syncwarp();
-#pragma unroll 4
-                for (int q = half; q < n; q += 2) {
-                    if (s.b[0][q * 3] == INT_MIN) continue;
-                    const int gx = s.b[tx][q * 3], gy = s.b[ty][q * 3 + 1], gz = s.b[tz][q * 3 + 2];
-                    const T w = s.w[tx][q * 12 + li] * s.w[ty][q * 12 + 4 + lj];
-                    using P = typename FPair<T>::type;
-                    const P za = reinterpret_cast<const P*>(&s.w[tz][q * 12 + 8])[0];
-                    const P zb = reinterpret_cast<const P*>(&s.w[tz][q * 12 + 8])[1];
-                    const T wz[4] = {za.x, za.y, zb.x, zb.y};
-                    const T fq = s.f[q];
-                    if (fits) {
-                        T* dst = copy + (gx - bx.lo[c][0] + li) * sx + (gy - bx.lo[c][1] + lj) * sy + (gz - bx.lo[c][2]);
+                component_keys(s, n, bx, fits);
+                __syncwarp();
+                if (fits) {
+                    spread_element<T, C>(s.box, s.key, s.f, s.w, s.w + 4, s.w + 8, n, sx, sy, s.perm, s.rs, s.rk);
+                } else {
+                    for (int q = half; q < n; q += 2) {
+                        const int gx = s.b[q * 3], gy = s.b[q * 3 + 1], gz = s.b[q * 3 + 2];
+                        if (gx == INT_MIN) continue;
+                        if (fpoint_inside(g, c, gx, gy, gz)) {
+                            const T w = (s.w[q * 12 + li] * s.w[q * 12 + 4 + lj]) * s.f[q];
+                            T* dst = field + ffield_index(g, c, gx + li, gy + lj, gz);
 #pragma unroll
-                        for (int k = 0; k < 4; ++k) dst[k] += (w * wz[k]) * fq;
-                    } else if (fpoint_inside(g, c, gx, gy, gz)) {
-                        T* dst = field + ffield_index(g, c, gx + li, gy + lj, gz);
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) atomicAdd(dst + k, (w * wz[k]) * fq);
-                    } else if ((lane & 15) == 0) {
-                        flag(status, AFSI_FLAG_INDEX);
+                            for (int k = 0; k < 4; ++k) atomicAdd(dst + k, w * s.w[q * 12 + 8 + k]);
+                        } else if ((lane & 15) == 0) {
+                            flag(status, AFSI_FLAG_INDEX);
+                        }
                     }
                 }
             }
             __syncwarp();
-            if (fits) {
-                fbox_walk(lane, bx.ext[c][0], bx.ext[c][1], bx.ext[c][2], [&](int, int xx, int yy, int zz) {
-                    const int o = xx * sx + yy * sy + zz;
-                    const T v = s.copy[0][o] + s.copy[1][o];
-                    if (v != T(0))
-                        atomicAdd(field + ffield_index(g, c, bx.lo[c][0] + xx, bx.lo[c][1] + yy, bx.lo[c][2] + zz), v);
+            if (any && fits) {
+                fbox_walk(lane, bx.ext[0], bx.ext[1], bx.ext[2], [&](int xx, int yy, int zz) {
+                    const T v = s.box[xx * sx + yy * sy + zz];
+                    if (v != T(0)) atomicAdd(field + ffield_index(g, c, bx.lo[0] + xx, bx.lo[1] + yy, bx.lo[2] + zz), v);
                 });
             }
         }
@@ -384,139 +403,169 @@ __global__ void __launch_bounds__(kFSpreadWarps * 32) fused_spread_kernel(
 }
 
 // ------------------------------------------------------------------ gather
+//
+// One lane per point: the lane forms the point's three weight rows of the
+// component in registers and sums the 64 links over the component's face
+// patch, staged in shared memory with fixed strides (kGSX, kGSY: immediate
+// offsets; 68 = 4 mod 16 and 8 put the support origins of nearby points in
+// different bank pairs, and lanes of one run read the same words).  The
+// velocities U_c(x_q) of a chunk are kept in shared memory and assembled by
+// lanes (a, c) in point order: rhs[a][c] = sum_q N[q,a] W_q U_c(x_q).
+
+constexpr int kGWarps = 4;
+constexpr int kGSX = 68, kGSY = 8, kGExt = 8;  // patch strides; extents up to 8 per axis
+constexpr int kGPatch = kGExt * kGSX;
 
 template <class TP, class T, int NPC>
-struct __align__(16) FGatherStage {
-    T w[2][FChunk<NPC>::value * 12];    // both lattices' rows: axis a at q*12 + a*4
-    int b[2][FChunk<NPC>::value * 3];
-    T patch[FPatch<T>::value];
+struct __align__(16) FGStage {
+    T patch[kGPatch];
+    T u[3][FChunk<NPC>::value];
+    T w[FChunk<NPC>::value];
+    TP pos[FChunk<NPC>::value * 3];
     TP xs[32];
 };
 
+// sum_ijk wx[i] wy[j] wz[k] p[i*sx + j*sy + k]
+template <class T, class I>
+__device__ __forceinline__ T support_dot(const T* p, I sx, I sy, const T wx[4], const T wy[4], const T wz[4]) {
+    T u = T(0);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        T ti = T(0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const T* r = p + i * sx + j * sy;
+            T tz = r[0] * wz[0];
+            tz = fma(r[1], wz[1], tz);
+            tz = fma(r[2], wz[2], tz);
+            tz = fma(r[3], wz[3], tz);
+            ti = fma(wy[j], tz, ti);
+        }
+        u = fma(wx[i], ti, u);
+    }
+    return u;
+}
+
 template <class TP, class T, int NPC, bool Local>
-__global__ void __launch_bounds__(kFGatherWarps * 32) fused_gather_kernel(
+__global__ void __launch_bounds__(kGWarps * 32, 4) fused_gather_kernel(
     const T* __restrict__ u0, const T* __restrict__ u1, const T* __restrict__ u2, const TP* __restrict__ x,
     const int64_t* __restrict__ cells, const TP* __restrict__ Npos, const T* __restrict__ N, const T* __restrict__ W,
     Geo<TP> geo, T* __restrict__ out, FusedDims g, int32_t* status) {
     extern __shared__ __align__(16) unsigned char fused_smem[];
-    FGatherStage<TP, T, NPC>& s = reinterpret_cast<FGatherStage<TP, T, NPC>*>(fused_smem)[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31, grp = lane >> 3, li = (lane >> 1) & 3, ljp = lane & 1, sub = lane & 7;
-    const int64_t warps = int64_t(gridDim.x) * kFGatherWarps;
-    const bool resident = g.nq <= FChunk<NPC>::value;
-    const T* fields[3] = {u0, u1, u2};
-    for (int64_t e = int64_t(blockIdx.x) * kFGatherWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
+    FGStage<TP, T, NPC>& s = reinterpret_cast<FGStage<TP, T, NPC>*>(fused_smem)[threadIdx.x >> 5];
+    constexpr int C = FChunk<NPC>::value, J = C / 32;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = int64_t(gridDim.x) * kGWarps;
+    const bool resident = g.nq <= C;
+    for (int64_t e = int64_t(blockIdx.x) * kGWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
         int64_t node;
         if (!stage_element<TP, T, NPC>(x, cells, static_cast<const T*>(nullptr), e, g.nodes, s.xs, nullptr, node,
                                         status))
             continue;
-        FBox bx;
-        const bool any = element_rows_and_box<TP, T, NPC>(s, Npos, g, geo, bx, status);
-        int64_t cells_all = 0;
-        bool fits = any;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            fits = fits && fcomponent_inside(bx, g, c);
-            cells_all += int64_t(bx.ext[c][0]) * bx.ext[c][1] * bx.ext[c][2];
-        }
-        fits = fits && cells_all <= FPatch<T>::value;
-        __syncwarp();
-        if (fits) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-                fbox_walk(lane, bx.ext[c][0], bx.ext[c][1], bx.ext[c][2], [&](int t, int xx, int yy, int zz) {
-                    s.patch[bx.off[c] + t] =
-                        fields[c][ffield_index(g, c, bx.lo[c][0] + xx, bx.lo[c][1] + yy, bx.lo[c][2] + zz)];
-                });
-        }
-        T acc[2][3] = {{T(0), T(0), T(0)}, {T(0), T(0), T(0)}};
-        for (int64_t q0 = 0; q0 < g.nq && any; q0 += FChunk<NPC>::value) {
-            const int n = int(g.nq - q0 < FChunk<NPC>::value ? g.nq - q0 : FChunk<NPC>::value);
-            if (!resident) {
-                __syncwarp();
-                fill_rows<TP, T, NPC>(Npos, s.xs, q0, n, geo, s.w[0], s.w[1], s.b[0], s.b[1]);
-            }
+        const unsigned long long valid = resident ? resident_positions<TP, NPC>(s, Npos, int(g.nq), geo, status) : 0ull;
+        FBox boxes[3];
+        bool anys[3] = {true, true, true};
+        if (!resident)
+#pragma unroll 1
+            for (int c = 0; c < 3; ++c) anys[c] = component_box_all<TP, NPC>(Npos, s.xs, g.nq, geo, c, boxes[c], status);
+        T acc = T(0);  // lane (a, cc) = (lane / 3, lane % 3), lane < NPC * 3
+        for (int64_t q0 = 0; q0 < g.nq; q0 += C) {
+            const int n = int(g.nq - q0 < C ? g.nq - q0 : C);
             __syncwarp();
-#pragma unroll 2
-            for (int qb = 0; qb < n; qb += 4) {
-                const int q = qb + grp;
-                const bool active = q < n && s.b[0][q * 3] != INT_MIN;
-                const int qq = active ? q : 0;
-                T U[3];
+            for (int q = lane; q < n; q += 32) s.w[q] = W[e * g.nq + q0 + q];
+#pragma unroll 1
+            for (int c = 0; c < 3; ++c) {
+                const T* field = c == 0 ? u0 : c == 1 ? u1 : u2;
+                TP sc[J][3];
+                int bb[J][3];
+                bool vv[J];
+                int mn[3], mx[3];
+                bounds_init(mn, mx);
 #pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const int tx = c != 0, ty = c != 1, tz = c != 2;
-                    const int gx = s.b[tx][qq * 3], gy = s.b[ty][qq * 3 + 1], gz = s.b[tz][qq * 3 + 2];
-                    const T wx = s.w[tx][qq * 12 + li];
-                    using P = typename FPair<T>::type;
-                    const P wy = reinterpret_cast<const P*>(&s.w[ty][qq * 12 + 4])[ljp];
-                    const P za = reinterpret_cast<const P*>(&s.w[tz][qq * 12 + 8])[0];
-                    const P zb = reinterpret_cast<const P*>(&s.w[tz][qq * 12 + 8])[1];
-                    const T wz[4] = {za.x, za.y, zb.x, zb.y};
-                    T s0 = T(0), s1 = T(0);
-                    if (active) {
-                        const T* src = nullptr;
-                        int64_t sy = 0;
+                for (int j = 0; j < J; ++j) {
+                    const int q = lane + 32 * j;
+                    vv[j] = false;
+                    if (q < n) {
+                        TP pos[3];
+                        if (resident) {
+#pragma unroll
+                            for (int d = 0; d < 3; ++d) pos[d] = s.pos[q * 3 + d];
+                            vv[j] = (valid >> q) & 1;
+                        } else {
+                            vv[j] = point_position<TP, NPC>(Npos, s.xs, q0 + q, geo, pos);
+                        }
+                        if (vv[j]) {
+#pragma unroll
+                            for (int a = 0; a < 3; ++a) {
+                                sc[j][a] = lattice_scaled(geo, pos[a], a, a != c);
+                                bb[j][a] = int(static_cast<int64_t>(floor(sc[j][a] - TP(1))));
+                            }
+                            bounds_add(mn, mx, bb[j]);
+                        }
+                    }
+                }
+                FBox bx;
+                bool any;
+                if (resident) {
+                    any = bounds_finish(mn, mx, bx);
+                } else {
+                    bx = boxes[c];
+                    any = anys[c];
+                }
+                const int64_t fe[3] = {g.nx + (c == 0), g.ny + (c == 1), g.nz + (c == 2)};
+                bool fits = any;
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                    fits = fits && bx.lo[a] >= 0 && int64_t(bx.lo[a]) + bx.ext[a] <= fe[a] && bx.ext[a] <= kGExt;
+                __syncwarp();  // the previous component's patch reads are done
+                if (fits)
+                    fbox_walk(lane, bx.ext[0], bx.ext[1], bx.ext[2], [&](int xx, int yy, int zz) {
+                        s.patch[xx * kGSX + yy * kGSY + zz] =
+                            field[ffield_index(g, c, bx.lo[0] + xx, bx.lo[1] + yy, bx.lo[2] + zz)];
+                    });
+                __syncwarp();
+#pragma unroll
+                for (int j = 0; j < J; ++j) {
+                    const int q = lane + 32 * j;
+                    if (q >= n) continue;
+                    T U = T(0);
+                    if (vv[j]) {
+                        T wr[3][4];
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            TP r[4];
+                            peskin_radical(sc[j][a] - TP(bb[j][a]) - TP(1), r);
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) wr[a][k] = T(r[k]);
+                        }
                         if (fits) {
-                            src = s.patch + bx.off[c] +
-                                  ((gx - bx.lo[c][0] + li) * bx.ext[c][1] + (gy - bx.lo[c][1] + 2 * ljp)) * bx.ext[c][2] +
-                                  (gz - bx.lo[c][2]);
-                            sy = bx.ext[c][2];
-                        } else if (fpoint_inside(g, c, gx, gy, gz)) {
-                            src = fields[c] + ffield_index(g, c, gx + li, gy + 2 * ljp, gz);
-                            sy = g.nz + (c == 2);
-                        } else if (sub == 0) {
+                            const T* p0 = s.patch + (bb[j][0] - bx.lo[0]) * kGSX + (bb[j][1] - bx.lo[1]) * kGSY +
+                                          (bb[j][2] - bx.lo[2]);
+                            U = support_dot(p0, kGSX, kGSY, wr[0], wr[1], wr[2]);
+                        } else if (fpoint_inside(g, c, bb[j][0], bb[j][1], bb[j][2])) {
+                            const int64_t sz = g.nz + (c == 2), sy = (g.ny + (c == 1)) * sz;
+                            U = support_dot(field + ffield_index(g, c, bb[j][0], bb[j][1], bb[j][2]), sy, sz, wr[0],
+                                            wr[1], wr[2]);
+                        } else {
                             flag(status, AFSI_FLAG_INDEX);
                         }
-                        if (src) {
-#pragma unroll
-                            for (int k = 0; k < 4; ++k) {
-                                s0 = fma(src[k], wz[k], s0);
-                                s1 = fma(src[sy + k], wz[k], s1);
-                            }
-                        }
                     }
-                    T sum = wx * (wy.x * s0 + wy.y * s1);
-                    sum += __shfl_xor_sync(0xffffffffu, sum, 1);
-                    sum += __shfl_xor_sync(0xffffffffu, sum, 2);
-                    sum += __shfl_xor_sync(0xffffffffu, sum, 4);
-                    U[c] = sum;
+                    s.u[c][q] = U;
                 }
-                if (active) {
-                    const T wq = W[e * g.nq + q0 + q];
-#pragma unroll
-                    for (int m = 0; m < 2; ++m) {
-                        const int a = sub + 8 * m;
-                        if (a < NPC) {
-                            const T nw = N[(q0 + q) * NPC + a] * wq;
-#pragma unroll
-                            for (int c = 0; c < 3; ++c) acc[m][c] = fma(nw, U[c], acc[m][c]);
-                        }
-                    }
-                }
+            }
+            __syncwarp();
+            if (lane < NPC * 3) {
+                const int a = lane / 3, cc = lane - 3 * (lane / 3);
+                for (int q = 0; q < n; ++q) acc = fma(N[(q0 + q) * NPC + a] * s.w[q], s.u[cc][q], acc);
             }
         }
-#pragma unroll
-        for (int m = 0; m < 2; ++m)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                T v = acc[m][c];
-                v += __shfl_xor_sync(0xffffffffu, v, 8);
-                v += __shfl_xor_sync(0xffffffffu, v, 16);
-                acc[m][c] = v;
-            }
-#pragma unroll
-        for (int m = 0; m < 2; ++m) {
-            const int a = sub + 8 * m;
-            const int64_t nd = __shfl_sync(0xffffffffu, node, a < NPC ? a : 0);
-            if (grp == 0 && a < NPC) {
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    if (Local)
-                        out[(e * NPC + a) * 3 + c] = acc[m][c];
-                    else
-                        atomicAdd(out + nd * 3 + c, acc[m][c]);
-                }
-            }
+        const int64_t nd = __shfl_sync(0xffffffffu, node, lane < NPC * 3 ? lane / 3 : 0);
+        if (lane < NPC * 3) {
+            const int a = lane / 3, cc = lane - 3 * (lane / 3);
+            if (Local)
+                out[(e * NPC + a) * 3 + cc] = acc;
+            else
+                atomicAdd(out + nd * 3 + cc, acc);
         }
         __syncwarp();
     }
@@ -525,10 +574,18 @@ __global__ void __launch_bounds__(kFGatherWarps * 32) fused_gather_kernel(
 template <class TP>
 Geo<TP> make_geo(const double* origin, const double* spacing, const double* limits) {
     Geo<TP> geo;
+    geo.pow2 = 0;
     for (int a = 0; a < 3; ++a) {
         geo.origin[a] = TP(origin[a]);
         geo.spacing[a] = TP(spacing[a]);
         geo.limits[a] = TP(limits[a]);
+        int ex = 0;
+        const TP h = geo.spacing[a];
+        // a power of two: its reciprocal is exact and x * (1/h) rounds as x / h
+        const bool pow2 = std::isfinite(double(h)) && h > TP(0) && std::frexp(double(h), &ex) == 0.5 &&
+                          TP(1) / h == TP(std::ldexp(1.0, 1 - ex)) && std::isnormal(double(TP(1) / h));
+        geo.inv[a] = pow2 ? TP(1) / h : TP(0);
+        if (pow2) geo.pow2 |= 1 << a;
     }
     return geo;
 }
@@ -590,14 +647,14 @@ extern "C" int32_t afsi_b200_fe_fused_spread(int32_t nodes_per_cell, const void*
     const FusedDims g{nx, ny, nz, nodes, elements, nq};
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     AFSI_FUSED_DISPATCH(nodes_per_cell, pos_dtype, dtype, {
-        const size_t smem = sizeof(FSpreadStage<TP, T, NPC>) * kFSpreadWarps;
+        const size_t smem = sizeof(FStage<TP, T, NPC>) * kFWarps;
         static bool configured = false;  // once per instantiation, before any graph capture of it
         if (!configured) {
             cudaFuncSetAttribute(fused_spread_kernel<TP, T, NPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(smem));
             configured = true;
         }
-        fused_spread_kernel<TP, T, NPC><<<fused_blocks(elements, kFSpreadWarps), kFSpreadWarps * 32, smem, s>>>(
+        fused_spread_kernel<TP, T, NPC><<<fused_blocks(elements, kFWarps), kFWarps * 32, smem, s>>>(
             static_cast<const TP*>(x), cells, static_cast<const TP*>(N_pos), static_cast<const T*>(N),
             static_cast<const T*>(W), static_cast<const T*>(value), make_geo<TP>(origin, spacing, limits),
             static_cast<T*>(u0), static_cast<T*>(u1), static_cast<T*>(u2), g, T(volume), status);
@@ -619,14 +676,14 @@ static int32_t fused_gather(int32_t nodes_per_cell, const void* x, int64_t nodes
     const FusedDims g{nx, ny, nz, nodes, elements, nq};
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     AFSI_FUSED_DISPATCH(nodes_per_cell, pos_dtype, dtype, {
-        const size_t smem = sizeof(FGatherStage<TP, T, NPC>) * kFGatherWarps;
+        const size_t smem = sizeof(FGStage<TP, T, NPC>) * kGWarps;
         static bool configured = false;  // once per instantiation, before any graph capture of it
         if (!configured) {
             cudaFuncSetAttribute(fused_gather_kernel<TP, T, NPC, Local>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(smem));
             configured = true;
         }
-        fused_gather_kernel<TP, T, NPC, Local><<<fused_blocks(elements, kFGatherWarps), kFGatherWarps * 32, smem, s>>>(
+        fused_gather_kernel<TP, T, NPC, Local><<<fused_blocks(elements, kGWarps), kGWarps * 32, smem, s>>>(
             static_cast<const T*>(u0), static_cast<const T*>(u1), static_cast<const T*>(u2),
             static_cast<const TP*>(x), cells, static_cast<const TP*>(N_pos), static_cast<const T*>(N),
             static_cast<const T*>(W), make_geo<TP>(origin, spacing, limits), static_cast<T*>(out), g, status);

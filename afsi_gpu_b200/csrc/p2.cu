@@ -23,8 +23,9 @@
 // right-hand side (or written per element for the deterministic node
 // reduction).
 // Rules of at most 64 points per element take a spread variant that stages the
-// element's stencil rows in shared memory with asynchronous copies first
-// (p2_spread_rows_kernel).
+// element's stencil rows in shared memory with bulk copies first and merges
+// runs of points with the same support origin in registers before adding them
+// to a single box copy (p2_spread_rows_kernel, runs.cuh).
 // Point forces F = (Σ_a N[q,a] value[a]) * W (mac/compact_transfer.py:29-35)
 // are computed once per point and component by a lanes-over-points pass; the
 // spread contribution is (φx·φy)·φz · (F/volume), one division per point
@@ -35,6 +36,7 @@
 #include <climits>
 #include "common.cuh"
 #include "p2.cuh"
+#include "runs.cuh"
 
 namespace afsi {
 
@@ -157,9 +159,7 @@ __device__ __forceinline__ bool spread_layout(const Box& bx, const P2Dims& g, in
     const int ey = bx.ext[c][1], ez = bx.ext[c][2];
     sy = sx = 0;
     if (!component_inside(bx, g, c) || ey > 64 || ez > 64) return false;
-    sy = ez | 1;
-    sx = ey * sy;
-    sx += (12 - (sx & 7)) & 7;
+    padded_strides(ey, ez, sx, sy);
     return int64_t(bx.ext[c][0]) * sx <= kSpreadCap;
 }
 
@@ -315,8 +315,9 @@ __global__ void __launch_bounds__(kWarps * 32, kSpreadBlocks) p2_spread_kernel(
 // instead of one chain of dependent global loads per point; the element's
 // boxes come from the staged bases.  The wait on the mbarrier is bounded by
 // a clock budget: a copy that does not complete flags AFSI_FLAG_TIMEOUT and
-// the element is skipped.  The accumulation is the padded-box,
-// half-warp-per-point scheme of p2_spread_kernel.
+// the element is skipped.  The accumulation is spread_runs (runs.cuh): each
+// run of consecutive points with one support origin is summed in registers
+// and added to the padded box once.
 
 constexpr int kRowPoints = 64;
 constexpr int kRowWarps = 2;
@@ -370,12 +371,15 @@ struct __align__(16) RowStage {  // size a multiple of 16: every warp's copy tar
     int64_t base[2][kRowPoints * 3];
     T f[kRowPoints];
     T coef[32];
-    T copy[2][kSpreadCap];
+    T box[kSpreadCap];
+    int key[kRowPoints];
+    int perm[kRowPoints];       // points grouped by key (spread_element)
+    int rs[kRowPoints + 1], rk[kRowPoints];
     unsigned long long bar;  // completion of this warp's bulk copies
 };
 
 template <class T>
-__global__ void __launch_bounds__(kRowWarps * 32, 4) p2_spread_rows_kernel(
+__global__ void __launch_bounds__(kRowWarps * 32, 6) p2_spread_rows_kernel(
     const T* __restrict__ value, const int64_t* __restrict__ cells, const T* __restrict__ N, const T* __restrict__ W,
     const int64_t* __restrict__ base, const T* __restrict__ phi, T* __restrict__ u0, T* __restrict__ u1,
     T* __restrict__ u2, P2Dims g, T volume, int32_t* status) {
@@ -471,7 +475,6 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) p2_spread_rows_kernel(
                     bx.ext[c][a] = mx[c][a] - mn[c][a] + 4;
                 }
         }
-        T* copy = s.copy[half];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {  // unrolled: the box, tables and field of c stay in registers
             T* field = c == 0 ? u0 : c == 1 ? u1 : u2;
@@ -480,42 +483,38 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) p2_spread_rows_kernel(
             const int tx = c != 0, ty = c != 1, tz = c != 2;
             __syncwarp();
             if (fits)
-                for (int t = lane; t < 2 * kSpreadCap; t += 32) (&s.copy[0][0])[t] = T(0);
-            for (int q = lane; q < n; q += 32) {  // component c of the forces, lanes over points
+                for (int t = lane; t < kSpreadCap; t += 32) s.box[t] = T(0);
+            for (int q = lane; q < n; q += 32) {  // component c of the forces and the run keys, lanes over points
                 T F = T(0);
 #pragma unroll
                 for (int a = 0; a < 10; ++a) F += N[q * 10 + a] * s.coef[a * 3 + c];
                 s.f[q] = (F * W[e * g.nq + q]) / volume;
-            }
-            __syncwarp();
-#pragma unroll 4
-            for (int q = half; q < n; q += 2) {
-                const int gx = int(s.base[tx][q * 3]), gy = int(s.base[ty][q * 3 + 1]),
-                          gz = int(s.base[tz][q * 3 + 2]);
-                const T w = s.phi[tx][q * 12 + li] * s.phi[ty][q * 12 + 4 + lj];
-                T wz[4];
-                load_row4(&s.phi[tz][q * 12 + 8], wz);
-                const T fq = s.f[q];
-                if (fits) {
-                    T* dst = copy + (gx - bx.lo[c][0] + li) * sx + (gy - bx.lo[c][1] + lj) * sy + (gz - bx.lo[c][2]);
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) dst[k] += (w * wz[k]) * fq;
-                } else if (point_inside(g, c, gx, gy, gz)) {
-                    T* dst = field + face_index(g, c, gx + li, gy + lj, gz);
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) atomicAdd(dst + k, (w * wz[k]) * fq);
-                } else if ((lane & 15) == 0) {
-                    flag(status, AFSI_FLAG_INDEX);
-                }
+                if (fits)
+                    s.key[q] = run_key(int(s.base[tx][q * 3]) - bx.lo[c][0], int(s.base[ty][q * 3 + 1]) - bx.lo[c][1],
+                                       int(s.base[tz][q * 3 + 2]) - bx.lo[c][2]);
             }
             __syncwarp();
             if (fits) {
+                spread_element<T, kRowPoints>(s.box, s.key, s.f, s.phi[tx], s.phi[ty] + 4, s.phi[tz] + 8, n, sx, sy, s.perm, s.rs, s.rk);
+                __syncwarp();
                 box_walk(lane, bx.ext[c][0], bx.ext[c][1], bx.ext[c][2], [&](int, int x, int y, int z) {
-                    const int o = x * sx + y * sy + z;
-                    const T v = s.copy[0][o] + s.copy[1][o];
+                    const T v = s.box[x * sx + y * sy + z];
                     if (v != T(0))
                         atomicAdd(field + face_index(g, c, bx.lo[c][0] + x, bx.lo[c][1] + y, bx.lo[c][2] + z), v);
                 });
+            } else {
+                for (int q = half; q < n; q += 2) {
+                    const int gx = int(s.base[tx][q * 3]), gy = int(s.base[ty][q * 3 + 1]),
+                              gz = int(s.base[tz][q * 3 + 2]);
+                    if (point_inside(g, c, gx, gy, gz)) {
+                        const T w = (s.phi[tx][q * 12 + li] * s.phi[ty][q * 12 + 4 + lj]) * s.f[q];
+                        T* dst = field + face_index(g, c, gx + li, gy + lj, gz);
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) atomicAdd(dst + k, w * s.phi[tz][q * 12 + 8 + k]);
+                    } else if ((lane & 15) == 0) {
+                        flag(status, AFSI_FLAG_INDEX);
+                    }
+                }
             }
         }
         __syncwarp();
