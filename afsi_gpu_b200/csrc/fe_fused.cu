@@ -406,15 +406,11 @@ __global__ void __launch_bounds__(kFWarps * 32, 8) fused_spread_kernel(
 //
 // One lane per point: the lane forms the point's three weight rows of the
 // component in registers and sums the 64 links over the component's face
-// patch, staged in shared memory with fixed strides (kGSX, kGSY: immediate
-// offsets; 68 = 4 mod 16 and 8 put the support origins of nearby points in
-// different bank pairs, and lanes of one run read the same words).  The
+// patch (support_dot over the fixed-stride patch of runs.cuh).  The
 // velocities U_c(x_q) of a chunk are kept in shared memory and assembled by
 // lanes (a, c) in point order: rhs[a][c] = sum_q N[q,a] W_q U_c(x_q).
 
 constexpr int kGWarps = 4;
-constexpr int kGSX = 68, kGSY = 8, kGExt = 8;  // patch strides; extents up to 8 per axis
-constexpr int kGPatch = kGExt * kGSX;
 
 template <class TP, class T, int NPC>
 struct __align__(16) FGStage {
@@ -424,27 +420,6 @@ struct __align__(16) FGStage {
     TP pos[FChunk<NPC>::value * 3];
     TP xs[32];
 };
-
-// sum_ijk wx[i] wy[j] wz[k] p[i*sx + j*sy + k]
-template <class T, class I>
-__device__ __forceinline__ T support_dot(const T* p, I sx, I sy, const T wx[4], const T wy[4], const T wz[4]) {
-    T u = T(0);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        T ti = T(0);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const T* r = p + i * sx + j * sy;
-            T tz = r[0] * wz[0];
-            tz = fma(r[1], wz[1], tz);
-            tz = fma(r[2], wz[2], tz);
-            tz = fma(r[3], wz[3], tz);
-            ti = fma(wy[j], tz, ti);
-        }
-        u = fma(wx[i], ti, u);
-    }
-    return u;
-}
 
 template <class TP, class T, int NPC, bool Local>
 __global__ void __launch_bounds__(kGWarps * 32, 4) fused_gather_kernel(

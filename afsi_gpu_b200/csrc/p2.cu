@@ -15,13 +15,11 @@
 // lies.  The two copies are summed and flushed to the face array with one L2
 // reduction per non-zero face — about 130 per element and component instead
 // of 64 per point.
-// Gather: the face values of the element's boxes are staged in shared memory
-// once per element; four points are in flight per warp, lane group g =
-// lane>>3 taking one, its eight lanes owning (x offset i, y offsets
-// 2jp..2jp+1) with all four z links, reduced with three shuffles.  The nodal
-// sums Σ_q N[q,a] W U(x_q) are accumulated in registers and added to the
-// right-hand side (or written per element for the deterministic node
-// reduction).
+// Gather: one lane per point reads the point's table rows and sums its
+// support over the component's face patch, staged in shared memory once per
+// element and component; the nodal sums Σ_q N[q,a] W U(x_q) are formed by
+// lanes (a, c) in point order and added to the right-hand side (or written
+// per element for the deterministic node reduction).
 // Rules of at most 64 points per element take a spread variant that stages the
 // element's stencil rows in shared memory with bulk copies first and merges
 // runs of points with the same support origin in registers before adding them
@@ -42,7 +40,6 @@ namespace afsi {
 
 constexpr int kWarps = 4;       // warps per block
 constexpr int kChunk = 64;      // points whose forces are held at once
-template <class T> struct BoxCap { static constexpr int value = 4608 / sizeof(T); };  // gather patch (576 doubles)
 constexpr int kSpreadCap = 288;   // spread: entries of one component's padded box per copy
 
 // f(t, x, y, z) for the cells t = lane, lane + 32, ... of an ex x ey x ez box
@@ -68,13 +65,8 @@ __device__ __forceinline__ void box_walk(int lane, int ex, int ey, int ez, F f) 
 constexpr int kSpreadBlocks = 6;  // resident blocks per SM the spread is compiled for
 constexpr int kGatherBlocks = 6;  // same for the gather
 
-template <class T>
-struct GatherStage {
-    T patch[BoxCap<T>::value];
-};
-
 struct Box {
-    int lo[3][3], ext[3][3], off[4];
+    int lo[3][3], ext[3][3];
 };
 
 __device__ __forceinline__ int64_t table_row(int64_t total, int64_t row, int c, int a) {
@@ -120,9 +112,6 @@ __device__ __forceinline__ void element_box(const int64_t* __restrict__ base, co
             bx.lo[c][a] = mn[c][a];
             bx.ext[c][a] = mx[c][a] - mn[c][a] + 4;
         }
-    bx.off[0] = 0;  // patch offsets, meaningful when box_fits holds
-#pragma unroll
-    for (int c = 0; c < 3; ++c) bx.off[c + 1] = bx.off[c] + int(min(int64_t(bx.ext[c][0]) * bx.ext[c][1] * bx.ext[c][2], int64_t(1) << 20));
 }
 
 __device__ __forceinline__ bool component_inside(const Box& bx, const P2Dims& g, int c) {
@@ -133,22 +122,6 @@ __device__ __forceinline__ bool component_inside(const Box& bx, const P2Dims& g,
     return inside;
 }
 
-__device__ __forceinline__ int64_t component_cells(const Box& bx, int c) {
-    return int64_t(bx.ext[c][0]) * bx.ext[c][1] * bx.ext[c][2];
-}
-
-// All three boxes lie in their face arrays and fit one gather patch.
-template <class T>
-__device__ __forceinline__ bool box_fits(const Box& bx, const P2Dims& g) {
-    int64_t cells = 0;
-    bool inside = true;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        inside = inside && component_inside(bx, g, c);
-        cells += component_cells(bx, c);
-    }
-    return inside && cells <= BoxCap<T>::value;
-}
 
 // Padded strides of component c's box in a spread copy: sy = ez|1 (odd) and
 // sx = 4 (mod 8), sx >= ey*sy.  Entry (x,y,z) sits at x*sx + y*sy + z, and the
@@ -173,13 +146,7 @@ __device__ __forceinline__ bool point_inside(const P2Dims& g, int c, int x, int 
            z + 3 < g.nz + (c == 2);
 }
 
-// ------------------------------------------------------------------ lanes
-//
-// Gather lane layout: group g = lane>>3 takes one of four points in flight; within a
-// group, lane bits (i = (lane>>1)&3, jp = lane&1) own the x offset i and the
-// y offsets 2jp, 2jp+1 of the point's support, and all four z offsets: eight
-// links per component.  The z row of four weights is one 32-byte pair of
-// vector loads.
+// Rows of four weights are read as one 32-byte pair of vector loads.
 
 template <class T> struct Pair;
 template <> struct Pair<double> { using type = double2; };
@@ -194,28 +161,6 @@ __device__ __forceinline__ void load_row4(const T* __restrict__ w, T out[4]) {
     out[1] = a.y;
     out[2] = b.x;
     out[3] = b.y;
-}
-
-// One point's view for component c: support origin and the weights this lane needs.
-template <class T>
-struct PointView {
-    int gx, gy, gz;
-    T wx, wy0, wy1, wz[4];
-};
-
-template <class T>
-__device__ __forceinline__ void point_view(const int64_t* __restrict__ base, const T* __restrict__ phi, int64_t total,
-                                           int64_t row, int c, int li, int ljp, PointView<T>& v) {
-    const int64_t rx = table_row(total, row, c, 0), ry = table_row(total, row, c, 1), rz = table_row(total, row, c, 2);
-    v.gx = int(base[rx]);
-    v.gy = int(base[ry]);
-    v.gz = int(base[rz]);
-    v.wx = phi[rx * 4 + li];
-    using P = typename Pair<T>::type;
-    const P y = reinterpret_cast<const P*>(phi + ry * 4)[ljp];
-    v.wy0 = y.x;
-    v.wy1 = y.y;
-    load_row4(phi + rz * 4, v.wz);
 }
 
 // ------------------------------------------------------------------ spread
@@ -522,6 +467,23 @@ __global__ void __launch_bounds__(kRowWarps * 32, 6) p2_spread_rows_kernel(
 }
 
 // ------------------------------------------------------------------ gather
+//
+// One lane per point: the lane reads its point's three table rows of the
+// component (bases and four weights per axis, one 32-byte row each) and sums
+// the 64 links over the component's face patch in shared memory (fixed
+// strides, runs.cuh), or over the face array where the element's box does
+// not fit.  The velocities U_c(x_q) of up to 64 points are kept in shared
+// memory and assembled by lanes (a, c) in point order:
+// rhs[a][c] = sum_q N[q,a] W_q U_c(x_q) (mac/csrc/p2_transfer.cu:150-188).
+
+constexpr int kGatherPoints = 64;
+
+template <class T>
+struct GatherStage {
+    T patch[kGPatch];
+    T u[3][kGatherPoints];
+    T w[kGatherPoints];
+};
 
 template <class T, bool Local>
 __global__ void __launch_bounds__(kWarps * 32, kGatherBlocks) p2_gather_kernel(const T* __restrict__ u0, const T* __restrict__ u1,
@@ -531,11 +493,11 @@ __global__ void __launch_bounds__(kWarps * 32, kGatherBlocks) p2_gather_kernel(c
                                                                 const int64_t* __restrict__ base,
                                                                 const T* __restrict__ phi, T* __restrict__ out,
                                                                 P2Dims g, int32_t* status) {
-    __shared__ GatherStage<T> stage_all[kWarps];
+    __shared__ __align__(16) GatherStage<T> stage_all[kWarps];
     GatherStage<T>& s = stage_all[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31, grp = lane >> 3, li = (lane >> 1) & 3, ljp = lane & 1, sub = lane & 7;
+    const int lane = threadIdx.x & 31;
     const int64_t warps = int64_t(gridDim.x) * kWarps;
-    const T* fields[3] = {u0, u1, u2};
+    using P = typename Pair<T>::type;
     for (int64_t e = int64_t(blockIdx.x) * kWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
         const int64_t node = lane < 10 ? cells[e * 10 + lane] : 0;
         if (__any_sync(0xffffffffu, lane < 10 && (node < 0 || node >= g.nodes))) {
@@ -544,96 +506,69 @@ __global__ void __launch_bounds__(kWarps * 32, kGatherBlocks) p2_gather_kernel(c
         }
         Box bx;
         element_box(base, g, e, bx);
-        const bool fits = box_fits<T>(bx, g);
-        __syncwarp();
-        if (fits) {
-#pragma unroll
+        T acc = T(0);  // lane (a, cc) = (lane / 3, lane % 3), lane < 30
+        for (int64_t q0 = 0; q0 < g.nq; q0 += kGatherPoints) {
+            const int n = int(g.nq - q0 < kGatherPoints ? g.nq - q0 : kGatherPoints);
+            __syncwarp();
+            for (int q = lane; q < n; q += 32) s.w[q] = W[e * g.nq + q0 + q];
+#pragma unroll 1
             for (int c = 0; c < 3; ++c) {
-                box_walk(lane, bx.ext[c][0], bx.ext[c][1], bx.ext[c][2], [&](int t, int x, int y, int z) {
-                    s.patch[bx.off[c] + t] = fields[c][face_index(g, c, bx.lo[c][0] + x, bx.lo[c][1] + y,
-                                                                  bx.lo[c][2] + z)];
-                });
-            }
-        }
-        __syncwarp();
-        // lane sub of each group accumulates nodes a = sub and sub+8 over the group's points
-        T acc[2][3] = {{T(0), T(0), T(0)}, {T(0), T(0), T(0)}};
-#pragma unroll 2
-        for (int64_t qb = 0; qb < g.nq; qb += 4) {
-            const int64_t q = qb + grp;
-            const bool active = q < g.nq;
-            const int64_t row = g.offset + e * g.nq + (active ? q : 0);
-            T U[3];
+                const T* field = c == 0 ? u0 : c == 1 ? u1 : u2;
+                bool fits = component_inside(bx, g, c);
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                PointView<T> v;
-                point_view(base, phi, g.total, row, c, li, ljp, v);
-                T s0 = T(0), s1 = T(0);
-                if (active) {
-                    const T* src = nullptr;
-                    int64_t sy = 0;
+                for (int a = 0; a < 3; ++a) fits = fits && bx.ext[c][a] <= kGExt;
+                __syncwarp();  // the previous component's patch reads are done
+                if (fits)
+                    box_walk(lane, bx.ext[c][0], bx.ext[c][1], bx.ext[c][2], [&](int, int x, int y, int z) {
+                        s.patch[x * kGSX + y * kGSY + z] =
+                            field[face_index(g, c, bx.lo[c][0] + x, bx.lo[c][1] + y, bx.lo[c][2] + z)];
+                    });
+                __syncwarp();
+#pragma unroll
+                for (int j = 0; j < kGatherPoints / 32; ++j) {
+                    const int q = lane + 32 * j;
+                    if (q >= n) continue;
+                    const int64_t row = g.offset + e * g.nq + q0 + q;
+                    int b[3];
+                    T wr[3][4];
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        const int64_t ra = table_row(g.total, row, c, a);
+                        b[a] = int(base[ra]);
+                        const P w01 = reinterpret_cast<const P*>(phi + ra * 4)[0];
+                        const P w23 = reinterpret_cast<const P*>(phi + ra * 4)[1];
+                        wr[a][0] = w01.x;
+                        wr[a][1] = w01.y;
+                        wr[a][2] = w23.x;
+                        wr[a][3] = w23.y;
+                    }
+                    T U = T(0);
                     if (fits) {
-                        src = s.patch + bx.off[c] +
-                              ((v.gx - bx.lo[c][0] + li) * bx.ext[c][1] + (v.gy - bx.lo[c][1] + 2 * ljp)) *
-                                  bx.ext[c][2] +
-                              (v.gz - bx.lo[c][2]);
-                        sy = bx.ext[c][2];
-                    } else if (point_inside(g, c, v.gx, v.gy, v.gz)) {
-                        src = fields[c] + face_index(g, c, v.gx + li, v.gy + 2 * ljp, v.gz);
-                        sy = g.nz + (c == 2);
-                    } else if (sub == 0) {
+                        const T* p0 =
+                            s.patch + (b[0] - bx.lo[c][0]) * kGSX + (b[1] - bx.lo[c][1]) * kGSY + (b[2] - bx.lo[c][2]);
+                        U = support_dot(p0, kGSX, kGSY, wr[0], wr[1], wr[2]);
+                    } else if (point_inside(g, c, b[0], b[1], b[2])) {
+                        const int64_t sz = g.nz + (c == 2), sy = (g.ny + (c == 1)) * sz;
+                        U = support_dot(field + face_index(g, c, b[0], b[1], b[2]), sy, sz, wr[0], wr[1], wr[2]);
+                    } else {
                         flag(status, AFSI_FLAG_INDEX);
                     }
-                    if (src) {
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            s0 = fma(src[k], v.wz[k], s0);
-                            s1 = fma(src[sy + k], v.wz[k], s1);
-                        }
-                    }
+                    s.u[c][q] = U;
                 }
-                T sum = v.wx * (v.wy0 * s0 + v.wy1 * s1);
-                sum += __shfl_xor_sync(0xffffffffu, sum, 1);
-                sum += __shfl_xor_sync(0xffffffffu, sum, 2);
-                sum += __shfl_xor_sync(0xffffffffu, sum, 4);
-                U[c] = sum;
             }
-            if (active) {
-                const T wq = W[e * g.nq + q];
-#pragma unroll
-                for (int m = 0; m < 2; ++m) {
-                    const int a = sub + 8 * m;
-                    if (a < 10) {
-                        const T nw = N[q * 10 + a] * wq;
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) acc[m][c] = fma(nw, U[c], acc[m][c]);
-                    }
-                }
+            __syncwarp();
+            if (lane < 30) {
+                const int a = lane / 3, cc = lane - 3 * (lane / 3);
+                for (int q = 0; q < n; ++q) acc = fma(N[(q0 + q) * 10 + a] * s.w[q], s.u[cc][q], acc);
             }
         }
-        // combine the four groups: node a sums lanes sub, sub+8, sub+16, sub+24
-#pragma unroll
-        for (int m = 0; m < 2; ++m)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                T v = acc[m][c];
-                v += __shfl_xor_sync(0xffffffffu, v, 8);
-                v += __shfl_xor_sync(0xffffffffu, v, 16);
-                acc[m][c] = v;
-            }
-#pragma unroll
-        for (int m = 0; m < 2; ++m) {
-            const int a = sub + 8 * m;
-            const int64_t nd = __shfl_sync(0xffffffffu, node, a < 10 ? a : 0);
-            if (grp == 0 && a < 10) {
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    if (Local)
-                        out[(e * 10 + a) * 3 + c] = acc[m][c];
-                    else
-                        atomicAdd(out + nd * 3 + c, acc[m][c]);
-                }
-            }
+        const int64_t nd = __shfl_sync(0xffffffffu, node, lane < 30 ? lane / 3 : 0);
+        if (lane < 30) {
+            const int a = lane / 3, cc = lane - 3 * (lane / 3);
+            if (Local)
+                out[(e * 10 + a) * 3 + cc] = acc;
+            else
+                atomicAdd(out + nd * 3 + cc, acc);
         }
         __syncwarp();
     }

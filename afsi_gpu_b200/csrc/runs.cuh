@@ -179,4 +179,35 @@ __device__ __forceinline__ void spread_element(T* box, const int* key, const T* 
         spread_runs<T, C>(box, key, f, wx, wy, wz, n, sx, sy);
 }
 
+// ------------------------------------------------------------------ gather
+//
+// Face patch of one component for the lane-per-point gathers: entry (x,y,z)
+// at x*kGSX + y*kGSY + z with fixed strides, so the 64 loads of a support
+// have immediate offsets; kGSX = 68 (4 mod 16) and kGSY = 8 put the support
+// origins of nearby points in different bank pairs, and lanes whose points
+// share an origin read the same words.  Extents up to kGExt per axis.
+constexpr int kGSX = 68, kGSY = 8, kGExt = 8;
+constexpr int kGPatch = kGExt * kGSX;
+
+// sum_ijk wx[i] wy[j] wz[k] p[i*sx + j*sy + k]
+template <class T, class I>
+__device__ __forceinline__ T support_dot(const T* p, I sx, I sy, const T wx[4], const T wy[4], const T wz[4]) {
+    T u = T(0);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        T ti = T(0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const T* r = p + i * sx + j * sy;
+            T tz = r[0] * wz[0];
+            tz = fma(r[1], wz[1], tz);
+            tz = fma(r[2], wz[2], tz);
+            tz = fma(r[3], wz[3], tz);
+            ti = fma(wy[j], tz, ti);
+        }
+        u = fma(wx[i], ti, u);
+    }
+    return u;
+}
+
 }  // namespace afsi
