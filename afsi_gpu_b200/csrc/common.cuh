@@ -87,6 +87,21 @@ __device__ __forceinline__ double sum_partials(const double* partial, int count,
 // after every block of this one has started, so waiting blocks never hold back
 // a kernel they depend on.  Both are no-ops for a launch without the
 // programmatic-serialization attribute.
+// 1/v when v is a positive normal power of two whose reciprocal is normal
+// (then x * (1/v) rounds exactly as x / v), else 0.
+template <class T>
+__device__ __forceinline__ T exact_reciprocal(T v) {
+    if constexpr (sizeof(T) == 8) {
+        const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(double(v)));
+        const unsigned e = unsigned(b >> 52) & 0x7FFu;
+        return ((b & 0x800FFFFFFFFFFFFFull) == 0 && e > 0 && e <= 0x7FDu) ? T(1) / v : T(0);
+    } else {
+        const unsigned b = __float_as_uint(float(v));
+        const unsigned e = (b >> 23) & 0xFFu;
+        return ((b & 0x807FFFFFu) == 0 && e > 0 && e <= 0xFDu) ? T(1) / v : T(0);
+    }
+}
+
 __device__ __forceinline__ void pdl_enter() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     asm volatile("griddepcontrol.wait;" ::: "memory");

@@ -282,7 +282,7 @@ template <class TP, class T, int NPC>
 __device__ __forceinline__ void component_pass(FStage<TP, T, NPC>& s, const TP* __restrict__ Npos,
                                                const T* __restrict__ N, const T* __restrict__ W, bool resident,
                                                unsigned long long valid_bits, int64_t e, int64_t nq, int64_t q0,
-                                               int n, const Geo<TP>& geo, int c, const T* coef, T volume, int mn[3],
+                                               int n, const Geo<TP>& geo, int c, const T* coef, T volume, T inv_volume, int mn[3],
                                                int mx[3]) {
     const int lane = threadIdx.x & 31;
 #pragma unroll 1
@@ -311,7 +311,8 @@ __device__ __forceinline__ void component_pass(FStage<TP, T, NPC>& s, const TP* 
             T F = T(0);
 #pragma unroll
             for (int a = 0; a < NPC; ++a) F += N[(q0 + q) * NPC + a] * coef[a * 3 + c];
-            s.f[q] = (F * W[e * nq + q0 + q]) / volume;
+            const T fw = F * W[e * nq + q0 + q];
+            s.f[q] = inv_volume != T(0) ? fw * inv_volume : fw / volume;
         }
     }
 }
@@ -341,6 +342,7 @@ __global__ void __launch_bounds__(kFWarps * 32, 8) fused_spread_kernel(
     const int lane = threadIdx.x & 31, half = lane >> 4, li = (lane >> 2) & 3, lj = lane & 3;
     const int64_t warps = int64_t(gridDim.x) * kFWarps;
     const bool resident = g.nq <= C;
+    const T inv_volume = exact_reciprocal(volume);
     for (int64_t e = int64_t(blockIdx.x) * kFWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
         int64_t node;
         if (!stage_element<TP, T, NPC>(x, cells, value, e, g.nodes, s.xs, s.coef, node, status)) continue;
@@ -360,7 +362,7 @@ __global__ void __launch_bounds__(kFWarps * 32, 8) fused_spread_kernel(
                 int mn[3], mx[3];
                 bounds_init(mn, mx);
                 component_pass<TP, T, NPC>(s, Npos, N, W, resident, valid, e, g.nq, q0, n, geo, c, s.coef, volume,
-                                           mn, mx);
+                                           inv_volume, mn, mx);
                 if (resident) {
                     any = bounds_finish(mn, mx, bx);
                     if (!any) break;

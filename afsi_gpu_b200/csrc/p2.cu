@@ -181,6 +181,7 @@ __global__ void __launch_bounds__(kWarps * 32, kSpreadBlocks) p2_spread_kernel(
     SpreadStage<T>& s = stage_all[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31, half = lane >> 4, li = (lane >> 2) & 3, lj = lane & 3;
     const int64_t warps = int64_t(gridDim.x) * kWarps;
+    const T inv_volume = exact_reciprocal(volume);
     for (int64_t e = int64_t(blockIdx.x) * kWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
         const int64_t node = lane < 10 ? cells[e * 10 + lane] : 0;
         if (__any_sync(0xffffffffu, lane < 10 && (node < 0 || node >= g.nodes))) {
@@ -208,7 +209,8 @@ __global__ void __launch_bounds__(kWarps * 32, kSpreadBlocks) p2_spread_kernel(
                     T F = T(0);
 #pragma unroll
                     for (int a = 0; a < 10; ++a) F += N[(q0 + q) * 10 + a] * s.coef[a * 3 + c];
-                    s.f[q] = (F * W[e * g.nq + q0 + q]) / volume;
+                    const T fw = F * W[e * g.nq + q0 + q];
+                    s.f[q] = inv_volume != T(0) ? fw * inv_volume : fw / volume;
                 }
                 __syncwarp();
 #pragma unroll 2
@@ -333,6 +335,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 6) p2_spread_rows_kernel(
     const int lane = threadIdx.x & 31, half = lane >> 4, li = (lane >> 2) & 3, lj = lane & 3;
     const int64_t warps = int64_t(gridDim.x) * kRowWarps;
     const int n = int(g.nq);
+    const T inv_volume = exact_reciprocal(volume);
     // weights: n*12*sizeof(T) bytes per lattice, a multiple of 16 (n even for T=float)
     const unsigned phi_bytes = unsigned(n * 12 * int(sizeof(T)));
     const bool phi_bulk = phi_bytes % 16 == 0;
@@ -433,7 +436,8 @@ __global__ void __launch_bounds__(kRowWarps * 32, 6) p2_spread_rows_kernel(
                 T F = T(0);
 #pragma unroll
                 for (int a = 0; a < 10; ++a) F += N[q * 10 + a] * s.coef[a * 3 + c];
-                s.f[q] = (F * W[e * g.nq + q]) / volume;
+                const T fw = F * W[e * g.nq + q];
+                s.f[q] = inv_volume != T(0) ? fw * inv_volume : fw / volume;
                 if (fits)
                     s.key[q] = run_key(int(s.base[tx][q * 3]) - bx.lo[c][0], int(s.base[ty][q * 3 + 1]) - bx.lo[c][1],
                                        int(s.base[tz][q * 3 + 2]) - bx.lo[c][2]);

@@ -126,9 +126,14 @@ class Clocks:
 # ----------------------------------------------------------------- the step
 
 class Step:
-    """Device-resident inputs; one call = one hot-path step."""
+    """Device-resident inputs; one call = one hot-path step.
 
-    def __init__(self, grid, X, cells, coef, vel, rhs, device):
+    form: 'table-free' (the transfer kernels form each point's position, bases
+    and weights themselves; the prepare selects and checks the rule) or
+    'tables' (the prepare writes the (2,P,3) / (2,P,3,4) stencil tables that the
+    spread and gather-assemble read back, the reference's P2 transfer)."""
+
+    def __init__(self, grid, X, cells, coef, vel, rhs, device, form='table-free'):
         from afsi_gpu_b200 import p2_cuda_transfer as p2t
         from afsi_gpu_b200.multigrid import GeometricMultigrid
         self.p2t = p2t
@@ -140,6 +145,7 @@ class Step:
         self.rhs = torch.as_tensor(rhs, device=device)
         self.tr = p2t.P2Transfer(grid, self.x, self.cells)
         self.mg = GeometricMultigrid(grid, device=device, backend='b200-graph')
+        self.form = form
         self.events = None
         self.cycles = []
 
@@ -152,7 +158,8 @@ class Step:
         # rule selection without a host read: the prepare runs with the cached
         # rule and is confirmed after the solve's own host read; a changed rule
         # (never on this workload) redoes the transfers
-        deferred = self.tr.prepare_deferred(self.x if x is None else x)
+        x = self.x if x is None else x
+        deferred = self.tr.prepare_table_free(x) if self.form == 'table-free' else self.tr.prepare_deferred(x)
         st = deferred.stencil
         if ev is not None:
             ev[1].record()
@@ -174,6 +181,16 @@ class Step:
             nodal = self.p2t.assemble_velocity(self.tr, vel, st)
         self.cycles.append(info['cycles'])
         return st, fields, nodal, p
+
+
+def algorithmic_bytes_table_free(points, elements, nodes, faces, s=8):
+    """Bytes a table-free transfer launch must move at minimum: node
+    positions and element connectivity (3*s per node, 80 per element), W
+    (s per point), the rule tables (negligible), the nodal values (3*s per
+    node) and the face field read and written (2*s per face; the gather reads
+    it once and writes the nodal rhs, 3*s per node)."""
+    common = nodes * 3 * s + elements * 80 + points * s + nodes * 3 * s
+    return dict(spread=common + 2 * faces * s, gather=common + faces * s + nodes * 3 * s)
 
 
 def algorithmic_bytes(points, elements, nodes, faces, s=8):
@@ -774,6 +791,39 @@ def p1_oracle_errors(grid, X, cells, coef, vel, rhs, device, forms, sample_eleme
     return out
 
 
+def table_form_row(grid, X, cells, coef, vel, rhs, device, steps, warmup, pk):
+    """The headline step with the stencil tables (the reference's P2 transfer:
+    the prepare writes the (2,P,3) / (2,P,3,4) tables, the spread and
+    gather-assemble read them back), timed like the headline but without the
+    flush (590 MB of tables per step exceed L2): steps/s, the phases, and the
+    HBM roofline of its spread and gather-assemble kernels."""
+    step = Step(grid, X, cells, coef, vel, rhs, device, form='tables')
+    for _ in range(max(warmup, 3)):
+        step()
+    torch.cuda.synchronize(device)
+    evs = []
+    for _ in range(steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(9)]
+        step(timing=ev)
+        evs.append(ev)
+    torch.cuda.synchronize(device)
+    elapsed = sum(ev[0].elapsed_time(ev[4]) for ev in evs) / 1e3
+    names = ('prepare', 'spread', 'gather_assemble', 'mg_solve')
+    phase_ms = {n: float(np.mean([ev[i].elapsed_time(ev[i + 1]) for ev in evs])) for i, n in enumerate(names)}
+    P = step.tr.rule(step.x).point_count
+    faces = sum(np.prod(grid.face_shape(c)) for c in range(3))
+    ab = algorithmic_bytes(P, cells.shape[0], X.shape[0], faces)
+    traffic = load_traffic()
+    out = dict(steps_per_s=steps / elapsed, ms_per_step=elapsed / steps * 1e3, phases_ms=phase_ms)
+    for key, name, a, b in (('spread', 'p2_spread', 5, 6), ('gather', 'p2_gather_assemble', 7, 8)):
+        dt = float(np.mean([ev[a].elapsed_time(ev[b]) for ev in evs])) / 1e3
+        achieved = ab[key] / dt / 1e9
+        out[f'roofline_{key}'] = dict(bound='hbm', kernel=name, achieved=achieved, peak=pk['hbm_gbs'], unit='GB/s',
+                                      frac=achieved / pk['hbm_gbs'], traffic=traffic.get(name),
+                                      algorithmic_bytes=ab[key], launch_ms=dt * 1e3)
+    return out
+
+
 def deterministic_row(step, coef, device, reps=10):
     """The P2 spread of the step in its deterministic mode (tile-sorted,
     atomic-free, bitwise reproducible) beside the atomic spread: CUDA events
@@ -1023,8 +1073,12 @@ def run_b200(args):
     from afsi_gpu_b200 import _lib
     _lib.load()
     grid, X, cells, coef, vel, rhs = workload()
-    step = Step(grid, X, cells, coef, vel, rhs, device)
+    step = Step(grid, X, cells, coef, vel, rhs, device, form='table-free')
     stream = torch.cuda.current_stream(device)
+    # the table-free step's inputs and fields fit in L2 (126 MB): every timed
+    # step starts from a flushed L2 (a 256 MB buffer written just before it,
+    # outside the step's events)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=device)
 
     def barrier():
         if dist:
@@ -1042,12 +1096,14 @@ def run_b200(args):
         start.record(stream)
         for _ in range(args.steps):
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(9)]
+            flush.zero_()
             step(timing=ev)
             phases.append(ev)
         stop.record(stream)
         barrier()
     launches = _lib.launch_count() - launches0
-    elapsed = max_over_ranks(start.elapsed_time(stop) / 1e3, dist, device)
+    # the K steps' device time, each from the start of its prepare to the end of its solve
+    elapsed = max_over_ranks(sum(ev[0].elapsed_time(ev[4]) for ev in phases) / 1e3, dist, device)
     names = ('prepare', 'spread', 'gather_assemble', 'mg_solve')
     phase_ms = {n: float(np.mean([ev[i].elapsed_time(ev[i + 1]) for ev in phases])) for i, n in enumerate(names)}
     spread_t = float(np.mean([ev[5].elapsed_time(ev[6]) for ev in phases])) / 1e3
@@ -1123,9 +1179,10 @@ def run_b200(args):
         pk, pk_kind = peaks()
         P = step.tr.rule(step.x).point_count
         faces = sum(np.prod(grid.face_shape(c)) for c in range(3))
-        ab = algorithmic_bytes(P, cells.shape[0], X.shape[0], faces)
-        dominant, dt = ('p2_spread', spread_t) if spread_t >= gather_t else ('p2_gather_assemble', gather_t)
-        byte_key = 'spread' if dominant == 'p2_spread' else 'gather'
+        ab = algorithmic_bytes_table_free(P, cells.shape[0], X.shape[0], faces)
+        dominant, dt = (('p2_fused_spread', spread_t) if spread_t >= gather_t else
+                        ('p2_fused_gather_assemble', gather_t))
+        byte_key = 'spread' if dominant == 'p2_fused_spread' else 'gather'
         achieved = ab[byte_key] / dt / 1e9
         traffic = load_traffic().get(dominant)
         cpu = None
@@ -1149,6 +1206,7 @@ def run_b200(args):
         if extra:
             precision['p1_128'] = precision_p1_row(device)
         deterministic = deterministic_row(step, coef, device) if extra else None
+        tables = table_form_row(grid, X, cells, coef, vel, rhs, device, args.steps, args.warmup, pk) if extra else None
         batch = batch_form_row(device) if extra else None
         config1 = config1_row(device) if extra else None
         stokes = stokes_row(grid, device) if extra else None
@@ -1162,13 +1220,19 @@ def run_b200(args):
                         grid=list(GRID['shape']), elements=int(cells.shape[0]), points=int(P),
                         mg='Neumann V-cycles to 1e-10, Jacobi 2/3 x4, graph-replayed blocks of 2, cycles per solve '
                            f'{sorted(set(step.cycles))}',
-                        l2='inputs larger than L2 (590 MB of stencil tables per step)',
+                        transfers='table-free: the spread and gather-assemble kernels form each point\'s position, '
+                                  'bases and IB_4 weights from the nodal positions (no stencil tables); the prepare '
+                                  'selects and checks the rule',
+                        l2='L2 flushed before every timed step (256 MB written outside the step\'s events)',
                         parallelism=f'replicas x{world}'),
             roofline=dict(bound='hbm', kernel=dominant, achieved=achieved, peak=pk['hbm_gbs'], unit='GB/s',
                           frac=achieved / pk['hbm_gbs'], peak_kind=pk_kind,
                           traffic=(traffic * 1.0 if traffic else None),
                           algorithmic_bytes=ab[byte_key], launch_ms=dt * 1e3,
-                          phases_ms=phase_ms),
+                          phases_ms=phase_ms,
+                          note='the table-free kernels move about 40 MB per launch and are bound by FP64 issue and '
+                               'latency, not HBM; the table form (the same step with stencil tables, '
+                               'table_form_step) carries the HBM-bound roofline of its spread'),
             e2e=dict(value=whole_job_rate(world, e2e_steps, e2e_elapsed), unit='steps/s', h2d_bytes_per_step=int(h2d),
                      d2h_bytes_per_step=int(d2h)),
             gpu_launches=int(launches),
@@ -1180,6 +1244,7 @@ def run_b200(args):
             mg_forms=forms,
             precision_form=precision,
             deterministic_spread=deterministic,
+            table_form_step=tables,
             batch_form=batch,
             config1=config1,
             stokes_fgmres=stokes,
