@@ -215,15 +215,15 @@ __device__ __forceinline__ bool stage_element(const TP* __restrict__ x, const in
 // Per-warp shared memory of both kernels.
 template <class TP, class T, int NPC>
 struct __align__(16) FStage {
-    T w[FChunk<NPC>::value * 12];      // one component's rows: x at q*12, y at q*12+4, z at q*12+8
+    T w[(FChunk<NPC>::value + 1) * 12];  // one component's rows: x at q*12, y at q*12+4, z at q*12+8; the last stays zero
     TP pos[FChunk<NPC>::value * 3];    // positions of a resident rule
     int b[FChunk<NPC>::value * 3];     // support origins (absolute) of the component
     int key[FChunk<NPC>::value];       // run keys in the box, -1 for an invalid point
-    T f[FChunk<NPC>::value];           // spread: force factors of the component
+    T f[FChunk<NPC>::value + 1];       // spread: force factors of the component; the last stays zero
     T box[kFBoxCap];                   // padded box
     T coef[32];
     TP xs[32];
-    int perm[FChunk<NPC>::value];      // points grouped by key (spread_element)
+    int perm[4 * FChunk<NPC>::value];  // points grouped by key (spread_element)
     int rs[FChunk<NPC>::value + 1], rk[FChunk<NPC>::value];
 };
 
@@ -343,6 +343,9 @@ __global__ void __launch_bounds__(kFWarps * 32, 8) fused_spread_kernel(
     const int64_t warps = int64_t(gridDim.x) * kFWarps;
     const bool resident = g.nq <= C;
     const T inv_volume = exact_reciprocal(volume);
+    if (lane < 12) s.w[C * 12 + lane] = T(0);
+    if (lane == 0) s.f[C] = T(0);
+    __syncwarp();
     for (int64_t e = int64_t(blockIdx.x) * kFWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
         int64_t node;
         if (!stage_element<TP, T, NPC>(x, cells, value, e, g.nodes, s.xs, s.coef, node, status)) continue;

@@ -314,13 +314,13 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 
 template <class T>
 struct __align__(16) RowStage {  // size a multiple of 16: every warp's copy targets start 16-byte aligned
-    T phi[2][kRowPoints * 12];
+    T phi[2][(kRowPoints + 1) * 12];  // row kRowPoints stays zero (spread_element's padding row)
     int64_t base[2][kRowPoints * 3];
-    T f[kRowPoints];
+    T f[kRowPoints + 1];
     T coef[32];
     T box[kSpreadCap];
     int key[kRowPoints];
-    int perm[kRowPoints];       // points grouped by key (spread_element)
+    int perm[4 * kRowPoints];   // points grouped by key (spread_element)
     int rs[kRowPoints + 1], rk[kRowPoints];
     unsigned long long bar;  // completion of this warp's bulk copies
 };
@@ -340,6 +340,8 @@ __global__ void __launch_bounds__(kRowWarps * 32, 6) p2_spread_rows_kernel(
     const unsigned phi_bytes = unsigned(n * 12 * int(sizeof(T)));
     const bool phi_bulk = phi_bytes % 16 == 0;
     if (lane == 0) mbar_init(&s.bar);
+    if (lane < 24) s.phi[lane / 12][kRowPoints * 12 + lane % 12] = T(0);
+    if (lane == 0) s.f[kRowPoints] = T(0);
     __syncwarp();
     unsigned parity = 0;
     for (int64_t e = int64_t(blockIdx.x) * kRowWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {

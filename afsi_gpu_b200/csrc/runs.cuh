@@ -78,43 +78,38 @@ __device__ __forceinline__ void spread_runs(T* box, const int* key, const T* f, 
     }
 }
 
-// Groups points 0..n-1 (n <= C) by key: perm lists the points with key >= 0
-// run by run (keys in order of first appearance, points of a run in index
-// order); run r spans perm[rs[r] .. rs[r+1]) and has key rk[r].  Returns the
-// number of runs.  Lane 0 writes rs and rk; perm is written by the lanes of
-// the points.
+// Groups points 0..n-1 (n <= C) by key, 32 points at a time (one per
+// lane, __match_any_sync): perm lists, run by run, the points of one key
+// among points j*32 .. j*32+31 in index order, padded with `zero` (the index of
+// an all-zero row) to a multiple of four; run r spans perm[rs[r] .. rs[r+1])
+// and has key rk[r].  Points with key < 0 take no part.  perm needs room for
+// 4 n entries.  Returns the number of runs.
 template <int C>
-__device__ __forceinline__ int group_runs(const int* key, int n, int* perm, int* rs, int* rk) {
-    constexpr int J = C / 32;
+__device__ __forceinline__ int group_runs(const int* key, int n, int* perm, int* rs, int* rk, int zero) {
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
-    int k[J];
-    unsigned rem[J];
-#pragma unroll
-    for (int j = 0; j < J; ++j) {
-        const int q = lane + 32 * j;
-        k[j] = q < n ? key[q] : -1;
-        rem[j] = __ballot_sync(0xffffffffu, k[j] >= 0);
-    }
     int pos = 0, r = 0;
-    while (true) {
-        int K = -1;
 #pragma unroll
-        for (int j = J - 1; j >= 0; --j)
-            if (rem[j]) K = __shfl_sync(0xffffffffu, k[j], __ffs(rem[j]) - 1);
-        if (K < 0) break;
-        if (lane == 0) {
-            rs[r] = pos;
-            rk[r] = K;
+    for (int j = 0; j < C / 32; ++j) {
+        const int q = lane + 32 * j;
+        const int k = q < n ? key[q] : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, k);
+        unsigned leaders = __ballot_sync(0xffffffffu, k >= 0 && (peers & below) == 0u);
+        while (leaders) {
+            const int l = __ffs(leaders) - 1;
+            leaders &= leaders - 1u;
+            const unsigned grp = __shfl_sync(0xffffffffu, peers, l);
+            const int kl = __shfl_sync(0xffffffffu, k, l);
+            const int cnt = __popc(grp), padded = (cnt + 3) & ~3;
+            if ((grp >> lane) & 1u) perm[pos + __popc(grp & below)] = q;
+            if (lane < padded - cnt) perm[pos + cnt + lane] = zero;
+            if (lane == 0) {
+                rs[r] = pos;
+                rk[r] = kl;
+            }
+            pos += padded;
+            ++r;
         }
-#pragma unroll
-        for (int j = 0; j < J; ++j) {
-            const unsigned g = __ballot_sync(0xffffffffu, k[j] == K);
-            if ((g >> lane) & 1u) perm[pos + __popc(g & below)] = lane + 32 * j;
-            pos += __popc(g);
-            rem[j] &= ~g;
-        }
-        ++r;
     }
     if (lane == 0) rs[r] = pos;
     __syncwarp();
@@ -135,23 +130,27 @@ __device__ __forceinline__ void mma884(double d[2], double a, double b) {
 // S[i][j][k] = sum_p X_p[i] (f_p Y_p[j] Z_p[k]) is the product of the 4 x L
 // matrix of x weights and the L x 16 matrix of (f Y (x) Z) rows, taken four
 // points at a time by two m8n8k4 steps (j = 0-1 and j = 2-3; rows 4-7 of A
-// are zero).  Lanes 0-15 then add their two pairs of z links to the box.
+// read the zero row).  Lanes 0-15 then add their two pairs of z links to the
+// box.  Row `zero` (index C) of wx/wy/wz and f must be all zero; perm, rs and
+// rk are group_runs' scratch.
 template <int C>
 __device__ __forceinline__ void spread_runs_mma(double* box, const int* key, const double* f, const double* wx,
                                                 const double* wy, const double* wz, int n, int sx, int sy,
                                                 int* perm, int* rs, int* rk) {
     const int lane = threadIdx.x & 31;
-    const int runs = group_runs<C>(key, n, perm, rs, rk);
+    const int runs = group_runs<C>(key, n, perm, rs, rk, C);
     const int slot = lane & 3, row = lane >> 2;     // A: x offset `row`, point `slot`
     const int jb = lane >> 4, kb = (lane >> 2) & 3;  // B column lane/4 = (j, k) = (jb [+2], kb)
+    const int ax = row & 3;
     for (int r = 0; r < runs; ++r) {
         const int s0 = rs[r], e0 = rs[r + 1], K = rk[r];
         double d0[2] = {0.0, 0.0}, d1[2] = {0.0, 0.0};
-        for (int b = s0; b < e0; b += 4) {
-            const bool live = b + slot < e0;
-            const int q = perm[live ? b + slot : s0];
-            const double a = (live && row < 4) ? wx[q * 12 + (row & 3)] : 0.0;
-            const double fz = live ? f[q] * wz[q * 12 + kb] : 0.0;
+#pragma unroll 2
+        for (int b = s0 + slot; b < e0; b += 4) {
+            const int q = perm[b];
+            const int qa = row < 4 ? q : C;
+            const double a = wx[qa * 12 + ax];
+            const double fz = f[q] * wz[q * 12 + kb];
             mma884(d0, a, wy[q * 12 + jb] * fz);
             mma884(d1, a, wy[q * 12 + jb + 2] * fz);
         }
