@@ -229,8 +229,9 @@ __global__ void __launch_bounds__(kCoarseThreads) cluster_kernel(const T* __rest
                                                                 const double* rhs_sum, const T* p_global, T* p_out,
                                                                 const TC* __restrict__ cinv, ClusterLevels<T> cl,
                                                                 int smooth) {
-    pdl_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    cluster_tables<BC, T>(reinterpret_cast<T*>(smem_raw), cl);
+    pdl_enter();
     cluster_cycle<BC, T, TC>(reinterpret_cast<T*>(smem_raw), rhs_global, rhs_sum, p_global, p_out, cinv, cl, smooth);
 }
 
@@ -521,13 +522,17 @@ struct Runner {
             cfg.blockDim = dim3(kCoarseThreads);
             cfg.dynamicSmemBytes = cluster_bytes;
             cfg.stream = stream;
-            cudaLaunchAttribute attr;
-            attr.id = cudaLaunchAttributeClusterDimension;
-            attr.val.clusterDim.x = cluster_size;
-            attr.val.clusterDim.y = 1;
-            attr.val.clusterDim.z = 1;
-            cfg.attrs = &attr;
-            cfg.numAttrs = 1;
+            // programmatic dependent launch as for the level kernels: the cluster's
+            // CTAs may start while the restriction drains and wait in pdl_enter
+            cudaLaunchAttribute attr[2];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = cluster_size;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attr[1].val.programmaticStreamSerializationAllowed = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 2;
             const cudaError_t err =
                 cudaLaunchKernelEx(&cfg, cluster_kernel<BC, T, TC>, static_cast<const T*>(R(l)), rhs_sum,
                                    static_cast<const T*>(l == 0 ? P(0) : nullptr), P(l),

@@ -58,17 +58,28 @@ __device__ __forceinline__ Slab<T> slab_of(const T* local, int rank, int ranks) 
     return s;
 }
 
-// Cluster-wide sum, identical in every CTA: one block barrier, one cluster
-// barrier.  slot: two doubles per CTA (alternating), red: block scratch.
-__device__ __forceinline__ double cluster_sum(double v, double* slot, int& parity, double (*red)[32], int& rt,
-                                              int ranks) {
+// Cluster-wide sum, identical in every CTA: the CTA sums are added in rank
+// order.  One block barrier, one cluster barrier, then warp 0 reads the
+// ranks' sums (lane r from rank r, one distributed-shared-memory round trip
+// per CTA instead of one per thread and rank) and publishes the total.
+// slot: two doubles per CTA (alternating), bcast: two doubles (alternating),
+// red: block scratch.
+__device__ __forceinline__ double cluster_sum(double v, double* slot, double* bcast, int& parity, double (*red)[32],
+                                              int& rt, int ranks) {
     const double mine = block_sum_all(v, red[rt]);
     rt ^= 1;
     if (threadIdx.x == 0) slot[parity] = mine;
     cg::this_cluster().sync();
-    double total = 0.0;
-    for (int r = 0; r < ranks; ++r)
-        total += static_cast<const double*>(__cluster_map_shared_rank(slot, r))[parity];
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        const double x =
+            lane < ranks ? static_cast<const double*>(__cluster_map_shared_rank(slot, lane))[parity] : 0.0;
+        double total = 0.0;
+        for (int r = 0; r < ranks; ++r) total += __shfl_sync(0xffffffffu, x, r);
+        if (lane == 0) bcast[parity] = total;
+    }
+    __syncthreads();
+    const double total = bcast[parity];
     parity ^= 1;
     return total;
 }
@@ -107,8 +118,8 @@ __device__ __forceinline__ void slab_coords(int i, const Lv<T>& L, int& xl, int&
 // the pending mean (singular BCs) of the level's iterate over the cluster.
 template <int BC, class T>
 __device__ T* dist_smooth(T* cur, T* oth, T* R, const ClusterLevel<T>& lv, const T* wrd, int smooth, bool zero,
-                          T rhs_shift, int rank, int ranks, double* slot, int& parity, double (*red)[32], int& rt,
-                          T* mean) {
+                          T rhs_shift, int rank, int ranks, double* slot, double* bcast, int& parity, double (*red)[32],
+                          int& rt, T* mean) {
     constexpr bool singular = singular_bc(BC);
     const Lv<T>& L = lv.L;
     const int x0 = rank * lv.ppc;
@@ -134,7 +145,7 @@ __device__ T* dist_smooth(T* cur, T* oth, T* R, const ClusterLevel<T>& lv, const
             if (last) acc += double(v);
         }
         if (last && singular) {
-            *mean = T(cluster_sum(acc, slot, parity, red, rt, ranks) / double(L.n));
+            *mean = T(cluster_sum(acc, slot, bcast, parity, red, rt, ranks) / double(L.n));
         } else {
             cg::this_cluster().sync();
         }
@@ -146,6 +157,14 @@ __device__ T* dist_smooth(T* cur, T* oth, T* R, const ClusterLevel<T>& lv, const
     return cur;
 }
 
+// omega/diag tables of levels first..last (cluster_cycle's arena): no input
+// of the predecessor kernel is read, so the kernel builds them before its
+// programmatic-dependent-launch wait.
+template <int BC, class T>
+__device__ void cluster_tables(T* arena, const ClusterLevels<T>& cl) {
+    for (int l = cl.first; l <= cl.last; ++l) omega_table<BC>(cl.lv[l].L, arena + cl.tables + 64 * (l - cl.first));
+}
+
 // Levels first..last of one V-cycle in a cluster (3D BCs).  As coarse_cycle:
 // rhs of level `first` from global memory (shifted by rhs_sum/n), p from
 // p_global (first == 0) or zero; the final p of level `first`, mean removed
@@ -154,7 +173,7 @@ template <int BC, class T, class TC>
 __device__ void cluster_cycle(T* arena, const T* __restrict__ rhs_global, const double* rhs_sum, const T* p_global,
                               T* p_out, const TC* __restrict__ cinv, const ClusterLevels<T>& cl, int smooth) {
     __shared__ double red[2][32];
-    __shared__ double slot[2];
+    __shared__ double slot[2], bcast[2];
     __shared__ T down_mean[AFSI_MG_MAX_LEVELS];
     constexpr bool singular = singular_bc(BC);
     int rt = 0, parity = 0;
@@ -162,8 +181,7 @@ __device__ void cluster_cycle(T* arena, const T* __restrict__ rhs_global, const 
     const int ranks = int(cg::this_cluster().num_blocks());
     const int f = cl.first, last = cl.last;
     auto P_of = [&](int l) { return arena + cl.lv[l].off; };
-    T* tables = arena + cl.tables;
-    for (int l = f; l <= last; ++l) omega_table<BC>(cl.lv[l].L, tables + 64 * (l - f));
+    T* tables = arena + cl.tables;  // filled by cluster_tables before the kernel waits on its predecessor
     {
         const ClusterLevel<T>& lv = cl.lv[f];
         const T mr = T(site_mean(rhs_sum, lv.L.n));
@@ -189,7 +207,7 @@ __device__ void cluster_cycle(T* arena, const T* __restrict__ rhs_global, const 
         const T* cur;
         if (F.ppc) {
             cur = dist_smooth<BC>(P, P + F.cells, R, F, wrd, smooth, l > f || !p_global, rhs_shift, rank, ranks, slot,
-                                  parity, red, rt, &m);
+                                  bcast, parity, red, rt, &m);
         } else {
             FastCoords<T> fcF;
             fcF.init(F.L);
@@ -221,7 +239,7 @@ __device__ void cluster_cycle(T* arena, const T* __restrict__ rhs_global, const 
                 acc += double(v);
             }
             if (singular) {
-                rhs_shift = T(cluster_sum(acc, slot, parity, red, rt, ranks) / double(C.L.n));
+                rhs_shift = T(cluster_sum(acc, slot, bcast, parity, red, rt, ranks) / double(C.L.n));
             } else {
                 cg::this_cluster().sync();
             }
@@ -378,7 +396,8 @@ __device__ void cluster_cycle(T* arena, const T* __restrict__ rhs_global, const 
                 P[i] = (down[i] - dm) + add;
             }
             cg::this_cluster().sync();
-            corr = dist_smooth<BC>(P, Q, R, F, wrd, smooth, false, T(0), rank, ranks, slot, parity, red, rt, &m);
+            corr = dist_smooth<BC>(P, Q, R, F, wrd, smooth, false, T(0), rank, ranks, slot, bcast, parity, red, rt,
+                                   &m);
             corr_distributed = true;
         } else {
             FastCoords<T> fcL;
