@@ -43,6 +43,10 @@ def parse():
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='b200', choices=('b200', 'reference'))
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--form', default='table-free', choices=('table-free', 'tables'),
+                    help="transfer form of the headline step: 'table-free' (the transfer kernels form the stencil "
+                         "rows) or 'tables' (the prepare writes the stencil tables; for profiler runs of the table "
+                         "kernels)")
     ap.add_argument('--rows', default='all', choices=('all', 'step', 'p1', 'batch', 'p1free', 'stokes'),
                     help="'step': the headline step line only, without the mass-solve, MG-form, batching and "
                          "serving rows (for profiler runs); 'p1': only the precision-form row on the 128^3 P1 "
@@ -1073,7 +1077,7 @@ def run_b200(args):
     from afsi_gpu_b200 import _lib
     _lib.load()
     grid, X, cells, coef, vel, rhs = workload()
-    step = Step(grid, X, cells, coef, vel, rhs, device, form='table-free')
+    step = Step(grid, X, cells, coef, vel, rhs, device, form=args.form)
     stream = torch.cuda.current_stream(device)
     # the table-free step's inputs and fields fit in L2 (126 MB): every timed
     # step starts from a flushed L2 (a 256 MB buffer written just before it,
@@ -1179,10 +1183,11 @@ def run_b200(args):
         pk, pk_kind = peaks()
         P = step.tr.rule(step.x).point_count
         faces = sum(np.prod(grid.face_shape(c)) for c in range(3))
-        ab = algorithmic_bytes_table_free(P, cells.shape[0], X.shape[0], faces)
-        dominant, dt = (('p2_fused_spread', spread_t) if spread_t >= gather_t else
-                        ('p2_fused_gather_assemble', gather_t))
-        byte_key = 'spread' if dominant == 'p2_fused_spread' else 'gather'
+        free = args.form == 'table-free'
+        ab = (algorithmic_bytes_table_free if free else algorithmic_bytes)(P, cells.shape[0], X.shape[0], faces)
+        names = ('p2_fused_spread', 'p2_fused_gather_assemble') if free else ('p2_spread', 'p2_gather_assemble')
+        dominant, dt = (names[0], spread_t) if spread_t >= gather_t else (names[1], gather_t)
+        byte_key = 'spread' if dominant == names[0] else 'gather'
         achieved = ab[byte_key] / dt / 1e9
         traffic = load_traffic().get(dominant)
         cpu = None
@@ -1220,9 +1225,11 @@ def run_b200(args):
                         grid=list(GRID['shape']), elements=int(cells.shape[0]), points=int(P),
                         mg='Neumann V-cycles to 1e-10, Jacobi 2/3 x4, graph-replayed blocks of 2, cycles per solve '
                            f'{sorted(set(step.cycles))}',
-                        transfers='table-free: the spread and gather-assemble kernels form each point\'s position, '
-                                  'bases and IB_4 weights from the nodal positions (no stencil tables); the prepare '
-                                  'selects and checks the rule',
+                        transfers=('table-free: the spread and gather-assemble kernels form each point\'s position, '
+                                   'bases and IB_4 weights from the nodal positions (no stencil tables); the prepare '
+                                   'selects and checks the rule' if free else
+                                   'tables: the prepare writes the (2,P,3) bases and (2,P,3,4) weights that the spread '
+                                   'and gather-assemble read back'),
                         l2='L2 flushed before every timed step (256 MB written outside the step\'s events)',
                         parallelism=f'replicas x{world}'),
             roofline=dict(bound='hbm', kernel=dominant, achieved=achieved, peak=pk['hbm_gbs'], unit='GB/s',
