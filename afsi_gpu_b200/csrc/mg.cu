@@ -36,6 +36,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 #include "mg_cluster.cuh"
 
@@ -92,6 +93,111 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(const T* __restrict__ p
         out[i] = v;
         local += double(v);
     });
+    if (do_emit) site_finish(emit, local);
+}
+
+// The fast-form Jacobi sweep of a 3D level (Neumann or Dirichlet) with two
+// z-adjacent cells per thread, z = 2k and 2k+1 (nz even): the pair's p and
+// rhs and its x and y neighbours are 16-byte loads, the outer z neighbours
+// two 8-byte loads, and the pair shares its address and x/y tests.  No
+// pending shift of p (the launched sweeps take none); fix_rhs subtracts the
+// rhs mean and writes it back.  Per cell the same operations in the same
+// order as sweep_kernel's fast form, so out is bitwise equal; the emitted sum
+// is added per block in this kernel's cell order.
+template <int BC, class T>
+__global__ void __launch_bounds__(kThreads) sweep_zpair_kernel(const T* __restrict__ p, T* __restrict__ rhs,
+                                                               T* __restrict__ out, Lv<T> L, const double* rhs_sum,
+                                                               Site emit, int fix_rhs, int do_emit) {
+    using V = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+    __shared__ T wtab[64];
+    {
+        const unsigned t = thread_linear();
+        if (t < 64) wtab[t] = omega_of_class<BC>(int(t), L);
+        __syncthreads();
+    }
+    pdl_enter();
+    double local = 0.0;
+    const T mr = T(site_mean(rhs_sum, L.n));
+    const int zp = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = 2 * zp;
+    if (z < L.nz && y < L.ny) {
+        const int64_t sx = int64_t(L.ny) * L.nz, sy = L.nz;
+        const bool ym_in = y > 0, yp_in = y + 1 < L.ny, zm_in = z > 0, zp_in = z + 2 < L.nz;
+        for (int x = blockIdx.z; x < L.nx; x += gridDim.z) {
+            const int64_t i = (int64_t(x) * L.ny + y) * L.nz + z;
+            const V rv = *reinterpret_cast<const V*>(rhs + i);
+            T r0 = rv.x, r1 = rv.y;
+            if (fix_rhs) {
+                r0 = r0 - mr;
+                r1 = r1 - mr;
+                V w;
+                w.x = r0;
+                w.y = r1;
+                *reinterpret_cast<V*>(rhs + i) = w;
+            }
+            const T w0 = wtab[boundary_class(x, y, z, L.nx, L.ny, L.nz)];
+            const T w1 = wtab[boundary_class(x, y, z + 1, L.nx, L.ny, L.nz)];
+            T v0, v1;
+            if (p) {
+                const V c = *reinterpret_cast<const V*>(p + i);
+                const T pc0 = c.x, pc1 = c.y;
+                const bool xm_in = x > 0, xp_in = x + 1 < L.nx;
+                V xp, xm, yp, ym;
+                if (xp_in) xp = *reinterpret_cast<const V*>(p + i + sx);
+                if (xm_in) xm = *reinterpret_cast<const V*>(p + i - sx);
+                if (yp_in) yp = *reinterpret_cast<const V*>(p + i + sy);
+                if (ym_in) ym = *reinterpret_cast<const V*>(p + i - sy);
+                const T zm = zm_in ? p[i - 1] : T(0), zq = zp_in ? p[i + 2] : T(0);
+                T a0 = T(0), a1 = T(0);
+                if (BC == AFSI_BC_DIRICHLET) {
+                    a0 = xp_in ? a0 - (xp.x - pc0) * L.ih2[0] : a0 + (pc0 + pc0) * L.ih2[0];
+                    a1 = xp_in ? a1 - (xp.y - pc1) * L.ih2[0] : a1 + (pc1 + pc1) * L.ih2[0];
+                    a0 = xm_in ? a0 + (pc0 - xm.x) * L.ih2[0] : a0 + (pc0 + pc0) * L.ih2[0];
+                    a1 = xm_in ? a1 + (pc1 - xm.y) * L.ih2[0] : a1 + (pc1 + pc1) * L.ih2[0];
+                    a0 = yp_in ? a0 - (yp.x - pc0) * L.ih2[1] : a0 + (pc0 + pc0) * L.ih2[1];
+                    a1 = yp_in ? a1 - (yp.y - pc1) * L.ih2[1] : a1 + (pc1 + pc1) * L.ih2[1];
+                    a0 = ym_in ? a0 + (pc0 - ym.x) * L.ih2[1] : a0 + (pc0 + pc0) * L.ih2[1];
+                    a1 = ym_in ? a1 + (pc1 - ym.y) * L.ih2[1] : a1 + (pc1 + pc1) * L.ih2[1];
+                    a0 = a0 - (pc1 - pc0) * L.ih2[2];
+                    a1 = zp_in ? a1 - (zq - pc1) * L.ih2[2] : a1 + (pc1 + pc1) * L.ih2[2];
+                    a0 = zm_in ? a0 + (pc0 - zm) * L.ih2[2] : a0 + (pc0 + pc0) * L.ih2[2];
+                    a1 = a1 + (pc1 - pc0) * L.ih2[2];
+                } else {
+                    if (xp_in) {
+                        a0 = a0 - (xp.x - pc0) * L.ih2[0];
+                        a1 = a1 - (xp.y - pc1) * L.ih2[0];
+                    }
+                    if (xm_in) {
+                        a0 = a0 + (pc0 - xm.x) * L.ih2[0];
+                        a1 = a1 + (pc1 - xm.y) * L.ih2[0];
+                    }
+                    if (yp_in) {
+                        a0 = a0 - (yp.x - pc0) * L.ih2[1];
+                        a1 = a1 - (yp.y - pc1) * L.ih2[1];
+                    }
+                    if (ym_in) {
+                        a0 = a0 + (pc0 - ym.x) * L.ih2[1];
+                        a1 = a1 + (pc1 - ym.y) * L.ih2[1];
+                    }
+                    a0 = a0 - (pc1 - pc0) * L.ih2[2];
+                    if (zp_in) a1 = a1 - (zq - pc1) * L.ih2[2];
+                    if (zm_in) a0 = a0 + (pc0 - zm) * L.ih2[2];
+                    a1 = a1 + (pc1 - pc0) * L.ih2[2];
+                }
+                v0 = jacobi_update(pc0, r0, a0, w0);
+                v1 = jacobi_update(pc1, r1, a1, w1);
+            } else {
+                v0 = r0 * w0;
+                v1 = r1 * w1;
+            }
+            V o;
+            o.x = v0;
+            o.y = v1;
+            *reinterpret_cast<V*>(out + i) = o;
+            local += double(v0);
+            local += double(v1);
+        }
+    }
     if (do_emit) site_finish(emit, local);
 }
 
@@ -378,6 +484,13 @@ Geometry launch_for(const Lv<T>& L, int bc) {
     return g;
 }
 
+// Geometry of sweep_zpair_kernel: launch_for with the z extent halved.
+template <class T>
+Geometry launch_for_zpairs(Lv<T> L) {
+    L.nz /= 2;
+    return launch_for(L, AFSI_BC_NEUMANN);
+}
+
 int flat_grid(int64_t n) {
     int64_t b = (n + kThreads - 1) / kThreads;
     return int(b < 4096 ? (b > 0 ? b : 1) : 4096);
@@ -494,6 +607,17 @@ struct Runner {
     T* Q(int l) const { return static_cast<T*>(plan->level[l].ping); }
     T* R(int l) const { return static_cast<T*>(plan->level[l].rhs); }
     static constexpr bool singular = singular_bc(BC);
+
+    // Two z cells per thread (sweep_zpair_kernel) on 3D levels with even nz
+    // whose buffers are 16-byte aligned.
+    bool zpairs(int l) const {
+        if constexpr (BC == AFSI_BC_NEUMANN || BC == AFSI_BC_DIRICHLET) {
+            const auto a16 = [](const void* q) { return reinterpret_cast<uintptr_t>(q) % 16 == 0; };
+            return lv[l].nz % 2 == 0 && a16(P(l)) && a16(Q(l)) && a16(R(l));
+        } else {
+            return false;
+        }
+    }
 
     int32_t coarse(int l, const double* rhs_sum, T** out) {
         CoarseLevels<T> cl;
@@ -639,15 +763,22 @@ struct Runner {
         }
         const Lv<T>& L = lv[l];
         const Geometry g = launch_for(L, BC);
+        const Geometry gz = launch_for_zpairs(L);
         T* cur = P(l);
         T* oth = Q(l);
         for (int s = 0; s < plan->smooth; ++s) {
             const bool first = s == 0;
             const bool last = s == plan->smooth - 1;
-            rc = launch_pdl("mg sweep", sweep_kernel<BC, false, T>, g.grid, g.block, 0, stream,
-                            (first && l > 0) ? nullptr : cur, R(l), oth, L, static_cast<const double*>(nullptr),
-                            (first && l > 0 && singular) ? st.s[l][2].result : nullptr, st.s[l][0],
-                            (first && l > 0 && singular) ? 1 : 0, (last && singular) ? 1 : 0);
+            if (zpairs(l))
+                rc = launch_pdl("mg sweep", sweep_zpair_kernel<BC, T>, gz.grid, gz.block, 0, stream,
+                                static_cast<const T*>((first && l > 0) ? nullptr : cur), R(l), oth, L,
+                                (first && l > 0 && singular) ? st.s[l][2].result : nullptr, st.s[l][0],
+                                (first && l > 0 && singular) ? 1 : 0, (last && singular) ? 1 : 0);
+            else
+                rc = launch_pdl("mg sweep", sweep_kernel<BC, false, T>, g.grid, g.block, 0, stream,
+                                (first && l > 0) ? nullptr : cur, R(l), oth, L, static_cast<const double*>(nullptr),
+                                (first && l > 0 && singular) ? st.s[l][2].result : nullptr, st.s[l][0],
+                                (first && l > 0 && singular) ? 1 : 0, (last && singular) ? 1 : 0);
             if (rc) return rc;
             T* t = cur; cur = oth; oth = t;
         }
@@ -667,9 +798,14 @@ struct Runner {
         oth = Q(l);
         for (int s = 0; s < plan->smooth; ++s) {
             const bool last = s == plan->smooth - 1;
-            rc = launch_pdl("mg sweep", sweep_kernel<BC, false, T>, g.grid, g.block, 0, stream, cur, R(l), oth, L,
-                            static_cast<const double*>(nullptr), static_cast<const double*>(nullptr), st.s[l][1], 0,
-                            (last && singular) ? 1 : 0);
+            if (zpairs(l))
+                rc = launch_pdl("mg sweep", sweep_zpair_kernel<BC, T>, gz.grid, gz.block, 0, stream,
+                                static_cast<const T*>(cur), R(l), oth, L, static_cast<const double*>(nullptr),
+                                st.s[l][1], 0, (last && singular) ? 1 : 0);
+            else
+                rc = launch_pdl("mg sweep", sweep_kernel<BC, false, T>, g.grid, g.block, 0, stream, cur, R(l), oth,
+                                L, static_cast<const double*>(nullptr), static_cast<const double*>(nullptr),
+                                st.s[l][1], 0, (last && singular) ? 1 : 0);
             if (rc) return rc;
             T* t = cur; cur = oth; oth = t;
         }
