@@ -96,6 +96,66 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(const T* __restrict__ p
     if (do_emit) site_finish(emit, local);
 }
 
+// (A p) of the z-adjacent cells (x,y,z) and (x,y,z+1), z even, of a 3D
+// level (Neumann or Dirichlet), every load shifted by m: neg_lap's fast-form
+// terms in neg_lap's order for each cell, with the pair and its x and y
+// neighbours read as 16-byte vectors and the two outer z neighbours as
+// scalars.  Returns the shifted centre values in pc0, pc1.
+template <int BC, class T>
+__device__ __forceinline__ void pair_neg_lap(const T* __restrict__ p, int64_t i, int x, int y, int z, const Lv<T>& L,
+                                             T m, T& pc0, T& pc1, T& a0, T& a1) {
+    using V = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+    const int64_t sx = int64_t(L.ny) * L.nz, sy = L.nz;
+    const bool xp_in = x + 1 < L.nx, xm_in = x > 0, yp_in = y + 1 < L.ny, ym_in = y > 0, zm_in = z > 0,
+               zp_in = z + 2 < L.nz;
+    const V c = *reinterpret_cast<const V*>(p + i);
+    pc0 = c.x - m;
+    pc1 = c.y - m;
+    V xp, xm, yp, ym;
+    if (xp_in) xp = *reinterpret_cast<const V*>(p + i + sx);
+    if (xm_in) xm = *reinterpret_cast<const V*>(p + i - sx);
+    if (yp_in) yp = *reinterpret_cast<const V*>(p + i + sy);
+    if (ym_in) ym = *reinterpret_cast<const V*>(p + i - sy);
+    const T zm = zm_in ? p[i - 1] - m : T(0), zq = zp_in ? p[i + 2] - m : T(0);
+    a0 = T(0);
+    a1 = T(0);
+    if (BC == AFSI_BC_DIRICHLET) {
+        a0 = xp_in ? a0 - ((xp.x - m) - pc0) * L.ih2[0] : a0 + (pc0 + pc0) * L.ih2[0];
+        a1 = xp_in ? a1 - ((xp.y - m) - pc1) * L.ih2[0] : a1 + (pc1 + pc1) * L.ih2[0];
+        a0 = xm_in ? a0 + (pc0 - (xm.x - m)) * L.ih2[0] : a0 + (pc0 + pc0) * L.ih2[0];
+        a1 = xm_in ? a1 + (pc1 - (xm.y - m)) * L.ih2[0] : a1 + (pc1 + pc1) * L.ih2[0];
+        a0 = yp_in ? a0 - ((yp.x - m) - pc0) * L.ih2[1] : a0 + (pc0 + pc0) * L.ih2[1];
+        a1 = yp_in ? a1 - ((yp.y - m) - pc1) * L.ih2[1] : a1 + (pc1 + pc1) * L.ih2[1];
+        a0 = ym_in ? a0 + (pc0 - (ym.x - m)) * L.ih2[1] : a0 + (pc0 + pc0) * L.ih2[1];
+        a1 = ym_in ? a1 + (pc1 - (ym.y - m)) * L.ih2[1] : a1 + (pc1 + pc1) * L.ih2[1];
+        a0 = a0 - (pc1 - pc0) * L.ih2[2];
+        a1 = zp_in ? a1 - (zq - pc1) * L.ih2[2] : a1 + (pc1 + pc1) * L.ih2[2];
+        a0 = zm_in ? a0 + (pc0 - zm) * L.ih2[2] : a0 + (pc0 + pc0) * L.ih2[2];
+        a1 = a1 + (pc1 - pc0) * L.ih2[2];
+    } else {
+        if (xp_in) {
+            a0 = a0 - ((xp.x - m) - pc0) * L.ih2[0];
+            a1 = a1 - ((xp.y - m) - pc1) * L.ih2[0];
+        }
+        if (xm_in) {
+            a0 = a0 + (pc0 - (xm.x - m)) * L.ih2[0];
+            a1 = a1 + (pc1 - (xm.y - m)) * L.ih2[0];
+        }
+        if (yp_in) {
+            a0 = a0 - ((yp.x - m) - pc0) * L.ih2[1];
+            a1 = a1 - ((yp.y - m) - pc1) * L.ih2[1];
+        }
+        if (ym_in) {
+            a0 = a0 + (pc0 - (ym.x - m)) * L.ih2[1];
+            a1 = a1 + (pc1 - (ym.y - m)) * L.ih2[1];
+        }
+        a0 = a0 - (pc1 - pc0) * L.ih2[2];
+        if (zp_in) a1 = a1 - (zq - pc1) * L.ih2[2];
+        if (zm_in) a0 = a0 + (pc0 - zm) * L.ih2[2];
+        a1 = a1 + (pc1 - pc0) * L.ih2[2];
+    }
+}
+
 // The fast-form Jacobi sweep of a 3D level (Neumann or Dirichlet) with two
 // z-adjacent cells per thread, z = 2k and 2k+1 (nz even): the pair's p and
 // rhs and its x and y neighbours are 16-byte loads, the outer z neighbours
@@ -121,8 +181,6 @@ __global__ void __launch_bounds__(kThreads) sweep_zpair_kernel(const T* __restri
     const int zp = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = 2 * zp;
     if (z < L.nz && y < L.ny) {
-        const int64_t sx = int64_t(L.ny) * L.nz, sy = L.nz;
-        const bool ym_in = y > 0, yp_in = y + 1 < L.ny, zm_in = z > 0, zp_in = z + 2 < L.nz;
         for (int x = blockIdx.z; x < L.nx; x += gridDim.z) {
             const int64_t i = (int64_t(x) * L.ny + y) * L.nz + z;
             const V rv = *reinterpret_cast<const V*>(rhs + i);
@@ -139,51 +197,8 @@ __global__ void __launch_bounds__(kThreads) sweep_zpair_kernel(const T* __restri
             const T w1 = wtab[boundary_class(x, y, z + 1, L.nx, L.ny, L.nz)];
             T v0, v1;
             if (p) {
-                const V c = *reinterpret_cast<const V*>(p + i);
-                const T pc0 = c.x, pc1 = c.y;
-                const bool xm_in = x > 0, xp_in = x + 1 < L.nx;
-                V xp, xm, yp, ym;
-                if (xp_in) xp = *reinterpret_cast<const V*>(p + i + sx);
-                if (xm_in) xm = *reinterpret_cast<const V*>(p + i - sx);
-                if (yp_in) yp = *reinterpret_cast<const V*>(p + i + sy);
-                if (ym_in) ym = *reinterpret_cast<const V*>(p + i - sy);
-                const T zm = zm_in ? p[i - 1] : T(0), zq = zp_in ? p[i + 2] : T(0);
-                T a0 = T(0), a1 = T(0);
-                if (BC == AFSI_BC_DIRICHLET) {
-                    a0 = xp_in ? a0 - (xp.x - pc0) * L.ih2[0] : a0 + (pc0 + pc0) * L.ih2[0];
-                    a1 = xp_in ? a1 - (xp.y - pc1) * L.ih2[0] : a1 + (pc1 + pc1) * L.ih2[0];
-                    a0 = xm_in ? a0 + (pc0 - xm.x) * L.ih2[0] : a0 + (pc0 + pc0) * L.ih2[0];
-                    a1 = xm_in ? a1 + (pc1 - xm.y) * L.ih2[0] : a1 + (pc1 + pc1) * L.ih2[0];
-                    a0 = yp_in ? a0 - (yp.x - pc0) * L.ih2[1] : a0 + (pc0 + pc0) * L.ih2[1];
-                    a1 = yp_in ? a1 - (yp.y - pc1) * L.ih2[1] : a1 + (pc1 + pc1) * L.ih2[1];
-                    a0 = ym_in ? a0 + (pc0 - ym.x) * L.ih2[1] : a0 + (pc0 + pc0) * L.ih2[1];
-                    a1 = ym_in ? a1 + (pc1 - ym.y) * L.ih2[1] : a1 + (pc1 + pc1) * L.ih2[1];
-                    a0 = a0 - (pc1 - pc0) * L.ih2[2];
-                    a1 = zp_in ? a1 - (zq - pc1) * L.ih2[2] : a1 + (pc1 + pc1) * L.ih2[2];
-                    a0 = zm_in ? a0 + (pc0 - zm) * L.ih2[2] : a0 + (pc0 + pc0) * L.ih2[2];
-                    a1 = a1 + (pc1 - pc0) * L.ih2[2];
-                } else {
-                    if (xp_in) {
-                        a0 = a0 - (xp.x - pc0) * L.ih2[0];
-                        a1 = a1 - (xp.y - pc1) * L.ih2[0];
-                    }
-                    if (xm_in) {
-                        a0 = a0 + (pc0 - xm.x) * L.ih2[0];
-                        a1 = a1 + (pc1 - xm.y) * L.ih2[0];
-                    }
-                    if (yp_in) {
-                        a0 = a0 - (yp.x - pc0) * L.ih2[1];
-                        a1 = a1 - (yp.y - pc1) * L.ih2[1];
-                    }
-                    if (ym_in) {
-                        a0 = a0 + (pc0 - ym.x) * L.ih2[1];
-                        a1 = a1 + (pc1 - ym.y) * L.ih2[1];
-                    }
-                    a0 = a0 - (pc1 - pc0) * L.ih2[2];
-                    if (zp_in) a1 = a1 - (zq - pc1) * L.ih2[2];
-                    if (zm_in) a0 = a0 + (pc0 - zm) * L.ih2[2];
-                    a1 = a1 + (pc1 - pc0) * L.ih2[2];
-                }
+                T pc0, pc1, a0, a1;
+                pair_neg_lap<BC>(p, i, x, y, z, L, T(0), pc0, pc1, a0, a1);
                 v0 = jacobi_update(pc0, r0, a0, w0);
                 v1 = jacobi_update(pc1, r1, a1, w1);
             } else {
@@ -198,6 +213,41 @@ __global__ void __launch_bounds__(kThreads) sweep_zpair_kernel(const T* __restri
             local += double(v1);
         }
     }
+    if (do_emit) site_finish(emit, local);
+}
+
+// residual_restrict_kernel's fast form for 3D levels (Neumann or Dirichlet)
+// with the fine z pairs of each coarse cell read by pair_neg_lap: the eight
+// children summed in the same order (x, y, then z), so coarse is bitwise
+// equal.
+template <int BC, class T>
+__global__ void __launch_bounds__(kThreads) residual_restrict_zpair_kernel(const T* __restrict__ p,
+                                                                          const T* __restrict__ rhs,
+                                                                          T* __restrict__ coarse, Lv<T> L, Lv<T> C,
+                                                                          const double* p_sum, Site emit,
+                                                                          int do_emit) {
+    using V = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+    pdl_enter();
+    double local = 0.0;
+    const T m = T(site_mean(p_sum, L.n));
+    for_my_cells<BC>(C, [&](int cx, int cy, int cz) {
+        T v = T(0);
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                const int x = 2 * cx + a, y = 2 * cy + b, z = 2 * cz;
+                const int64_t i = index_of(x, y, z, L);
+                T pc0, pc1, a0, a1;
+                pair_neg_lap<BC>(p, i, x, y, z, L, m, pc0, pc1, a0, a1);
+                const V r = *reinterpret_cast<const V*>(rhs + i);
+                v = v + (r.x - a0);
+                v = v + (r.y - a1);
+            }
+        v = v * T(.125);
+        coarse[index_of(cx, cy, cz, C)] = v;
+        local += double(v);
+    });
     if (do_emit) site_finish(emit, local);
 }
 
@@ -785,8 +835,12 @@ struct Runner {
         const double* down_sum = singular ? st.s[l][0].result : nullptr;
         const Lv<T>& C = lv[l + 1];
         const Geometry gc = launch_for(C, BC);
-        rc = launch_pdl("mg residual_restrict", residual_restrict_kernel<BC, false, T>, gc.grid, gc.block, 0, stream,
-                        cur, R(l), R(l + 1), L, C, down_sum, st.s[l + 1][2], singular ? 1 : 0);
+        if (zpairs(l))
+            rc = launch_pdl("mg residual_restrict", residual_restrict_zpair_kernel<BC, T>, gc.grid, gc.block, 0, stream,
+                            cur, R(l), R(l + 1), L, C, down_sum, st.s[l + 1][2], singular ? 1 : 0);
+        else
+            rc = launch_pdl("mg residual_restrict", residual_restrict_kernel<BC, false, T>, gc.grid, gc.block, 0, stream,
+                            cur, R(l), R(l + 1), L, C, down_sum, st.s[l + 1][2], singular ? 1 : 0);
         if (rc) return rc;
         T* corr;
         const double* corr_sum;
