@@ -93,6 +93,8 @@ _SIGNATURES = {
                            ctypes.c_double, c_int32, c_void_p],
     'afsi_b200_mg_solve_graph_create': [ctypes.POINTER(MGPlan), c_int32, c_int32, c_void_p, c_void_p,
                                         ctypes.POINTER(c_void_p)],
+    'afsi_b200_mg_solve_graph_create_started': [ctypes.POINTER(MGPlan), c_int32, c_int32, c_void_p, c_void_p,
+                                                c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_void_p)],
     'afsi_b200_mg_solve_graph_launch': [c_void_p, c_void_p],
     'afsi_b200_mg_solve_graph_destroy': [c_void_p],
     'afsi_b200_indexed_gather': [c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_int64, c_int64, c_void_p,

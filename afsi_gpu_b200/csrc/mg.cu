@@ -280,6 +280,39 @@ __global__ void __launch_bounds__(kThreads) prolong_kernel(const T* src, const T
     });
 }
 
+// The end of a check block of the solve loop in one launch: the last V-cycle's
+// finalize (dst = src - m, the pending mean m of src; no write when src is
+// dst and there is no mean) fused with the residual norm of the finalized
+// iterate (residual_norm_kernel's exact form and geometry on the values
+// src - m, which are the finalized values bit for bit, so the norm is the
+// same) and, in the last block, the loop decision of mg_decide_kernel.
+template <int BC, class T>
+__global__ void __launch_bounds__(kThreads) finalize_check_kernel(const T* src, T* dst, const T* __restrict__ rhs,
+                                                                  Lv<T> L, const double* sum, Site s, double* norm,
+                                                                  double* loop, int check_every, int max_cycles,
+                                                                  cudaGraphConditionalHandle handle) {
+    pdl_enter();
+    const T m = T(site_mean(sum, L.n));
+    const bool write = src != dst;
+    double local = 0.0;
+    for_my_cells<BC>(L, [&](int x, int y, int z) {
+        const int64_t i = index_of(x, y, z, L);
+        const T pc = src[i] - m;
+        if (write) dst[i] = pc;
+        const T r = rhs[i] - neg_lap<BC, true>(src, i, x, y, z, L, m, pc);
+        local += double(r) * double(r);
+    });
+    site_finish_then(s, local, norm, [&](double r) {
+        const double cycles = loop[1] + check_every;
+        loop[1] = cycles;
+        loop[2] = r;
+        const bool finite = isfinite(r);
+        if (!finite) loop[3] = 1.0;
+        const bool again = finite && r > loop[0] && cycles + check_every <= max_cycles;
+        cudaGraphSetConditional(handle, again ? 1u : 0u);
+    });
+}
+
 // dst = src - sum/n (or a copy when sum is null); flat grid-stride.
 template <class T>
 __global__ void __launch_bounds__(kThreads) shift_kernel(const T* src, T* dst, int64_t n, const double* sum) {
@@ -597,6 +630,22 @@ int32_t check_shape(const int64_t* shape, int dim) {
     return AFSI_OK;
 }
 
+// Loop decision of the solve graph: count the block's cycles, keep the norm,
+// flag a nonfinite norm, and continue while the norm is above loop[0] and
+// another block fits max_cycles.
+__global__ void mg_decide_kernel(double* loop, const double* norm, int check_every, int max_cycles,
+                                 cudaGraphConditionalHandle handle) {
+    pdl_enter();
+    const double cycles = loop[1] + check_every;
+    const double r = *norm;
+    loop[1] = cycles;
+    loop[2] = r;
+    const bool finite = isfinite(r);
+    if (!finite) loop[3] = 1.0;
+    const bool again = finite && r > loop[0] && cycles + check_every <= max_cycles;
+    cudaGraphSetConditional(handle, again ? 1u : 0u);
+}
+
 // ---- fused V-cycle plan execution ----
 
 // Scratch layout: kSites reduction sites, each `width` partial doubles (the
@@ -845,11 +894,15 @@ struct Runner {
         T* corr;
         const double* corr_sum;
         if ((rc = level(l + 1, &corr, &corr_sum))) return rc;
+        // the finest level of a singular operator prolongs into the buffer the
+        // pre-smoothing left free, so its post-smoothing ends in Q(0) and the
+        // finalize (and the fused check of the solve loop) never shifts in place
+        T* pdst = (l == 0 && singular && cur == P(l)) ? Q(l) : P(l);
         rc = launch_pdl("mg prolong_add", prolong_kernel<BC, T>, g.grid, g.block, 0, stream, cur,
-                        static_cast<const T*>(corr), P(l), L, C, down_sum, corr_sum);
+                        static_cast<const T*>(corr), pdst, L, C, down_sum, corr_sum);
         if (rc) return rc;
-        cur = P(l);
-        oth = Q(l);
+        cur = pdst;
+        oth = pdst == P(l) ? Q(l) : P(l);
         for (int s = 0; s < plan->smooth; ++s) {
             const bool last = s == plan->smooth - 1;
             if (zpairs(l))
@@ -881,6 +934,34 @@ struct Runner {
             }
         }
         return AFSI_OK;
+    }
+
+    // One check block of the solve loop: `count` V-cycles, the residual norm
+    // into norm and the loop decision; the last cycle's finalize, the norm and
+    // the decision are one launch (finalize_check_kernel) unless the finalize
+    // would shift in place.
+    int32_t checked_block(int count, double* norm, double* loop, int check_every, int max_cycles,
+                          cudaGraphConditionalHandle handle) {
+        int32_t rc = cycles(count - 1);
+        if (rc) return rc;
+        T* out;
+        const double* sum;
+        if ((rc = level(0, &out, &sum))) return rc;
+        const Geometry g = launch_for(lv[0], BC);
+        if (out == P(0) && sum) {
+            rc = launch_pdl("mg finalize", shift_kernel<T>, dim3(flat_grid(lv[0].n)), dim3(kThreads), 0, stream,
+                            static_cast<const T*>(out), P(0), lv[0].n, sum);
+            if (!rc)
+                rc = launch_pdl("mg residual_norm", residual_norm_kernel<BC, true, T>, g.grid, g.block, 0, stream,
+                                static_cast<const T*>(P(0)), static_cast<const T*>(R(0)), lv[0], st.norm, norm);
+            if (!rc)
+                rc = launch_pdl("mg solve decide", mg_decide_kernel, dim3(1), dim3(1), 0, stream, loop,
+                                static_cast<const double*>(norm), check_every, max_cycles, handle);
+            return rc;
+        }
+        return launch_pdl("mg finalize check", finalize_check_kernel<BC, T>, g.grid, g.block, 0, stream,
+                          static_cast<const T*>(out), P(0), static_cast<const T*>(R(0)), lv[0], sum, st.norm, norm,
+                          loop, check_every, max_cycles, handle);
     }
 };
 
@@ -936,8 +1017,7 @@ size_t coarse_smem_bytes(const Lv<T>* lv, int first, int levels) {
 }
 
 template <int BC, class T, class TC>
-int32_t run_plan(const afsi_mg_plan* plan, int cycles, cudaStream_t stream) {
-    Runner<BC, T, TC> r;
+void setup_runner(Runner<BC, T, TC>& r, const afsi_mg_plan* plan, cudaStream_t stream) {
     r.plan = plan;
     r.stream = stream;
     r.st = sites_for(plan);
@@ -945,7 +1025,21 @@ int32_t run_plan(const afsi_mg_plan* plan, int cycles, cudaStream_t stream) {
         r.lv[l] = make_level<T>(plan->level[l].shape, plan->level[l].h2, plan->level[l].inv_h2, plan->dim);
     r.first_coarse = coarse_start(r.lv, plan->levels);
     r.plan_cluster();
+}
+
+template <int BC, class T, class TC>
+int32_t run_plan(const afsi_mg_plan* plan, int cycles, cudaStream_t stream) {
+    Runner<BC, T, TC> r;
+    setup_runner(r, plan, stream);
     return r.cycles(cycles);
+}
+
+template <int BC, class T, class TC>
+int32_t run_plan_checked(const afsi_mg_plan* plan, int cycles, cudaStream_t stream, double* norm, double* loop,
+                         int max_cycles, cudaGraphConditionalHandle handle) {
+    Runner<BC, T, TC> r;
+    setup_runner(r, plan, stream);
+    return r.checked_block(cycles, norm, loop, cycles, max_cycles, handle);
 }
 
 }  // namespace
@@ -1118,18 +1212,6 @@ extern "C" int32_t afsi_b200_mg_residual_norm(const afsi_mg_plan* plan, double* 
 
 namespace {
 
-__global__ void mg_decide_kernel(double* loop, const double* norm, int check_every, int max_cycles,
-                                 cudaGraphConditionalHandle handle) {
-    pdl_enter();
-    const double cycles = loop[1] + check_every;
-    const double r = *norm;
-    loop[1] = cycles;
-    loop[2] = r;
-    const bool finite = isfinite(r);
-    if (!finite) loop[3] = 1.0;
-    const bool again = finite && r > loop[0] && cycles + check_every <= max_cycles;
-    cudaGraphSetConditional(handle, again ? 1u : 0u);
-}
 
 struct SolveGraph {
     cudaGraph_t graph = nullptr;
@@ -1146,6 +1228,51 @@ void release(SolveGraph* sg) {
 }
 
 }  // namespace
+
+// Start of a solve in the started loop graph: the tolerance
+// max(atol, rtol ||b||) from the shifted right-hand side's sum of squares,
+// the compatibility screen of a singular operator, and the WHILE condition
+// (the initial residual above the tolerance, every input finite and
+// compatible).  params: [rtol, atol, rel, n] (rel: the screen's relative
+// bound); stats: vector_stats of the raw rhs [0:4], of the initial iterate
+// [4:8] and of the shifted rhs [8:12].
+__global__ void mg_loop_start_kernel(double* loop, const double* norm, const double* stats, const double* params,
+                                     int singular, int check_every, int max_cycles,
+                                     cudaGraphConditionalHandle handle) {
+    pdl_enter();
+    const double rhs_norm = sqrt(stats[10]);
+    const double tol = fmax(params[1], params[0] * rhs_norm);
+    const double r = *norm, n = params[3];
+    const bool compatible = !singular || fabs(stats[0] / n) <= 1e-12 + params[2] * (stats[1] / n);
+    loop[0] = tol;
+    loop[1] = 0.0;
+    loop[2] = r;
+    loop[3] = isfinite(r) ? 0.0 : 1.0;
+    const bool go = stats[3] != 0.0 && stats[7] != 0.0 && compatible && isfinite(rhs_norm) && isfinite(r) && r > tol &&
+                    check_every <= max_cycles;
+    cudaGraphSetConditional(handle, go ? 1u : 0u);
+}
+
+// Body of the solve loop: check_every V-cycles, the residual norm and the
+// decision (fused into one launch for the Jacobi schedule).
+int32_t check_block(const afsi_mg_plan* plan, int check_every, int max_cycles, double* loop, double* norm,
+                    cudaGraphConditionalHandle handle, cudaStream_t stream) {
+    if (plan->smoother == AFSI_MG_JACOBI) {
+        AFSI_BC_DISPATCH(plan->bc, {
+            AFSI_DISPATCH(plan->dtype, {
+                if (plan->coarse_dtype == AFSI_F64)
+                    return run_plan_checked<BC, T, double>(plan, check_every, stream, norm, loop, max_cycles, handle);
+                return run_plan_checked<BC, T, T>(plan, check_every, stream, norm, loop, max_cycles, handle);
+            });
+        });
+    }
+    int32_t rc = afsi_b200_mg_vcycles(plan, check_every, stream);
+    if (!rc) rc = afsi_b200_mg_residual_norm(plan, norm, stream);
+    if (!rc)
+        rc = launch_pdl("mg solve decide", mg_decide_kernel, dim3(1), dim3(1), 0, stream, loop,
+                        static_cast<const double*>(norm), check_every, max_cycles, handle);
+    return rc;
+}
 
 extern "C" int32_t afsi_b200_mg_solve_graph_create(const afsi_mg_plan* plan, int32_t check_every,
                                                    int32_t max_cycles, double* loop, double* norm,
@@ -1180,14 +1307,101 @@ extern "C" int32_t afsi_b200_mg_solve_graph_create(const afsi_mg_plan* plan, int
         release(sg);
         return fail(AFSI_ERR_CUDA, "solve graph capture failed: %s", cudaGetErrorString(cudaGetLastError()));
     }
-    rc = afsi_b200_mg_vcycles(plan, check_every, sg->capture);
-    if (!rc) rc = afsi_b200_mg_residual_norm(plan, norm, sg->capture);
-    if (!rc) {
-        rc = launch_pdl("mg solve decide", mg_decide_kernel, dim3(1), dim3(1), 0, sg->capture, loop,
-                        static_cast<const double*>(norm), check_every, max_cycles, handle);
-    }
+    rc = check_block(plan, check_every, max_cycles, loop, norm, handle, sg->capture);
     cudaGraph_t captured = nullptr;
     const cudaError_t end = cudaStreamEndCapture(sg->capture, &captured);
+    if (rc) {
+        release(sg);
+        return rc;
+    }
+    if (end != cudaSuccess || cudaGraphInstantiate(&sg->exec, sg->graph, 0) != cudaSuccess) {
+        release(sg);
+        return fail(AFSI_ERR_CUDA, "solve graph instantiation failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    *graph_out = sg;
+    return AFSI_OK;
+}
+
+extern "C" int32_t afsi_b200_vector_stats(const void* x, int64_t n, double* stats_out, void* scratch, int32_t dtype,
+                                          afsi_stream_t stream);
+extern "C" int32_t afsi_b200_subtract_mean(void* x, int64_t n, const double* stats, int32_t dtype,
+                                          afsi_stream_t stream);
+
+extern "C" int32_t afsi_b200_mg_solve_graph_create_started(const afsi_mg_plan* plan, int32_t check_every,
+                                                           int32_t max_cycles, double* loop, double* norm,
+                                                           double* stats, void* stat_scratch, const double* params,
+                                                           void** graph_out) {
+    int32_t rc = validate_plan(plan);
+    if (rc) return rc;
+    AFSI_REQUIRE(graph_out && loop && norm && stats && stat_scratch && params, "null solve-graph argument");
+    AFSI_REQUIRE(check_every >= 1 && max_cycles >= check_every, "solve graph needs 1 <= check_every <= max_cycles");
+    AFSI_REQUIRE(plan->coarse_dtype == AFSI_F64 || plan->coarse_dtype == plan->dtype, "unsupported coarse dtype");
+    *graph_out = nullptr;
+    const int singular = plan->bc == AFSI_BC_NEUMANN || plan->bc == AFSI_BC_PERIODIC ? 1 : 0;
+    int64_t n = 1;
+    for (int a = 0; a < plan->dim; ++a) n *= plan->level[0].shape[a];
+    SolveGraph* sg = new SolveGraph;
+    cudaGraphConditionalHandle handle;
+    if (cudaStreamCreateWithFlags(&sg->capture, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaGraphCreate(&sg->graph, 0) != cudaSuccess ||
+        cudaGraphConditionalHandleCreate(&handle, sg->graph, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
+        release(sg);
+        return fail(AFSI_ERR_CUDA, "solve graph setup failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    // the start: statistics, gauge shift, initial residual, tolerance and condition
+    if (cudaStreamBeginCaptureToGraph(sg->capture, sg->graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+        cudaSuccess) {
+        release(sg);
+        return fail(AFSI_ERR_CUDA, "solve graph capture failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    void* rhs = plan->level[0].rhs;
+    void* p0 = plan->level[0].p;
+    rc = afsi_b200_vector_stats(rhs, n, stats, stat_scratch, plan->dtype, sg->capture);
+    if (!rc) rc = afsi_b200_vector_stats(p0, n, stats + 4, stat_scratch, plan->dtype, sg->capture);
+    if (!rc && singular) {
+        rc = afsi_b200_subtract_mean(rhs, n, stats, plan->dtype, sg->capture);
+        if (!rc) rc = afsi_b200_subtract_mean(p0, n, stats + 4, plan->dtype, sg->capture);
+        if (!rc) rc = afsi_b200_vector_stats(rhs, n, stats + 8, stat_scratch, plan->dtype, sg->capture);
+    } else if (!rc && cudaMemcpyAsync(stats + 8, stats, 4 * sizeof(double), cudaMemcpyDeviceToDevice, sg->capture) !=
+                          cudaSuccess) {
+        rc = fail(AFSI_ERR_CUDA, "solve graph statistics copy failed");
+    }
+    if (!rc) rc = afsi_b200_mg_residual_norm(plan, norm, sg->capture);
+    if (!rc)
+        rc = launch_pdl("mg solve start", mg_loop_start_kernel, dim3(1), dim3(1), 0, sg->capture, loop,
+                        static_cast<const double*>(norm), static_cast<const double*>(stats), params, singular,
+                        check_every, max_cycles, handle);
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaStreamCaptureStatus status;
+    if (!rc && cudaStreamGetCaptureInfo(sg->capture, &status, nullptr, nullptr, &deps, &ndeps) != cudaSuccess)
+        rc = fail(AFSI_ERR_CUDA, "solve graph capture info failed");
+    std::vector<cudaGraphNode_t> start_leaves(deps, deps + (rc ? 0 : ndeps));
+    cudaGraph_t captured = nullptr;
+    cudaError_t end = cudaStreamEndCapture(sg->capture, &captured);
+    if (rc || end != cudaSuccess) {
+        release(sg);
+        return rc ? rc : fail(AFSI_ERR_CUDA, "solve graph capture failed: %s", cudaGetErrorString(end));
+    }
+    // the loop, after the start
+    cudaGraphNodeParams np = {};
+    cudaGraphNode_t node;
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = handle;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    if (cudaGraphAddNode(&node, sg->graph, start_leaves.data(), start_leaves.size(), &np) != cudaSuccess) {
+        release(sg);
+        return fail(AFSI_ERR_CUDA, "solve graph conditional node failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(sg->capture, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+        cudaSuccess) {
+        release(sg);
+        return fail(AFSI_ERR_CUDA, "solve graph capture failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    rc = check_block(plan, check_every, max_cycles, loop, norm, handle, sg->capture);
+    end = cudaStreamEndCapture(sg->capture, &captured);
     if (rc) {
         release(sg);
         return rc;

@@ -298,6 +298,34 @@ __device__ __forceinline__ void site_finish(const Site& s, double v, double* sqr
     }
 }
 
+// site_finish, then tail(result) in thread 0 of the last block, after the
+// result is written.
+template <class Tail>
+__device__ __forceinline__ void site_finish_then(const Site& s, double v, double* sqrt_out, Tail tail) {
+    __shared__ double warp_sums[32];
+    __shared__ bool last;
+    v = block_sum2(v, warp_sums);
+    const unsigned t = thread_linear();
+    const unsigned blocks = gridDim.x * gridDim.y * gridDim.z;
+    if (t == 0) s.partial[block_linear()] = v;
+    __threadfence();
+    __syncthreads();
+    if (t == 0) last = atomicAdd(s.counter, 1u) == blocks - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double acc = 0.0;
+    const unsigned threads = blockDim.x * blockDim.y;
+    for (unsigned i = t; i < blocks; i += threads) acc += __ldcg(s.partial + i);
+    acc = block_sum2(acc, warp_sums);
+    if (t == 0) {
+        if (sqrt_out) *sqrt_out = sqrt(acc);
+        else *s.result = acc;
+        *s.counter = 0u;
+        tail(sqrt_out ? sqrt(acc) : acc);
+    }
+}
+
 template <int BC, bool Exact, class T>
 __device__ __forceinline__ T restrict_residual_at(const T* __restrict__ p, const T* __restrict__ rhs, int cx, int cy,
                                                   int cz, const Lv<T>& L, T m) {

@@ -304,15 +304,29 @@ class _Solver:
         self.loop_graph = handle.value
         self.loop_body_launches = _lib.launch_count() - before
         _lib.forget_launches(self.loop_body_launches)
+        # the same loop with the solve's start in front of it: one launch and one host read per solve
+        self.params = torch.zeros(4, dtype=torch.float64, device=w.p[0].device)
+        self._params_key = None
+        handle = ctypes.c_void_p()
+        before = _lib.launch_count()
+        with torch.cuda.device(w.p[0].device):
+            _lib.call('afsi_b200_mg_solve_graph_create_started', ctypes.byref(w.plan), self.options.check_every,
+                      self.options.max_cycles, _lib.ptr(self.loop), _lib.ptr(w.norm), _lib.ptr(w.stats),
+                      _lib.ptr(w.stat_scratch), _lib.ptr(self.params), ctypes.byref(handle))
+        self.started_graph = handle.value
+        captured = _lib.launch_count() - before
+        _lib.forget_launches(captured)
+        self.start_launches = captured - self.loop_body_launches
 
     def __del__(self):
-        graph = getattr(self, 'loop_graph', None)
-        if graph:
-            try:
-                _lib.call('afsi_b200_mg_solve_graph_destroy', graph)
-            except Exception:
-                pass
-            self.loop_graph = None
+        for name in ('loop_graph', 'started_graph'):
+            graph = getattr(self, name, None)
+            if graph:
+                try:
+                    _lib.call('afsi_b200_mg_solve_graph_destroy', graph)
+                except Exception:
+                    pass
+                setattr(self, name, None)
 
     def _run_loop(self, tol):
         """Device-side check loop from cycle 0; returns (cycles, residual)."""
@@ -373,6 +387,28 @@ class _Solver:
         v = torch.cat((st, w.norm)).tolist()
         return dict(rhs_sum=v[0], rhs_abs=v[1], rhs_finite=v[3], p_finite=v[7], rhs_sq=v[10], residual=v[12])
 
+    def _start_and_loop(self, rhs, initial, rtol, rel, n):
+        """The started loop graph (``afsi_b200_mg_solve_graph_create_started``):
+        copy in, start (statistics, gauge shift, initial residual, tolerance on
+        the device) and the check loop in one launch, then one host read.
+        Returns the start metrics of ``_start``, the tolerance, the cycles run,
+        the last residual norm and the loop's nonfinite flag; the checks of the
+        inputs follow in ``solve`` (the device loop is not entered when one of
+        them fails)."""
+        w = self.workspace
+        w.rhs[0].copy_(rhs)
+        w.p[0].zero_() if initial is None else w.p[0].copy_(initial)
+        key = (float(rtol), float(self.options.atol), rel, float(n))
+        if key != self._params_key:
+            self.params.copy_(torch.tensor(key, dtype=torch.float64))
+            self._params_key = key
+        _lib.call('afsi_b200_mg_solve_graph_launch', self.started_graph, _lib.stream(w.p[0].device))
+        v = torch.cat((w.stats, w.norm, self.loop)).tolist()
+        tol, cycles, residual, nonfinite = v[13], int(v[14]), v[15], v[16]
+        _lib.count_replay(self.start_launches + cycles // self.options.check_every * self.loop_body_launches)
+        m = dict(rhs_sum=v[0], rhs_abs=v[1], rhs_finite=v[3], p_finite=v[7], rhs_sq=v[10], residual=v[12])
+        return m, tol, cycles, residual, nonfinite
+
     def solve(self, rhs, initial=None, *, rtol=None):
         rtol = self.options.rtol if rtol is None else rtol
         if not isfinite(rtol) or rtol < 0:
@@ -383,14 +419,18 @@ class _Solver:
                                     or initial.dtype != rhs.dtype):
             raise ValueError(self._bad_initial)
         w = self.workspace
-        m = self._start(rhs, initial)
         n = rhs.numel()
+        rel = 1e-10 if self.dtype == torch.float64 else 1e-6
+        started = getattr(self, 'started_graph', None) and not self.persistent
+        if started:
+            m, tol, cycle, loop_residual, nonfinite = self._start_and_loop(rhs, initial, rtol, rel, n)
+        else:
+            m = self._start(rhs, initial)
         if self.singular:
             if not m['rhs_finite']:
                 raise ValueError('invalid pressure RHS')
             # the reference's screen in FP64; an FP32 right-hand side that was
             # mean-free before rounding keeps a mean of its rounding errors
-            rel = 1e-10 if self.dtype == torch.float64 else 1e-6
             if abs(m['rhs_sum'] / n) > 1e-12 + rel * (m['rhs_abs'] / n):
                 raise ValueError('incompatible Neumann pressure RHS: net flux must vanish')
             if not m['p_finite']:
@@ -402,8 +442,13 @@ class _Solver:
             if self.bc == 'dirichlet':
                 raise ValueError(self._nonfinite_input)
             raise RuntimeError('nonfinite multigrid residual or RHS norm')
-        tol = max(self.options.atol, rtol * rhs_norm)
-        cycle = 0
+        if started:
+            if nonfinite:
+                raise RuntimeError(self._nonfinite_residual)
+            residual = loop_residual
+        else:
+            tol = max(self.options.atol, rtol * rhs_norm)
+            cycle = 0
         if self.persistent and residual > tol:
             # whole loop on the device: same check schedule, one host read
             w.persistent(self.options.max_cycles, tol=tol, check_every=self.options.check_every)
@@ -413,7 +458,7 @@ class _Solver:
                 raise RuntimeError('persistent multigrid barrier timed out')
             if not isfinite(residual):
                 raise RuntimeError('nonfinite multigrid residual')
-        if getattr(self, 'loop_graph', None) and residual > tol:
+        if not started and getattr(self, 'loop_graph', None) and residual > tol:
             cycle, residual = self._run_loop(tol)
         while residual > tol and cycle < self.options.max_cycles:
             count = min(self.options.check_every, self.options.max_cycles - cycle)

@@ -369,6 +369,22 @@ int32_t afsi_b200_mg_vcycles(const afsi_mg_plan* plan, int32_t cycles, afsi_stre
  * graph is captured on a private stream and launched on the caller's. */
 int32_t afsi_b200_mg_solve_graph_create(const afsi_mg_plan* plan, int32_t check_every, int32_t max_cycles,
     double* loop, double* norm, void** graph_out);
+/* The same loop with the start of a solve in front of it, so that a solve is
+ * one graph launch and one host read (mac/multigrid.py:125-172): the
+ * statistics of the right-hand side and the initial iterate in level 0
+ * (afsi_b200_vector_stats into `stats` [0:4] and [4:8]), for singular
+ * operators their gauge shift (afsi_b200_subtract_mean) and the statistics
+ * of the shifted right-hand side [8:12] (else a copy of [0:4]), the initial
+ * residual norm, then a one-thread kernel that writes loop[0] =
+ * max(atol, rtol sqrt(stats[10])), loop[1] = 0, loop[2] = the initial norm,
+ * loop[3] = its nonfinite flag, and enters the loop only when that norm is
+ * above the tolerance and the inputs are finite and (singular operators)
+ * pass the compatibility screen |sum b|/n <= 1e-12 + rel |b|_1/n.
+ * params: device double[4] = [rtol, atol, rel, n], written by the caller;
+ * stat_scratch: the scratch of afsi_b200_vector_stats. */
+int32_t afsi_b200_mg_solve_graph_create_started(const afsi_mg_plan* plan, int32_t check_every,
+    int32_t max_cycles, double* loop, double* norm, double* stats, void* stat_scratch, const double* params,
+    void** graph_out);
 int32_t afsi_b200_mg_solve_graph_launch(void* graph, afsi_stream_t stream);
 int32_t afsi_b200_mg_solve_graph_destroy(void* graph);
 
