@@ -307,6 +307,7 @@ class _Solver:
         # the same loop with the solve's start in front of it: one launch and one host read per solve
         self.params = torch.zeros(4, dtype=torch.float64, device=w.p[0].device)
         self._params_key = None
+        self._generation = 0
         handle = ctypes.c_void_p()
         before = _lib.launch_count()
         with torch.cuda.device(w.p[0].device):
@@ -387,14 +388,11 @@ class _Solver:
         v = torch.cat((st, w.norm)).tolist()
         return dict(rhs_sum=v[0], rhs_abs=v[1], rhs_finite=v[3], p_finite=v[7], rhs_sq=v[10], residual=v[12])
 
-    def _start_and_loop(self, rhs, initial, rtol, rel, n):
-        """The started loop graph (``afsi_b200_mg_solve_graph_create_started``):
-        copy in, start (statistics, gauge shift, initial residual, tolerance on
-        the device) and the check loop in one launch, then one host read.
-        Returns the start metrics of ``_start``, the tolerance, the cycles run,
-        the last residual norm and the loop's nonfinite flag; the checks of the
-        inputs follow in ``solve`` (the device loop is not entered when one of
-        them fails)."""
+    def _launch_started(self, rhs, initial, rtol, rel, n):
+        """Copy in and launch the started loop graph
+        (``afsi_b200_mg_solve_graph_create_started``: start and check loop on
+        the device); returns the device snapshot of the statistics, the initial
+        norm and the loop state, to be read by ``_read_started``."""
         w = self.workspace
         w.rhs[0].copy_(rhs)
         w.p[0].zero_() if initial is None else w.p[0].copy_(initial)
@@ -403,13 +401,20 @@ class _Solver:
             self.params.copy_(torch.tensor(key, dtype=torch.float64))
             self._params_key = key
         _lib.call('afsi_b200_mg_solve_graph_launch', self.started_graph, _lib.stream(w.p[0].device))
-        v = torch.cat((w.stats, w.norm, self.loop)).tolist()
+        self._generation += 1
+        return torch.cat((w.stats, w.norm, self.loop))
+
+    def _read_started(self, snapshot):
+        """One host read of a started solve: the start metrics of ``_start``,
+        the tolerance, the cycles run, the last residual norm and the loop's
+        nonfinite flag."""
+        v = snapshot.tolist()
         tol, cycles, residual, nonfinite = v[13], int(v[14]), v[15], v[16]
         _lib.count_replay(self.start_launches + cycles // self.options.check_every * self.loop_body_launches)
         m = dict(rhs_sum=v[0], rhs_abs=v[1], rhs_finite=v[3], p_finite=v[7], rhs_sq=v[10], residual=v[12])
         return m, tol, cycles, residual, nonfinite
 
-    def solve(self, rhs, initial=None, *, rtol=None):
+    def _solve_args(self, rhs, initial, rtol):
         rtol = self.options.rtol if rtol is None else rtol
         if not isfinite(rtol) or rtol < 0:
             raise ValueError('invalid multigrid solve tolerance')
@@ -418,12 +423,43 @@ class _Solver:
         if initial is not None and (initial.shape != rhs.shape or initial.device != rhs.device
                                     or initial.dtype != rhs.dtype):
             raise ValueError(self._bad_initial)
+        return rtol
+
+    def _started(self):
+        return getattr(self, 'started_graph', None) and not self.persistent
+
+    def solve(self, rhs, initial=None, *, rtol=None):
+        rtol = self._solve_args(rhs, initial, rtol)
+        if self._started():
+            n = rhs.numel()
+            rel = 1e-10 if self.dtype == torch.float64 else 1e-6
+            snapshot = self._launch_started(rhs, initial, rtol, rel, n)
+            return self._solve_now(rhs, initial, rtol, self._read_started(snapshot))
+        return self._solve_now(rhs, initial, rtol, None)
+
+    def solve_deferred(self, rhs, initial=None, *, rtol=None):
+        """``solve`` in two halves: the device work is launched now and the
+        returned ``PendingSolve``'s ``result()`` makes the host read, the input
+        checks and any host tail later, so that a caller can queue further
+        work first.  With the started loop graph the solution is copied out at
+        launch time; other backends solve at once."""
+        rtol = self._solve_args(rhs, initial, rtol)
+        if self._started():
+            n = rhs.numel()
+            rel = 1e-10 if self.dtype == torch.float64 else 1e-6
+            snapshot = self._launch_started(rhs, initial, rtol, rel, n)
+            return PendingSolve(self, snapshot, self.workspace.p[0].clone(), rhs, initial, rtol, self._generation)
+        return PendingSolve.done(self._solve_now(rhs, initial, rtol, None))
+
+    def _solve_now(self, rhs, initial, rtol, started):
+        """The host half of a solve (``mac/multigrid.py:125-172``); `started`
+        is the result of ``_read_started`` for a launched started graph, else
+        the start runs here."""
         w = self.workspace
         n = rhs.numel()
         rel = 1e-10 if self.dtype == torch.float64 else 1e-6
-        started = getattr(self, 'started_graph', None) and not self.persistent
-        if started:
-            m, tol, cycle, loop_residual, nonfinite = self._start_and_loop(rhs, initial, rtol, rel, n)
+        if started is not None:
+            m, tol, cycle, loop_residual, nonfinite = started
         else:
             m = self._start(rhs, initial)
         if self.singular:
@@ -442,7 +478,7 @@ class _Solver:
             if self.bc == 'dirichlet':
                 raise ValueError(self._nonfinite_input)
             raise RuntimeError('nonfinite multigrid residual or RHS norm')
-        if started:
+        if started is not None:
             if nonfinite:
                 raise RuntimeError(self._nonfinite_residual)
             residual = loop_residual
@@ -458,7 +494,7 @@ class _Solver:
                 raise RuntimeError('persistent multigrid barrier timed out')
             if not isfinite(residual):
                 raise RuntimeError('nonfinite multigrid residual')
-        if not started and getattr(self, 'loop_graph', None) and residual > tol:
+        if started is None and getattr(self, 'loop_graph', None) and residual > tol:
             cycle, residual = self._run_loop(tol)
         while residual > tol and cycle < self.options.max_cycles:
             count = min(self.options.check_every, self.options.max_cycles - cycle)
@@ -470,6 +506,43 @@ class _Solver:
         if residual > tol:
             raise RuntimeError(f'{self._not_converged}: {residual:g} > {tol:g}')
         return w.p[0].clone(), dict(cycles=cycle, residual_norm=residual, tolerance=tol, backend=self.backend)
+
+
+class PendingSolve:
+    """The host half of a multigrid solve launched by ``solve_deferred``:
+    ``result()`` reads the device state once, makes the reference's input
+    checks (raising as ``solve`` does) and returns (p, info).  A solve that
+    needs host cycles after the device loop (the loop stopped short of
+    max_cycles) runs them on the solver's workspace while no later solve has
+    been launched on it, else solves again from a copy of its inputs."""
+
+    def __init__(self, solver, snapshot, p, rhs, initial, rtol, generation):
+        self.solver, self.snapshot, self.p, self.rtol, self.generation = solver, snapshot, p, rtol, generation
+        self.rhs = rhs.clone()
+        self.initial = None if initial is None else initial.clone()
+        self._done = None
+
+    @classmethod
+    def done(cls, outcome):
+        pending = cls.__new__(cls)
+        pending._done = outcome
+        pending.p = outcome[0]
+        return pending
+
+    def result(self):
+        if self._done is None:
+            s = self.solver
+            started = s._read_started(self.snapshot)
+            m, tol, cycles, residual, nonfinite = started
+            needs_host = (residual > tol and cycles < s.options.max_cycles and not nonfinite and isfinite(residual)
+                          and m['rhs_finite'] and m['p_finite'])
+            if needs_host and s._generation != self.generation:
+                # the workspace holds a later solve: solve this one again
+                self._done = s.solve(self.rhs, self.initial, rtol=self.rtol)
+            else:
+                p, info = s._solve_now(self.rhs, self.initial, self.rtol, started)
+                self._done = (p if needs_host else self.p), info
+        return self._done
 
 
 class GeometricMultigrid(_Solver):

@@ -47,6 +47,8 @@ class DeferredStencil:
     summary: torch.Tensor   # pinned host copy of the order summary and status word
     ready: torch.cuda.Event
     buffers: tuple = None
+    status: torch.Tensor = None             # pinned copy of a table-free stencil's flags (note_transfers)
+    status_ready: torch.cuda.Event = None
 
 
 @dataclass(frozen=True)
@@ -175,6 +177,18 @@ class P2Transfer:
         ready.record(torch.cuda.current_stream(x.device))
         return DeferredStencil(TableFreeStencil(x, last, status), x, orders, host, ready)
 
+    def note_transfers(self, deferred):
+        """After the transfers that use a deferred table-free stencil: copy its
+        flag word to pinned memory behind them, so that ``confirm`` reads the
+        copy (waiting for those transfers only) instead of the device word
+        (which waits for everything queued on the stream since)."""
+        if isinstance(deferred.stencil, TableFreeStencil):
+            host = torch.empty((), dtype=torch.int32, pin_memory=True)
+            host.copy_(deferred.stencil.status, non_blocking=True)
+            ready = torch.cuda.Event()
+            ready.record(torch.cuda.current_stream(deferred.stencil.status.device))
+            deferred.status, deferred.status_ready = host, ready
+
     def check(self, stencil):
         """Raise the flags a table-free stencil's transfers set (one host read)."""
         flags = int(stencil.status.item())
@@ -196,7 +210,14 @@ class P2Transfer:
                 rule = self.rules.finish(deferred.x, deferred.orders, counts)
                 if rule is not st.rule:
                     return TableFreeStencil(st.x, rule, torch.zeros_like(st.status))
-            self.check(st)
+            if deferred.status is not None:
+                deferred.status_ready.synchronize()
+                flags = int(deferred.status.item())
+                if flags:
+                    st.status.zero_()
+                    _raise_flags(flags)
+            else:
+                self.check(st)
             return st
         if deferred.summary is None:
             return deferred.stencil

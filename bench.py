@@ -186,6 +186,29 @@ class Step:
         self.cycles.append(info['cycles'])
         return st, fields, nodal, p
 
+    def launch(self, x, coef, vel, rhs):
+        """The step's device work with no host read (the end-to-end loop):
+        the prepare, the transfers and the pressure solve are queued, and
+        ``finish`` makes the step's host reads later, after the next step has
+        been queued."""
+        deferred = self.tr.prepare_table_free(x) if self.form == 'table-free' else self.tr.prepare_deferred(x)
+        st = deferred.stencil
+        fields = self.p2t.spread(self.tr, coef, st)
+        nodal = self.p2t.assemble_velocity(self.tr, vel, st)
+        self.tr.note_transfers(deferred)
+        pending = self.mg.solve_deferred(rhs)
+        return dict(deferred=deferred, st=st, fields=fields, nodal=nodal, pending=pending)
+
+    def finish(self, h):
+        """The host half of a launched step: the solve's checks and cycle
+        count, and the rule confirmation (a changed rule, never on this
+        workload, would need the transfers again and is an error here)."""
+        p, info = h['pending'].result()
+        if self.tr.confirm(h['deferred']) is not h['st']:
+            raise RuntimeError('the interaction rule changed inside the end-to-end loop')
+        self.cycles.append(info['cycles'])
+        return p
+
 
 def algorithmic_bytes_table_free(points, elements, nodes, faces, s=8):
     """Bytes a table-free transfer launch must move at minimum: node
@@ -1141,9 +1164,12 @@ def run_b200(args):
         return ev
 
     def e2e_run(count, outs=None):
-        """`count` pipelined steps; returns the pinned result buffers."""
+        """`count` pipelined steps; returns the pinned result buffers.  Step k
+        is queued before step k-1's host reads are made, so the device always
+        has the next step in its queue."""
         ready = {0: copy_in(0)}
         done = None
+        previous = None
         for k in range(count):
             if k + 1 < count:
                 if done is not None:
@@ -1151,8 +1177,8 @@ def run_b200(args):
                 ready[k + 1] = copy_in((k + 1) % 2)
             stream.wait_event(ready.pop(k))
             b = dev_in[k % 2]
-            st, fields, nodal, p = step(b['x'], b['coef'], b['vel'], b['rhs'])
-            results = list(fields) + [nodal, p]
+            h = step.launch(b['x'], b['coef'], b['vel'], b['rhs'])
+            results = list(h['fields']) + [h['nodal'], h['pending'].p]
             done = torch.cuda.Event()
             done.record(stream)
             if outs is None:  # pinned result buffers, allocated once outside the timed region
@@ -1162,6 +1188,10 @@ def run_b200(args):
                 for o, t in zip(outs[k % 2], results):
                     t.record_stream(copy)
                     o.copy_(t, non_blocking=True)
+            if previous is not None:
+                step.finish(previous)
+            previous = h
+        step.finish(previous)
         stream.wait_stream(copy)
         return outs
 

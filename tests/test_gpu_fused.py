@@ -173,3 +173,23 @@ def test_table_free_support_and_connectivity_errors_do_not_trap():
     tr.assemble_velocity(tuple(v.to(DEV) for v in synthetic.fourier_velocity3d(grid, seed=3)), bad)
     with pytest.raises(RuntimeError, match='connectivity'):
         tr.check(bad)
+
+
+def test_deferred_flags_are_read_from_the_pinned_copy():
+    """note_transfers copies a table-free stencil's flag word behind its
+    transfers; confirm then raises the support flag from that copy."""
+    X, cells = synthetic.prolate_shell(1, 6, 8, inner=(.125, .075, .075), outer=(.16, .11, .11))
+    grid = MACGrid((32, 32, 32), (1., 1., 1.))
+    Xd = t(X)
+    tr = p2t.P1Transfer(grid, Xd, t(cells))
+    tr.confirm(tr.prepare_table_free(Xd))
+    ok = tr.prepare_table_free(Xd)
+    tr.spread(t(np.ones((X.shape[0], 3))), ok.stencil)
+    tr.note_transfers(ok)
+    assert tr.confirm(ok) is ok.stencil
+    moved = Xd - torch.tensor([.45, 0., 0.], device=DEV, dtype=torch.float64)  # the same rule, part outside
+    bad = tr.prepare_table_free(moved)
+    tr.spread(t(np.ones((X.shape[0], 3))), bad.stencil)
+    tr.note_transfers(bad)
+    with pytest.raises(ValueError, match='support'):
+        tr.confirm(bad)

@@ -379,3 +379,32 @@ def test_red_black_smoother_option_checks():
     rhs = synthetic.mean_free_normal(grid.shape, seed=3).to(DEV)
     p, info = refined.solve(rhs)
     assert info['residual_norm'] <= info['tolerance'] and info['backend'].endswith('red-black-refined')
+
+
+def test_deferred_solves_equal_synchronous_solves():
+    """solve_deferred queues the started loop graph and reads later: two
+    solves queued back to back give, read in either order, the solutions,
+    cycle counts and norms of the synchronous solves; bad input raises at
+    result() as solve raises it."""
+    grid = MACGrid((32, 32, 32), (1., 1., 1.))
+    mg = GeometricMultigrid(grid)
+    rhs = [synthetic.mean_free_normal(grid.shape, seed=s).to(DEV) for s in (21, 22)]
+    sync = [mg.solve(r) for r in rhs]
+    pending = [mg.solve_deferred(r) for r in rhs]
+    for (p, info), pend in zip(reversed(sync), reversed(pending)):
+        q, qinfo = pend.result()
+        assert torch.equal(p, q)
+        assert qinfo['cycles'] == info['cycles'] and qinfo['residual_norm'] == info['residual_norm']
+        assert pend.result()[0] is q  # read once
+    bad = rhs[0] + 1.0  # net flux
+    pend = mg.solve_deferred(bad)
+    with pytest.raises(ValueError, match='incompatible'):
+        pend.result()
+    # a deferred solve whose device loop leaves host cycles, read after a later solve
+    short = GeometricMultigrid(grid, options=MGOptions(max_cycles=5))
+    first = short.solve_deferred(rhs[0], rtol=1e-30)
+    later = short.solve_deferred(rhs[1])
+    with pytest.raises(RuntimeError, match='did not converge'):
+        first.result()
+    with pytest.raises(RuntimeError, match='did not converge'):
+        later.result()
