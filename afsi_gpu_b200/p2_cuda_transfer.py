@@ -40,7 +40,12 @@ from .quadrature import RuleBuilder, InteractionRule
 class DeferredStencil:
     """Tables prepared with the cached rule before the rule was checked
     (``P2Transfer.prepare_deferred``): ``stencil`` is usable at once;
-    ``P2Transfer.confirm`` settles it."""
+    ``P2Transfer.confirm`` settles it.  Until then a point outside the support
+    may have rows with base -1 (the prepare's invalid-point rows); the spread
+    and gather-assemble kernels check every support against the face arrays
+    before they touch it (an element whose box leaves the arrays takes the
+    per-point path, and a point outside is skipped with AFSI_FLAG_INDEX), and
+    any other reader of unconfirmed tables must do the same."""
     stencil: 'SharedAdaptiveStencil'
     x: torch.Tensor
     orders: torch.Tensor

@@ -402,10 +402,10 @@ int32_t afsi_b200_mg_residual_norm(const afsi_mg_plan* plan, double* norm_out, a
  * needs more than 4096 reduction blocks are rejected with AFSI_ERR_ARG (2D
  * grids above about 2^20 cells; 3D grids whose y-z section exceeds about 2^20
  * cells).  The
- * first call on a device looks the array's address up (cudaGetSymbolAddress);
- * make that first call before any stream capture.  The address is cached per
- * device ordinal and assumes the device's primary context and no device reset
- * afterwards.  Every call shares the array: calls that overlap on the GPU race. */
+ * first call on a device looks the array's address up (cudaGetSymbolAddress)
+ * and caches it per device ordinal, which assumes the device's primary context
+ * and no device reset afterwards.  Every call shares the array: calls that
+ * overlap on the GPU race. */
 int32_t afsi_b200_mg_residual_norm_noalloc(const void* p, const void* rhs, const int64_t* shape,
     const double* h2, int32_t dim, int32_t bc, double* norm_out, int32_t dtype, afsi_stream_t stream);
 

@@ -61,3 +61,29 @@ def test_noalloc_residual_norm_2d_channel_and_rejects_large_grids():
     big = torch.zeros((2048, 4096), device='cuda')  # 2^23 cells: 32768 reduction blocks
     with pytest.raises(RuntimeError, match='at most 4096'):
         _noalloc_norm(big, big, (1 / 2048, 1 / 4096), _lib.BC_CHANNEL)
+
+
+@pytest.mark.parametrize('case', ['dirichlet', 'periodic'])
+def test_noalloc_residual_norm_other_boundaries(case):
+    """Dirichlet (3D) and periodic-x (2D) against the scratch-using norm of
+    their own solvers, bitwise."""
+    from afsi_gpu_b200.multigrid import DirichletMultigrid
+    rng = np.random.default_rng(23)
+    if case == 'dirichlet':
+        grid = MACGrid((32, 32, 32), (1., 1., 1.))
+        mg, bc = DirichletMultigrid(grid, backend='b200'), _lib.BC_DIRICHLET
+    else:
+        grid = ChannelGrid((128, 32), (4., 1.), periodic=True)
+        mg, bc = ChannelMultigrid(grid, backend='b200'), _lib.BC_PERIODIC
+    for trial in range(2):
+        p = torch.as_tensor(rng.standard_normal(grid.shape), device='cuda')
+        rhs = torch.as_tensor(rng.standard_normal(grid.shape), device='cuda')
+        got = _noalloc_norm(p, rhs, grid.spacing, bc)
+        assert got.item() == _scratch_norm(mg, p, rhs).item() > 0
+
+
+def test_noalloc_residual_norm_rejects_large_3d_sections():
+    """A 3D grid whose y-z section needs more than 4096 reduction blocks."""
+    big = torch.zeros((2, 1024, 1040), device='cuda')
+    with pytest.raises(RuntimeError, match='at most 4096'):
+        _noalloc_norm(big, big, (.5, 1 / 1024, 1 / 1040), _lib.BC_NEUMANN)
