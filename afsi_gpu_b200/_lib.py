@@ -153,6 +153,10 @@ _SIGNATURES = {
     'afsi_b200_fe_fused_spread': [c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p, c_int64,
                                   c_void_p, c_void_p, P_F64, P_F64, P_F64, c_void_p, c_void_p, c_void_p, c_int64,
                                   c_int64, c_int64, c_double, c_void_p, c_int32, c_int32, c_void_p],
+    'afsi_b200_fe_det_spread_bytes': [c_int64, c_int64, c_int64, c_int64, c_int32],
+    'afsi_b200_fe_det_spread': [c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p, c_int64,
+                                c_void_p, c_void_p, P_F64, P_F64, P_F64, c_void_p, c_void_p, c_void_p, c_int64,
+                                c_int64, c_int64, c_double, c_void_p, c_int64, c_void_p, c_int32, c_int32, c_void_p],
     'afsi_b200_fe_fused_gather': [c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p, c_int64,
                                   c_void_p, c_void_p, c_void_p, c_void_p, P_F64, P_F64, P_F64, c_void_p, c_int64,
                                   c_int64, c_int64, c_void_p, c_int32, c_int32, c_void_p],
@@ -203,7 +207,7 @@ _RESTYPES = {'afsi_b200_last_error': ctypes.c_char_p, 'afsi_b200_mg_scratch_byte
              'afsi_b200_p1_plan_scratch_bytes': ctypes.c_int64, 'afsi_b200_hash_csr_scratch_bytes': ctypes.c_int64,
              'afsi_b200_pcg_scratch_bytes': ctypes.c_int64, 'afsi_b200_mg_refine_scratch_bytes': ctypes.c_int64,
              'afsi_b200_stokes_partial_blocks': ctypes.c_int64, 'afsi_b200_cache_scratch_bytes': ctypes.c_int64,
-             'afsi_b200_det_plan_bytes': ctypes.c_int64}
+             'afsi_b200_det_plan_bytes': ctypes.c_int64, 'afsi_b200_fe_det_spread_bytes': ctypes.c_int64}
 
 
 def exported_symbols():

@@ -38,6 +38,7 @@
 // [0, nodes) sets AFSI_FLAG_INDEX and is skipped.
 #include <climits>
 #include <cmath>
+#include <cub/device/device_radix_sort.cuh>
 #include "common.cuh"
 #include "peskin.cuh"
 #include "runs.cuh"
@@ -50,6 +51,8 @@ constexpr int kFWarps = 2;        // warps per block (spread and gather)
 // have 15 or 64 points), 32 for P1 (orders 2 and 3 have 8 and 27 points).
 template <int NPC> struct FChunk { static constexpr int value = NPC == 10 ? 64 : 32; };
 constexpr int kFBoxCap = 288;     // entries of one component's padded box (spread) or patch (gather)
+constexpr int kDetBoxCap = 640;   // padded box of the deterministic spread (extents up to 8 x 8 x 8)
+constexpr int kDetExt = 8;        // largest box extent per axis of the deterministic spread
 
 struct FusedDims {
     int64_t nx, ny, nz, nodes, elements, nq;
@@ -159,9 +162,9 @@ __device__ __forceinline__ bool fpoint_inside(const FusedDims& g, int c, int x, 
 }
 
 // Padded strides of component c's box; false when the box leaves the face
-// array or does not fit kFBoxCap entries (the element then takes the direct
+// array or does not fit `cap` entries (the element then takes the direct
 // L2 path).
-__device__ __forceinline__ bool fbox_layout(const FBox& bx, const FusedDims& g, int c, int& sx, int& sy) {
+__device__ __forceinline__ bool fbox_layout(const FBox& bx, const FusedDims& g, int c, int& sx, int& sy, int cap) {
     const int64_t fe[3] = {g.nx + (c == 0), g.ny + (c == 1), g.nz + (c == 2)};
     bool inside = true;
 #pragma unroll
@@ -169,7 +172,7 @@ __device__ __forceinline__ bool fbox_layout(const FBox& bx, const FusedDims& g, 
     sx = sy = 0;
     if (!inside || bx.ext[1] > 64 || bx.ext[2] > 64) return false;
     padded_strides(bx.ext[1], bx.ext[2], sx, sy);
-    return int64_t(bx.ext[0]) * sx <= kFBoxCap;
+    return int64_t(bx.ext[0]) * sx <= cap;
 }
 
 template <class F>
@@ -213,14 +216,14 @@ __device__ __forceinline__ bool stage_element(const TP* __restrict__ x, const in
 }
 
 // Per-warp shared memory of both kernels.
-template <class TP, class T, int NPC>
+template <class TP, class T, int NPC, int Cap = kFBoxCap>
 struct __align__(16) FStage {
     T w[(FChunk<NPC>::value + 1) * 12];  // one component's rows: x at q*12, y at q*12+4, z at q*12+8; the last stays zero
     TP pos[FChunk<NPC>::value * 3];    // positions of a resident rule
     int b[FChunk<NPC>::value * 3];     // support origins (absolute) of the component
     int key[FChunk<NPC>::value];       // run keys in the box, -1 for an invalid point
     T f[FChunk<NPC>::value + 1];       // spread: force factors of the component; the last stays zero
-    T box[kFBoxCap];                   // padded box
+    T box[Cap];                        // padded box
     T coef[32];
     TP xs[32];
     int perm[4 * FChunk<NPC>::value];  // points grouped by key (spread_element)
@@ -278,8 +281,8 @@ __device__ __forceinline__ bool component_box_all(const TP* __restrict__ Npos, c
 // weight rows and absolute support origins into shared memory, the spread's
 // force factors when coef != null; the bounds of the valid points' origins
 // are added to mn/mx.  Invalid points get b[q*3] = INT_MIN.
-template <class TP, class T, int NPC>
-__device__ __forceinline__ void component_pass(FStage<TP, T, NPC>& s, const TP* __restrict__ Npos,
+template <class TP, class T, int NPC, int Cap>
+__device__ __forceinline__ void component_pass(FStage<TP, T, NPC, Cap>& s, const TP* __restrict__ Npos,
                                                const T* __restrict__ N, const T* __restrict__ W, bool resident,
                                                unsigned long long valid_bits, int64_t e, int64_t nq, int64_t q0,
                                                int n, const Geo<TP>& geo, int c, const T* coef, T volume, T inv_volume, int mn[3],
@@ -319,8 +322,8 @@ __device__ __forceinline__ void component_pass(FStage<TP, T, NPC>& s, const TP* 
 
 // Run keys of points 0..n-1 in box bx (-1 for invalid points, or all -1 when
 // the box does not fit).
-template <class TP, class T, int NPC>
-__device__ __forceinline__ void component_keys(FStage<TP, T, NPC>& s, int n, const FBox& bx, bool fits) {
+template <class TP, class T, int NPC, int Cap>
+__device__ __forceinline__ void component_keys(FStage<TP, T, NPC, Cap>& s, int n, const FBox& bx, bool fits) {
     for (int q = threadIdx.x & 31; q < n; q += 32) {
         const int bx0 = s.b[q * 3];
         s.key[q] = (fits && bx0 != INT_MIN)
@@ -331,13 +334,26 @@ __device__ __forceinline__ void component_keys(FStage<TP, T, NPC>& s, int n, con
 
 // ------------------------------------------------------------------ spread
 
-template <class TP, class T, int NPC>
+// Element boxes of the deterministic form: box b = e * 3 + c is component
+// c's box of element e, stored dense (ext0 x ext1 x ext2, z fastest) in slot
+// b of kDetSlot entries, with meta[b * 8 + 0..5] = lo0, lo1, lo2, ext0, ext1,
+// ext2 (zeroed by the caller: ext0 == 0 is no box).
+constexpr int kDetSlot = kDetExt * kDetExt * kDetExt;
+constexpr int kDetMeta = 8;
+
+// Boxes: instead of adding each element's box to the face arrays with L2
+// reductions, write it to its slot (plain stores); the box may then take
+// kDetBoxCap padded entries with extents up to kDetExt, and an element whose
+// box does not fit sets AFSI_FLAG_OVERFLOW and contributes nothing.
+template <class TP, class T, int NPC, bool Boxes>
 __global__ void __launch_bounds__(kFWarps * 32, 8) fused_spread_kernel(
     const TP* __restrict__ x, const int64_t* __restrict__ cells, const TP* __restrict__ Npos,
     const T* __restrict__ N, const T* __restrict__ W, const T* __restrict__ value, Geo<TP> geo, T* __restrict__ u0,
-    T* __restrict__ u1, T* __restrict__ u2, FusedDims g, T volume, int32_t* status) {
+    T* __restrict__ u1, T* __restrict__ u2, FusedDims g, T volume, int32_t* status, T* __restrict__ slots,
+    int32_t* __restrict__ meta) {
     extern __shared__ __align__(16) unsigned char fused_smem[];
-    FStage<TP, T, NPC>& s = reinterpret_cast<FStage<TP, T, NPC>*>(fused_smem)[threadIdx.x >> 5];
+    constexpr int Cap = Boxes ? kDetBoxCap : kFBoxCap;
+    FStage<TP, T, NPC, Cap>& s = reinterpret_cast<FStage<TP, T, NPC, Cap>*>(fused_smem)[threadIdx.x >> 5];
     constexpr int C = FChunk<NPC>::value;
     const int lane = threadIdx.x & 31, half = lane >> 4, li = (lane >> 2) & 3, lj = lane & 3;
     const int64_t warps = int64_t(gridDim.x) * kFWarps;
@@ -364,22 +380,26 @@ __global__ void __launch_bounds__(kFWarps * 32, 8) fused_spread_kernel(
                 __syncwarp();
                 int mn[3], mx[3];
                 bounds_init(mn, mx);
-                component_pass<TP, T, NPC>(s, Npos, N, W, resident, valid, e, g.nq, q0, n, geo, c, s.coef, volume,
+                component_pass(s, Npos, N, W, resident, valid, e, g.nq, q0, n, geo, c, s.coef, volume,
                                            inv_volume, mn, mx);
                 if (resident) {
                     any = bounds_finish(mn, mx, bx);
                     if (!any) break;
                 }
                 if (q0 == 0) {
-                    fits = fbox_layout(bx, g, c, sx, sy);
+                    fits = fbox_layout(bx, g, c, sx, sy, Cap) &&
+                           (!Boxes || (bx.ext[0] <= kDetExt && bx.ext[1] <= kDetExt && bx.ext[2] <= kDetExt));
                     if (fits)
-                        for (int t = lane; t < kFBoxCap; t += 32) s.box[t] = T(0);
+                        for (int t = lane; t < Cap; t += 32) s.box[t] = T(0);
                 }
                 __syncwarp();
                 component_keys(s, n, bx, fits);
                 __syncwarp();
                 if (fits) {
                     spread_element<T, C>(s.box, s.key, s.f, s.w, s.w + 4, s.w + 8, n, sx, sy, s.perm, s.rs, s.rk);
+                } else if (Boxes) {
+                    if (lane == 0) flag(status, AFSI_FLAG_OVERFLOW);
+                    break;
                 } else {
                     for (int q = half; q < n; q += 2) {
                         const int gx = s.b[q * 3], gy = s.b[q * 3 + 1], gz = s.b[q * 3 + 2];
@@ -397,14 +417,231 @@ __global__ void __launch_bounds__(kFWarps * 32, 8) fused_spread_kernel(
             }
             __syncwarp();
             if (any && fits) {
-                fbox_walk(lane, bx.ext[0], bx.ext[1], bx.ext[2], [&](int xx, int yy, int zz) {
-                    const T v = s.box[xx * sx + yy * sy + zz];
-                    if (v != T(0)) atomicAdd(field + ffield_index(g, c, bx.lo[0] + xx, bx.lo[1] + yy, bx.lo[2] + zz), v);
-                });
+                if (Boxes) {
+                    const int64_t b = e * 3 + c;
+                    T* slot = slots + b * kDetSlot;
+                    const int ey = bx.ext[1], ez = bx.ext[2];
+                    fbox_walk(lane, bx.ext[0], ey, ez, [&](int xx, int yy, int zz) {
+                        slot[(xx * ey + yy) * ez + zz] = s.box[xx * sx + yy * sy + zz];
+                    });
+                    const int mv = lane == 0   ? bx.lo[0]
+                                   : lane == 1 ? bx.lo[1]
+                                   : lane == 2 ? bx.lo[2]
+                                   : lane == 3 ? bx.ext[0]
+                                   : lane == 4 ? ey
+                                               : ez;
+                    if (lane < 6) meta[b * kDetMeta + lane] = mv;
+                } else {
+                    fbox_walk(lane, bx.ext[0], bx.ext[1], bx.ext[2], [&](int xx, int yy, int zz) {
+                        const T v = s.box[xx * sx + yy * sy + zz];
+                        if (v != T(0))
+                            atomicAdd(field + ffield_index(g, c, bx.lo[0] + xx, bx.lo[1] + yy, bx.lo[2] + zz), v);
+                    });
+                }
             }
         }
         __syncwarp();
     }
+}
+
+// ------------------------------------------------- deterministic reduction
+//
+// The element boxes (fused_spread_kernel<..., true>) are added to the face
+// arrays in a fixed order per face: every box names the 4x4x4 face tiles it
+// overlaps (at most three per axis), the (tile, box) pairs are sorted by tile
+// with a stable radix sort (boxes of a tile stay in box order), and one CTA
+// per tile adds, face by face, the covering boxes' entries in an order fixed
+// by that list (det_box_reduce_kernel).  Small tiles keep the box list short:
+// on a shell, 8x8x8 tiles put up to about 5000 boxes in one tile.  No
+// atomics: the result is bitwise the same on every run, and equals the
+// L2-reduction spread to rounding.
+
+constexpr int kDetTile = 4;
+constexpr int kDetKeys = 27;  // tile keys per box
+
+struct DetTiles {
+    int64_t n[3][3];  // tiles per axis of each component's face array
+    int64_t first[4]; // first tile id of each component; first[3] = all tiles
+};
+
+inline DetTiles det_tiles(int64_t nx, int64_t ny, int64_t nz) {
+    DetTiles t;
+    int64_t acc = 0;
+    for (int c = 0; c < 3; ++c) {
+        const int64_t fe[3] = {nx + (c == 0), ny + (c == 1), nz + (c == 2)};
+        for (int a = 0; a < 3; ++a) t.n[c][a] = (fe[a] + kDetTile - 1) / kDetTile;
+        t.first[c] = acc;
+        acc += t.n[c][0] * t.n[c][1] * t.n[c][2];
+    }
+    t.first[3] = acc;
+    return t;
+}
+
+// Keys of box b: the ids of the tiles it overlaps, then `none`; a box that
+// spans more than three tiles along an axis sets AFSI_FLAG_OVERFLOW.
+__global__ void det_box_keys_kernel(const int32_t* __restrict__ meta, int64_t boxes, DetTiles t, uint32_t none,
+                                    uint32_t* __restrict__ keys, int32_t* __restrict__ vals, int32_t* status) {
+    for (int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; b < boxes; b += int64_t(gridDim.x) * blockDim.x) {
+        const int32_t* m = meta + b * kDetMeta;
+        const int c = int(b % 3);
+        const int64_t first = c == 2 ? t.first[2] : c == 1 ? t.first[1] : t.first[0];
+        const int64_t n1 = c == 2 ? t.n[2][1] : c == 1 ? t.n[1][1] : t.n[0][1];
+        const int64_t n2 = c == 2 ? t.n[2][2] : c == 1 ? t.n[1][2] : t.n[0][2];
+        uint32_t* kb = keys + b * kDetKeys;
+        int32_t* vb = vals + b * kDetKeys;
+        int j = 0;
+        if (m[3] > 0) {
+            int lo[3], hi[3];
+            bool ok = true;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = m[a] / kDetTile;
+                hi[a] = (m[a] + m[3 + a] - 1) / kDetTile;
+                ok = ok && hi[a] - lo[a] <= 2;
+            }
+            if (ok) {
+                for (int i = lo[0]; i <= hi[0]; ++i)
+                    for (int jy = lo[1]; jy <= hi[1]; ++jy)
+                        for (int kz = lo[2]; kz <= hi[2]; ++kz) {
+                            kb[j] = uint32_t(first + (int64_t(i) * n1 + jy) * n2 + kz);
+                            vb[j] = int32_t(b);
+                            ++j;
+                        }
+            } else {
+                flag(status, AFSI_FLAG_OVERFLOW);
+            }
+        }
+        for (; j < kDetKeys; ++j) {
+            kb[j] = none;
+            vb[j] = int32_t(b);
+        }
+    }
+}
+
+// [start, end) of every tile's pairs in the sorted keys (zeroed by the
+// caller: an absent tile keeps an empty range).
+__global__ void det_box_ranges_kernel(const uint32_t* __restrict__ keys, int64_t n, uint32_t none,
+                                      int32_t* __restrict__ start, int32_t* __restrict__ end) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const uint32_t k = keys[i];
+        if (k == none) continue;
+        if (i == 0 || keys[i - 1] != k) start[k] = int32_t(i);
+        if (i + 1 == n || keys[i + 1] != k) end[k] = int32_t(i + 1);
+    }
+}
+
+constexpr int kDetBatch = 64;   // boxes staged per step of the reduction
+constexpr int kDetParts = 4;    // threads per face, each over its quarter of every staged batch
+constexpr int kDetAhead = kDetBatch / kDetParts;  // loads a thread issues before adding them
+
+// One CTA of 256 threads per tile: thread t takes face f = t % 64 of the
+// tile ((f/16, f/4 % 4, f % 4)) and part q = t / 64.  The tile's boxes are
+// staged 64 at a time; part q reads the entries of boxes 16q .. 16q+15 of
+// each batch that cover its face (all 16 loads issued before the adds, so one
+// memory round trip per batch rather than per box) and adds them in order to
+// its partial sum; the face then adds the four partials in part order.  The
+// association is fixed by the tile's box list alone: bitwise reproducible.
+template <class T>
+__global__ void __launch_bounds__(kDetBatch * kDetParts) det_box_reduce_kernel(
+    const T* __restrict__ slots, const int32_t* __restrict__ meta, const int32_t* __restrict__ vals,
+    const int32_t* __restrict__ start, const int32_t* __restrict__ end, DetTiles t, FusedDims g, T* __restrict__ u0,
+    T* __restrict__ u1, T* __restrict__ u2) {
+    __shared__ int4 s_lo[kDetBatch], s_ext[kDetBatch];
+    __shared__ T part[kDetParts][kDetBatch];
+    const int64_t tile = blockIdx.x;
+    const int s0 = start[tile], e0 = end[tile];
+    if (s0 >= e0) return;
+    const int c = tile >= t.first[2] ? 2 : tile >= t.first[1] ? 1 : 0;
+    const int64_t r = tile - (c == 2 ? t.first[2] : c == 1 ? t.first[1] : t.first[0]);
+    const int64_t n1 = c == 2 ? t.n[2][1] : c == 1 ? t.n[1][1] : t.n[0][1];
+    const int64_t n2 = c == 2 ? t.n[2][2] : c == 1 ? t.n[1][2] : t.n[0][2];
+    const int64_t tz = r % n2, ty = (r / n2) % n1, tx = r / (n2 * n1);
+    const int th = threadIdx.x, f = th % kDetBatch, q = th / kDetBatch;
+    const int fx = int(tx) * kDetTile + (f >> 4), fy = int(ty) * kDetTile + ((f >> 2) & 3),
+              fz = int(tz) * kDetTile + (f & 3);
+    const int64_t fe0 = g.nx + (c == 0), fe1 = g.ny + (c == 1), fe2 = g.nz + (c == 2);
+    T acc = T(0);
+    for (int i0 = s0; i0 < e0; i0 += kDetBatch) {
+        const int n = min(kDetBatch, e0 - i0);
+        __syncthreads();
+        if (th < n) {
+            const int b = vals[i0 + th];
+            const int32_t* m = meta + int64_t(b) * kDetMeta;
+            s_lo[th] = make_int4(m[0], m[1], m[2], b);
+            s_ext[th] = make_int4(m[3], m[4], m[5], 0);
+        }
+        __syncthreads();
+        T v[kDetAhead];
+#pragma unroll
+        for (int u = 0; u < kDetAhead; ++u) {
+            const int j = q * kDetAhead + u;
+            v[u] = T(0);
+            if (j < n) {
+                const int4 lo = s_lo[j], ex = s_ext[j];
+                const int dx = fx - lo.x, dy = fy - lo.y, dz = fz - lo.z;
+                if (unsigned(dx) < unsigned(ex.x) && unsigned(dy) < unsigned(ex.y) && unsigned(dz) < unsigned(ex.z))
+                    v[u] = slots[int64_t(lo.w) * kDetSlot + (dx * ex.y + dy) * ex.z + dz];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kDetAhead; ++u) acc += v[u];
+    }
+    part[q][f] = acc;
+    __syncthreads();
+    if (q == 0 && fx < fe0 && fy < fe1 && fz < fe2) {
+        T* field = c == 0 ? u0 : c == 1 ? u1 : u2;
+        T* out = field + (int64_t(fx) * fe1 + fy) * fe2 + fz;
+        T sum = part[0][f];
+#pragma unroll
+        for (int k = 1; k < kDetParts; ++k) sum += part[k][f];
+        *out = *out + sum;
+    }
+}
+
+// Scratch of the deterministic table-free spread of `elements` elements:
+// slots, meta, keys and values (in and out), tile ranges, sort temporary.
+struct DetBoxLayout {
+    int64_t slots, meta, keys_in, keys_out, vals_in, vals_out, start, end, temp, temp_bytes, bytes;
+    int bits;
+};
+
+inline int64_t det_align(int64_t v) { return (v + 255) / 256 * 256; }
+
+inline int det_key_bits(int64_t limit) {
+    int bits = 1;
+    while (bits < 32 && (int64_t(1) << bits) <= limit) ++bits;
+    return bits;
+}
+
+inline DetBoxLayout det_box_layout(int64_t elements, const DetTiles& t, int64_t esize) {
+    DetBoxLayout L;
+    const int64_t boxes = elements * 3, pairs = boxes * kDetKeys;
+    int64_t off = 0;
+    L.slots = off;
+    off = det_align(off + boxes * kDetSlot * esize);
+    L.meta = off;
+    off = det_align(off + boxes * kDetMeta * 4);
+    L.keys_in = off;
+    off = det_align(off + pairs * 4);
+    L.keys_out = off;
+    off = det_align(off + pairs * 4);
+    L.vals_in = off;
+    off = det_align(off + pairs * 4);
+    L.vals_out = off;
+    off = det_align(off + pairs * 4);
+    L.start = off;
+    off = det_align(off + t.first[3] * 4);
+    L.end = off;
+    off = det_align(off + t.first[3] * 4);
+    L.bits = det_key_bits(t.first[3]);
+    size_t temp = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, temp, static_cast<const uint32_t*>(nullptr),
+                                    static_cast<uint32_t*>(nullptr), static_cast<const int32_t*>(nullptr),
+                                    static_cast<int32_t*>(nullptr), int(pairs > 0 ? pairs : 1), 0, L.bits);
+    L.temp = off;
+    L.temp_bytes = int64_t(temp);
+    L.bytes = det_align(off + L.temp_bytes);
+    return L;
 }
 
 // ------------------------------------------------------------------ gather
@@ -630,16 +867,95 @@ extern "C" int32_t afsi_b200_fe_fused_spread(int32_t nodes_per_cell, const void*
         const size_t smem = sizeof(FStage<TP, T, NPC>) * kFWarps;
         static bool configured = false;  // once per instantiation, before any graph capture of it
         if (!configured) {
-            cudaFuncSetAttribute(fused_spread_kernel<TP, T, NPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(fused_spread_kernel<TP, T, NPC, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            configured = true;
+        }
+        fused_spread_kernel<TP, T, NPC, false><<<fused_blocks(elements, kFWarps), kFWarps * 32, smem, s>>>(
+            static_cast<const TP*>(x), cells, static_cast<const TP*>(N_pos), static_cast<const T*>(N),
+            static_cast<const T*>(W), static_cast<const T*>(value), make_geo<TP>(origin, spacing, limits),
+            static_cast<T*>(u0), static_cast<T*>(u1), static_cast<T*>(u2), g, T(volume), status,
+            static_cast<T*>(nullptr), static_cast<int32_t*>(nullptr));
+    });
+    return launched(nodes_per_cell == 10 ? "p2_fused_spread" : "p1_fused_spread");
+}
+
+extern "C" int64_t afsi_b200_fe_det_spread_bytes(int64_t elements, int64_t nx, int64_t ny, int64_t nz,
+                                                 int32_t dtype) {
+    if (elements < 0 || elements * 3 * kDetKeys >= (int64_t(1) << 31)) return -1;  // sort items are int
+    if (nx < 4 || ny < 4 || nz < 4 || nx >= (1 << 28) || ny >= (1 << 28) || nz >= (1 << 28)) return -1;
+    if (dtype != AFSI_F32 && dtype != AFSI_F64) return -1;
+    const DetTiles t = det_tiles(nx, ny, nz);
+    if (t.first[3] >= (int64_t(1) << 31)) return -1;
+    return det_box_layout(elements, t, dtype == AFSI_F64 ? 8 : 4).bytes;
+}
+
+extern "C" int32_t afsi_b200_fe_det_spread(int32_t nodes_per_cell, const void* x, int64_t nodes,
+                                           const int64_t* cells, int64_t elements, const void* N_pos,
+                                           const void* N, int64_t nq, const void* W, const void* value,
+                                           const double* origin, const double* spacing, const double* limits,
+                                           void* u0, void* u1, void* u2, int64_t nx, int64_t ny, int64_t nz,
+                                           double volume, void* scratch, int64_t scratch_bytes, int32_t* status,
+                                           int32_t pos_dtype, int32_t dtype, afsi_stream_t stream) {
+    int32_t rc = check_fused(nodes_per_cell, nodes, elements, nq, nx, ny, nz, origin, spacing, limits, pos_dtype,
+                             dtype);
+    if (rc) return rc;
+    AFSI_REQUIRE(isfinite(volume) && volume > 0, "invalid cell volume");
+    if (elements == 0) return AFSI_OK;
+    AFSI_REQUIRE(x && cells && N_pos && N && W && value && u0 && u1 && u2 && scratch, "null device pointer");
+    const int64_t need = afsi_b200_fe_det_spread_bytes(elements, nx, ny, nz, dtype);
+    AFSI_REQUIRE(need >= 0, "too many elements or tiles for the deterministic spread");
+    AFSI_REQUIRE(scratch_bytes >= need, "deterministic spread scratch too small (%lld of %lld bytes)",
+                 static_cast<long long>(scratch_bytes), static_cast<long long>(need));
+    const FusedDims g{nx, ny, nz, nodes, elements, nq};
+    const DetTiles t = det_tiles(nx, ny, nz);
+    const int64_t boxes = elements * 3, pairs = boxes * kDetKeys;
+    const uint32_t none = uint32_t(t.first[3]);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned char* base = static_cast<unsigned char*>(scratch);
+    AFSI_FUSED_DISPATCH(nodes_per_cell, pos_dtype, dtype, {
+        const DetBoxLayout L = det_box_layout(elements, t, int64_t(sizeof(T)));
+        T* slots = reinterpret_cast<T*>(base + L.slots);
+        int32_t* meta = reinterpret_cast<int32_t*>(base + L.meta);
+        uint32_t* keys_in = reinterpret_cast<uint32_t*>(base + L.keys_in);
+        uint32_t* keys_out = reinterpret_cast<uint32_t*>(base + L.keys_out);
+        int32_t* vals_in = reinterpret_cast<int32_t*>(base + L.vals_in);
+        int32_t* vals_out = reinterpret_cast<int32_t*>(base + L.vals_out);
+        int32_t* start = reinterpret_cast<int32_t*>(base + L.start);
+        int32_t* end = reinterpret_cast<int32_t*>(base + L.end);
+        if (cudaMemsetAsync(meta, 0, size_t(boxes) * kDetMeta * 4, s) != cudaSuccess ||
+            cudaMemsetAsync(start, 0, size_t(t.first[3]) * 4, s) != cudaSuccess ||
+            cudaMemsetAsync(end, 0, size_t(t.first[3]) * 4, s) != cudaSuccess)
+            return fail(AFSI_ERR_CUDA, "deterministic spread: clearing the scratch failed");
+        const size_t smem = sizeof(FStage<TP, T, NPC, kDetBoxCap>) * kFWarps;
+        static bool configured = false;  // once per instantiation, before any graph capture of it
+        if (!configured) {
+            cudaFuncSetAttribute(fused_spread_kernel<TP, T, NPC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(smem));
             configured = true;
         }
-        fused_spread_kernel<TP, T, NPC><<<fused_blocks(elements, kFWarps), kFWarps * 32, smem, s>>>(
+        fused_spread_kernel<TP, T, NPC, true><<<fused_blocks(elements, kFWarps), kFWarps * 32, smem, s>>>(
             static_cast<const TP*>(x), cells, static_cast<const TP*>(N_pos), static_cast<const T*>(N),
             static_cast<const T*>(W), static_cast<const T*>(value), make_geo<TP>(origin, spacing, limits),
-            static_cast<T*>(u0), static_cast<T*>(u1), static_cast<T*>(u2), g, T(volume), status);
+            static_cast<T*>(u0), static_cast<T*>(u1), static_cast<T*>(u2), g, T(volume), status, slots, meta);
+        if ((rc = launched("fe_det_spread boxes"))) return rc;
+        det_box_keys_kernel<<<unsigned(std::min<int64_t>((boxes + 255) / 256, 148 * 32)), 256, 0, s>>>(
+            meta, boxes, t, none, keys_in, vals_in, status);
+        if ((rc = launched("fe_det_spread keys"))) return rc;
+        size_t temp = size_t(L.temp_bytes);
+        if (cub::DeviceRadixSort::SortPairs(base + L.temp, temp, keys_in, keys_out, vals_in, vals_out, int(pairs), 0,
+                                            L.bits, s) != cudaSuccess)
+            return fail(AFSI_ERR_CUDA, "deterministic spread: sort failed");
+        det_box_ranges_kernel<<<unsigned(std::min<int64_t>((pairs + 255) / 256, 148 * 32)), 256, 0, s>>>(
+            keys_out, pairs, none, start, end);
+        if ((rc = launched("fe_det_spread ranges"))) return rc;
+        det_box_reduce_kernel<T><<<unsigned(t.first[3]), kDetBatch * kDetParts, 0, s>>>(slots, meta, vals_out, start,
+                                                                                        end, t, g,
+                                                                      static_cast<T*>(u0), static_cast<T*>(u1),
+                                                                      static_cast<T*>(u2));
+        if ((rc = launched("fe_det_spread reduce"))) return rc;
     });
-    return launched(nodes_per_cell == 10 ? "p2_fused_spread" : "p1_fused_spread");
+    return AFSI_OK;
 }
 
 template <bool Local>

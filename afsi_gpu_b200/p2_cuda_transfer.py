@@ -331,6 +331,9 @@ def _launch_prepare(transfer, x, rule, base, phi, word):
 
 
 def _raise_flags(flags):
+    if flags & _lib.FLAG_OVERFLOW:
+        raise RuntimeError('an element support box exceeds the deterministic table-free spread\'s slot '
+                           '(8 faces per axis); use the table form with deterministic=True')
     if flags & _lib.FLAG_TIMEOUT:
         raise RuntimeError('a P2 transfer gave up waiting for its staged stencil rows')
     if flags & _lib.FLAG_INDEX:
@@ -391,11 +394,15 @@ def _group_tables(transfer, rule):
 
 
 def spread_deterministic(transfer, coefficient, stencil):
-    """:func:`spread` without atomics and bitwise reproducible: point forces
-    (``afsi_b200_p2_point_forces``), then the tile-sorted deterministic spread
-    (``afsi_b200_det_spread``) over the stencil's plan."""
+    """:func:`spread` without atomics and bitwise reproducible.  Tables: point
+    forces (``afsi_b200_p2_point_forces``), then the tile-sorted deterministic
+    spread (``afsi_b200_det_spread``) over the stencil's plan.  Table-free:
+    element boxes in scratch slots reduced per face tile in element order
+    (``afsi_b200_fe_det_spread``)."""
     _lib.require_cuda(coefficient)
     coefficient = coefficient.contiguous()
+    if isinstance(stencil, TableFreeStencil):
+        return _table_free_spread(transfer, coefficient, stencil, deterministic=True)
     if coefficient.dtype != stencil.phi.dtype:
         raise ValueError('P2 spread coefficient dtype must match the stencil weights')
     g = transfer.grid
@@ -453,6 +460,8 @@ def assemble_velocity_deterministic(transfer, velocity, stencil):
     """Same result as :func:`assemble_velocity`, bitwise reproducible: element
     sums are written without atomics, then reduced per node in CSR order."""
     velocity = _velocity(transfer, velocity)
+    if isinstance(stencil, TableFreeStencil):
+        return _table_free_assemble(transfer, velocity, stencil, deterministic=True)
     rule = stencil.rule
     elements = sum(grp.cells.shape[0] for grp in rule.groups)
     local = torch.empty((elements, 10, 3), device=velocity[0].device, dtype=velocity[0].dtype)
@@ -480,31 +489,55 @@ def _geometry(transfer):
     return _lib.doubles(g.origin), _lib.doubles(g.spacing), _lib.doubles([n - 2 for n in g.shape])
 
 
-def _table_free_spread(transfer, coefficient, stencil, events=None):
-    """Spread with the rows formed in the kernel (``afsi_b200_fe_fused_spread``)."""
+def _det_scratch(transfer, rule, dtype, device):
+    """Scratch of the deterministic table-free spread for the largest group
+    of `rule` (kept on the transfer and grown when needed)."""
+    elements = max(grp.cells.shape[0] for grp in rule.groups)
+    n = _lib.load().afsi_b200_fe_det_spread_bytes(elements, *transfer.grid.shape, dtype_code(dtype))
+    if n < 0:
+        raise ValueError('too many elements for the deterministic table-free spread')
+    held = getattr(transfer, '_fe_det', None)
+    if held is None or held.numel() < n or held.device != device:
+        held = torch.empty(int(n), dtype=torch.uint8, device=device)
+        transfer._fe_det = held
+    return held
+
+
+def _table_free_spread(transfer, coefficient, stencil, events=None, deterministic=False):
+    """Spread with the rows formed in the kernel (``afsi_b200_fe_fused_spread``,
+    or ``afsi_b200_fe_det_spread`` in the deterministic form)."""
     x = stencil.x
     if coefficient.dtype != transfer.transfer_dtype:
         raise ValueError('spread coefficient dtype must match the transfer dtype')
     g = transfer.grid
     fields = g.zeros(device=coefficient.device, dtype=coefficient.dtype)
     origin, spacing, limits = _geometry(transfer)
+    scratch = _det_scratch(transfer, stencil.rule, coefficient.dtype, coefficient.device) if deterministic else None
     if events is not None:
         events[0].record()
     for group, (values, weights) in zip(stencil.rule.groups, _group_tables(transfer, stencil.rule)):
-        call('afsi_b200_fe_fused_spread', transfer.nodes_per_cell, ptr(x), x.shape[0], ptr(group.cells),
-             group.cells.shape[0], ptr(group.values), ptr(values), values.shape[0], ptr(weights), ptr(coefficient),
-             origin, spacing, limits, *(ptr(f) for f in fields), *g.shape, float(g.volume), ptr(stencil.status),
-             dtype_code(x.dtype), dtype_code(coefficient.dtype), stream(coefficient.device))
+        args = (transfer.nodes_per_cell, ptr(x), x.shape[0], ptr(group.cells), group.cells.shape[0],
+                ptr(group.values), ptr(values), values.shape[0], ptr(weights), ptr(coefficient), origin, spacing,
+                limits, *(ptr(f) for f in fields), *g.shape, float(g.volume))
+        tail = (ptr(stencil.status), dtype_code(x.dtype), dtype_code(coefficient.dtype), stream(coefficient.device))
+        if deterministic:
+            call('afsi_b200_fe_det_spread', *args, ptr(scratch), scratch.numel(), *tail)
+        else:
+            call('afsi_b200_fe_fused_spread', *args, *tail)
     if events is not None:
         events[1].record()
     return fields
 
 
-def _table_free_assemble(transfer, velocity, stencil, events=None):
-    """Gather-assemble with the rows formed in the kernel (``afsi_b200_fe_fused_gather``)."""
+def _table_free_assemble(transfer, velocity, stencil, events=None, deterministic=False):
+    """Gather-assemble with the rows formed in the kernel (``afsi_b200_fe_fused_gather``;
+    in the deterministic form element sums from ``afsi_b200_fe_fused_gather_local``
+    reduced per node in CSR order)."""
     x = stencil.x
     if velocity[0].dtype != transfer.transfer_dtype:
         raise ValueError('velocity dtype must match the transfer dtype')
+    if deterministic:
+        return _table_free_assemble_local(transfer, velocity, stencil)
     rhs = torch.zeros_like(transfer.diagonal)
     origin, spacing, limits = _geometry(transfer)
     g = transfer.grid
@@ -517,6 +550,28 @@ def _table_free_assemble(transfer, velocity, stencil, events=None):
              dtype_code(x.dtype), dtype_code(rhs.dtype), stream(rhs.device))
     if events is not None:
         events[1].record()
+    return rhs
+
+
+def _table_free_assemble_local(transfer, velocity, stencil):
+    rule = stencil.rule
+    npc = transfer.nodes_per_cell
+    elements = sum(grp.cells.shape[0] for grp in rule.groups)
+    x = stencil.x
+    local = torch.empty((elements, npc, 3), device=velocity[0].device, dtype=velocity[0].dtype)
+    origin, spacing, limits = _geometry(transfer)
+    g = transfer.grid
+    first = 0
+    for group, (values, weights) in zip(rule.groups, _group_tables(transfer, rule)):
+        call('afsi_b200_fe_fused_gather_local', npc, ptr(x), x.shape[0], ptr(group.cells), group.cells.shape[0],
+             ptr(group.values), ptr(values), values.shape[0], ptr(weights), *(ptr(v) for v in velocity), origin,
+             spacing, limits, local[first:].data_ptr(), *g.shape, ptr(stencil.status), dtype_code(x.dtype),
+             dtype_code(local.dtype), stream(local.device))
+        first += group.cells.shape[0]
+    crow, slot = transfer.node_csr(rule)
+    rhs = torch.empty_like(transfer.diagonal)
+    call('afsi_b200_node_reduce', ptr(local), elements * npc, ptr(crow), ptr(slot), rhs.shape[0], ptr(rhs), 0,
+         ptr(stencil.status), dtype_code(rhs.dtype), stream(rhs.device))
     return rhs
 
 
@@ -540,10 +595,4 @@ class P1Transfer(P2Transfer):
 
     prepare_deferred = P2Transfer.prepare_table_free
 
-    def spread(self, coefficient, stencil):
-        return spread(self, coefficient, stencil)
-
-    def assemble_velocity(self, velocity, stencil):
-        return assemble_velocity(self, velocity, stencil)
-
-    interpolate_rhs = assemble_velocity
+    interpolate_rhs = P2Transfer.assemble_velocity

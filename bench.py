@@ -851,23 +851,31 @@ def table_form_row(grid, X, cells, coef, vel, rhs, device, steps, warmup, pk):
     return out
 
 
-def deterministic_row(step, coef, device, reps=10):
-    """The P2 spread of the step in its deterministic mode (tile-sorted,
-    atomic-free, bitwise reproducible) beside the atomic spread: CUDA events
-    around `reps` spreads each (the plan is built once per stencil, outside
-    the timing), and the largest difference between the two."""
+def deterministic_row(step, coef, vel, device, reps=10):
+    """The P2 transfers of the step in their deterministic modes (atomic-free,
+    bitwise reproducible) beside the atomic ones, CUDA events around `reps`
+    calls each.  Table form: the spread over the stencil tables, tile-sorted
+    (the plan is built once per stencil, outside the timing).  Table-free
+    form: the spread with element boxes in scratch slots reduced per face
+    tile in element order, and the gather-assemble with element sums reduced
+    per node.  Each deterministic output is computed twice (bitwise equal)
+    and compared with the atomic one."""
     from afsi_gpu_b200 import p2_cuda_transfer as p2t
     tr = step.tr
     st = tr.prepare(step.x)
+    free = tr.confirm(tr.prepare_table_free(step.x))
     c = torch.as_tensor(coef, device=device)
+    v = tuple(torch.as_tensor(x, device=device) for x in vel)
     det = p2t.P2Transfer(step.grid, step.x, step.cells, deterministic=True)
     det.rules = tr.rules
-    a = tr.spread(c, st)
-    d = det.spread(c, st)
-    again = det.spread(c, st)
     stream = torch.cuda.current_stream(device)
     out = {}
-    for name, fn in (('atomic', lambda: tr.spread(c, st)), ('deterministic', lambda: det.spread(c, st))):
+    runs = (('atomic', lambda: tr.spread(c, st)), ('deterministic', lambda: det.spread(c, st)),
+            ('table_free_atomic', lambda: tr.spread(c, free)), ('table_free_deterministic', lambda: det.spread(c, free)),
+            ('gather_table_free_atomic', lambda: tr.assemble_velocity(v, free)),
+            ('gather_table_free_deterministic', lambda: det.assemble_velocity(v, free)))
+    for name, fn in runs:
+        ref, first, second = None, fn(), fn()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize(device)
         e0.record(stream)
@@ -876,8 +884,17 @@ def deterministic_row(step, coef, device, reps=10):
         e1.record(stream)
         torch.cuda.synchronize(device)
         out[f'{name}_ms'] = e0.elapsed_time(e1) / reps
-    out['bitwise_reproducible'] = all(torch.equal(x, y) for x, y in zip(d, again))
-    out['max_rel_diff_vs_atomic'] = max(float((x - y).abs().max() / y.abs().max()) for x, y in zip(d, a))
+        out.setdefault('_outputs', {})[name] = (first, second)
+    tr.check(free)
+    det.check(free)
+    outs = out.pop('_outputs')
+    as_list = lambda o: list(o) if isinstance(o, (tuple, list)) else [o]
+    for name, ref in (('deterministic', 'atomic'), ('table_free_deterministic', 'table_free_atomic'),
+                      ('gather_table_free_deterministic', 'gather_table_free_atomic')):
+        d, again = (as_list(o) for o in outs[name])
+        a = as_list(outs[ref][0])
+        out[f'{name}_bitwise_reproducible'] = all(torch.equal(x, y) for x, y in zip(d, again))
+        out[f'{name}_max_rel_diff_vs_atomic'] = max(float((x - y).abs().max() / y.abs().max()) for x, y in zip(d, a))
     return out
 
 
@@ -1240,7 +1257,7 @@ def run_b200(args):
         precision = precision_form_row(grid, X, cells, coef, vel, rhs, device, oracle_out) if extra else None
         if extra:
             precision['p1_128'] = precision_p1_row(device)
-        deterministic = deterministic_row(step, coef, device) if extra else None
+        deterministic = deterministic_row(step, coef, vel, device) if extra else None
         tables = table_form_row(grid, X, cells, coef, vel, rhs, device, args.steps, args.warmup, pk) if extra else None
         batch = batch_form_row(device) if extra else None
         config1 = config1_row(device) if extra else None

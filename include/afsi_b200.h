@@ -598,6 +598,29 @@ int32_t afsi_b200_fe_fused_spread(int32_t nodes_per_cell, const void* x, int64_t
     int64_t elements, const void* N_pos, const void* N, int64_t nq, const void* W, const void* value,
     const double* origin, const double* spacing, const double* limits, void* u0, void* u1, void* u2, int64_t nx,
     int64_t ny, int64_t nz, double volume, int32_t* status, int32_t pos_dtype, int32_t dtype, afsi_stream_t stream);
+/* Deterministic table-free spread (no counterpart in the reference, whose
+ * spreads add atomically): afsi_b200_fe_fused_spread's arithmetic up to the
+ * element boxes (each accumulated in a fixed order), but a box is written to
+ * its own scratch slot instead of being added to the face arrays with L2
+ * reductions.  The boxes are then keyed by the 4x4x4 face tiles they overlap
+ * and stably sorted by tile, and one CTA per tile adds, face by face, the
+ * covering boxes' entries to u0/u1/u2 in an order fixed by the tile's sorted
+ * box list (four element-ordered partial sums, added in turn).  No atomics: the
+ * result is bitwise the same on every run and equals
+ * afsi_b200_fe_fused_spread's to rounding.  scratch:
+ * afsi_b200_fe_det_spread_bytes(elements, nx, ny, nz, dtype) device bytes
+ * (one 512-entry slot per element and component, the tile keys and the sort
+ * temporary), -1 when out of range (elements * 81 must stay below 2^31).  An
+ * element whose box exceeds its slot (an extent above 8 faces on an axis, or
+ * a padded shared-memory box above 640 entries) sets AFSI_FLAG_OVERFLOW and
+ * contributes nothing; the other status bits as for
+ * afsi_b200_fe_fused_spread. */
+int64_t afsi_b200_fe_det_spread_bytes(int64_t elements, int64_t nx, int64_t ny, int64_t nz, int32_t dtype);
+int32_t afsi_b200_fe_det_spread(int32_t nodes_per_cell, const void* x, int64_t nodes, const int64_t* cells,
+    int64_t elements, const void* N_pos, const void* N, int64_t nq, const void* W, const void* value,
+    const double* origin, const double* spacing, const double* limits, void* u0, void* u1, void* u2, int64_t nx,
+    int64_t ny, int64_t nz, double volume, void* scratch, int64_t scratch_bytes, int32_t* status,
+    int32_t pos_dtype, int32_t dtype, afsi_stream_t stream);
 int32_t afsi_b200_fe_fused_gather(int32_t nodes_per_cell, const void* x, int64_t nodes, const int64_t* cells,
     int64_t elements, const void* N_pos, const void* N, int64_t nq, const void* W, const void* u0, const void* u1,
     const void* u2, const double* origin, const double* spacing, const double* limits, void* rhs, int64_t nx,

@@ -193,3 +193,62 @@ def test_deferred_flags_are_read_from_the_pinned_copy():
     tr.note_transfers(bad)
     with pytest.raises(ValueError, match='support'):
         tr.confirm(bad)
+
+
+@pytest.mark.parametrize('kind', ['p2', 'p1'])
+def test_deterministic_table_free_transfers_are_reproducible(kind):
+    """The deterministic table-free forms use no atomics.  The spread writes
+    each element's box to a scratch slot and reduces the boxes per 8x8x8 face
+    tile in element order.  The gather-assemble writes element sums and
+    reduces them per node.  Two runs are bitwise equal.  They match the
+    atomic table-free forms within 1e-14 of the scale and the FP64 oracle
+    within 1e-12.  P2 uses rules of several orders; P1 uses rules of more
+    than 64 points, so the kernels' chunked path runs too."""
+    if kind == 'p2':
+        X, cells = synthetic.p2_shell(2, 12, 16, inner=(.125, .075, .075), outer=(.16, .11, .11))
+        grid = MACGrid((64, 64, 64), (1., 1., 1.))
+        cls, kw = p2t.P2Transfer, dict(max_order=22)
+    else:
+        X, cells = synthetic.prolate_shell(2, 10, 16, inner=(.125, .075, .075), outer=(.16, .11, .11))
+        grid = MACGrid((32, 32, 32), (1., 1., 1.))
+        cls, kw = p2t.P1Transfer, dict(point_density=6., max_order=12)
+    Xd = t(X)
+    det = cls(grid, Xd, t(cells), deterministic=True, **kw)
+    atomic = cls(grid, Xd, t(cells), **kw)
+    st = det.confirm(det.prepare_table_free(Xd))
+    assert isinstance(st, p2t.TableFreeStencil) and len(st.rule.groups) > 1
+    rng = np.random.default_rng(21)
+    coef = t(rng.standard_normal((X.shape[0], 3)))
+    vel = tuple(v.to(DEV) for v in synthetic.fourier_velocity3d(grid, seed=5))
+    f1, f2 = det.spread(coef, st), det.spread(coef, st)
+    r1, r2 = det.assemble_velocity(vel, st), det.assemble_velocity(vel, st)
+    det.check(st)
+    fa, ra = atomic.spread(coef, st), atomic.assemble_velocity(vel, st)
+    atomic.check(st)
+    full = [(gr.cells.cpu().numpy(), gr.values.cpu().numpy(), gr.weights.cpu().numpy()) for gr in st.rule.groups]
+    ob, op, invalid = oracle.p2_prepare(X, [(c, N) for c, N, _ in full], grid.origin, grid.spacing, grid.shape)
+    assert invalid == 0
+    ref_f = oracle.p2_spread(coef.cpu().numpy(), full, ob, op, grid.shape, grid.volume)
+    ref_r = oracle.p2_gather_assemble([v.cpu().numpy() for v in vel], full, ob, op, grid.shape, X.shape[0])
+    for c in range(3):
+        assert torch.equal(f1[c], f2[c])
+        close(f1[c], fa[c].cpu().numpy(), 1e-14)
+        close(f1[c], ref_f[c], 1e-12)
+    assert torch.equal(r1, r2)
+    close(r1, ra.cpu().numpy(), 1e-14)
+    close(r1, ref_r, 1e-12)
+
+
+def test_deterministic_spread_reports_boxes_beyond_its_slots():
+    """Elements of a coarse shell on a 128^3 grid span more than 8 faces per
+    axis, beyond the deterministic spread's slots: they set the overflow
+    flag (no trap, finite fields) and check raises."""
+    X, cells = synthetic.p2_shell(1, 6, 8, inner=(.125, .075, .075), outer=(.16, .11, .11))
+    grid = MACGrid((128, 128, 128), (1., 1., 1.))
+    Xd = t(X)
+    det = p2t.P2Transfer(grid, Xd, t(cells), deterministic=True, max_order=26)
+    st = det.confirm(det.prepare_table_free(Xd))
+    fields = det.spread(t(np.ones((X.shape[0], 3))), st)
+    assert all(torch.isfinite(f).all() for f in fields)
+    with pytest.raises(RuntimeError, match='deterministic'):
+        det.check(st)
