@@ -47,14 +47,15 @@ def parse():
                     help="transfer form of the headline step: 'table-free' (the transfer kernels form the stencil "
                          "rows) or 'tables' (the prepare writes the stencil tables; for profiler runs of the table "
                          "kernels)")
-    ap.add_argument('--rows', default='all', choices=('all', 'step', 'p1', 'batch', 'p1free', 'stokes'),
+    ap.add_argument('--rows', default='all', choices=('all', 'step', 'p1', 'batch', 'p1free', 'stokes', 'det'),
                     help="'step': the headline step line only, without the mass-solve, MG-form, batching and "
                          "serving rows (for profiler runs); 'p1': only the precision-form row on the 128^3 P1 "
                          "configuration, printed as its own JSON object (for profiler runs); 'batch': only "
                          "`--steps` replays of the refined batch step after `--warmup`, summarised as JSON "
                          "(for profiler runs); 'p1free': `--steps` matrix-free P1 steps of the 128^3 "
                          "configuration (FP64 transfers, FP64 V-cycles); 'stokes': `--steps` FGMRES Stokes "
-                         "solves of the 64^3 row (for profiler runs)")
+                         "solves of the 64^3 row (for profiler runs); 'det': the deterministic-transfer row of "
+                         "the headline workload with `--steps` calls of each form (for profiler runs)")
     return ap.parse_args()
 
 
@@ -1374,6 +1375,14 @@ def stokes_only(args):
                           ms_per_solve=(time.perf_counter() - t0) * 1e3 / max(args.steps, 1))))
 
 
+def det_only(args):
+    """The deterministic-transfer row of the headline workload, alone."""
+    device = torch.device('cuda', torch.cuda.current_device())
+    grid, X, cells, coef, vel, rhs = workload()
+    step = Step(grid, X, cells, coef, vel, rhs, device)
+    print(json.dumps(deterministic_row(step, coef, vel, device, reps=max(args.steps, 1)), default=_json))
+
+
 def main():
     args = parse()
     if args.impl == 'reference':
@@ -1384,6 +1393,8 @@ def main():
         p1free_only(args)
     elif args.rows == 'stokes':
         stokes_only(args)
+    elif args.rows == 'det':
+        det_only(args)
     elif args.rows == 'p1':
         print(json.dumps(precision_p1_row(torch.device('cuda', torch.cuda.current_device())), default=_json))
     else:
