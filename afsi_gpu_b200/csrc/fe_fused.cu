@@ -449,7 +449,8 @@ __global__ void __launch_bounds__(kFWarps * 32, 8) fused_spread_kernel(
 // The element boxes (fused_spread_kernel<..., true>) are added to the face
 // arrays in a fixed order per face: every box names the 4x4x4 face tiles it
 // overlaps (at most three per axis), the (tile, box) pairs are sorted by tile
-// with a stable radix sort (boxes of a tile stay in box order), and one CTA
+// with a stable radix sort (a tile's boxes stay in the order of their key
+// slots, a function of the boxes alone), and one CTA
 // per tile adds, face by face, the covering boxes' entries in an order fixed
 // by that list (det_box_reduce_kernel).  Small tiles keep the box list short:
 // on a shell, 8x8x8 tiles put up to about 5000 boxes in one tile.  No
@@ -477,8 +478,10 @@ inline DetTiles det_tiles(int64_t nx, int64_t ny, int64_t nz) {
     return t;
 }
 
-// Keys of box b: the ids of the tiles it overlaps, then `none`; a box that
-// spans more than three tiles along an axis sets AFSI_FLAG_OVERFLOW.
+// Keys of box b: the ids of the tiles it overlaps, then `none`, stored
+// slot-major (key j of box b at j * boxes + b, so the stores of a warp are
+// contiguous); a box that spans more than three tiles along an axis sets
+// AFSI_FLAG_OVERFLOW.
 __global__ void det_box_keys_kernel(const int32_t* __restrict__ meta, int64_t boxes, DetTiles t, uint32_t none,
                                     uint32_t* __restrict__ keys, int32_t* __restrict__ vals, int32_t* status) {
     for (int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; b < boxes; b += int64_t(gridDim.x) * blockDim.x) {
@@ -487,8 +490,6 @@ __global__ void det_box_keys_kernel(const int32_t* __restrict__ meta, int64_t bo
         const int64_t first = c == 2 ? t.first[2] : c == 1 ? t.first[1] : t.first[0];
         const int64_t n1 = c == 2 ? t.n[2][1] : c == 1 ? t.n[1][1] : t.n[0][1];
         const int64_t n2 = c == 2 ? t.n[2][2] : c == 1 ? t.n[1][2] : t.n[0][2];
-        uint32_t* kb = keys + b * kDetKeys;
-        int32_t* vb = vals + b * kDetKeys;
         int j = 0;
         if (m[3] > 0) {
             int lo[3], hi[3];
@@ -503,8 +504,8 @@ __global__ void det_box_keys_kernel(const int32_t* __restrict__ meta, int64_t bo
                 for (int i = lo[0]; i <= hi[0]; ++i)
                     for (int jy = lo[1]; jy <= hi[1]; ++jy)
                         for (int kz = lo[2]; kz <= hi[2]; ++kz) {
-                            kb[j] = uint32_t(first + (int64_t(i) * n1 + jy) * n2 + kz);
-                            vb[j] = int32_t(b);
+                            keys[j * boxes + b] = uint32_t(first + (int64_t(i) * n1 + jy) * n2 + kz);
+                            vals[j * boxes + b] = int32_t(b);
                             ++j;
                         }
             } else {
@@ -512,8 +513,8 @@ __global__ void det_box_keys_kernel(const int32_t* __restrict__ meta, int64_t bo
             }
         }
         for (; j < kDetKeys; ++j) {
-            kb[j] = none;
-            vb[j] = int32_t(b);
+            keys[j * boxes + b] = none;
+            vals[j * boxes + b] = int32_t(b);
         }
     }
 }

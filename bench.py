@@ -176,9 +176,12 @@ class Step:
         nodal = self.p2t.assemble_velocity(self.tr, vel, st, events=None if ev is None else ev[7:9])
         if ev is not None:
             ev[3].record()
-        p, info = self.mg.solve(self.rhs if rhs is None else rhs)
+        # the solve is queued without its host read (GeometricMultigrid.solve_deferred, as the
+        # end-to-end loop runs it), so the step's end event marks the end of the device work
+        pending = self.mg.solve_deferred(self.rhs if rhs is None else rhs)
         if ev is not None:
             ev[4].record()
+        p, info = pending.result()
         confirmed = self.tr.confirm(deferred)
         if confirmed is not st:
             st = confirmed
