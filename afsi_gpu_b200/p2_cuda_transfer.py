@@ -397,7 +397,7 @@ def spread_deterministic(transfer, coefficient, stencil):
     """:func:`spread` without atomics and bitwise reproducible.  Tables: point
     forces (``afsi_b200_p2_point_forces``), then the tile-sorted deterministic
     spread (``afsi_b200_det_spread``) over the stencil's plan.  Table-free:
-    element boxes in scratch slots reduced per face tile in element order
+    element boxes in scratch slots reduced per face tile in a fixed order
     (``afsi_b200_fe_det_spread``)."""
     _lib.require_cuda(coefficient)
     coefficient = coefficient.contiguous()

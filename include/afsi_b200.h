@@ -605,7 +605,7 @@ int32_t afsi_b200_fe_fused_spread(int32_t nodes_per_cell, const void* x, int64_t
  * reductions.  The boxes are then keyed by the 4x4x4 face tiles they overlap
  * and stably sorted by tile, and one CTA per tile adds, face by face, the
  * covering boxes' entries to u0/u1/u2 in an order fixed by the tile's sorted
- * box list (four element-ordered partial sums, added in turn).  No atomics: the
+ * box list (four partial sums over that list, added in turn).  No atomics: the
  * result is bitwise the same on every run and equals
  * afsi_b200_fe_fused_spread's to rounding.  scratch:
  * afsi_b200_fe_det_spread_bytes(elements, nx, ny, nz, dtype) device bytes

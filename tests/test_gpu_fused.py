@@ -199,7 +199,7 @@ def test_deferred_flags_are_read_from_the_pinned_copy():
 def test_deterministic_table_free_transfers_are_reproducible(kind):
     """The deterministic table-free forms use no atomics.  The spread writes
     each element's box to a scratch slot and reduces the boxes per 8x8x8 face
-    tile in element order.  The gather-assemble writes element sums and
+    tile in a fixed order.  The gather-assemble writes element sums and
     reduces them per node.  Two runs are bitwise equal.  They match the
     atomic table-free forms within 1e-14 of the scale and the FP64 oracle
     within 1e-12.  P2 uses rules of several orders; P1 uses rules of more
