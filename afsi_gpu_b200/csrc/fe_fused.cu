@@ -341,18 +341,22 @@ __device__ __forceinline__ void component_keys(FStage<TP, T, NPC, Cap>& s, int n
 constexpr int kDetSlot = kDetExt * kDetExt * kDetExt;
 constexpr int kDetMeta = 8;
 
-// Boxes: instead of adding each element's box to the face arrays with L2
-// reductions, write it to its slot (plain stores); the box may then take
-// kDetBoxCap padded entries with extents up to kDetExt, and an element whose
-// box does not fit sets AFSI_FLAG_OVERFLOW and contributes nothing.
-template <class TP, class T, int NPC, bool Boxes>
+// Mode 0: each element's box is added to the face arrays with L2
+// reductions.  Modes 1 and 2 write it to its slot instead (plain stores), with
+// extents up to kDetExt: mode 1 with the padded box of mode 0 (kFBoxCap
+// entries, the same occupancy), queueing each (element, component) box that
+// does not fit as e * 3 + c in `queue`; mode 2 takes only the queued boxes,
+// with kDetBoxCap entries, and a box that still does not fit sets
+// AFSI_FLAG_OVERFLOW and contributes nothing.
+template <class TP, class T, int NPC, int Mode>
 __global__ void __launch_bounds__(kFWarps * 32, 8) fused_spread_kernel(
     const TP* __restrict__ x, const int64_t* __restrict__ cells, const TP* __restrict__ Npos,
     const T* __restrict__ N, const T* __restrict__ W, const T* __restrict__ value, Geo<TP> geo, T* __restrict__ u0,
     T* __restrict__ u1, T* __restrict__ u2, FusedDims g, T volume, int32_t* status, T* __restrict__ slots,
-    int32_t* __restrict__ meta) {
+    int32_t* __restrict__ meta, int32_t* __restrict__ queue, int32_t* __restrict__ queued) {
     extern __shared__ __align__(16) unsigned char fused_smem[];
-    constexpr int Cap = Boxes ? kDetBoxCap : kFBoxCap;
+    constexpr bool Boxes = Mode != 0;
+    constexpr int Cap = Mode == 2 ? kDetBoxCap : kFBoxCap;
     FStage<TP, T, NPC, Cap>& s = reinterpret_cast<FStage<TP, T, NPC, Cap>*>(fused_smem)[threadIdx.x >> 5];
     constexpr int C = FChunk<NPC>::value;
     const int lane = threadIdx.x & 31, half = lane >> 4, li = (lane >> 2) & 3, lj = lane & 3;
@@ -362,13 +366,17 @@ __global__ void __launch_bounds__(kFWarps * 32, 8) fused_spread_kernel(
     if (lane < 12) s.w[C * 12 + lane] = T(0);
     if (lane == 0) s.f[C] = T(0);
     __syncwarp();
-    for (int64_t e = int64_t(blockIdx.x) * kFWarps + (threadIdx.x >> 5); e < g.elements; e += warps) {
+    const int64_t items = Mode == 2 ? int64_t(*queued) : g.elements;
+    for (int64_t it = int64_t(blockIdx.x) * kFWarps + (threadIdx.x >> 5); it < items; it += warps) {
+        const int64_t e = Mode == 2 ? int64_t(queue[it]) / 3 : it;
+        const int only = Mode == 2 ? queue[it] % 3 : -1;
         int64_t node;
         if (!stage_element<TP, T, NPC>(x, cells, value, e, g.nodes, s.xs, s.coef, node, status)) continue;
         const unsigned long long valid =
             resident ? resident_positions<TP, NPC>(s, Npos, int(g.nq), geo, status) : 0ull;
 #pragma unroll 1
         for (int c = 0; c < 3; ++c) {
+            if (Mode == 2 && c != only) continue;
             T* field = c == 0 ? u0 : c == 1 ? u1 : u2;
             FBox bx;
             bool any = true;
@@ -397,7 +405,10 @@ __global__ void __launch_bounds__(kFWarps * 32, 8) fused_spread_kernel(
                 __syncwarp();
                 if (fits) {
                     spread_element<T, C>(s.box, s.key, s.f, s.w, s.w + 4, s.w + 8, n, sx, sy, s.perm, s.rs, s.rk);
-                } else if (Boxes) {
+                } else if (Mode == 1) {
+                    if (lane == 0) queue[atomicAdd(queued, 1)] = int32_t(e * 3 + c);
+                    break;
+                } else if (Mode == 2) {
                     if (lane == 0) flag(status, AFSI_FLAG_OVERFLOW);
                     break;
                 } else {
@@ -602,7 +613,7 @@ __global__ void __launch_bounds__(kDetBatch * kDetParts) det_box_reduce_kernel(
 // Scratch of the deterministic table-free spread of `elements` elements:
 // slots, meta, keys and values (in and out), tile ranges, sort temporary.
 struct DetBoxLayout {
-    int64_t slots, meta, keys_in, keys_out, vals_in, vals_out, start, end, temp, temp_bytes, bytes;
+    int64_t slots, meta, keys_in, keys_out, vals_in, vals_out, start, end, queue, queued, temp, temp_bytes, bytes;
     int bits;
 };
 
@@ -634,6 +645,10 @@ inline DetBoxLayout det_box_layout(int64_t elements, const DetTiles& t, int64_t 
     off = det_align(off + t.first[3] * 4);
     L.end = off;
     off = det_align(off + t.first[3] * 4);
+    L.queue = off;
+    off = det_align(off + boxes * 4);
+    L.queued = off;
+    off = det_align(off + 4);
     L.bits = det_key_bits(t.first[3]);
     size_t temp = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, temp, static_cast<const uint32_t*>(nullptr),
@@ -868,15 +883,16 @@ extern "C" int32_t afsi_b200_fe_fused_spread(int32_t nodes_per_cell, const void*
         const size_t smem = sizeof(FStage<TP, T, NPC>) * kFWarps;
         static bool configured = false;  // once per instantiation, before any graph capture of it
         if (!configured) {
-            cudaFuncSetAttribute(fused_spread_kernel<TP, T, NPC, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            cudaFuncSetAttribute(fused_spread_kernel<TP, T, NPC, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(smem));
             configured = true;
         }
-        fused_spread_kernel<TP, T, NPC, false><<<fused_blocks(elements, kFWarps), kFWarps * 32, smem, s>>>(
+        fused_spread_kernel<TP, T, NPC, 0><<<fused_blocks(elements, kFWarps), kFWarps * 32, smem, s>>>(
             static_cast<const TP*>(x), cells, static_cast<const TP*>(N_pos), static_cast<const T*>(N),
             static_cast<const T*>(W), static_cast<const T*>(value), make_geo<TP>(origin, spacing, limits),
             static_cast<T*>(u0), static_cast<T*>(u1), static_cast<T*>(u2), g, T(volume), status,
-            static_cast<T*>(nullptr), static_cast<int32_t*>(nullptr));
+            static_cast<T*>(nullptr), static_cast<int32_t*>(nullptr), static_cast<int32_t*>(nullptr),
+            static_cast<int32_t*>(nullptr));
     });
     return launched(nodes_per_cell == 10 ? "p2_fused_spread" : "p1_fused_spread");
 }
@@ -924,22 +940,36 @@ extern "C" int32_t afsi_b200_fe_det_spread(int32_t nodes_per_cell, const void* x
         int32_t* vals_out = reinterpret_cast<int32_t*>(base + L.vals_out);
         int32_t* start = reinterpret_cast<int32_t*>(base + L.start);
         int32_t* end = reinterpret_cast<int32_t*>(base + L.end);
+        int32_t* queue = reinterpret_cast<int32_t*>(base + L.queue);
+        int32_t* queued = reinterpret_cast<int32_t*>(base + L.queued);
         if (cudaMemsetAsync(meta, 0, size_t(boxes) * kDetMeta * 4, s) != cudaSuccess ||
             cudaMemsetAsync(start, 0, size_t(t.first[3]) * 4, s) != cudaSuccess ||
-            cudaMemsetAsync(end, 0, size_t(t.first[3]) * 4, s) != cudaSuccess)
+            cudaMemsetAsync(end, 0, size_t(t.first[3]) * 4, s) != cudaSuccess ||
+            cudaMemsetAsync(queued, 0, 4, s) != cudaSuccess)
             return fail(AFSI_ERR_CUDA, "deterministic spread: clearing the scratch failed");
-        const size_t smem = sizeof(FStage<TP, T, NPC, kDetBoxCap>) * kFWarps;
+        const Geo<TP> geo = make_geo<TP>(origin, spacing, limits);
+        const size_t smem1 = sizeof(FStage<TP, T, NPC, kFBoxCap>) * kFWarps;
+        const size_t smem2 = sizeof(FStage<TP, T, NPC, kDetBoxCap>) * kFWarps;
         static bool configured = false;  // once per instantiation, before any graph capture of it
         if (!configured) {
-            cudaFuncSetAttribute(fused_spread_kernel<TP, T, NPC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(smem));
+            cudaFuncSetAttribute(fused_spread_kernel<TP, T, NPC, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(smem1));
+            cudaFuncSetAttribute(fused_spread_kernel<TP, T, NPC, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(smem2));
             configured = true;
         }
-        fused_spread_kernel<TP, T, NPC, true><<<fused_blocks(elements, kFWarps), kFWarps * 32, smem, s>>>(
+        fused_spread_kernel<TP, T, NPC, 1><<<fused_blocks(elements, kFWarps), kFWarps * 32, smem1, s>>>(
             static_cast<const TP*>(x), cells, static_cast<const TP*>(N_pos), static_cast<const T*>(N),
-            static_cast<const T*>(W), static_cast<const T*>(value), make_geo<TP>(origin, spacing, limits),
-            static_cast<T*>(u0), static_cast<T*>(u1), static_cast<T*>(u2), g, T(volume), status, slots, meta);
+            static_cast<const T*>(W), static_cast<const T*>(value), geo, static_cast<T*>(u0), static_cast<T*>(u1),
+            static_cast<T*>(u2), g, T(volume), status, slots, meta, queue, queued);
         if ((rc = launched("fe_det_spread boxes"))) return rc;
+        // the boxes that did not fit the first pass's shared-memory box (none on most shells)
+        fused_spread_kernel<TP, T, NPC, 2><<<unsigned(std::min<int64_t>(fused_blocks(elements, kFWarps), 148 * 4)),
+                                             kFWarps * 32, smem2, s>>>(
+            static_cast<const TP*>(x), cells, static_cast<const TP*>(N_pos), static_cast<const T*>(N),
+            static_cast<const T*>(W), static_cast<const T*>(value), geo, static_cast<T*>(u0), static_cast<T*>(u1),
+            static_cast<T*>(u2), g, T(volume), status, slots, meta, queue, queued);
+        if ((rc = launched("fe_det_spread large boxes"))) return rc;
         det_box_keys_kernel<<<unsigned(std::min<int64_t>((boxes + 255) / 256, 148 * 32)), 256, 0, s>>>(
             meta, boxes, t, none, keys_in, vals_in, status);
         if ((rc = launched("fe_det_spread keys"))) return rc;

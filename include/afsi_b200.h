@@ -614,7 +614,8 @@ int32_t afsi_b200_fe_fused_spread(int32_t nodes_per_cell, const void* x, int64_t
  * element whose box exceeds its slot (an extent above 8 faces on an axis, or
  * a padded shared-memory box above 640 entries) sets AFSI_FLAG_OVERFLOW and
  * contributes nothing; the other status bits as for
- * afsi_b200_fe_fused_spread. */
+ * afsi_b200_fe_fused_spread.  Boxes of up to 288 padded entries take a first
+ * pass at the atomic spread's occupancy, larger ones a second launch. */
 int64_t afsi_b200_fe_det_spread_bytes(int64_t elements, int64_t nx, int64_t ny, int64_t nz, int32_t dtype);
 int32_t afsi_b200_fe_det_spread(int32_t nodes_per_cell, const void* x, int64_t nodes, const int64_t* cells,
     int64_t elements, const void* N_pos, const void* N, int64_t nq, const void* W, const void* value,
