@@ -457,16 +457,16 @@ __global__ void __launch_bounds__(kFWarps * 32, 8) fused_spread_kernel(
 
 // ------------------------------------------------- deterministic reduction
 //
-// The element boxes (fused_spread_kernel<..., true>) are added to the face
-// arrays in a fixed order per face: every box names the 4x4x4 face tiles it
-// overlaps (at most three per axis), the (tile, box) pairs are sorted by tile
-// with a stable radix sort (a tile's boxes stay in the order of their key
-// slots, a function of the boxes alone), and one CTA
-// per tile adds, face by face, the covering boxes' entries in an order fixed
-// by that list (det_box_reduce_kernel).  Small tiles keep the box list short:
-// on a shell, 8x8x8 tiles put up to about 5000 boxes in one tile.  No
-// atomics: the result is bitwise the same on every run, and equals the
-// L2-reduction spread to rounding.
+// The element boxes (fused_spread_kernel modes 1 and 2) are added to the
+// face arrays in a fixed order per face: every box names the 4x4x4 face
+// tiles it overlaps (at most three per axis), the (tile, box) pairs are
+// sorted by tile with a stable radix sort (a tile's boxes stay in the order
+// of their key slots, a function of the boxes alone), and one CTA per tile
+// adds, face by face, the covering boxes' entries in an order fixed by that
+// list (det_box_reduce_kernel).  Small tiles keep the box list short: on a
+// shell, 8x8x8 tiles put up to about 5000 boxes in one tile.  No atomics:
+// the result is bitwise the same on every run, and equals the L2-reduction
+// spread to rounding.
 
 constexpr int kDetTile = 4;
 constexpr int kDetKeys = 27;  // tile keys per box
