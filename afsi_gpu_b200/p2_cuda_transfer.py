@@ -171,11 +171,12 @@ class P2Transfer:
         support / connectivity flags of the transfers that used it."""
         _lib.require_cuda(x)
         x = x.contiguous()
-        status = torch.zeros((), dtype=torch.int32, device=x.device)
         last = self.rules.last
         if last is None:
+            status = torch.zeros((), dtype=torch.int32, device=x.device)
             return DeferredStencil(TableFreeStencil(x, self.rules(x), status), x, None, None, None)
         orders, summary = self.rules.launch(x)
+        status = summary[-1]  # the summary's spare slot, zeroed with it, takes the transfers' flags
         host = torch.empty(summary.shape, dtype=summary.dtype, pin_memory=True)
         host.copy_(summary, non_blocking=True)
         ready = torch.cuda.Event()

@@ -140,8 +140,7 @@ class RuleBuilder:
         x = x.contiguous()
         E = self.cells.shape[0]
         orders = torch.empty(E, dtype=torch.int64, device=x.device)
-        summary = torch.empty(4 + self.bins, dtype=torch.int32, device=x.device)
-        summary[-1:].zero_()
+        summary = torch.zeros(4 + self.bins, dtype=torch.int32, device=x.device)
         last = None if self._last is None else self._last.orders
         _lib.call('afsi_b200_p2_orders' if self.p2 else 'afsi_b200_p1_orders', _lib.ptr(x), x.shape[0],
                   _lib.ptr(self.cells), E, float(min(self.grid.spacing)), self.density, self.min_order,
