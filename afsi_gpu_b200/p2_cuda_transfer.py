@@ -486,8 +486,13 @@ def assemble_velocity_deterministic(transfer, velocity, stencil):
 # ------------------------------------------------------------ table-free form
 
 def _geometry(transfer):
-    g = transfer.grid
-    return _lib.doubles(g.origin), _lib.doubles(g.spacing), _lib.doubles([n - 2 for n in g.shape])
+    """origin, spacing and support limits as ctypes arrays (made once per transfer)."""
+    geo = getattr(transfer, '_geo', None)
+    if geo is None:
+        g = transfer.grid
+        geo = _lib.doubles(g.origin), _lib.doubles(g.spacing), _lib.doubles([n - 2 for n in g.shape])
+        transfer._geo = geo
+    return geo
 
 
 def _det_scratch(transfer, rule, dtype, device):
